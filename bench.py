@@ -1,0 +1,389 @@
+#!/usr/bin/env python3
+"""Benchmark: maximal cliques per second (exact count) on one B200.
+
+Workloads (synthetic, seeded; the reference's public datasets are not
+available here):
+  batch  (default) 4,096 independent Chung-Lu graphs, seed 11, n log-uniform in
+         [64, 16384], exponent 2.3, mean degree U[8, 32], 0-5 planted cliques
+         of size U[5, 40]; counted in one pass over their disjoint union.
+  rmat   R-MAT (0.57, 0.19, 0.19, 0.05), edge factor 16, seed 7, at --scale
+         (default 15).  The configuration's scale 22 is infeasible for any
+         exact enumerator: the count grows 4-15x per scale step.
+  ba     Barabasi-Albert n = 4,000,000, m = 8, seed 23, + 200 overlapping
+         planted cliques of size U[20, 60].
+  er     Erdos-Renyi G(10000, 0.002), seed 1, + 20 planted cliques U[6, 12].
+
+One step = peel + orient + search over the whole workload with the graph
+resident in HBM (`value`), or through the public API with the CSR copied
+from pinned host memory and the count read back inside the timed region
+(`e2e`).  `--impl reference` times the reference implementation (its CUDA
+binary built from source into oracle/_ref) on the same workload.
+"""
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "mce-gpu_b200"))
+
+METRIC = "maximal cliques/s (exact count), batched+learned vs plain on 1 B200; p99 ms"
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "parallel_mce_on_gpus")
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["mine", "reference"], default="mine")
+    p.add_argument("--workload", choices=["batch", "rmat", "ba", "er"], default="batch")
+    p.add_argument("--scale", type=int, default=15)
+    p.add_argument("--graphs", type=int, default=4096)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+# ---------------------------------------------------------------------------
+def make_workload(args):
+    import mce_b200 as mce
+    if args.workload == "batch":
+        b = mce.gen_chung_lu_batch(args.graphs, 64, 16384, 2.3, 8.0, 32.0, 5, 5, 40, 11)
+        g = mce.union(b)
+        cfg = {"workload": f"chung-lu batch: {args.graphs} graphs, n log-uniform [64,16384], "
+                           "gamma 2.3, mean degree U[8,32], 0-5 planted cliques U[5,40], seed 11",
+               "graphs": args.graphs}
+    elif args.workload == "rmat":
+        g = mce.gen_rmat(args.scale, 16, 0.57, 0.19, 0.19, 7)
+        cfg = {"workload": f"R-MAT scale {args.scale}, edge factor 16, (0.57,0.19,0.19,0.05), seed 7"}
+    elif args.workload == "ba":
+        g = mce.gen_ba(4_000_000, 8, 23, 200, 20, 60)
+        cfg = {"workload": "Barabasi-Albert n=4e6 m=8 seed 23 + 200 overlapping planted cliques U[20,60]"}
+    else:
+        g = mce.gen_er(10000, 0.002, 1, 20, 6, 12)
+        cfg = {"workload": "Erdos-Renyi G(10000,0.002) seed 1 + 20 planted cliques U[6,12]"}
+    cfg.update({"n": int(g.n), "arcs": int(g.m)})
+    return g, cfg
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu, self.rows, self.proc = gpu, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows if len(r) > 8
+                          for i, v in enumerate(r[5:9]) if "Active" in v and "Not" not in v})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def algorithmic_bytes(g, split):
+    """Bytes the search must read per launch: for each root, its row and the
+    later lists (with their offsets) of every neighbour it encodes."""
+    rp = g.row_ptr[:g.n + 1].astype(np.int64)
+    dplus = rp[1:] - split
+    deg = rp[1:] - rp[:-1]
+    a = 8 + 4 * dplus                               # offsets + later list of a neighbour
+    nb_sum = np.zeros(g.n, np.int64)
+    nz = deg > 0
+    if g.m:
+        acc = np.add.reduceat(a[g.col], rp[:-1][nz])
+        nb_sum[nz] = acc
+    roots = dplus > 0
+    search = int(np.sum(8 + 4 * deg[roots] + nb_sum[roots]))
+    peel = 4 * (g.n + 1) + 4 * g.m + 8 * g.m + 12 * g.n      # rows, arcs, degree RMW, init
+    orient = 4 * (g.n + 1) + 4 * g.m + 4 * g.m + 4 * g.m + 16 * g.n  # arcs, prio gather, write
+    return {"search": search, "peel": peel, "orient": orient}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def cpu_baseline(g, budget_s=15.0):
+    """The oracle (C, OpenMP, all host cores) on a bounded sample of roots.
+
+    Peeling and orientation run once on the whole graph; their time is
+    charged in proportion to the sampled share of roots."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    prep = oracle.prepare(g)
+    t_prep = time.perf_counter() - t0
+    split = prep[0]
+    nroots = int(np.count_nonzero(g.row_ptr[1:g.n + 1] - split))
+
+    def sample(stride):
+        t0 = time.perf_counter()
+        tot = oracle.roots(g, stride=stride, threads=cores, prepared=prep)[0]
+        return tot, time.perf_counter() - t0, len(range(0, g.n, stride))
+
+    stride = 1024
+    tot, dt, k = sample(stride)
+    if dt < budget_s / 10:
+        stride = int(min(1024, max(1, stride * dt / budget_s)))
+        tot, dt, k = sample(stride)
+    frac = k / max(g.n, 1)
+    t = dt + t_prep * frac
+    return {"value": tot / t if t > 0 else None, "unit": "maximal cliques/s", "cores": cores,
+            "kind": "port",
+            "sample": f"every {stride}th vertex as root ({tot} maximal cliques, {dt:.2f} s search "
+                      f"+ {frac:.3f} x {t_prep:.2f} s peel/orient); {nroots} roots in the workload"}
+
+
+# ---------------------------------------------------------------------------
+def run_mine(args, rank, world, local_rank):
+    import torch
+    import mce_b200 as mce
+    torch.cuda.set_device(local_rank)
+    g, cfg = make_workload(args)
+    stream = torch.cuda.Stream()
+    sptr = stream.cuda_stream
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    dg = mce.Graph.from_host(g, device=local_rank, stream=sptr)
+    torch.cuda.synchronize()
+    res = None
+    for _ in range(args.warmup):
+        res = dg.count(stream=sptr)
+    split, _ = dg.split_csr()
+    total = res.total if res else dg.count(stream=sptr).total
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    # ---- device-resident steps
+    times, stats = [], []
+    with ClockSampler(local_rank) as clk:
+        barrier()
+        for _ in range(args.steps):
+            flush.zero_()  # evict L2 between steps (outside the timed region)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            r = dg.count(stream=sptr)
+            e1.record(stream)
+            e1.synchronize()
+            assert r.total == total, "count changed between steps"
+            times.append(e0.elapsed_time(e1))
+            stats.append(r.stats)
+        barrier()
+    step_ms = sum(times) / len(times)
+    # ---- end to end: pinned host CSR -> device -> count -> host, per step
+    rp_h = torch.from_numpy(np.ascontiguousarray(g.row_ptr[:g.n + 1])).pin_memory()
+    col_h = torch.from_numpy(np.ascontiguousarray(g.col)).pin_memory()
+    e2e_times = []
+    barrier()
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        dg.reload_ptr(rp_h.data_ptr(), col_h.data_ptr(), g.n, g.m, stream=sptr)
+        r = dg.count(stream=sptr)
+        e1.record(stream)
+        e1.synchronize()
+        assert r.total == total
+        e2e_times.append(e0.elapsed_time(e1))
+    barrier()
+    e2e_ms = sum(e2e_times) / len(e2e_times)
+
+    # max over ranks
+    if world > 1:
+        t = torch.tensor([step_ms, e2e_ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        step_ms, e2e_ms = float(t[0]), float(t[1])
+    if rank != 0:
+        dg.close()
+        return None
+    clocks = clk.summary()
+    peaks, peak_kind = measured_peaks()
+    ab = algorithmic_bytes(g, split)
+    count_ms = statistics.mean(s["count_ms"] for s in stats)
+    peel_ms = statistics.mean(s["peel_ms"] for s in stats)
+    orient_ms = statistics.mean(s["orient_ms"] for s in stats)
+    # dominant phase by device time
+    phases = {"search": count_ms, "peel": peel_ms, "orient": orient_ms}
+    dom = max(phases, key=phases.get)
+    achieved = ab[dom] / (phases[dom] / 1e3) / 1e9
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            traffic = json.load(f).get(f"{args.workload}:{dom}")
+    except Exception:
+        pass
+    line = {
+        "metric": METRIC,
+        "value": world * total / (step_ms / 1e3),
+        "unit": "maximal cliques/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": step_ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u32", "data": "synthetic (seeded generators; no datasets)",
+        "config": dict(cfg, maximal_cliques=total, parallelism=f"replicas x{world}",
+                       l2="flushed between steps (256 MiB write) and inputs larger than L2",
+                       sched="plain", phases_ms={k: round(v, 3) for k, v in phases.items()},
+                       tree_nodes=stats[-1]["tree_nodes"], degeneracy=stats[-1]["degeneracy"],
+                       max_later_degree=stats[-1]["max_later_degree"],
+                       class_roots=stats[-1]["class_roots"][:3]),
+        "e2e": {"value": world * total / (e2e_ms / 1e3), "unit": "maximal cliques/s",
+                "h2d_bytes_per_step": int(4 * (g.n + 1) + 4 * g.m),
+                "d2h_bytes_per_step": int(8 * 4096 + 64 + 8 + 4 + 128),
+                "ms_per_step": e2e_ms},
+        "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved,
+                     "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
+                     "algorithmic_bytes": ab[dom], "peak_source": peak_kind},
+        "clocks": clocks,
+    }
+    if not args.no_cpu_baseline and world == 1:
+        try:
+            line["cpu_baseline"] = cpu_baseline(g)
+        except Exception as e:  # the baseline is reported, never required
+            line["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
+    dg.close()
+    return line
+
+
+# ---------------------------------------------------------------------------
+def run_reference(args, rank, world):
+    """The reference's CUDA binary (built from its own sources) on a sample."""
+    if rank != 0:
+        return None
+    if not os.path.exists(REF_BIN):
+        return {"impl": "reference", "unavailable": "oracle/_ref/parallel_mce_on_gpus not built"}
+    import mce_b200 as mce
+    sample_graphs = None
+    if args.workload == "batch":
+        sample_graphs = min(args.graphs, 1024)
+        b = mce.gen_chung_lu_batch(args.graphs, 64, 16384, 2.3, 8.0, 32.0, 5, 5, 40, 11)
+        # the first 1024 graphs of the same seeded batch, as one disjoint union
+        vo, ao = b.vtx_offsets, b.arc_offsets
+        sub = mce.HostGraph(b.row_ptr[:vo[sample_graphs]].copy(), b.col[:ao[sample_graphs]].copy(),
+                            int(vo[sample_graphs] - sample_graphs), int(ao[sample_graphs]),
+                            sample_graphs, vo[:sample_graphs + 1].copy(), ao[:sample_graphs + 1].copy())
+        g = mce.union(sub)
+        _, cfg = g, {"workload": f"chung-lu batch, first {sample_graphs} of {args.graphs} graphs "
+                                 "(seed 11) as one disjoint union"}
+    else:
+        g, cfg = make_workload(args)
+    cfg.update({"n": int(g.n), "arcs": int(g.m)})
+    tmp = tempfile.mkdtemp(prefix="mce_ref_")
+    bel = os.path.join(tmp, "g.bel")
+    mce.bel_write(bel, g)
+    runs = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        r = subprocess.run([REF_BIN, "-m", "mce", "-g", bel, "-d", "0", "-p", "l1", "-i", "p",
+                            "-w", "nowl"], capture_output=True, text=True, timeout=1800)
+        wall = time.perf_counter() - t0
+        out = re.sub(r"\x1b\[[0-9;]*m", "", r.stdout)
+        found = re.findall(r"Found (.*) maximal cliques in total", out)
+        degt = re.findall(r"Degeneracy ordering time: (.*) s", out)
+        cnt = re.findall(r"count time (.*) s", out)
+        if r.returncode != 0 or not found or not degt or not cnt:
+            return {"impl": "reference", "unavailable": f"reference run failed (rc {r.returncode}): "
+                    + (r.stderr or out)[-200:].replace("\n", " ")}
+        if i >= args.warmup:
+            runs.append((int(found[0].replace(",", "")), float(degt[0]), float(cnt[0]), wall))
+    os.remove(bel)
+    os.rmdir(tmp)
+    total = runs[0][0]
+    dev_s = statistics.mean(d + c for _, d, c, _ in runs)
+    value = total / dev_s
+    return {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "maximal cliques/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_s * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic (seeded generators; no datasets)",
+        "config": dict(cfg, maximal_cliques=total,
+                       timed="reference's own timers: 'Degeneracy ordering time' + 'count time' "
+                             "(-m mce -p l1 -i p -w nowl)",
+                       wall_s_per_run=statistics.mean(w for *_, w in runs)),
+        "cpu_baseline": {"value": value, "unit": "maximal cliques/s", "cores": os.cpu_count(),
+                         "kind": "reference",
+                         "sample": (f"first {sample_graphs} graphs of the batch" if sample_graphs
+                                    else "whole workload")
+                                   + "; the reference has no CPU implementation of the search, "
+                                     "its own implementation is this CUDA binary"},
+        "e2e": {"value": value, "unit": "maximal cliques/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if world > 1:
+        import datetime
+        import torch
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        if args.impl == "reference":
+            line = run_reference(args, rank, world)
+        else:
+            line = run_mine(args, rank, world, local_rank)
+        if rank == 0 and line is not None:
+            print(json.dumps(line), flush=True)
+    finally:
+        if world > 1:
+            import torch
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

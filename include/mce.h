@@ -1,0 +1,216 @@
+/*
+ * mce.h - C ABI of the B200 maximal-clique enumerator (libmce.so).
+ *
+ * The library counts the maximal cliques (size >= 2) of an undirected simple
+ * graph with the method of yen-hsiang-chang/mce-gpu: a degeneracy order from
+ * k-core peeling, then one Bron-Kerbosch search per root vertex with Tomita
+ * pivoting over the bitmap-encoded subgraph induced by the root's
+ * later-ordered neighbours.  Isolated vertices (maximal cliques of size 1)
+ * are never counted, exactly as in the reference (mce/mce_kernel_wl.cuh:70-79:
+ * a root with no later neighbour yields nothing).
+ *
+ * Conventions (all entry points):
+ *   - return MCE_OK (0) or a negative MCE_E* code; nothing calls exit();
+ *   - the caller owns every host buffer it passes in; buffers the library
+ *     returns (mce_hgraph_t arrays) are released with mce_hgraph_free();
+ *   - device memory is owned by the handle that allocated it;
+ *   - a handle is used by one host thread at a time; its work is queued on
+ *     the stream given in mce_opts_t.stream (or the handle's own stream).
+ *
+ * Vertex ids and CSR offsets are int32 (the reference's DataType is uint32,
+ * include/defs.h:10); graphs with 2^31 or more arcs are rejected.
+ */
+#ifndef MCE_H
+#define MCE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define MCE_OK 0
+#define MCE_EINVAL (-1)   /* bad argument                                   */
+#define MCE_ENOMEM (-2)   /* host or device allocation failed               */
+#define MCE_ECUDA (-3)    /* CUDA runtime error                             */
+#define MCE_EIO (-4)      /* file could not be opened / read / written      */
+#define MCE_EFORMAT (-5)  /* malformed input (.bel or CSR)                  */
+#define MCE_ELIMIT (-6)   /* a size cap was exceeded (degree, depth, queue) */
+#define MCE_ETIMEOUT (-7) /* a bounded device wait ran out                  */
+#define MCE_ENODEV (-8)   /* no usable CUDA device                          */
+#define MCE_ESTATE (-9)   /* call out of order (e.g. serve handle closed)   */
+
+/* Clique-size histogram length: hist[s] counts maximal cliques of size s.  */
+#define MCE_HIST_MAX 4096
+
+/* Largest later-neighbour count (bitmap width) a root may have.  The
+ * reference caps this at MAX_DEGEN = 2048 (mce/parameter.cuh:3); so do we.  */
+#define MCE_MAX_LATER_DEGREE 2048
+
+/* ---- options ------------------------------------------------------------ */
+/* -p (include/config.h:52-61): level of the subtrees that are parallelised */
+#define MCE_LEVEL_L1 1
+#define MCE_LEVEL_L2 2
+/* -i (include/config.h:72-81): which sets the induced subgraph is built on */
+#define MCE_INDUCED_P 1
+#define MCE_INDUCED_PX 2
+/* -w (include/config.h:92-101): worker list (donation) off / on           */
+#define MCE_WL_OFF 1
+#define MCE_WL_ON 2
+/* root scheduling */
+#define MCE_SCHED_PLAIN 0   /* roots in vertex-id order (the reference's order) */
+#define MCE_SCHED_DEGREE 1  /* roots sorted by a degree-based cost estimate     */
+#define MCE_SCHED_LEARNED 2 /* roots sorted by the cost MLP's prediction        */
+
+typedef struct mce_opts {
+  int32_t level;            /* MCE_LEVEL_*                                    */
+  int32_t induced;          /* MCE_INDUCED_*                                  */
+  int32_t worker_list;      /* MCE_WL_*                                       */
+  int32_t sched;            /* MCE_SCHED_*                                    */
+  int32_t bitmap_width;     /* 0 = auto; 32 or 64: word width of the rows of
+                               roots with at most 32 later neighbours          */
+  int32_t warps_per_root;   /* 0 = auto; 1 = one warp per root               */
+  int32_t donate_threshold; /* 0 = default (10, the reference's SZTH,
+                               mce/parameter.cuh:5): smallest candidate set a
+                               subtree must have to be donated                 */
+  int32_t log_roots;        /* 1 = record per-root search-tree node counts    */
+  int32_t x_pivot;          /* 1 = also take pivots from the root's earlier
+                               neighbours (the -i px pivot rule)               */
+  int32_t reserved[7];
+  void *stream;             /* cudaStream_t to queue work on; NULL = own      */
+} mce_opts_t;
+
+/* Fill *o with the defaults: L1, P, worker list on, plain schedule, auto.   */
+void mce_opts_default(mce_opts_t *o);
+
+/* Per-call statistics; device times are CUDA-event times on the call's stream. */
+typedef struct mce_stats {
+  double peel_ms;           /* k-core peeling (degeneracy order)              */
+  double orient_ms;         /* orientation / split CSR + root classification  */
+  double count_ms;          /* Bron-Kerbosch search                           */
+  double total_ms;          /* first kernel to last copy back                 */
+  int32_t degeneracy;       /* max core number                                */
+  int32_t max_later_degree; /* largest later-neighbour count of any root      */
+  int64_t max_degree;
+  int64_t roots;            /* vertices with at least one later neighbour     */
+  uint64_t tree_nodes;      /* search-tree nodes visited (branches taken)     */
+  uint64_t donations;       /* subtrees handed to another warp                */
+  int32_t kernel_launches;  /* this library's kernels launched by the call    */
+  uint32_t error_flags;     /* device-side status bits (0 = clean)            */
+  int64_t class_roots[8];   /* roots per engine class                         */
+} mce_stats_t;
+
+/* ---- host graphs -------------------------------------------------------- */
+/* A CSR graph in host memory whose arrays belong to the library.  For a
+ * batch of graphs, the arrays hold every graph's CSR back to back:
+ *   graph g's rows are row_ptr[vtx_offsets[g] .. vtx_offsets[g+1]) (n_g + 1
+ *   entries, local offsets starting at 0) and its arcs are
+ *   col[arc_offsets[g] .. arc_offsets[g+1]) (local vertex ids).
+ * For a single graph num_graphs = 1, vtx_offsets = {0, n+1},
+ * arc_offsets = {0, m}.                                                      */
+typedef struct mce_hgraph {
+  int64_t n;             /* total vertices (sum over graphs)                */
+  int64_t m;             /* total directed arcs (2 x undirected edges)      */
+  int32_t *row_ptr;      /* n + num_graphs entries                          */
+  int32_t *col;          /* m entries                                       */
+  int32_t num_graphs;
+  int64_t *vtx_offsets;  /* num_graphs + 1 entries, into row_ptr            */
+  int64_t *arc_offsets;  /* num_graphs + 1 entries, into col                */
+} mce_hgraph_t;
+
+/* Release the arrays of *g and zero it. */
+void mce_hgraph_free(mce_hgraph_t *g);
+
+/* Build a normalised CSR from an undirected edge list: both directions are
+ * added, self-loops dropped, duplicates removed, rows sorted - the same
+ * normalisation as graph::convert_to_bel (include/fileop.h:28-41).
+ * n = max(n_hint, max id + 1).                                               */
+int mce_hgraph_from_edges(const int64_t *src, const int64_t *dst, int64_t count,
+                          int64_t n_hint, mce_hgraph_t *out);
+
+/* Check that a CSR is a valid simple undirected graph: offsets monotone,
+ * ids in range, rows strictly increasing, no self-loops, symmetric.         */
+int mce_csr_validate(const int32_t *row_ptr, const int32_t *col, int64_t n, int64_t m);
+
+/* ---- .bel files ---------------------------------------------------------- */
+/* Read a .bel file (24-byte records: u64 dst, u64 src, u64 0; sorted by
+ * (src, dst)).  Replaces graph::read_bel (include/fileop.h:81-129) followed by
+ * CSRCOO::from_edgelist (include/csrcoo.cuh:41-81): n = max src + 1, empty
+ * rows are filled, ids are narrowed to 32 bits.  Returns MCE_EFORMAT if the
+ * records are not sorted by source (the reference asserts this,
+ * include/csrcoo.cuh:57-61) or the file size is not a multiple of 24.       */
+int mce_bel_read(const char *path, mce_hgraph_t *out);
+
+/* Write a host CSR as a .bel file (the record layout written by
+ * graph::convert_to_bel, include/fileop.h:62-71).                          */
+int mce_bel_write(const char *path, const mce_hgraph_t *g);
+
+/* Text edge list -> .bel.  Replaces graph::convert_to_bel
+ * (include/fileop.h:13-79): lines not starting with a digit are skipped,
+ * "u v" lines with u != v add both directions, then sort + unique.  On
+ * success *n_out = max id + 1 and *undirected_edges_out = m / 2 (the two
+ * numbers the reference prints).                                           */
+int mce_convert_to_bel(const char *txt_path, const char *bel_path, int64_t *n_out,
+                       int64_t *undirected_edges_out);
+
+/* ---- device graphs -------------------------------------------------------- */
+typedef struct mce_graph *mce_graph_t;
+
+/* Copy a CSR (host pointers, pageable or pinned) to device `device` and
+ * create a handle.  Replaces the managed-memory upload in main
+ * (src/main.cu:53-93).  `stream` may be NULL (the handle's own stream).     */
+int mce_graph_upload(const int32_t *row_ptr, const int32_t *col, int64_t n, int64_t m,
+                     int32_t device, void *stream, mce_graph_t *out);
+
+/* Replace the CSR of an existing handle with a new one of the same or
+ * smaller size, reusing its device buffers (no allocation when it fits).    */
+int mce_graph_reload(mce_graph_t g, const int32_t *row_ptr, const int32_t *col, int64_t n,
+                     int64_t m, void *stream);
+
+/* Free a handle and every device buffer it owns. */
+int mce_graph_free(mce_graph_t g);
+
+/* Degeneracy order of the uploaded graph.  Replaces
+ * graph::SingleGPU_Kcore::findKcoreIncremental_async (include/kcore.cuh:233-316).
+ * priority_out[v] (nullable, n entries) is the synchronous peel round in
+ * which v was removed, with the reference's numbering: rounds are numbered
+ * from 0 over all levels, and the vertices of the final round keep the value
+ * m (include/kcore.cuh:258,276).  core_out[v] (nullable) is v's core number;
+ * *degeneracy (nullable) the max core number (include/kcore.cuh:313-315).   */
+int mce_degeneracy(mce_graph_t g, uint32_t *priority_out, int32_t *core_out,
+                   int32_t *degeneracy);
+
+/* Oriented ("split") CSR after mce_degeneracy/mce_count: split_out[v]
+ * (n entries) is where v's later neighbours begin, col_out (m entries) holds
+ * each row as [earlier neighbours | later neighbours], both parts sorted by
+ * id.  Replaces set_priority/split_pointer/split_data
+ * (include/main_support.cuh:6-84, driven from src/main.cu:102-146).        */
+int mce_split_csr(mce_graph_t g, int32_t *split_out, int32_t *col_out);
+
+/* Count the maximal cliques (size >= 2).  Runs peeling, orientation and the
+ * search on the device; replaces MultiGPU_MCE::mce_count + show
+ * (mce/mce.cuh:107-422).  hist (nullable, MCE_HIST_MAX entries) receives the
+ * clique-size histogram; stats (nullable) the timings and counters.         */
+int mce_count(mce_graph_t g, const mce_opts_t *opts, uint64_t *total, uint64_t *hist,
+              mce_stats_t *stats);
+
+/* Per-root search-tree node counts of the last mce_count that ran with
+ * opts.log_roots = 1 (n entries, 0 for non-roots).                          */
+int mce_root_log(mce_graph_t g, uint64_t *nodes_out);
+
+/* Per-root maximal-clique counts of the last mce_count that ran with
+ * opts.log_roots = 1 (n entries, 0 for non-roots).                          */
+int mce_root_counts(mce_graph_t g, uint64_t *count_out);
+
+/* Text for a status code. */
+const char *mce_strerror(int code);
+
+/* Library version string. */
+const char *mce_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MCE_H */

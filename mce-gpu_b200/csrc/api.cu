@@ -1,0 +1,468 @@
+// C ABI of libmce.so: device graph handles and the counting pipeline.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace mce {
+
+static thread_local char g_last_detail[512];
+
+void set_last_cuda_error(cudaError_t e, const char *what, const char *file, int line) {
+  std::snprintf(g_last_detail, sizeof(g_last_detail), "%s: %s (%s:%d)", cudaGetErrorString(e),
+                what, file, line);
+}
+
+template <typename T>
+static int dalloc(T **p, size_t count) {
+  *p = nullptr;
+  if (count == 0) count = 1;
+  MCE_CUDA(cudaMalloc((void **)p, sizeof(T) * count));
+  return MCE_OK;
+}
+
+template <typename T>
+static void dfree(T *&p) {
+  if (p) cudaFree((void *)p);
+  p = nullptr;
+}
+
+}  // namespace mce
+
+using namespace mce;
+
+struct mce_graph {
+  int device = 0;
+  int sms = 0;
+  cudaStream_t own = nullptr;
+  int64_t n = 0, m = 0, cap_n = -1, cap_m = -1;
+  // graph
+  int32_t *rp = nullptr, *col = nullptr, *cs = nullptr, *split = nullptr;
+  // peeling
+  uint32_t *prio = nullptr;
+  int32_t *core = nullptr, *deg = nullptr, *alA = nullptr, *alB = nullptr;
+  int32_t *f0 = nullptr, *f1 = nullptr, *f2 = nullptr;
+  void *peel_ctl = nullptr;
+  // roots
+  uint32_t *keys_in = nullptr, *keys_out = nullptr;
+  int32_t *vals_in = nullptr, *roots = nullptr;
+  ShapeInfo *shape = nullptr;
+  void *sort_tmp = nullptr;
+  size_t sort_tmp_bytes = 0;
+  // search
+  uint32_t *fetch = nullptr, *err = nullptr;
+  unsigned long long *hist = nullptr, *nodes = nullptr;
+  unsigned long long *root_nodes = nullptr, *root_count = nullptr;
+  unsigned long long *slab = nullptr;
+  size_t slab_bytes = 0;
+  bool logged = false;
+  // host copies of the last call
+  ShapeInfo shape_h{};
+  int32_t degeneracy = 0;
+  cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+};
+
+namespace {
+
+constexpr uint64_t WAIT_LIMIT_NS = 20ull * 1000 * 1000 * 1000;  // 20 s per barrier wait
+
+void free_graph_bufs(mce_graph *g) {
+  dfree(g->rp); dfree(g->col); dfree(g->cs); dfree(g->split);
+  dfree(g->prio); dfree(g->core); dfree(g->deg); dfree(g->alA); dfree(g->alB);
+  dfree(g->f0); dfree(g->f1); dfree(g->f2);
+  dfree(g->keys_in); dfree(g->keys_out); dfree(g->vals_in); dfree(g->roots);
+  dfree(g->root_nodes); dfree(g->root_count);
+  g->cap_n = g->cap_m = -1;
+}
+
+int alloc_graph_bufs(mce_graph *g, int64_t n, int64_t m) {
+  free_graph_bufs(g);
+  const size_t N = (size_t)n + 1, M = (size_t)m;
+  int rc;
+  if ((rc = dalloc(&g->rp, N)) || (rc = dalloc(&g->col, M)) || (rc = dalloc(&g->cs, M)) ||
+      (rc = dalloc(&g->split, N)) || (rc = dalloc(&g->prio, N)) || (rc = dalloc(&g->core, N)) ||
+      (rc = dalloc(&g->deg, N)) || (rc = dalloc(&g->alA, N)) || (rc = dalloc(&g->alB, N)) ||
+      (rc = dalloc(&g->f0, N)) || (rc = dalloc(&g->f1, N)) || (rc = dalloc(&g->f2, N)) ||
+      (rc = dalloc(&g->keys_in, N)) || (rc = dalloc(&g->keys_out, N)) ||
+      (rc = dalloc(&g->vals_in, N)) || (rc = dalloc(&g->roots, N))) {
+    free_graph_bufs(g);
+    return rc;
+  }
+  g->cap_n = n;
+  g->cap_m = m;
+  return MCE_OK;
+}
+
+int alloc_fixed_bufs(mce_graph *g) {
+  int rc;
+  if ((rc = dalloc((char **)&g->peel_ctl, peel_ctl_bytes())) || (rc = dalloc(&g->shape, 1)) ||
+      (rc = dalloc(&g->fetch, 8)) || (rc = dalloc(&g->err, 4)) ||
+      (rc = dalloc(&g->hist, MCE_HIST_MAX)) || (rc = dalloc(&g->nodes, 4)))
+    return rc;
+  for (auto &e : g->ev) MCE_CUDA(cudaEventCreate(&e));
+  return MCE_OK;
+}
+
+cudaStream_t pick_stream(mce_graph *g, void *s) { return s ? (cudaStream_t)s : g->own; }
+
+int check_args(const int32_t *row_ptr, const int32_t *col, int64_t n, int64_t m) {
+  if (n < 0 || m < 0 || (n > 0 && !row_ptr) || (m > 0 && !col)) return MCE_EINVAL;
+  if (n >= ((int64_t)1 << 31) - 1 || m >= ((int64_t)1 << 31)) return MCE_ELIMIT;
+  return MCE_OK;
+}
+
+int upload_csr(mce_graph *g, const int32_t *row_ptr, const int32_t *col, int64_t n, int64_t m,
+               cudaStream_t s) {
+  if (n > g->cap_n || m > g->cap_m) {
+    int rc = alloc_graph_bufs(g, n, m);
+    if (rc) return rc;
+  }
+  g->n = n;
+  g->m = m;
+  if (n > 0)
+    MCE_CUDA(cudaMemcpyAsync(g->rp, row_ptr, sizeof(int32_t) * (size_t)(n + 1),
+                             cudaMemcpyHostToDevice, s));
+  if (m > 0)
+    MCE_CUDA(cudaMemcpyAsync(g->col, col, sizeof(int32_t) * (size_t)m, cudaMemcpyHostToDevice, s));
+  g->logged = false;
+  return MCE_OK;
+}
+
+// Stage 1: peel -> prio, core.
+int run_peel(mce_graph *g, cudaStream_t s, int *launches) {
+  if (g->n == 0) return MCE_OK;
+  PeelArgs pa;
+  pa.n = g->n;
+  pa.m = g->m;
+  pa.rp = g->rp;
+  pa.col = g->col;
+  pa.deg = g->deg;
+  pa.core = g->core;
+  pa.prio = g->prio;
+  pa.alistA = g->alA;
+  pa.alistB = g->alB;
+  pa.front0 = g->f0;
+  pa.front1 = g->f1;
+  pa.front2 = g->f2;
+  pa.ctl = g->peel_ctl;
+  pa.wait_limit_ns = WAIT_LIMIT_NS;
+  return peel_launch(pa, s, launches);
+}
+
+// Stage 2: orient + classify + sort roots (keys plain: class only).
+int run_orient(mce_graph *g, cudaStream_t s, int *launches) {
+  OrientArgs oa;
+  oa.n = g->n;
+  oa.rp = g->rp;
+  oa.col = g->col;
+  oa.prio = g->prio;
+  oa.split = g->split;
+  oa.cs = g->cs;
+  oa.keys_in = g->keys_in;
+  oa.vals_in = g->vals_in;
+  oa.shape = g->shape;
+  oa.cost = nullptr;
+  oa.sched = MCE_SCHED_PLAIN;
+  int rc = orient_launch(oa, s, launches);
+  if (rc) return rc;
+  return roots_sort(g->n, g->keys_in, g->keys_out, g->vals_in, g->roots, 3, &g->sort_tmp,
+                    &g->sort_tmp_bytes, g->shape, s, launches);
+}
+
+int read_shape(mce_graph *g, cudaStream_t s) {
+  MCE_CUDA(cudaMemcpyAsync(&g->shape_h, g->shape, sizeof(ShapeInfo), cudaMemcpyDeviceToHost, s));
+  MCE_CUDA(cudaStreamSynchronize(s));
+  return MCE_OK;
+}
+
+int ensure_slab(mce_graph *g, size_t bytes) {
+  if (bytes <= g->slab_bytes) return MCE_OK;
+  dfree(g->slab);
+  g->slab_bytes = 0;
+  MCE_CUDA(cudaMalloc((void **)&g->slab, bytes));
+  g->slab_bytes = bytes;
+  return MCE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void mce_opts_default(mce_opts_t *o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->level = MCE_LEVEL_L1;
+  o->induced = MCE_INDUCED_P;
+  o->worker_list = MCE_WL_ON;
+  o->sched = MCE_SCHED_PLAIN;
+  o->bitmap_width = 0;
+  o->warps_per_root = 0;
+  o->donate_threshold = 0;
+  o->log_roots = 0;
+  o->x_pivot = 0;
+  o->stream = nullptr;
+}
+
+const char *mce_strerror(int code) {
+  switch (code) {
+    case MCE_OK: return "ok";
+    case MCE_EINVAL: return "invalid argument";
+    case MCE_ENOMEM: return "out of memory";
+    case MCE_ECUDA: return g_last_detail[0] ? g_last_detail : "CUDA error";
+    case MCE_EIO: return "I/O error";
+    case MCE_EFORMAT: return "malformed input";
+    case MCE_ELIMIT: return "size limit exceeded";
+    case MCE_ETIMEOUT: return "device wait limit reached";
+    case MCE_ENODEV: return "no usable CUDA device";
+    case MCE_ESTATE: return "call out of order";
+    default: return "unknown error";
+  }
+}
+
+const char *mce_version(void) { return "mce-b200 0.1 (sm_100a)"; }
+
+int mce_graph_upload(const int32_t *row_ptr, const int32_t *col, int64_t n, int64_t m,
+                     int32_t device, void *stream, mce_graph_t *out) {
+  if (!out) return MCE_EINVAL;
+  *out = nullptr;
+  int rc = check_args(row_ptr, col, n, m);
+  if (rc) return rc;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return MCE_ENODEV;
+  if (device < 0 || device >= ndev) return MCE_EINVAL;
+  MCE_CUDA(cudaSetDevice(device));
+  mce_graph *g = new (std::nothrow) mce_graph();
+  if (!g) return MCE_ENOMEM;
+  g->device = device;
+  if (cudaDeviceGetAttribute(&g->sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&g->own, cudaStreamNonBlocking) != cudaSuccess) {
+    delete g;
+    return MCE_ECUDA;
+  }
+  rc = alloc_fixed_bufs(g);
+  if (!rc) rc = upload_csr(g, row_ptr, col, n, m, pick_stream(g, stream));
+  if (!rc) {
+    cudaError_t e = cudaStreamSynchronize(pick_stream(g, stream));
+    if (e != cudaSuccess) rc = MCE_ECUDA;
+  }
+  if (rc) {
+    mce_graph_free(g);
+    return rc;
+  }
+  *out = g;
+  return MCE_OK;
+}
+
+int mce_graph_reload(mce_graph_t g, const int32_t *row_ptr, const int32_t *col, int64_t n,
+                     int64_t m, void *stream) {
+  if (!g) return MCE_EINVAL;
+  int rc = check_args(row_ptr, col, n, m);
+  if (rc) return rc;
+  MCE_CUDA(cudaSetDevice(g->device));
+  return upload_csr(g, row_ptr, col, n, m, pick_stream(g, stream));
+}
+
+int mce_graph_free(mce_graph_t g) {
+  if (!g) return MCE_OK;
+  cudaSetDevice(g->device);
+  if (g->own) cudaStreamSynchronize(g->own);
+  free_graph_bufs(g);
+  dfree(g->peel_ctl);
+  dfree(g->shape);
+  dfree(g->fetch);
+  dfree(g->err);
+  dfree(g->hist);
+  dfree(g->nodes);
+  dfree(g->slab);
+  dfree(g->sort_tmp);
+  for (auto &e : g->ev)
+    if (e) cudaEventDestroy(e);
+  if (g->own) cudaStreamDestroy(g->own);
+  delete g;
+  return MCE_OK;
+}
+
+int mce_degeneracy(mce_graph_t g, uint32_t *priority_out, int32_t *core_out,
+                   int32_t *degeneracy) {
+  if (!g) return MCE_EINVAL;
+  MCE_CUDA(cudaSetDevice(g->device));
+  cudaStream_t s = g->own;
+  int launches = 0, rc = run_peel(g, s, &launches);
+  if (rc) return rc;
+  int32_t dg = 0;
+  uint32_t err = 0, rounds = 0;
+  if (g->n > 0) {
+    rc = peel_read(g->peel_ctl, &dg, &err, &rounds, s);
+    if (rc) return rc;
+    if (err) return MCE_ETIMEOUT;
+    if (priority_out)
+      MCE_CUDA(cudaMemcpyAsync(priority_out, g->prio, sizeof(uint32_t) * (size_t)g->n,
+                               cudaMemcpyDeviceToHost, s));
+    if (core_out)
+      MCE_CUDA(cudaMemcpyAsync(core_out, g->core, sizeof(int32_t) * (size_t)g->n,
+                               cudaMemcpyDeviceToHost, s));
+    MCE_CUDA(cudaStreamSynchronize(s));
+  }
+  g->degeneracy = dg;
+  if (degeneracy) *degeneracy = dg;
+  return MCE_OK;
+}
+
+int mce_split_csr(mce_graph_t g, int32_t *split_out, int32_t *col_out) {
+  if (!g) return MCE_EINVAL;
+  MCE_CUDA(cudaSetDevice(g->device));
+  cudaStream_t s = g->own;
+  int launches = 0, rc = run_peel(g, s, &launches);
+  if (!rc) rc = run_orient(g, s, &launches);
+  if (rc) return rc;
+  if (split_out && g->n)
+    MCE_CUDA(cudaMemcpyAsync(split_out, g->split, sizeof(int32_t) * (size_t)g->n,
+                             cudaMemcpyDeviceToHost, s));
+  if (col_out && g->m)
+    MCE_CUDA(cudaMemcpyAsync(col_out, g->cs, sizeof(int32_t) * (size_t)g->m,
+                             cudaMemcpyDeviceToHost, s));
+  MCE_CUDA(cudaStreamSynchronize(s));
+  return MCE_OK;
+}
+
+int mce_count(mce_graph_t g, const mce_opts_t *opts, uint64_t *total, uint64_t *hist,
+              mce_stats_t *stats) {
+  if (!g || !total) return MCE_EINVAL;
+  mce_opts_t o;
+  if (opts)
+    o = *opts;
+  else
+    mce_opts_default(&o);
+  if (o.bitmap_width != 0 && o.bitmap_width != 32 && o.bitmap_width != 64) return MCE_EINVAL;
+  MCE_CUDA(cudaSetDevice(g->device));
+  cudaStream_t s = pick_stream(g, o.stream);
+  int launches = 0, rc;
+  mce_stats_t st;
+  std::memset(&st, 0, sizeof(st));
+  MCE_CUDA(cudaEventRecord(g->ev[0], s));
+  if ((rc = run_peel(g, s, &launches))) return rc;
+  MCE_CUDA(cudaEventRecord(g->ev[1], s));
+  if ((rc = run_orient(g, s, &launches))) return rc;
+  MCE_CUDA(cudaEventRecord(g->ev[2], s));
+  if ((rc = read_shape(g, s))) return rc;
+  const ShapeInfo &sh = g->shape_h;
+  if (sh.cls_cnt[CLS_BIG]) return MCE_ELIMIT;
+  // search scratch
+  int grid[NCLS] = {0}, block[NCLS] = {0}, smem[NCLS] = {0};
+  const int dcap = (int)(sh.max_dplus > 0 ? sh.max_dplus : 1);
+  const int xcap = (int)(sh.max_dminus_mem > 0 ? sh.max_dminus_mem : 1);
+  size_t slab_need = 0;
+  for (int c = CLS_R32; c <= CLS_MEM; ++c) {
+    if (!sh.cls_cnt[c]) continue;
+    int warps = 0;
+    if ((rc = bk_warps_for_class(c, g->sms, &warps, &block[c], &smem[c]))) return rc;
+    // never more warps than roots (rounded up to whole blocks)
+    const int wpb = block[c] / 32;
+    int64_t want = c == CLS_MEM ? (int64_t)sh.cls_cnt[c] : ((int64_t)sh.cls_cnt[c] + 3) / 4;
+    if (want < warps) warps = (int)((want + wpb - 1) / wpb) * wpb;
+    grid[c] = warps / wpb;
+    const size_t need = (size_t)warps * bk_slab_words(c, dcap, xcap) * 8;
+    if (need > slab_need) slab_need = need;
+  }
+  if ((rc = ensure_slab(g, slab_need))) return rc;
+  if (o.log_roots) {
+    if (!g->root_nodes) {
+      if ((rc = dalloc(&g->root_nodes, (size_t)g->cap_n + 1))) return rc;
+      if ((rc = dalloc(&g->root_count, (size_t)g->cap_n + 1))) return rc;
+    }
+    MCE_CUDA(cudaMemsetAsync(g->root_nodes, 0, sizeof(unsigned long long) * (size_t)(g->n + 1), s));
+    MCE_CUDA(cudaMemsetAsync(g->root_count, 0, sizeof(unsigned long long) * (size_t)(g->n + 1), s));
+  }
+  MCE_CUDA(cudaMemsetAsync(g->fetch, 0, sizeof(uint32_t) * 8, s));
+  MCE_CUDA(cudaMemsetAsync(g->err, 0, sizeof(uint32_t) * 4, s));
+  MCE_CUDA(cudaMemsetAsync(g->hist, 0, sizeof(unsigned long long) * MCE_HIST_MAX, s));
+  MCE_CUDA(cudaMemsetAsync(g->nodes, 0, sizeof(unsigned long long) * 4, s));
+  BKArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.rp = g->rp;
+  a.split = g->split;
+  a.cs = g->cs;
+  a.roots = g->roots;
+  a.shape = g->shape;
+  a.fetch = g->fetch;
+  a.hist = g->hist;
+  a.nodes = g->nodes;
+  a.root_nodes = o.log_roots ? g->root_nodes : nullptr;
+  a.root_count = o.log_roots ? g->root_count : nullptr;
+  a.err = g->err;
+  a.slab = g->slab;
+  a.dcap = dcap;
+  a.xcap = xcap;
+  const int wbits = o.bitmap_width == 64 ? 64 : 32;
+  // widest roots first so the long trees start early
+  const int order[3] = {CLS_MEM, CLS_R64, CLS_R32};
+  for (int c : order) {
+    if (!grid[c]) continue;
+    a.slab_words = bk_slab_words(c, dcap, xcap);
+    if ((rc = bk_launch(c, wbits, a, grid[c], block[c], smem[c], s, &launches))) return rc;
+  }
+  MCE_CUDA(cudaEventRecord(g->ev[3], s));
+  unsigned long long h_hist[MCE_HIST_MAX];
+  unsigned long long h_nodes = 0;
+  uint32_t h_err = 0;
+  MCE_CUDA(cudaMemcpyAsync(h_hist, g->hist, sizeof(h_hist), cudaMemcpyDeviceToHost, s));
+  MCE_CUDA(cudaMemcpyAsync(&h_nodes, g->nodes, sizeof(h_nodes), cudaMemcpyDeviceToHost, s));
+  MCE_CUDA(cudaMemcpyAsync(&h_err, g->err, sizeof(h_err), cudaMemcpyDeviceToHost, s));
+  MCE_CUDA(cudaEventRecord(g->ev[4], s));
+  MCE_CUDA(cudaStreamSynchronize(s));
+  int32_t dg = 0;
+  uint32_t perr = 0, rounds = 0;
+  if (g->n > 0 && (rc = peel_read(g->peel_ctl, &dg, &perr, &rounds, s))) return rc;
+  g->degeneracy = dg;
+  g->logged = o.log_roots != 0;
+  uint64_t tot = 0;
+  for (int i = 0; i < MCE_HIST_MAX; ++i) tot += h_hist[i];
+  *total = tot;
+  if (hist)
+    for (int i = 0; i < MCE_HIST_MAX; ++i) hist[i] = h_hist[i];
+  float ms = 0;
+  cudaEventElapsedTime(&ms, g->ev[0], g->ev[1]);
+  st.peel_ms = ms;
+  cudaEventElapsedTime(&ms, g->ev[1], g->ev[2]);
+  st.orient_ms = ms;
+  cudaEventElapsedTime(&ms, g->ev[2], g->ev[3]);
+  st.count_ms = ms;
+  cudaEventElapsedTime(&ms, g->ev[0], g->ev[4]);
+  st.total_ms = ms;
+  st.degeneracy = dg;
+  st.max_later_degree = (int32_t)sh.max_dplus;
+  st.max_degree = sh.max_deg;
+  st.roots = (int64_t)sh.cls_cnt[CLS_R32] + sh.cls_cnt[CLS_R64] + sh.cls_cnt[CLS_MEM];
+  st.tree_nodes = h_nodes;
+  st.kernel_launches = launches;
+  st.error_flags = h_err | (perr ? MCE_ERR_WAIT_TIMEOUT : 0);
+  for (int c = 0; c < NCLS && c < 8; ++c) st.class_roots[c] = sh.cls_cnt[c];
+  if (stats) *stats = st;
+  if (perr) return MCE_ETIMEOUT;
+  if (h_err & MCE_ERR_WAIT_TIMEOUT) return MCE_ETIMEOUT;
+  if (h_err) return MCE_ELIMIT;
+  return MCE_OK;
+}
+
+int mce_root_log(mce_graph_t g, uint64_t *nodes_out) {
+  if (!g || !nodes_out) return MCE_EINVAL;
+  if (!g->logged || !g->root_nodes) return MCE_ESTATE;
+  MCE_CUDA(cudaSetDevice(g->device));
+  MCE_CUDA(cudaMemcpy(nodes_out, g->root_nodes, sizeof(uint64_t) * (size_t)g->n,
+                      cudaMemcpyDeviceToHost));
+  return MCE_OK;
+}
+
+int mce_root_counts(mce_graph_t g, uint64_t *count_out) {
+  if (!g || !count_out) return MCE_EINVAL;
+  if (!g->logged || !g->root_count) return MCE_ESTATE;
+  MCE_CUDA(cudaSetDevice(g->device));
+  MCE_CUDA(cudaMemcpy(count_out, g->root_count, sizeof(uint64_t) * (size_t)g->n,
+                      cudaMemcpyDeviceToHost));
+  return MCE_OK;
+}
+
+}  // extern "C"

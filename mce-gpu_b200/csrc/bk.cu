@@ -1,0 +1,640 @@
+// Per-root Bron-Kerbosch search with Tomita pivoting, one warp per root.
+//
+// Replaces the block-per-root kernels mce_kernel_l1_ip_{nowl,wl}
+// (mce/mce_kernel_nowl.cuh:9-109, mce/mce_kernel_wl.cuh:9-154) and the
+// helpers they call in mce/mce_utils.cuh.  The search rules are the
+// reference's (cited inline); the execution model is not:
+//  - a warp, not a 128/256-thread block, owns a root, so a tree step costs
+//    a few warp instructions instead of several __syncthreads;
+//  - the induced subgraph of the root's later neighbours lives in registers
+//    (lane i holds adjacency row i, and row i+32 for the 64-bit engine) or,
+//    for wide roots, in a per-warp slab, instead of per-block global arrays;
+//  - the pivot is the candidate u maximising popc(P & N(u)), found with one
+//    __reduce_max_sync over (score, -index) keys: every lane scores its own
+//    row(s) in parallel;
+//  - the DFS stack is an explicit array of (P, X, branch set, chosen set)
+//    frames in shared memory (register engine) or the slab (wide engine);
+//  - earlier neighbours of the root (the reference's Xx list, tested with a
+//    binary search per tree node, mce/mce_utils.cuh:265-292) are encoded once
+//    per root as bitmaps over the root's later neighbours; a leaf is maximal
+//    only if no such bitmap contains the leaf's clique.
+// Tie-breaking: the pivot with the lowest index among the best scores, so
+// per-root tree sizes are deterministic.
+#include <climits>
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace mce {
+
+namespace {
+
+using u64 = unsigned long long;
+
+template <typename W>
+struct WOps;
+template <>
+struct WOps<uint32_t> {
+  static __device__ __forceinline__ int popc(uint32_t x) { return __popc(x); }
+  static __device__ __forceinline__ int ctz(uint32_t x) { return __ffs(x) - 1; }
+  static __device__ __forceinline__ uint32_t bit(int i) { return 1u << i; }
+  static __device__ __forceinline__ uint32_t low(int d) { return d >= 32 ? ~0u : ((1u << d) - 1u); }
+};
+template <>
+struct WOps<u64> {
+  static __device__ __forceinline__ int popc(u64 x) { return __popcll(x); }
+  static __device__ __forceinline__ int ctz(u64 x) { return __ffsll((long long)x) - 1; }
+  static __device__ __forceinline__ u64 bit(int i) { return 1ull << i; }
+  static __device__ __forceinline__ u64 low(int d) { return d >= 64 ? ~0ull : ((1ull << d) - 1ull); }
+};
+
+constexpr int REG_BLOCK = 256;  // 8 warps
+constexpr int MEM_BLOCK = 128;  // 4 warps
+constexpr int REG_CHUNK = 4;    // roots fetched per atomic by the register engine
+
+__device__ __forceinline__ int warp_incl_scan(int x) {
+  const int lane = (int)lane_id();
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(MCE_FULL, x, o);
+    if (lane >= o) x += y;
+  }
+  return x;
+}
+
+// index t of the chunk item owning flattened element e: the last t with
+// off[t] <= e (off is the exclusive prefix of the items' list lengths).
+__device__ __forceinline__ int chunk_owner(const int32_t *off, int e) {
+  int lo = 0, hi = 32;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (off[mid] <= e)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo - 1;
+}
+
+__device__ __forceinline__ int lower_bound_g(const int32_t *a, int n, int32_t key) {
+  int lo = 0, len = n;
+  while (len > 0) {
+    const int half = len >> 1;
+    const bool right = a[lo + half] < key;
+    lo = right ? lo + half + 1 : lo;
+    len = right ? len - half - 1 : half;
+  }
+  return lo;
+}
+
+// ---------------------------------------------------------------------------
+// Register engine: d+ <= 32 * NR; lane i holds rows i (and i + 32).
+// ---------------------------------------------------------------------------
+template <typename Word, int NR>
+struct RegSmem {
+  Word rows[32 * NR];       // induced-subgraph rows while they are built
+  Word xs[32];              // earlier-neighbour rows while they are built
+  Word stk[32 * NR + 1][4]; // DFS frames: P, X, branch set, chosen set
+  int32_t pl[32 * NR];      // the root's later neighbours (sorted ids), padded
+  int32_t off[32];          // chunk prefix offsets
+  int32_t beg[32];          // chunk list starts
+};
+
+template <typename Word, int NR>
+__device__ __forceinline__ Word row_of(Word r0, Word r1, int j) {
+  if constexpr (NR == 2) return __shfl_sync(MCE_FULL, j >= 32 ? r1 : r0, j & 31);
+  return __shfl_sync(MCE_FULL, r0, j & 31);
+}
+
+template <typename Word, int NR>
+__device__ void search_root_reg(const BKArgs &a, RegSmem<Word, NR> &sm, Word *xr, Word *xl,
+                                int32_t r, u64 &h0, u64 &h1, u64 &nodes_total) {
+  using O = WOps<Word>;
+  const int lane = (int)lane_id();
+  const uint32_t lt = (1u << lane) - 1u;
+  const int32_t sb = a.split[r], d = a.rp[r + 1] - sb, ub = a.rp[r], u = sb - ub;
+
+  // setup_stack_original_L1_IP (mce/mce_utils.cuh:565-611): P = N+(r)
+#pragma unroll
+  for (int k = 0; k < NR; ++k) {
+    const int i = lane + 32 * k;
+    sm.pl[i] = i < d ? a.cs[sb + i] : INT_MAX;
+    sm.rows[i] = 0;
+  }
+  __syncwarp();
+
+  // warp_sorted_count_and_encode_full (mce/mce_utils.cuh:90-117): bit (j, i)
+  // and (i, j) for every later neighbour w = P[i] of v = P[j].  The later
+  // lists of 32 P vertices are flattened over the lanes.
+  for (int c = 0; c * 32 < d; ++c) {
+    const int items = min(32, d - c * 32);
+    int vb = 0, vlen = 0;
+    if (lane < items) {
+      const int32_t v = sm.pl[c * 32 + lane];
+      vb = a.split[v];
+      vlen = a.rp[v + 1] - vb;
+    }
+    const int incl = warp_incl_scan(vlen);
+    const int T = __shfl_sync(MCE_FULL, incl, 31);
+    sm.off[lane] = incl - vlen;
+    sm.beg[lane] = vb;
+    __syncwarp();
+    for (int e = lane; e < T; e += 32) {
+      const int t = chunk_owner(sm.off, e);
+      const int32_t w = a.cs[sm.beg[t] + (e - sm.off[t])];
+      const int i = lower_bound_g(sm.pl, 32 * NR, w);
+      if (i < d && sm.pl[i] == w) {
+        const int j = c * 32 + t;
+        atomicOr(&sm.rows[j], O::bit(i));
+        atomicOr(&sm.rows[i], O::bit(j));
+      }
+    }
+    __syncwarp();
+  }
+  const Word r0 = sm.rows[lane];
+  Word r1 = 0;
+  if constexpr (NR == 2) r1 = sm.rows[lane + 32];
+
+  // Earlier neighbours x of r: row(x) = N(x) & P.  Only non-empty rows are
+  // kept; x is earlier than every vertex of P, so N(x) & P lies in N+(x).
+  int nX = 0;
+  for (int c = 0; c * 32 < u; ++c) {
+    const int items = min(32, u - c * 32);
+    int xb = 0, xlen = 0;
+    if (lane < items) {
+      const int32_t x = a.cs[ub + c * 32 + lane];
+      xb = a.split[x];
+      xlen = a.rp[x + 1] - xb;
+    }
+    sm.xs[lane] = 0;
+    const int incl = warp_incl_scan(xlen);
+    const int T = __shfl_sync(MCE_FULL, incl, 31);
+    sm.off[lane] = incl - xlen;
+    sm.beg[lane] = xb;
+    __syncwarp();
+    for (int e = lane; e < T; e += 32) {
+      const int t = chunk_owner(sm.off, e);
+      const int32_t w = a.cs[sm.beg[t] + (e - sm.off[t])];
+      const int i = lower_bound_g(sm.pl, 32 * NR, w);
+      if (i < d && sm.pl[i] == w) atomicOr(&sm.xs[t], O::bit(i));
+    }
+    __syncwarp();
+    const Word row = sm.xs[lane];
+    const bool nz = lane < items && row != 0;
+    const uint32_t mk = __ballot_sync(MCE_FULL, nz);
+    if (nz) xr[nX + __popc(mk & lt)] = row;
+    nX += __popc(mk);
+    __syncwarp();
+  }
+
+  // Root level: pivot from P only (select_pivot_from_P, mce/mce_utils.cuh:338-364),
+  // branch set P \ N(pivot) (apply_pivot_to_first_level, :204-216).
+  const Word Pall = O::low(d);
+  int key = 0;
+  if (lane < d) key = ((O::popc(Pall & r0) + 1) << 7) | (127 - lane);
+  if constexpr (NR == 2)
+    if (lane + 32 < d) key = max(key, ((O::popc(Pall & r1) + 1) << 7) | (127 - (lane + 32)));
+  key = (int)__reduce_max_sync(MCE_FULL, (unsigned)key);
+  Word P = Pall, X = 0, S = 0;
+  Word B = Pall & ~row_of<Word, NR>(r0, r1, 127 - (key & 127));
+  int depth = 0, nL = 0;
+  u64 nodes = 0, cnt = 0;
+  for (;;) {
+    if (B == 0) {  // get_next_candidate found nothing: backtrack (:526-563)
+      if (depth == 0) break;
+      --depth;
+      P = sm.stk[depth][0];
+      X = sm.stk[depth][1];
+      B = sm.stk[depth][2];
+      S = sm.stk[depth][3];
+      continue;
+    }
+    const int v = O::ctz(B);
+    B &= B - 1;
+    const Word vb = O::bit(v);
+    const Word rv = row_of<Word, NR>(r0, r1, v);
+    // populate_xl_and_cl (:321-336): child P' = P & N(v), X' = X & N(v);
+    // v leaves P for X in this frame.
+    const Word Pc = P & rv, Xc = X & rv, Sc = S | vb;
+    P &= ~vb;
+    X |= vb;
+    ++nodes;
+    if (depth == 0 && nX > 0) {  // earlier neighbours adjacent to v
+      nL = 0;
+      for (int i0 = 0; i0 < nX; i0 += 32) {
+        const int i = i0 + lane;
+        const Word row = i < nX ? xr[i] : (Word)0;
+        const bool has = (row & vb) != 0;
+        const uint32_t mk = __ballot_sync(MCE_FULL, has);
+        if (has) xl[nL + __popc(mk & lt)] = row;
+        nL += __popc(mk);
+      }
+      __syncwarp();
+    }
+    if (Pc == 0) {
+      // test_maximality (:507-524): P' and X' empty and no earlier
+      // neighbour of the root adjacent to the whole clique.
+      if (Xc == 0) {
+        bool covered = false;
+        for (int i0 = 0; i0 < nL; i0 += 32) {
+          const int i = i0 + lane;
+          const bool hit = i < nL && (xl[i] & Sc) == Sc;
+          if (__any_sync(MCE_FULL, hit)) {
+            covered = true;
+            break;
+          }
+        }
+        if (!covered) {
+          ++cnt;
+          const int bin = O::popc(Sc) - 1;  // clique size - 2
+          if (lane == (bin & 31)) {
+            if (bin < 32)
+              ++h0;
+            else
+              ++h1;
+          }
+        }
+      }
+      continue;
+    }
+    // select_pivot_from_P_and_Xp (:366-402): pivot over P' | X'; an X'
+    // vertex adjacent to all of P' ends the path.
+    const Word cand = Pc | Xc;
+    const int pc = O::popc(Pc);
+    int k = 0;
+    bool el = false;
+    if ((cand >> lane) & 1) {
+      const int s = O::popc(Pc & r0);
+      k = ((s + 1) << 7) | (127 - lane);
+      el = ((Xc >> lane) & 1) && s == pc;
+    }
+    if constexpr (NR == 2) {
+      if ((cand >> (lane + 32)) & 1) {
+        const int s = O::popc(Pc & r1);
+        k = max(k, ((s + 1) << 7) | (127 - (lane + 32)));
+        el = el || (((Xc >> (lane + 32)) & 1) && s == pc);
+      }
+    }
+    if (__any_sync(MCE_FULL, el)) continue;
+    k = (int)__reduce_max_sync(MCE_FULL, (unsigned)k);
+    if (lane == 0) {
+      sm.stk[depth][0] = P;
+      sm.stk[depth][1] = X;
+      sm.stk[depth][2] = B;
+      sm.stk[depth][3] = S;
+    }
+    __syncwarp();
+    ++depth;
+    P = Pc;
+    X = Xc;
+    S = Sc;
+    // apply_pivot_to_next_level (:218-239)
+    B = Pc & ~row_of<Word, NR>(r0, r1, 127 - (k & 127));
+  }
+  nodes_total += nodes;
+  if (lane == 0) {
+    if (a.root_nodes) a.root_nodes[r] = nodes;
+    if (a.root_count) a.root_count[r] = cnt;
+    if (a.graph_count && cnt) atomicAdd(&a.graph_count[a.graph_of[r]], cnt);
+  }
+}
+
+template <typename Word, int NR>
+__global__ void __launch_bounds__(REG_BLOCK) bk_reg_kernel(BKArgs a, int cls) {
+  __shared__ RegSmem<Word, NR> sm_all[REG_BLOCK / 32];
+  RegSmem<Word, NR> &sm = sm_all[threadIdx.x >> 5];
+  const int lane = (int)lane_id();
+  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  Word *xr = (Word *)(a.slab + (size_t)gw * a.slab_words);
+  Word *xl = xr + REG_XCAP;
+  const uint32_t beg = a.shape->cls_off[cls], end = a.shape->cls_off[cls + 1];
+  u64 h0 = 0, h1 = 0, nodes = 0;
+  for (;;) {
+    uint32_t i0 = 0;
+    if (lane == 0) i0 = atomicAdd(&a.fetch[cls], (uint32_t)REG_CHUNK);
+    i0 = __shfl_sync(MCE_FULL, i0, 0);
+    if (i0 >= end - beg) break;
+    for (int k = 0; k < REG_CHUNK; ++k) {
+      const uint32_t idx = beg + i0 + k;
+      if (idx >= end) break;
+      search_root_reg<Word, NR>(a, sm, xr, xl, a.roots[idx], h0, h1, nodes);
+    }
+  }
+  if (h0) atomicAdd(&a.hist[lane + 2], h0);
+  if (h1) atomicAdd(&a.hist[lane + 34], h1);
+  if (lane == 0 && nodes) atomicAdd(a.nodes, nodes);  // warp-uniform count
+}
+
+// ---------------------------------------------------------------------------
+// Wide engine: any d+ <= 2048, rows of W = ceil(d+/64) words in a slab.
+// ---------------------------------------------------------------------------
+struct MemSmem {
+  int32_t off[32];
+  int32_t beg[32];
+};
+
+struct Slab {
+  int32_t *pl;
+  u64 *rows, *stk, *xs, *xr;
+  int32_t *xl;
+};
+
+__device__ __forceinline__ Slab slab_of(const BKArgs &a, int64_t gw) {
+  const int D = a.dcap, WM = (a.dcap + 63) / 64, XC = a.xcap;
+  u64 *base = a.slab + (size_t)gw * a.slab_words;
+  Slab s;
+  s.rows = base;
+  s.stk = s.rows + (size_t)D * WM;
+  s.xs = s.stk + (size_t)(D + 1) * 4 * WM;
+  s.xr = s.xs + (size_t)32 * WM;
+  s.pl = (int32_t *)(s.xr + (size_t)XC * WM);
+  s.xl = s.pl + D;
+  return s;
+}
+
+__device__ void search_root_mem(const BKArgs &a, MemSmem &sm, const Slab &sl, int32_t r,
+                                u64 &h0, u64 &h1, u64 &nodes_total) {
+  const int lane = (int)lane_id();
+  const uint32_t lt = (1u << lane) - 1u;
+  const int32_t sb = a.split[r], d = a.rp[r + 1] - sb, ub = a.rp[r], u = sb - ub;
+  if (d > a.dcap) {
+    if (lane == 0) atomicOr(a.err, MCE_ERR_DEGREE);
+    return;
+  }
+  const int Wr = (d + 63) >> 6;
+  int32_t *pl = sl.pl;
+  u64 *rows = sl.rows;
+  for (int i = lane; i < d; i += 32) pl[i] = a.cs[sb + i];
+  for (int i = lane; i < d * Wr; i += 32) rows[i] = 0;
+  __syncwarp();
+  for (int c = 0; c * 32 < d; ++c) {
+    const int items = min(32, d - c * 32);
+    int vb = 0, vlen = 0;
+    if (lane < items) {
+      const int32_t v = pl[c * 32 + lane];
+      vb = a.split[v];
+      vlen = a.rp[v + 1] - vb;
+    }
+    const int incl = warp_incl_scan(vlen);
+    const int T = __shfl_sync(MCE_FULL, incl, 31);
+    sm.off[lane] = incl - vlen;
+    sm.beg[lane] = vb;
+    __syncwarp();
+    for (int e = lane; e < T; e += 32) {
+      const int t = chunk_owner(sm.off, e);
+      const int32_t w = a.cs[sm.beg[t] + (e - sm.off[t])];
+      const int i = lower_bound_g(pl, d, w);
+      if (i < d && pl[i] == w) {
+        const int j = c * 32 + t;
+        atomicOr(&rows[(size_t)j * Wr + (i >> 6)], 1ull << (i & 63));
+        atomicOr(&rows[(size_t)i * Wr + (j >> 6)], 1ull << (j & 63));
+      }
+    }
+    __syncwarp();
+  }
+  // earlier-neighbour rows (non-empty only)
+  int nX = 0;
+  for (int c = 0; c * 32 < u; ++c) {
+    const int items = min(32, u - c * 32);
+    int xb = 0, xlen = 0;
+    if (lane < items) {
+      const int32_t x = a.cs[ub + c * 32 + lane];
+      xb = a.split[x];
+      xlen = a.rp[x + 1] - xb;
+    }
+    for (int i = lane; i < 32 * Wr; i += 32) sl.xs[i] = 0;
+    const int incl = warp_incl_scan(xlen);
+    const int T = __shfl_sync(MCE_FULL, incl, 31);
+    sm.off[lane] = incl - xlen;
+    sm.beg[lane] = xb;
+    __syncwarp();
+    for (int e = lane; e < T; e += 32) {
+      const int t = chunk_owner(sm.off, e);
+      const int32_t w = a.cs[sm.beg[t] + (e - sm.off[t])];
+      const int i = lower_bound_g(pl, d, w);
+      if (i < d && pl[i] == w) atomicOr(&sl.xs[(size_t)t * Wr + (i >> 6)], 1ull << (i & 63));
+    }
+    __syncwarp();
+    bool nz = false;
+    if (lane < items)
+      for (int w = 0; w < Wr; ++w) nz |= sl.xs[(size_t)lane * Wr + w] != 0;
+    const uint32_t mk = __ballot_sync(MCE_FULL, nz);
+    if (nX + __popc(mk) > a.xcap) {
+      if (lane == 0) atomicOr(a.err, MCE_ERR_XROWS);
+      return;
+    }
+    if (nz) {
+      const int pos = nX + __popc(mk & lt);
+      for (int w = 0; w < Wr; ++w) sl.xr[(size_t)pos * Wr + w] = sl.xs[(size_t)lane * Wr + w];
+    }
+    nX += __popc(mk);
+    __syncwarp();
+  }
+
+  // root frame
+  u64 *F0 = sl.stk;
+  int key = 0;
+  for (int j = lane; j < d; j += 32) {
+    int s = 0;
+    for (int w = 0; w < Wr; ++w) s += __popcll(rows[(size_t)j * Wr + w]);
+    key = max(key, ((s + 1) << 11) | (2047 - j));
+  }
+  key = (int)__reduce_max_sync(MCE_FULL, (unsigned)key);
+  {
+    const int piv = 2047 - (key & 2047);
+    if (lane < Wr) {
+      const u64 all = (lane == Wr - 1 && (d & 63)) ? ((1ull << (d & 63)) - 1ull) : ~0ull;
+      F0[lane] = all;
+      F0[Wr + lane] = 0;
+      F0[2 * Wr + lane] = all & ~rows[(size_t)piv * Wr + lane];
+      F0[3 * Wr + lane] = 0;
+    }
+  }
+  __syncwarp();
+  int depth = 0, nL = 0;
+  u64 nodes = 0, cnt = 0;
+  for (;;) {
+    u64 *F = sl.stk + (size_t)depth * 4 * Wr;
+    u64 *Fp = F, *Fx = F + Wr, *Fb = F + 2 * Wr, *Fs = F + 3 * Wr;
+    // lowest set bit of the branch set
+    const u64 bw = lane < Wr ? Fb[lane] : 0ull;
+    const uint32_t mk = __ballot_sync(MCE_FULL, bw != 0);
+    if (!mk) {
+      if (depth == 0) break;
+      --depth;
+      continue;
+    }
+    const int wl = __ffs(mk) - 1;
+    const u64 word = __shfl_sync(MCE_FULL, bw, wl);
+    const int v = wl * 64 + __ffsll((long long)word) - 1;
+    const int vw = v >> 6;
+    const u64 vbit = 1ull << (v & 63);
+    if (lane == 0) {
+      Fb[vw] &= ~vbit;
+      Fp[vw] &= ~vbit;
+      Fx[vw] |= vbit;
+    }
+    __syncwarp();
+    ++nodes;
+    u64 *C = F + 4 * Wr;
+    int pc = 0;
+    bool xnz = false;
+    if (lane < Wr) {
+      const u64 rw = rows[(size_t)v * Wr + lane];
+      const u64 pcw = Fp[lane] & rw, xcw = Fx[lane] & rw;
+      C[lane] = pcw;
+      C[Wr + lane] = xcw;
+      C[3 * Wr + lane] = Fs[lane] | (lane == vw ? vbit : 0ull);
+      pc = __popcll(pcw);
+      xnz = xcw != 0;
+    }
+    pc = (int)__reduce_add_sync(MCE_FULL, (unsigned)pc);
+    xnz = __any_sync(MCE_FULL, xnz);
+    if (depth == 0 && nX > 0) {
+      nL = 0;
+      for (int i0 = 0; i0 < nX; i0 += 32) {
+        const int i = i0 + lane;
+        const bool has = i < nX && (sl.xr[(size_t)i * Wr + vw] & vbit);
+        const uint32_t m2 = __ballot_sync(MCE_FULL, has);
+        if (has) sl.xl[nL + __popc(m2 & lt)] = i;
+        nL += __popc(m2);
+      }
+    }
+    __syncwarp();
+    if (pc == 0) {
+      if (!xnz) {
+        const u64 *Cs = C + 3 * Wr;
+        bool covered = false;
+        for (int i0 = 0; i0 < nL; i0 += 32) {
+          const int i = i0 + lane;
+          bool hit = false;
+          if (i < nL) {
+            const u64 *xrow = sl.xr + (size_t)sl.xl[i] * Wr;
+            hit = true;
+            for (int w = 0; w < Wr && hit; ++w) hit = (xrow[w] & Cs[w]) == Cs[w];
+          }
+          if (__any_sync(MCE_FULL, hit)) {
+            covered = true;
+            break;
+          }
+        }
+        if (!covered) {
+          ++cnt;
+          const int bin = depth;  // clique size - 2 (root + depth + 1 vertices)
+          if (bin < 64) {
+            if (lane == (bin & 31)) {
+              if (bin < 32)
+                ++h0;
+              else
+                ++h1;
+            }
+          } else if (lane == 0 && bin + 2 < MCE_HIST_MAX) {
+            atomicAdd(&a.hist[bin + 2], 1ull);
+          }
+        }
+      }
+      continue;
+    }
+    int k = 0;
+    bool el = false;
+    for (int uu = lane; uu < d; uu += 32) {
+      const int uw = uu >> 6;
+      const u64 ub2 = 1ull << (uu & 63);
+      const bool inP = (C[uw] & ub2) != 0, inX = (C[Wr + uw] & ub2) != 0;
+      if (!(inP || inX)) continue;
+      int s = 0;
+      const u64 *ru = rows + (size_t)uu * Wr;
+      for (int w = 0; w < Wr; ++w) s += __popcll(C[w] & ru[w]);
+      k = max(k, ((s + 1) << 11) | (2047 - uu));
+      el = el || (inX && s == pc);
+    }
+    if (__any_sync(MCE_FULL, el)) continue;
+    k = (int)__reduce_max_sync(MCE_FULL, (unsigned)k);
+    const int up = 2047 - (k & 2047);
+    if (lane < Wr) C[2 * Wr + lane] = C[lane] & ~rows[(size_t)up * Wr + lane];
+    __syncwarp();
+    ++depth;
+  }
+  nodes_total += nodes;
+  if (lane == 0) {
+    if (a.root_nodes) a.root_nodes[r] = nodes;
+    if (a.root_count) a.root_count[r] = cnt;
+    if (a.graph_count && cnt) atomicAdd(&a.graph_count[a.graph_of[r]], cnt);
+  }
+}
+
+__global__ void __launch_bounds__(MEM_BLOCK) bk_mem_kernel(BKArgs a, int cls) {
+  __shared__ MemSmem sm_all[MEM_BLOCK / 32];
+  MemSmem &sm = sm_all[threadIdx.x >> 5];
+  const int lane = (int)lane_id();
+  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const Slab sl = slab_of(a, gw);
+  const uint32_t beg = a.shape->cls_off[cls], end = a.shape->cls_off[cls + 1];
+  u64 h0 = 0, h1 = 0, nodes = 0;
+  for (;;) {
+    uint32_t i0 = 0;
+    if (lane == 0) i0 = atomicAdd(&a.fetch[cls], 1u);
+    i0 = __shfl_sync(MCE_FULL, i0, 0);
+    if (i0 >= end - beg) break;
+    search_root_mem(a, sm, sl, a.roots[beg + i0], h0, h1, nodes);
+  }
+  if (h0) atomicAdd(&a.hist[lane + 2], h0);
+  if (h1) atomicAdd(&a.hist[lane + 34], h1);
+  if (lane == 0 && nodes) atomicAdd(a.nodes, nodes);  // warp-uniform count
+}
+
+}  // namespace
+
+size_t bk_slab_words(int cls, int dcap, int xcap) {
+  if (cls == CLS_R32 || cls == CLS_R64) return 2 * (size_t)REG_XCAP;  // x rows + leaf list
+  const size_t WM = (size_t)(dcap + 63) / 64;
+  size_t w = (size_t)dcap * WM + (size_t)(dcap + 1) * 4 * WM + 32 * WM + (size_t)xcap * WM;
+  w += ((size_t)dcap + (size_t)xcap + 1) / 2 + 1;  // pl and xl (int32)
+  return (w + 31) & ~(size_t)31;                    // 256-byte aligned slabs
+}
+
+int bk_warps_for_class(int cls, int sms, int *warps, int *block, int *smem) {
+  int per_sm = 0;
+  if (cls == CLS_R32 || cls == CLS_R64) {
+    *block = REG_BLOCK;
+    *smem = 0;
+    if (cls == CLS_R32)
+      MCE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bk_reg_kernel<uint32_t, 1>, REG_BLOCK, 0));
+    else
+      MCE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bk_reg_kernel<u64, 2>, REG_BLOCK, 0));
+    if (per_sm < 1) per_sm = 1;
+    *warps = sms * per_sm * (REG_BLOCK / 32);
+  } else {
+    *block = MEM_BLOCK;
+    *smem = 0;
+    per_sm = 4;
+    *warps = sms * per_sm * (MEM_BLOCK / 32);
+  }
+  return MCE_OK;
+}
+
+int bk_launch(int cls, int word_bits, const BKArgs &a, int grid, int block, int smem,
+              cudaStream_t s, int *launches) {
+  if (grid <= 0) return MCE_OK;
+  switch (cls) {
+    case CLS_R32:
+      if (word_bits == 64)
+        bk_reg_kernel<u64, 1><<<grid, block, smem, s>>>(a, cls);
+      else
+        bk_reg_kernel<uint32_t, 1><<<grid, block, smem, s>>>(a, cls);
+      break;
+    case CLS_R64:
+      bk_reg_kernel<u64, 2><<<grid, block, smem, s>>>(a, cls);
+      break;
+    case CLS_MEM:
+      bk_mem_kernel<<<grid, block, smem, s>>>(a, cls);
+      break;
+    default:
+      return MCE_EINVAL;
+  }
+  MCE_CUDA(cudaGetLastError());
+  if (launches) *launches += 1;
+  return MCE_OK;
+}
+
+}  // namespace mce

@@ -1,0 +1,89 @@
+// Launch wrappers shared by the .cu files of libmce.so (internal).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+namespace mce {
+
+// ---- peeling ---------------------------------------------------------------
+struct PeelArgs {
+  int64_t n, m;
+  const int32_t *rp, *col;
+  int32_t *deg, *core;
+  uint32_t *prio;
+  int32_t *alistA, *alistB, *front0, *front1, *front2;
+  void *ctl;  // peel_ctl_bytes() of device memory
+  uint64_t wait_limit_ns;
+};
+size_t peel_ctl_bytes();
+int peel_launch(const PeelArgs &a, cudaStream_t s, int *launches);
+int peel_read(const void *ctl_dev, int32_t *degeneracy, uint32_t *err, uint32_t *rounds,
+              cudaStream_t s);
+
+// ---- orientation + root classes ------------------------------------------------
+// Engine classes of a root (by later degree d+ and earlier degree d-).
+enum RootClass : uint32_t {
+  CLS_R32 = 0,   // 1 <= d+ <= 32, d- <= REG_XCAP: warp engine, rows in registers
+  CLS_R64 = 1,   // 33 <= d+ <= 64, d- <= REG_XCAP: warp engine, two rows per lane
+  CLS_MEM = 2,   // any other root with d+ <= 2048: warp engine, rows in a slab
+  CLS_NONE = 3,  // d+ == 0: not a root
+  CLS_BIG = 4,   // d+ > 2048: rejected (the reference's MAX_DEGEN)
+  NCLS = 5
+};
+constexpr int REG_XCAP = 1024;  // earlier-neighbour rows a register-engine warp keeps
+
+// Per-call summary the device writes and the host reads once.
+struct ShapeInfo {
+  uint32_t cls_cnt[8];
+  uint32_t cls_off[9];
+  uint32_t max_dplus;      // over all roots
+  uint32_t max_dminus_mem; // over roots of CLS_MEM
+  uint32_t max_deg;
+  uint32_t pad;
+};
+
+struct OrientArgs {
+  int64_t n;
+  const int32_t *rp, *col;
+  const uint32_t *prio;
+  int32_t *split, *cs;
+  uint32_t *keys_in;    // sort keys (class / cost), n
+  int32_t *vals_in;     // vertex ids, n
+  ShapeInfo *shape;     // zeroed by the launcher
+  const float *cost;    // nullable: per-vertex cost estimate (larger first)
+  int sched;
+};
+int orient_launch(const OrientArgs &a, cudaStream_t s, int *launches);
+
+// Sort roots by key (stable) and compute class offsets.  temp grows on demand.
+int roots_sort(int64_t n, const uint32_t *keys_in, uint32_t *keys_out, const int32_t *vals_in,
+               int32_t *vals_out, int end_bit, void **temp, size_t *temp_bytes,
+               ShapeInfo *shape, cudaStream_t s, int *launches);
+
+// ---- search ------------------------------------------------------------------
+struct BKArgs {
+  const int32_t *rp, *split, *cs;
+  const int32_t *roots;          // class-sorted roots
+  const ShapeInfo *shape;        // cls_off on the device
+  uint32_t *fetch;               // [NCLS] root fetch counters, zeroed per call
+  unsigned long long *hist;      // [MCE_HIST_MAX]
+  unsigned long long *nodes;     // total tree nodes
+  unsigned long long *root_nodes;  // nullable [n]: search-tree nodes per root
+  unsigned long long *root_count;  // nullable [n]: maximal cliques per root
+  const int32_t *graph_of;       // nullable [n]: graph of each vertex (batch)
+  unsigned long long *graph_count; // nullable [num_graphs]
+  uint32_t *err;
+  unsigned long long *slab;      // per-warp scratch
+  size_t slab_words;             // u64 words per warp
+  int32_t dcap, xcap;            // slab capacities (later degree, x rows)
+};
+
+// Launch the engine of one class.  warps_out: number of warps launched (slab sizing).
+int bk_warps_for_class(int cls, int sms, int *warps, int *block, int *smem);
+size_t bk_slab_words(int cls, int dcap, int xcap);
+int bk_launch(int cls, int word_bits, const BKArgs &a, int grid, int block, int smem,
+              cudaStream_t s, int *launches);
+
+}  // namespace mce

@@ -1,0 +1,232 @@
+// Degeneracy order by synchronous k-core peeling: one cooperative launch.
+//
+// Replaces graph::SingleGPU_Kcore::findKcoreIncremental_async
+// (include/kcore.cuh:233-316), which drives every peel round from the host
+// with several launches and a cudaDeviceSynchronize + scalar read-backs per
+// round.  Here all levels and rounds run inside one persistent kernel whose
+// blocks meet at a bounded grid barrier between phases; the host launches
+// once and reads nothing until the end.
+//
+// Semantics kept from the reference (so priorities are bit-identical):
+//  - at level k, round 0 is every remaining vertex of remaining degree k
+//    (filter_window + filter_with_random_append, include/kcore.cuh:21-48);
+//  - removing a round lowers neighbour degrees; a neighbour whose degree
+//    falls from k+1 to k joins the next round (process_degree, :80-95);
+//  - rounds are numbered over all levels; priority[v] = v's round number,
+//    and the round that empties the graph is not processed, so its vertices
+//    keep priority = m (:258, :276);
+//  - a level with no vertex of degree k runs no round (the scan below jumps
+//    straight to the smallest remaining degree, which numbers rounds the
+//    same way).
+// Decrements of a vertex that is already removed or queued are skipped;
+// they cannot change any round's membership.
+#include <cooperative_groups.h>
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace mce {
+
+struct PeelCtl {
+  GridBarrier bar;
+  uint32_t err;
+  uint32_t fcnt[3];    // frontier sizes, rotating: cur, next, to-reset
+  uint32_t acnt[3];    // alive-list sizes, rotating
+  uint32_t amin[3];    // min degree over the alive list written by a scan
+  int32_t degeneracy;
+  uint32_t rounds;
+  uint32_t levels;
+};
+
+namespace {
+
+constexpr int PEEL_BLOCK = 512;
+
+// warp-aggregated append of `pred` items to list[*cnt]
+__device__ __forceinline__ void warp_append(bool pred, int32_t val, int32_t *list,
+                                            uint32_t *cnt) {
+  const uint32_t mask = __ballot_sync(MCE_FULL, pred);
+  if (!mask) return;
+  const uint32_t lane = lane_id();
+  uint32_t base = 0;
+  const int leader = __ffs(mask) - 1;
+  if ((int)lane == leader) base = atomicAdd(cnt, (uint32_t)__popc(mask));
+  base = __shfl_sync(MCE_FULL, base, leader);
+  if (pred) list[base + __popc(mask & ((1u << lane) - 1u))] = val;
+}
+
+__global__ void __launch_bounds__(PEEL_BLOCK)
+    peel_kernel(int32_t n, uint32_t m, const int32_t *__restrict__ rp,
+                const int32_t *__restrict__ col, int32_t *deg, int32_t *core, uint32_t *prio,
+                int32_t *alistA, int32_t *alistB, int32_t *front0, int32_t *front1,
+                int32_t *front2, PeelCtl *ctl, uint64_t limit_ns) {
+  const uint32_t nblocks = gridDim.x;
+  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t nthr = (int64_t)gridDim.x * blockDim.x;
+  const int64_t gwarp = tid >> 5, nwarps = nthr >> 5;
+  const uint32_t lane = lane_id();
+  int32_t *fr[3] = {front0, front1, front2};
+  int32_t *alist[2] = {alistA, alistB};
+
+  for (int64_t v = tid; v < n; v += nthr) {
+    deg[v] = rp[v + 1] - rp[v];
+    core[v] = -1;
+    prio[v] = m;
+    alistA[v] = (int32_t)v;
+  }
+  if (tid == 0) {
+    ctl->fcnt[0] = ctl->fcnt[1] = ctl->fcnt[2] = 0;
+    ctl->acnt[0] = (uint32_t)n;
+    ctl->acnt[1] = ctl->acnt[2] = 0;
+    ctl->amin[0] = ctl->amin[1] = ctl->amin[2] = 0xFFFFFFFFu;
+  }
+  if (!grid_sync(&ctl->bar, nblocks, &ctl->err, limit_ns)) return;
+
+  int64_t todo = n;
+  int32_t level = 0, degen = 0;
+  uint32_t priority = 0, rounds = 0, levels = 0;
+  // Counter rotation invariant at the start of every phase: fcnt[fc] is the
+  // current frontier's size (0 before a scan) and fcnt[(fc + 1) % 3] == 0;
+  // each phase resets fcnt[(fc + 2) % 3], the counter that becomes "next"
+  // once fc advances.  The alive-list counters rotate the same way.
+  int fc = 0;     // index of the current frontier counter / buffer
+  int ac = 0;     // index of the current alive counter
+  int al = 0;     // which alive buffer is current
+
+  while (todo > 0) {
+    // ---- level scan: split the alive list into {deg == level} and the rest
+    const uint32_t nalive = ld_volatile(&ctl->acnt[ac]);
+    const int an = (ac + 1) % 3, ar = (ac + 2) % 3;
+    const int32_t *A = alist[al];
+    int32_t *A2 = alist[al ^ 1];
+    int32_t *F = fr[fc];
+    if (tid == 0) {  // reset the counters two phases ahead
+      ctl->acnt[ar] = 0;
+      ctl->amin[ar] = 0xFFFFFFFFu;
+      ctl->fcnt[(fc + 2) % 3] = 0;
+    }
+    {
+      uint32_t mymin = 0xFFFFFFFFu;
+      const int64_t lim = ((int64_t)nalive + 31) & ~(int64_t)31;
+      for (int64_t i = tid; i < lim; i += nthr) {
+        int32_t v = 0, d = 0;
+        bool live = false;
+        if (i < nalive) {
+          v = A[i];
+          live = ld_volatile((const uint32_t *)&core[v]) == 0xFFFFFFFFu;
+          d = deg[v];
+        }
+        const bool inF = live && d == level;
+        const bool keep = live && d > level;
+        if (inF) core[v] = level;
+        warp_append(inF, v, F, &ctl->fcnt[fc]);
+        warp_append(keep, v, A2, &ctl->acnt[an]);
+        if (keep) mymin = min(mymin, (uint32_t)d);
+      }
+      mymin = __reduce_min_sync(MCE_FULL, mymin);
+      if (lane == 0 && mymin != 0xFFFFFFFFu) atomicMin(&ctl->amin[an], mymin);
+    }
+    if (!grid_sync(&ctl->bar, nblocks, &ctl->err, limit_ns)) return;
+    ac = an;
+    al ^= 1;
+    uint32_t cnt = ld_volatile(&ctl->fcnt[fc]);
+    if (cnt == 0) {
+      // no vertex of degree `level` remains: jump to the smallest degree
+      // (a rescan at that level always finds the vertex that attains it)
+      const uint32_t mn = ld_volatile(&ctl->amin[ac]);
+      if (mn == 0xFFFFFFFFu || (int32_t)mn <= level) {
+        if (tid == 0) atomicOr(&ctl->err, MCE_ERR_QUEUE);  // inconsistent state: stop
+        break;
+      }
+      level = (int32_t)mn;
+      continue;
+    }
+    ++levels;
+    // ---- rounds of this level
+    while (cnt > 0) {
+      degen = level;
+      todo -= cnt;
+      if (todo == 0) break;  // the final round keeps priority = m
+      const int fn = (fc + 1) % 3;
+      if (tid == 0) ctl->fcnt[(fc + 2) % 3] = 0;
+      int32_t *Fc = fr[fc], *Fn = fr[fn];
+      for (int64_t i = tid; i < cnt; i += nthr) prio[Fc[i]] = priority;
+      for (int64_t i = gwarp; i < cnt; i += nwarps) {
+        const int32_t v = Fc[i];
+        const int32_t b = rp[v], e = rp[v + 1];
+        for (int32_t j0 = b; j0 < e; j0 += 32) {
+          const int32_t j = j0 + (int32_t)lane;
+          bool push = false;
+          int32_t u = 0;
+          if (j < e) {
+            u = col[j];
+            if (ld_volatile((const uint32_t *)&core[u]) == 0xFFFFFFFFu) {
+              const int32_t old = atomicSub(&deg[u], 1);
+              if (old == level + 1) {
+                core[u] = level;
+                push = true;
+              }
+            }
+          }
+          warp_append(push, u, Fn, &ctl->fcnt[fn]);
+        }
+      }
+      if (!grid_sync(&ctl->bar, nblocks, &ctl->err, limit_ns)) return;
+      fc = fn;
+      cnt = ld_volatile(&ctl->fcnt[fc]);
+      ++priority;
+      ++rounds;
+    }
+    if (todo == 0) break;
+    // The empty next frontier fc (count 0) is the next scan's output and its
+    // successor's counter was reset during the last round, so the next scan
+    // can start without another barrier.
+    ++level;
+  }
+  if (tid == 0) {
+    ctl->degeneracy = degen;
+    ctl->rounds = rounds;
+    ctl->levels = levels;
+  }
+}
+
+}  // namespace
+
+size_t peel_ctl_bytes() { return sizeof(PeelCtl); }
+
+int peel_launch(const PeelArgs &a, cudaStream_t s, int *launches) {
+  int dev = 0, sms = 0, per_sm = 0, coop = 0;
+  MCE_CUDA(cudaGetDevice(&dev));
+  MCE_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  MCE_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+  if (!coop) return MCE_ENODEV;
+  MCE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, peel_kernel, PEEL_BLOCK, 0));
+  if (per_sm < 1) return MCE_ECUDA;
+  per_sm = per_sm > 2 ? 2 : per_sm;
+  int32_t n = (int32_t)a.n;
+  uint32_t m = (uint32_t)a.m;
+  PeelCtl *ctl = (PeelCtl *)a.ctl;
+  MCE_CUDA(cudaMemsetAsync(ctl, 0, sizeof(PeelCtl), s));
+  uint64_t limit = a.wait_limit_ns;
+  void *args[] = {(void *)&n,        (void *)&m,        (void *)&a.rp,     (void *)&a.col,
+                  (void *)&a.deg,    (void *)&a.core,   (void *)&a.prio,   (void *)&a.alistA,
+                  (void *)&a.alistB, (void *)&a.front0, (void *)&a.front1, (void *)&a.front2,
+                  (void *)&ctl,      (void *)&limit};
+  MCE_CUDA(cudaLaunchCooperativeKernel((void *)peel_kernel, dim3(sms * per_sm), dim3(PEEL_BLOCK),
+                                       args, 0, s));
+  if (launches) *launches += 1;
+  return MCE_OK;
+}
+
+int peel_read(const void *ctl_dev, int32_t *degeneracy, uint32_t *err, uint32_t *rounds,
+              cudaStream_t s) {
+  PeelCtl h;
+  MCE_CUDA(cudaMemcpyAsync(&h, ctl_dev, sizeof(PeelCtl), cudaMemcpyDeviceToHost, s));
+  MCE_CUDA(cudaStreamSynchronize(s));
+  if (degeneracy) *degeneracy = h.degeneracy;
+  if (err) *err = h.err;
+  if (rounds) *rounds = h.rounds;
+  return MCE_OK;
+}
+
+}  // namespace mce

@@ -1,0 +1,354 @@
+"""ctypes binding of libmce.so, the B200 maximal-clique enumerator.
+
+The library is C++/CUDA behind a C ABI (include/mce.h, include/mce_gen.h);
+this module only marshals numpy arrays in and out of it.  Importing fails
+loudly if the shared library has not been built: there is no fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libmce.so")
+HIST_MAX = 4096
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(
+        f"libmce.so not found at {LIB_PATH}; build it with `make -C mce-gpu_b200` "
+        "(or __graft_entry__.build())")
+_lib = C.CDLL(LIB_PATH)
+
+# status codes (include/mce.h)
+OK, EINVAL, ENOMEM, ECUDA, EIO, EFORMAT, ELIMIT, ETIMEOUT, ENODEV, ESTATE = (
+    0, -1, -2, -3, -4, -5, -6, -7, -8, -9)
+LEVEL_L1, LEVEL_L2 = 1, 2
+INDUCED_P, INDUCED_PX = 1, 2
+WL_OFF, WL_ON = 1, 2
+SCHED_PLAIN, SCHED_DEGREE, SCHED_LEARNED = 0, 1, 2
+
+
+class MceError(RuntimeError):
+    def __init__(self, code: int, what: str):
+        self.code = code
+        msg = _lib.mce_strerror(code).decode()
+        super().__init__(f"{what}: {msg} ({code})")
+
+
+class _Opts(C.Structure):
+    _fields_ = [("level", C.c_int32), ("induced", C.c_int32), ("worker_list", C.c_int32),
+                ("sched", C.c_int32), ("bitmap_width", C.c_int32),
+                ("warps_per_root", C.c_int32), ("donate_threshold", C.c_int32),
+                ("log_roots", C.c_int32), ("x_pivot", C.c_int32),
+                ("reserved", C.c_int32 * 7), ("stream", C.c_void_p)]
+
+
+class _Stats(C.Structure):
+    _fields_ = [("peel_ms", C.c_double), ("orient_ms", C.c_double), ("count_ms", C.c_double),
+                ("total_ms", C.c_double), ("degeneracy", C.c_int32),
+                ("max_later_degree", C.c_int32), ("max_degree", C.c_int64),
+                ("roots", C.c_int64), ("tree_nodes", C.c_uint64), ("donations", C.c_uint64),
+                ("kernel_launches", C.c_int32), ("error_flags", C.c_uint32),
+                ("class_roots", C.c_int64 * 8)]
+
+
+class _HGraph(C.Structure):
+    _fields_ = [("n", C.c_int64), ("m", C.c_int64), ("row_ptr", C.POINTER(C.c_int32)),
+                ("col", C.POINTER(C.c_int32)), ("num_graphs", C.c_int32),
+                ("vtx_offsets", C.POINTER(C.c_int64)), ("arc_offsets", C.POINTER(C.c_int64))]
+
+
+_P = C.c_void_p
+_sigs = {
+    "mce_opts_default": (None, [_P]),
+    "mce_strerror": (C.c_char_p, [C.c_int]),
+    "mce_version": (C.c_char_p, []),
+    "mce_hgraph_free": (None, [_P]),
+    "mce_hgraph_from_edges": (C.c_int, [_P, _P, C.c_int64, C.c_int64, _P]),
+    "mce_csr_validate": (C.c_int, [_P, _P, C.c_int64, C.c_int64]),
+    "mce_bel_read": (C.c_int, [C.c_char_p, _P]),
+    "mce_bel_write": (C.c_int, [C.c_char_p, _P]),
+    "mce_convert_to_bel": (C.c_int, [C.c_char_p, C.c_char_p, _P, _P]),
+    "mce_graph_upload": (C.c_int, [_P, _P, C.c_int64, C.c_int64, C.c_int32, _P, _P]),
+    "mce_graph_reload": (C.c_int, [_P, _P, _P, C.c_int64, C.c_int64, _P]),
+    "mce_graph_free": (C.c_int, [_P]),
+    "mce_degeneracy": (C.c_int, [_P, _P, _P, _P]),
+    "mce_split_csr": (C.c_int, [_P, _P, _P]),
+    "mce_count": (C.c_int, [_P, _P, _P, _P, _P]),
+    "mce_root_log": (C.c_int, [_P, _P]),
+    "mce_root_counts": (C.c_int, [_P, _P]),
+    "mce_gen_er": (C.c_int, [C.c_int64, C.c_double, C.c_uint64, C.c_int32, C.c_int32,
+                             C.c_int32, _P]),
+    "mce_gen_rmat": (C.c_int, [C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,
+                               C.c_uint64, _P]),
+    "mce_gen_ba": (C.c_int, [C.c_int64, C.c_int32, C.c_uint64, C.c_int32, C.c_int32,
+                             C.c_int32, _P]),
+    "mce_gen_chung_lu_batch": (C.c_int, [C.c_int32, C.c_int64, C.c_int64, C.c_double,
+                                         C.c_double, C.c_double, C.c_int32, C.c_int32,
+                                         C.c_int32, C.c_uint64, _P]),
+    "mce_gen_permute": (C.c_int, [_P, C.c_uint64, _P]),
+    "mce_hgraph_union": (C.c_int, [_P, _P]),
+    "mce_ego_subgraph": (C.c_int, [_P, _P, C.c_int64, C.c_int64, C.c_int64, _P, _P]),
+}
+for _name, (_res, _args) in _sigs.items():
+    _f = getattr(_lib, _name)
+    _f.restype = _res
+    _f.argtypes = _args
+
+# every entry point the C headers declare (checked by the CPU tests)
+EXPORTED = tuple(_sigs)
+
+
+def _check(rc: int, what: str) -> None:
+    if rc != OK:
+        raise MceError(rc, what)
+
+
+def _ptr(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def version() -> str:
+    return _lib.mce_version().decode()
+
+
+# ---------------------------------------------------------------------------
+# host graphs
+# ---------------------------------------------------------------------------
+@dataclass
+class HostGraph:
+    """A CSR graph (or a batch of them) in numpy arrays.
+
+    For a batch, row_ptr / col hold every graph back to back and
+    vtx_offsets / arc_offsets (num_graphs + 1 entries) locate graph g's rows
+    (n_g + 1 local offsets) and arcs (local ids).
+    """
+    row_ptr: np.ndarray
+    col: np.ndarray
+    n: int
+    m: int
+    num_graphs: int = 1
+    vtx_offsets: np.ndarray | None = None
+    arc_offsets: np.ndarray | None = None
+
+    def graph(self, g: int) -> "HostGraph":
+        """Graph g of a batch as a single graph."""
+        a, b = int(self.vtx_offsets[g]), int(self.vtx_offsets[g + 1])
+        c, d = int(self.arc_offsets[g]), int(self.arc_offsets[g + 1])
+        rp = self.row_ptr[a:b].copy()
+        return HostGraph(rp, self.col[c:d].copy(), b - a - 1, d - c)
+
+    def _as_struct(self) -> tuple[_HGraph, list]:
+        keep = []
+        h = _HGraph()
+        h.n, h.m, h.num_graphs = self.n, self.m, self.num_graphs
+        rp = np.ascontiguousarray(self.row_ptr, dtype=np.int32)
+        col = np.ascontiguousarray(self.col, dtype=np.int32)
+        vo = self.vtx_offsets if self.vtx_offsets is not None else np.array([0, self.n + 1], np.int64)
+        ao = self.arc_offsets if self.arc_offsets is not None else np.array([0, self.m], np.int64)
+        vo = np.ascontiguousarray(vo, dtype=np.int64)
+        ao = np.ascontiguousarray(ao, dtype=np.int64)
+        keep += [rp, col, vo, ao]
+        h.row_ptr = rp.ctypes.data_as(C.POINTER(C.c_int32))
+        h.col = col.ctypes.data_as(C.POINTER(C.c_int32))
+        h.vtx_offsets = vo.ctypes.data_as(C.POINTER(C.c_int64))
+        h.arc_offsets = ao.ctypes.data_as(C.POINTER(C.c_int64))
+        return h, keep
+
+
+def _take(h: _HGraph) -> HostGraph:
+    """Copy a library-owned mce_hgraph_t into numpy and release it."""
+    try:
+        G = h.num_graphs
+        nrp = h.n + G
+        rp = np.ctypeslib.as_array(h.row_ptr, shape=(nrp,)).copy() if nrp > 0 else np.zeros(1, np.int32)
+        col = (np.ctypeslib.as_array(h.col, shape=(h.m,)).copy() if h.m > 0
+               else np.zeros(0, np.int32))
+        vo = np.ctypeslib.as_array(h.vtx_offsets, shape=(G + 1,)).copy()
+        ao = np.ctypeslib.as_array(h.arc_offsets, shape=(G + 1,)).copy()
+        return HostGraph(rp, col, int(h.n), int(h.m), int(G), vo, ao)
+    finally:
+        _lib.mce_hgraph_free(C.byref(h))
+
+
+def from_edges(src, dst, n: int = 0) -> HostGraph:
+    s = np.ascontiguousarray(src, dtype=np.int64)
+    d = np.ascontiguousarray(dst, dtype=np.int64)
+    h = _HGraph()
+    _check(_lib.mce_hgraph_from_edges(_ptr(s), _ptr(d), len(s), n, C.byref(h)), "from_edges")
+    return _take(h)
+
+
+def validate(g: HostGraph) -> int:
+    rp = np.ascontiguousarray(g.row_ptr, dtype=np.int32)
+    col = np.ascontiguousarray(g.col, dtype=np.int32)
+    return _lib.mce_csr_validate(_ptr(rp), _ptr(col), g.n, g.m)
+
+
+def gen_er(n, p, seed, planted=0, cmin=6, cmax=12) -> HostGraph:
+    h = _HGraph()
+    _check(_lib.mce_gen_er(n, p, seed, planted, cmin, cmax, C.byref(h)), "gen_er")
+    return _take(h)
+
+
+def gen_rmat(scale, edge_factor, a, b, c, seed) -> HostGraph:
+    h = _HGraph()
+    _check(_lib.mce_gen_rmat(scale, edge_factor, a, b, c, seed, C.byref(h)), "gen_rmat")
+    return _take(h)
+
+
+def gen_ba(n, m, seed, planted=0, cmin=20, cmax=60) -> HostGraph:
+    h = _HGraph()
+    _check(_lib.mce_gen_ba(n, m, seed, planted, cmin, cmax, C.byref(h)), "gen_ba")
+    return _take(h)
+
+
+def gen_chung_lu_batch(num_graphs, n_min, n_max, gamma, deg_min, deg_max, max_planted,
+                       cmin, cmax, seed) -> HostGraph:
+    h = _HGraph()
+    _check(_lib.mce_gen_chung_lu_batch(num_graphs, n_min, n_max, gamma, deg_min, deg_max,
+                                       max_planted, cmin, cmax, seed, C.byref(h)),
+           "gen_chung_lu_batch")
+    return _take(h)
+
+
+def permute(g: HostGraph, seed: int) -> HostGraph:
+    s, keep = g._as_struct()
+    h = _HGraph()
+    _check(_lib.mce_gen_permute(C.byref(s), seed, C.byref(h)), "permute")
+    return _take(h)
+
+
+def union(batch: HostGraph) -> HostGraph:
+    s, keep = batch._as_struct()
+    h = _HGraph()
+    _check(_lib.mce_hgraph_union(C.byref(s), C.byref(h)), "union")
+    return _take(h)
+
+
+def ego_subgraph(g: HostGraph, seed_vertex: int, cap: int) -> tuple[HostGraph, np.ndarray]:
+    rp = np.ascontiguousarray(g.row_ptr, dtype=np.int32)
+    col = np.ascontiguousarray(g.col, dtype=np.int32)
+    vmap = np.zeros(cap, np.int32)
+    h = _HGraph()
+    _check(_lib.mce_ego_subgraph(_ptr(rp), _ptr(col), g.n, seed_vertex, cap, C.byref(h),
+                                 _ptr(vmap)), "ego_subgraph")
+    eg = _take(h)
+    return eg, vmap[:eg.n].copy()
+
+
+def bel_read(path: str) -> HostGraph:
+    h = _HGraph()
+    _check(_lib.mce_bel_read(path.encode(), C.byref(h)), f"bel_read({path})")
+    return _take(h)
+
+
+def bel_write(path: str, g: HostGraph) -> None:
+    s, keep = g._as_struct()
+    _check(_lib.mce_bel_write(path.encode(), C.byref(s)), f"bel_write({path})")
+
+
+def convert_to_bel(txt: str, bel: str) -> tuple[int, int]:
+    n = C.c_int64()
+    e = C.c_int64()
+    _check(_lib.mce_convert_to_bel(txt.encode(), bel.encode(), C.byref(n), C.byref(e)),
+           "convert_to_bel")
+    return n.value, e.value
+
+
+# ---------------------------------------------------------------------------
+# device graphs
+# ---------------------------------------------------------------------------
+@dataclass
+class CountResult:
+    total: int
+    hist: np.ndarray
+    stats: dict
+
+
+def _stats_dict(st: _Stats) -> dict:
+    d = {k: getattr(st, k) for k, _ in _Stats._fields_ if k != "class_roots"}
+    d["class_roots"] = list(st.class_roots)
+    return d
+
+
+class Graph:
+    """A graph resident on one GPU (wraps mce_graph_t)."""
+
+    def __init__(self, row_ptr: np.ndarray, col: np.ndarray, device: int = 0, stream=None):
+        self._h = C.c_void_p()
+        self.row_ptr = np.ascontiguousarray(row_ptr, dtype=np.int32)
+        self.col = np.ascontiguousarray(col, dtype=np.int32)
+        self.n = len(self.row_ptr) - 1
+        self.m = len(self.col)
+        _check(_lib.mce_graph_upload(_ptr(self.row_ptr), _ptr(self.col), self.n, self.m,
+                                     device, stream, C.byref(self._h)), "upload")
+
+    @classmethod
+    def from_host(cls, g: HostGraph, device: int = 0, stream=None) -> "Graph":
+        return cls(g.row_ptr[:g.n + 1], g.col, device, stream)
+
+    def reload_ptr(self, row_ptr_addr: int, col_addr: int, n: int, m: int, stream=None) -> None:
+        """Re-upload from raw host addresses (e.g. pinned buffers), no copy in Python."""
+        _check(_lib.mce_graph_reload(self._h, C.c_void_p(row_ptr_addr), C.c_void_p(col_addr), n,
+                                     m, stream), "reload")
+        self.n, self.m = n, m
+
+    def close(self) -> None:
+        if self._h:
+            _lib.mce_graph_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def count(self, *, sched=SCHED_PLAIN, bitmap_width=0, log_roots=False, level=LEVEL_L1,
+              induced=INDUCED_P, worker_list=WL_ON, donate_threshold=0, x_pivot=0,
+              stream=None) -> CountResult:
+        o = _Opts()
+        _lib.mce_opts_default(C.byref(o))
+        o.sched, o.bitmap_width, o.log_roots = sched, bitmap_width, int(bool(log_roots))
+        o.level, o.induced, o.worker_list = level, induced, worker_list
+        o.donate_threshold, o.x_pivot = donate_threshold, x_pivot
+        o.stream = stream
+        total = C.c_uint64()
+        hist = np.zeros(HIST_MAX, np.uint64)
+        st = _Stats()
+        _check(_lib.mce_count(self._h, C.byref(o), C.byref(total), _ptr(hist), C.byref(st)),
+               "count")
+        return CountResult(int(total.value), hist, _stats_dict(st))
+
+    def degeneracy(self) -> tuple[np.ndarray, np.ndarray, int]:
+        prio = np.zeros(max(self.n, 1), np.uint32)
+        core = np.zeros(max(self.n, 1), np.int32)
+        dg = C.c_int32()
+        _check(_lib.mce_degeneracy(self._h, _ptr(prio), _ptr(core), C.byref(dg)), "degeneracy")
+        return prio[:self.n], core[:self.n], int(dg.value)
+
+    def split_csr(self) -> tuple[np.ndarray, np.ndarray]:
+        split = np.zeros(max(self.n, 1), np.int32)
+        cs = np.zeros(max(self.m, 1), np.int32)
+        _check(_lib.mce_split_csr(self._h, _ptr(split), _ptr(cs)), "split_csr")
+        return split[:self.n], cs[:self.m]
+
+    def root_log(self) -> np.ndarray:
+        out = np.zeros(max(self.n, 1), np.uint64)
+        _check(_lib.mce_root_log(self._h, _ptr(out)), "root_log")
+        return out[:self.n]
+
+    def root_counts(self) -> np.ndarray:
+        out = np.zeros(max(self.n, 1), np.uint64)
+        _check(_lib.mce_root_counts(self._h, _ptr(out)), "root_counts")
+        return out[:self.n]

@@ -1,0 +1,163 @@
+"""CUDA path vs the CPU oracle: bit-exact counts, histograms, orders and trees."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import mce_b200 as mce
+import oracle
+from graphs import KNOWN, build
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CLI = os.path.join(ROOT, "mce-gpu_b200", "bin", "parallel_mce_on_gpus")
+
+
+def gpu_count(g, **kw):
+    with mce.Graph.from_host(g) as dg:
+        return dg.count(**kw)
+
+
+def assert_same(g, **kw):
+    r = gpu_count(g, **kw)
+    t, h, dg = oracle.count(g)
+    assert r.total == t, (r.total, t)
+    assert np.array_equal(r.hist, h)
+    assert r.stats["error_flags"] == 0
+    return r
+
+
+@pytest.mark.parametrize("name,make,total,sizes", KNOWN, ids=[k[0] for k in KNOWN])
+def test_known_answers(name, make, total, sizes):
+    r = gpu_count(make())
+    assert r.total == total
+    assert {int(i): int(r.hist[i]) for i in np.nonzero(r.hist)[0]} == sizes
+
+
+@pytest.mark.parametrize("seed", range(12))
+@pytest.mark.parametrize("width", [32, 64])
+def test_random_small(seed, width):
+    rng = np.random.default_rng(1000 + seed)
+    n = int(rng.integers(5, 400))
+    p = float(rng.uniform(0.01, 0.5))
+    g = mce.gen_er(n, p, seed, planted=int(rng.integers(0, 4)), cmin=4, cmax=min(n, 30))
+    assert_same(g, bitmap_width=width)
+
+
+def test_small_plain_config():
+    """ER(10000, 0.002), seed 1, + 20 planted cliques of size 6..12, 32-bit rows."""
+    g = mce.gen_er(10000, 0.002, 1, 20, 6, 12)
+    r = assert_same(g, bitmap_width=32)
+    assert r.total == 97157  # pinned: see tests/golden
+
+
+@pytest.mark.parametrize("maker", [
+    lambda: mce.gen_er(3000, 0.01, 3, 10, 6, 20),
+    lambda: mce.gen_rmat(11, 16, 0.57, 0.19, 0.19, 7),
+    lambda: mce.gen_ba(20000, 8, 5, 20, 20, 60),
+    lambda: build(5, [(0, 1), (1, 2), (2, 3), (3, 4)]),
+])
+def test_degeneracy_bit_exact(maker):
+    g = maker()
+    prio_o, core_o, dg_o = oracle.peel(g)
+    with mce.Graph.from_host(g) as dg:
+        prio, core, d = dg.degeneracy()
+        assert d == dg_o
+        assert np.array_equal(core, core_o)
+        assert np.array_equal(prio, prio_o)
+        split, cs = dg.split_csr()
+    split_o, cs_o = oracle.orient(g, prio_o)
+    assert np.array_equal(split, split_o)
+    assert np.array_equal(cs, cs_o)
+
+
+@pytest.mark.parametrize("maker", [
+    lambda: mce.gen_er(4000, 0.01, 9, 12, 8, 40),
+    lambda: mce.gen_rmat(11, 16, 0.57, 0.19, 0.19, 7),
+])
+def test_per_root_counts_and_tree_sizes(maker):
+    g = maker()
+    tot, h, rc_o, rn_o = oracle.roots(g)
+    with mce.Graph.from_host(g) as dg:
+        r = dg.count(log_roots=True)
+        rc, rn = dg.root_counts(), dg.root_log()
+    assert r.total == tot
+    assert np.array_equal(rc, rc_o)
+    assert np.array_equal(rn, rn_o)  # same pivot rule and tie-break -> same trees
+    assert r.stats["tree_nodes"] == int(rn_o.sum())
+
+
+def test_rmat_scale13_wide_roots():
+    """R-MAT (0.57,0.19,0.19,0.05) scale 13: later degrees up to 90 (wide engine)."""
+    g = mce.gen_rmat(13, 16, 0.57, 0.19, 0.19, 7)
+    r = assert_same(g)
+    assert r.stats["class_roots"][2] > 0  # wide-engine roots exercised
+
+
+def test_hub_with_many_earlier_neighbours():
+    """A hub of degree 4999 lands in the wide engine through its earlier list."""
+    base = mce.gen_er(5000, 0.002, 11, 5, 5, 12)
+    s, d = [], []
+    for v in range(base.n):
+        for w in base.col[base.row_ptr[v]:base.row_ptr[v + 1]]:
+            if v < w:
+                s.append(v); d.append(int(w))
+    s += [0] * 4999
+    d += list(range(1, 5000))
+    g = mce.from_edges(np.array(s), np.array(d), 5000)
+    r = assert_same(g)
+    assert r.stats["class_roots"][2] >= 1
+
+
+def test_cliques_wider_than_64():
+    """Planted cliques of 70..300 vertices: roots with d+ up to 299."""
+    g = mce.gen_er(2000, 0.005, 21, 6, 70, 300)
+    assert_same(g)
+
+
+def test_ba_with_planted_cliques():
+    g = mce.gen_ba(100000, 8, 23, 40, 20, 60)
+    assert_same(g)
+
+
+def test_chung_lu_batch_union():
+    b = mce.gen_chung_lu_batch(48, 64, 16384, 2.3, 8, 32, 5, 5, 40, 11)
+    assert_same(mce.union(b))
+
+
+def test_permutation_invariance():
+    g = mce.gen_rmat(12, 16, 0.57, 0.19, 0.19, 3)
+    a = gpu_count(g)
+    b = gpu_count(mce.permute(g, 5))
+    assert a.total == b.total and np.array_equal(a.hist, b.hist)
+
+
+def test_degenerate_graphs():
+    assert gpu_count(build(10, [])).total == 0
+    assert gpu_count(build(2, [(0, 1)])).total == 1
+    g = mce.HostGraph(np.zeros(1, np.int32), np.zeros(0, np.int32), 0, 0)
+    assert gpu_count(g).total == 0
+
+
+def test_repeated_calls_identical():
+    g = mce.gen_ba(50000, 6, 1, 10, 10, 30)
+    with mce.Graph.from_host(g) as dg:
+        a = dg.count()
+        b = dg.count(bitmap_width=64)
+        c = dg.count()
+    assert a.total == b.total == c.total
+    assert np.array_equal(a.hist, c.hist) and np.array_equal(a.hist, b.hist)
+
+
+def test_cli_matches_oracle(tmp_path):
+    g = mce.gen_er(3000, 0.01, 4, 8, 6, 16)
+    bel = str(tmp_path / "g.bel")
+    mce.bel_write(bel, g)
+    r = subprocess.run([CLI, "-m", "mce", "-g", bel, "-d", "0", "-p", "l1", "-i", "p", "-w", "wl"],
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    t, _, dgn = oracle.count(g)
+    assert f"Found {t} maximal cliques in total." in r.stdout
+    assert f"Max Core = {dgn}" in r.stdout
+    assert "Degeneracy ordering time:" in r.stdout and "count time" in r.stdout

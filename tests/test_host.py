@@ -1,0 +1,167 @@
+"""Host-side library code: generators, .bel I/O, CSR checks, exported symbols, CLI."""
+import ctypes
+import glob
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import mce_b200 as mce
+import oracle
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CLI = os.path.join(ROOT, "mce-gpu_b200", "bin", "parallel_mce_on_gpus")
+
+
+def declared_functions():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        src = open(h).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        for m in re.finditer(r"^[A-Za-z_][\w \*]*?\b(mce_\w+)\s*\(", src, flags=re.M):
+            names.add(m.group(1))
+    return sorted(names)
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(mce.LIB_PATH)
+    names = declared_functions()
+    assert len(names) > 20
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_generators_deterministic():
+    a = mce.gen_rmat(12, 16, 0.57, 0.19, 0.19, 7)
+    b = mce.gen_rmat(12, 16, 0.57, 0.19, 0.19, 7)
+    c = mce.gen_rmat(12, 16, 0.57, 0.19, 0.19, 8)
+    assert np.array_equal(a.col, b.col) and np.array_equal(a.row_ptr, b.row_ptr)
+    assert not (a.m == c.m and np.array_equal(a.col, c.col))
+    for g in (a, mce.gen_er(2000, 0.01, 1, 5), mce.gen_ba(5000, 4, 3, 5, 5, 10)):
+        assert mce.validate(g) == 0
+
+
+def test_er_config_shape():
+    """ER(10000, 0.002) + 20 planted cliques of size 6..12 (the small plain config)."""
+    g = mce.gen_er(10000, 0.002, 1, 20, 6, 12)
+    assert g.n == 10000
+    assert 190_000 < g.m < 215_000  # ~1e5 edges from G(n,p) + planted pairs
+
+
+def test_chung_lu_batch_layout():
+    b = mce.gen_chung_lu_batch(16, 64, 2048, 2.3, 8, 32, 5, 5, 40, 11)
+    assert b.num_graphs == 16
+    assert b.vtx_offsets[-1] == b.n + 16 and b.arc_offsets[-1] == b.m
+    u = mce.union(b)
+    assert mce.validate(u) == 0
+    tot_u = oracle.count(u)[0]
+    assert tot_u == sum(oracle.count(b.graph(i))[0] for i in range(16))
+
+
+def test_permutation_invariance_oracle():
+    g = mce.gen_er(800, 0.03, 2, 6, 6, 14)
+    p = mce.permute(g, 99)
+    assert mce.validate(p) == 0
+    t, h, _ = oracle.count(g)
+    tp, hp, _ = oracle.count(p)
+    assert t == tp and np.array_equal(h, hp)
+
+
+def test_bel_roundtrip(tmp_path):
+    g = mce.gen_er(500, 0.05, 3, 3, 5, 9)
+    path = str(tmp_path / "g.bel")
+    mce.bel_write(path, g)
+    assert os.path.getsize(path) == 24 * g.m
+    raw = np.fromfile(path, dtype=np.uint64).reshape(-1, 3)
+    # record layout: dst, src, 0 ; sorted by (src, dst)
+    assert np.all(raw[:, 2] == 0)
+    src, dst = raw[:, 1], raw[:, 0]
+    assert np.all(np.diff(src.astype(np.int64)) >= 0)
+    h = mce.bel_read(path)
+    # n = max src + 1 (trailing isolated vertices vanish, as in the reference)
+    nmax = int(src.max()) + 1
+    assert h.n == nmax and h.m == g.m
+    assert np.array_equal(h.col, g.col)
+    assert np.array_equal(h.row_ptr[:nmax + 1], g.row_ptr[:nmax + 1])
+
+
+def test_bel_rejects_bad_files(tmp_path):
+    p = tmp_path / "bad.bel"
+    p.write_bytes(b"\0" * 25)
+    with pytest.raises(mce.MceError) as e:
+        mce.bel_read(str(p))
+    assert e.value.code == mce.EFORMAT
+    # unsorted sources
+    recs = np.array([[1, 2, 0], [2, 1, 0]], np.uint64)  # (dst, src): src 2 then 1
+    p.write_bytes(recs.tobytes())
+    with pytest.raises(mce.MceError):
+        mce.bel_read(str(p))
+    with pytest.raises(mce.MceError) as e:
+        mce.bel_read(str(tmp_path / "missing.bel"))
+    assert e.value.code == mce.EIO
+
+
+def test_convert_to_bel(tmp_path):
+    txt = tmp_path / "g.txt"
+    txt.write_text("# comment\n0 1\n1 2\n2 0\n2 2\n3 1\n% other\n1 0\n")
+    bel = str(tmp_path / "g.bel")
+    n, e = mce.convert_to_bel(str(txt), bel)
+    assert (n, e) == (4, 4)  # edges {01, 12, 02, 13}; self-loop dropped; duplicate merged
+    g = mce.bel_read(bel)
+    assert g.n == 4 and g.m == 8
+    assert list(g.col) == [1, 2, 0, 2, 3, 0, 1, 1]
+    assert oracle.count(g)[0] == 2  # triangle 012 + edge 13
+
+
+def test_validate_rejects_asymmetric():
+    rp = np.array([0, 1, 1], np.int32)
+    col = np.array([1], np.int32)
+    g = mce.HostGraph(rp, col, 2, 1)
+    assert mce.validate(g) == mce.EFORMAT
+
+
+def test_ego_subgraph():
+    g = mce.gen_er(400, 0.05, 4)
+    eg, vmap = mce.ego_subgraph(g, 7, 64)
+    assert eg.n <= 64 and vmap[0] == 7
+    assert mce.validate(eg) == 0
+    # every ego edge is an edge of g
+    for u in range(eg.n):
+        for w in eg.col[eg.row_ptr[u]:eg.row_ptr[u + 1]]:
+            a, b = vmap[u], vmap[w]
+            assert b in g.col[g.row_ptr[a]:g.row_ptr[a + 1]]
+
+
+@pytest.mark.skipif(not os.path.exists(CLI), reason="CLI not built")
+class TestCli:
+    def run(self, *args):
+        return subprocess.run([CLI, *args], capture_output=True, text=True, timeout=60)
+
+    def test_missing_task(self):
+        r = self.run("-g", "x.bel")
+        assert r.returncode == 0 and "Must specify -m option" in r.stderr
+
+    def test_bad_options_exit_zero(self):
+        for args, msg in [(("-m", "foo"), "Unrecognized -m option"),
+                          (("-m", "mce", "-g", "a", "-d", "0", "-p", "l3"), "Unrecognized -p option"),
+                          (("-m", "mce", "-g", "a", "-d", "0", "-p", "l1", "-i", "q"), "Unrecognized -i option"),
+                          (("-m", "mce", "-g", "a", "-p", "l1", "-i", "p", "-w", "wl"), "Must specify -d option"),
+                          (("-m", "mce-bd-eval", "-g", "a", "-d", "0", "-p", "l1", "-i", "p", "-w", "nowl"),
+                           "No breakdown for kernels without worker list")]:
+            r = self.run(*args)
+            assert r.returncode == 0 and msg in r.stderr, (args, r.stderr)
+
+    def test_help(self):
+        r = self.run("-h")
+        assert r.returncode == 0 and "Usage:" in r.stderr
+
+    def test_convert_task(self, tmp_path):
+        txt = tmp_path / "g.txt"
+        txt.write_text("0 1\n1 2\n2 0\n")
+        bel = tmp_path / "g.bel"
+        r = self.run("-m", "convert", "-g", str(txt), "-r", str(bel))
+        assert r.returncode == 0
+        assert "Main Task = convert" in r.stdout and "n = 3 and m = 3" in r.stdout
+        assert os.path.getsize(bel) == 6 * 24
