@@ -30,8 +30,8 @@ namespace mce {
 struct PeelCtl {
   GridBarrier bar;
   uint32_t err;
-  uint32_t fcnt[3];    // frontier sizes, rotating: cur, next, to-reset
-  uint32_t acnt[3];    // alive-list sizes, rotating
+  uint32_t fcnt[3];    // frontier sizes, one slot per phase mod 3
+  uint32_t acnt[3];    // alive-list sizes, one slot per scan mod 3
   uint32_t amin[3];    // min degree over the alive list written by a scan
   int32_t degeneracy;
   uint32_t rounds;
@@ -74,7 +74,7 @@ __global__ void __launch_bounds__(PEEL_BLOCK)
     prio[v] = m;
     alistA[v] = (int32_t)v;
   }
-  if (tid == 0) {
+  if (tid == 0) {  // phase/scan 0 reads acnt[0]; every other counter starts at 0
     ctl->fcnt[0] = ctl->fcnt[1] = ctl->fcnt[2] = 0;
     ctl->acnt[0] = (uint32_t)n;
     ctl->acnt[1] = ctl->acnt[2] = 0;
@@ -85,25 +85,25 @@ __global__ void __launch_bounds__(PEEL_BLOCK)
   int64_t todo = n;
   int32_t level = 0, degen = 0;
   uint32_t priority = 0, rounds = 0, levels = 0;
-  // Counter rotation invariant at the start of every phase: fcnt[fc] is the
-  // current frontier's size (0 before a scan) and fcnt[(fc + 1) % 3] == 0;
-  // each phase resets fcnt[(fc + 2) % 3], the counter that becomes "next"
-  // once fc advances.  The alive-list counters rotate the same way.
-  int fc = 0;     // index of the current frontier counter / buffer
-  int ac = 0;     // index of the current alive counter
-  int al = 0;     // which alive buffer is current
-
+  // Phases (scans and rounds) are numbered q = 0, 1, 2, ...  Phase q appends
+  // its output frontier to buffer/counter slot (q + 1) % 3 and resets slot
+  // (q + 2) % 3; after barrier q every thread reads slot (q + 1) % 3.  A
+  // slot is reset two phases after it was read, so a slow reader can never
+  // see a counter that another block has already started to refill.  Scans
+  // are numbered s the same way for the alive-list counters (3 slots) and
+  // buffers (2 slots).
+  uint32_t q = 0, s = 0;
   while (todo > 0) {
-    // ---- level scan: split the alive list into {deg == level} and the rest
-    const uint32_t nalive = ld_volatile(&ctl->acnt[ac]);
-    const int an = (ac + 1) % 3, ar = (ac + 2) % 3;
-    const int32_t *A = alist[al];
-    int32_t *A2 = alist[al ^ 1];
-    int32_t *F = fr[fc];
-    if (tid == 0) {  // reset the counters two phases ahead
-      ctl->acnt[ar] = 0;
-      ctl->amin[ar] = 0xFFFFFFFFu;
-      ctl->fcnt[(fc + 2) % 3] = 0;
+    // ---- scan: split the alive list into {deg == level} and {deg > level}
+    const uint32_t nalive = ld_volatile(&ctl->acnt[s % 3]);
+    const int32_t *A = alist[s & 1];
+    int32_t *A2 = alist[(s + 1) & 1];
+    const int fo = (q + 1) % 3, ao = (s + 1) % 3;
+    int32_t *F = fr[fo];
+    if (tid == 0) {
+      ctl->acnt[(s + 2) % 3] = 0;
+      ctl->amin[(s + 2) % 3] = 0xFFFFFFFFu;
+      ctl->fcnt[(q + 2) % 3] = 0;
     }
     {
       uint32_t mymin = 0xFFFFFFFFu;
@@ -119,21 +119,21 @@ __global__ void __launch_bounds__(PEEL_BLOCK)
         const bool inF = live && d == level;
         const bool keep = live && d > level;
         if (inF) core[v] = level;
-        warp_append(inF, v, F, &ctl->fcnt[fc]);
-        warp_append(keep, v, A2, &ctl->acnt[an]);
+        warp_append(inF, v, F, &ctl->fcnt[fo]);
+        warp_append(keep, v, A2, &ctl->acnt[ao]);
         if (keep) mymin = min(mymin, (uint32_t)d);
       }
       mymin = __reduce_min_sync(MCE_FULL, mymin);
-      if (lane == 0 && mymin != 0xFFFFFFFFu) atomicMin(&ctl->amin[an], mymin);
+      if (lane == 0 && mymin != 0xFFFFFFFFu) atomicMin(&ctl->amin[ao], mymin);
     }
     if (!grid_sync(&ctl->bar, nblocks, &ctl->err, limit_ns)) return;
-    ac = an;
-    al ^= 1;
-    uint32_t cnt = ld_volatile(&ctl->fcnt[fc]);
+    ++q;
+    ++s;
+    uint32_t cnt = ld_volatile(&ctl->fcnt[q % 3]);
     if (cnt == 0) {
       // no vertex of degree `level` remains: jump to the smallest degree
       // (a rescan at that level always finds the vertex that attains it)
-      const uint32_t mn = ld_volatile(&ctl->amin[ac]);
+      const uint32_t mn = ld_volatile(&ctl->amin[s % 3]);
       if (mn == 0xFFFFFFFFu || (int32_t)mn <= level) {
         if (tid == 0) atomicOr(&ctl->err, MCE_ERR_QUEUE);  // inconsistent state: stop
         break;
@@ -142,14 +142,15 @@ __global__ void __launch_bounds__(PEEL_BLOCK)
       continue;
     }
     ++levels;
-    // ---- rounds of this level
+    // ---- rounds of this level: phase q reads frontier q % 3
     while (cnt > 0) {
       degen = level;
       todo -= cnt;
       if (todo == 0) break;  // the final round keeps priority = m
-      const int fn = (fc + 1) % 3;
-      if (tid == 0) ctl->fcnt[(fc + 2) % 3] = 0;
-      int32_t *Fc = fr[fc], *Fn = fr[fn];
+      const int fn = (q + 1) % 3;
+      if (tid == 0) ctl->fcnt[(q + 2) % 3] = 0;
+      const int32_t *Fc = fr[q % 3];
+      int32_t *Fn = fr[fn];
       for (int64_t i = tid; i < cnt; i += nthr) prio[Fc[i]] = priority;
       for (int64_t i = gwarp; i < cnt; i += nwarps) {
         const int32_t v = Fc[i];
@@ -172,15 +173,12 @@ __global__ void __launch_bounds__(PEEL_BLOCK)
         }
       }
       if (!grid_sync(&ctl->bar, nblocks, &ctl->err, limit_ns)) return;
-      fc = fn;
-      cnt = ld_volatile(&ctl->fcnt[fc]);
+      ++q;
+      cnt = ld_volatile(&ctl->fcnt[q % 3]);
       ++priority;
       ++rounds;
     }
     if (todo == 0) break;
-    // The empty next frontier fc (count 0) is the next scan's output and its
-    // successor's counter was reset during the last round, so the next scan
-    // can start without another barrier.
     ++level;
   }
   if (tid == 0) {

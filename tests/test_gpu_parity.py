@@ -49,7 +49,7 @@ def test_small_plain_config():
     """ER(10000, 0.002), seed 1, + 20 planted cliques of size 6..12, 32-bit rows."""
     g = mce.gen_er(10000, 0.002, 1, 20, 6, 12)
     r = assert_same(g, bitmap_width=32)
-    assert r.total == 97157  # pinned: see tests/golden
+    assert r.total == 97157  # the reference binary prints the same count (tests/golden)
 
 
 @pytest.mark.parametrize("maker", [
