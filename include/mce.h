@@ -204,6 +204,34 @@ int mce_root_log(mce_graph_t g, uint64_t *nodes_out);
  * opts.log_roots = 1 (n entries, 0 for non-roots).                          */
 int mce_root_counts(mce_graph_t g, uint64_t *count_out);
 
+/* ---- allocation-free search ------------------------------------------------ */
+/* Bytes of the file-scope device array that mce_count_oriented_noalloc uses
+ * as scratch.  Every GPU that loads libmce.so holds this array until the
+ * process exits.                                                             */
+#define MCE_NOALLOC_SCRATCH_BYTES (32u << 20)
+
+/* Search an oriented graph that is already in device memory without
+ * allocating anything.  No counterpart in the reference: it exists for
+ * callers that cannot call cudaMalloc - a process whose device memory is
+ * owned by another allocator (for example a framework's caching allocator
+ * that reserved the GPU), or a latency-critical loop where cudaMalloc's
+ * implicit device synchronisation is not acceptable.
+ *
+ * Inputs (device pointers, caller-owned): d_row_ptr (n+1), d_split (n) and
+ * d_col_split (m) - the oriented CSR that mce_split_csr returns - and
+ * d_roots (num_roots vertex ids).  Output: d_hist (MCE_HIST_MAX uint64,
+ * device) receives the number of maximal cliques of each size found from
+ * those roots; the call zeroes it first.  Every root must have 1 to 32
+ * later and at most 1024 earlier neighbours; otherwise nothing is searched
+ * and MCE_ELIMIT is returned.  Work is queued on `stream` (NULL = legacy
+ * default stream) and the call waits for it.  The call uses the
+ * MCE_NOALLOC_SCRATCH_BYTES array: the first call on a device looks up that
+ * array's address (make it before any stream capture), and calls that
+ * overlap on the GPU race on the array, so serialise them.                   */
+int mce_count_oriented_noalloc(const int32_t *d_row_ptr, const int32_t *d_split,
+                               const int32_t *d_col_split, const int32_t *d_roots,
+                               int64_t num_roots, uint64_t *d_hist, void *stream);
+
 /* Text for a status code. */
 const char *mce_strerror(int code);
 

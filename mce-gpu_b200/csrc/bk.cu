@@ -21,6 +21,7 @@
 // Tie-breaking: the pivot with the lowest index among the best scores, so
 // per-root tree sizes are deterministic.
 #include <climits>
+#include <cstring>
 
 #include "common.cuh"
 #include "kernels.h"
@@ -635,6 +636,131 @@ int bk_launch(int cls, int word_bits, const BKArgs &a, int grid, int block, int 
   MCE_CUDA(cudaGetLastError());
   if (launches) *launches += 1;
   return MCE_OK;
+}
+
+// ===========================================================================
+// Allocation-free search entry point.
+//
+// For callers that cannot allocate device memory: processes whose GPU memory
+// is owned entirely by another allocator (a framework's caching allocator
+// that has reserved the device), and latency-critical loops in which
+// cudaMalloc's implicit device-wide synchronisation is not acceptable.  The
+// caller passes an oriented graph, a root list and a histogram, all already
+// in device memory; the search runs the 32-wide register engine with its
+// per-warp scratch in the file-scope array below, which every GPU that loads
+// this library holds until the process exits.
+//
+// Set-up: the first call on a device (with that device current) resolves the
+// array's device address with cudaGetSymbolAddress and caches it; make that
+// first call before any stream capture.  Every call shares the array and
+// clears the part that must start at zero, so calls whose work overlaps on
+// the GPU race with each other: serialise them (one stream, or events).
+// ===========================================================================
+namespace {
+
+constexpr size_t NOALLOC_CTL_BYTES = 1024;  // ShapeInfo, fetch counters, status, nodes
+constexpr size_t NOALLOC_SLAB_WORDS = REG_XCAP;  // u64 words per warp: 2 x REG_XCAP u32 rows
+static_assert(MCE_NOALLOC_SCRATCH_BYTES % 256 == 0, "scratch size");
+
+static __device__ __align__(256) unsigned long long g_noalloc_scratch[MCE_NOALLOC_SCRATCH_BYTES / 8];
+
+struct NoallocCtl {
+  ShapeInfo shape;
+  uint32_t fetch[8];
+  uint32_t err[4];
+  unsigned long long nodes[4];
+};
+static_assert(sizeof(NoallocCtl) <= NOALLOC_CTL_BYTES, "control block");
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+unsigned long long *g_noalloc_addr[NOALLOC_MAX_DEVICES];  // host cache of device addresses
+bool g_noalloc_ready[NOALLOC_MAX_DEVICES];
+
+int noalloc_scratch(int dev, unsigned long long **out) {
+  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return MCE_ELIMIT;
+  if (!g_noalloc_ready[dev]) {
+    // the host-side name g_noalloc_scratch is not a device address: resolve it
+    void *p = nullptr;
+    MCE_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    g_noalloc_addr[dev] = (unsigned long long *)p;
+    g_noalloc_ready[dev] = true;
+  }
+  *out = g_noalloc_addr[dev];
+  return MCE_OK;
+}
+
+// Every root must fit the 32-wide engine: 1..32 later and <= REG_XCAP
+// earlier neighbours.  A root outside those limits sets err[0].
+__global__ void noalloc_check_kernel(const int32_t *rp, const int32_t *split,
+                                     const int32_t *roots, uint32_t num_roots, NoallocCtl *ctl) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    ctl->shape.cls_off[CLS_R32] = 0;
+    ctl->shape.cls_off[CLS_R32 + 1] = num_roots;
+  }
+  if (i >= num_roots) return;
+  const int32_t r = roots[i];
+  const int32_t dplus = rp[r + 1] - split[r], dminus = split[r] - rp[r];
+  if (dplus < 1 || dplus > 32 || dminus > REG_XCAP) atomicOr(&ctl->err[0], MCE_ERR_DEGREE);
+}
+
+}  // namespace
+
+extern "C" int mce_count_oriented_noalloc(const int32_t *d_row_ptr, const int32_t *d_split,
+                                          const int32_t *d_col_split, const int32_t *d_roots,
+                                          int64_t num_roots, uint64_t *d_hist, void *stream) {
+  if (num_roots < 0 || !d_hist ||
+      (num_roots > 0 && (!d_row_ptr || !d_split || !d_col_split || !d_roots)))
+    return MCE_EINVAL;
+  if (num_roots >= ((int64_t)1 << 31)) return MCE_ELIMIT;
+  int dev = 0, sms = 0, per_sm = 0;
+  MCE_CUDA(cudaGetDevice(&dev));
+  unsigned long long *base = nullptr;
+  int rc = noalloc_scratch(dev, &base);
+  if (rc) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  NoallocCtl *ctl = (NoallocCtl *)base;
+  MCE_CUDA(cudaMemsetAsync(ctl, 0, NOALLOC_CTL_BYTES, s));
+  MCE_CUDA(cudaMemsetAsync(d_hist, 0, sizeof(uint64_t) * MCE_HIST_MAX, s));
+  const uint32_t nr = (uint32_t)num_roots;
+  noalloc_check_kernel<<<(nr + 255) / 256 + 1, 256, 0, s>>>(d_row_ptr, d_split, d_roots, nr, ctl);
+  MCE_CUDA(cudaGetLastError());
+  uint32_t err = 0;
+  MCE_CUDA(cudaMemcpyAsync(&err, &ctl->err[0], sizeof(err), cudaMemcpyDeviceToHost, s));
+  MCE_CUDA(cudaStreamSynchronize(s));
+  if (err) return MCE_ELIMIT;
+  if (nr == 0) return MCE_OK;
+  // as many whole blocks of warps as the occupancy, the roots and the array allow
+  MCE_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  MCE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bk_reg_kernel<uint32_t, 1>,
+                                                         REG_BLOCK, 0));
+  const int wpb = REG_BLOCK / 32;
+  const int64_t slab_warps =
+      (int64_t)((MCE_NOALLOC_SCRATCH_BYTES - NOALLOC_CTL_BYTES) / (NOALLOC_SLAB_WORDS * 8));
+  int64_t blocks = (int64_t)sms * (per_sm > 0 ? per_sm : 1);
+  blocks = blocks < slab_warps / wpb ? blocks : slab_warps / wpb;
+  const int64_t want = ((int64_t)nr + REG_CHUNK * wpb - 1) / (REG_CHUNK * wpb);
+  if (want < blocks) blocks = want;
+  BKArgs a;
+  memset(&a, 0, sizeof(a));
+  a.rp = d_row_ptr;
+  a.split = d_split;
+  a.cs = d_col_split;
+  a.roots = d_roots;
+  a.shape = &ctl->shape;
+  a.fetch = ctl->fetch;
+  a.hist = (unsigned long long *)d_hist;
+  a.nodes = ctl->nodes;
+  a.err = &ctl->err[1];
+  a.slab = base + NOALLOC_CTL_BYTES / 8;
+  a.slab_words = NOALLOC_SLAB_WORDS;
+  a.dcap = 32;
+  a.xcap = REG_XCAP;
+  bk_reg_kernel<uint32_t, 1><<<(unsigned)blocks, REG_BLOCK, 0, s>>>(a, CLS_R32);
+  MCE_CUDA(cudaGetLastError());
+  MCE_CUDA(cudaMemcpyAsync(&err, &ctl->err[1], sizeof(err), cudaMemcpyDeviceToHost, s));
+  MCE_CUDA(cudaStreamSynchronize(s));
+  return err ? MCE_ELIMIT : MCE_OK;
 }
 
 }  // namespace mce

@@ -80,6 +80,7 @@ _sigs = {
     "mce_count": (C.c_int, [_P, _P, _P, _P, _P]),
     "mce_root_log": (C.c_int, [_P, _P]),
     "mce_root_counts": (C.c_int, [_P, _P]),
+    "mce_count_oriented_noalloc": (C.c_int, [_P, _P, _P, _P, C.c_int64, _P, _P]),
     "mce_gen_er": (C.c_int, [C.c_int64, C.c_double, C.c_uint64, C.c_int32, C.c_int32,
                              C.c_int32, _P]),
     "mce_gen_rmat": (C.c_int, [C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,
