@@ -58,6 +58,8 @@ struct mce_graph {
   unsigned long long *root_nodes = nullptr, *root_count = nullptr;
   unsigned long long *slab = nullptr;
   size_t slab_bytes = 0;
+  void *qbuf[NCLS] = {nullptr};   // task queue per engine class
+  size_t qbytes[NCLS] = {0};
   bool logged = false;
   // host copies of the last call
   ShapeInfo shape_h{};
@@ -68,6 +70,9 @@ struct mce_graph {
 namespace {
 
 constexpr uint64_t WAIT_LIMIT_NS = 20ull * 1000 * 1000 * 1000;  // 20 s per barrier wait
+constexpr uint64_t IDLE_LIMIT_NS = 30ull * 1000 * 1000 * 1000;  // 30 s without any progress
+constexpr uint32_t QUEUE_CAP = 1u << 14;                        // tasks per class queue
+constexpr int DEFAULT_DONATE_MIN = 10;  // the reference's SZTH (mce/parameter.cuh:5)
 
 void free_graph_bufs(mce_graph *g) {
   dfree(g->rp); dfree(g->col); dfree(g->cs); dfree(g->split);
@@ -178,6 +183,25 @@ int read_shape(mce_graph *g, cudaStream_t s) {
   return MCE_OK;
 }
 
+// Queue of class c laid out in one buffer: header | seq[cap] | payload.
+int ensure_queue(mce_graph *g, int c, uint32_t words, QueueView *out) {
+  const size_t hdr = 256, seq = (size_t)QUEUE_CAP * 4;
+  const size_t need = hdr + seq + (size_t)QUEUE_CAP * words * 8;
+  if (need > g->qbytes[c]) {
+    dfree(g->qbuf[c]);
+    g->qbytes[c] = 0;
+    MCE_CUDA(cudaMalloc(&g->qbuf[c], need));
+    g->qbytes[c] = need;
+  }
+  char *b = (char *)g->qbuf[c];
+  out->hdr = (QueueHdr *)b;
+  out->seq = (uint32_t *)(b + hdr);
+  out->pay = (unsigned long long *)(b + hdr + seq);
+  out->cap = QUEUE_CAP;
+  out->words = words;
+  return MCE_OK;
+}
+
 int ensure_slab(mce_graph *g, size_t bytes) {
   if (bytes <= g->slab_bytes) return MCE_OK;
   dfree(g->slab);
@@ -278,6 +302,7 @@ int mce_graph_free(mce_graph_t g) {
   dfree(g->nodes);
   dfree(g->slab);
   dfree(g->sort_tmp);
+  for (auto &q : g->qbuf) dfree(q);
   for (auto &e : g->ev)
     if (e) cudaEventDestroy(e);
   if (g->own) cudaStreamDestroy(g->own);
@@ -351,6 +376,7 @@ int mce_count(mce_graph_t g, const mce_opts_t *opts, uint64_t *total, uint64_t *
   const ShapeInfo &sh = g->shape_h;
   if (sh.cls_cnt[CLS_BIG]) return MCE_ELIMIT;
   // search scratch
+  const bool share = o.worker_list != MCE_WL_OFF;
   int grid[NCLS] = {0}, block[NCLS] = {0}, smem[NCLS] = {0};
   const int dcap = (int)(sh.max_dplus > 0 ? sh.max_dplus : 1);
   const int xcap = (int)(sh.max_dminus_mem > 0 ? sh.max_dminus_mem : 1);
@@ -359,9 +385,11 @@ int mce_count(mce_graph_t g, const mce_opts_t *opts, uint64_t *total, uint64_t *
     if (!sh.cls_cnt[c]) continue;
     int warps = 0;
     if ((rc = bk_warps_for_class(c, g->sms, &warps, &block[c], &smem[c]))) return rc;
-    // never more warps than roots (rounded up to whole blocks)
+    // never more warps than roots (rounded up to whole blocks); with task
+    // sharing keep at least a full wave so idle warps can take subtrees
     const int wpb = block[c] / 32;
     int64_t want = c == CLS_MEM ? (int64_t)sh.cls_cnt[c] : ((int64_t)sh.cls_cnt[c] + 3) / 4;
+    if (share) want = want > warps ? want : warps;
     if (want < warps) warps = (int)((want + wpb - 1) / wpb) * wpb;
     grid[c] = warps / wpb;
     const size_t need = (size_t)warps * bk_slab_words(c, dcap, xcap) * 8;
@@ -396,12 +424,19 @@ int mce_count(mce_graph_t g, const mce_opts_t *opts, uint64_t *total, uint64_t *
   a.slab = g->slab;
   a.dcap = dcap;
   a.xcap = xcap;
+  a.donate_min = o.donate_threshold > 0 ? o.donate_threshold : DEFAULT_DONATE_MIN;
+  a.wait_limit_ns = IDLE_LIMIT_NS;
   const int wbits = o.bitmap_width == 64 ? 64 : 32;
   // widest roots first so the long trees start early
   const int order[3] = {CLS_MEM, CLS_R64, CLS_R32};
   for (int c : order) {
     if (!grid[c]) continue;
     a.slab_words = bk_slab_words(c, dcap, xcap);
+    a.q = QueueView();
+    if (share) {
+      if ((rc = ensure_queue(g, c, bk_task_words(c, dcap), &a.q))) return rc;
+      if ((rc = queue_launch_init(a.q, s, &launches))) return rc;
+    }
     if ((rc = bk_launch(c, wbits, a, grid[c], block[c], smem[c], s, &launches))) return rc;
   }
   MCE_CUDA(cudaEventRecord(g->ev[3], s));

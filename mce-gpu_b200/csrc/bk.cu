@@ -16,17 +16,26 @@
 //    frames in shared memory (register engine) or the slab (wide engine);
 //  - earlier neighbours of the root (the reference's Xx list, tested with a
 //    binary search per tree node, mce/mce_utils.cuh:265-292) are encoded once
-//    per root as bitmaps over the root's later neighbours; a leaf is maximal
-//    only if no such bitmap contains the leaf's clique.
+//    per root as bitmaps over the root's later neighbours, duplicates
+//    dropped; a leaf is maximal only if none of them contains the clique;
+//  - load balance: a warp about to descend into a child with many candidates
+//    hands the child to the device task queue instead while other warps are
+//    idle (queue.cuh), the counterpart of the reference's worker list.
 // Tie-breaking: the pivot with the lowest index among the best scores, so
-// per-root tree sizes are deterministic.
+// per-root tree sizes are deterministic and independent of who walks them.
 #include <climits>
 #include <cstring>
 
 #include "common.cuh"
 #include "kernels.h"
+#include "queue.cuh"
 
 namespace mce {
+
+__global__ void queue_init_kernel(QueueView q) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < q.cap; i += gridDim.x * blockDim.x)
+    q.seq[i] = i;
+}
 
 namespace {
 
@@ -88,6 +97,75 @@ __device__ __forceinline__ int lower_bound_g(const int32_t *a, int n, int32_t ke
   return lo;
 }
 
+__device__ __forceinline__ uint32_t hash_word(u64 x) {
+  return (uint32_t)((x * 0x9E3779B97F4A7C15ull) >> 32);
+}
+
+// warp-uniform answer to "should this warp hand a child to the queue?"
+__device__ __forceinline__ bool wants_task(const QueueView &q) {
+  int w = 0;
+  if (lane_id() == 0) w = q_wants(q) ? 1 : 0;
+  return __shfl_sync(MCE_FULL, w, 0) != 0;
+}
+
+// Per-root outputs shared by donor and takers: accumulate.
+__device__ __forceinline__ void root_done(const BKArgs &a, int32_t r, u64 nodes, u64 cnt) {
+  if (lane_id() != 0) return;
+  if (a.root_nodes && nodes) atomicAdd(&a.root_nodes[r], nodes);
+  if (a.root_count && cnt) atomicAdd(&a.root_count[r], cnt);
+  if (a.graph_count && cnt) atomicAdd(&a.graph_count[a.graph_of[r]], cnt);
+}
+
+// Idle phase shared by the engines: take tasks until no work is left.
+// `run(words)` processes one task whose words were stored by `put`.
+template <typename Put, typename Run>
+__device__ void idle_phase(const BKArgs &a, Put put, Run run) {
+  const QueueView &q = a.q;
+  const uint32_t lane = lane_id();
+  if (lane == 0) atomicAdd(&q.hdr->idle, 1u);
+  uint32_t last_epoch = 0;
+  uint64_t t_last = 0;
+  if (lane == 0) {
+    last_epoch = ld_volatile(&q.hdr->epoch);
+    t_last = globaltimer_ns();
+  }
+  uint32_t ns = 64;
+  for (;;) {
+    if (q_pop(q, put)) {
+      if (lane == 0) atomicSub(&q.hdr->idle, 1u);
+      run();
+      if (lane == 0) {
+        atomicSub(&q.hdr->work, 1u);
+        atomicAdd(&q.hdr->epoch, 1u);
+        atomicAdd(&q.hdr->idle, 1u);
+        t_last = globaltimer_ns();
+      }
+      ns = 64;
+      continue;
+    }
+    int stop = 0;
+    if (lane == 0) {
+      if (ld_volatile(&q.hdr->work) == 0) {
+        stop = 1;
+      } else {
+        const uint32_t e = ld_volatile(&q.hdr->epoch);
+        const uint64_t now = globaltimer_ns();
+        if (e != last_epoch) {
+          last_epoch = e;
+          t_last = now;
+        } else if (now - t_last > a.wait_limit_ns) {
+          atomicOr(a.err, MCE_ERR_WAIT_TIMEOUT);  // no progress anywhere: give up
+          stop = 1;
+        }
+      }
+    }
+    if (__shfl_sync(MCE_FULL, stop, 0)) break;
+    __nanosleep(ns);
+    if (ns < 2048) ns <<= 1;
+  }
+  if (lane == 0) atomicSub(&q.hdr->idle, 1u);
+}
+
 // ---------------------------------------------------------------------------
 // Register engine: d+ <= 32 * NR; lane i holds rows i (and i + 32).
 // ---------------------------------------------------------------------------
@@ -101,15 +179,41 @@ struct RegSmem {
   int32_t beg[32];          // chunk list starts
 };
 
+// Per-warp slab of the register engine, in Words: a hash set used while the
+// earlier-neighbour rows are built (2 * REG_XCAP), the distinct rows
+// (REG_XCAP) and the rows adjacent to the current branch (REG_XCAP).
+template <typename Word>
+struct RegSlab {
+  Word *hash, *xr, *xl;
+};
+
+template <typename Word>
+__device__ __forceinline__ RegSlab<Word> reg_slab(const BKArgs &a, int64_t gw) {
+  Word *base = (Word *)(a.slab + (size_t)gw * a.slab_words);
+  RegSlab<Word> s;
+  s.hash = base;
+  s.xr = base + 2 * REG_XCAP;
+  s.xl = s.xr + REG_XCAP;
+  return s;
+}
+
 template <typename Word, int NR>
 __device__ __forceinline__ Word row_of(Word r0, Word r1, int j) {
   if constexpr (NR == 2) return __shfl_sync(MCE_FULL, j >= 32 ? r1 : r0, j & 31);
   return __shfl_sync(MCE_FULL, r0, j & 31);
 }
 
+// Encoded state of the root a warp currently works on.
+template <typename Word>
+struct RegRoot {
+  int32_t r = -1;
+  int d = 0, nX = 0;
+  Word r0 = 0, r1 = 0;
+};
+
 template <typename Word, int NR>
-__device__ void search_root_reg(const BKArgs &a, RegSmem<Word, NR> &sm, Word *xr, Word *xl,
-                                int32_t r, u64 &h0, u64 &h1, u64 &nodes_total) {
+__device__ void reg_encode(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<Word> &sl,
+                           int32_t r, RegRoot<Word> &rt) {
   using O = WOps<Word>;
   const int lane = (int)lane_id();
   const uint32_t lt = (1u << lane) - 1u;
@@ -152,54 +256,120 @@ __device__ void search_root_reg(const BKArgs &a, RegSmem<Word, NR> &sm, Word *xr
     }
     __syncwarp();
   }
-  const Word r0 = sm.rows[lane];
-  Word r1 = 0;
-  if constexpr (NR == 2) r1 = sm.rows[lane + 32];
+  rt.r0 = sm.rows[lane];
+  rt.r1 = 0;
+  if constexpr (NR == 2) rt.r1 = sm.rows[lane + 32];
 
-  // Earlier neighbours x of r: row(x) = N(x) & P.  Only non-empty rows are
-  // kept; x is earlier than every vertex of P, so N(x) & P lies in N+(x).
+  // Earlier neighbours x of r: row(x) = N(x) & P, kept once per distinct
+  // non-empty value; x is earlier than every vertex of P, so N(x) & P lies
+  // in N+(x).
   int nX = 0;
-  for (int c = 0; c * 32 < u; ++c) {
-    const int items = min(32, u - c * 32);
-    int xb = 0, xlen = 0;
-    if (lane < items) {
-      const int32_t x = a.cs[ub + c * 32 + lane];
-      xb = a.split[x];
-      xlen = a.rp[x + 1] - xb;
-    }
-    sm.xs[lane] = 0;
-    const int incl = warp_incl_scan(xlen);
-    const int T = __shfl_sync(MCE_FULL, incl, 31);
-    sm.off[lane] = incl - xlen;
-    sm.beg[lane] = xb;
+  if (u > 0) {
+    int hc = 32;
+    while (hc < 2 * u && hc < 2 * REG_XCAP) hc <<= 1;
+    for (int i = lane; i < hc; i += 32) sl.hash[i] = 0;
     __syncwarp();
-    for (int e = lane; e < T; e += 32) {
-      const int t = chunk_owner(sm.off, e);
-      const int32_t w = a.cs[sm.beg[t] + (e - sm.off[t])];
-      const int i = lower_bound_g(sm.pl, 32 * NR, w);
-      if (i < d && sm.pl[i] == w) atomicOr(&sm.xs[t], O::bit(i));
+    for (int c = 0; c * 32 < u; ++c) {
+      const int items = min(32, u - c * 32);
+      int xb = 0, xlen = 0;
+      if (lane < items) {
+        const int32_t x = a.cs[ub + c * 32 + lane];
+        xb = a.split[x];
+        xlen = a.rp[x + 1] - xb;
+      }
+      sm.xs[lane] = 0;
+      const int incl = warp_incl_scan(xlen);
+      const int T = __shfl_sync(MCE_FULL, incl, 31);
+      sm.off[lane] = incl - xlen;
+      sm.beg[lane] = xb;
+      __syncwarp();
+      for (int e = lane; e < T; e += 32) {
+        const int t = chunk_owner(sm.off, e);
+        const int32_t w = a.cs[sm.beg[t] + (e - sm.off[t])];
+        const int i = lower_bound_g(sm.pl, 32 * NR, w);
+        if (i < d && sm.pl[i] == w) atomicOr(&sm.xs[t], O::bit(i));
+      }
+      __syncwarp();
+      const Word row = sm.xs[lane];
+      bool fresh = false;
+      if (lane < items && row != 0) {
+        uint32_t h = hash_word((u64)row) & (uint32_t)(hc - 1);
+        for (int probe = 0; probe < hc; ++probe) {
+          const Word old = atomicCAS(&sl.hash[h], (Word)0, row);
+          if (old == 0) {
+            fresh = true;
+            break;
+          }
+          if (old == row) break;
+          h = (h + 1) & (uint32_t)(hc - 1);
+        }
+      }
+      const uint32_t mk = __ballot_sync(MCE_FULL, fresh);
+      if (fresh) sl.xr[nX + __popc(mk & lt)] = row;
+      nX += __popc(mk);
+      __syncwarp();
     }
-    __syncwarp();
-    const Word row = sm.xs[lane];
-    const bool nz = lane < items && row != 0;
-    const uint32_t mk = __ballot_sync(MCE_FULL, nz);
-    if (nz) xr[nX + __popc(mk & lt)] = row;
-    nX += __popc(mk);
+  }
+  rt.r = r;
+  rt.d = d;
+  rt.nX = nX;
+}
+
+// Walk the subtree under node (P, X, S) of root rt.r.  For the root itself
+// S = 0; for a task S holds the vertices chosen above the node.
+template <typename Word, int NR>
+__device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<Word> &sl,
+                         const RegRoot<Word> &rt, Word P, Word X, Word S, u64 &h0, u64 &h1,
+                         u64 &nodes, u64 &cnt) {
+  using O = WOps<Word>;
+  const int lane = (int)lane_id();
+  const uint32_t lt = (1u << lane) - 1u;
+  const Word r0 = rt.r0, r1 = rt.r1;
+  const int nX = rt.nX;
+  const bool share = a.q.hdr != nullptr;
+  // pivot of the start node (select_pivot_from_P / _and_Xp, mce/mce_utils.cuh:338-402)
+  int start_k = 0;
+  {
+    const Word cand = P | X;
+    const int pc = O::popc(P);
+    int k = 0;
+    bool el = false;
+    if ((cand >> lane) & 1) {
+      const int s = O::popc(P & r0);
+      k = ((s + 1) << 7) | (127 - lane);
+      el = ((X >> lane) & 1) && s == pc;
+    }
+    if constexpr (NR == 2) {
+      if ((cand >> (lane + 32)) & 1) {
+        const int s = O::popc(P & r1);
+        k = max(k, ((s + 1) << 7) | (127 - (lane + 32)));
+        el = el || (((X >> (lane + 32)) & 1) && s == pc);
+      }
+    }
+    if (__any_sync(MCE_FULL, el) || P == 0) return;
+    k = (int)__reduce_max_sync(MCE_FULL, (unsigned)k);
+    start_k = k;
+  }
+  // apply_pivot_to_first_level (:204-216) / apply_pivot_to_next_level (:218-239)
+  Word B = P & ~row_of<Word, NR>(r0, r1, 127 - (start_k & 127));
+  // Leaf filter: for the root it is rebuilt at every depth-0 branch (rows
+  // adjacent to that branch vertex); for a task it is built once (rows
+  // containing the whole chosen set).
+  const bool per_branch = (S == 0);
+  int nL = 0;
+  if (!per_branch && nX > 0) {
+    for (int i0 = 0; i0 < nX; i0 += 32) {
+      const int i = i0 + lane;
+      const Word row = i < nX ? sl.xr[i] : (Word)0;
+      const bool has = i < nX && (row & S) == S;
+      const uint32_t mk = __ballot_sync(MCE_FULL, has);
+      if (has) sl.xl[nL + __popc(mk & lt)] = row;
+      nL += __popc(mk);
+    }
     __syncwarp();
   }
-
-  // Root level: pivot from P only (select_pivot_from_P, mce/mce_utils.cuh:338-364),
-  // branch set P \ N(pivot) (apply_pivot_to_first_level, :204-216).
-  const Word Pall = O::low(d);
-  int key = 0;
-  if (lane < d) key = ((O::popc(Pall & r0) + 1) << 7) | (127 - lane);
-  if constexpr (NR == 2)
-    if (lane + 32 < d) key = max(key, ((O::popc(Pall & r1) + 1) << 7) | (127 - (lane + 32)));
-  key = (int)__reduce_max_sync(MCE_FULL, (unsigned)key);
-  Word P = Pall, X = 0, S = 0;
-  Word B = Pall & ~row_of<Word, NR>(r0, r1, 127 - (key & 127));
-  int depth = 0, nL = 0;
-  u64 nodes = 0, cnt = 0;
+  int depth = 0, recheck = 0;
+  bool want = false;
   for (;;) {
     if (B == 0) {  // get_next_candidate found nothing: backtrack (:526-563)
       if (depth == 0) break;
@@ -220,14 +390,14 @@ __device__ void search_root_reg(const BKArgs &a, RegSmem<Word, NR> &sm, Word *xr
     P &= ~vb;
     X |= vb;
     ++nodes;
-    if (depth == 0 && nX > 0) {  // earlier neighbours adjacent to v
+    if (per_branch && depth == 0 && nX > 0) {  // earlier neighbours adjacent to v
       nL = 0;
       for (int i0 = 0; i0 < nX; i0 += 32) {
         const int i = i0 + lane;
-        const Word row = i < nX ? xr[i] : (Word)0;
+        const Word row = i < nX ? sl.xr[i] : (Word)0;
         const bool has = (row & vb) != 0;
         const uint32_t mk = __ballot_sync(MCE_FULL, has);
-        if (has) xl[nL + __popc(mk & lt)] = row;
+        if (has) sl.xl[nL + __popc(mk & lt)] = row;
         nL += __popc(mk);
       }
       __syncwarp();
@@ -239,7 +409,7 @@ __device__ void search_root_reg(const BKArgs &a, RegSmem<Word, NR> &sm, Word *xr
         bool covered = false;
         for (int i0 = 0; i0 < nL; i0 += 32) {
           const int i = i0 + lane;
-          const bool hit = i < nL && (xl[i] & Sc) == Sc;
+          const bool hit = i < nL && (sl.xl[i] & Sc) == Sc;
           if (__any_sync(MCE_FULL, hit)) {
             covered = true;
             break;
@@ -277,6 +447,20 @@ __device__ void search_root_reg(const BKArgs &a, RegSmem<Word, NR> &sm, Word *xr
       }
     }
     if (__any_sync(MCE_FULL, el)) continue;
+    // hand the child to an idle warp (try_dequeue / do_fork_L1,
+    // mce/mce_utils.cuh:872-880,1063-1113)
+    if (share && pc >= a.donate_min) {
+      if (--recheck <= 0) {  // the queue state is read every 32 candidate nodes
+        want = wants_task(a.q);
+        recheck = 32;
+      }
+      if (want) {
+        const u64 w0 = (u64)(uint32_t)rt.r, w1 = (u64)Pc, w2 = (u64)Xc, w3 = (u64)Sc;
+        if (q_push(a.q, [&](uint32_t k2) { return k2 == 0 ? w0 : k2 == 1 ? w1 : k2 == 2 ? w2 : w3; }))
+          continue;
+        want = false;
+      }
+    }
     k = (int)__reduce_max_sync(MCE_FULL, (unsigned)k);
     if (lane == 0) {
       sm.stk[depth][0] = P;
@@ -292,12 +476,6 @@ __device__ void search_root_reg(const BKArgs &a, RegSmem<Word, NR> &sm, Word *xr
     // apply_pivot_to_next_level (:218-239)
     B = Pc & ~row_of<Word, NR>(r0, r1, 127 - (k & 127));
   }
-  nodes_total += nodes;
-  if (lane == 0) {
-    if (a.root_nodes) a.root_nodes[r] = nodes;
-    if (a.root_count) a.root_count[r] = cnt;
-    if (a.graph_count && cnt) atomicAdd(&a.graph_count[a.graph_of[r]], cnt);
-  }
 }
 
 template <typename Word, int NR>
@@ -306,10 +484,12 @@ __global__ void __launch_bounds__(REG_BLOCK) bk_reg_kernel(BKArgs a, int cls) {
   RegSmem<Word, NR> &sm = sm_all[threadIdx.x >> 5];
   const int lane = (int)lane_id();
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  Word *xr = (Word *)(a.slab + (size_t)gw * a.slab_words);
-  Word *xl = xr + REG_XCAP;
+  const RegSlab<Word> sl = reg_slab<Word>(a, gw);
   const uint32_t beg = a.shape->cls_off[cls], end = a.shape->cls_off[cls + 1];
+  const bool share = a.q.hdr != nullptr;
   u64 h0 = 0, h1 = 0, nodes = 0;
+  RegRoot<Word> rt;
+  if (share && lane == 0) atomicAdd(&a.q.hdr->work, 1u);
   for (;;) {
     uint32_t i0 = 0;
     if (lane == 0) i0 = atomicAdd(&a.fetch[cls], (uint32_t)REG_CHUNK);
@@ -318,8 +498,40 @@ __global__ void __launch_bounds__(REG_BLOCK) bk_reg_kernel(BKArgs a, int cls) {
     for (int k = 0; k < REG_CHUNK; ++k) {
       const uint32_t idx = beg + i0 + k;
       if (idx >= end) break;
-      search_root_reg<Word, NR>(a, sm, xr, xl, a.roots[idx], h0, h1, nodes);
+      const int32_t r = a.roots[idx];
+      reg_encode<Word, NR>(a, sm, sl, r, rt);
+      u64 nd = 0, cnt = 0;
+      reg_tree<Word, NR>(a, sm, sl, rt, WOps<Word>::low(rt.d), (Word)0, (Word)0, h0, h1, nd, cnt);
+      nodes += nd;
+      root_done(a, r, nd, cnt);
     }
+  }
+  if (share) {
+    if (lane == 0) {
+      atomicSub(&a.q.hdr->work, 1u);
+      atomicAdd(&a.q.hdr->epoch, 1u);
+    }
+    u64 t0 = 0, t1 = 0, t2 = 0, t3 = 0;
+    idle_phase(
+        a,
+        [&](uint32_t k, u64 w) {  // lane k receives word k
+          if (k == 0) t0 = w;
+          if (k == 1) t1 = w;
+          if (k == 2) t2 = w;
+          if (k == 3) t3 = w;
+        },
+        [&]() {
+          // word k of the task arrived on lane k
+          const int32_t r = (int32_t)__shfl_sync(MCE_FULL, t0, 0);
+          const Word P = (Word)__shfl_sync(MCE_FULL, t1, 1);
+          const Word X = (Word)__shfl_sync(MCE_FULL, t2, 2);
+          const Word S = (Word)__shfl_sync(MCE_FULL, t3, 3);
+          if (r != rt.r) reg_encode<Word, NR>(a, sm, sl, r, rt);
+          u64 nd = 0, cnt = 0;
+          reg_tree<Word, NR>(a, sm, sl, rt, P, X, S, h0, h1, nd, cnt);
+          nodes += nd;
+          root_done(a, r, nd, cnt);
+        });
   }
   if (h0) atomicAdd(&a.hist[lane + 2], h0);
   if (h1) atomicAdd(&a.hist[lane + 34], h1);
@@ -336,7 +548,7 @@ struct MemSmem {
 
 struct Slab {
   int32_t *pl;
-  u64 *rows, *stk, *xs, *xr;
+  u64 *rows, *stk, *xs, *xr, *hash;
   int32_t *xl;
 };
 
@@ -348,21 +560,31 @@ __device__ __forceinline__ Slab slab_of(const BKArgs &a, int64_t gw) {
   s.stk = s.rows + (size_t)D * WM;
   s.xs = s.stk + (size_t)(D + 1) * 4 * WM;
   s.xr = s.xs + (size_t)32 * WM;
-  s.pl = (int32_t *)(s.xr + (size_t)XC * WM);
+  s.hash = s.xr + (size_t)XC * WM;
+  s.pl = (int32_t *)(s.hash + 2 * (size_t)XC);
   s.xl = s.pl + D;
   return s;
 }
 
-__device__ void search_root_mem(const BKArgs &a, MemSmem &sm, const Slab &sl, int32_t r,
-                                u64 &h0, u64 &h1, u64 &nodes_total) {
+struct MemRoot {
+  int32_t r = -1;
+  int d = 0, Wr = 0, nX = 0;
+};
+
+__device__ void mem_encode(const BKArgs &a, MemSmem &sm, const Slab &sl, int32_t r, MemRoot &rt) {
   const int lane = (int)lane_id();
   const uint32_t lt = (1u << lane) - 1u;
   const int32_t sb = a.split[r], d = a.rp[r + 1] - sb, ub = a.rp[r], u = sb - ub;
-  if (d > a.dcap) {
-    if (lane == 0) atomicOr(a.err, MCE_ERR_DEGREE);
+  rt.r = r;
+  rt.d = d;
+  rt.nX = 0;
+  if (d > a.dcap || u > a.xcap) {
+    if (lane == 0) atomicOr(a.err, d > a.dcap ? MCE_ERR_DEGREE : MCE_ERR_XROWS);
+    rt.d = 0;
     return;
   }
   const int Wr = (d + 63) >> 6;
+  rt.Wr = Wr;
   int32_t *pl = sl.pl;
   u64 *rows = sl.rows;
   for (int i = lane; i < d; i += 32) pl[i] = a.cs[sb + i];
@@ -393,7 +615,12 @@ __device__ void search_root_mem(const BKArgs &a, MemSmem &sm, const Slab &sl, in
     }
     __syncwarp();
   }
-  // earlier-neighbour rows (non-empty only)
+  // earlier-neighbour rows: non-empty ones, distinct when one word wide
+  int hc = 32;
+  if (Wr == 1) {
+    while (hc < 2 * u && hc < 2 * a.xcap) hc <<= 1;
+    for (int i = lane; i < hc; i += 32) sl.hash[i] = 0;
+  }
   int nX = 0;
   for (int c = 0; c * 32 < u; ++c) {
     const int items = min(32, u - c * 32);
@@ -416,44 +643,92 @@ __device__ void search_root_mem(const BKArgs &a, MemSmem &sm, const Slab &sl, in
       if (i < d && pl[i] == w) atomicOr(&sl.xs[(size_t)t * Wr + (i >> 6)], 1ull << (i & 63));
     }
     __syncwarp();
-    bool nz = false;
-    if (lane < items)
-      for (int w = 0; w < Wr; ++w) nz |= sl.xs[(size_t)lane * Wr + w] != 0;
-    const uint32_t mk = __ballot_sync(MCE_FULL, nz);
-    if (nX + __popc(mk) > a.xcap) {
-      if (lane == 0) atomicOr(a.err, MCE_ERR_XROWS);
-      return;
+    bool keep = false;
+    if (lane < items) {
+      for (int w = 0; w < Wr; ++w) keep |= sl.xs[(size_t)lane * Wr + w] != 0;
+      if (keep && Wr == 1) {
+        const u64 row = sl.xs[lane];
+        uint32_t h = hash_word(row) & (uint32_t)(hc - 1);
+        keep = false;
+        for (int probe = 0; probe < hc; ++probe) {
+          const u64 old = atomicCAS(&sl.hash[h], 0ull, row);
+          if (old == 0) {
+            keep = true;
+            break;
+          }
+          if (old == row) break;
+          h = (h + 1) & (uint32_t)(hc - 1);
+        }
+      }
     }
-    if (nz) {
+    const uint32_t mk = __ballot_sync(MCE_FULL, keep);
+    if (keep) {
       const int pos = nX + __popc(mk & lt);
       for (int w = 0; w < Wr; ++w) sl.xr[(size_t)pos * Wr + w] = sl.xs[(size_t)lane * Wr + w];
     }
     nX += __popc(mk);
     __syncwarp();
   }
+  rt.nX = nX;
+}
 
-  // root frame
+// Walk the subtree under frame 0 of the slab stack (P, X, S already there).
+__device__ void mem_tree(const BKArgs &a, const Slab &sl, const MemRoot &rt, u64 &h0, u64 &h1,
+                         u64 &nodes, u64 &cnt) {
+  const int lane = (int)lane_id();
+  const uint32_t lt = (1u << lane) - 1u;
+  const int d = rt.d, Wr = rt.Wr, nX = rt.nX;
+  const u64 *rows = sl.rows;
+  const bool share = a.q.hdr != nullptr;
   u64 *F0 = sl.stk;
-  int key = 0;
-  for (int j = lane; j < d; j += 32) {
-    int s = 0;
-    for (int w = 0; w < Wr; ++w) s += __popcll(rows[(size_t)j * Wr + w]);
-    key = max(key, ((s + 1) << 11) | (2047 - j));
-  }
-  key = (int)__reduce_max_sync(MCE_FULL, (unsigned)key);
+  // pivot of the start node
+  int s_base = 0;  // chosen vertices above frame 0
   {
-    const int piv = 2047 - (key & 2047);
+    int pc = 0, sc = 0;
     if (lane < Wr) {
-      const u64 all = (lane == Wr - 1 && (d & 63)) ? ((1ull << (d & 63)) - 1ull) : ~0ull;
-      F0[lane] = all;
-      F0[Wr + lane] = 0;
-      F0[2 * Wr + lane] = all & ~rows[(size_t)piv * Wr + lane];
-      F0[3 * Wr + lane] = 0;
+      pc = __popcll(F0[lane]);
+      sc = __popcll(F0[3 * Wr + lane]);
     }
+    pc = (int)__reduce_add_sync(MCE_FULL, (unsigned)pc);
+    s_base = (int)__reduce_add_sync(MCE_FULL, (unsigned)sc);
+    int k = 0;
+    bool el = false;
+    for (int uu = lane; uu < d; uu += 32) {
+      const int uw = uu >> 6;
+      const u64 ub2 = 1ull << (uu & 63);
+      const bool inP = (F0[uw] & ub2) != 0, inX = (F0[Wr + uw] & ub2) != 0;
+      if (!(inP || inX)) continue;
+      int s = 0;
+      const u64 *ru = rows + (size_t)uu * Wr;
+      for (int w = 0; w < Wr; ++w) s += __popcll(F0[w] & ru[w]);
+      k = max(k, ((s + 1) << 11) | (2047 - uu));
+      el = el || (inX && s == pc);
+    }
+    if (__any_sync(MCE_FULL, el) || pc == 0) return;
+    k = (int)__reduce_max_sync(MCE_FULL, (unsigned)k);
+    const int piv = 2047 - (k & 2047);
+    if (lane < Wr) F0[2 * Wr + lane] = F0[lane] & ~rows[(size_t)piv * Wr + lane];
+    __syncwarp();
   }
-  __syncwarp();
-  int depth = 0, nL = 0;
-  u64 nodes = 0, cnt = 0;
+  const bool per_branch = (s_base == 0);
+  int nL = 0;
+  if (!per_branch && nX > 0) {  // rows containing the whole chosen set
+    const u64 *S0 = F0 + 3 * Wr;
+    for (int i0 = 0; i0 < nX; i0 += 32) {
+      const int i = i0 + lane;
+      bool has = false;
+      if (i < nX) {
+        has = true;
+        for (int w = 0; w < Wr && has; ++w) has = (sl.xr[(size_t)i * Wr + w] & S0[w]) == S0[w];
+      }
+      const uint32_t m2 = __ballot_sync(MCE_FULL, has);
+      if (has) sl.xl[nL + __popc(m2 & lt)] = i;
+      nL += __popc(m2);
+    }
+    __syncwarp();
+  }
+  int depth = 0, recheck = 0;
+  bool want = false;
   for (;;) {
     u64 *F = sl.stk + (size_t)depth * 4 * Wr;
     u64 *Fp = F, *Fx = F + Wr, *Fb = F + 2 * Wr, *Fs = F + 3 * Wr;
@@ -491,7 +766,7 @@ __device__ void search_root_mem(const BKArgs &a, MemSmem &sm, const Slab &sl, in
     }
     pc = (int)__reduce_add_sync(MCE_FULL, (unsigned)pc);
     xnz = __any_sync(MCE_FULL, xnz);
-    if (depth == 0 && nX > 0) {
+    if (per_branch && depth == 0 && nX > 0) {
       nL = 0;
       for (int i0 = 0; i0 < nX; i0 += 32) {
         const int i = i0 + lane;
@@ -521,7 +796,7 @@ __device__ void search_root_mem(const BKArgs &a, MemSmem &sm, const Slab &sl, in
         }
         if (!covered) {
           ++cnt;
-          const int bin = depth;  // clique size - 2 (root + depth + 1 vertices)
+          const int bin = s_base + depth;  // clique size - 2
           if (bin < 64) {
             if (lane == (bin & 31)) {
               if (bin < 32)
@@ -550,17 +825,23 @@ __device__ void search_root_mem(const BKArgs &a, MemSmem &sm, const Slab &sl, in
       el = el || (inX && s == pc);
     }
     if (__any_sync(MCE_FULL, el)) continue;
+    if (share && pc >= a.donate_min && (--recheck <= 0 ? (recheck = 32, want = wants_task(a.q)) : want)) {
+      const int WM = (a.dcap + 63) >> 6;
+      const u64 *Cp = C, *Cx = C + Wr, *Cs = C + 3 * Wr;
+      if (q_push(a.q, [&](uint32_t k2) -> u64 {
+            if (k2 == 0) return (u64)(uint32_t)rt.r;
+            const uint32_t part = (k2 - 1) / WM, w = (k2 - 1) % WM;
+            if ((int)w >= Wr) return 0ull;
+            return part == 0 ? Cp[w] : part == 1 ? Cx[w] : Cs[w];
+          }))
+        continue;
+      want = false;
+    }
     k = (int)__reduce_max_sync(MCE_FULL, (unsigned)k);
     const int up = 2047 - (k & 2047);
     if (lane < Wr) C[2 * Wr + lane] = C[lane] & ~rows[(size_t)up * Wr + lane];
     __syncwarp();
     ++depth;
-  }
-  nodes_total += nodes;
-  if (lane == 0) {
-    if (a.root_nodes) a.root_nodes[r] = nodes;
-    if (a.root_count) a.root_count[r] = cnt;
-    if (a.graph_count && cnt) atomicAdd(&a.graph_count[a.graph_of[r]], cnt);
   }
 }
 
@@ -571,13 +852,73 @@ __global__ void __launch_bounds__(MEM_BLOCK) bk_mem_kernel(BKArgs a, int cls) {
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const Slab sl = slab_of(a, gw);
   const uint32_t beg = a.shape->cls_off[cls], end = a.shape->cls_off[cls + 1];
+  const bool share = a.q.hdr != nullptr;
   u64 h0 = 0, h1 = 0, nodes = 0;
+  MemRoot rt;
+  if (share && lane == 0) atomicAdd(&a.q.hdr->work, 1u);
   for (;;) {
     uint32_t i0 = 0;
     if (lane == 0) i0 = atomicAdd(&a.fetch[cls], 1u);
     i0 = __shfl_sync(MCE_FULL, i0, 0);
     if (i0 >= end - beg) break;
-    search_root_mem(a, sm, sl, a.roots[beg + i0], h0, h1, nodes);
+    const int32_t r = a.roots[beg + i0];
+    mem_encode(a, sm, sl, r, rt);
+    if (rt.d == 0) continue;
+    const int Wr = rt.Wr;
+    if (lane < Wr) {  // root frame: P = all of N+(r), X = 0, S = 0
+      const u64 all = (lane == Wr - 1 && (rt.d & 63)) ? ((1ull << (rt.d & 63)) - 1ull) : ~0ull;
+      sl.stk[lane] = all;
+      sl.stk[Wr + lane] = 0;
+      sl.stk[3 * Wr + lane] = 0;
+    }
+    __syncwarp();
+    u64 nd = 0, cnt = 0;
+    mem_tree(a, sl, rt, h0, h1, nd, cnt);
+    nodes += nd;
+    root_done(a, r, nd, cnt);
+  }
+  if (share) {
+    if (lane == 0) {
+      atomicSub(&a.q.hdr->work, 1u);
+      atomicAdd(&a.q.hdr->epoch, 1u);
+    }
+    const int WM = (a.dcap + 63) >> 6;
+    int32_t task_root = -1;
+    idle_phase(
+        a,
+        [&](uint32_t k, u64 w) {
+          if (k == 0) {
+            task_root = (int32_t)w;  // lane 0 reads word 0
+          } else {
+            const uint32_t part = (k - 1) / WM, ww = (k - 1) % WM;
+            sl.xs[part * WM + ww] = w;  // staged; moved to frame 0 after encode
+          }
+        },
+        [&]() {
+          const int32_t r = __shfl_sync(MCE_FULL, task_root, 0);
+          __syncwarp();
+          // the staging area is rewritten by mem_encode: keep the task first
+          u64 tp = 0, tx = 0, ts = 0;
+          if (lane < WM) {
+            tp = sl.xs[lane];
+            tx = sl.xs[WM + lane];
+            ts = sl.xs[2 * WM + lane];
+          }
+          __syncwarp();
+          if (r != rt.r) mem_encode(a, sm, sl, r, rt);
+          if (rt.d == 0) return;
+          const int Wr = rt.Wr;
+          if (lane < Wr) {
+            sl.stk[lane] = tp;
+            sl.stk[Wr + lane] = tx;
+            sl.stk[3 * Wr + lane] = ts;
+          }
+          __syncwarp();
+          u64 nd = 0, cnt = 0;
+          mem_tree(a, sl, rt, h0, h1, nd, cnt);
+          nodes += nd;
+          root_done(a, r, nd, cnt);
+        });
   }
   if (h0) atomicAdd(&a.hist[lane + 2], h0);
   if (h1) atomicAdd(&a.hist[lane + 34], h1);
@@ -587,11 +928,18 @@ __global__ void __launch_bounds__(MEM_BLOCK) bk_mem_kernel(BKArgs a, int cls) {
 }  // namespace
 
 size_t bk_slab_words(int cls, int dcap, int xcap) {
-  if (cls == CLS_R32 || cls == CLS_R64) return 2 * (size_t)REG_XCAP;  // x rows + leaf list
+  if (cls == CLS_R32 || cls == CLS_R64) return 4 * (size_t)REG_XCAP;  // hash, rows, leaf list
   const size_t WM = (size_t)(dcap + 63) / 64;
   size_t w = (size_t)dcap * WM + (size_t)(dcap + 1) * 4 * WM + 32 * WM + (size_t)xcap * WM;
+  w += 2 * (size_t)xcap;                            // hash set (one-word rows)
   w += ((size_t)dcap + (size_t)xcap + 1) / 2 + 1;  // pl and xl (int32)
+  w = w > 3 * WM + 1 ? w : 3 * WM + 1;
   return (w + 31) & ~(size_t)31;                    // 256-byte aligned slabs
+}
+
+uint32_t bk_task_words(int cls, int dcap) {
+  if (cls == CLS_R32 || cls == CLS_R64) return 4;
+  return 1 + 3 * (uint32_t)((dcap + 63) / 64);
 }
 
 int bk_warps_for_class(int cls, int sms, int *warps, int *block, int *smem) {
@@ -638,6 +986,14 @@ int bk_launch(int cls, int word_bits, const BKArgs &a, int grid, int block, int 
   return MCE_OK;
 }
 
+int queue_launch_init(const QueueView &q, cudaStream_t s, int *launches) {
+  MCE_CUDA(cudaMemsetAsync(q.hdr, 0, sizeof(QueueHdr), s));
+  queue_init_kernel<<<(q.cap + 255) / 256, 256, 0, s>>>(q);
+  MCE_CUDA(cudaGetLastError());
+  if (launches) *launches += 1;
+  return MCE_OK;
+}
+
 // ===========================================================================
 // Allocation-free search entry point.
 //
@@ -659,7 +1015,7 @@ int bk_launch(int cls, int word_bits, const BKArgs &a, int grid, int block, int 
 namespace {
 
 constexpr size_t NOALLOC_CTL_BYTES = 1024;  // ShapeInfo, fetch counters, status, nodes
-constexpr size_t NOALLOC_SLAB_WORDS = REG_XCAP;  // u64 words per warp: 2 x REG_XCAP u32 rows
+constexpr size_t NOALLOC_SLAB_WORDS = 2 * REG_XCAP;  // u64 words per warp: 4 x REG_XCAP u32 words
 static_assert(MCE_NOALLOC_SCRATCH_BYTES % 256 == 0, "scratch size");
 
 static __device__ __align__(256) unsigned long long g_noalloc_scratch[MCE_NOALLOC_SCRATCH_BYTES / 8];

@@ -88,7 +88,7 @@ __device__ __forceinline__ bool grid_sync(GridBarrier *b, uint32_t nblocks, uint
           break;
         }
         __nanosleep(ns);
-        if (ns < 1024) ns <<= 1;
+        if (ns < 256) ns <<= 1;
       }
     }
     __threadfence();

@@ -5,6 +5,8 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include "queue.cuh"
+
 namespace mce {
 
 // ---- peeling ---------------------------------------------------------------
@@ -78,11 +80,16 @@ struct BKArgs {
   unsigned long long *slab;      // per-warp scratch
   size_t slab_words;             // u64 words per warp
   int32_t dcap, xcap;            // slab capacities (later degree, x rows)
+  QueueView q;                   // task queue (q.hdr == nullptr: no sharing)
+  int32_t donate_min;            // hand off children with at least this many candidates
+  uint64_t wait_limit_ns;        // an idle warp gives up after this long without progress
 };
 
 // Launch the engine of one class.  warps_out: number of warps launched (slab sizing).
 int bk_warps_for_class(int cls, int sms, int *warps, int *block, int *smem);
 size_t bk_slab_words(int cls, int dcap, int xcap);
+uint32_t bk_task_words(int cls, int dcap);
+int queue_launch_init(const QueueView &q, cudaStream_t s, int *launches);
 int bk_launch(int cls, int word_bits, const BKArgs &a, int grid, int block, int smem,
               cudaStream_t s, int *launches);
 

@@ -36,11 +36,21 @@ struct PeelCtl {
   int32_t degeneracy;
   uint32_t rounds;
   uint32_t levels;
+  // state handed back by a solo section (written by block 0, read by all)
+  uint32_t solo_q, solo_cnt, solo_priority, solo_rounds;
+  int64_t solo_todo;
+  int32_t solo_degen;
+  uint32_t solo_sections;
 };
 
 namespace {
 
 constexpr int PEEL_BLOCK = 512;
+// A frontier of at most SOLO_MAX vertices is peeled by block 0 alone, round
+// after round with __syncthreads between them, for up to SOLO_ROUNDS rounds
+// (well inside the other blocks' barrier wait limit).
+constexpr uint32_t SOLO_MAX = 1024;
+constexpr uint32_t SOLO_ROUNDS = 65536;
 
 // warp-aggregated append of `pred` items to list[*cnt]
 __device__ __forceinline__ void warp_append(bool pred, int32_t val, int32_t *list,
@@ -55,6 +65,44 @@ __device__ __forceinline__ void warp_append(bool pred, int32_t val, int32_t *lis
   if (pred) list[base + __popc(mask & ((1u << lane) - 1u))] = val;
 }
 
+// One peel round (phase q) over the frontier in slot q % 3, executed by the
+// threads [t0, t0 + nt) (the whole grid, or block 0 alone): set the round's
+// priority, lower the neighbours' degrees and append every neighbour whose
+// degree falls to `level` to the frontier in slot (q + 1) % 3.
+__device__ __forceinline__ void peel_round(uint32_t q, uint32_t cnt, int32_t level,
+                                           uint32_t priority, int64_t t0, int64_t nt,
+                                           const int32_t *__restrict__ rp,
+                                           const int32_t *__restrict__ col, int32_t *deg,
+                                           int32_t *core, uint32_t *prio, int32_t *const *fr,
+                                           PeelCtl *ctl) {
+  const uint32_t lane = lane_id();
+  const int fn = (q + 1) % 3;
+  if (t0 == 0) ctl->fcnt[(q + 2) % 3] = 0;
+  const int32_t *Fc = fr[q % 3];
+  int32_t *Fn = fr[fn];
+  for (int64_t i = t0; i < cnt; i += nt) prio[Fc[i]] = priority;
+  for (int64_t i = t0 >> 5; i < cnt; i += nt >> 5) {
+    const int32_t v = Fc[i];
+    const int32_t b = rp[v], e = rp[v + 1];
+    for (int32_t j0 = b; j0 < e; j0 += 32) {
+      const int32_t j = j0 + (int32_t)lane;
+      bool push = false;
+      int32_t u = 0;
+      if (j < e) {
+        u = col[j];
+        if (ld_volatile((const uint32_t *)&core[u]) == 0xFFFFFFFFu) {
+          const int32_t old = atomicSub(&deg[u], 1);
+          if (old == level + 1) {
+            core[u] = level;
+            push = true;
+          }
+        }
+      }
+      warp_append(push, u, Fn, &ctl->fcnt[fn]);
+    }
+  }
+}
+
 __global__ void __launch_bounds__(PEEL_BLOCK)
     peel_kernel(int32_t n, uint32_t m, const int32_t *__restrict__ rp,
                 const int32_t *__restrict__ col, int32_t *deg, int32_t *core, uint32_t *prio,
@@ -63,9 +111,8 @@ __global__ void __launch_bounds__(PEEL_BLOCK)
   const uint32_t nblocks = gridDim.x;
   const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t nthr = (int64_t)gridDim.x * blockDim.x;
-  const int64_t gwarp = tid >> 5, nwarps = nthr >> 5;
   const uint32_t lane = lane_id();
-  int32_t *fr[3] = {front0, front1, front2};
+  int32_t *const fr[3] = {front0, front1, front2};
   int32_t *alist[2] = {alistA, alistB};
 
   for (int64_t v = tid; v < n; v += nthr) {
@@ -147,31 +194,47 @@ __global__ void __launch_bounds__(PEEL_BLOCK)
       degen = level;
       todo -= cnt;
       if (todo == 0) break;  // the final round keeps priority = m
-      const int fn = (q + 1) % 3;
-      if (tid == 0) ctl->fcnt[(q + 2) % 3] = 0;
-      const int32_t *Fc = fr[q % 3];
-      int32_t *Fn = fr[fn];
-      for (int64_t i = tid; i < cnt; i += nthr) prio[Fc[i]] = priority;
-      for (int64_t i = gwarp; i < cnt; i += nwarps) {
-        const int32_t v = Fc[i];
-        const int32_t b = rp[v], e = rp[v + 1];
-        for (int32_t j0 = b; j0 < e; j0 += 32) {
-          const int32_t j = j0 + (int32_t)lane;
-          bool push = false;
-          int32_t u = 0;
-          if (j < e) {
-            u = col[j];
-            if (ld_volatile((const uint32_t *)&core[u]) == 0xFFFFFFFFu) {
-              const int32_t old = atomicSub(&deg[u], 1);
-              if (old == level + 1) {
-                core[u] = level;
-                push = true;
-              }
-            }
+      if (cnt <= SOLO_MAX) {
+        // Small frontier: block 0 peels consecutive rounds alone.  The first
+        // barrier lets every block read `cnt` before block 0 recycles slots.
+        if (!grid_sync(&ctl->bar, nblocks, &ctl->err, limit_ns)) return;
+        if (blockIdx.x == 0) {
+          uint32_t it = 0;
+          for (;;) {
+            peel_round(q, cnt, level, priority, threadIdx.x, blockDim.x, rp, col, deg, core,
+                       prio, fr, ctl);
+            __syncthreads();
+            ++q;
+            cnt = ld_volatile(&ctl->fcnt[q % 3]);
+            ++priority;
+            ++rounds;
+            if (cnt == 0 || cnt > SOLO_MAX || ++it >= SOLO_ROUNDS) break;  // cnt not yet counted
+            degen = level;
+            todo -= cnt;
+            if (todo == 0) break;  // the final round keeps priority = m
+            __syncthreads();       // every thread has read cnt before slots rotate
           }
-          warp_append(push, u, Fn, &ctl->fcnt[fn]);
+          if (threadIdx.x == 0) {
+            ctl->solo_q = q;
+            ctl->solo_cnt = cnt;
+            ctl->solo_priority = priority;
+            ctl->solo_rounds = rounds;
+            ctl->solo_todo = todo;
+            ctl->solo_degen = degen;
+            ++ctl->solo_sections;
+          }
         }
+        if (!grid_sync(&ctl->bar, nblocks, &ctl->err, limit_ns)) return;
+        q = ld_volatile(&ctl->solo_q);
+        cnt = ld_volatile(&ctl->solo_cnt);
+        priority = ld_volatile(&ctl->solo_priority);
+        rounds = ld_volatile(&ctl->solo_rounds);
+        todo = *(volatile int64_t *)&ctl->solo_todo;
+        degen = *(volatile int32_t *)&ctl->solo_degen;
+        if (todo == 0) break;
+        continue;
       }
+      peel_round(q, cnt, level, priority, tid, nthr, rp, col, deg, core, prio, fr, ctl);
       if (!grid_sync(&ctl->bar, nblocks, &ctl->err, limit_ns)) return;
       ++q;
       cnt = ld_volatile(&ctl->fcnt[q % 3]);
