@@ -161,3 +161,39 @@ def test_cli_matches_oracle(tmp_path):
     assert f"Found {t} maximal cliques in total." in r.stdout
     assert f"Max Core = {dgn}" in r.stdout
     assert "Degeneracy ordering time:" in r.stdout and "count time" in r.stdout
+
+
+def _hub_over(g_inner, extra=3):
+    """g_inner plus `extra` hubs adjacent to every vertex: the hubs' trees are
+    the whole search of g_inner, so they are split among warps."""
+    s, d = [], []
+    n = g_inner.n
+    for v in range(n):
+        for w in g_inner.col[g_inner.row_ptr[v]:g_inner.row_ptr[v + 1]]:
+            if v < w:
+                s.append(v); d.append(int(w))
+    for h in range(extra):
+        for v in range(n):
+            s.append(n + h); d.append(v)
+    return mce.from_edges(np.array(s), np.array(d), n + extra)
+
+
+@pytest.mark.parametrize("maker", [
+    lambda: mce.gen_rmat(12, 16, 0.57, 0.19, 0.19, 7),
+    lambda: _hub_over(__import__("graphs").moon_moser(9)),      # 3^9 cliques under the hubs
+    lambda: _hub_over(mce.gen_er(60, 0.5, 3)),                   # 60 later neighbours: 64-bit engine
+    lambda: _hub_over(mce.gen_er(120, 0.45, 4), extra=2),        # wide engine
+])
+def test_worker_list_on_off_identical(maker):
+    g = maker()
+    t, h, rc_o, rn_o = oracle.roots(g)
+    out = {}
+    with mce.Graph.from_host(g) as dg:
+        for wl in (mce.WL_ON, mce.WL_OFF):
+            for dmin in ((2, 10) if wl == mce.WL_ON else (10,)):
+                r = dg.count(worker_list=wl, donate_threshold=dmin, log_roots=True)
+                out[(wl, dmin)] = (r.total, r.hist.copy(), dg.root_counts(), dg.root_log())
+    for (tot, hist, rc, rn) in out.values():
+        assert tot == t and np.array_equal(hist, h)
+        assert np.array_equal(rc, rc_o)
+        assert np.array_equal(rn, rn_o)  # donation moves subtrees, never changes them
