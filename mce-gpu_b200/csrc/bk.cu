@@ -550,7 +550,14 @@ struct Slab {
   int32_t *pl;
   u64 *rows, *stk, *xs, *xr, *hash;
   int32_t *xl;
+  int hcap;  // hash set entries: a power of two >= 2 * xcap
 };
+
+__host__ __device__ __forceinline__ int hash_cap(int xcap) {
+  int h = 32;
+  while (h < 2 * xcap) h <<= 1;
+  return h;
+}
 
 __device__ __forceinline__ Slab slab_of(const BKArgs &a, int64_t gw) {
   const int D = a.dcap, WM = (a.dcap + 63) / 64, XC = a.xcap;
@@ -561,7 +568,8 @@ __device__ __forceinline__ Slab slab_of(const BKArgs &a, int64_t gw) {
   s.xs = s.stk + (size_t)(D + 1) * 4 * WM;
   s.xr = s.xs + (size_t)32 * WM;
   s.hash = s.xr + (size_t)XC * WM;
-  s.pl = (int32_t *)(s.hash + 2 * (size_t)XC);
+  s.hcap = hash_cap(XC);
+  s.pl = (int32_t *)(s.hash + (size_t)s.hcap);
   s.xl = s.pl + D;
   return s;
 }
@@ -618,7 +626,7 @@ __device__ void mem_encode(const BKArgs &a, MemSmem &sm, const Slab &sl, int32_t
   // earlier-neighbour rows: non-empty ones, distinct when one word wide
   int hc = 32;
   if (Wr == 1) {
-    while (hc < 2 * u && hc < 2 * a.xcap) hc <<= 1;
+    while (hc < 2 * u && hc < sl.hcap) hc <<= 1;
     for (int i = lane; i < hc; i += 32) sl.hash[i] = 0;
   }
   int nX = 0;
@@ -931,7 +939,7 @@ size_t bk_slab_words(int cls, int dcap, int xcap) {
   if (cls == CLS_R32 || cls == CLS_R64) return 4 * (size_t)REG_XCAP;  // hash, rows, leaf list
   const size_t WM = (size_t)(dcap + 63) / 64;
   size_t w = (size_t)dcap * WM + (size_t)(dcap + 1) * 4 * WM + 32 * WM + (size_t)xcap * WM;
-  w += 2 * (size_t)xcap;                            // hash set (one-word rows)
+  w += (size_t)hash_cap(xcap);                      // hash set (one-word rows)
   w += ((size_t)dcap + (size_t)xcap + 1) / 2 + 1;  // pl and xl (int32)
   w = w > 3 * WM + 1 ? w : 3 * WM + 1;
   return (w + 31) & ~(size_t)31;                    // 256-byte aligned slabs
