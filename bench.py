@@ -49,6 +49,10 @@ def parse_args():
     p.add_argument("--scale", type=int, default=15)
     p.add_argument("--graphs", type=int, default=4096)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--wl", choices=["on", "off"], default="on", help="subtree sharing")
+    p.add_argument("--donate", type=int, default=0, help="donation threshold (0: default)")
+    p.add_argument("--solo", type=int, default=0, help="peel solo frontier size (0: default)")
+    p.add_argument("--after", type=int, default=0, help="donate after N nodes (0: default)")
     return p.parse_args()
 
 
@@ -182,6 +186,8 @@ def cpu_baseline(g, budget_s=15.0):
 def run_mine(args, rank, world, local_rank):
     import torch
     import mce_b200 as mce
+    kw = dict(worker_list=mce.WL_ON if args.wl == "on" else mce.WL_OFF,
+              donate_threshold=args.donate, peel_solo_max=args.solo, donate_after=args.after)
     torch.cuda.set_device(local_rank)
     g, cfg = make_workload(args)
     stream = torch.cuda.Stream()
@@ -191,9 +197,9 @@ def run_mine(args, rank, world, local_rank):
     torch.cuda.synchronize()
     res = None
     for _ in range(args.warmup):
-        res = dg.count(stream=sptr)
+        res = dg.count(stream=sptr, **kw)
     split, _ = dg.split_csr()
-    total = res.total if res else dg.count(stream=sptr).total
+    total = res.total if res else dg.count(stream=sptr, **kw).total
 
     def barrier():
         if world > 1:
@@ -210,7 +216,7 @@ def run_mine(args, rank, world, local_rank):
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            r = dg.count(stream=sptr)
+            r = dg.count(stream=sptr, **kw)
             e1.record(stream)
             e1.synchronize()
             assert r.total == total, "count changed between steps"
@@ -230,7 +236,7 @@ def run_mine(args, rank, world, local_rank):
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         dg.reload_ptr(rp_h.data_ptr(), col_h.data_ptr(), g.n, g.m, stream=sptr)
-        r = dg.count(stream=sptr)
+        r = dg.count(stream=sptr, **kw)
         e1.record(stream)
         e1.synchronize()
         assert r.total == total
@@ -275,7 +281,12 @@ def run_mine(args, rank, world, local_rank):
                        sched="plain", phases_ms={k: round(v, 3) for k, v in phases.items()},
                        tree_nodes=stats[-1]["tree_nodes"], degeneracy=stats[-1]["degeneracy"],
                        max_later_degree=stats[-1]["max_later_degree"],
-                       class_roots=stats[-1]["class_roots"][:3]),
+                       class_roots=stats[-1]["class_roots"][:3],
+                       peel_rounds=stats[-1]["peel_rounds"],
+                       peel_solo_sections=stats[-1]["peel_solo_sections"],
+                       tasks_shared=stats[-1]["donations"],
+                       worker_list=args.wl, donate=args.donate, solo=args.solo,
+                       donate_after=args.after),
         "e2e": {"value": world * total / (e2e_ms / 1e3), "unit": "maximal cliques/s",
                 "h2d_bytes_per_step": int(4 * (g.n + 1) + 4 * g.m),
                 "d2h_bytes_per_step": int(8 * 4096 + 64 + 8 + 4 + 128),

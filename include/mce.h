@@ -78,7 +78,11 @@ typedef struct mce_opts {
   int32_t log_roots;        /* 1 = record per-root search-tree node counts    */
   int32_t x_pivot;          /* 1 = also take pivots from the root's earlier
                                neighbours (the -i px pivot rule)               */
-  int32_t reserved[7];
+  int32_t peel_solo_max;    /* 0 = default (off); < 0 = off; > 0: frontiers of at most
+                               this many vertices are peeled by one block           */
+  int32_t donate_after;     /* 0 = default (256): a warp shares subtrees of a
+                               root only after walking this many of its nodes */
+  int32_t reserved[5];
   void *stream;             /* cudaStream_t to queue work on; NULL = own      */
 } mce_opts_t;
 
@@ -100,6 +104,8 @@ typedef struct mce_stats {
   int32_t kernel_launches;  /* this library's kernels launched by the call    */
   uint32_t error_flags;     /* device-side status bits (0 = clean)            */
   int64_t class_roots[8];   /* roots per engine class                         */
+  int64_t peel_rounds;      /* synchronous peel rounds                        */
+  int64_t peel_solo_sections; /* runs of rounds peeled by a single block      */
 } mce_stats_t;
 
 /* ---- host graphs -------------------------------------------------------- */

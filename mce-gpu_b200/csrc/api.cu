@@ -72,7 +72,9 @@ namespace {
 constexpr uint64_t WAIT_LIMIT_NS = 20ull * 1000 * 1000 * 1000;  // 20 s per barrier wait
 constexpr uint64_t IDLE_LIMIT_NS = 30ull * 1000 * 1000 * 1000;  // 30 s without any progress
 constexpr uint32_t QUEUE_CAP = 1u << 14;                        // tasks per class queue
-constexpr int DEFAULT_DONATE_MIN = 10;  // the reference's SZTH (mce/parameter.cuh:5)
+constexpr int DEFAULT_DONATE_MIN = 10;
+constexpr uint32_t DEFAULT_SOLO_MAX = 0;     // measured slower than grid-wide rounds
+constexpr uint32_t DEFAULT_DONATE_AFTER = 256;  // the reference's SZTH (mce/parameter.cuh:5)
 
 void free_graph_bufs(mce_graph *g) {
   dfree(g->rp); dfree(g->col); dfree(g->cs); dfree(g->split);
@@ -137,7 +139,7 @@ int upload_csr(mce_graph *g, const int32_t *row_ptr, const int32_t *col, int64_t
 }
 
 // Stage 1: peel -> prio, core.
-int run_peel(mce_graph *g, cudaStream_t s, int *launches) {
+int run_peel(mce_graph *g, cudaStream_t s, int *launches, int solo_opt = 0) {
   if (g->n == 0) return MCE_OK;
   PeelArgs pa;
   pa.n = g->n;
@@ -154,6 +156,7 @@ int run_peel(mce_graph *g, cudaStream_t s, int *launches) {
   pa.front2 = g->f2;
   pa.ctl = g->peel_ctl;
   pa.wait_limit_ns = WAIT_LIMIT_NS;
+  pa.solo_max = solo_opt < 0 ? 0u : solo_opt == 0 ? DEFAULT_SOLO_MAX : (uint32_t)solo_opt;
   return peel_launch(pa, s, launches);
 }
 
@@ -320,7 +323,7 @@ int mce_degeneracy(mce_graph_t g, uint32_t *priority_out, int32_t *core_out,
   int32_t dg = 0;
   uint32_t err = 0, rounds = 0;
   if (g->n > 0) {
-    rc = peel_read(g->peel_ctl, &dg, &err, &rounds, s);
+    rc = peel_read(g->peel_ctl, &dg, &err, &rounds, nullptr, s);
     if (rc) return rc;
     if (err) return MCE_ETIMEOUT;
     if (priority_out)
@@ -368,7 +371,7 @@ int mce_count(mce_graph_t g, const mce_opts_t *opts, uint64_t *total, uint64_t *
   mce_stats_t st;
   std::memset(&st, 0, sizeof(st));
   MCE_CUDA(cudaEventRecord(g->ev[0], s));
-  if ((rc = run_peel(g, s, &launches))) return rc;
+  if ((rc = run_peel(g, s, &launches, o.peel_solo_max))) return rc;
   MCE_CUDA(cudaEventRecord(g->ev[1], s));
   if ((rc = run_orient(g, s, &launches))) return rc;
   MCE_CUDA(cudaEventRecord(g->ev[2], s));
@@ -425,6 +428,7 @@ int mce_count(mce_graph_t g, const mce_opts_t *opts, uint64_t *total, uint64_t *
   a.dcap = dcap;
   a.xcap = xcap;
   a.donate_min = o.donate_threshold > 0 ? o.donate_threshold : DEFAULT_DONATE_MIN;
+  a.donate_after = o.donate_after > 0 ? (uint32_t)o.donate_after : DEFAULT_DONATE_AFTER;
   a.wait_limit_ns = IDLE_LIMIT_NS;
   const int wbits = o.bitmap_width == 64 ? 64 : 32;
   // widest roots first so the long trees start early
@@ -446,13 +450,23 @@ int mce_count(mce_graph_t g, const mce_opts_t *opts, uint64_t *total, uint64_t *
   MCE_CUDA(cudaMemcpyAsync(h_hist, g->hist, sizeof(h_hist), cudaMemcpyDeviceToHost, s));
   MCE_CUDA(cudaMemcpyAsync(&h_nodes, g->nodes, sizeof(h_nodes), cudaMemcpyDeviceToHost, s));
   MCE_CUDA(cudaMemcpyAsync(&h_err, g->err, sizeof(h_err), cudaMemcpyDeviceToHost, s));
+  QueueHdr qh[NCLS];
+  bool qused[NCLS] = {false};
+  for (int c = 0; c < NCLS; ++c)
+    if (share && grid[c] && g->qbuf[c]) {
+      MCE_CUDA(cudaMemcpyAsync(&qh[c], g->qbuf[c], sizeof(QueueHdr), cudaMemcpyDeviceToHost, s));
+      qused[c] = true;
+    }
   MCE_CUDA(cudaEventRecord(g->ev[4], s));
   MCE_CUDA(cudaStreamSynchronize(s));
   int32_t dg = 0;
-  uint32_t perr = 0, rounds = 0;
-  if (g->n > 0 && (rc = peel_read(g->peel_ctl, &dg, &perr, &rounds, s))) return rc;
+  uint32_t perr = 0, rounds = 0, solo = 0;
+  if (g->n > 0 && (rc = peel_read(g->peel_ctl, &dg, &perr, &rounds, &solo, s))) return rc;
   g->degeneracy = dg;
   g->logged = o.log_roots != 0;
+  uint64_t pushed = 0;
+  for (int c = 0; c < NCLS; ++c)
+    if (qused[c]) pushed += qh[c].pushed;
   uint64_t tot = 0;
   for (int i = 0; i < MCE_HIST_MAX; ++i) tot += h_hist[i];
   *total = tot;
@@ -475,6 +489,9 @@ int mce_count(mce_graph_t g, const mce_opts_t *opts, uint64_t *total, uint64_t *
   st.kernel_launches = launches;
   st.error_flags = h_err | (perr ? MCE_ERR_WAIT_TIMEOUT : 0);
   for (int c = 0; c < NCLS && c < 8; ++c) st.class_roots[c] = sh.cls_cnt[c];
+  st.peel_rounds = rounds;
+  st.peel_solo_sections = solo;
+  st.donations = pushed;
   if (stats) *stats = st;
   if (perr) return MCE_ETIMEOUT;
   if (h_err & MCE_ERR_WAIT_TIMEOUT) return MCE_ETIMEOUT;

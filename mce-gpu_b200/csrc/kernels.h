@@ -18,11 +18,12 @@ struct PeelArgs {
   int32_t *alistA, *alistB, *front0, *front1, *front2;
   void *ctl;  // peel_ctl_bytes() of device memory
   uint64_t wait_limit_ns;
+  uint32_t solo_max;  // frontiers up to this size are peeled by block 0 alone (0: never)
 };
 size_t peel_ctl_bytes();
 int peel_launch(const PeelArgs &a, cudaStream_t s, int *launches);
 int peel_read(const void *ctl_dev, int32_t *degeneracy, uint32_t *err, uint32_t *rounds,
-              cudaStream_t s);
+              uint32_t *solo_sections, cudaStream_t s);
 
 // ---- orientation + root classes ------------------------------------------------
 // Engine classes of a root (by later degree d+ and earlier degree d-).
@@ -82,6 +83,7 @@ struct BKArgs {
   int32_t dcap, xcap;            // slab capacities (later degree, x rows)
   QueueView q;                   // task queue (q.hdr == nullptr: no sharing)
   int32_t donate_min;            // hand off children with at least this many candidates
+  uint32_t donate_after;         // ... once this many nodes of the root/task were walked
   uint64_t wait_limit_ns;        // an idle warp gives up after this long without progress
 };
 

@@ -30,7 +30,8 @@ namespace mce {
 struct PeelCtl {
   GridBarrier bar;
   uint32_t err;
-  uint32_t fcnt[3];    // frontier sizes, one slot per phase mod 3
+  uint32_t fcnt[3];    // light frontier sizes, one slot per phase mod 3
+  uint32_t hcnt[3];    // heavy frontier sizes (same slots)
   uint32_t acnt[3];    // alive-list sizes, one slot per scan mod 3
   uint32_t amin[3];    // min degree over the alive list written by a scan
   int32_t degeneracy;
@@ -46,11 +47,15 @@ struct PeelCtl {
 namespace {
 
 constexpr int PEEL_BLOCK = 512;
-// A frontier of at most SOLO_MAX vertices is peeled by block 0 alone, round
+// A frontier of at most solo_max vertices is peeled by block 0 alone, round
 // after round with __syncthreads between them, for up to SOLO_ROUNDS rounds
 // (well inside the other blocks' barrier wait limit).
-constexpr uint32_t SOLO_MAX = 1024;
 constexpr uint32_t SOLO_ROUNDS = 65536;
+// A frontier vertex with more neighbours than this is "heavy": it is stored
+// from the back of the frontier buffer and its neighbour list is walked in
+// 32-edge chunks by every warp, so no single warp serialises a hub while the
+// rest of the grid waits at the next barrier.
+constexpr int32_t HEAVY_DEG = 256;
 
 // warp-aggregated append of `pred` items to list[*cnt]
 __device__ __forceinline__ void warp_append(bool pred, int32_t val, int32_t *list,
@@ -65,40 +70,83 @@ __device__ __forceinline__ void warp_append(bool pred, int32_t val, int32_t *lis
   if (pred) list[base + __popc(mask & ((1u << lane) - 1u))] = val;
 }
 
+// append at the back: list[cap - 1 - k] for the k-th item
+__device__ __forceinline__ void warp_append_back(bool pred, int32_t val, int32_t *list,
+                                                 int64_t cap, uint32_t *cnt) {
+  const uint32_t mask = __ballot_sync(MCE_FULL, pred);
+  if (!mask) return;
+  const uint32_t lane = lane_id();
+  uint32_t base = 0;
+  const int leader = __ffs(mask) - 1;
+  if ((int)lane == leader) base = atomicAdd(cnt, (uint32_t)__popc(mask));
+  base = __shfl_sync(MCE_FULL, base, leader);
+  if (pred) list[cap - 1 - (int64_t)(base + __popc(mask & ((1u << lane) - 1u)))] = val;
+}
+
+__device__ __forceinline__ uint32_t frontier_size(const PeelCtl *ctl, int slot) {
+  return ld_volatile(&ctl->fcnt[slot]) + ld_volatile(&ctl->hcnt[slot]);
+}
+
+// Lower the degree of neighbour col[j] of a vertex being removed; true if it
+// falls to `level` (it then joins the next round).
+__device__ __forceinline__ bool peel_edge(int32_t j, int32_t e, int32_t level,
+                                          const int32_t *__restrict__ col, int32_t *deg,
+                                          int32_t *core, int32_t &u) {
+  u = 0;
+  if (j >= e) return false;
+  u = col[j];
+  if (ld_volatile((const uint32_t *)&core[u]) != 0xFFFFFFFFu) return false;
+  const int32_t old = atomicSub(&deg[u], 1);
+  if (old != level + 1) return false;
+  core[u] = level;
+  return true;
+}
+
 // One peel round (phase q) over the frontier in slot q % 3, executed by the
 // threads [t0, t0 + nt) (the whole grid, or block 0 alone): set the round's
 // priority, lower the neighbours' degrees and append every neighbour whose
 // degree falls to `level` to the frontier in slot (q + 1) % 3.
-__device__ __forceinline__ void peel_round(uint32_t q, uint32_t cnt, int32_t level,
-                                           uint32_t priority, int64_t t0, int64_t nt,
+__device__ __forceinline__ void peel_round(uint32_t q, int32_t level, uint32_t priority,
+                                           int64_t t0, int64_t nt, int64_t cap,
                                            const int32_t *__restrict__ rp,
                                            const int32_t *__restrict__ col, int32_t *deg,
                                            int32_t *core, uint32_t *prio, int32_t *const *fr,
                                            PeelCtl *ctl) {
   const uint32_t lane = lane_id();
   const int fn = (q + 1) % 3;
-  if (t0 == 0) ctl->fcnt[(q + 2) % 3] = 0;
+  if (t0 == 0) {
+    ctl->fcnt[(q + 2) % 3] = 0;
+    ctl->hcnt[(q + 2) % 3] = 0;
+  }
+  const uint32_t lc = ld_volatile(&ctl->fcnt[q % 3]), hc = ld_volatile(&ctl->hcnt[q % 3]);
   const int32_t *Fc = fr[q % 3];
   int32_t *Fn = fr[fn];
-  for (int64_t i = t0; i < cnt; i += nt) prio[Fc[i]] = priority;
-  for (int64_t i = t0 >> 5; i < cnt; i += nt >> 5) {
+  for (int64_t i = t0; i < lc; i += nt) prio[Fc[i]] = priority;
+  for (int64_t i = t0; i < hc; i += nt) prio[Fc[cap - 1 - i]] = priority;
+  auto push = [&](bool p, int32_t u) {
+    bool heavy = false;
+    if (p) heavy = rp[u + 1] - rp[u] > HEAVY_DEG;
+    warp_append(p && !heavy, u, Fn, &ctl->fcnt[fn]);
+    warp_append_back(p && heavy, u, Fn, cap, &ctl->hcnt[fn]);
+  };
+  // light vertices: a warp each
+  for (int64_t i = t0 >> 5; i < lc; i += nt >> 5) {
     const int32_t v = Fc[i];
     const int32_t b = rp[v], e = rp[v + 1];
     for (int32_t j0 = b; j0 < e; j0 += 32) {
-      const int32_t j = j0 + (int32_t)lane;
-      bool push = false;
-      int32_t u = 0;
-      if (j < e) {
-        u = col[j];
-        if (ld_volatile((const uint32_t *)&core[u]) == 0xFFFFFFFFu) {
-          const int32_t old = atomicSub(&deg[u], 1);
-          if (old == level + 1) {
-            core[u] = level;
-            push = true;
-          }
-        }
-      }
-      warp_append(push, u, Fn, &ctl->fcnt[fn]);
+      int32_t u;
+      const bool p = peel_edge(j0 + (int32_t)lane, e, level, col, deg, core, u);
+      push(p, u);
+    }
+  }
+  // heavy vertices: their 32-edge chunks spread over all warps
+  for (uint32_t h = 0; h < hc; ++h) {
+    const int32_t v = Fc[cap - 1 - h];
+    const int32_t b = rp[v], e = rp[v + 1];
+    for (int64_t j0 = b + 32 * (t0 >> 5); j0 < e; j0 += 32 * (nt >> 5)) {
+      int32_t u;
+      const bool p = peel_edge((int32_t)j0 + (int32_t)lane, e, level, col, deg, core, u);
+      push(p, u);
     }
   }
 }
@@ -107,7 +155,7 @@ __global__ void __launch_bounds__(PEEL_BLOCK)
     peel_kernel(int32_t n, uint32_t m, const int32_t *__restrict__ rp,
                 const int32_t *__restrict__ col, int32_t *deg, int32_t *core, uint32_t *prio,
                 int32_t *alistA, int32_t *alistB, int32_t *front0, int32_t *front1,
-                int32_t *front2, PeelCtl *ctl, uint64_t limit_ns) {
+                int32_t *front2, PeelCtl *ctl, uint64_t limit_ns, uint32_t solo_max) {
   const uint32_t nblocks = gridDim.x;
   const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t nthr = (int64_t)gridDim.x * blockDim.x;
@@ -123,6 +171,7 @@ __global__ void __launch_bounds__(PEEL_BLOCK)
   }
   if (tid == 0) {  // phase/scan 0 reads acnt[0]; every other counter starts at 0
     ctl->fcnt[0] = ctl->fcnt[1] = ctl->fcnt[2] = 0;
+    ctl->hcnt[0] = ctl->hcnt[1] = ctl->hcnt[2] = 0;
     ctl->acnt[0] = (uint32_t)n;
     ctl->acnt[1] = ctl->acnt[2] = 0;
     ctl->amin[0] = ctl->amin[1] = ctl->amin[2] = 0xFFFFFFFFu;
@@ -151,6 +200,7 @@ __global__ void __launch_bounds__(PEEL_BLOCK)
       ctl->acnt[(s + 2) % 3] = 0;
       ctl->amin[(s + 2) % 3] = 0xFFFFFFFFu;
       ctl->fcnt[(q + 2) % 3] = 0;
+      ctl->hcnt[(q + 2) % 3] = 0;
     }
     {
       uint32_t mymin = 0xFFFFFFFFu;
@@ -166,7 +216,9 @@ __global__ void __launch_bounds__(PEEL_BLOCK)
         const bool inF = live && d == level;
         const bool keep = live && d > level;
         if (inF) core[v] = level;
-        warp_append(inF, v, F, &ctl->fcnt[fo]);
+        const bool heavy = inF && rp[v + 1] - rp[v] > HEAVY_DEG;
+        warp_append(inF && !heavy, v, F, &ctl->fcnt[fo]);
+        warp_append_back(heavy, v, F, (int64_t)n + 1, &ctl->hcnt[fo]);
         warp_append(keep, v, A2, &ctl->acnt[ao]);
         if (keep) mymin = min(mymin, (uint32_t)d);
       }
@@ -176,7 +228,7 @@ __global__ void __launch_bounds__(PEEL_BLOCK)
     if (!grid_sync(&ctl->bar, nblocks, &ctl->err, limit_ns)) return;
     ++q;
     ++s;
-    uint32_t cnt = ld_volatile(&ctl->fcnt[q % 3]);
+    uint32_t cnt = frontier_size(ctl, q % 3);
     if (cnt == 0) {
       // no vertex of degree `level` remains: jump to the smallest degree
       // (a rescan at that level always finds the vertex that attains it)
@@ -194,21 +246,21 @@ __global__ void __launch_bounds__(PEEL_BLOCK)
       degen = level;
       todo -= cnt;
       if (todo == 0) break;  // the final round keeps priority = m
-      if (cnt <= SOLO_MAX) {
+      if (cnt <= solo_max) {
         // Small frontier: block 0 peels consecutive rounds alone.  The first
         // barrier lets every block read `cnt` before block 0 recycles slots.
         if (!grid_sync(&ctl->bar, nblocks, &ctl->err, limit_ns)) return;
         if (blockIdx.x == 0) {
           uint32_t it = 0;
           for (;;) {
-            peel_round(q, cnt, level, priority, threadIdx.x, blockDim.x, rp, col, deg, core,
-                       prio, fr, ctl);
+            peel_round(q, level, priority, threadIdx.x, blockDim.x, (int64_t)n + 1, rp, col,
+                       deg, core, prio, fr, ctl);
             __syncthreads();
             ++q;
-            cnt = ld_volatile(&ctl->fcnt[q % 3]);
+            cnt = frontier_size(ctl, q % 3);
             ++priority;
             ++rounds;
-            if (cnt == 0 || cnt > SOLO_MAX || ++it >= SOLO_ROUNDS) break;  // cnt not yet counted
+            if (cnt == 0 || cnt > solo_max || ++it >= SOLO_ROUNDS) break;  // cnt not yet counted
             degen = level;
             todo -= cnt;
             if (todo == 0) break;  // the final round keeps priority = m
@@ -234,10 +286,10 @@ __global__ void __launch_bounds__(PEEL_BLOCK)
         if (todo == 0) break;
         continue;
       }
-      peel_round(q, cnt, level, priority, tid, nthr, rp, col, deg, core, prio, fr, ctl);
+      peel_round(q, level, priority, tid, nthr, (int64_t)n + 1, rp, col, deg, core, prio, fr, ctl);
       if (!grid_sync(&ctl->bar, nblocks, &ctl->err, limit_ns)) return;
       ++q;
-      cnt = ld_volatile(&ctl->fcnt[q % 3]);
+      cnt = frontier_size(ctl, q % 3);
       ++priority;
       ++rounds;
     }
@@ -269,10 +321,11 @@ int peel_launch(const PeelArgs &a, cudaStream_t s, int *launches) {
   PeelCtl *ctl = (PeelCtl *)a.ctl;
   MCE_CUDA(cudaMemsetAsync(ctl, 0, sizeof(PeelCtl), s));
   uint64_t limit = a.wait_limit_ns;
+  uint32_t solo_max = a.solo_max;
   void *args[] = {(void *)&n,        (void *)&m,        (void *)&a.rp,     (void *)&a.col,
                   (void *)&a.deg,    (void *)&a.core,   (void *)&a.prio,   (void *)&a.alistA,
                   (void *)&a.alistB, (void *)&a.front0, (void *)&a.front1, (void *)&a.front2,
-                  (void *)&ctl,      (void *)&limit};
+                  (void *)&ctl,      (void *)&limit,    (void *)&solo_max};
   MCE_CUDA(cudaLaunchCooperativeKernel((void *)peel_kernel, dim3(sms * per_sm), dim3(PEEL_BLOCK),
                                        args, 0, s));
   if (launches) *launches += 1;
@@ -280,13 +333,14 @@ int peel_launch(const PeelArgs &a, cudaStream_t s, int *launches) {
 }
 
 int peel_read(const void *ctl_dev, int32_t *degeneracy, uint32_t *err, uint32_t *rounds,
-              cudaStream_t s) {
+              uint32_t *solo_sections, cudaStream_t s) {
   PeelCtl h;
   MCE_CUDA(cudaMemcpyAsync(&h, ctl_dev, sizeof(PeelCtl), cudaMemcpyDeviceToHost, s));
   MCE_CUDA(cudaStreamSynchronize(s));
   if (degeneracy) *degeneracy = h.degeneracy;
   if (err) *err = h.err;
   if (rounds) *rounds = h.rounds;
+  if (solo_sections) *solo_sections = h.solo_sections;
   return MCE_OK;
 }
 

@@ -43,7 +43,9 @@ class _Opts(C.Structure):
                 ("sched", C.c_int32), ("bitmap_width", C.c_int32),
                 ("warps_per_root", C.c_int32), ("donate_threshold", C.c_int32),
                 ("log_roots", C.c_int32), ("x_pivot", C.c_int32),
-                ("reserved", C.c_int32 * 7), ("stream", C.c_void_p)]
+                ("peel_solo_max", C.c_int32), ("donate_after", C.c_int32),
+                ("reserved", C.c_int32 * 5),
+                ("stream", C.c_void_p)]
 
 
 class _Stats(C.Structure):
@@ -52,7 +54,8 @@ class _Stats(C.Structure):
                 ("max_later_degree", C.c_int32), ("max_degree", C.c_int64),
                 ("roots", C.c_int64), ("tree_nodes", C.c_uint64), ("donations", C.c_uint64),
                 ("kernel_launches", C.c_int32), ("error_flags", C.c_uint32),
-                ("class_roots", C.c_int64 * 8)]
+                ("class_roots", C.c_int64 * 8), ("peel_rounds", C.c_int64),
+                ("peel_solo_sections", C.c_int64)]
 
 
 class _HGraph(C.Structure):
@@ -317,12 +320,13 @@ class Graph:
 
     def count(self, *, sched=SCHED_PLAIN, bitmap_width=0, log_roots=False, level=LEVEL_L1,
               induced=INDUCED_P, worker_list=WL_ON, donate_threshold=0, x_pivot=0,
-              stream=None) -> CountResult:
+              peel_solo_max=0, donate_after=0, stream=None) -> CountResult:
         o = _Opts()
         _lib.mce_opts_default(C.byref(o))
         o.sched, o.bitmap_width, o.log_roots = sched, bitmap_width, int(bool(log_roots))
         o.level, o.induced, o.worker_list = level, induced, worker_list
         o.donate_threshold, o.x_pivot = donate_threshold, x_pivot
+        o.peel_solo_max, o.donate_after = peel_solo_max, donate_after
         o.stream = stream
         total = C.c_uint64()
         hist = np.zeros(HIST_MAX, np.uint64)

@@ -189,10 +189,13 @@ def test_worker_list_on_off_identical(maker):
     t, h, rc_o, rn_o = oracle.roots(g)
     out = {}
     with mce.Graph.from_host(g) as dg:
-        for wl in (mce.WL_ON, mce.WL_OFF):
-            for dmin in ((2, 10) if wl == mce.WL_ON else (10,)):
-                r = dg.count(worker_list=wl, donate_threshold=dmin, log_roots=True)
-                out[(wl, dmin)] = (r.total, r.hist.copy(), dg.root_counts(), dg.root_log())
+        # (sharing, smallest shared candidate set, nodes walked before sharing)
+        for wl, dmin, after in ((mce.WL_ON, 2, 1), (mce.WL_ON, 10, 1), (mce.WL_ON, 10, 0),
+                                (mce.WL_OFF, 10, 0)):
+            r = dg.count(worker_list=wl, donate_threshold=dmin, donate_after=after, log_roots=True)
+            out[(wl, dmin, after)] = (r.total, r.hist.copy(), dg.root_counts(), dg.root_log())
+            if wl == mce.WL_ON and after == 1:
+                assert r.stats["donations"] > 0  # the sharing path really ran
     for (tot, hist, rc, rn) in out.values():
         assert tot == t and np.array_equal(hist, h)
         assert np.array_equal(rc, rc_o)
