@@ -45,6 +45,7 @@ struct mce_graph {
   uint32_t *prio = nullptr;
   int32_t *core = nullptr, *deg = nullptr, *alA = nullptr, *alB = nullptr;
   int32_t *f0 = nullptr, *f1 = nullptr, *f2 = nullptr;
+  int32_t *hb0 = nullptr, *hb1 = nullptr, *hb2 = nullptr;
   void *peel_ctl = nullptr;
   // roots
   uint32_t *keys_in = nullptr, *keys_out = nullptr;
@@ -80,6 +81,7 @@ void free_graph_bufs(mce_graph *g) {
   dfree(g->rp); dfree(g->col); dfree(g->cs); dfree(g->split);
   dfree(g->prio); dfree(g->core); dfree(g->deg); dfree(g->alA); dfree(g->alB);
   dfree(g->f0); dfree(g->f1); dfree(g->f2);
+  dfree(g->hb0); dfree(g->hb1); dfree(g->hb2);
   dfree(g->keys_in); dfree(g->keys_out); dfree(g->vals_in); dfree(g->roots);
   dfree(g->root_nodes); dfree(g->root_count);
   g->cap_n = g->cap_m = -1;
@@ -93,6 +95,7 @@ int alloc_graph_bufs(mce_graph *g, int64_t n, int64_t m) {
       (rc = dalloc(&g->split, N)) || (rc = dalloc(&g->prio, N)) || (rc = dalloc(&g->core, N)) ||
       (rc = dalloc(&g->deg, N)) || (rc = dalloc(&g->alA, N)) || (rc = dalloc(&g->alB, N)) ||
       (rc = dalloc(&g->f0, N)) || (rc = dalloc(&g->f1, N)) || (rc = dalloc(&g->f2, N)) ||
+      (rc = dalloc(&g->hb0, N)) || (rc = dalloc(&g->hb1, N)) || (rc = dalloc(&g->hb2, N)) ||
       (rc = dalloc(&g->keys_in, N)) || (rc = dalloc(&g->keys_out, N)) ||
       (rc = dalloc(&g->vals_in, N)) || (rc = dalloc(&g->roots, N))) {
     free_graph_bufs(g);
@@ -154,6 +157,9 @@ int run_peel(mce_graph *g, cudaStream_t s, int *launches, int solo_opt = 0) {
   pa.front0 = g->f0;
   pa.front1 = g->f1;
   pa.front2 = g->f2;
+  pa.hb0 = g->hb0;
+  pa.hb1 = g->hb1;
+  pa.hb2 = g->hb2;
   pa.ctl = g->peel_ctl;
   pa.wait_limit_ns = WAIT_LIMIT_NS;
   pa.solo_max = solo_opt < 0 ? 0u : solo_opt == 0 ? DEFAULT_SOLO_MAX : (uint32_t)solo_opt;

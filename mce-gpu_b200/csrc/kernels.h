@@ -16,6 +16,7 @@ struct PeelArgs {
   int32_t *deg, *core;
   uint32_t *prio;
   int32_t *alistA, *alistB, *front0, *front1, *front2;
+  int32_t *hb0, *hb1, *hb2;  // heavy chunk bases per frontier slot (n + 1 each)
   void *ctl;  // peel_ctl_bytes() of device memory
   uint64_t wait_limit_ns;
   uint32_t solo_max;  // frontiers up to this size are peeled by block 0 alone (0: never)

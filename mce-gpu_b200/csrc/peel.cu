@@ -31,7 +31,7 @@ struct PeelCtl {
   GridBarrier bar;
   uint32_t err;
   uint32_t fcnt[3];    // light frontier sizes, one slot per phase mod 3
-  uint32_t hcnt[3];    // heavy frontier sizes (same slots)
+  unsigned long long hpack[3];  // heavy frontier: (count << 32) | 32-edge chunks
   uint32_t acnt[3];    // alive-list sizes, one slot per scan mod 3
   uint32_t amin[3];    // min degree over the alive list written by a scan
   int32_t degeneracy;
@@ -52,9 +52,11 @@ constexpr int PEEL_BLOCK = 512;
 // (well inside the other blocks' barrier wait limit).
 constexpr uint32_t SOLO_ROUNDS = 65536;
 // A frontier vertex with more neighbours than this is "heavy": it is stored
-// from the back of the frontier buffer and its neighbour list is walked in
-// 32-edge chunks by every warp, so no single warp serialises a hub while the
-// rest of the grid waits at the next barrier.
+// from the back of the frontier buffer, its first chunk number goes to the
+// slot's chunk-base array, and the round spreads all heavy chunks (32 edges
+// each) over every warp, so no single warp serialises a hub while the rest
+// of the grid waits at the next barrier.  One 64-bit atomic hands out both
+// the slot and the chunk base, so bases increase with the slot.
 constexpr int32_t HEAVY_DEG = 256;
 
 // warp-aggregated append of `pred` items to list[*cnt]
@@ -70,21 +72,24 @@ __device__ __forceinline__ void warp_append(bool pred, int32_t val, int32_t *lis
   if (pred) list[base + __popc(mask & ((1u << lane) - 1u))] = val;
 }
 
-// append at the back: list[cap - 1 - k] for the k-th item
-__device__ __forceinline__ void warp_append_back(bool pred, int32_t val, int32_t *list,
-                                                 int64_t cap, uint32_t *cnt) {
-  const uint32_t mask = __ballot_sync(MCE_FULL, pred);
-  if (!mask) return;
-  const uint32_t lane = lane_id();
-  uint32_t base = 0;
-  const int leader = __ffs(mask) - 1;
-  if ((int)lane == leader) base = atomicAdd(cnt, (uint32_t)__popc(mask));
-  base = __shfl_sync(MCE_FULL, base, leader);
-  if (pred) list[cap - 1 - (int64_t)(base + __popc(mask & ((1u << lane) - 1u)))] = val;
+// Append a heavy vertex: slot k at list[cap - 1 - k], first chunk at base[k].
+__device__ __forceinline__ void heavy_append(bool pred, int32_t v, int32_t degv, int32_t *list,
+                                             int32_t *base, int64_t cap,
+                                             unsigned long long *pack) {
+  if (!pred) return;
+  const unsigned long long chunks = (unsigned long long)((degv + 31) / 32);
+  const unsigned long long old = atomicAdd(pack, (1ull << 32) | chunks);
+  const uint32_t slot = (uint32_t)(old >> 32);
+  list[cap - 1 - (int64_t)slot] = v;
+  base[slot] = (int32_t)(uint32_t)old;
+}
+
+__device__ __forceinline__ unsigned long long ld_volatile64(const unsigned long long *p) {
+  return *(const volatile unsigned long long *)p;
 }
 
 __device__ __forceinline__ uint32_t frontier_size(const PeelCtl *ctl, int slot) {
-  return ld_volatile(&ctl->fcnt[slot]) + ld_volatile(&ctl->hcnt[slot]);
+  return ld_volatile(&ctl->fcnt[slot]) + (uint32_t)(ld_volatile64(&ctl->hpack[slot]) >> 32);
 }
 
 // Lower the degree of neighbour col[j] of a vertex being removed; true if it
@@ -111,23 +116,26 @@ __device__ __forceinline__ void peel_round(uint32_t q, int32_t level, uint32_t p
                                            const int32_t *__restrict__ rp,
                                            const int32_t *__restrict__ col, int32_t *deg,
                                            int32_t *core, uint32_t *prio, int32_t *const *fr,
-                                           PeelCtl *ctl) {
+                                           int32_t *const *hb, PeelCtl *ctl) {
   const uint32_t lane = lane_id();
   const int fn = (q + 1) % 3;
   if (t0 == 0) {
     ctl->fcnt[(q + 2) % 3] = 0;
-    ctl->hcnt[(q + 2) % 3] = 0;
+    ctl->hpack[(q + 2) % 3] = 0;
   }
-  const uint32_t lc = ld_volatile(&ctl->fcnt[q % 3]), hc = ld_volatile(&ctl->hcnt[q % 3]);
-  const int32_t *Fc = fr[q % 3];
-  int32_t *Fn = fr[fn];
+  const uint32_t lc = ld_volatile(&ctl->fcnt[q % 3]);
+  const unsigned long long hp = ld_volatile64(&ctl->hpack[q % 3]);
+  const uint32_t hc = (uint32_t)(hp >> 32), hch = (uint32_t)hp;
+  const int32_t *Fc = fr[q % 3], *HB = hb[q % 3];
+  int32_t *Fn = fr[fn], *HBn = hb[fn];
   for (int64_t i = t0; i < lc; i += nt) prio[Fc[i]] = priority;
   for (int64_t i = t0; i < hc; i += nt) prio[Fc[cap - 1 - i]] = priority;
   auto push = [&](bool p, int32_t u) {
-    bool heavy = false;
-    if (p) heavy = rp[u + 1] - rp[u] > HEAVY_DEG;
+    int32_t du = 0;
+    if (p) du = rp[u + 1] - rp[u];
+    const bool heavy = p && du > HEAVY_DEG;
     warp_append(p && !heavy, u, Fn, &ctl->fcnt[fn]);
-    warp_append_back(p && heavy, u, Fn, cap, &ctl->hcnt[fn]);
+    heavy_append(heavy, u, du, Fn, HBn, cap, &ctl->hpack[fn]);
   };
   // light vertices: a warp each
   for (int64_t i = t0 >> 5; i < lc; i += nt >> 5) {
@@ -139,15 +147,23 @@ __device__ __forceinline__ void peel_round(uint32_t q, int32_t level, uint32_t p
       push(p, u);
     }
   }
-  // heavy vertices: their 32-edge chunks spread over all warps
-  for (uint32_t h = 0; h < hc; ++h) {
-    const int32_t v = Fc[cap - 1 - h];
-    const int32_t b = rp[v], e = rp[v + 1];
-    for (int64_t j0 = b + 32 * (t0 >> 5); j0 < e; j0 += 32 * (nt >> 5)) {
-      int32_t u;
-      const bool p = peel_edge((int32_t)j0 + (int32_t)lane, e, level, col, deg, core, u);
-      push(p, u);
+  // heavy vertices: chunk c belongs to the last slot whose base is <= c
+  for (int64_t c = t0 >> 5; c < hch; c += nt >> 5) {
+    int lo = 0, hi = (int)hc;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (HB[mid] <= (int32_t)c)
+        lo = mid + 1;
+      else
+        hi = mid;
     }
+    const int h = lo - 1;
+    const int32_t v = Fc[cap - 1 - h];
+    const int32_t e = rp[v + 1];
+    const int32_t j = rp[v] + ((int32_t)c - HB[h]) * 32 + (int32_t)lane;
+    int32_t u;
+    const bool p = peel_edge(j, e, level, col, deg, core, u);
+    push(p, u);
   }
 }
 
@@ -155,12 +171,14 @@ __global__ void __launch_bounds__(PEEL_BLOCK)
     peel_kernel(int32_t n, uint32_t m, const int32_t *__restrict__ rp,
                 const int32_t *__restrict__ col, int32_t *deg, int32_t *core, uint32_t *prio,
                 int32_t *alistA, int32_t *alistB, int32_t *front0, int32_t *front1,
-                int32_t *front2, PeelCtl *ctl, uint64_t limit_ns, uint32_t solo_max) {
+                int32_t *front2, int32_t *hb0, int32_t *hb1, int32_t *hb2, PeelCtl *ctl,
+                uint64_t limit_ns, uint32_t solo_max) {
   const uint32_t nblocks = gridDim.x;
   const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t nthr = (int64_t)gridDim.x * blockDim.x;
   const uint32_t lane = lane_id();
   int32_t *const fr[3] = {front0, front1, front2};
+  int32_t *const hb[3] = {hb0, hb1, hb2};
   int32_t *alist[2] = {alistA, alistB};
 
   for (int64_t v = tid; v < n; v += nthr) {
@@ -171,7 +189,7 @@ __global__ void __launch_bounds__(PEEL_BLOCK)
   }
   if (tid == 0) {  // phase/scan 0 reads acnt[0]; every other counter starts at 0
     ctl->fcnt[0] = ctl->fcnt[1] = ctl->fcnt[2] = 0;
-    ctl->hcnt[0] = ctl->hcnt[1] = ctl->hcnt[2] = 0;
+    ctl->hpack[0] = ctl->hpack[1] = ctl->hpack[2] = 0;
     ctl->acnt[0] = (uint32_t)n;
     ctl->acnt[1] = ctl->acnt[2] = 0;
     ctl->amin[0] = ctl->amin[1] = ctl->amin[2] = 0xFFFFFFFFu;
@@ -200,7 +218,7 @@ __global__ void __launch_bounds__(PEEL_BLOCK)
       ctl->acnt[(s + 2) % 3] = 0;
       ctl->amin[(s + 2) % 3] = 0xFFFFFFFFu;
       ctl->fcnt[(q + 2) % 3] = 0;
-      ctl->hcnt[(q + 2) % 3] = 0;
+      ctl->hpack[(q + 2) % 3] = 0;
     }
     {
       uint32_t mymin = 0xFFFFFFFFu;
@@ -216,9 +234,10 @@ __global__ void __launch_bounds__(PEEL_BLOCK)
         const bool inF = live && d == level;
         const bool keep = live && d > level;
         if (inF) core[v] = level;
-        const bool heavy = inF && rp[v + 1] - rp[v] > HEAVY_DEG;
+        const int32_t dv = inF ? rp[v + 1] - rp[v] : 0;
+        const bool heavy = inF && dv > HEAVY_DEG;
         warp_append(inF && !heavy, v, F, &ctl->fcnt[fo]);
-        warp_append_back(heavy, v, F, (int64_t)n + 1, &ctl->hcnt[fo]);
+        heavy_append(heavy, v, dv, F, hb[fo], (int64_t)n + 1, &ctl->hpack[fo]);
         warp_append(keep, v, A2, &ctl->acnt[ao]);
         if (keep) mymin = min(mymin, (uint32_t)d);
       }
@@ -254,7 +273,7 @@ __global__ void __launch_bounds__(PEEL_BLOCK)
           uint32_t it = 0;
           for (;;) {
             peel_round(q, level, priority, threadIdx.x, blockDim.x, (int64_t)n + 1, rp, col,
-                       deg, core, prio, fr, ctl);
+                       deg, core, prio, fr, hb, ctl);
             __syncthreads();
             ++q;
             cnt = frontier_size(ctl, q % 3);
@@ -286,7 +305,8 @@ __global__ void __launch_bounds__(PEEL_BLOCK)
         if (todo == 0) break;
         continue;
       }
-      peel_round(q, level, priority, tid, nthr, (int64_t)n + 1, rp, col, deg, core, prio, fr, ctl);
+      peel_round(q, level, priority, tid, nthr, (int64_t)n + 1, rp, col, deg, core, prio, fr, hb,
+                 ctl);
       if (!grid_sync(&ctl->bar, nblocks, &ctl->err, limit_ns)) return;
       ++q;
       cnt = frontier_size(ctl, q % 3);
@@ -325,6 +345,7 @@ int peel_launch(const PeelArgs &a, cudaStream_t s, int *launches) {
   void *args[] = {(void *)&n,        (void *)&m,        (void *)&a.rp,     (void *)&a.col,
                   (void *)&a.deg,    (void *)&a.core,   (void *)&a.prio,   (void *)&a.alistA,
                   (void *)&a.alistB, (void *)&a.front0, (void *)&a.front1, (void *)&a.front2,
+                  (void *)&a.hb0,    (void *)&a.hb1,    (void *)&a.hb2,
                   (void *)&ctl,      (void *)&limit,    (void *)&solo_max};
   MCE_CUDA(cudaLaunchCooperativeKernel((void *)peel_kernel, dim3(sms * per_sm), dim3(PEEL_BLOCK),
                                        args, 0, s));
