@@ -284,6 +284,8 @@ def run_mine(args, rank, world, local_rank):
                        class_roots=stats[-1]["class_roots"][:3],
                        peel_rounds=stats[-1]["peel_rounds"],
                        peel_solo_sections=stats[-1]["peel_solo_sections"],
+                       peel_split_ms={k: round(stats[-1]["peel_" + k + "_ms"], 3)
+                                      for k in ("scan", "round", "wait")},
                        tasks_shared=stats[-1]["donations"],
                        worker_list=args.wl, donate=args.donate, solo=args.solo,
                        donate_after=args.after),

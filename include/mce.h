@@ -106,6 +106,9 @@ typedef struct mce_stats {
   int64_t class_roots[8];   /* roots per engine class                         */
   int64_t peel_rounds;      /* synchronous peel rounds                        */
   int64_t peel_solo_sections; /* runs of rounds peeled by a single block      */
+  double peel_scan_ms;      /* peel time split as seen by one block: level    */
+  double peel_round_ms;     /* scans, round work, and waits at grid barriers  */
+  double peel_wait_ms;
 } mce_stats_t;
 
 /* ---- host graphs -------------------------------------------------------- */

@@ -467,7 +467,8 @@ int mce_count(mce_graph_t g, const mce_opts_t *opts, uint64_t *total, uint64_t *
   MCE_CUDA(cudaStreamSynchronize(s));
   int32_t dg = 0;
   uint32_t perr = 0, rounds = 0, solo = 0;
-  if (g->n > 0 && (rc = peel_read(g->peel_ctl, &dg, &perr, &rounds, &solo, s))) return rc;
+  double pms[3] = {0, 0, 0};
+  if (g->n > 0 && (rc = peel_read(g->peel_ctl, &dg, &perr, &rounds, &solo, s, pms))) return rc;
   g->degeneracy = dg;
   g->logged = o.log_roots != 0;
   uint64_t pushed = 0;
@@ -497,6 +498,9 @@ int mce_count(mce_graph_t g, const mce_opts_t *opts, uint64_t *total, uint64_t *
   for (int c = 0; c < NCLS && c < 8; ++c) st.class_roots[c] = sh.cls_cnt[c];
   st.peel_rounds = rounds;
   st.peel_solo_sections = solo;
+  st.peel_scan_ms = pms[0];
+  st.peel_round_ms = pms[1];
+  st.peel_wait_ms = pms[2];
   st.donations = pushed;
   if (stats) *stats = st;
   if (perr) return MCE_ETIMEOUT;

@@ -24,7 +24,7 @@ struct PeelArgs {
 size_t peel_ctl_bytes();
 int peel_launch(const PeelArgs &a, cudaStream_t s, int *launches);
 int peel_read(const void *ctl_dev, int32_t *degeneracy, uint32_t *err, uint32_t *rounds,
-              uint32_t *solo_sections, cudaStream_t s);
+              uint32_t *solo_sections, cudaStream_t s, double *phase_ms = nullptr);
 
 // ---- orientation + root classes ------------------------------------------------
 // Engine classes of a root (by later degree d+ and earlier degree d-).

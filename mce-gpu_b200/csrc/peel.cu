@@ -42,6 +42,7 @@ struct PeelCtl {
   int64_t solo_todo;
   int32_t solo_degen;
   uint32_t solo_sections;
+  unsigned long long t_scan, t_round, t_wait;  // ns seen by block 0 (diagnostics)
 };
 
 namespace {
@@ -70,6 +71,37 @@ __device__ __forceinline__ void warp_append(bool pred, int32_t val, int32_t *lis
   if ((int)lane == leader) base = atomicAdd(cnt, (uint32_t)__popc(mask));
   base = __shfl_sync(MCE_FULL, base, leader);
   if (pred) list[base + __popc(mask & ((1u << lane) - 1u))] = val;
+}
+
+// Block-aggregated appends to two lists (one atomic per list per block);
+// every thread of the block must call it.
+__device__ __forceinline__ void block_append2(bool p1, int32_t v1, int32_t *l1, uint32_t *c1,
+                                              bool p2, int32_t v2, int32_t *l2, uint32_t *c2) {
+  __shared__ uint32_t w1[PEEL_BLOCK / 32], w2[PEEL_BLOCK / 32], base1, base2;
+  const uint32_t lane = lane_id(), wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const uint32_t lt = (1u << lane) - 1u;
+  const uint32_t m1 = __ballot_sync(MCE_FULL, p1), m2 = __ballot_sync(MCE_FULL, p2);
+  if (lane == 0) {
+    w1[wid] = __popc(m1);
+    w2[wid] = __popc(m2);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t a = 0, b = 0;
+    for (uint32_t w = 0; w < nw; ++w) {
+      const uint32_t x = w1[w], y = w2[w];
+      w1[w] = a;
+      w2[w] = b;
+      a += x;
+      b += y;
+    }
+    base1 = a ? atomicAdd(c1, a) : 0;
+    base2 = b ? atomicAdd(c2, b) : 0;
+  }
+  __syncthreads();
+  if (p1) l1[base1 + w1[wid] + __popc(m1 & lt)] = v1;
+  if (p2) l2[base2 + w2[wid] + __popc(m2 & lt)] = v2;
+  __syncthreads();  // the shared counters are reused by the next call
 }
 
 // Append a heavy vertex: slot k at list[cap - 1 - k], first chunk at base[k].
@@ -196,6 +228,15 @@ __global__ void __launch_bounds__(PEEL_BLOCK)
   }
   if (!grid_sync(&ctl->bar, nblocks, &ctl->err, limit_ns)) return;
 
+  // phase timers of block 0 (diagnostics only)
+  unsigned long long t_ts = 0, t_tr = 0, t_w = 0, mark = tid == 0 ? globaltimer_ns() : 0;
+  auto tick = [&](unsigned long long &acc) {
+    if (tid == 0) {
+      const unsigned long long now = globaltimer_ns();
+      acc += now - mark;
+      mark = now;
+    }
+  };
   int64_t todo = n;
   int32_t level = 0, degen = 0;
   uint32_t priority = 0, rounds = 0, levels = 0;
@@ -222,7 +263,10 @@ __global__ void __launch_bounds__(PEEL_BLOCK)
     }
     {
       uint32_t mymin = 0xFFFFFFFFu;
-      const int64_t lim = ((int64_t)nalive + 31) & ~(int64_t)31;
+      // block-strided so that every thread of a block runs the same number
+      // of iterations: appends are aggregated per block (one atomic each)
+      const int64_t bs = blockDim.x;
+      const int64_t lim = ((int64_t)nalive + bs - 1) / bs * bs;
       for (int64_t i = tid; i < lim; i += nthr) {
         int32_t v = 0, d = 0;
         bool live = false;
@@ -236,15 +280,16 @@ __global__ void __launch_bounds__(PEEL_BLOCK)
         if (inF) core[v] = level;
         const int32_t dv = inF ? rp[v + 1] - rp[v] : 0;
         const bool heavy = inF && dv > HEAVY_DEG;
-        warp_append(inF && !heavy, v, F, &ctl->fcnt[fo]);
+        block_append2(inF && !heavy, v, F, &ctl->fcnt[fo], keep, v, A2, &ctl->acnt[ao]);
         heavy_append(heavy, v, dv, F, hb[fo], (int64_t)n + 1, &ctl->hpack[fo]);
-        warp_append(keep, v, A2, &ctl->acnt[ao]);
         if (keep) mymin = min(mymin, (uint32_t)d);
       }
       mymin = __reduce_min_sync(MCE_FULL, mymin);
       if (lane == 0 && mymin != 0xFFFFFFFFu) atomicMin(&ctl->amin[ao], mymin);
     }
+    tick(t_ts);
     if (!grid_sync(&ctl->bar, nblocks, &ctl->err, limit_ns)) return;
+    tick(t_w);
     ++q;
     ++s;
     uint32_t cnt = frontier_size(ctl, q % 3);
@@ -268,7 +313,9 @@ __global__ void __launch_bounds__(PEEL_BLOCK)
       if (cnt <= solo_max) {
         // Small frontier: block 0 peels consecutive rounds alone.  The first
         // barrier lets every block read `cnt` before block 0 recycles slots.
+        tick(t_tr);
         if (!grid_sync(&ctl->bar, nblocks, &ctl->err, limit_ns)) return;
+        tick(t_w);
         if (blockIdx.x == 0) {
           uint32_t it = 0;
           for (;;) {
@@ -295,7 +342,9 @@ __global__ void __launch_bounds__(PEEL_BLOCK)
             ++ctl->solo_sections;
           }
         }
+        tick(t_tr);
         if (!grid_sync(&ctl->bar, nblocks, &ctl->err, limit_ns)) return;
+        tick(t_w);
         q = ld_volatile(&ctl->solo_q);
         cnt = ld_volatile(&ctl->solo_cnt);
         priority = ld_volatile(&ctl->solo_priority);
@@ -307,7 +356,9 @@ __global__ void __launch_bounds__(PEEL_BLOCK)
       }
       peel_round(q, level, priority, tid, nthr, (int64_t)n + 1, rp, col, deg, core, prio, fr, hb,
                  ctl);
+      tick(t_tr);
       if (!grid_sync(&ctl->bar, nblocks, &ctl->err, limit_ns)) return;
+      tick(t_w);
       ++q;
       cnt = frontier_size(ctl, q % 3);
       ++priority;
@@ -318,6 +369,9 @@ __global__ void __launch_bounds__(PEEL_BLOCK)
   }
   if (tid == 0) {
     ctl->degeneracy = degen;
+    ctl->t_scan = t_ts;
+    ctl->t_round = t_tr;
+    ctl->t_wait = t_w;
     ctl->rounds = rounds;
     ctl->levels = levels;
   }
@@ -354,7 +408,7 @@ int peel_launch(const PeelArgs &a, cudaStream_t s, int *launches) {
 }
 
 int peel_read(const void *ctl_dev, int32_t *degeneracy, uint32_t *err, uint32_t *rounds,
-              uint32_t *solo_sections, cudaStream_t s) {
+              uint32_t *solo_sections, cudaStream_t s, double *phase_ms) {
   PeelCtl h;
   MCE_CUDA(cudaMemcpyAsync(&h, ctl_dev, sizeof(PeelCtl), cudaMemcpyDeviceToHost, s));
   MCE_CUDA(cudaStreamSynchronize(s));
@@ -362,6 +416,11 @@ int peel_read(const void *ctl_dev, int32_t *degeneracy, uint32_t *err, uint32_t 
   if (err) *err = h.err;
   if (rounds) *rounds = h.rounds;
   if (solo_sections) *solo_sections = h.solo_sections;
+  if (phase_ms) {
+    phase_ms[0] = h.t_scan * 1e-6;
+    phase_ms[1] = h.t_round * 1e-6;
+    phase_ms[2] = h.t_wait * 1e-6;
+  }
   return MCE_OK;
 }
 

@@ -55,7 +55,8 @@ class _Stats(C.Structure):
                 ("roots", C.c_int64), ("tree_nodes", C.c_uint64), ("donations", C.c_uint64),
                 ("kernel_launches", C.c_int32), ("error_flags", C.c_uint32),
                 ("class_roots", C.c_int64 * 8), ("peel_rounds", C.c_int64),
-                ("peel_solo_sections", C.c_int64)]
+                ("peel_solo_sections", C.c_int64), ("peel_scan_ms", C.c_double),
+                ("peel_round_ms", C.c_double), ("peel_wait_ms", C.c_double)]
 
 
 class _HGraph(C.Structure):
