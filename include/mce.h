@@ -82,7 +82,9 @@ typedef struct mce_opts {
                                this many vertices are peeled by one block           */
   int32_t donate_after;     /* 0 = default (256): a warp shares subtrees of a
                                root only after walking this many of its nodes */
-  int32_t reserved[5];
+  int32_t cuda_graph;       /* 1 = capture the search launches in a CUDA graph
+                               once and replay it (default for batches)      */
+  int32_t reserved[4];
   void *stream;             /* cudaStream_t to queue work on; NULL = own      */
 } mce_opts_t;
 
@@ -212,6 +214,35 @@ int mce_root_log(mce_graph_t g, uint64_t *nodes_out);
 /* Per-root maximal-clique counts of the last mce_count that ran with
  * opts.log_roots = 1 (n entries, 0 for non-roots).                          */
 int mce_root_counts(mce_graph_t g, uint64_t *count_out);
+
+/* ---- batches of graphs ------------------------------------------------------ */
+typedef struct mce_batch *mce_batch_t;
+
+/* Upload many graphs at once (host pointers).  Graph g's CSR is
+ * row_ptr[vtx_offsets[g] .. vtx_offsets[g+1]) (n_g + 1 local offsets) and
+ * col[arc_offsets[g] .. arc_offsets[g+1]) (local ids) - the layout of a
+ * batch mce_hgraph_t.  On the device the graphs become one disjoint union
+ * with a vertex -> graph map, so one peel, one orientation and one search
+ * launch per engine class serve the whole batch.  No counterpart in the
+ * reference, which counts one graph per run (src/main.cu:18-187).          */
+int mce_batch_upload(const int32_t *row_ptr, const int32_t *col, const int64_t *vtx_offsets,
+                     const int64_t *arc_offsets, int32_t num_graphs, int32_t device,
+                     void *stream, mce_batch_t *out);
+
+/* Replace the graphs of a batch handle, reusing its device memory when the
+ * new batch fits.                                                           */
+int mce_batch_reload(mce_batch_t b, const int32_t *row_ptr, const int32_t *col,
+                     const int64_t *vtx_offsets, const int64_t *arc_offsets, int32_t num_graphs,
+                     void *stream);
+
+/* Count every graph of the batch: per_graph_total (num_graphs entries) gets
+ * each graph's maximal cliques, *total their sum, hist (nullable) the size
+ * histogram over the batch.  opts NULL = defaults with cuda_graph = 1: the
+ * search launches are captured once and replayed on later calls.           */
+int mce_batch_count(mce_batch_t b, const mce_opts_t *opts, uint64_t *per_graph_total,
+                    uint64_t *total, uint64_t *hist, mce_stats_t *stats);
+
+int mce_batch_free(mce_batch_t b);
 
 /* ---- allocation-free search ------------------------------------------------ */
 /* Bytes of the file-scope device array that mce_count_oriented_noalloc uses

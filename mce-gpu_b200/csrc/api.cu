@@ -66,6 +66,9 @@ struct mce_graph {
   ShapeInfo shape_h{};
   int32_t degeneracy = 0;
   cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  // search launches captured as a CUDA graph, replayed while the key matches
+  cudaGraphExec_t search_exec = nullptr;
+  unsigned char search_key[256] = {0};
 };
 
 namespace {
@@ -117,6 +120,14 @@ int alloc_fixed_bufs(mce_graph *g) {
 }
 
 cudaStream_t pick_stream(mce_graph *g, void *s) { return s ? (cudaStream_t)s : g->own; }
+
+// Per-graph counting of a batch handle.
+struct BatchCtx {
+  const int32_t *graph_of;             // device, n
+  unsigned long long *graph_count;     // device, G
+  uint64_t *per_graph_out;             // host, G
+  int64_t G;
+};
 
 int check_args(const int32_t *row_ptr, const int32_t *col, int64_t n, int64_t m) {
   if (n < 0 || m < 0 || (n > 0 && !row_ptr) || (m > 0 && !col)) return MCE_EINVAL;
@@ -211,6 +222,28 @@ int ensure_queue(mce_graph *g, int c, uint32_t words, QueueView *out) {
   return MCE_OK;
 }
 
+int graph_create(int32_t device, mce_graph **out) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return MCE_ENODEV;
+  if (device < 0 || device >= ndev) return MCE_EINVAL;
+  MCE_CUDA(cudaSetDevice(device));
+  mce_graph *g = new (std::nothrow) mce_graph();
+  if (!g) return MCE_ENOMEM;
+  g->device = device;
+  if (cudaDeviceGetAttribute(&g->sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&g->own, cudaStreamNonBlocking) != cudaSuccess) {
+    delete g;
+    return MCE_ECUDA;
+  }
+  int rc = alloc_fixed_bufs(g);
+  if (rc) {
+    mce_graph_free(g);
+    return rc;
+  }
+  *out = g;
+  return MCE_OK;
+}
+
 int ensure_slab(mce_graph *g, size_t bytes) {
   if (bytes <= g->slab_bytes) return MCE_OK;
   dfree(g->slab);
@@ -263,20 +296,9 @@ int mce_graph_upload(const int32_t *row_ptr, const int32_t *col, int64_t n, int6
   *out = nullptr;
   int rc = check_args(row_ptr, col, n, m);
   if (rc) return rc;
-  int ndev = 0;
-  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return MCE_ENODEV;
-  if (device < 0 || device >= ndev) return MCE_EINVAL;
-  MCE_CUDA(cudaSetDevice(device));
-  mce_graph *g = new (std::nothrow) mce_graph();
-  if (!g) return MCE_ENOMEM;
-  g->device = device;
-  if (cudaDeviceGetAttribute(&g->sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&g->own, cudaStreamNonBlocking) != cudaSuccess) {
-    delete g;
-    return MCE_ECUDA;
-  }
-  rc = alloc_fixed_bufs(g);
-  if (!rc) rc = upload_csr(g, row_ptr, col, n, m, pick_stream(g, stream));
+  mce_graph *g = nullptr;
+  if ((rc = graph_create(device, &g))) return rc;
+  rc = upload_csr(g, row_ptr, col, n, m, pick_stream(g, stream));
   if (!rc) {
     cudaError_t e = cudaStreamSynchronize(pick_stream(g, stream));
     if (e != cudaSuccess) rc = MCE_ECUDA;
@@ -312,6 +334,7 @@ int mce_graph_free(mce_graph_t g) {
   dfree(g->slab);
   dfree(g->sort_tmp);
   for (auto &q : g->qbuf) dfree(q);
+  if (g->search_exec) cudaGraphExecDestroy(g->search_exec);
   for (auto &e : g->ev)
     if (e) cudaEventDestroy(e);
   if (g->own) cudaStreamDestroy(g->own);
@@ -362,14 +385,14 @@ int mce_split_csr(mce_graph_t g, int32_t *split_out, int32_t *col_out) {
   return MCE_OK;
 }
 
-int mce_count(mce_graph_t g, const mce_opts_t *opts, uint64_t *total, uint64_t *hist,
-              mce_stats_t *stats) {
-  if (!g || !total) return MCE_EINVAL;
-  mce_opts_t o;
-  if (opts)
-    o = *opts;
-  else
-    mce_opts_default(&o);
+}  // extern "C"
+
+namespace {
+
+// The counting pipeline shared by mce_count and mce_batch_count.  With a
+// batch context, each root's count also goes to its graph's counter.
+int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *hist,
+               mce_stats_t *stats, const BatchCtx *bc) {
   if (o.bitmap_width != 0 && o.bitmap_width != 32 && o.bitmap_width != 64) return MCE_EINVAL;
   MCE_CUDA(cudaSetDevice(g->device));
   cudaStream_t s = pick_stream(g, o.stream);
@@ -405,18 +428,10 @@ int mce_count(mce_graph_t g, const mce_opts_t *opts, uint64_t *total, uint64_t *
     if (need > slab_need) slab_need = need;
   }
   if ((rc = ensure_slab(g, slab_need))) return rc;
-  if (o.log_roots) {
-    if (!g->root_nodes) {
-      if ((rc = dalloc(&g->root_nodes, (size_t)g->cap_n + 1))) return rc;
-      if ((rc = dalloc(&g->root_count, (size_t)g->cap_n + 1))) return rc;
-    }
-    MCE_CUDA(cudaMemsetAsync(g->root_nodes, 0, sizeof(unsigned long long) * (size_t)(g->n + 1), s));
-    MCE_CUDA(cudaMemsetAsync(g->root_count, 0, sizeof(unsigned long long) * (size_t)(g->n + 1), s));
+  if (o.log_roots && !g->root_nodes) {
+    if ((rc = dalloc(&g->root_nodes, (size_t)g->cap_n + 1))) return rc;
+    if ((rc = dalloc(&g->root_count, (size_t)g->cap_n + 1))) return rc;
   }
-  MCE_CUDA(cudaMemsetAsync(g->fetch, 0, sizeof(uint32_t) * 8, s));
-  MCE_CUDA(cudaMemsetAsync(g->err, 0, sizeof(uint32_t) * 4, s));
-  MCE_CUDA(cudaMemsetAsync(g->hist, 0, sizeof(unsigned long long) * MCE_HIST_MAX, s));
-  MCE_CUDA(cudaMemsetAsync(g->nodes, 0, sizeof(unsigned long long) * 4, s));
   BKArgs a;
   std::memset(&a, 0, sizeof(a));
   a.rp = g->rp;
@@ -429,6 +444,8 @@ int mce_count(mce_graph_t g, const mce_opts_t *opts, uint64_t *total, uint64_t *
   a.nodes = g->nodes;
   a.root_nodes = o.log_roots ? g->root_nodes : nullptr;
   a.root_count = o.log_roots ? g->root_count : nullptr;
+  a.graph_of = bc ? bc->graph_of : nullptr;
+  a.graph_count = bc ? bc->graph_count : nullptr;
   a.err = g->err;
   a.slab = g->slab;
   a.dcap = dcap;
@@ -437,17 +454,94 @@ int mce_count(mce_graph_t g, const mce_opts_t *opts, uint64_t *total, uint64_t *
   a.donate_after = o.donate_after > 0 ? (uint32_t)o.donate_after : DEFAULT_DONATE_AFTER;
   a.wait_limit_ns = IDLE_LIMIT_NS;
   const int wbits = o.bitmap_width == 64 ? 64 : 32;
-  // widest roots first so the long trees start early
-  const int order[3] = {CLS_MEM, CLS_R64, CLS_R32};
-  for (int c : order) {
-    if (!grid[c]) continue;
-    a.slab_words = bk_slab_words(c, dcap, xcap);
-    a.q = QueueView();
-    if (share) {
-      if ((rc = ensure_queue(g, c, bk_task_words(c, dcap), &a.q))) return rc;
-      if ((rc = queue_launch_init(a.q, s, &launches))) return rc;
+  QueueView qv[NCLS];
+  for (int c = CLS_R32; c <= CLS_MEM; ++c)
+    if (share && grid[c] && (rc = ensure_queue(g, c, bk_task_words(c, dcap), &qv[c]))) return rc;
+  // Everything from here to the end of the search is a fixed sequence of
+  // memsets and launches whose arguments depend only on `key`: with
+  // opts.cuda_graph it is captured once and replayed.
+  struct SearchKey {
+    int grid[NCLS], block[NCLS];
+    int dcap, xcap, wbits, share, dmin, log;
+    uint32_t dafter;
+    const void *slab, *graph_count, *graph_of, *root_nodes, *q[NCLS], *bufs[4];
+    int64_t n, G;
+  } key;
+  std::memset(&key, 0, sizeof(key));
+  for (int c = 0; c < NCLS; ++c) {
+    key.grid[c] = grid[c];
+    key.block[c] = block[c];
+    key.q[c] = qv[c].hdr;
+  }
+  key.dcap = dcap;
+  key.xcap = xcap;
+  key.wbits = wbits;
+  key.share = share;
+  key.dmin = a.donate_min;
+  key.dafter = a.donate_after;
+  key.log = o.log_roots != 0;
+  key.slab = g->slab;
+  key.graph_count = a.graph_count;
+  key.root_nodes = a.root_nodes;
+  key.graph_of = a.graph_of;
+  key.bufs[0] = g->rp;
+  key.bufs[1] = g->split;
+  key.bufs[2] = g->cs;
+  key.bufs[3] = g->roots;
+  key.n = g->n;
+  key.G = bc ? bc->G : 0;
+  static_assert(sizeof(SearchKey) <= sizeof(g->search_key), "search key");
+  auto record = [&]() -> int {
+    int r2;
+    if (o.log_roots) {
+      MCE_CUDA(cudaMemsetAsync(g->root_nodes, 0, sizeof(unsigned long long) * (size_t)(g->n + 1), s));
+      MCE_CUDA(cudaMemsetAsync(g->root_count, 0, sizeof(unsigned long long) * (size_t)(g->n + 1), s));
     }
-    if ((rc = bk_launch(c, wbits, a, grid[c], block[c], smem[c], s, &launches))) return rc;
+    if (bc) MCE_CUDA(cudaMemsetAsync(bc->graph_count, 0, sizeof(unsigned long long) * bc->G, s));
+    MCE_CUDA(cudaMemsetAsync(g->fetch, 0, sizeof(uint32_t) * 8, s));
+    MCE_CUDA(cudaMemsetAsync(g->err, 0, sizeof(uint32_t) * 4, s));
+    MCE_CUDA(cudaMemsetAsync(g->hist, 0, sizeof(unsigned long long) * MCE_HIST_MAX, s));
+    MCE_CUDA(cudaMemsetAsync(g->nodes, 0, sizeof(unsigned long long) * 4, s));
+    // widest roots first so the long trees start early
+    const int order[3] = {CLS_MEM, CLS_R64, CLS_R32};
+    for (int c : order) {
+      if (!grid[c]) continue;
+      a.slab_words = bk_slab_words(c, dcap, xcap);
+      a.q = share ? qv[c] : QueueView();
+      if (share && (r2 = queue_launch_init(a.q, s, &launches))) return r2;
+      if ((r2 = bk_launch(c, wbits, a, grid[c], block[c], smem[c], s, &launches))) return r2;
+    }
+    return MCE_OK;
+  };
+  if (o.cuda_graph) {
+    if (!g->search_exec || std::memcmp(g->search_key, &key, sizeof(key)) != 0) {
+      if (g->search_exec) {
+        cudaGraphExecDestroy(g->search_exec);
+        g->search_exec = nullptr;
+      }
+      cudaGraph_t graph = nullptr;
+      MCE_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      const int lc = launches;
+      rc = record();
+      cudaError_t e = cudaStreamEndCapture(s, &graph);
+      launches = lc;
+      if (rc) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+      }
+      if (e != cudaSuccess) return MCE_ECUDA;
+      e = cudaGraphInstantiate(&g->search_exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (e != cudaSuccess) {
+        g->search_exec = nullptr;
+        return MCE_ECUDA;
+      }
+      std::memcpy(g->search_key, &key, sizeof(key));
+    }
+    MCE_CUDA(cudaGraphLaunch(g->search_exec, s));
+    for (int c = CLS_R32; c <= CLS_MEM; ++c) launches += grid[c] ? (share ? 2 : 1) : 0;
+  } else {
+    if ((rc = record())) return rc;
   }
   MCE_CUDA(cudaEventRecord(g->ev[3], s));
   unsigned long long h_hist[MCE_HIST_MAX];
@@ -464,6 +558,8 @@ int mce_count(mce_graph_t g, const mce_opts_t *opts, uint64_t *total, uint64_t *
       qused[c] = true;
     }
   MCE_CUDA(cudaEventRecord(g->ev[4], s));
+  if (bc) MCE_CUDA(cudaMemcpyAsync(bc->per_graph_out, bc->graph_count,
+                                   sizeof(unsigned long long) * bc->G, cudaMemcpyDeviceToHost, s));
   MCE_CUDA(cudaStreamSynchronize(s));
   int32_t dg = 0;
   uint32_t perr = 0, rounds = 0, solo = 0;
@@ -509,6 +605,21 @@ int mce_count(mce_graph_t g, const mce_opts_t *opts, uint64_t *total, uint64_t *
   return MCE_OK;
 }
 
+}  // namespace
+
+extern "C" {
+
+int mce_count(mce_graph_t g, const mce_opts_t *opts, uint64_t *total, uint64_t *hist,
+              mce_stats_t *stats) {
+  if (!g || !total) return MCE_EINVAL;
+  mce_opts_t o;
+  if (opts)
+    o = *opts;
+  else
+    mce_opts_default(&o);
+  return count_impl(g, o, total, hist, stats, nullptr);
+}
+
 int mce_root_log(mce_graph_t g, uint64_t *nodes_out) {
   if (!g || !nodes_out) return MCE_EINVAL;
   if (!g->logged || !g->root_nodes) return MCE_ESTATE;
@@ -524,6 +635,148 @@ int mce_root_counts(mce_graph_t g, uint64_t *count_out) {
   MCE_CUDA(cudaSetDevice(g->device));
   MCE_CUDA(cudaMemcpy(count_out, g->root_count, sizeof(uint64_t) * (size_t)g->n,
                       cudaMemcpyDeviceToHost));
+  return MCE_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batches of graphs
+// ---------------------------------------------------------------------------
+struct mce_batch {
+  mce_graph *g = nullptr;  // the disjoint union, resident
+  int32_t G = 0;
+  int32_t *graph_of = nullptr;
+  unsigned long long *graph_count = nullptr;
+  int32_t *rp_local = nullptr, *col_local = nullptr;  // uploaded concatenations
+  int64_t *vtx_off = nullptr, *arc_off = nullptr;
+  int64_t cap_rows = -1, cap_m = -1, cap_g = -1;
+};
+
+namespace {
+
+int batch_check(const int32_t *row_ptr, const int32_t *col, const int64_t *vo, const int64_t *ao,
+                int32_t G, int64_t *n, int64_t *m) {
+  if (G < 1 || !row_ptr || !vo || !ao) return MCE_EINVAL;
+  if (vo[0] != 0 || ao[0] != 0) return MCE_EINVAL;
+  for (int32_t g = 0; g < G; ++g)
+    if (vo[g + 1] < vo[g] + 1 || ao[g + 1] < ao[g]) return MCE_EINVAL;
+  *n = vo[G] - G;
+  *m = ao[G];
+  if (*m > 0 && !col) return MCE_EINVAL;
+  if (*n >= ((int64_t)1 << 31) - 1 || *m >= ((int64_t)1 << 31)) return MCE_ELIMIT;
+  return MCE_OK;
+}
+
+void batch_free_bufs(mce_batch *b) {
+  dfree(b->graph_of);
+  dfree(b->graph_count);
+  dfree(b->rp_local);
+  dfree(b->col_local);
+  dfree(b->vtx_off);
+  dfree(b->arc_off);
+  b->cap_rows = b->cap_m = b->cap_g = -1;
+}
+
+int batch_load(mce_batch *b, const int32_t *row_ptr, const int32_t *col, const int64_t *vo,
+               const int64_t *ao, int32_t G, int64_t n, int64_t m, cudaStream_t s) {
+  mce_graph *g = b->g;
+  int rc;
+  if (n > g->cap_n || m > g->cap_m) {
+    if ((rc = alloc_graph_bufs(g, n, m))) return rc;
+  }
+  const int64_t rows = n + G;
+  if (rows > b->cap_rows || m > b->cap_m || G > b->cap_g) {
+    batch_free_bufs(b);
+    if ((rc = dalloc(&b->graph_of, (size_t)n + 1)) || (rc = dalloc(&b->graph_count, (size_t)G)) ||
+        (rc = dalloc(&b->rp_local, (size_t)rows)) || (rc = dalloc(&b->col_local, (size_t)m)) ||
+        (rc = dalloc(&b->vtx_off, (size_t)G + 1)) || (rc = dalloc(&b->arc_off, (size_t)G + 1)))
+      return rc;
+    b->cap_rows = rows;
+    b->cap_m = m;
+    b->cap_g = G;
+  }
+  b->G = G;
+  g->n = n;
+  g->m = m;
+  g->logged = false;
+  MCE_CUDA(cudaMemcpyAsync(b->rp_local, row_ptr, sizeof(int32_t) * (size_t)rows,
+                           cudaMemcpyHostToDevice, s));
+  if (m > 0)
+    MCE_CUDA(cudaMemcpyAsync(b->col_local, col, sizeof(int32_t) * (size_t)m,
+                             cudaMemcpyHostToDevice, s));
+  MCE_CUDA(cudaMemcpyAsync(b->vtx_off, vo, sizeof(int64_t) * (size_t)(G + 1),
+                           cudaMemcpyHostToDevice, s));
+  MCE_CUDA(cudaMemcpyAsync(b->arc_off, ao, sizeof(int64_t) * (size_t)(G + 1),
+                           cudaMemcpyHostToDevice, s));
+  return batch_rebase_launch(b->rp_local, b->col_local, b->vtx_off, b->arc_off, G, n, m, g->rp,
+                             g->col, b->graph_of, g->sms, s, nullptr);
+}
+
+}  // namespace
+
+extern "C" {
+
+int mce_batch_upload(const int32_t *row_ptr, const int32_t *col, const int64_t *vtx_offsets,
+                     const int64_t *arc_offsets, int32_t num_graphs, int32_t device,
+                     void *stream, mce_batch_t *out) {
+  if (!out) return MCE_EINVAL;
+  *out = nullptr;
+  int64_t n = 0, m = 0;
+  int rc = batch_check(row_ptr, col, vtx_offsets, arc_offsets, num_graphs, &n, &m);
+  if (rc) return rc;
+  mce_batch *b = new (std::nothrow) mce_batch();
+  if (!b) return MCE_ENOMEM;
+  if ((rc = graph_create(device, &b->g))) {
+    delete b;
+    return rc;
+  }
+  cudaStream_t s = pick_stream(b->g, stream);
+  rc = batch_load(b, row_ptr, col, vtx_offsets, arc_offsets, num_graphs, n, m, s);
+  if (!rc && cudaStreamSynchronize(s) != cudaSuccess) rc = MCE_ECUDA;
+  if (rc) {
+    mce_batch_free(b);
+    return rc;
+  }
+  *out = b;
+  return MCE_OK;
+}
+
+int mce_batch_reload(mce_batch_t b, const int32_t *row_ptr, const int32_t *col,
+                     const int64_t *vtx_offsets, const int64_t *arc_offsets, int32_t num_graphs,
+                     void *stream) {
+  if (!b) return MCE_EINVAL;
+  int64_t n = 0, m = 0;
+  int rc = batch_check(row_ptr, col, vtx_offsets, arc_offsets, num_graphs, &n, &m);
+  if (rc) return rc;
+  MCE_CUDA(cudaSetDevice(b->g->device));
+  return batch_load(b, row_ptr, col, vtx_offsets, arc_offsets, num_graphs, n, m,
+                    pick_stream(b->g, stream));
+}
+
+int mce_batch_count(mce_batch_t b, const mce_opts_t *opts, uint64_t *per_graph_total,
+                    uint64_t *total, uint64_t *hist, mce_stats_t *stats) {
+  if (!b || !total || !per_graph_total) return MCE_EINVAL;
+  mce_opts_t o;
+  if (opts)
+    o = *opts;
+  else {
+    mce_opts_default(&o);
+    o.cuda_graph = 1;
+  }
+  BatchCtx bc{b->graph_of, b->graph_count, per_graph_total, b->G};
+  return count_impl(b->g, o, total, hist, stats, &bc);
+}
+
+int mce_batch_free(mce_batch_t b) {
+  if (!b) return MCE_OK;
+  if (b->g) {
+    cudaSetDevice(b->g->device);
+    cudaStreamSynchronize(b->g->own);
+  }
+  batch_free_bufs(b);
+  if (b->g) mce_graph_free(b->g);
+  delete b;
   return MCE_OK;
 }
 

@@ -93,6 +93,12 @@ int bk_warps_for_class(int cls, int sms, int *warps, int *block, int *smem);
 size_t bk_slab_words(int cls, int dcap, int xcap);
 uint32_t bk_task_words(int cls, int dcap);
 int queue_launch_init(const QueueView &q, cudaStream_t s, int *launches);
+
+// ---- batches ------------------------------------------------------------------
+int batch_rebase_launch(const int32_t *rp_local, const int32_t *col_local,
+                        const int64_t *vtx_off, const int64_t *arc_off, int32_t G, int64_t n,
+                        int64_t m, int32_t *rp, int32_t *col, int32_t *graph_of, int sms,
+                        cudaStream_t s, int *launches);
 int bk_launch(int cls, int word_bits, const BKArgs &a, int grid, int block, int smem,
               cudaStream_t s, int *launches);
 

@@ -44,7 +44,7 @@ class _Opts(C.Structure):
                 ("warps_per_root", C.c_int32), ("donate_threshold", C.c_int32),
                 ("log_roots", C.c_int32), ("x_pivot", C.c_int32),
                 ("peel_solo_max", C.c_int32), ("donate_after", C.c_int32),
-                ("reserved", C.c_int32 * 5),
+                ("cuda_graph", C.c_int32), ("reserved", C.c_int32 * 4),
                 ("stream", C.c_void_p)]
 
 
@@ -85,6 +85,10 @@ _sigs = {
     "mce_root_log": (C.c_int, [_P, _P]),
     "mce_root_counts": (C.c_int, [_P, _P]),
     "mce_count_oriented_noalloc": (C.c_int, [_P, _P, _P, _P, C.c_int64, _P, _P]),
+    "mce_batch_upload": (C.c_int, [_P, _P, _P, _P, C.c_int32, C.c_int32, _P, _P]),
+    "mce_batch_reload": (C.c_int, [_P, _P, _P, _P, _P, C.c_int32, _P]),
+    "mce_batch_count": (C.c_int, [_P, _P, _P, _P, _P, _P]),
+    "mce_batch_free": (C.c_int, [_P]),
     "mce_gen_er": (C.c_int, [C.c_int64, C.c_double, C.c_uint64, C.c_int32, C.c_int32,
                              C.c_int32, _P]),
     "mce_gen_rmat": (C.c_int, [C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,
@@ -280,6 +284,19 @@ def _stats_dict(st: _Stats) -> dict:
     return d
 
 
+def make_opts(*, sched=SCHED_PLAIN, bitmap_width=0, log_roots=False, level=LEVEL_L1,
+              induced=INDUCED_P, worker_list=WL_ON, donate_threshold=0, x_pivot=0,
+              peel_solo_max=0, donate_after=0, cuda_graph=0, stream=None) -> _Opts:
+    o = _Opts()
+    _lib.mce_opts_default(C.byref(o))
+    o.sched, o.bitmap_width, o.log_roots = sched, bitmap_width, int(bool(log_roots))
+    o.level, o.induced, o.worker_list = level, induced, worker_list
+    o.donate_threshold, o.x_pivot = donate_threshold, x_pivot
+    o.peel_solo_max, o.donate_after, o.cuda_graph = peel_solo_max, donate_after, cuda_graph
+    o.stream = stream
+    return o
+
+
 class Graph:
     """A graph resident on one GPU (wraps mce_graph_t)."""
 
@@ -319,16 +336,8 @@ class Graph:
     def __exit__(self, *a):
         self.close()
 
-    def count(self, *, sched=SCHED_PLAIN, bitmap_width=0, log_roots=False, level=LEVEL_L1,
-              induced=INDUCED_P, worker_list=WL_ON, donate_threshold=0, x_pivot=0,
-              peel_solo_max=0, donate_after=0, stream=None) -> CountResult:
-        o = _Opts()
-        _lib.mce_opts_default(C.byref(o))
-        o.sched, o.bitmap_width, o.log_roots = sched, bitmap_width, int(bool(log_roots))
-        o.level, o.induced, o.worker_list = level, induced, worker_list
-        o.donate_threshold, o.x_pivot = donate_threshold, x_pivot
-        o.peel_solo_max, o.donate_after = peel_solo_max, donate_after
-        o.stream = stream
+    def count(self, *, stream=None, **opts) -> CountResult:
+        o = make_opts(stream=stream, **opts)
         total = C.c_uint64()
         hist = np.zeros(HIST_MAX, np.uint64)
         st = _Stats()
@@ -358,3 +367,65 @@ class Graph:
         out = np.zeros(max(self.n, 1), np.uint64)
         _check(_lib.mce_root_counts(self._h, _ptr(out)), "root_counts")
         return out[:self.n]
+
+
+@dataclass
+class BatchResult:
+    total: int
+    per_graph: np.ndarray
+    hist: np.ndarray
+    stats: dict
+
+
+class Batch:
+    """Many graphs resident on one GPU as one disjoint union (wraps mce_batch_t)."""
+
+    def __init__(self, hg: HostGraph, device: int = 0, stream=None):
+        self._h = C.c_void_p()
+        self._keep = self._arrays(hg)
+        rp, col, vo, ao = self._keep
+        self.num_graphs = hg.num_graphs
+        _check(_lib.mce_batch_upload(_ptr(rp), _ptr(col), _ptr(vo), _ptr(ao), hg.num_graphs,
+                                     device, stream, C.byref(self._h)), "batch_upload")
+
+    @staticmethod
+    def _arrays(hg: HostGraph):
+        vo = hg.vtx_offsets if hg.vtx_offsets is not None else np.array([0, hg.n + 1], np.int64)
+        ao = hg.arc_offsets if hg.arc_offsets is not None else np.array([0, hg.m], np.int64)
+        return (np.ascontiguousarray(hg.row_ptr, dtype=np.int32),
+                np.ascontiguousarray(hg.col, dtype=np.int32),
+                np.ascontiguousarray(vo, dtype=np.int64), np.ascontiguousarray(ao, dtype=np.int64))
+
+    def reload_ptr(self, rp_addr, col_addr, vo_addr, ao_addr, num_graphs, stream=None) -> None:
+        """Re-upload from raw host addresses (e.g. pinned buffers)."""
+        _check(_lib.mce_batch_reload(self._h, C.c_void_p(rp_addr), C.c_void_p(col_addr),
+                                     C.c_void_p(vo_addr), C.c_void_p(ao_addr), num_graphs,
+                                     stream), "batch_reload")
+        self.num_graphs = num_graphs
+
+    def count(self, *, stream=None, cuda_graph=1, **opts) -> BatchResult:
+        o = make_opts(stream=stream, cuda_graph=cuda_graph, **opts)
+        per = np.zeros(self.num_graphs, np.uint64)
+        total = C.c_uint64()
+        hist = np.zeros(HIST_MAX, np.uint64)
+        st = _Stats()
+        _check(_lib.mce_batch_count(self._h, C.byref(o), _ptr(per), C.byref(total), _ptr(hist),
+                                    C.byref(st)), "batch_count")
+        return BatchResult(int(total.value), per, hist, _stats_dict(st))
+
+    def close(self) -> None:
+        if self._h:
+            _lib.mce_batch_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

@@ -1,0 +1,60 @@
+"""Batched counting (mce_batch_*): per-graph counts against the oracle."""
+import numpy as np
+import pytest
+
+import mce_b200 as mce
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def per_graph_oracle(b):
+    return np.array([oracle.count(b.graph(i))[0] for i in range(b.num_graphs)], np.uint64)
+
+
+def test_batch_per_graph_counts_exact():
+    b = mce.gen_chung_lu_batch(96, 64, 4096, 2.3, 8, 32, 5, 5, 40, 11)
+    want = per_graph_oracle(b)
+    _, h_union, _ = oracle.count(mce.union(b))
+    with mce.Batch(b) as db:
+        r = db.count()
+        r2 = db.count()  # replay of the captured search launches
+    assert np.array_equal(r.per_graph, want)
+    assert r.total == int(want.sum()) and np.array_equal(r.hist, h_union)
+    assert np.array_equal(r2.per_graph, want) and np.array_equal(r2.hist, r.hist)
+
+
+def test_batch_graph_mode_and_plain_mode_agree():
+    b = mce.gen_chung_lu_batch(40, 64, 2048, 2.3, 8, 32, 5, 5, 40, 7)
+    with mce.Batch(b) as db:
+        a = db.count(cuda_graph=1)
+        p = db.count(cuda_graph=0)
+        w = db.count(cuda_graph=1, worker_list=mce.WL_OFF)
+    assert np.array_equal(a.per_graph, p.per_graph) and np.array_equal(a.per_graph, w.per_graph)
+
+
+def test_batch_reload_smaller_and_larger():
+    b1 = mce.gen_chung_lu_batch(32, 64, 2048, 2.3, 8, 32, 5, 5, 40, 1)
+    b2 = mce.gen_chung_lu_batch(8, 64, 1024, 2.3, 8, 32, 5, 5, 40, 2)
+    b3 = mce.gen_chung_lu_batch(64, 64, 4096, 2.3, 8, 32, 5, 5, 40, 3)
+    with mce.Batch(b1) as db:
+        assert np.array_equal(db.count().per_graph, per_graph_oracle(b1))
+        for b in (b2, b3, b1):
+            rp, col, vo, ao = mce.Batch._arrays(b)
+            db.reload_ptr(rp.ctypes.data, col.ctypes.data, vo.ctypes.data, ao.ctypes.data,
+                          b.num_graphs)
+            assert np.array_equal(db.count().per_graph, per_graph_oracle(b))
+
+
+def test_batch_with_empty_and_tiny_graphs():
+    graphs = [mce.from_edges(np.array([], np.int64), np.array([], np.int64), 5),   # no edges
+              mce.from_edges(np.array([0]), np.array([1]), 2),                       # one edge
+              mce.gen_er(50, 0.2, 4)]
+    rp = np.concatenate([g.row_ptr[:g.n + 1] for g in graphs]).astype(np.int32)
+    col = np.concatenate([g.col for g in graphs]).astype(np.int32)
+    vo = np.cumsum([0] + [g.n + 1 for g in graphs]).astype(np.int64)
+    ao = np.cumsum([0] + [g.m for g in graphs]).astype(np.int64)
+    hb = mce.HostGraph(rp, col, int(sum(g.n for g in graphs)), int(col.size), 3, vo, ao)
+    with mce.Batch(hb) as db:
+        r = db.count()
+    assert list(r.per_graph) == [0, 1, oracle.count(graphs[2])[0]]
