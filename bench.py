@@ -64,7 +64,9 @@ def make_workload(args):
         g = mce.union(b)
         cfg = {"workload": f"chung-lu batch: {args.graphs} graphs, n log-uniform [64,16384], "
                            "gamma 2.3, mean degree U[8,32], 0-5 planted cliques U[5,40], seed 11",
-               "graphs": args.graphs}
+               "graphs": args.graphs, "path": "mce_batch_count (one union, captured search)"}
+        cfg.update({"n": int(g.n), "arcs": int(g.m)})
+        return g, cfg, b
     elif args.workload == "rmat":
         g = mce.gen_rmat(args.scale, 16, 0.57, 0.19, 0.19, 7)
         cfg = {"workload": f"R-MAT scale {args.scale}, edge factor 16, (0.57,0.19,0.19,0.05), seed 7"}
@@ -74,8 +76,28 @@ def make_workload(args):
     else:
         g = mce.gen_er(10000, 0.002, 1, 20, 6, 12)
         cfg = {"workload": "Erdos-Renyi G(10000,0.002) seed 1 + 20 planted cliques U[6,12]"}
-    cfg.update({"n": int(g.n), "arcs": int(g.m)})
-    return g, cfg
+    cfg.update({"n": int(g.n), "arcs": int(g.m), "path": "mce_count"})
+    return g, cfg, None
+
+
+def plain_per_graph(hb, graphs, stream, kw):
+    """The plain path for a batch: each graph its own mce_count call."""
+    import torch
+    import mce_b200 as mce
+    tot, ms = 0, 0.0
+    for i in range(min(graphs, hb.num_graphs)):
+        with mce.Graph.from_host(hb.graph(i), stream=stream.cuda_stream) as dg:
+            dg.count(stream=stream.cuda_stream, **kw)  # warm
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            r = dg.count(stream=stream.cuda_stream, **kw)
+            e1.record(stream)
+            e1.synchronize()
+            tot += r.total
+            ms += e0.elapsed_time(e1)
+    return {"graphs": min(graphs, hb.num_graphs), "maximal_cliques": tot, "ms": round(ms, 3),
+            "value": tot / (ms / 1e3) if ms > 0 else None}
 
 
 class ClockSampler:
@@ -189,16 +211,21 @@ def run_mine(args, rank, world, local_rank):
     kw = dict(worker_list=mce.WL_ON if args.wl == "on" else mce.WL_OFF,
               donate_threshold=args.donate, peel_solo_max=args.solo, donate_after=args.after)
     torch.cuda.set_device(local_rank)
-    g, cfg = make_workload(args)
+    g, cfg, hb = make_workload(args)
     stream = torch.cuda.Stream()
     sptr = stream.cuda_stream
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
-    dg = mce.Graph.from_host(g, device=local_rank, stream=sptr)
+    with mce.Graph.from_host(g, device=local_rank, stream=sptr) as ug:
+        split, _ = ug.split_csr()  # for the algorithmic-byte count only
+    if hb is not None:
+        dg = mce.Batch(hb, device=local_rank, stream=sptr)
+        kw = dict(kw, cuda_graph=1)
+    else:
+        dg = mce.Graph.from_host(g, device=local_rank, stream=sptr)
     torch.cuda.synchronize()
     res = None
     for _ in range(args.warmup):
         res = dg.count(stream=sptr, **kw)
-    split, _ = dg.split_csr()
     total = res.total if res else dg.count(stream=sptr, **kw).total
 
     def barrier():
@@ -225,8 +252,18 @@ def run_mine(args, rank, world, local_rank):
         barrier()
     step_ms = sum(times) / len(times)
     # ---- end to end: pinned host CSR -> device -> count -> host, per step
-    rp_h = torch.from_numpy(np.ascontiguousarray(g.row_ptr[:g.n + 1])).pin_memory()
-    col_h = torch.from_numpy(np.ascontiguousarray(g.col)).pin_memory()
+    if hb is not None:
+        rp_h, col_h, vo_h, ao_h = (torch.from_numpy(x).pin_memory() for x in mce.Batch._arrays(hb))
+        h2d = sum(x.numel() * x.element_size() for x in (rp_h, col_h, vo_h, ao_h))
+        reload = lambda: dg.reload_ptr(rp_h.data_ptr(), col_h.data_ptr(), vo_h.data_ptr(),
+                                       ao_h.data_ptr(), hb.num_graphs, stream=sptr)
+        d2h = 8 * hb.num_graphs
+    else:
+        rp_h = torch.from_numpy(np.ascontiguousarray(g.row_ptr[:g.n + 1])).pin_memory()
+        col_h = torch.from_numpy(np.ascontiguousarray(g.col)).pin_memory()
+        h2d = 4 * (g.n + 1) + 4 * g.m
+        reload = lambda: dg.reload_ptr(rp_h.data_ptr(), col_h.data_ptr(), g.n, g.m, stream=sptr)
+        d2h = 0
     e2e_times = []
     barrier()
     for _ in range(args.steps):
@@ -235,7 +272,7 @@ def run_mine(args, rank, world, local_rank):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        dg.reload_ptr(rp_h.data_ptr(), col_h.data_ptr(), g.n, g.m, stream=sptr)
+        reload()
         r = dg.count(stream=sptr, **kw)
         e1.record(stream)
         e1.synchronize()
@@ -290,8 +327,8 @@ def run_mine(args, rank, world, local_rank):
                        worker_list=args.wl, donate=args.donate, solo=args.solo,
                        donate_after=args.after),
         "e2e": {"value": world * total / (e2e_ms / 1e3), "unit": "maximal cliques/s",
-                "h2d_bytes_per_step": int(4 * (g.n + 1) + 4 * g.m),
-                "d2h_bytes_per_step": int(8 * 4096 + 64 + 8 + 4 + 128),
+                "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h + 8 * 4096 + 64 + 8 + 4 + 128),
                 "ms_per_step": e2e_ms},
         "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved,
@@ -300,6 +337,9 @@ def run_mine(args, rank, world, local_rank):
                      "algorithmic_bytes": ab[dom], "peak_source": peak_kind},
         "clocks": clocks,
     }
+    if hb is not None:
+        kw_plain = {k: v for k, v in kw.items() if k != "cuda_graph"}
+        line["config"]["plain_per_graph"] = plain_per_graph(hb, 256, stream, kw_plain)
     if not args.no_cpu_baseline and world == 1:
         try:
             line["cpu_baseline"] = cpu_baseline(g)
@@ -330,7 +370,7 @@ def run_reference(args, rank, world):
         _, cfg = g, {"workload": f"chung-lu batch, first {sample_graphs} of {args.graphs} graphs "
                                  "(seed 11) as one disjoint union"}
     else:
-        g, cfg = make_workload(args)
+        g, cfg, _ = make_workload(args)
     cfg.update({"n": int(g.n), "arcs": int(g.m)})
     tmp = tempfile.mkdtemp(prefix="mce_ref_")
     bel = os.path.join(tmp, "g.bel")
