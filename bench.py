@@ -53,6 +53,9 @@ def parse_args():
     p.add_argument("--donate", type=int, default=0, help="donation threshold (0: default)")
     p.add_argument("--solo", type=int, default=0, help="peel solo frontier size (0: default)")
     p.add_argument("--after", type=int, default=0, help="donate after N nodes (0: default)")
+    p.add_argument("--sched", choices=["plain", "degree", "learned"], default="learned",
+                   help="root order (learned: the shipped cost model of the workload family)")
+    p.add_argument("--no-compare", action="store_true", help="skip the other schedules")
     return p.parse_args()
 
 
@@ -210,6 +213,15 @@ def run_mine(args, rank, world, local_rank):
     import mce_b200 as mce
     kw = dict(worker_list=mce.WL_ON if args.wl == "on" else mce.WL_OFF,
               donate_threshold=args.donate, peel_solo_max=args.solo, donate_after=args.after)
+    scheds = {"plain": dict(sched=mce.SCHED_PLAIN), "degree": dict(sched=mce.SCHED_DEGREE)}
+    wpath = os.path.join(ROOT, "mce-gpu_b200", "data", f"cost_mlp_{args.workload}.f32")
+    model = None
+    if os.path.exists(wpath):
+        model = mce.Model(device=local_rank)
+        model.load(wpath)
+        scheds["learned"] = dict(sched=mce.SCHED_LEARNED, model=model)
+    sched_used = args.sched if args.sched in scheds else "degree"
+    kw.update(scheds[sched_used])
     torch.cuda.set_device(local_rank)
     g, cfg, hb = make_workload(args)
     stream = torch.cuda.Stream()
@@ -315,7 +327,7 @@ def run_mine(args, rank, world, local_rank):
         "dtype": "u32", "data": "synthetic (seeded generators; no datasets)",
         "config": dict(cfg, maximal_cliques=total, parallelism=f"replicas x{world}",
                        l2="flushed between steps (256 MiB write) and inputs larger than L2",
-                       sched="plain", phases_ms={k: round(v, 3) for k, v in phases.items()},
+                       sched=sched_used, phases_ms={k: round(v, 3) for k, v in phases.items()},
                        tree_nodes=stats[-1]["tree_nodes"], degeneracy=stats[-1]["degeneracy"],
                        max_later_degree=stats[-1]["max_later_degree"],
                        class_roots=stats[-1]["class_roots"][:3],
@@ -337,8 +349,32 @@ def run_mine(args, rank, world, local_rank):
                      "algorithmic_bytes": ab[dom], "peak_source": peak_kind},
         "clocks": clocks,
     }
+    if not args.no_compare:  # the other root orders on the same resident graph
+        cmp = {}
+        for name, extra in scheds.items():
+            if name == sched_used:
+                continue
+            kk = dict(kw, **extra)
+            if name != "learned":
+                kk.pop("model", None)
+            dg.count(stream=sptr, **kk)
+            ts = []
+            for _ in range(max(2, args.steps // 2)):
+                flush.zero_()
+                torch.cuda.synchronize()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                r = dg.count(stream=sptr, **kk)
+                e1.record(stream)
+                e1.synchronize()
+                assert r.total == total, f"{name} schedule changed the count"
+                ts.append(e0.elapsed_time(e1))
+            ms = sum(ts) / len(ts)
+            cmp[name] = {"ms_per_step": round(ms, 3), "value": total / (ms / 1e3)}
+        line["config"]["other_schedules"] = cmp
     if hb is not None:
-        kw_plain = {k: v for k, v in kw.items() if k != "cuda_graph"}
+        kw_plain = {k: v for k, v in kw.items() if k not in ("cuda_graph", "model", "sched")}
         line["config"]["plain_per_graph"] = plain_per_graph(hb, 256, stream, kw_plain)
     if not args.no_cpu_baseline and world == 1:
         try:

@@ -86,6 +86,8 @@ typedef struct mce_opts {
                                once and replay it (default for batches)      */
   int32_t reserved[4];
   void *stream;             /* cudaStream_t to queue work on; NULL = own      */
+  void *model;              /* mce_model_t for MCE_SCHED_LEARNED (NULL: the
+                               degree heuristic is used instead)              */
 } mce_opts_t;
 
 /* Fill *o with the defaults: L1, P, worker list on, plain schedule, auto.   */
@@ -243,6 +245,49 @@ int mce_batch_count(mce_batch_t b, const mce_opts_t *opts, uint64_t *per_graph_t
                     uint64_t *total, uint64_t *hist, mce_stats_t *stats);
 
 int mce_batch_free(mce_batch_t b);
+
+/* ---- learned scheduling ------------------------------------------------------ */
+/* A cost model predicts each root's search-tree size (log2(1 + nodes)) from
+ * eight features (later / earlier / total degree, core number, density and
+ * largest degree of the subgraph induced by the later neighbours, first-level
+ * branches left by that degree, later-list mass).  Network 8 -> 64 -> 64 -> 1
+ * with ReLU, FP16 weights and FP32 accumulation; trained on the device by
+ * this library's own forward/backward/Adam kernels on the tree sizes that
+ * mce_count logs (opts.log_roots = 1).  With opts.sched = MCE_SCHED_LEARNED
+ * and opts.model set, roots run longest-predicted first and only roots
+ * predicted large share subtrees.  The count never depends on the model.
+ * No counterpart in the reference, whose only static choice is per graph
+ * (table.py:127).                                                           */
+#define MCE_MLP_INPUTS 8
+#define MCE_MLP_HIDDEN 64
+#define MCE_MLP_PARAMS 4801  /* W1 64x8, b1 64, W2 64x64, b2 64, W3 64, b3 1 */
+typedef struct mce_model *mce_model_t;
+
+/* A model with seeded He-uniform weights and zero biases. */
+int mce_model_create(int32_t device, uint64_t seed, mce_model_t *out);
+int mce_model_free(mce_model_t m);
+/* Set the FP32 master weights (MCE_MLP_PARAMS, layout above); the FP16
+ * copy used by the kernels is their round-to-nearest.                      */
+int mce_model_set(mce_model_t m, const float *params);
+/* Read the FP32 master weights and/or the FP16 copy (either nullable).     */
+int mce_model_get(mce_model_t m, float *params_out, uint16_t *fp16_out);
+/* Features of every vertex (n x MCE_MLP_INPUTS, zeros for non-roots). */
+int mce_root_features(mce_graph_t g, float *features_out);
+/* Train on the roots of g against the tree sizes of the last mce_count that
+ * ran with log_roots = 1 (MCE_ESTATE otherwise): `epochs` passes of Adam
+ * over seeded shuffles in minibatches of `batch`; loss_out (nullable,
+ * `epochs` entries) gets each epoch's mean squared error.                  */
+int mce_model_train(mce_model_t m, mce_graph_t g, int32_t epochs, int32_t batch, float lr,
+                    uint64_t seed, float *loss_out);
+/* Predicted log2(1 + tree nodes) of every vertex of g (n entries). */
+int mce_model_predict(mce_model_t m, mce_graph_t g, float *pred_out);
+/* Forward pass on host features (count x MCE_MLP_INPUTS). */
+int mce_model_eval(mce_model_t m, const float *X, int64_t count, float *out);
+/* Gradient of the mean squared error over (X, Y) (host arrays) with respect
+ * to the parameters, as the training kernel computes it (FP16 weights, FP32
+ * accumulation); the model is not updated.                                  */
+int mce_model_grad(mce_model_t m, const float *X, const float *Y, int64_t count,
+                   float *grad_out, float *loss_out);
 
 /* ---- allocation-free search ------------------------------------------------ */
 /* Bytes of the file-scope device array that mce_count_oriented_noalloc uses

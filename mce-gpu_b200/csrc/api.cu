@@ -4,6 +4,13 @@
 #include <cstring>
 #include <new>
 
+#include <cuda_fp16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "../host/host.h"
 #include "common.cuh"
 #include "kernels.h"
 
@@ -57,6 +64,8 @@ struct mce_graph {
   uint32_t *fetch = nullptr, *err = nullptr;
   unsigned long long *hist = nullptr, *nodes = nullptr;
   unsigned long long *root_nodes = nullptr, *root_count = nullptr;
+  float *feat = nullptr, *pred = nullptr;  // per-vertex features (n x 8) and predicted cost
+  uint8_t *policy = nullptr;              // per-root sharing policy from the model
   unsigned long long *slab = nullptr;
   size_t slab_bytes = 0;
   void *qbuf[NCLS] = {nullptr};   // task queue per engine class
@@ -87,6 +96,7 @@ void free_graph_bufs(mce_graph *g) {
   dfree(g->hb0); dfree(g->hb1); dfree(g->hb2);
   dfree(g->keys_in); dfree(g->keys_out); dfree(g->vals_in); dfree(g->roots);
   dfree(g->root_nodes); dfree(g->root_count);
+  dfree(g->feat); dfree(g->pred); dfree(g->policy);
   g->cap_n = g->cap_m = -1;
 }
 
@@ -178,7 +188,12 @@ int run_peel(mce_graph *g, cudaStream_t s, int *launches, int solo_opt = 0) {
 }
 
 // Stage 2: orient + classify + sort roots (keys plain: class only).
-int run_orient(mce_graph *g, cudaStream_t s, int *launches) {
+int run_sort(mce_graph *g, int end_bit, cudaStream_t s, int *launches) {
+  return roots_sort(g->n, g->keys_in, g->keys_out, g->vals_in, g->roots, end_bit, &g->sort_tmp,
+                    &g->sort_tmp_bytes, g->shape, s, launches);
+}
+
+int run_orient(mce_graph *g, cudaStream_t s, int *launches, bool skip_sort = false) {
   OrientArgs oa;
   oa.n = g->n;
   oa.rp = g->rp;
@@ -193,8 +208,7 @@ int run_orient(mce_graph *g, cudaStream_t s, int *launches) {
   oa.sched = MCE_SCHED_PLAIN;
   int rc = orient_launch(oa, s, launches);
   if (rc) return rc;
-  return roots_sort(g->n, g->keys_in, g->keys_out, g->vals_in, g->roots, 3, &g->sort_tmp,
-                    &g->sort_tmp_bytes, g->shape, s, launches);
+  return skip_sort ? MCE_OK : run_sort(g, 3, s, launches);  // keys: class only
 }
 
 int read_shape(mce_graph *g, cudaStream_t s) {
@@ -389,6 +403,36 @@ int mce_split_csr(mce_graph_t g, int32_t *split_out, int32_t *col_out) {
 
 namespace {
 
+}  // namespace
+
+struct mce_model {
+  int device = 0;
+  int sms = 0;
+  cudaStream_t own = nullptr;
+  float *master = nullptr, *grad = nullptr, *m1 = nullptr, *m2 = nullptr, *loss = nullptr;
+  __half *wh = nullptr;
+  int step = 0;
+};
+
+namespace {
+
+constexpr float HEAVY_COST = 10.0f;  // predicted log2(tree nodes): roots above it share at once
+
+int ensure_feat(mce_graph *g) {
+  int rc;
+  if (!g->feat && (rc = dalloc(&g->feat, (size_t)(g->cap_n + 1) * MLP_IN))) return rc;
+  if (!g->pred && (rc = dalloc(&g->pred, (size_t)g->cap_n + 1))) return rc;
+  if (!g->policy && (rc = dalloc(&g->policy, (size_t)g->cap_n + 1))) return rc;
+  return MCE_OK;
+}
+
+// Features of every vertex of the (peeled, oriented) graph into g->feat.
+int compute_features(mce_graph *g, cudaStream_t s, int *launches) {
+  int rc = ensure_feat(g);
+  if (rc) return rc;
+  return features_launch(g->n, g->rp, g->split, g->cs, g->core, g->feat, g->sms, s, launches);
+}
+
 // The counting pipeline shared by mce_count and mce_batch_count.  With a
 // batch context, each root's count also goes to its graph's counter.
 int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *hist,
@@ -402,7 +446,29 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   MCE_CUDA(cudaEventRecord(g->ev[0], s));
   if ((rc = run_peel(g, s, &launches, o.peel_solo_max))) return rc;
   MCE_CUDA(cudaEventRecord(g->ev[1], s));
-  if ((rc = run_orient(g, s, &launches))) return rc;
+  // Root order: plain = vertex id within each engine class; degree = a
+  // degree-based cost; learned = the model's predicted tree size.  Larger
+  // costs first; the learned order also sets which roots share subtrees.
+  const mce_model *model = (const mce_model *)o.model;
+  const int sched = o.sched == MCE_SCHED_LEARNED && !model ? MCE_SCHED_DEGREE : o.sched;
+  if ((rc = run_orient(g, s, &launches, sched != MCE_SCHED_PLAIN))) return rc;
+  const uint8_t *policy = nullptr;
+  if (sched == MCE_SCHED_DEGREE && g->n > 0) {
+    if ((rc = rekey_launch(g->n, g->keys_in, nullptr, g->rp, g->split, nullptr, 0.f, g->sms, s,
+                           &launches)) ||
+        (rc = run_sort(g, 32, s, &launches)))
+      return rc;
+  } else if (sched == MCE_SCHED_LEARNED && g->n > 0) {
+    if (model->device != g->device) return MCE_EINVAL;
+    if ((rc = compute_features(g, s, &launches)) ||
+        (rc = mlp_forward_launch(model->wh, g->feat, nullptr, g->n, g->pred, g->sms, s,
+                                 &launches)) ||
+        (rc = rekey_launch(g->n, g->keys_in, g->pred, g->rp, g->split, g->policy, HEAVY_COST,
+                           g->sms, s, &launches)) ||
+        (rc = run_sort(g, 32, s, &launches)))
+      return rc;
+    policy = g->policy;
+  }
   MCE_CUDA(cudaEventRecord(g->ev[2], s));
   if ((rc = read_shape(g, s))) return rc;
   const ShapeInfo &sh = g->shape_h;
@@ -453,6 +519,7 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   a.donate_min = o.donate_threshold > 0 ? o.donate_threshold : DEFAULT_DONATE_MIN;
   a.donate_after = o.donate_after > 0 ? (uint32_t)o.donate_after : DEFAULT_DONATE_AFTER;
   a.wait_limit_ns = IDLE_LIMIT_NS;
+  a.policy = policy;
   const int wbits = o.bitmap_width == 64 ? 64 : 32;
   QueueView qv[NCLS];
   for (int c = CLS_R32; c <= CLS_MEM; ++c)
@@ -464,7 +531,7 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
     int grid[NCLS], block[NCLS];
     int dcap, xcap, wbits, share, dmin, log;
     uint32_t dafter;
-    const void *slab, *graph_count, *graph_of, *root_nodes, *q[NCLS], *bufs[4];
+    const void *slab, *graph_count, *graph_of, *root_nodes, *policy, *q[NCLS], *bufs[4];
     int64_t n, G;
   } key;
   std::memset(&key, 0, sizeof(key));
@@ -484,6 +551,7 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   key.graph_count = a.graph_count;
   key.root_nodes = a.root_nodes;
   key.graph_of = a.graph_of;
+  key.policy = a.policy;
   key.bufs[0] = g->rp;
   key.bufs[1] = g->split;
   key.bufs[2] = g->cs;
@@ -778,6 +846,251 @@ int mce_batch_free(mce_batch_t b) {
   if (b->g) mce_graph_free(b->g);
   delete b;
   return MCE_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Cost model
+// ---------------------------------------------------------------------------
+namespace {
+
+int model_upload(mce_model *m, const float *params) {
+  std::vector<__half> h(MLP_PARAMS);
+  for (int i = 0; i < MLP_PARAMS; ++i) h[i] = __float2half_rn(params[i]);
+  MCE_CUDA(cudaMemcpyAsync(m->master, params, sizeof(float) * MLP_PARAMS, cudaMemcpyHostToDevice,
+                           m->own));
+  MCE_CUDA(cudaMemcpyAsync(m->wh, h.data(), sizeof(__half) * MLP_PARAMS, cudaMemcpyHostToDevice,
+                           m->own));
+  MCE_CUDA(cudaMemsetAsync(m->m1, 0, sizeof(float) * MLP_PARAMS, m->own));
+  MCE_CUDA(cudaMemsetAsync(m->m2, 0, sizeof(float) * MLP_PARAMS, m->own));
+  MCE_CUDA(cudaMemsetAsync(m->grad, 0, sizeof(float) * MLP_PARAMS, m->own));
+  MCE_CUDA(cudaStreamSynchronize(m->own));
+  m->step = 0;
+  return MCE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mce_model_create(int32_t device, uint64_t seed, mce_model_t *out) {
+  if (!out) return MCE_EINVAL;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return MCE_ENODEV;
+  if (device < 0 || device >= ndev) return MCE_EINVAL;
+  MCE_CUDA(cudaSetDevice(device));
+  mce_model *m = new (std::nothrow) mce_model();
+  if (!m) return MCE_ENOMEM;
+  m->device = device;
+  int rc;
+  if (cudaStreamCreateWithFlags(&m->own, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaDeviceGetAttribute(&m->sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
+    delete m;
+    return MCE_ECUDA;
+  }
+  if ((rc = dalloc(&m->master, MLP_PARAMS)) || (rc = dalloc(&m->grad, MLP_PARAMS)) ||
+      (rc = dalloc(&m->m1, MLP_PARAMS)) || (rc = dalloc(&m->m2, MLP_PARAMS)) ||
+      (rc = dalloc(&m->loss, 4)) || (rc = dalloc(&m->wh, MLP_PARAMS))) {
+    mce_model_free(m);
+    return rc;
+  }
+  // He-uniform weights, zero biases (seeded)
+  std::vector<float> p(MLP_PARAMS, 0.f);
+  mce::Rng rng(seed, 0x4d4c50ull);
+  const int F = MLP_IN, H = MLP_HIDDEN;
+  auto fill = [&](int off, int count, float fan_in) {
+    const float lim = std::sqrt(6.0f / fan_in);
+    for (int i = 0; i < count; ++i) p[off + i] = (float)((rng.uniform() * 2.0 - 1.0) * lim);
+  };
+  fill(0, H * F, (float)F);
+  fill(H * F + H, H * H, (float)H);
+  fill(H * F + H + H * H + H, H, (float)H);
+  if ((rc = model_upload(m, p.data()))) {
+    mce_model_free(m);
+    return rc;
+  }
+  *out = m;
+  return MCE_OK;
+}
+
+int mce_model_free(mce_model_t m) {
+  if (!m) return MCE_OK;
+  cudaSetDevice(m->device);
+  if (m->own) cudaStreamSynchronize(m->own);
+  dfree(m->master);
+  dfree(m->grad);
+  dfree(m->m1);
+  dfree(m->m2);
+  dfree(m->loss);
+  dfree(m->wh);
+  if (m->own) cudaStreamDestroy(m->own);
+  delete m;
+  return MCE_OK;
+}
+
+int mce_model_set(mce_model_t m, const float *params) {
+  if (!m || !params) return MCE_EINVAL;
+  MCE_CUDA(cudaSetDevice(m->device));
+  return model_upload(m, params);
+}
+
+int mce_model_get(mce_model_t m, float *params_out, uint16_t *fp16_out) {
+  if (!m || (!params_out && !fp16_out)) return MCE_EINVAL;
+  MCE_CUDA(cudaSetDevice(m->device));
+  if (params_out)
+    MCE_CUDA(cudaMemcpyAsync(params_out, m->master, sizeof(float) * MLP_PARAMS,
+                             cudaMemcpyDeviceToHost, m->own));
+  if (fp16_out)
+    MCE_CUDA(cudaMemcpyAsync(fp16_out, m->wh, sizeof(uint16_t) * MLP_PARAMS,
+                             cudaMemcpyDeviceToHost, m->own));
+  MCE_CUDA(cudaStreamSynchronize(m->own));
+  return MCE_OK;
+}
+
+int mce_root_features(mce_graph_t g, float *features_out) {
+  if (!g) return MCE_EINVAL;
+  MCE_CUDA(cudaSetDevice(g->device));
+  cudaStream_t s = g->own;
+  int launches = 0, rc;
+  if ((rc = run_peel(g, s, &launches)) || (rc = run_orient(g, s, &launches)) ||
+      (rc = compute_features(g, s, &launches)))
+    return rc;
+  if (features_out && g->n)
+    MCE_CUDA(cudaMemcpyAsync(features_out, g->feat, sizeof(float) * MLP_IN * (size_t)g->n,
+                             cudaMemcpyDeviceToHost, s));
+  MCE_CUDA(cudaStreamSynchronize(s));
+  return MCE_OK;
+}
+
+int mce_model_train(mce_model_t m, mce_graph_t g, int32_t epochs, int32_t batch, float lr,
+                    uint64_t seed, float *loss_out) {
+  if (!m || !g || epochs < 1 || batch < 1 || !(lr > 0.f)) return MCE_EINVAL;
+  if (m->device != g->device) return MCE_EINVAL;
+  if (!g->logged || !g->root_nodes) return MCE_ESTATE;  // needs a count with log_roots = 1
+  MCE_CUDA(cudaSetDevice(g->device));
+  cudaStream_t s = m->own;
+  // the logged tree sizes belong to the current orientation; recompute features for it
+  std::vector<unsigned long long> nodes((size_t)g->n);
+  MCE_CUDA(cudaMemcpy(nodes.data(), g->root_nodes, sizeof(unsigned long long) * (size_t)g->n,
+                      cudaMemcpyDeviceToHost));
+  int rc = mce_root_features(g, nullptr);
+  if (rc) return rc;
+  std::vector<int32_t> idx;
+  std::vector<float> y((size_t)g->n, 0.f);
+  for (int64_t v = 0; v < g->n; ++v)
+    if (nodes[v]) {
+      idx.push_back((int32_t)v);
+      y[v] = std::log2(1.0f + (float)nodes[v]);
+    }
+  const int64_t N = (int64_t)idx.size();
+  if (N == 0) return MCE_EINVAL;
+  float *dy = nullptr;
+  int32_t *didx = nullptr;
+  if ((rc = dalloc(&dy, (size_t)g->n)) || (rc = dalloc(&didx, (size_t)N))) {
+    dfree(dy);
+    return rc;
+  }
+  MCE_CUDA(cudaMemcpyAsync(dy, y.data(), sizeof(float) * (size_t)g->n, cudaMemcpyHostToDevice, s));
+  mce::Rng rng(seed, 0x5452ull);
+  for (int e = 0; e < epochs && !rc; ++e) {
+    for (int64_t i = N - 1; i > 0; --i) std::swap(idx[i], idx[(int64_t)rng.below(i + 1)]);
+    if (cudaMemcpyAsync(didx, idx.data(), sizeof(int32_t) * (size_t)N, cudaMemcpyHostToDevice, s) !=
+            cudaSuccess ||
+        cudaMemsetAsync(m->loss, 0, sizeof(float), s) != cudaSuccess) {
+      rc = MCE_ECUDA;
+      break;
+    }
+    for (int64_t b = 0; b < N && !rc; b += batch) {
+      const int64_t end = std::min<int64_t>(N, b + batch);
+      rc = mlp_grad_launch(m->wh, g->feat, dy, didx, b, end, m->grad, m->loss, s);
+      if (!rc) rc = mlp_adam_launch(m->master, m->wh, m->grad, m->m1, m->m2, lr, ++m->step, s);
+    }
+    float l = 0.f;
+    if (!rc && cudaMemcpyAsync(&l, m->loss, sizeof(float), cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+        cudaStreamSynchronize(s) == cudaSuccess) {
+      if (loss_out) loss_out[e] = l / (float)N;
+    } else if (!rc) {
+      rc = MCE_ECUDA;
+    }
+  }
+  cudaStreamSynchronize(s);
+  dfree(dy);
+  dfree(didx);
+  return rc;
+}
+
+int mce_model_predict(mce_model_t m, mce_graph_t g, float *pred_out) {
+  if (!m || !g) return MCE_EINVAL;
+  if (m->device != g->device) return MCE_EINVAL;
+  int rc = mce_root_features(g, nullptr);
+  if (rc) return rc;
+  cudaStream_t s = g->own;
+  if ((rc = mlp_forward_launch(m->wh, g->feat, nullptr, g->n, g->pred, g->sms, s, nullptr)))
+    return rc;
+  if (pred_out && g->n)
+    MCE_CUDA(cudaMemcpyAsync(pred_out, g->pred, sizeof(float) * (size_t)g->n,
+                             cudaMemcpyDeviceToHost, s));
+  MCE_CUDA(cudaStreamSynchronize(s));
+  return MCE_OK;
+}
+
+int mce_model_eval(mce_model_t m, const float *X, int64_t count, float *out) {
+  if (!m || count < 0 || (count > 0 && (!X || !out))) return MCE_EINVAL;
+  if (count == 0) return MCE_OK;
+  MCE_CUDA(cudaSetDevice(m->device));
+  float *dx = nullptr, *dout = nullptr;
+  int rc;
+  if ((rc = dalloc(&dx, (size_t)count * MLP_IN)) || (rc = dalloc(&dout, (size_t)count))) {
+    dfree(dx);
+    return rc;
+  }
+  cudaStream_t s = m->own;
+  if (cudaMemcpyAsync(dx, X, sizeof(float) * MLP_IN * (size_t)count, cudaMemcpyHostToDevice, s) !=
+      cudaSuccess)
+    rc = MCE_ECUDA;
+  if (!rc) rc = mlp_forward_launch(m->wh, dx, nullptr, count, dout, m->sms, s, nullptr);
+  if (!rc && (cudaMemcpyAsync(out, dout, sizeof(float) * (size_t)count, cudaMemcpyDeviceToHost,
+                              s) != cudaSuccess ||
+              cudaStreamSynchronize(s) != cudaSuccess))
+    rc = MCE_ECUDA;
+  dfree(dx);
+  dfree(dout);
+  return rc;
+}
+
+int mce_model_grad(mce_model_t m, const float *X, const float *Y, int64_t count, float *grad_out,
+                   float *loss_out) {
+  if (!m || count < 1 || !X || !Y || !grad_out) return MCE_EINVAL;
+  MCE_CUDA(cudaSetDevice(m->device));
+  float *dx = nullptr, *dy = nullptr;
+  int rc;
+  if ((rc = dalloc(&dx, (size_t)count * MLP_IN)) || (rc = dalloc(&dy, (size_t)count))) {
+    dfree(dx);
+    return rc;
+  }
+  cudaStream_t s = m->own;
+  float l = 0.f;
+  if (cudaMemcpyAsync(dx, X, sizeof(float) * MLP_IN * (size_t)count, cudaMemcpyHostToDevice, s) !=
+          cudaSuccess ||
+      cudaMemcpyAsync(dy, Y, sizeof(float) * (size_t)count, cudaMemcpyHostToDevice, s) !=
+          cudaSuccess ||
+      cudaMemsetAsync(m->grad, 0, sizeof(float) * MLP_PARAMS, s) != cudaSuccess ||
+      cudaMemsetAsync(m->loss, 0, sizeof(float), s) != cudaSuccess)
+    rc = MCE_ECUDA;
+  if (!rc) rc = mlp_grad_launch(m->wh, dx, dy, nullptr, 0, count, m->grad, m->loss, s);
+  if (!rc && (cudaMemcpyAsync(grad_out, m->grad, sizeof(float) * MLP_PARAMS,
+                              cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+              cudaMemcpyAsync(&l, m->loss, sizeof(float), cudaMemcpyDeviceToHost, s) !=
+                  cudaSuccess ||
+              cudaMemsetAsync(m->grad, 0, sizeof(float) * MLP_PARAMS, s) != cudaSuccess ||
+              cudaStreamSynchronize(s) != cudaSuccess))
+    rc = MCE_ECUDA;
+  if (loss_out) *loss_out = l / (float)count;
+  dfree(dx);
+  dfree(dy);
+  return rc;
 }
 
 }  // extern "C"

@@ -86,6 +86,7 @@ struct BKArgs {
   int32_t donate_min;            // hand off children with at least this many candidates
   uint32_t donate_after;         // ... once this many nodes of the root/task were walked
   uint64_t wait_limit_ns;        // an idle warp gives up after this long without progress
+  const uint8_t *policy;         // nullable [n]: 1 = root may share subtrees at once, 0 = never
 };
 
 // Launch the engine of one class.  warps_out: number of warps launched (slab sizing).
@@ -93,6 +94,22 @@ int bk_warps_for_class(int cls, int sms, int *warps, int *block, int *smem);
 size_t bk_slab_words(int cls, int dcap, int xcap);
 uint32_t bk_task_words(int cls, int dcap);
 int queue_launch_init(const QueueView &q, cudaStream_t s, int *launches);
+
+// ---- cost model -----------------------------------------------------------------
+constexpr int MLP_IN = 8, MLP_HIDDEN = 64;
+constexpr int MLP_PARAMS = MLP_HIDDEN * MLP_IN + MLP_HIDDEN + MLP_HIDDEN * MLP_HIDDEN + MLP_HIDDEN +
+                           MLP_HIDDEN + 1;
+int features_launch(int64_t n, const int32_t *rp, const int32_t *split, const int32_t *cs,
+                    const int32_t *core, float *out, int sms, cudaStream_t s, int *launches);
+int mlp_forward_launch(const void *wh, const float *X, const int32_t *idx, int64_t count,
+                       float *out, int sms, cudaStream_t s, int *launches);
+int mlp_grad_launch(const void *wh, const float *X, const float *Y, const int32_t *idx,
+                    int64_t begin, int64_t end, float *grad, float *loss, cudaStream_t s);
+int mlp_adam_launch(float *master, void *wh, float *grad, float *m1, float *m2, float lr,
+                    int step, cudaStream_t s);
+int rekey_launch(int64_t n, uint32_t *keys, const float *cost, const int32_t *rp,
+                 const int32_t *split, uint8_t *policy, float heavy_cost, int sms, cudaStream_t s,
+                 int *launches);
 
 // ---- batches ------------------------------------------------------------------
 int batch_rebase_launch(const int32_t *rp_local, const int32_t *col_local,

@@ -45,7 +45,7 @@ class _Opts(C.Structure):
                 ("log_roots", C.c_int32), ("x_pivot", C.c_int32),
                 ("peel_solo_max", C.c_int32), ("donate_after", C.c_int32),
                 ("cuda_graph", C.c_int32), ("reserved", C.c_int32 * 4),
-                ("stream", C.c_void_p)]
+                ("stream", C.c_void_p), ("model", C.c_void_p)]
 
 
 class _Stats(C.Structure):
@@ -89,6 +89,15 @@ _sigs = {
     "mce_batch_reload": (C.c_int, [_P, _P, _P, _P, _P, C.c_int32, _P]),
     "mce_batch_count": (C.c_int, [_P, _P, _P, _P, _P, _P]),
     "mce_batch_free": (C.c_int, [_P]),
+    "mce_model_create": (C.c_int, [C.c_int32, C.c_uint64, _P]),
+    "mce_model_free": (C.c_int, [_P]),
+    "mce_model_set": (C.c_int, [_P, _P]),
+    "mce_model_get": (C.c_int, [_P, _P, _P]),
+    "mce_root_features": (C.c_int, [_P, _P]),
+    "mce_model_train": (C.c_int, [_P, _P, C.c_int32, C.c_int32, C.c_float, C.c_uint64, _P]),
+    "mce_model_predict": (C.c_int, [_P, _P, _P]),
+    "mce_model_eval": (C.c_int, [_P, _P, C.c_int64, _P]),
+    "mce_model_grad": (C.c_int, [_P, _P, _P, C.c_int64, _P, _P]),
     "mce_gen_er": (C.c_int, [C.c_int64, C.c_double, C.c_uint64, C.c_int32, C.c_int32,
                              C.c_int32, _P]),
     "mce_gen_rmat": (C.c_int, [C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,
@@ -286,7 +295,7 @@ def _stats_dict(st: _Stats) -> dict:
 
 def make_opts(*, sched=SCHED_PLAIN, bitmap_width=0, log_roots=False, level=LEVEL_L1,
               induced=INDUCED_P, worker_list=WL_ON, donate_threshold=0, x_pivot=0,
-              peel_solo_max=0, donate_after=0, cuda_graph=0, stream=None) -> _Opts:
+              peel_solo_max=0, donate_after=0, cuda_graph=0, model=None, stream=None) -> _Opts:
     o = _Opts()
     _lib.mce_opts_default(C.byref(o))
     o.sched, o.bitmap_width, o.log_roots = sched, bitmap_width, int(bool(log_roots))
@@ -294,6 +303,7 @@ def make_opts(*, sched=SCHED_PLAIN, bitmap_width=0, log_roots=False, level=LEVEL
     o.donate_threshold, o.x_pivot = donate_threshold, x_pivot
     o.peel_solo_max, o.donate_after, o.cuda_graph = peel_solo_max, donate_after, cuda_graph
     o.stream = stream
+    o.model = model._h if model is not None else None
     return o
 
 
@@ -429,3 +439,74 @@ class Batch:
 
     def __exit__(self, *a):
         self.close()
+
+
+MLP_INPUTS, MLP_HIDDEN, MLP_PARAMS = 8, 64, 4801
+
+
+class Model:
+    """The cost MLP (wraps mce_model_t)."""
+
+    def __init__(self, device: int = 0, seed: int = 1):
+        self._h = C.c_void_p()
+        _check(_lib.mce_model_create(device, seed, C.byref(self._h)), "model_create")
+
+    def set(self, params: np.ndarray) -> None:
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        assert p.size == MLP_PARAMS
+        _check(_lib.mce_model_set(self._h, _ptr(p)), "model_set")
+
+    def get(self) -> tuple[np.ndarray, np.ndarray]:
+        p = np.zeros(MLP_PARAMS, np.float32)
+        h = np.zeros(MLP_PARAMS, np.uint16)
+        _check(_lib.mce_model_get(self._h, _ptr(p), _ptr(h)), "model_get")
+        return p, h.view(np.float16)
+
+    def save(self, path: str) -> None:
+        self.get()[0].tofile(path)
+
+    def load(self, path: str) -> None:
+        self.set(np.fromfile(path, dtype=np.float32))
+
+    def train(self, g: "Graph", epochs=8, batch=1024, lr=2e-3, seed=7) -> np.ndarray:
+        loss = np.zeros(epochs, np.float32)
+        _check(_lib.mce_model_train(self._h, g._h, epochs, batch, lr, seed, _ptr(loss)),
+               "model_train")
+        return loss
+
+    def predict(self, g: "Graph") -> np.ndarray:
+        out = np.zeros(max(g.n, 1), np.float32)
+        _check(_lib.mce_model_predict(self._h, g._h, _ptr(out)), "model_predict")
+        return out[:g.n]
+
+    def eval(self, X: np.ndarray) -> np.ndarray:
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        out = np.zeros(len(X), np.float32)
+        _check(_lib.mce_model_eval(self._h, _ptr(X), len(X), _ptr(out)), "model_eval")
+        return out
+
+    def grad(self, X: np.ndarray, Y: np.ndarray) -> tuple[np.ndarray, float]:
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        Y = np.ascontiguousarray(Y, dtype=np.float32)
+        g = np.zeros(MLP_PARAMS, np.float32)
+        loss = C.c_float()
+        _check(_lib.mce_model_grad(self._h, _ptr(X), _ptr(Y), len(X), _ptr(g), C.byref(loss)),
+               "model_grad")
+        return g, float(loss.value)
+
+    def close(self) -> None:
+        if self._h:
+            _lib.mce_model_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def root_features(g: "Graph") -> np.ndarray:
+    out = np.zeros((max(g.n, 1), MLP_INPUTS), np.float32)
+    _check(_lib.mce_root_features(g._h, _ptr(out)), "root_features")
+    return out[:g.n]

@@ -556,3 +556,75 @@ int oracle_tomita(int64_t n, const int32_t *row_ptr, const int32_t *col, uint64_
   free(adj); free(P); free(X); free(buf);
   return ORACLE_OK;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Cost-model reference in double precision (checks the GPU MLP kernels).    */
+/* Layout: W1[64][8], b1[64], W2[64][64], b2[64], W3[64], b3; ReLU;          */
+/* loss = mean (out - y)^2.  The caller passes the weights the GPU uses       */
+/* (its FP16 copy, widened), so only the accumulation precision differs.     */
+/* ------------------------------------------------------------------------ */
+#define MLP_F 8
+#define MLP_H 64
+#define MLP_NP (MLP_H * MLP_F + MLP_H + MLP_H * MLP_H + MLP_H + MLP_H + 1)
+
+static double mlp_fwd(const double *w, const float *x, double *h1, double *h2) {
+  const double *W1 = w, *b1 = W1 + MLP_H * MLP_F, *W2 = b1 + MLP_H, *b2 = W2 + MLP_H * MLP_H;
+  const double *W3 = b2 + MLP_H, *b3 = W3 + MLP_H;
+  for (int j = 0; j < MLP_H; ++j) {
+    double a = b1[j];
+    for (int i = 0; i < MLP_F; ++i) a += W1[j * MLP_F + i] * x[i];
+    h1[j] = a > 0 ? a : 0;
+  }
+  double out = b3[0];
+  for (int k = 0; k < MLP_H; ++k) {
+    double a = b2[k];
+    for (int j = 0; j < MLP_H; ++j) a += W2[k * MLP_H + j] * h1[j];
+    h2[k] = a > 0 ? a : 0;
+    out += W3[k] * h2[k];
+  }
+  return out;
+}
+
+int oracle_mlp_forward(const float *params, const float *X, int64_t count, double *out) {
+  double w[MLP_NP], h1[MLP_H], h2[MLP_H];
+  for (int p = 0; p < MLP_NP; ++p) w[p] = params[p];
+  for (int64_t s = 0; s < count; ++s) out[s] = mlp_fwd(w, X + s * MLP_F, h1, h2);
+  return ORACLE_OK;
+}
+
+int oracle_mlp_grad(const float *params, const float *X, const float *Y, int64_t count,
+                    double *grad, double *loss) {
+  if (count < 1) return ORACLE_EINVAL;
+  double w[MLP_NP], h1[MLP_H], h2[MLP_H], d2[MLP_H], a1;
+  for (int p = 0; p < MLP_NP; ++p) {
+    w[p] = params[p];
+    grad[p] = 0;
+  }
+  const double *W2 = w + MLP_H * MLP_F + MLP_H, *W3 = W2 + MLP_H * MLP_H + MLP_H;
+  double *gW1 = grad, *gb1 = gW1 + MLP_H * MLP_F, *gW2 = gb1 + MLP_H, *gb2 = gW2 + MLP_H * MLP_H;
+  double *gW3 = gb2 + MLP_H, *gb3 = gW3 + MLP_H;
+  double L = 0;
+  for (int64_t s = 0; s < count; ++s) {
+    const float *x = X + s * MLP_F;
+    const double e = mlp_fwd(w, x, h1, h2) - Y[s];
+    L += e * e;
+    const double g = 2 * e / (double)count;
+    gb3[0] += g;
+    for (int k = 0; k < MLP_H; ++k) {
+      gW3[k] += g * h2[k];
+      d2[k] = h2[k] > 0 ? g * W3[k] : 0;
+      gb2[k] += d2[k];
+      for (int j = 0; j < MLP_H; ++j) gW2[k * MLP_H + j] += d2[k] * h1[j];
+    }
+    for (int j = 0; j < MLP_H; ++j) {
+      double a = 0;
+      if (h1[j] > 0)
+        for (int k = 0; k < MLP_H; ++k) a += W2[k * MLP_H + j] * d2[k];
+      a1 = a;
+      gb1[j] += a1;
+      for (int i = 0; i < MLP_F; ++i) gW1[j * MLP_F + i] += a * x[i];
+    }
+  }
+  *loss = L / (double)count;
+  return ORACLE_OK;
+}

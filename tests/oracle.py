@@ -95,3 +95,26 @@ def tomita(g):
     hist = np.zeros(HIST, np.uint64)
     assert _o.oracle_tomita(g.n, _p(rp), _p(col), C.byref(tot), _p(hist), HIST) == 0
     return tot.value, hist
+
+
+_o.oracle_mlp_forward.argtypes = [_P, _P, C.c_int64, _P]
+_o.oracle_mlp_grad.argtypes = [_P, _P, _P, C.c_int64, _P, _P]
+MLP_PARAMS = 4801
+
+
+def mlp_forward(params, X):
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    out = np.zeros(len(X), np.float64)
+    assert _o.oracle_mlp_forward(_p(p), _p(X), len(X), _p(out)) == 0
+    return out
+
+
+def mlp_grad(params, X, Y):
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    Y = np.ascontiguousarray(Y, dtype=np.float32)
+    g = np.zeros(MLP_PARAMS, np.float64)
+    loss = C.c_double()
+    assert _o.oracle_mlp_grad(_p(p), _p(X), _p(Y), len(X), _p(g), C.byref(loss)) == 0
+    return g, loss.value

@@ -1,0 +1,82 @@
+"""The cost model's GPU kernels against the double-precision reference, and
+scheduling by it (which must never change a count or a search tree)."""
+import numpy as np
+import pytest
+
+import mce_b200 as mce
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def sample(seed, k=200):
+    rng = np.random.default_rng(seed)
+    X = rng.uniform(0, 9, (k, 8)).astype(np.float32)
+    X[:, 4] = rng.uniform(0, 1, k)  # density feature lies in [0, 1]
+    Y = rng.uniform(0, 14, k).astype(np.float32)
+    return X, Y
+
+
+def test_forward_matches_reference():
+    m = mce.Model(seed=3)
+    X, _ = sample(1)
+    w16 = m.get()[1].astype(np.float32)  # the weights the kernels use
+    got = m.eval(X)
+    want = oracle.mlp_forward(w16, X)
+    # FP16 weights in both; FP32 vs FP64 accumulation over <= 64 terms
+    np.testing.assert_allclose(got, want, rtol=1e-4, atol=1e-4)
+
+
+def test_gradient_matches_reference():
+    m = mce.Model(seed=5)
+    X, Y = sample(2, 300)  # three blocks of the training kernel
+    w16 = m.get()[1].astype(np.float32)
+    g, loss = m.grad(X, Y)
+    gr, lr = oracle.mlp_grad(w16, X, Y)
+    assert abs(loss - lr) <= 1e-4 * max(1.0, lr)
+    scale = np.abs(gr).max()
+    np.testing.assert_allclose(g, gr, rtol=1e-3, atol=1e-5 * scale)
+
+
+def test_training_learns_tree_sizes():
+    train = mce.gen_ba(60000, 8, 24, 30, 20, 60)
+    test = mce.gen_ba(60000, 8, 23, 30, 20, 60)
+    m = mce.Model(seed=1)
+    with mce.Graph.from_host(train) as dg:
+        dg.count(log_roots=True)
+        losses = m.train(dg, epochs=6, batch=512, lr=2e-3)
+    assert losses[-1] < 0.5 * losses[0]
+    with mce.Graph.from_host(test) as dg:
+        dg.count(log_roots=True)
+        nodes = dg.root_log()
+        pred = m.predict(dg)
+    roots = nodes > 0
+    y = np.log2(1 + nodes[roots].astype(np.float64))
+    p = pred[roots]
+    # rank agreement with the true tree sizes on a graph it was not trained on
+    ry, rp = np.argsort(np.argsort(y)), np.argsort(np.argsort(p))
+    assert np.corrcoef(ry, rp)[0, 1] > 0.6
+
+
+@pytest.mark.parametrize("maker", [
+    lambda: mce.gen_ba(40000, 8, 9, 20, 20, 60),
+    lambda: mce.union(mce.gen_chung_lu_batch(32, 64, 4096, 2.3, 8, 32, 5, 5, 40, 13)),
+    lambda: mce.gen_rmat(12, 16, 0.57, 0.19, 0.19, 7),
+])
+def test_schedules_change_order_never_results(maker):
+    g = maker()
+    m = mce.Model(seed=2)
+    with mce.Graph.from_host(g) as dg:
+        dg.count(log_roots=True)
+        m.train(dg, epochs=2, batch=512)
+        runs = []
+        for kw in (dict(sched=mce.SCHED_PLAIN), dict(sched=mce.SCHED_DEGREE),
+                   dict(sched=mce.SCHED_LEARNED, model=m),
+                   dict(sched=mce.SCHED_LEARNED, model=m, worker_list=mce.WL_OFF)):
+            r = dg.count(log_roots=True, **kw)
+            runs.append((r.total, r.hist.copy(), dg.root_counts(), dg.root_log()))
+    t0, h0, c0, n0 = runs[0]
+    assert t0 == oracle.count(g)[0]
+    for t, h, c, n in runs[1:]:
+        assert t == t0 and np.array_equal(h, h0)
+        assert np.array_equal(c, c0) and np.array_equal(n, n0)
