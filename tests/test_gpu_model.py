@@ -50,12 +50,15 @@ def test_training_learns_tree_sizes():
         dg.count(log_roots=True)
         nodes = dg.root_log()
         pred = m.predict(dg)
+    from scipy.stats import spearmanr
     roots = nodes > 0
-    y = np.log2(1 + nodes[roots].astype(np.float64))
+    y = nodes[roots].astype(np.float64)
     p = pred[roots]
-    # rank agreement with the true tree sizes on a graph it was not trained on
-    ry, rp = np.argsort(np.argsort(y)), np.argsort(np.argsort(p))
-    assert np.corrcoef(ry, rp)[0, 1] > 0.6
+    # on a graph it was not trained on: tie-aware rank agreement, and the
+    # roots it ranks in the top 1% carry many times 1% of all tree nodes
+    assert spearmanr(y, p).correlation > 0.5
+    top = np.argsort(-p)[:max(1, len(p) // 100)]
+    assert y[top].sum() / y.sum() > 0.10
 
 
 @pytest.mark.parametrize("maker", [
