@@ -273,8 +273,10 @@ int mce_model_set(mce_model_t m, const float *params);
 int mce_model_get(mce_model_t m, float *params_out, uint16_t *fp16_out);
 /* Features of every vertex (n x MCE_MLP_INPUTS, zeros for non-roots). */
 int mce_root_features(mce_graph_t g, float *features_out);
-/* Train on the roots of g against the tree sizes of the last mce_count that
- * ran with log_roots = 1 (MCE_ESTATE otherwise): `epochs` passes of Adam
+/* Train on the roots of g with at least 16 later neighbours (the roots the
+ * model ranks; smaller trees are not worth scheduling) against the tree
+ * sizes of the last mce_count that ran with log_roots = 1 (MCE_ESTATE
+ * otherwise): `epochs` passes of Adam
  * over seeded shuffles in minibatches of `batch`; loss_out (nullable,
  * `epochs` entries) gets each epoch's mean squared error.                  */
 int mce_model_train(mce_model_t m, mce_graph_t g, int32_t epochs, int32_t batch, float lr,

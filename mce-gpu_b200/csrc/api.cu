@@ -416,7 +416,8 @@ struct mce_model {
 
 namespace {
 
-constexpr float HEAVY_COST = 10.0f;  // predicted log2(tree nodes): roots above it share at once
+constexpr float HEAVY_COST = 10.0f;   // predicted log2(tree nodes): run first, share at once
+constexpr float DEGREE_HEAVY = 12.0f; // degree-heuristic cost above which a root runs first
 
 int ensure_feat(mce_graph *g) {
   int rc;
@@ -454,8 +455,8 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   if ((rc = run_orient(g, s, &launches, sched != MCE_SCHED_PLAIN))) return rc;
   const uint8_t *policy = nullptr;
   if (sched == MCE_SCHED_DEGREE && g->n > 0) {
-    if ((rc = rekey_launch(g->n, g->keys_in, nullptr, g->rp, g->split, nullptr, 0.f, g->sms, s,
-                           &launches)) ||
+    if ((rc = rekey_launch(g->n, g->keys_in, nullptr, g->rp, g->split, nullptr, DEGREE_HEAVY,
+                           g->sms, s, &launches)) ||
         (rc = run_sort(g, 32, s, &launches)))
       return rc;
   } else if (sched == MCE_SCHED_LEARNED && g->n > 0) {
@@ -977,10 +978,15 @@ int mce_model_train(mce_model_t m, mce_graph_t g, int32_t epochs, int32_t batch,
                       cudaMemcpyDeviceToHost));
   int rc = mce_root_features(g, nullptr);
   if (rc) return rc;
+  std::vector<int32_t> split((size_t)g->n), rp((size_t)g->n + 1);
+  MCE_CUDA(cudaMemcpy(split.data(), g->split, sizeof(int32_t) * (size_t)g->n,
+                      cudaMemcpyDeviceToHost));
+  MCE_CUDA(cudaMemcpy(rp.data(), g->rp, sizeof(int32_t) * (size_t)(g->n + 1),
+                      cudaMemcpyDeviceToHost));
   std::vector<int32_t> idx;
   std::vector<float> y((size_t)g->n, 0.f);
   for (int64_t v = 0; v < g->n; ++v)
-    if (nodes[v]) {
+    if (nodes[v] && rp[v + 1] - split[v] >= MLP_MIN_LATER) {  // the roots the model ranks
       idx.push_back((int32_t)v);
       y[v] = std::log2(1.0f + (float)nodes[v]);
     }

@@ -86,7 +86,7 @@ struct BKArgs {
   int32_t donate_min;            // hand off children with at least this many candidates
   uint32_t donate_after;         // ... once this many nodes of the root/task were walked
   uint64_t wait_limit_ns;        // an idle warp gives up after this long without progress
-  const uint8_t *policy;         // nullable [n]: 1 = root may share subtrees at once, 0 = never
+  const uint8_t *policy;         // nullable [n]: 1 = root may share subtrees at once
 };
 
 // Launch the engine of one class.  warps_out: number of warps launched (slab sizing).
@@ -97,6 +97,7 @@ int queue_launch_init(const QueueView &q, cudaStream_t s, int *launches);
 
 // ---- cost model -----------------------------------------------------------------
 constexpr int MLP_IN = 8, MLP_HIDDEN = 64;
+constexpr int MLP_MIN_LATER = 16;  // roots the model sees: at least this many later neighbours
 constexpr int MLP_PARAMS = MLP_HIDDEN * MLP_IN + MLP_HIDDEN + MLP_HIDDEN * MLP_HIDDEN + MLP_HIDDEN +
                            MLP_HIDDEN + 1;
 int features_launch(int64_t n, const int32_t *rp, const int32_t *split, const int32_t *cs,

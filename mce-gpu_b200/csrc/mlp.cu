@@ -42,6 +42,9 @@ __device__ __forceinline__ float lg(float x) { return log2f(1.0f + x); }
 // pivot).  Non-roots get zeros.
 // ---------------------------------------------------------------------------
 constexpr int FEAT_CAP = 64;
+// Roots with fewer later neighbours have trees too small to be worth
+// scheduling: their features stay zero and the model is not run on them.
+constexpr int FEAT_MIN = MLP_MIN_LATER;
 
 __global__ void features_kernel(int64_t n, const int32_t *__restrict__ rp,
                                 const int32_t *__restrict__ split, const int32_t *__restrict__ cs,
@@ -55,7 +58,7 @@ __global__ void features_kernel(int64_t n, const int32_t *__restrict__ rp,
     const int32_t v = (int32_t)vv;
     const int32_t sb = split[v], dp = rp[v + 1] - sb, dm = sb - rp[v];
     float *o = out + (size_t)v * F;
-    if (dp == 0) {
+    if (dp < FEAT_MIN) {
       if (lane < F) o[lane] = 0.f;
       continue;
     }
@@ -144,7 +147,7 @@ __global__ void mlp_forward_kernel(const __half *__restrict__ wh, const float *_
     float x[F];
 #pragma unroll
     for (int i = 0; i < F; ++i) x[i] = X[(size_t)s * F + i];
-    out[t] = mlp_eval(w, x);
+    out[t] = x[0] > 0.f ? mlp_eval(w, x) : 0.f;  // all-zero features: not a candidate
   }
 }
 
@@ -263,7 +266,10 @@ __global__ void adam_kernel(float *__restrict__ master, __half *__restrict__ wh,
   grad[p] = 0.f;
 }
 
-// Sort key from a cost: class in the top 4 bits, larger cost first.
+// Sort key: class in the top 4 bits; then roots whose cost reaches `heavy`,
+// larger first; every other root keeps the key 0x0FFFFFFF, so the stable
+// sort leaves them in vertex order (neighbouring roots share adjacency
+// lists, and in a batch each graph stays together in L2).
 __global__ void rekey_kernel(int64_t n, uint32_t *keys, const float *__restrict__ cost,
                              const int32_t *__restrict__ rp, const int32_t *__restrict__ split,
                              uint8_t *policy, float heavy_cost) {
@@ -273,15 +279,15 @@ __global__ void rekey_kernel(int64_t n, uint32_t *keys, const float *__restrict_
     float c;
     if (cost) {
       c = cost[v];
-    } else {  // degree heuristic: trees grow with the later degree and core
+    } else {  // degree heuristic: trees grow with the later degree
       const float dp = (float)(rp[v + 1] - split[v]);
-      c = dp * dp * log2f(2.f + (float)(split[v] - rp[v]));
-      c = log2f(1.f + c);
+      c = dp >= 16.f ? log2f(1.f + dp * dp * log2f(2.f + (float)(split[v] - rp[v]))) : 0.f;
     }
     c = c < 0.f ? 0.f : (c > 63.f ? 63.f : c);
-    const uint32_t q = (uint32_t)(c * (float)(1 << 22));  // < 2^28
+    const bool heavy = c >= heavy_cost;
+    const uint32_t q = heavy ? (uint32_t)(c * (float)(1 << 22)) : 0u;  // < 2^28
     keys[v] = (cls << 28) | (0x0FFFFFFFu - q);
-    if (policy) policy[v] = cost && cost[v] >= heavy_cost ? 1 : 0;
+    if (policy) policy[v] = cost && heavy ? 1 : 0;
   }
 }
 
