@@ -41,9 +41,16 @@ def rank_corr(a, b):
 def train(family: str, epochs=8, seed=1) -> dict:
     make_train, make_test = FAMILIES[family]
     m = mce.Model(seed=seed)
-    with mce.Graph.from_host(make_train()) as dg:
+    g = make_train()
+    with mce.Graph.from_host(g) as dg:
         dg.count(log_roots=True)
-        losses = m.train(dg, epochs=epochs, batch=1024, lr=2e-3, seed=seed)
+        split, _ = dg.split_csr()
+        # the model ranks roots with >= 16 later neighbours; size the run by
+        # Adam steps (>= 3000) rather than by passes over few samples
+        ncand = int(np.count_nonzero(g.row_ptr[1:g.n + 1] - split >= 16))
+        batch = 1024 if ncand > 200_000 else 256
+        epochs = max(epochs, 3000 // max(1, -(-ncand // batch)))
+        losses = m.train(dg, epochs=epochs, batch=batch, lr=2e-3, seed=seed)
     with mce.Graph.from_host(make_test()) as dg:
         dg.count(log_roots=True)
         nodes = dg.root_log()
@@ -51,7 +58,8 @@ def train(family: str, epochs=8, seed=1) -> dict:
     roots = nodes > 0
     corr = rank_corr(np.log2(1 + nodes[roots].astype(np.float64)), pred[roots])
     m.save(weights_path(family))
-    return {"family": family, "loss_first": float(losses[0]), "loss_last": float(losses[-1]),
+    return {"family": family, "samples": ncand, "epochs": epochs, "batch": batch,
+            "loss_first": float(losses[0]), "loss_last": float(losses[-1]),
             "heldout_rank_corr": corr}
 
 

@@ -44,7 +44,11 @@ def test_training_learns_tree_sizes():
     m = mce.Model(seed=1)
     with mce.Graph.from_host(train) as dg:
         dg.count(log_roots=True)
-        losses = m.train(dg, epochs=6, batch=512, lr=2e-3)
+        split, _ = dg.split_csr()
+        ncand = int(np.count_nonzero(train.row_ptr[1:train.n + 1] - split >= 16))
+        batch = 64
+        epochs = max(6, 1500 // max(1, -(-ncand // batch)))  # about 1500 Adam steps
+        losses = m.train(dg, epochs=epochs, batch=batch, lr=2e-3)
     assert losses[-1] < 0.5 * losses[0]
     with mce.Graph.from_host(test) as dg:
         dg.count(log_roots=True)
