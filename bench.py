@@ -12,6 +12,13 @@ available here):
   ba     Barabasi-Albert n = 4,000,000, m = 8, seed 23, + 200 overlapping
          planted cliques of size U[20, 60].
   er     Erdos-Renyi G(10000, 0.002), seed 1, + 20 planted cliques U[6, 12].
+  serve  a resident graph answering ego-subgraph requests (2-hop ego graph of a
+         uniform random seed vertex, capped at --ego-cap vertices) arriving as a
+         Poisson process at --rate requests/s; reports cliques/s and p50/p99
+         latency.  --serve-graph picks the resident graph: ba (default;
+         Barabasi-Albert n = 4,000,000, m = 8, seed 31, + 200 planted cliques
+         U[20, 60]), cl (Chung-Lu n = 4,000,000, exponent 2.3, mean degree 8,
+         seed 31) or rmat (R-MAT --scale, edge factor 32, seed 31).
 
 One step = peel + orient + search over the whole workload with the graph
 resident in HBM (`value`), or through the public API with the CSR copied
@@ -45,7 +52,12 @@ def parse_args():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["mine", "reference"], default="mine")
-    p.add_argument("--workload", choices=["batch", "rmat", "ba", "er"], default="batch")
+    p.add_argument("--workload", choices=["batch", "rmat", "ba", "er", "serve"], default="batch")
+    p.add_argument("--serve-graph", choices=["ba", "cl", "rmat"], default="ba")
+    p.add_argument("--ego-cap", type=int, default=16384)
+    p.add_argument("--rate", type=float, default=2000.0, help="serve: Poisson arrivals per second")
+    p.add_argument("--requests", type=int, default=4000, help="serve: requests per timed step")
+    p.add_argument("--max-nodes", type=int, default=0, help="serve: search-node budget per request")
     p.add_argument("--scale", type=int, default=15)
     p.add_argument("--graphs", type=int, default=4096)
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -53,8 +65,9 @@ def parse_args():
     p.add_argument("--donate", type=int, default=0, help="donation threshold (0: default)")
     p.add_argument("--solo", type=int, default=0, help="peel solo frontier size (0: default)")
     p.add_argument("--after", type=int, default=0, help="donate after N nodes (0: default)")
-    p.add_argument("--sched", choices=["plain", "degree", "learned"], default="learned",
-                   help="root order (learned: the shipped cost model of the workload family)")
+    p.add_argument("--sched", choices=["plain", "degree", "learned"], default="degree",
+                   help="root order (learned: the shipped cost model of the workload family; "
+                        "the others are timed beside it unless --no-compare)")
     p.add_argument("--no-compare", action="store_true", help="skip the other schedules")
     return p.parse_args()
 
@@ -386,6 +399,178 @@ def run_mine(args, rank, world, local_rank):
 
 
 # ---------------------------------------------------------------------------
+def serve_graph(args):
+    import mce_b200 as mce
+    if args.serve_graph == "ba":
+        return (mce.gen_ba(4_000_000, 8, 31, 200, 20, 60),
+                "Barabasi-Albert n=4e6 m=8 seed 31 + 200 planted cliques U[20,60]")
+    if args.serve_graph == "cl":
+        return (mce.gen_chung_lu_batch(1, 4_000_000, 4_000_000, 2.3, 8.0, 8.0, 5, 5, 40, 31).graph(0),
+                "Chung-Lu n=4e6 exponent 2.3 mean degree 8 seed 31 + 5 planted cliques U[5,40]")
+    return (mce.gen_rmat(args.scale, 32, 0.57, 0.19, 0.19, 31),
+            f"R-MAT scale {args.scale} edge factor 32 (0.57,0.19,0.19,0.05) seed 31")
+
+
+def serve_trace(n, count, rate, seed):
+    """Uniform random seed vertices and Poisson arrival times (microseconds)."""
+    rng = np.random.default_rng(seed)
+    seeds = rng.integers(0, n, count).astype(np.int64)
+    arrival = np.cumsum(rng.exponential(1e6 / rate, count)) if rate > 0 else None
+    return seeds, arrival
+
+
+def pct(x, q):
+    return float(np.percentile(np.asarray(x, np.float64), q)) if len(x) else None
+
+
+def run_serve(args, rank, world, local_rank):
+    """Serving: requests against a resident graph, one session per GPU."""
+    import torch
+    import mce_b200 as mce
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle
+    torch.cuda.set_device(local_rank)
+    hg, desc = serve_graph(args)
+    g = mce.Graph.from_host(hg, device=local_rank)
+    s = mce.Serve(g, ego_cap=args.ego_cap, max_nodes=args.max_nodes)
+    try:
+        for w in range(args.warmup):  # short traces: first-touch of arenas and code
+            seeds, arr = serve_trace(hg.n, 256, args.rate, 1000 + w)
+            s.run(seeds, arr)
+        with ClockSampler(local_rank) as clk:
+            if world > 1:
+                torch.distributed.barrier()
+            res_all, lat_all, makespans = [], [], []
+            for k in range(args.steps):
+                seeds, arr = serve_trace(hg.n, args.requests, args.rate, 31 + 1000 * rank + k)
+                t0 = time.perf_counter()
+                res, lat = s.run(seeds, arr)
+                makespans.append(time.perf_counter() - t0)
+                res_all.append(res)
+                lat_all.append(lat)
+            if world > 1:
+                torch.distributed.barrier()
+        res = np.concatenate(res_all)
+        lat = np.concatenate(lat_all) / 1e3  # ms
+        ok = res["status"] == mce.OK
+        cliques = int(res["count"][ok].sum())
+        wall = sum(makespans)
+        # capacity: every request of one trace admitted at once
+        seeds_b, _ = serve_trace(hg.n, args.requests, 0, 77 + rank)
+        t0 = time.perf_counter()
+        res_b, lat_b = s.run(seeds_b, None)
+        burst_s = time.perf_counter() - t0
+        st = s.stats()
+        # oracle check on a sample of the timed requests
+        rng = np.random.default_rng(5)
+        pick = rng.choice(len(res), size=min(24, len(res)), replace=False)
+        mism, checked = 0, 0
+        for i in pick:
+            r = res[i]
+            if r["status"] != mce.OK:
+                continue
+            eg, _ = mce.ego_subgraph(hg, int(r["seed"]), args.ego_cap)
+            checked += 1
+            mism += int(oracle.count(eg)[0] != int(r["count"]))
+    finally:
+        s.close()
+        g.close()
+    vals = torch.tensor([cliques / wall, wall], dtype=torch.float64, device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(vals[:1], op=torch.distributed.ReduceOp.SUM)
+    if rank != 0:
+        return None
+    dev_ms = res["device_ns"][ok] / 1e6
+    line = {
+        "metric": METRIC, "value": float(vals[0]), "unit": "maximal cliques/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * wall / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic (seeded generator; uniform random seeds, Poisson arrivals)",
+        "p99_ms": pct(lat, 99),
+        "config": {
+            "workload": f"serve: resident {desc}; 2-hop ego graphs capped at {args.ego_cap} "
+                        f"vertices; Poisson {args.rate:g} req/s, {args.requests} requests per step",
+            "n": int(hg.n), "arcs": int(hg.m), "requests": int(len(res)),
+            "ok": int(ok.sum()), "over_limits": int((~ok).sum()),
+            "maximal_cliques": cliques, "requests_per_s": len(res) / wall,
+            "latency_ms": {"p50": pct(lat, 50), "p90": pct(lat, 90), "p99": pct(lat, 99),
+                           "max": float(lat.max())},
+            "device_ms": {"p50": pct(dev_ms, 50), "p99": pct(dev_ms, 99)},
+            "ego_n": {"p50": pct(res["ego_n"], 50), "max": int(res["ego_n"].max())},
+            "ego_arcs": {"p50": pct(res["ego_arcs"], 50), "max": int(res["ego_arcs"].max())},
+            "cliques_per_request": {"p50": pct(res["count"][ok], 50),
+                                    "max": int(res["count"][ok].max()) if ok.any() else 0},
+            "capacity": {"requests": len(res_b), "seconds": burst_s,
+                         "requests_per_s": len(res_b) / burst_s,
+                         "cliques_per_s": float(res_b["count"][res_b["status"] == mce.OK].sum())
+                         / burst_s, "p99_ms": pct(lat_b / 1e3, 99)},
+            "slots": st["slots"], "arena_bytes": st["arena_bytes"], "slab_bytes": st["slab_bytes"],
+            "oracle_sample": {"checked": checked, "mismatches": mism},
+            "parallelism": f"replicas x{world}",
+        },
+        "e2e": {"value": float(vals[0]), "unit": "maximal cliques/s",
+                "h2d_bytes_per_step": 12 * args.requests, "d2h_bytes_per_step": 48 * args.requests,
+                "note": "requests and answers cross the bus through mapped pinned memory; "
+                        "latency is host-observed, from arrival to answer"},
+        "gpu_launches": int(st["kernel_launches"]),
+        "roofline": None,
+        "clocks": clk.summary(),
+    }
+    return line
+
+
+def run_reference_serve(args, rank, world):
+    """The reference answers one ego graph per process run: a sample of the
+    same trace's requests, each written as .bel and run through its binary."""
+    if rank != 0:
+        return None
+    if not os.path.exists(REF_BIN):
+        return {"impl": "reference", "unavailable": "oracle/_ref/parallel_mce_on_gpus not built"}
+    import mce_b200 as mce
+    hg, desc = serve_graph(args)
+    seeds, _ = serve_trace(hg.n, args.requests, args.rate, 31)
+    tmp = tempfile.mkdtemp(prefix="mce_ref_")
+    bel = os.path.join(tmp, "ego.bel")
+    lat, tot, per = [], 0, 0
+    sample = seeds[:args.warmup + max(args.steps, 1) * 8]
+    for i, sd in enumerate(sample):
+        eg, _ = mce.ego_subgraph(hg, int(sd), args.ego_cap)
+        mce.bel_write(bel, eg)
+        t0 = time.perf_counter()
+        r = subprocess.run([REF_BIN, "-m", "mce", "-g", bel, "-d", "0", "-p", "l1", "-i", "p",
+                            "-w", "nowl"], capture_output=True, text=True, timeout=600)
+        wall = time.perf_counter() - t0
+        out = re.sub(r"\x1b\[[0-9;]*m", "", r.stdout)
+        found = re.findall(r"Found (.*) maximal cliques in total", out)
+        if r.returncode != 0 or not found:
+            return {"impl": "reference", "unavailable": f"reference run failed (rc {r.returncode})"}
+        if i >= args.warmup:
+            lat.append(wall * 1e3)
+            tot += int(found[0].replace(",", ""))
+            per += 1
+    os.remove(bel)
+    os.rmdir(tmp)
+    value = tot / (sum(lat) / 1e3)
+    return {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "maximal cliques/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": sum(lat) / max(args.steps, 1), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic (seeded generator; uniform random seeds)",
+        "p99_ms": pct(lat, 99),
+        "config": {"workload": f"serve: resident {desc}; ego cap {args.ego_cap}; the reference "
+                               "has no serving loop: each request is one run of its binary on "
+                               "the ego graph (.bel), sequentially",
+                   "requests": per, "maximal_cliques": tot,
+                   "latency_ms": {"p50": pct(lat, 50), "p99": pct(lat, 99)}},
+        "cpu_baseline": {"value": value, "unit": "maximal cliques/s", "cores": os.cpu_count(),
+                         "kind": "reference", "sample": f"{per} requests of the trace"},
+        "e2e": {"value": value, "unit": "maximal cliques/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+
+
 def run_reference(args, rank, world):
     """The reference's CUDA binary (built from its own sources) on a sample."""
     if rank != 0:
@@ -463,7 +648,10 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     try:
         if args.impl == "reference":
-            line = run_reference(args, rank, world)
+            line = (run_reference_serve(args, rank, world) if args.workload == "serve"
+                    else run_reference(args, rank, world))
+        elif args.workload == "serve":
+            line = run_serve(args, rank, world, local_rank)
         else:
             line = run_mine(args, rank, world, local_rank)
         if rank == 0 and line is not None:

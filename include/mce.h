@@ -41,6 +41,7 @@ extern "C" {
 #define MCE_ETIMEOUT (-7) /* a bounded device wait ran out                  */
 #define MCE_ENODEV (-8)   /* no usable CUDA device                          */
 #define MCE_ESTATE (-9)   /* call out of order (e.g. serve handle closed)   */
+#define MCE_EAGAIN (-10) /* not finished yet (mce_serve_poll)              */
 
 /* Clique-size histogram length: hist[s] counts maximal cliques of size s.  */
 #define MCE_HIST_MAX 4096
@@ -318,6 +319,78 @@ int mce_model_grad(mce_model_t m, const float *X, const float *Y, int64_t count,
 int mce_count_oriented_noalloc(const int32_t *d_row_ptr, const int32_t *d_split,
                                const int32_t *d_col_split, const int32_t *d_roots,
                                int64_t num_roots, uint64_t *d_hist, void *stream);
+
+/* ---- serving ------------------------------------------------------------ */
+/* A serving session answers requests against a resident graph from one
+ * persistent kernel (no counterpart in the reference, which runs one graph
+ * per process).  A request is a seed vertex; its answer is the number of
+ * maximal cliques of the seed's 2-hop ego subgraph, the graph that
+ * mce_ego_subgraph (mce_gen.h) builds with the same cap.  Each resident
+ * block (a slot) takes one request at a time; requests are admitted as
+ * slots free up, so a request never waits for a batch to fill.  The graph
+ * handle must outlive the session and must not be reloaded meanwhile.
+ * While requests keep coming the kernel stays resident on every SM; a
+ * cudaDeviceSynchronize by the caller returns only after the slots have
+ * been idle for idle_ms (or after mce_serve_close).                       */
+typedef struct mce_serve *mce_serve_t;
+
+typedef struct mce_serve_opts {
+  int32_t ego_cap;  /* ego-graph vertex cap, 2..4096 (default 1024)          */
+  int32_t slots;    /* concurrent requests; <= 0: as many blocks as fit      */
+  uint32_t ring;    /* requests submitted and not yet polled (default 4096)  */
+  int32_t idle_ms;  /* a slot idle this long leaves; the next submit or poll
+                       relaunches the kernel (default 1000)                  */
+  int64_t max_arcs; /* arcs per ego graph; 0: 128 * ego_cap (capped at
+                       ego_cap * (ego_cap - 1)).  More: status MCE_ELIMIT    */
+  int64_t max_nodes; /* search-tree nodes per request; 0: no limit.  More:
+                        status MCE_ELIMIT (the request's search stops)       */
+  int64_t reserved[3];
+} mce_serve_opts_t;
+
+typedef struct mce_serve_result {
+  uint64_t count;     /* maximal cliques of the ego graph                   */
+  int64_t seed;
+  int32_t status;     /* MCE_OK, MCE_EINVAL (seed out of range) or
+                         MCE_ELIMIT (see `limits`)                          */
+  int32_t ego_n;      /* ego-graph vertices                                 */
+  int32_t ego_arcs;   /* ego-graph arcs (2 x edges)                         */
+  uint32_t limits;    /* MCE_SERVE_* bits of the limits a request hit       */
+  uint64_t device_ns; /* time the slot spent on the request                 */
+} mce_serve_result_t;
+
+#define MCE_SERVE_OVER_BUDGET 0x20u /* search passed max_nodes             */
+#define MCE_SERVE_OVER_ARCS 0x40u   /* ego graph above max_arcs             */
+#define MCE_SERVE_TOO_WIDE 0x0Cu    /* a root with more than 256 later (0x8)
+                                       or a slab's earlier rows (0x4)       */
+
+typedef struct mce_serve_stats {
+  int32_t slots, running;
+  uint32_t ring, pad;
+  uint64_t submitted, served, tree_nodes;
+  int64_t kernel_launches;
+  uint64_t arena_bytes, slab_bytes;
+} mce_serve_stats_t;
+
+void mce_serve_opts_default(mce_serve_opts_t *o);
+/* Start a session on graph g (uploaded with mce_graph_upload). */
+int mce_serve_open(mce_graph_t g, const mce_serve_opts_t *opts, mce_serve_t *out);
+/* Publish one request; *id_out names it.  MCE_ELIMIT: `ring` requests are
+ * outstanding - poll some first.                                          */
+int mce_serve_submit(mce_serve_t s, int64_t seed, uint64_t *id_out);
+/* MCE_OK and *res filled once the answer is there (each id is taken once),
+ * MCE_EAGAIN while it is not.                                             */
+int mce_serve_poll(mce_serve_t s, uint64_t id, mce_serve_result_t *res);
+/* Poll until done or timeout_ms (< 0: no limit) -> MCE_ETIMEOUT.          */
+int mce_serve_wait(mce_serve_t s, uint64_t id, int64_t timeout_ms, mce_serve_result_t *res);
+/* Open-loop trace: request i (seeds[i]) is submitted arrival_us[i]
+ * microseconds after the call (NULL: all at once, as the ring admits);
+ * results[i] and latency_us[i] (completion seen minus arrival; may be NULL)
+ * are filled.                                                             */
+int mce_serve_run(mce_serve_t s, const int64_t *seeds, const double *arrival_us, int64_t count,
+                  int64_t timeout_ms, mce_serve_result_t *results, double *latency_us);
+int mce_serve_stats(mce_serve_t s, mce_serve_stats_t *st);
+/* Finish the published requests, stop the kernel and free the session.    */
+int mce_serve_close(mce_serve_t s);
 
 /* Text for a status code. */
 const char *mce_strerror(int code);

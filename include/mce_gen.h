@@ -53,10 +53,11 @@ int mce_gen_permute(const mce_hgraph_t *in, uint64_t seed, mce_hgraph_t *out);
  * through the single-graph path).                                          */
 int mce_hgraph_union(const mce_hgraph_t *batch, mce_hgraph_t *out);
 
-/* The 2-hop ego subgraph of `seed_vertex`: the seed, its neighbours, then
- * 2-hop vertices in ascending id order until `cap` vertices are taken;
- * relabelled 0..k-1 in that order.  If vertex_map_out is not NULL it
- * receives the original ids (cap entries).                                 */
+/* The 2-hop ego subgraph of `seed_vertex`: the seed, its neighbours in row
+ * order, then 2-hop vertices in discovery order (the rows of the
+ * neighbours, in turn) until `cap` vertices are taken; relabelled 0..k-1 in
+ * ascending original id.  If vertex_map_out is not NULL it receives the
+ * original ids (cap entries).  The serving kernel extracts the same graph. */
 int mce_ego_subgraph(const int32_t *row_ptr, const int32_t *col, int64_t n,
                      int64_t seed_vertex, int64_t cap, mce_hgraph_t *out,
                      int32_t *vertex_map_out);

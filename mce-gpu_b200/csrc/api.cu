@@ -269,6 +269,19 @@ int ensure_slab(mce_graph *g, size_t bytes) {
 
 }  // namespace
 
+namespace mce {
+// device CSR of a graph handle, for the serving sessions (serve.cu)
+int graph_device_view(const struct ::mce_graph *g, const int32_t **rp, const int32_t **col,
+                      int64_t *n, int *device) {
+  if (!g || !g->rp) return MCE_ESTATE;
+  *rp = g->rp;
+  *col = g->col;
+  *n = g->n;
+  *device = g->device;
+  return MCE_OK;
+}
+}  // namespace mce
+
 extern "C" {
 
 void mce_opts_default(mce_opts_t *o) {
@@ -298,6 +311,7 @@ const char *mce_strerror(int code) {
     case MCE_ETIMEOUT: return "device wait limit reached";
     case MCE_ENODEV: return "no usable CUDA device";
     case MCE_ESTATE: return "call out of order";
+    case MCE_EAGAIN: return "not finished yet";
     default: return "unknown error";
   }
 }

@@ -27,6 +27,7 @@
 #include <cstring>
 
 #include "common.cuh"
+#include "engine.cuh"
 #include "kernels.h"
 #include "queue.cuh"
 
@@ -38,446 +39,6 @@ __global__ void queue_init_kernel(QueueView q) {
 }
 
 namespace {
-
-using u64 = unsigned long long;
-
-template <typename W>
-struct WOps;
-template <>
-struct WOps<uint32_t> {
-  static __device__ __forceinline__ int popc(uint32_t x) { return __popc(x); }
-  static __device__ __forceinline__ int ctz(uint32_t x) { return __ffs(x) - 1; }
-  static __device__ __forceinline__ uint32_t bit(int i) { return 1u << i; }
-  static __device__ __forceinline__ uint32_t low(int d) { return d >= 32 ? ~0u : ((1u << d) - 1u); }
-};
-template <>
-struct WOps<u64> {
-  static __device__ __forceinline__ int popc(u64 x) { return __popcll(x); }
-  static __device__ __forceinline__ int ctz(u64 x) { return __ffsll((long long)x) - 1; }
-  static __device__ __forceinline__ u64 bit(int i) { return 1ull << i; }
-  static __device__ __forceinline__ u64 low(int d) { return d >= 64 ? ~0ull : ((1ull << d) - 1ull); }
-};
-
-constexpr int REG_BLOCK = 256;  // 8 warps
-constexpr int MEM_BLOCK = 128;  // 4 warps
-constexpr int REG_CHUNK = 4;    // roots fetched per atomic by the register engine
-
-__device__ __forceinline__ int warp_incl_scan(int x) {
-  const int lane = (int)lane_id();
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int y = __shfl_up_sync(MCE_FULL, x, o);
-    if (lane >= o) x += y;
-  }
-  return x;
-}
-
-// index t of the chunk item owning flattened element e: the last t with
-// off[t] <= e (off is the exclusive prefix of the items' list lengths).
-__device__ __forceinline__ int chunk_owner(const int32_t *off, int e) {
-  int lo = 0, hi = 32;
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if (off[mid] <= e)
-      lo = mid + 1;
-    else
-      hi = mid;
-  }
-  return lo - 1;
-}
-
-__device__ __forceinline__ int lower_bound_g(const int32_t *a, int n, int32_t key) {
-  int lo = 0, len = n;
-  while (len > 0) {
-    const int half = len >> 1;
-    const bool right = a[lo + half] < key;
-    lo = right ? lo + half + 1 : lo;
-    len = right ? len - half - 1 : half;
-  }
-  return lo;
-}
-
-__device__ __forceinline__ uint32_t hash_word(u64 x) {
-  return (uint32_t)((x * 0x9E3779B97F4A7C15ull) >> 32);
-}
-
-// warp-uniform answer to "should this warp hand a child to the queue?"
-__device__ __forceinline__ bool wants_task(const QueueView &q) {
-  int w = 0;
-  if (lane_id() == 0) w = q_wants(q) ? 1 : 0;
-  return __shfl_sync(MCE_FULL, w, 0) != 0;
-}
-
-// Per-root outputs shared by donor and takers: accumulate.
-__device__ __forceinline__ void root_done(const BKArgs &a, int32_t r, u64 nodes, u64 cnt) {
-  if (lane_id() != 0) return;
-  if (a.root_nodes && nodes) atomicAdd(&a.root_nodes[r], nodes);
-  if (a.root_count && cnt) atomicAdd(&a.root_count[r], cnt);
-  if (a.graph_count && cnt) atomicAdd(&a.graph_count[a.graph_of[r]], cnt);
-}
-
-// Idle phase shared by the engines: take tasks until no work is left.
-// `run(words)` processes one task whose words were stored by `put`.
-template <typename Put, typename Run>
-__device__ void idle_phase(const BKArgs &a, Put put, Run run) {
-  const QueueView &q = a.q;
-  const uint32_t lane = lane_id();
-  if (lane == 0) atomicAdd(&q.hdr->idle, 1u);
-  uint32_t last_epoch = 0;
-  uint64_t t_last = 0;
-  if (lane == 0) {
-    last_epoch = ld_volatile(&q.hdr->epoch);
-    t_last = globaltimer_ns();
-  }
-  uint32_t ns = 64;
-  for (;;) {
-    if (q_pop(q, put)) {
-      if (lane == 0) atomicSub(&q.hdr->idle, 1u);
-      run();
-      if (lane == 0) {
-        atomicSub(&q.hdr->work, 1u);
-        atomicAdd(&q.hdr->epoch, 1u);
-        atomicAdd(&q.hdr->idle, 1u);
-        t_last = globaltimer_ns();
-      }
-      ns = 64;
-      continue;
-    }
-    int stop = 0;
-    if (lane == 0) {
-      if (ld_volatile(&q.hdr->work) == 0) {
-        stop = 1;
-      } else {
-        const uint32_t e = ld_volatile(&q.hdr->epoch);
-        const uint64_t now = globaltimer_ns();
-        if (e != last_epoch) {
-          last_epoch = e;
-          t_last = now;
-        } else if (now - t_last > a.wait_limit_ns) {
-          atomicOr(a.err, MCE_ERR_WAIT_TIMEOUT);  // no progress anywhere: give up
-          stop = 1;
-        }
-      }
-    }
-    if (__shfl_sync(MCE_FULL, stop, 0)) break;
-    __nanosleep(ns);
-    if (ns < 8192) ns <<= 1;
-  }
-  if (lane == 0) atomicSub(&q.hdr->idle, 1u);
-}
-
-// ---------------------------------------------------------------------------
-// Register engine: d+ <= 32 * NR; lane i holds rows i (and i + 32).
-// ---------------------------------------------------------------------------
-template <typename Word, int NR>
-struct RegSmem {
-  Word rows[32 * NR];       // induced-subgraph rows while they are built
-  Word xs[32];              // earlier-neighbour rows while they are built
-  Word stk[32 * NR + 1][4]; // DFS frames: P, X, branch set, chosen set
-  int32_t pl[32 * NR];      // the root's later neighbours (sorted ids), padded
-  int32_t off[32];          // chunk prefix offsets
-  int32_t beg[32];          // chunk list starts
-};
-
-// Per-warp slab of the register engine, in Words: a hash set used while the
-// earlier-neighbour rows are built (2 * REG_XCAP), the distinct rows
-// (REG_XCAP) and the rows adjacent to the current branch (REG_XCAP).
-template <typename Word>
-struct RegSlab {
-  Word *hash, *xr, *xl;
-};
-
-template <typename Word>
-__device__ __forceinline__ RegSlab<Word> reg_slab(const BKArgs &a, int64_t gw) {
-  Word *base = (Word *)(a.slab + (size_t)gw * a.slab_words);
-  RegSlab<Word> s;
-  s.hash = base;
-  s.xr = base + 2 * REG_XCAP;
-  s.xl = s.xr + REG_XCAP;
-  return s;
-}
-
-template <typename Word, int NR>
-__device__ __forceinline__ Word row_of(Word r0, Word r1, int j) {
-  if constexpr (NR == 2) return __shfl_sync(MCE_FULL, j >= 32 ? r1 : r0, j & 31);
-  return __shfl_sync(MCE_FULL, r0, j & 31);
-}
-
-// Encoded state of the root a warp currently works on.
-template <typename Word>
-struct RegRoot {
-  int32_t r = -1;
-  int d = 0, nX = 0;
-  Word r0 = 0, r1 = 0;
-};
-
-template <typename Word, int NR>
-__device__ void reg_encode(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<Word> &sl,
-                           int32_t r, RegRoot<Word> &rt) {
-  using O = WOps<Word>;
-  const int lane = (int)lane_id();
-  const uint32_t lt = (1u << lane) - 1u;
-  const int32_t sb = a.split[r], d = a.rp[r + 1] - sb, ub = a.rp[r], u = sb - ub;
-
-  // setup_stack_original_L1_IP (mce/mce_utils.cuh:565-611): P = N+(r)
-#pragma unroll
-  for (int k = 0; k < NR; ++k) {
-    const int i = lane + 32 * k;
-    sm.pl[i] = i < d ? a.cs[sb + i] : INT_MAX;
-    sm.rows[i] = 0;
-  }
-  __syncwarp();
-
-  // warp_sorted_count_and_encode_full (mce/mce_utils.cuh:90-117): bit (j, i)
-  // and (i, j) for every later neighbour w = P[i] of v = P[j].  The later
-  // lists of 32 P vertices are flattened over the lanes.
-  for (int c = 0; c * 32 < d; ++c) {
-    const int items = min(32, d - c * 32);
-    int vb = 0, vlen = 0;
-    if (lane < items) {
-      const int32_t v = sm.pl[c * 32 + lane];
-      vb = a.split[v];
-      vlen = a.rp[v + 1] - vb;
-    }
-    const int incl = warp_incl_scan(vlen);
-    const int T = __shfl_sync(MCE_FULL, incl, 31);
-    sm.off[lane] = incl - vlen;
-    sm.beg[lane] = vb;
-    __syncwarp();
-    for (int e = lane; e < T; e += 32) {
-      const int t = chunk_owner(sm.off, e);
-      const int32_t w = a.cs[sm.beg[t] + (e - sm.off[t])];
-      const int i = lower_bound_g(sm.pl, 32 * NR, w);
-      if (i < d && sm.pl[i] == w) {
-        const int j = c * 32 + t;
-        atomicOr(&sm.rows[j], O::bit(i));
-        atomicOr(&sm.rows[i], O::bit(j));
-      }
-    }
-    __syncwarp();
-  }
-  rt.r0 = sm.rows[lane];
-  rt.r1 = 0;
-  if constexpr (NR == 2) rt.r1 = sm.rows[lane + 32];
-
-  // Earlier neighbours x of r: row(x) = N(x) & P, kept once per distinct
-  // non-empty value; x is earlier than every vertex of P, so N(x) & P lies
-  // in N+(x).
-  int nX = 0;
-  if (u > 0) {
-    int hc = 32;
-    while (hc < 2 * u && hc < 2 * REG_XCAP) hc <<= 1;
-    for (int i = lane; i < hc; i += 32) sl.hash[i] = 0;
-    __syncwarp();
-    for (int c = 0; c * 32 < u; ++c) {
-      const int items = min(32, u - c * 32);
-      int xb = 0, xlen = 0;
-      if (lane < items) {
-        const int32_t x = a.cs[ub + c * 32 + lane];
-        xb = a.split[x];
-        xlen = a.rp[x + 1] - xb;
-      }
-      sm.xs[lane] = 0;
-      const int incl = warp_incl_scan(xlen);
-      const int T = __shfl_sync(MCE_FULL, incl, 31);
-      sm.off[lane] = incl - xlen;
-      sm.beg[lane] = xb;
-      __syncwarp();
-      for (int e = lane; e < T; e += 32) {
-        const int t = chunk_owner(sm.off, e);
-        const int32_t w = a.cs[sm.beg[t] + (e - sm.off[t])];
-        const int i = lower_bound_g(sm.pl, 32 * NR, w);
-        if (i < d && sm.pl[i] == w) atomicOr(&sm.xs[t], O::bit(i));
-      }
-      __syncwarp();
-      const Word row = sm.xs[lane];
-      bool fresh = false;
-      if (lane < items && row != 0) {
-        uint32_t h = hash_word((u64)row) & (uint32_t)(hc - 1);
-        for (int probe = 0; probe < hc; ++probe) {
-          const Word old = atomicCAS(&sl.hash[h], (Word)0, row);
-          if (old == 0) {
-            fresh = true;
-            break;
-          }
-          if (old == row) break;
-          h = (h + 1) & (uint32_t)(hc - 1);
-        }
-      }
-      const uint32_t mk = __ballot_sync(MCE_FULL, fresh);
-      if (fresh) sl.xr[nX + __popc(mk & lt)] = row;
-      nX += __popc(mk);
-      __syncwarp();
-    }
-  }
-  rt.r = r;
-  rt.d = d;
-  rt.nX = nX;
-}
-
-// Walk the subtree under node (P, X, S) of root rt.r.  For the root itself
-// S = 0; for a task S holds the vertices chosen above the node.
-template <typename Word, int NR>
-__device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<Word> &sl,
-                         const RegRoot<Word> &rt, Word P, Word X, Word S, u64 &h0, u64 &h1,
-                         u64 &nodes, u64 &cnt) {
-  using O = WOps<Word>;
-  const int lane = (int)lane_id();
-  const uint32_t lt = (1u << lane) - 1u;
-  const Word r0 = rt.r0, r1 = rt.r1;
-  const int nX = rt.nX;
-  const bool share = a.q.hdr != nullptr;
-  // pivot of the start node (select_pivot_from_P / _and_Xp, mce/mce_utils.cuh:338-402)
-  int start_k = 0;
-  {
-    const Word cand = P | X;
-    const int pc = O::popc(P);
-    int k = 0;
-    bool el = false;
-    if ((cand >> lane) & 1) {
-      const int s = O::popc(P & r0);
-      k = ((s + 1) << 7) | (127 - lane);
-      el = ((X >> lane) & 1) && s == pc;
-    }
-    if constexpr (NR == 2) {
-      if ((cand >> (lane + 32)) & 1) {
-        const int s = O::popc(P & r1);
-        k = max(k, ((s + 1) << 7) | (127 - (lane + 32)));
-        el = el || (((X >> (lane + 32)) & 1) && s == pc);
-      }
-    }
-    if (__any_sync(MCE_FULL, el) || P == 0) return;
-    k = (int)__reduce_max_sync(MCE_FULL, (unsigned)k);
-    start_k = k;
-  }
-  // apply_pivot_to_first_level (:204-216) / apply_pivot_to_next_level (:218-239)
-  Word B = P & ~row_of<Word, NR>(r0, r1, 127 - (start_k & 127));
-  // Leaf filter: for the root it is rebuilt at every depth-0 branch (rows
-  // adjacent to that branch vertex); for a task it is built once (rows
-  // containing the whole chosen set).
-  const bool per_branch = (S == 0);
-  int nL = 0;
-  if (!per_branch && nX > 0) {
-    for (int i0 = 0; i0 < nX; i0 += 32) {
-      const int i = i0 + lane;
-      const Word row = i < nX ? sl.xr[i] : (Word)0;
-      const bool has = i < nX && (row & S) == S;
-      const uint32_t mk = __ballot_sync(MCE_FULL, has);
-      if (has) sl.xl[nL + __popc(mk & lt)] = row;
-      nL += __popc(mk);
-    }
-    __syncwarp();
-  }
-  int depth = 0, recheck = 0;
-  bool want = false;
-  for (;;) {
-    if (B == 0) {  // get_next_candidate found nothing: backtrack (:526-563)
-      if (depth == 0) break;
-      --depth;
-      P = sm.stk[depth][0];
-      X = sm.stk[depth][1];
-      B = sm.stk[depth][2];
-      S = sm.stk[depth][3];
-      continue;
-    }
-    const int v = O::ctz(B);
-    B &= B - 1;
-    const Word vb = O::bit(v);
-    const Word rv = row_of<Word, NR>(r0, r1, v);
-    // populate_xl_and_cl (:321-336): child P' = P & N(v), X' = X & N(v);
-    // v leaves P for X in this frame.
-    const Word Pc = P & rv, Xc = X & rv, Sc = S | vb;
-    P &= ~vb;
-    X |= vb;
-    ++nodes;
-    if (per_branch && depth == 0 && nX > 0) {  // earlier neighbours adjacent to v
-      nL = 0;
-      for (int i0 = 0; i0 < nX; i0 += 32) {
-        const int i = i0 + lane;
-        const Word row = i < nX ? sl.xr[i] : (Word)0;
-        const bool has = (row & vb) != 0;
-        const uint32_t mk = __ballot_sync(MCE_FULL, has);
-        if (has) sl.xl[nL + __popc(mk & lt)] = row;
-        nL += __popc(mk);
-      }
-      __syncwarp();
-    }
-    if (Pc == 0) {
-      // test_maximality (:507-524): P' and X' empty and no earlier
-      // neighbour of the root adjacent to the whole clique.
-      if (Xc == 0) {
-        bool covered = false;
-        for (int i0 = 0; i0 < nL; i0 += 32) {
-          const int i = i0 + lane;
-          const bool hit = i < nL && (sl.xl[i] & Sc) == Sc;
-          if (__any_sync(MCE_FULL, hit)) {
-            covered = true;
-            break;
-          }
-        }
-        if (!covered) {
-          ++cnt;
-          const int bin = O::popc(Sc) - 1;  // clique size - 2
-          if (lane == (bin & 31)) {
-            if (bin < 32)
-              ++h0;
-            else
-              ++h1;
-          }
-        }
-      }
-      continue;
-    }
-    // select_pivot_from_P_and_Xp (:366-402): pivot over P' | X'; an X'
-    // vertex adjacent to all of P' ends the path.
-    const Word cand = Pc | Xc;
-    const int pc = O::popc(Pc);
-    int k = 0;
-    bool el = false;
-    if ((cand >> lane) & 1) {
-      const int s = O::popc(Pc & r0);
-      k = ((s + 1) << 7) | (127 - lane);
-      el = ((Xc >> lane) & 1) && s == pc;
-    }
-    if constexpr (NR == 2) {
-      if ((cand >> (lane + 32)) & 1) {
-        const int s = O::popc(Pc & r1);
-        k = max(k, ((s + 1) << 7) | (127 - (lane + 32)));
-        el = el || (((Xc >> (lane + 32)) & 1) && s == pc);
-      }
-    }
-    if (__any_sync(MCE_FULL, el)) continue;
-    // hand the child to an idle warp (try_dequeue / do_fork_L1,
-    // mce/mce_utils.cuh:872-880,1063-1113)
-    if (share && pc >= a.donate_min &&
-        (nodes >= a.donate_after || (a.policy && a.policy[rt.r]))) {
-      if (--recheck <= 0) {  // the queue state is read every 32 candidate nodes
-        want = wants_task(a.q);
-        recheck = 32;
-      }
-      if (want) {
-        const u64 w0 = (u64)(uint32_t)rt.r, w1 = (u64)Pc, w2 = (u64)Xc, w3 = (u64)Sc;
-        if (q_push(a.q, [&](uint32_t k2) { return k2 == 0 ? w0 : k2 == 1 ? w1 : k2 == 2 ? w2 : w3; }))
-          continue;
-        want = false;
-      }
-    }
-    k = (int)__reduce_max_sync(MCE_FULL, (unsigned)k);
-    if (lane == 0) {
-      sm.stk[depth][0] = P;
-      sm.stk[depth][1] = X;
-      sm.stk[depth][2] = B;
-      sm.stk[depth][3] = S;
-    }
-    __syncwarp();
-    ++depth;
-    P = Pc;
-    X = Xc;
-    S = Sc;
-    // apply_pivot_to_next_level (:218-239)
-    B = Pc & ~row_of<Word, NR>(r0, r1, 127 - (k & 127));
-  }
-}
 
 template <typename Word, int NR>
 __global__ void __launch_bounds__(REG_BLOCK) bk_reg_kernel(BKArgs a, int cls) {
@@ -537,323 +98,6 @@ __global__ void __launch_bounds__(REG_BLOCK) bk_reg_kernel(BKArgs a, int cls) {
   if (h0) atomicAdd(&a.hist[lane + 2], h0);
   if (h1) atomicAdd(&a.hist[lane + 34], h1);
   if (lane == 0 && nodes) atomicAdd(a.nodes, nodes);  // warp-uniform count
-}
-
-// ---------------------------------------------------------------------------
-// Wide engine: any d+ <= 2048, rows of W = ceil(d+/64) words in a slab.
-// ---------------------------------------------------------------------------
-struct MemSmem {
-  int32_t off[32];
-  int32_t beg[32];
-};
-
-struct Slab {
-  int32_t *pl;
-  u64 *rows, *stk, *xs, *xr, *hash;
-  int32_t *xl;
-  int hcap;  // hash set entries: a power of two >= 2 * xcap
-};
-
-__host__ __device__ __forceinline__ int hash_cap(int xcap) {
-  int h = 32;
-  while (h < 2 * xcap) h <<= 1;
-  return h;
-}
-
-__device__ __forceinline__ Slab slab_of(const BKArgs &a, int64_t gw) {
-  const int D = a.dcap, WM = (a.dcap + 63) / 64, XC = a.xcap;
-  u64 *base = a.slab + (size_t)gw * a.slab_words;
-  Slab s;
-  s.rows = base;
-  s.stk = s.rows + (size_t)D * WM;
-  s.xs = s.stk + (size_t)(D + 1) * 4 * WM;
-  s.xr = s.xs + (size_t)32 * WM;
-  s.hash = s.xr + (size_t)XC * WM;
-  s.hcap = hash_cap(XC);
-  s.pl = (int32_t *)(s.hash + (size_t)s.hcap);
-  s.xl = s.pl + D;
-  return s;
-}
-
-struct MemRoot {
-  int32_t r = -1;
-  int d = 0, Wr = 0, nX = 0;
-};
-
-__device__ void mem_encode(const BKArgs &a, MemSmem &sm, const Slab &sl, int32_t r, MemRoot &rt) {
-  const int lane = (int)lane_id();
-  const uint32_t lt = (1u << lane) - 1u;
-  const int32_t sb = a.split[r], d = a.rp[r + 1] - sb, ub = a.rp[r], u = sb - ub;
-  rt.r = r;
-  rt.d = d;
-  rt.nX = 0;
-  if (d > a.dcap || u > a.xcap) {
-    if (lane == 0) atomicOr(a.err, d > a.dcap ? MCE_ERR_DEGREE : MCE_ERR_XROWS);
-    rt.d = 0;
-    return;
-  }
-  const int Wr = (d + 63) >> 6;
-  rt.Wr = Wr;
-  int32_t *pl = sl.pl;
-  u64 *rows = sl.rows;
-  for (int i = lane; i < d; i += 32) pl[i] = a.cs[sb + i];
-  for (int i = lane; i < d * Wr; i += 32) rows[i] = 0;
-  __syncwarp();
-  for (int c = 0; c * 32 < d; ++c) {
-    const int items = min(32, d - c * 32);
-    int vb = 0, vlen = 0;
-    if (lane < items) {
-      const int32_t v = pl[c * 32 + lane];
-      vb = a.split[v];
-      vlen = a.rp[v + 1] - vb;
-    }
-    const int incl = warp_incl_scan(vlen);
-    const int T = __shfl_sync(MCE_FULL, incl, 31);
-    sm.off[lane] = incl - vlen;
-    sm.beg[lane] = vb;
-    __syncwarp();
-    for (int e = lane; e < T; e += 32) {
-      const int t = chunk_owner(sm.off, e);
-      const int32_t w = a.cs[sm.beg[t] + (e - sm.off[t])];
-      const int i = lower_bound_g(pl, d, w);
-      if (i < d && pl[i] == w) {
-        const int j = c * 32 + t;
-        atomicOr(&rows[(size_t)j * Wr + (i >> 6)], 1ull << (i & 63));
-        atomicOr(&rows[(size_t)i * Wr + (j >> 6)], 1ull << (j & 63));
-      }
-    }
-    __syncwarp();
-  }
-  // earlier-neighbour rows: non-empty ones, distinct when one word wide
-  int hc = 32;
-  if (Wr == 1) {
-    while (hc < 2 * u && hc < sl.hcap) hc <<= 1;
-    for (int i = lane; i < hc; i += 32) sl.hash[i] = 0;
-  }
-  int nX = 0;
-  for (int c = 0; c * 32 < u; ++c) {
-    const int items = min(32, u - c * 32);
-    int xb = 0, xlen = 0;
-    if (lane < items) {
-      const int32_t x = a.cs[ub + c * 32 + lane];
-      xb = a.split[x];
-      xlen = a.rp[x + 1] - xb;
-    }
-    for (int i = lane; i < 32 * Wr; i += 32) sl.xs[i] = 0;
-    const int incl = warp_incl_scan(xlen);
-    const int T = __shfl_sync(MCE_FULL, incl, 31);
-    sm.off[lane] = incl - xlen;
-    sm.beg[lane] = xb;
-    __syncwarp();
-    for (int e = lane; e < T; e += 32) {
-      const int t = chunk_owner(sm.off, e);
-      const int32_t w = a.cs[sm.beg[t] + (e - sm.off[t])];
-      const int i = lower_bound_g(pl, d, w);
-      if (i < d && pl[i] == w) atomicOr(&sl.xs[(size_t)t * Wr + (i >> 6)], 1ull << (i & 63));
-    }
-    __syncwarp();
-    bool keep = false;
-    if (lane < items) {
-      for (int w = 0; w < Wr; ++w) keep |= sl.xs[(size_t)lane * Wr + w] != 0;
-      if (keep && Wr == 1) {
-        const u64 row = sl.xs[lane];
-        uint32_t h = hash_word(row) & (uint32_t)(hc - 1);
-        keep = false;
-        for (int probe = 0; probe < hc; ++probe) {
-          const u64 old = atomicCAS(&sl.hash[h], 0ull, row);
-          if (old == 0) {
-            keep = true;
-            break;
-          }
-          if (old == row) break;
-          h = (h + 1) & (uint32_t)(hc - 1);
-        }
-      }
-    }
-    const uint32_t mk = __ballot_sync(MCE_FULL, keep);
-    if (keep) {
-      const int pos = nX + __popc(mk & lt);
-      for (int w = 0; w < Wr; ++w) sl.xr[(size_t)pos * Wr + w] = sl.xs[(size_t)lane * Wr + w];
-    }
-    nX += __popc(mk);
-    __syncwarp();
-  }
-  rt.nX = nX;
-}
-
-// Walk the subtree under frame 0 of the slab stack (P, X, S already there).
-__device__ void mem_tree(const BKArgs &a, const Slab &sl, const MemRoot &rt, u64 &h0, u64 &h1,
-                         u64 &nodes, u64 &cnt) {
-  const int lane = (int)lane_id();
-  const uint32_t lt = (1u << lane) - 1u;
-  const int d = rt.d, Wr = rt.Wr, nX = rt.nX;
-  const u64 *rows = sl.rows;
-  const bool share = a.q.hdr != nullptr;
-  u64 *F0 = sl.stk;
-  // pivot of the start node
-  int s_base = 0;  // chosen vertices above frame 0
-  {
-    int pc = 0, sc = 0;
-    if (lane < Wr) {
-      pc = __popcll(F0[lane]);
-      sc = __popcll(F0[3 * Wr + lane]);
-    }
-    pc = (int)__reduce_add_sync(MCE_FULL, (unsigned)pc);
-    s_base = (int)__reduce_add_sync(MCE_FULL, (unsigned)sc);
-    int k = 0;
-    bool el = false;
-    for (int uu = lane; uu < d; uu += 32) {
-      const int uw = uu >> 6;
-      const u64 ub2 = 1ull << (uu & 63);
-      const bool inP = (F0[uw] & ub2) != 0, inX = (F0[Wr + uw] & ub2) != 0;
-      if (!(inP || inX)) continue;
-      int s = 0;
-      const u64 *ru = rows + (size_t)uu * Wr;
-      for (int w = 0; w < Wr; ++w) s += __popcll(F0[w] & ru[w]);
-      k = max(k, ((s + 1) << 11) | (2047 - uu));
-      el = el || (inX && s == pc);
-    }
-    if (__any_sync(MCE_FULL, el) || pc == 0) return;
-    k = (int)__reduce_max_sync(MCE_FULL, (unsigned)k);
-    const int piv = 2047 - (k & 2047);
-    if (lane < Wr) F0[2 * Wr + lane] = F0[lane] & ~rows[(size_t)piv * Wr + lane];
-    __syncwarp();
-  }
-  const bool per_branch = (s_base == 0);
-  int nL = 0;
-  if (!per_branch && nX > 0) {  // rows containing the whole chosen set
-    const u64 *S0 = F0 + 3 * Wr;
-    for (int i0 = 0; i0 < nX; i0 += 32) {
-      const int i = i0 + lane;
-      bool has = false;
-      if (i < nX) {
-        has = true;
-        for (int w = 0; w < Wr && has; ++w) has = (sl.xr[(size_t)i * Wr + w] & S0[w]) == S0[w];
-      }
-      const uint32_t m2 = __ballot_sync(MCE_FULL, has);
-      if (has) sl.xl[nL + __popc(m2 & lt)] = i;
-      nL += __popc(m2);
-    }
-    __syncwarp();
-  }
-  int depth = 0, recheck = 0;
-  bool want = false;
-  for (;;) {
-    u64 *F = sl.stk + (size_t)depth * 4 * Wr;
-    u64 *Fp = F, *Fx = F + Wr, *Fb = F + 2 * Wr, *Fs = F + 3 * Wr;
-    // lowest set bit of the branch set
-    const u64 bw = lane < Wr ? Fb[lane] : 0ull;
-    const uint32_t mk = __ballot_sync(MCE_FULL, bw != 0);
-    if (!mk) {
-      if (depth == 0) break;
-      --depth;
-      continue;
-    }
-    const int wl = __ffs(mk) - 1;
-    const u64 word = __shfl_sync(MCE_FULL, bw, wl);
-    const int v = wl * 64 + __ffsll((long long)word) - 1;
-    const int vw = v >> 6;
-    const u64 vbit = 1ull << (v & 63);
-    if (lane == 0) {
-      Fb[vw] &= ~vbit;
-      Fp[vw] &= ~vbit;
-      Fx[vw] |= vbit;
-    }
-    __syncwarp();
-    ++nodes;
-    u64 *C = F + 4 * Wr;
-    int pc = 0;
-    bool xnz = false;
-    if (lane < Wr) {
-      const u64 rw = rows[(size_t)v * Wr + lane];
-      const u64 pcw = Fp[lane] & rw, xcw = Fx[lane] & rw;
-      C[lane] = pcw;
-      C[Wr + lane] = xcw;
-      C[3 * Wr + lane] = Fs[lane] | (lane == vw ? vbit : 0ull);
-      pc = __popcll(pcw);
-      xnz = xcw != 0;
-    }
-    pc = (int)__reduce_add_sync(MCE_FULL, (unsigned)pc);
-    xnz = __any_sync(MCE_FULL, xnz);
-    if (per_branch && depth == 0 && nX > 0) {
-      nL = 0;
-      for (int i0 = 0; i0 < nX; i0 += 32) {
-        const int i = i0 + lane;
-        const bool has = i < nX && (sl.xr[(size_t)i * Wr + vw] & vbit);
-        const uint32_t m2 = __ballot_sync(MCE_FULL, has);
-        if (has) sl.xl[nL + __popc(m2 & lt)] = i;
-        nL += __popc(m2);
-      }
-    }
-    __syncwarp();
-    if (pc == 0) {
-      if (!xnz) {
-        const u64 *Cs = C + 3 * Wr;
-        bool covered = false;
-        for (int i0 = 0; i0 < nL; i0 += 32) {
-          const int i = i0 + lane;
-          bool hit = false;
-          if (i < nL) {
-            const u64 *xrow = sl.xr + (size_t)sl.xl[i] * Wr;
-            hit = true;
-            for (int w = 0; w < Wr && hit; ++w) hit = (xrow[w] & Cs[w]) == Cs[w];
-          }
-          if (__any_sync(MCE_FULL, hit)) {
-            covered = true;
-            break;
-          }
-        }
-        if (!covered) {
-          ++cnt;
-          const int bin = s_base + depth;  // clique size - 2
-          if (bin < 64) {
-            if (lane == (bin & 31)) {
-              if (bin < 32)
-                ++h0;
-              else
-                ++h1;
-            }
-          } else if (lane == 0 && bin + 2 < MCE_HIST_MAX) {
-            atomicAdd(&a.hist[bin + 2], 1ull);
-          }
-        }
-      }
-      continue;
-    }
-    int k = 0;
-    bool el = false;
-    for (int uu = lane; uu < d; uu += 32) {
-      const int uw = uu >> 6;
-      const u64 ub2 = 1ull << (uu & 63);
-      const bool inP = (C[uw] & ub2) != 0, inX = (C[Wr + uw] & ub2) != 0;
-      if (!(inP || inX)) continue;
-      int s = 0;
-      const u64 *ru = rows + (size_t)uu * Wr;
-      for (int w = 0; w < Wr; ++w) s += __popcll(C[w] & ru[w]);
-      k = max(k, ((s + 1) << 11) | (2047 - uu));
-      el = el || (inX && s == pc);
-    }
-    if (__any_sync(MCE_FULL, el)) continue;
-    if (share && pc >= a.donate_min &&
-        (nodes >= a.donate_after || (a.policy && a.policy[rt.r])) &&
-        (--recheck <= 0 ? (recheck = 32, want = wants_task(a.q)) : want)) {
-      const int WM = (a.dcap + 63) >> 6;
-      const u64 *Cp = C, *Cx = C + Wr, *Cs = C + 3 * Wr;
-      if (q_push(a.q, [&](uint32_t k2) -> u64 {
-            if (k2 == 0) return (u64)(uint32_t)rt.r;
-            const uint32_t part = (k2 - 1) / WM, w = (k2 - 1) % WM;
-            if ((int)w >= Wr) return 0ull;
-            return part == 0 ? Cp[w] : part == 1 ? Cx[w] : Cs[w];
-          }))
-        continue;
-      want = false;
-    }
-    k = (int)__reduce_max_sync(MCE_FULL, (unsigned)k);
-    const int up = 2047 - (k & 2047);
-    if (lane < Wr) C[2 * Wr + lane] = C[lane] & ~rows[(size_t)up * Wr + lane];
-    __syncwarp();
-    ++depth;
-  }
 }
 
 __global__ void __launch_bounds__(MEM_BLOCK) bk_mem_kernel(BKArgs a, int cls) {
@@ -937,6 +181,7 @@ __global__ void __launch_bounds__(MEM_BLOCK) bk_mem_kernel(BKArgs a, int cls) {
 }
 
 }  // namespace
+
 
 size_t bk_slab_words(int cls, int dcap, int xcap) {
   if (cls == CLS_R32 || cls == CLS_R64) return 4 * (size_t)REG_XCAP;  // hash, rows, leaf list

@@ -14,6 +14,8 @@
 #define MCE_ERR_XROWS 0x4u          // earlier-neighbour rows above the slab capacity
 #define MCE_ERR_DEGREE 0x8u         // later degree above the engine's width
 #define MCE_ERR_QUEUE 0x10u         // task queue misuse
+#define MCE_ERR_BUDGET 0x20u        // a search passed its node budget (serving)
+#define MCE_ERR_ARCS 0x40u          // an ego graph above the arena's arc capacity (serving)
 
 // Check a CUDA call; on failure record it and return MCE_ECUDA from the caller.
 #define MCE_CUDA(call)                                                        \
@@ -50,6 +52,10 @@ __device__ __forceinline__ void st_release(uint32_t *p, uint32_t v) {
 
 __device__ __forceinline__ uint32_t ld_volatile(const uint32_t *p) {
   return *(const volatile uint32_t *)p;
+}
+
+__device__ __forceinline__ unsigned long long ld_volatile(const unsigned long long *p) {
+  return *(const volatile unsigned long long *)p;
 }
 
 // Grid-wide barrier for a kernel whose blocks are all resident (launched with

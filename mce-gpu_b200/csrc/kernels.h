@@ -87,6 +87,7 @@ struct BKArgs {
   uint32_t donate_after;         // ... once this many nodes of the root/task were walked
   uint64_t wait_limit_ns;        // an idle warp gives up after this long without progress
   const uint8_t *policy;         // nullable [n]: 1 = root may share subtrees at once
+  unsigned long long node_budget;  // 0: none; else a tree stops past this many nodes
 };
 
 // Launch the engine of one class.  warps_out: number of warps launched (slab sizing).

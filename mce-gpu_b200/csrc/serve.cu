@@ -1,0 +1,887 @@
+// Serving: a device-resident request loop over a resident graph.
+//
+// No counterpart in the reference, which runs one graph per process
+// (src/main.cu).  A request is a seed vertex; its answer is the number of
+// maximal cliques (size >= 2) of the seed's 2-hop ego subgraph: the seed,
+// its neighbours in row order, then 2-hop vertices in discovery order, at
+// most `ego_cap` vertices, relabelled in ascending id order
+// (mce_ego_subgraph builds the same graph on the host).
+//
+// One persistent kernel serves a session.  Each block is a slot: it claims
+// the next published request, extracts the ego subgraph into its own
+// arena, peels and orients it with block barriers (the same synchronous
+// rounds and orientation rule as peel.cu / orient.cu), searches its roots
+// with its 8 warps (the engines of engine.cuh) and writes the count back to
+// mapped host memory.  Requests that arrive while others run are taken by
+// whichever slot frees first, so unrelated requests overlap on the device:
+// continuous batching at request granularity with no launch per request.
+//
+// Ring protocol (mapped pinned host memory): the host writes entry
+// id % ring, then releases `tail` = id + 1.  On the device one waiting
+// thread at a time (the poller duty, at most every SV_POLL_NS) reads the
+// host tail and stop flag over the bus and mirrors them into device memory;
+// waiting slots watch the mirror and claim with a CAS on `next` only when a
+// request is published, so a slot that leaves never holds an unserved
+// request.  A slot with nothing to do for `idle_ms` leaves; the host
+// relaunches the kernel when requests are pending and no slot is left.
+// Every device wait is bounded.
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+#include "common.cuh"
+#include "engine.cuh"
+#include "kernels.h"
+
+namespace mce {
+
+namespace {
+
+constexpr int SV_BLOCK = 256;
+constexpr int SV_WARPS = SV_BLOCK / 32;
+constexpr int SV_DCAP = 256;            // widest root (later neighbours) a slot searches
+constexpr uint64_t SV_POLL_NS = 500;    // host tail read at most this often
+constexpr int SV_MAX_EGO = 16384;
+
+struct SvEntry {             // one request, in mapped host memory
+  int64_t seed;              // host -> device
+  unsigned long long count;  // device -> host
+  unsigned long long device_ns;
+  int32_t status, ego_n, ego_arcs;
+  uint32_t limits;           // MCE_ERR_* bits of the limits the request hit
+  uint32_t done;             // id + 1 once the answer is written
+  uint32_t pad;
+};
+
+struct SvHostHdr {           // mapped host memory, host-written
+  uint32_t tail;
+  uint32_t pad0[15];
+  uint32_t stop;
+  uint32_t pad1[15];
+};
+
+struct SvCtl {               // device memory
+  uint32_t next, dtail, dstop, pad;
+  unsigned long long poll_ns, served, nodes;
+};
+
+struct ServeArgs {
+  const int32_t *grp, *gcol;  // resident graph
+  int64_t gn;
+  const SvHostHdr *hdr;       // device views of the mapped ring
+  SvEntry *ent;
+  uint32_t ring;
+  SvCtl *ctl;
+  char *arena;                // per-slot ego-graph arenas
+  size_t arena_bytes;
+  int32_t ego_cap, arc_cap, hcap;
+  unsigned long long *slab;   // per-warp engine scratch: register part, then wide part
+  size_t slab_words, reg_words;
+  uint64_t idle_ns;
+  unsigned long long node_budget;  // per request; 0: none
+};
+
+struct Arena {
+  int32_t *hkey, *hval, *V, *rp, *col, *split, *cs, *deg, *core, *fa, *fb, *cnt;
+  uint32_t *prio, *err;
+  unsigned long long *hist;  // clique sizes above the engines' register bins
+};
+
+__host__ __device__ inline size_t arena_layout(int ego_cap, int arc_cap, int hcap, char *base,
+                                               Arena *a) {
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    char *p = base ? base + off : nullptr;
+    off += (bytes + 255) & ~(size_t)255;
+    return p;
+  };
+  Arena x;
+  x.hkey = (int32_t *)take(4 * (size_t)hcap);
+  x.hval = (int32_t *)take(4 * (size_t)hcap);
+  x.V = (int32_t *)take(4 * (size_t)ego_cap);
+  x.rp = (int32_t *)take(4 * ((size_t)ego_cap + 1));
+  x.col = (int32_t *)take(4 * (size_t)arc_cap);
+  x.split = (int32_t *)take(4 * (size_t)ego_cap);
+  x.cs = (int32_t *)take(4 * (size_t)arc_cap);
+  x.deg = (int32_t *)take(4 * (size_t)ego_cap);
+  x.core = (int32_t *)take(4 * (size_t)ego_cap);
+  x.fa = (int32_t *)take(4 * (size_t)ego_cap);
+  x.fb = (int32_t *)take(4 * (size_t)ego_cap);
+  x.cnt = (int32_t *)take(4 * (size_t)ego_cap);
+  x.prio = (uint32_t *)take(4 * (size_t)ego_cap);
+  x.err = (uint32_t *)take(4);
+  x.hist = (unsigned long long *)take(8 * (size_t)MCE_HIST_MAX);
+  if (a) *a = x;
+  return off;
+}
+
+__device__ __forceinline__ uint32_t ld_acquire_sys(const uint32_t *p) {
+  uint32_t v;
+  asm volatile("ld.acquire.sys.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ uint32_t hslot(int32_t key, int hcap) {
+  return (uint32_t)(((uint64_t)(uint32_t)key * 0x9E3779B97F4A7C15ull) >> 32) & (uint32_t)(hcap - 1);
+}
+
+// local id of a vertex, or -1 (not in the ego graph, or cut by the cap)
+__device__ __forceinline__ int32_t hget(const Arena &A, int hcap, int32_t key) {
+  uint32_t h = hslot(key, hcap);
+  for (int p = 0; p < hcap; ++p) {
+    const int32_t k = A.hkey[h];
+    if (k == key) return A.hval[h];
+    if (k == -1) return -1;
+    h = (h + 1) & (uint32_t)(hcap - 1);
+  }
+  return -1;
+}
+
+// insert key; true if it was absent (then *slot holds its entry)
+__device__ __forceinline__ bool hput(const Arena &A, int hcap, int32_t key, uint32_t *slot) {
+  uint32_t h = hslot(key, hcap);
+  for (int p = 0; p < hcap; ++p) {
+    const int32_t old = atomicCAS(&A.hkey[h], -1, key);
+    if (old == -1) {
+      *slot = h;
+      return true;
+    }
+    if (old == key) return false;
+    h = (h + 1) & (uint32_t)(hcap - 1);
+  }
+  return false;  // cannot happen: the table has twice the cap's entries
+}
+
+// exclusive scan of one value per thread over the block; returns the total
+__device__ __forceinline__ int block_scan(int x, int *excl, int *ws) {
+  const int lane = (int)lane_id(), w = threadIdx.x >> 5;
+  const int incl = warp_incl_scan(x);
+  if (lane == 31) ws[w] = incl;
+  __syncthreads();
+  int base = 0, total = 0;
+#pragma unroll
+  for (int i = 0; i < SV_WARPS; ++i) {
+    base += i < w ? ws[i] : 0;
+    total += ws[i];
+  }
+  *excl = base + incl - x;
+  __syncthreads();
+  return total;
+}
+
+// bitonic sort of buf[0 .. n_pow2) in shared memory
+__device__ void block_sort(int32_t *buf, int n_pow2) {
+  for (int k = 2; k <= n_pow2; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = threadIdx.x; i < n_pow2; i += blockDim.x) {
+        const int p = i ^ j;
+        if (p > i) {
+          const bool up = (i & k) == 0;
+          const int32_t a = buf[i], b = buf[p];
+          if ((a > b) == up) {
+            buf[i] = b;
+            buf[p] = a;
+          }
+        }
+      }
+      __syncthreads();
+    }
+}
+
+struct SvShared {
+  uint32_t req;
+  int32_t k, fcnt, ncnt, todo, level, minv, acnt;
+  uint32_t rootnext;
+  unsigned long long total, nodes;
+  int ws[SV_WARPS];
+};
+
+// Append the not-yet-seen vertices of row [b, e) of the resident graph to
+// the ego list in row order, stopping at the cap.
+__device__ void ego_append_row(const ServeArgs &S, const Arena &A, int32_t b, int32_t e,
+                               SvShared &sh) {
+  const int cap = S.ego_cap, hc = S.hcap;
+  for (int32_t j0 = b; j0 < e; j0 += (int32_t)blockDim.x) {
+    const int k = sh.k;  // read by all before thread 0 updates it below
+    if (k >= cap) break;
+    const int32_t j = j0 + (int32_t)threadIdx.x;
+    bool fresh = false;
+    uint32_t slot = 0;
+    if (j < e) fresh = hput(A, hc, S.gcol[j], &slot);
+    int pos;
+    const int tot = block_scan(fresh ? 1 : 0, &pos, sh.ws);
+    if (fresh) {
+      if (k + pos < cap) {
+        A.hval[slot] = k + pos;
+        A.V[k + pos] = S.gcol[j];
+      } else {
+        A.hval[slot] = -1;  // beyond the cap: not in the ego graph
+      }
+    }
+    if (threadIdx.x == 0) sh.k = min(cap, k + tot);
+    __syncthreads();
+  }
+}
+
+// Build the ego graph of `seed` in the arena: sorted local CSR in rp/col.
+// Returns its vertex count, or -1 if it has more arcs than the arena holds.
+__device__ int ego_extract(const ServeArgs &S, const Arena &A, int64_t seed, int32_t *sortbuf,
+                           SvShared &sh) {
+  const int hc = S.hcap;
+  for (int i = threadIdx.x; i < hc; i += blockDim.x) A.hkey[i] = -1;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t slot = 0;
+    hput(A, hc, (int32_t)seed, &slot);
+    A.hval[slot] = 0;
+    A.V[0] = (int32_t)seed;
+    sh.k = 1;
+  }
+  __syncthreads();
+  ego_append_row(S, A, S.grp[seed], S.grp[seed + 1], sh);  // 1-hop
+  const int k1 = sh.k;
+  for (int i = 1; i < k1; ++i) {  // 2-hop, in discovery order
+    if (sh.k >= S.ego_cap) break;
+    const int32_t u = A.V[i];
+    ego_append_row(S, A, S.grp[u], S.grp[u + 1], sh);
+  }
+  const int n = sh.k;
+  // local ids in ascending resident-graph id
+  int np2 = 1;
+  while (np2 < n) np2 <<= 1;
+  for (int i = threadIdx.x; i < np2; i += blockDim.x) sortbuf[i] = i < n ? A.V[i] : INT_MAX;
+  __syncthreads();
+  block_sort(sortbuf, np2);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const int32_t w = sortbuf[i];
+    A.V[i] = w;
+    uint32_t h = hslot(w, hc);
+    for (int p = 0; p < hc && A.hkey[h] != w; ++p) h = (h + 1) & (uint32_t)(hc - 1);
+    A.hval[h] = i;
+  }
+  __syncthreads();
+  // induced rows: count, scan, fill (filtering a sorted row keeps it sorted)
+  const int lane = (int)lane_id(), w = threadIdx.x >> 5;
+  for (int i = w; i < n; i += SV_WARPS) {
+    const int32_t g = A.V[i], gb = S.grp[g], ge = S.grp[g + 1];
+    int c = 0;
+    for (int32_t j0 = gb; j0 < ge; j0 += 32) {
+      const int32_t j = j0 + lane;
+      const bool in = j < ge && hget(A, hc, S.gcol[j]) >= 0;
+      c += __popc(__ballot_sync(MCE_FULL, in));
+    }
+    if (lane == 0) A.cnt[i] = c;
+  }
+  if (threadIdx.x == 0) sh.acnt = 0;
+  __syncthreads();
+  for (int i0 = 0; i0 < n; i0 += blockDim.x) {
+    const int i = i0 + (int)threadIdx.x;
+    const int base = sh.acnt;
+    int ex;
+    const int tot = block_scan(i < n ? A.cnt[i] : 0, &ex, sh.ws);
+    if (i < n) A.rp[i] = base + ex;
+    if (threadIdx.x == 0) sh.acnt = base + tot;
+    __syncthreads();
+  }
+  const int m = sh.acnt;
+  if (m > S.arc_cap) return -1;
+  if (threadIdx.x == 0) A.rp[n] = m;
+  for (int i = w; i < n; i += SV_WARPS) {
+    const int32_t g = A.V[i], gb = S.grp[g], ge = S.grp[g + 1];
+    int out = A.rp[i];
+    for (int32_t j0 = gb; j0 < ge; j0 += 32) {
+      const int32_t j = j0 + lane;
+      const int32_t loc = j < ge ? hget(A, hc, S.gcol[j]) : -1;
+      const uint32_t mk = __ballot_sync(MCE_FULL, loc >= 0);
+      if (loc >= 0) A.col[out + __popc(mk & ((1u << lane) - 1u))] = loc;
+      out += __popc(mk);
+    }
+  }
+  __syncthreads();
+  return n;
+}
+
+// Degeneracy priorities of the ego graph: synchronous peeling rounds over
+// all levels, the final round keeping priority m (peel.cu's order).
+__device__ void ego_peel(const Arena &A, int n, SvShared &sh) {
+  const int m = A.rp[n];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    A.deg[i] = A.rp[i + 1] - A.rp[i];
+    A.core[i] = -1;
+    A.prio[i] = (uint32_t)m;
+  }
+  if (threadIdx.x == 0) {
+    sh.todo = n;
+    sh.level = 0;
+  }
+  __syncthreads();
+  uint32_t priority = 0;
+  const int lane = (int)lane_id(), w = threadIdx.x >> 5;
+  while (sh.todo > 0) {
+    const int level = sh.level;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      sh.fcnt = 0;
+      sh.minv = INT_MAX;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+      if (A.core[i] == -1) {
+        if (A.deg[i] <= level) {  // == level: a remaining vertex never has less
+          A.core[i] = level;
+          A.fa[atomicAdd(&sh.fcnt, 1)] = i;
+        } else {
+          atomicMin(&sh.minv, A.deg[i]);
+        }
+      }
+    __syncthreads();
+    if (sh.fcnt == 0) {  // no vertex at this level: go to the lowest remaining degree
+      __syncthreads();
+      if (threadIdx.x == 0) sh.level = sh.minv;
+      __syncthreads();
+      continue;
+    }
+    int32_t *F = A.fa, *G = A.fb;
+    for (;;) {
+      const int cnt = sh.fcnt;
+      __syncthreads();
+      if (cnt == 0) break;
+      if (threadIdx.x == 0) {
+        sh.todo -= cnt;
+        sh.ncnt = 0;
+      }
+      __syncthreads();
+      if (sh.todo == 0) break;  // the final round keeps priority m
+      for (int i = threadIdx.x; i < cnt; i += blockDim.x) A.prio[F[i]] = priority;
+      for (int i = w; i < cnt; i += SV_WARPS) {
+        const int v = F[i];
+        for (int j = A.rp[v] + lane; j < A.rp[v + 1]; j += 32) {
+          const int u = A.col[j];
+          if (*(volatile int32_t *)&A.core[u] == -1) {
+            const int old = atomicSub(&A.deg[u], 1);
+            if (old == level + 1) {
+              A.core[u] = level;
+              G[atomicAdd(&sh.ncnt, 1)] = u;
+            }
+          }
+        }
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) sh.fcnt = sh.ncnt;
+      int32_t *t = F;
+      F = G;
+      G = t;
+      ++priority;
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) sh.level = level + 1;
+    __syncthreads();
+  }
+}
+
+// Rows become [earlier | later]; u is later than v iff
+// prio[v] == prio[u] ? v < u : prio[v] < prio[u] (include/main_support.cuh:14).
+__device__ void ego_orient(const Arena &A, int n) {
+  const int lane = (int)lane_id(), w = threadIdx.x >> 5;
+  const uint32_t lt = (1u << lane) - 1u;
+  for (int v = w; v < n; v += SV_WARPS) {
+    const int b = A.rp[v], e = A.rp[v + 1];
+    const uint32_t pv = A.prio[v];
+    int ne = 0;
+    for (int j0 = b; j0 < e; j0 += 32) {
+      const int j = j0 + lane;
+      bool earlier = false;
+      if (j < e) {
+        const int u = A.col[j];
+        const uint32_t pu = A.prio[u];
+        earlier = !(pv == pu ? v < u : pv < pu);
+      }
+      ne += __popc(__ballot_sync(MCE_FULL, earlier));
+    }
+    int eo = b, lo = b + ne;
+    for (int j0 = b; j0 < e; j0 += 32) {
+      const int j = j0 + lane;
+      const bool valid = j < e;
+      bool later = false;
+      int u = 0;
+      if (valid) {
+        u = A.col[j];
+        const uint32_t pu = A.prio[u];
+        later = pv == pu ? v < u : pv < pu;
+      }
+      const uint32_t mL = __ballot_sync(MCE_FULL, valid && later);
+      const uint32_t mE = __ballot_sync(MCE_FULL, valid && !later);
+      if (valid) A.cs[later ? lo + __popc(mL & lt) : eo + __popc(mE & lt)] = u;
+      eo += __popc(mE);
+      lo += __popc(mL);
+    }
+    if (lane == 0) A.split[v] = b + ne;
+  }
+  __syncthreads();
+}
+
+union WarpSmem {
+  RegSmem<uint32_t, 1> r32;
+  RegSmem<u64, 2> r64;
+  MemSmem mem;
+};
+
+constexpr uint32_t SV_EXIT = 0xFFFFFFFFu;
+
+// Thread 0 of a slot: wait for a published request and claim it; SV_EXIT
+// when the session stops or the slot has been idle for idle_ns.
+__device__ uint32_t claim(const ServeArgs &S) {
+  SvCtl *c = S.ctl;
+  const uint64_t t_idle = globaltimer_ns();
+  uint32_t ns = 64;
+  for (;;) {
+    const uint64_t now = globaltimer_ns();
+    const unsigned long long last = ld_volatile(&c->poll_ns);
+    if (now - last >= SV_POLL_NS && atomicCAS(&c->poll_ns, last, now) == last) {
+      // stop first: the host publishes its last request before stopping,
+      // so a tail read after a stop read sees that request
+      const uint32_t st = ld_acquire_sys(&S.hdr->stop);
+      const uint32_t t = ld_acquire_sys(&S.hdr->tail);
+      atomicMax(&c->dtail, t);
+      __threadfence();
+      if (st) atomicExch(&c->dstop, 1u);
+    }
+    const uint32_t stop = ld_volatile(&c->dstop);  // before dtail, as written above
+    __threadfence();
+    const uint32_t k = ld_volatile(&c->next);
+    if (k < ld_volatile(&c->dtail)) {
+      if (atomicCAS(&c->next, k, k + 1) == k) {
+        __threadfence_system();  // the entry's seed is read after this
+        return k;
+      }
+      continue;
+    }
+    if (stop) return SV_EXIT;
+    if (now - t_idle > S.idle_ns) return SV_EXIT;
+    __nanosleep(ns);
+    if (ns < 1024) ns <<= 1;
+  }
+}
+
+__global__ void __launch_bounds__(SV_BLOCK) serve_kernel(ServeArgs S) {
+  extern __shared__ int32_t sortbuf[];  // next power of two >= ego_cap ints
+  __shared__ SvShared sh;
+  __shared__ WarpSmem wsm[SV_WARPS];
+  const int lane = (int)lane_id(), w = threadIdx.x >> 5;
+  Arena A;
+  arena_layout(S.ego_cap, S.arc_cap, S.hcap, S.arena + (size_t)blockIdx.x * S.arena_bytes, &A);
+  unsigned long long *wslab =
+      S.slab + ((size_t)blockIdx.x * SV_WARPS + (size_t)w) * S.slab_words;
+  // engine arguments over the slot's arena (no task sharing, no per-root logs)
+  BKArgs a;
+  memset(&a, 0, sizeof(a));
+  a.rp = A.rp;
+  a.split = A.split;
+  a.cs = A.cs;
+  a.hist = A.hist;
+  a.err = A.err;
+  a.dcap = SV_DCAP;
+  a.xcap = S.ego_cap;
+  a.node_budget = S.node_budget;
+  a.slab = wslab + S.reg_words;
+  a.slab_words = 0;
+  const Slab msl = slab_of(a, 0);
+  BKArgs ar = a;
+  ar.slab = wslab;
+  const RegSlab<uint32_t> rs32 = reg_slab<uint32_t>(ar, 0);
+  const RegSlab<u64> rs64 = reg_slab<u64>(ar, 0);
+  for (;;) {
+    if (threadIdx.x == 0) {
+      sh.req = claim(S);
+      sh.total = 0;
+      sh.nodes = 0;
+      sh.rootnext = 0;
+      *A.err = 0;
+    }
+    __syncthreads();
+    const uint32_t req = sh.req;
+    if (req == SV_EXIT) break;
+    const uint64_t t0 = globaltimer_ns();
+    SvEntry *E = S.ent + (req % S.ring);
+    const int64_t seed = *(volatile int64_t *)&E->seed;
+    int32_t status = MCE_OK;
+    uint32_t limits = 0;
+    int n = 0;
+    if (seed < 0 || seed >= S.gn) {
+      status = MCE_EINVAL;
+    } else {
+      n = ego_extract(S, A, seed, sortbuf, sh);
+      if (n < 0) {
+        status = MCE_ELIMIT;
+        limits = MCE_ERR_ARCS;
+        n = 0;
+      }
+    }
+    if (status == MCE_OK) {
+      ego_peel(A, n, sh);
+      ego_orient(A, n);
+      unsigned long long mine = 0, h0 = 0, h1 = 0;
+      RegRoot<uint32_t> rt32;
+      RegRoot<u64> rt64;
+      MemRoot rtm;
+      WarpSmem &sm = wsm[w];
+      for (;;) {  // warps take roots in id order until done or over a limit
+        uint32_t r = 0;
+        if (lane == 0) {
+          const bool over = S.node_budget && ld_volatile(&sh.nodes) > S.node_budget;
+          if (over) atomicOr(A.err, MCE_ERR_BUDGET);
+          r = (over || ld_volatile(A.err)) ? 0xFFFFFFFFu : atomicAdd(&sh.rootnext, 1u);
+        }
+        r = __shfl_sync(MCE_FULL, r, 0);
+        if (r >= (uint32_t)n) break;
+        const int dp = A.rp[r + 1] - A.split[r], dm = A.split[r] - A.rp[r];
+        if (dp == 0) continue;
+        unsigned long long nd = 0, cnt = 0;
+        if (dp <= 32 && dm <= REG_XCAP) {
+          reg_encode<uint32_t, 1>(ar, sm.r32, rs32, (int32_t)r, rt32);
+          reg_tree<uint32_t, 1, true>(ar, sm.r32, rs32, rt32, WOps<uint32_t>::low(dp), 0u, 0u, h0, h1,
+                                nd, cnt);
+        } else if (dp <= 64 && dm <= REG_XCAP) {
+          reg_encode<u64, 2>(ar, sm.r64, rs64, (int32_t)r, rt64);
+          reg_tree<u64, 2, true>(ar, sm.r64, rs64, rt64, WOps<u64>::low(dp), 0ull, 0ull, h0, h1, nd,
+                           cnt);
+        } else {  // mem_encode flags roots wider than SV_DCAP
+          mem_encode(a, sm.mem, msl, (int32_t)r, rtm);
+          if (rtm.d > 0) {
+            const int Wr = rtm.Wr;
+            if (lane < Wr) {  // root frame: P = all of N+(r), X = 0, S = 0
+              msl.stk[lane] = (lane == Wr - 1 && (dp & 63)) ? ((1ull << (dp & 63)) - 1ull) : ~0ull;
+              msl.stk[Wr + lane] = 0;
+              msl.stk[3 * Wr + lane] = 0;
+            }
+            __syncwarp();
+            mem_tree<true>(a, msl, rtm, h0, h1, nd, cnt);
+          }
+        }
+        mine += cnt;
+        if (lane == 0 && nd) atomicAdd(&sh.nodes, nd);
+      }
+      if (lane == 0 && mine) atomicAdd(&sh.total, mine);
+      __syncthreads();
+      limits = ld_volatile(A.err);
+      if (limits) status = MCE_ELIMIT;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      E->count = status == MCE_OK ? sh.total : 0ull;
+      E->device_ns = globaltimer_ns() - t0;
+      E->status = status;
+      E->limits = limits;
+      E->ego_n = n;
+      E->ego_arcs = n > 0 ? A.rp[n] : 0;
+      __threadfence_system();
+      *(volatile uint32_t *)&E->done = req + 1;
+      atomicAdd(&S.ctl->served, 1ull);
+      atomicAdd(&S.ctl->nodes, sh.nodes);
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace
+
+int graph_device_view(const struct ::mce_graph *g, const int32_t **rp, const int32_t **col,
+                      int64_t *n, int *device);
+
+}  // namespace mce
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+using namespace mce;
+
+struct mce_serve {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  ServeArgs args{};
+  size_t smem = 0;
+  uint32_t slots = 0, ring = 0;
+  char *host = nullptr;        // mapped: SvHostHdr then the ring entries
+  SvHostHdr *hdr = nullptr;    // host views
+  SvEntry *ent = nullptr;
+  uint32_t tail = 0;           // requests published
+  uint32_t low = 0;            // lowest id whose entry is not yet free
+  std::vector<uint8_t> taken;  // per entry: answer handed to the caller
+  char *arena = nullptr;
+  unsigned long long *slab = nullptr;
+  SvCtl *ctl = nullptr;
+  int64_t launches = 0;
+  bool closed = false;
+};
+
+namespace {
+
+int sv_launch(mce_serve *s) {
+  serve_kernel<<<s->slots, SV_BLOCK, s->smem, s->stream>>>(s->args);
+  MCE_CUDA(cudaGetLastError());
+  ++s->launches;
+  return MCE_OK;
+}
+
+// relaunch when requests are waiting and every slot has left
+int sv_ensure_running(mce_serve *s) {
+  const cudaError_t q = cudaStreamQuery(s->stream);
+  if (q == cudaErrorNotReady) return MCE_OK;
+  if (q != cudaSuccess) return MCE_ECUDA;
+  SvCtl c;
+  MCE_CUDA(cudaMemcpy(&c, s->ctl, sizeof(c), cudaMemcpyDeviceToHost));
+  if (c.next >= s->tail) return MCE_OK;  // nothing unclaimed
+  return sv_launch(s);
+}
+
+bool sv_done(const mce_serve *s, uint32_t id) {
+  const SvEntry &e = s->ent[id % s->ring];
+  return __atomic_load_n(&e.done, __ATOMIC_ACQUIRE) == id + 1;
+}
+
+void sv_retire(mce_serve *s) {
+  while (s->low < s->tail && s->taken[s->low % s->ring]) {
+    s->taken[s->low % s->ring] = 0;
+    ++s->low;
+  }
+}
+
+void sv_free(mce_serve *s) {
+  if (s->stream) cudaStreamDestroy(s->stream);
+  if (s->host) cudaFreeHost(s->host);
+  if (s->arena) cudaFree(s->arena);
+  if (s->slab) cudaFree(s->slab);
+  if (s->ctl) cudaFree(s->ctl);
+  delete s;
+}
+
+}  // namespace
+
+extern "C" void mce_serve_opts_default(mce_serve_opts_t *o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->ego_cap = 1024;
+  o->max_arcs = 0;
+  o->slots = 0;
+  o->ring = 4096;
+  o->idle_ms = 1000;
+}
+
+extern "C" int mce_serve_open(mce_graph_t g, const mce_serve_opts_t *opts, mce_serve_t *out) {
+  if (!g || !out) return MCE_EINVAL;
+  mce_serve_opts_t o;
+  mce_serve_opts_default(&o);
+  if (opts) o = *opts;
+  if (o.ego_cap < 2 || o.ego_cap > SV_MAX_EGO || o.ring < 1 || o.ring > (1u << 24) ||
+      o.idle_ms < 1 || o.max_arcs < 0 || o.max_nodes < 0)
+    return MCE_EINVAL;
+  const int32_t *rp = nullptr, *col = nullptr;
+  int64_t n = 0;
+  int device = 0;
+  const int rc = graph_device_view(g, &rp, &col, &n, &device);
+  if (rc != MCE_OK) return rc;
+  MCE_CUDA(cudaSetDevice(device));
+  int sms = 0;
+  MCE_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  mce_serve *s = new mce_serve();
+  s->device = device;
+  s->ring = o.ring;
+  int np2 = 1;
+  while (np2 < o.ego_cap) np2 <<= 1;
+  s->smem = sizeof(int32_t) * (size_t)np2;
+  auto fail = [&](int code) {
+    sv_free(s);
+    return code;
+  };
+  if (cudaFuncSetAttribute(serve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)s->smem) != cudaSuccess)
+    return fail(MCE_ECUDA);
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, serve_kernel, SV_BLOCK, s->smem) !=
+          cudaSuccess ||
+      per_sm < 1)
+    return fail(MCE_ECUDA);
+  const uint32_t fit = (uint32_t)(sms * per_sm);  // every slot resident at once
+  s->slots = o.slots > 0 ? std::min((uint32_t)o.slots, fit) : fit;
+  if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return fail(MCE_ECUDA);
+  const size_t host_bytes = sizeof(SvHostHdr) + sizeof(SvEntry) * (size_t)o.ring;
+  if (cudaHostAlloc((void **)&s->host, host_bytes, cudaHostAllocMapped) != cudaSuccess)
+    return fail(MCE_ENOMEM);
+  std::memset(s->host, 0, host_bytes);
+  s->hdr = (SvHostHdr *)s->host;
+  s->ent = (SvEntry *)(s->host + sizeof(SvHostHdr));
+  s->taken.assign(o.ring, 0);
+  char *dh = nullptr;
+  if (cudaHostGetDevicePointer((void **)&dh, s->host, 0) != cudaSuccess) return fail(MCE_ECUDA);
+  ServeArgs &A = s->args;
+  A.grp = rp;
+  A.gcol = col;
+  A.gn = n;
+  A.hdr = (const SvHostHdr *)dh;
+  A.ent = (SvEntry *)(dh + sizeof(SvHostHdr));
+  A.ring = o.ring;
+  A.ego_cap = o.ego_cap;
+  // the table also takes the up to SV_BLOCK - 1 vertices of the chunk
+  // that crosses the cap
+  int hcap = 32;
+  while (hcap < 2 * (o.ego_cap + SV_BLOCK)) hcap <<= 1;
+  A.hcap = hcap;
+  const int64_t full = (int64_t)o.ego_cap * (o.ego_cap - 1);
+  const int64_t want = o.max_arcs > 0 ? o.max_arcs : (int64_t)o.ego_cap * 128;
+  A.arc_cap = (int32_t)std::max<int64_t>(1, std::min<int64_t>(std::min(full, want), INT32_MAX / 2));
+  A.arena_bytes = arena_layout(A.ego_cap, A.arc_cap, A.hcap, nullptr, nullptr);
+  A.reg_words = bk_slab_words(CLS_R64, 0, 0);
+  A.slab_words = A.reg_words + bk_slab_words(CLS_MEM, SV_DCAP, A.ego_cap);
+  A.idle_ns = (uint64_t)o.idle_ms * 1000000ull;
+  A.node_budget = (unsigned long long)o.max_nodes;
+  if (cudaMalloc((void **)&s->arena, A.arena_bytes * s->slots) != cudaSuccess ||
+      cudaMalloc((void **)&s->slab, A.slab_words * 8 * (size_t)s->slots * SV_WARPS) !=
+          cudaSuccess ||
+      cudaMalloc((void **)&s->ctl, sizeof(SvCtl)) != cudaSuccess)
+    return fail(MCE_ENOMEM);
+  if (cudaMemset(s->ctl, 0, sizeof(SvCtl)) != cudaSuccess) return fail(MCE_ECUDA);
+  A.arena = s->arena;
+  A.slab = s->slab;
+  A.ctl = s->ctl;
+  // the graph's upload (queued on its own stream) completes first
+  if (cudaDeviceSynchronize() != cudaSuccess) return fail(MCE_ECUDA);
+  if (sv_launch(s) != MCE_OK) return fail(MCE_ECUDA);
+  *out = s;
+  return MCE_OK;
+}
+
+extern "C" int mce_serve_submit(mce_serve_t s, int64_t seed, uint64_t *id_out) {
+  if (!s || !id_out) return MCE_EINVAL;
+  if (s->closed) return MCE_ESTATE;
+  sv_retire(s);
+  if (s->tail - s->low >= s->ring) return MCE_ELIMIT;  // ring full: take answers first
+  if (s->tail == 0xFFFFFFF0u) return MCE_ELIMIT;       // ids exhausted
+  const uint32_t id = s->tail;
+  SvEntry &e = s->ent[id % s->ring];
+  e.seed = seed;
+  __atomic_store_n(&e.done, 0u, __ATOMIC_RELAXED);
+  s->tail = id + 1;
+  __atomic_store_n(&s->hdr->tail, s->tail, __ATOMIC_RELEASE);
+  *id_out = id;
+  return sv_ensure_running(s);
+}
+
+extern "C" int mce_serve_poll(mce_serve_t s, uint64_t id, mce_serve_result_t *res) {
+  if (!s || !res) return MCE_EINVAL;
+  if (id >= s->tail || id < s->low || s->taken[id % s->ring]) return MCE_EINVAL;
+  const uint32_t i = (uint32_t)id;
+  if (!sv_done(s, i)) {
+    const int rc = s->closed ? MCE_OK : sv_ensure_running(s);
+    return rc != MCE_OK ? rc : MCE_EAGAIN;
+  }
+  const SvEntry &e = s->ent[i % s->ring];
+  res->count = e.count;
+  res->seed = e.seed;
+  res->status = e.status;
+  res->ego_n = e.ego_n;
+  res->ego_arcs = e.ego_arcs;
+  res->limits = e.limits;
+  res->device_ns = e.device_ns;
+  s->taken[i % s->ring] = 1;
+  sv_retire(s);
+  return MCE_OK;
+}
+
+extern "C" int mce_serve_wait(mce_serve_t s, uint64_t id, int64_t timeout_ms,
+                              mce_serve_result_t *res) {
+  const auto t0 = std::chrono::steady_clock::now();
+  for (;;) {
+    const int rc = mce_serve_poll(s, id, res);
+    if (rc != MCE_EAGAIN) return rc;
+    const auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(
+                        std::chrono::steady_clock::now() - t0)
+                        .count();
+    if (timeout_ms >= 0 && ms > timeout_ms) return MCE_ETIMEOUT;
+    std::this_thread::yield();
+  }
+}
+
+extern "C" int mce_serve_run(mce_serve_t s, const int64_t *seeds, const double *arrival_us,
+                             int64_t count, int64_t timeout_ms, mce_serve_result_t *results,
+                             double *latency_us) {
+  if (!s || count < 0 || (count > 0 && (!seeds || !results))) return MCE_EINVAL;
+  if (s->closed) return MCE_ESTATE;
+  using clk = std::chrono::steady_clock;
+  const auto t0 = clk::now();
+  auto now_us = [&]() { return std::chrono::duration<double, std::micro>(clk::now() - t0).count(); };
+  std::vector<uint64_t> ids((size_t)count);
+  std::vector<int64_t> open;  // submitted, answer not yet taken
+  open.reserve(s->ring);
+  int64_t next = 0, finished = 0;
+  while (finished < count) {
+    const double t = now_us();
+    while (next < count && (!arrival_us || arrival_us[next] <= t)) {
+      uint64_t id = 0;
+      const int rc = mce_serve_submit(s, seeds[next], &id);
+      if (rc == MCE_ELIMIT) break;  // ring full: admit once answers are taken
+      if (rc != MCE_OK) return rc;
+      ids[(size_t)next] = id;
+      open.push_back(next++);
+    }
+    size_t keep = 0;
+    for (size_t q = 0; q < open.size(); ++q) {
+      const int64_t r = open[q];
+      const int rc = mce_serve_poll(s, ids[(size_t)r], &results[r]);
+      if (rc == MCE_OK) {
+        if (latency_us) latency_us[r] = now_us() - (arrival_us ? arrival_us[r] : 0.0);
+        ++finished;
+      } else if (rc == MCE_EAGAIN) {
+        open[keep++] = r;
+      } else {
+        return rc;
+      }
+    }
+    open.resize(keep);
+    if (timeout_ms >= 0 && now_us() > 1000.0 * (double)timeout_ms) return MCE_ETIMEOUT;
+  }
+  return MCE_OK;
+}
+
+extern "C" int mce_serve_stats(mce_serve_t s, mce_serve_stats_t *st) {
+  if (!s || !st) return MCE_EINVAL;
+  SvCtl c;
+  MCE_CUDA(cudaMemcpy(&c, s->ctl, sizeof(c), cudaMemcpyDeviceToHost));
+  std::memset(st, 0, sizeof(*st));
+  st->slots = (int32_t)s->slots;
+  st->ring = s->ring;
+  st->submitted = s->tail;
+  st->served = c.served;
+  st->tree_nodes = c.nodes;
+  st->kernel_launches = s->launches;
+  st->arena_bytes = (uint64_t)s->args.arena_bytes * s->slots;
+  st->slab_bytes = (uint64_t)s->args.slab_words * 8 * s->slots * SV_WARPS;
+  st->running = cudaStreamQuery(s->stream) == cudaErrorNotReady ? 1 : 0;
+  return MCE_OK;
+}
+
+extern "C" int mce_serve_close(mce_serve_t s) {
+  if (!s) return MCE_EINVAL;
+  if (!s->closed) {
+    s->closed = true;
+    __atomic_store_n(&s->hdr->stop, 1u, __ATOMIC_RELEASE);
+  }
+  // Every slot finishes its request and leaves once nothing is published.
+  // A request published just as the last slot left idle is served by one
+  // more launch (which sees the stop flag and leaves when done).
+  int rc = MCE_OK;
+  for (int pass = 0; pass < 3 && rc == MCE_OK; ++pass) {
+    if (cudaStreamSynchronize(s->stream) != cudaSuccess) {
+      rc = MCE_ECUDA;
+      break;
+    }
+    SvCtl c;
+    if (cudaMemcpy(&c, s->ctl, sizeof(c), cudaMemcpyDeviceToHost) != cudaSuccess) rc = MCE_ECUDA;
+    if (rc != MCE_OK || c.next >= s->tail) break;
+    rc = sv_launch(s);
+  }
+  sv_free(s);
+  return rc;
+}

@@ -206,21 +206,13 @@ extern "C" int mce_ego_subgraph(const int32_t *row_ptr, const int32_t *col, int6
   in.insert((int32_t)seed_vertex);
   for (int64_t j = row_ptr[seed_vertex]; j < row_ptr[seed_vertex + 1] && (int64_t)verts.size() < cap; ++j)
     if (in.insert(col[j]).second) verts.push_back(col[j]);
-  if ((int64_t)verts.size() < cap) {
-    std::vector<int32_t> hop2;
-    const size_t k1 = verts.size();
-    for (size_t i = 1; i < k1; ++i) {
-      const int32_t u = verts[i];
-      for (int64_t j = row_ptr[u]; j < row_ptr[u + 1]; ++j)
-        if (!in.count(col[j])) hop2.push_back(col[j]);
-    }
-    std::sort(hop2.begin(), hop2.end());
-    hop2.erase(std::unique(hop2.begin(), hop2.end()), hop2.end());
-    for (size_t i = 0; i < hop2.size() && (int64_t)verts.size() < cap; ++i) {
-      in.insert(hop2[i]);
-      verts.push_back(hop2[i]);
-    }
+  const size_t k1 = verts.size();
+  for (size_t i = 1; i < k1 && (int64_t)verts.size() < cap; ++i) {  // 2-hop, discovery order
+    const int32_t u = verts[i];
+    for (int64_t j = row_ptr[u]; j < row_ptr[u + 1] && (int64_t)verts.size() < cap; ++j)
+      if (in.insert(col[j]).second) verts.push_back(col[j]);
   }
+  std::sort(verts.begin(), verts.end());
   // relabel
   std::unordered_map<int32_t, int64_t> id;
   id.reserve(verts.size() * 2);

@@ -23,8 +23,9 @@ if not os.path.exists(LIB_PATH):
 _lib = C.CDLL(LIB_PATH)
 
 # status codes (include/mce.h)
-OK, EINVAL, ENOMEM, ECUDA, EIO, EFORMAT, ELIMIT, ETIMEOUT, ENODEV, ESTATE = (
-    0, -1, -2, -3, -4, -5, -6, -7, -8, -9)
+OK, EINVAL, ENOMEM, ECUDA, EIO, EFORMAT, ELIMIT, ETIMEOUT, ENODEV, ESTATE, EAGAIN = (
+    0, -1, -2, -3, -4, -5, -6, -7, -8, -9, -10)
+SERVE_OVER_BUDGET, SERVE_OVER_ARCS, SERVE_TOO_WIDE = 0x20, 0x40, 0x0C
 LEVEL_L1, LEVEL_L2 = 1, 2
 INDUCED_P, INDUCED_PX = 1, 2
 WL_OFF, WL_ON = 1, 2
@@ -65,6 +66,25 @@ class _HGraph(C.Structure):
                 ("vtx_offsets", C.POINTER(C.c_int64)), ("arc_offsets", C.POINTER(C.c_int64))]
 
 
+class _ServeOpts(C.Structure):
+    _fields_ = [("ego_cap", C.c_int32), ("slots", C.c_int32), ("ring", C.c_uint32),
+                ("idle_ms", C.c_int32), ("max_arcs", C.c_int64), ("max_nodes", C.c_int64),
+                ("reserved", C.c_int64 * 3)]
+
+
+class _ServeResult(C.Structure):
+    _fields_ = [("count", C.c_uint64), ("seed", C.c_int64), ("status", C.c_int32),
+                ("ego_n", C.c_int32), ("ego_arcs", C.c_int32), ("limits", C.c_uint32),
+                ("device_ns", C.c_uint64)]
+
+
+class _ServeStats(C.Structure):
+    _fields_ = [("slots", C.c_int32), ("running", C.c_int32), ("ring", C.c_uint32),
+                ("pad", C.c_uint32), ("submitted", C.c_uint64), ("served", C.c_uint64),
+                ("tree_nodes", C.c_uint64), ("kernel_launches", C.c_int64),
+                ("arena_bytes", C.c_uint64), ("slab_bytes", C.c_uint64)]
+
+
 _P = C.c_void_p
 _sigs = {
     "mce_opts_default": (None, [_P]),
@@ -98,6 +118,14 @@ _sigs = {
     "mce_model_predict": (C.c_int, [_P, _P, _P]),
     "mce_model_eval": (C.c_int, [_P, _P, C.c_int64, _P]),
     "mce_model_grad": (C.c_int, [_P, _P, _P, C.c_int64, _P, _P]),
+    "mce_serve_opts_default": (None, [_P]),
+    "mce_serve_open": (C.c_int, [_P, _P, _P]),
+    "mce_serve_submit": (C.c_int, [_P, C.c_int64, _P]),
+    "mce_serve_poll": (C.c_int, [_P, C.c_uint64, _P]),
+    "mce_serve_wait": (C.c_int, [_P, C.c_uint64, C.c_int64, _P]),
+    "mce_serve_run": (C.c_int, [_P, _P, _P, C.c_int64, C.c_int64, _P, _P]),
+    "mce_serve_stats": (C.c_int, [_P, _P]),
+    "mce_serve_close": (C.c_int, [_P]),
     "mce_gen_er": (C.c_int, [C.c_int64, C.c_double, C.c_uint64, C.c_int32, C.c_int32,
                              C.c_int32, _P]),
     "mce_gen_rmat": (C.c_int, [C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,
@@ -510,3 +538,84 @@ def root_features(g: "Graph") -> np.ndarray:
     out = np.zeros((max(g.n, 1), MLP_INPUTS), np.float32)
     _check(_lib.mce_root_features(g._h, _ptr(out)), "root_features")
     return out[:g.n]
+
+
+# ---------------------------------------------------------------------------
+# serving
+# ---------------------------------------------------------------------------
+SERVE_RESULT_DTYPE = np.dtype([("count", np.uint64), ("seed", np.int64), ("status", np.int32),
+                               ("ego_n", np.int32), ("ego_arcs", np.int32), ("limits", np.uint32),
+                               ("device_ns", np.uint64)])
+assert SERVE_RESULT_DTYPE.itemsize == C.sizeof(_ServeResult)
+
+
+def _result_dict(r: _ServeResult) -> dict:
+    return {k: getattr(r, k) for k, _ in _ServeResult._fields_}
+
+
+class Serve:
+    """A serving session over a resident Graph (wraps mce_serve_t).
+
+    Each request is a seed vertex; its answer is the maximal-clique count of
+    the seed's 2-hop ego subgraph (ego_subgraph(host_graph, seed, ego_cap)).
+    """
+
+    def __init__(self, g: Graph, *, ego_cap=1024, slots=0, ring=4096, idle_ms=1000, max_arcs=0,
+                 max_nodes=0):
+        o = _ServeOpts()
+        _lib.mce_serve_opts_default(C.byref(o))
+        o.ego_cap, o.slots, o.ring, o.idle_ms = ego_cap, slots, ring, idle_ms
+        o.max_arcs, o.max_nodes = max_arcs, max_nodes
+        self._h = C.c_void_p()
+        self.graph = g  # the session reads the graph's device arrays
+        _check(_lib.mce_serve_open(g._h, C.byref(o), C.byref(self._h)), "serve_open")
+
+    def submit(self, seed: int) -> int:
+        rid = C.c_uint64()
+        _check(_lib.mce_serve_submit(self._h, seed, C.byref(rid)), "serve_submit")
+        return int(rid.value)
+
+    def poll(self, rid: int) -> dict | None:
+        r = _ServeResult()
+        rc = _lib.mce_serve_poll(self._h, rid, C.byref(r))
+        if rc == EAGAIN:
+            return None
+        _check(rc, "serve_poll")
+        return _result_dict(r)
+
+    def wait(self, rid: int, timeout_ms: int = 60000) -> dict:
+        r = _ServeResult()
+        _check(_lib.mce_serve_wait(self._h, rid, timeout_ms, C.byref(r)), "serve_wait")
+        return _result_dict(r)
+
+    def run(self, seeds, arrival_us=None, timeout_ms: int = 600000):
+        """Open-loop trace; returns (results structured array, latency_us array)."""
+        seeds = np.ascontiguousarray(seeds, dtype=np.int64)
+        arr = None if arrival_us is None else np.ascontiguousarray(arrival_us, dtype=np.float64)
+        res = np.zeros(len(seeds), SERVE_RESULT_DTYPE)
+        lat = np.zeros(len(seeds), np.float64)
+        _check(_lib.mce_serve_run(self._h, _ptr(seeds), _ptr(arr), len(seeds), timeout_ms,
+                                  _ptr(res), _ptr(lat)), "serve_run")
+        return res, lat
+
+    def stats(self) -> dict:
+        st = _ServeStats()
+        _check(_lib.mce_serve_stats(self._h, C.byref(st)), "serve_stats")
+        return {k: getattr(st, k) for k, _ in _ServeStats._fields_ if k != "pad"}
+
+    def close(self) -> None:
+        if self._h:
+            h, self._h = self._h, C.c_void_p()
+            _check(_lib.mce_serve_close(h), "serve_close")
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

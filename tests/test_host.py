@@ -122,16 +122,41 @@ def test_validate_rejects_asymmetric():
     assert mce.validate(g) == mce.EFORMAT
 
 
-def test_ego_subgraph():
-    g = mce.gen_er(400, 0.05, 4)
-    eg, vmap = mce.ego_subgraph(g, 7, 64)
-    assert eg.n <= 64 and vmap[0] == 7
+def ego_reference(g, seed, cap):
+    """The ego-graph definition in plain Python: seed, neighbours in row
+    order, then 2-hop vertices in discovery order, at most cap; ascending
+    relabel.  Returns (sorted vertex ids, set of edges in original ids)."""
+    rp, col = g.row_ptr, g.col
+    verts, seen = [seed], {seed}
+    for w in col[rp[seed]:rp[seed + 1]]:
+        if len(verts) >= cap:
+            break
+        if int(w) not in seen:
+            seen.add(int(w))
+            verts.append(int(w))
+    k1 = len(verts)
+    for u in verts[1:k1]:
+        for w in col[rp[u]:rp[u + 1]]:
+            if len(verts) >= cap:
+                break
+            if int(w) not in seen:
+                seen.add(int(w))
+                verts.append(int(w))
+    vs = sorted(verts)
+    edges = {(int(a), int(b)) for a in vs for b in col[rp[a]:rp[a + 1]] if int(b) in seen and a < b}
+    return vs, edges
+
+
+@pytest.mark.parametrize("seed,cap", [(7, 64), (0, 2), (3, 400), (11, 150)])
+def test_ego_subgraph(seed, cap):
+    g = mce.gen_ba(400, 4, 5, planted=3, cmin=6, cmax=10)
+    eg, vmap = mce.ego_subgraph(g, seed, cap)
     assert mce.validate(eg) == 0
-    # every ego edge is an edge of g
-    for u in range(eg.n):
-        for w in eg.col[eg.row_ptr[u]:eg.row_ptr[u + 1]]:
-            a, b = vmap[u], vmap[w]
-            assert b in g.col[g.row_ptr[a]:g.row_ptr[a + 1]]
+    vs, edges = ego_reference(g, seed, cap)
+    assert list(vmap) == vs and seed in vs
+    got = {(int(vmap[u]), int(vmap[w])) for u in range(eg.n)
+           for w in eg.col[eg.row_ptr[u]:eg.row_ptr[u + 1]] if u < w}
+    assert got == edges
 
 
 @pytest.mark.skipif(not os.path.exists(CLI), reason="CLI not built")
