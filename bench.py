@@ -69,6 +69,13 @@ def parse_args():
                    help="root order (learned: the shipped cost model of the workload family; "
                         "the others are timed beside it unless --no-compare)")
     p.add_argument("--no-compare", action="store_true", help="skip the other schedules")
+    p.add_argument("--tune", choices=["table", "retune", "off"], default="table",
+                   help="search settings: from the autotuner table (tuned and stored when the "
+                        "shape class is missing), re-tuned, or the library defaults")
+    p.add_argument("--tune-table", default=os.path.join(ROOT, "mce-gpu_b200", "data",
+                                                        "tune_table.txt"))
+    p.add_argument("--no-plain", action="store_true",
+                   help="skip the per-graph plain-path comparison (batch workload)")
     return p.parse_args()
 
 
@@ -247,6 +254,11 @@ def run_mine(args, rank, world, local_rank):
         kw = dict(kw, cuda_graph=1)
     else:
         dg = mce.Graph.from_host(g, device=local_rank, stream=sptr)
+    tuning = None
+    if args.tune != "off":
+        tkw = {k: v for k, v in kw.items() if k != "cuda_graph"}
+        tuning = dg.autotune(args.tune_table, reps=2, force=args.tune == "retune", **tkw)
+        kw.update(tuning["best"])
     torch.cuda.synchronize()
     res = None
     for _ in range(args.warmup):
@@ -349,8 +361,8 @@ def run_mine(args, rank, world, local_rank):
                        peel_split_ms={k: round(stats[-1]["peel_" + k + "_ms"], 3)
                                       for k in ("scan", "round", "wait")},
                        tasks_shared=stats[-1]["donations"],
-                       worker_list=args.wl, donate=args.donate, solo=args.solo,
-                       donate_after=args.after),
+                       settings={k: kw.get(k) for k in mce.TUNED_FIELDS},
+                       tuning=tuning),
         "e2e": {"value": world * total / (e2e_ms / 1e3), "unit": "maximal cliques/s",
                 "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h + 8 * 4096 + 64 + 8 + 4 + 128),
@@ -386,7 +398,7 @@ def run_mine(args, rank, world, local_rank):
             ms = sum(ts) / len(ts)
             cmp[name] = {"ms_per_step": round(ms, 3), "value": total / (ms / 1e3)}
         line["config"]["other_schedules"] = cmp
-    if hb is not None:
+    if hb is not None and not args.no_plain:
         kw_plain = {k: v for k, v in kw.items() if k not in ("cuda_graph", "model", "sched")}
         line["config"]["plain_per_graph"] = plain_per_graph(hb, 256, stream, kw_plain)
     if not args.no_cpu_baseline and world == 1:

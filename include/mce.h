@@ -320,6 +320,38 @@ int mce_count_oriented_noalloc(const int32_t *d_row_ptr, const int32_t *d_split,
                                const int32_t *d_col_split, const int32_t *d_roots,
                                int64_t num_roots, uint64_t *d_hist, void *stream);
 
+/* ---- autotuner ------------------------------------------------------------ */
+/* Per graph-shape class, the search settings (worker list, donation gate and
+ * threshold, bitmap word width of narrow roots, single-block peeling of small
+ * frontiers) that ran fastest in timed trials, kept in a text table with one
+ * line per class.  A class is floor(log2) of the vertex count, mean degree
+ * and degeneracy (and of the graph count for a batch), e.g. "n23-a4-k5" or
+ * "b12-n23-a4-k7".  No counterpart in the reference (its per-graph variant
+ * choice is a rule of thumb in table.py:127).                               */
+typedef struct mce_tune_result {
+  char key[48];       /* shape class                                        */
+  mce_opts_t best;    /* the base options with the tuned fields set         */
+  double best_ms;     /* device time of one count with `best`               */
+  double default_ms;  /* ... with the base options                          */
+  int32_t trials_run; /* counts timed by this call (0 when from the table)  */
+  int32_t from_table; /* 1: the class was in the table, nothing was timed   */
+} mce_tune_result_t;
+
+/* Shape class of a graph / a batch (runs the peel for the degeneracy).     */
+int mce_shape_key(mce_graph_t g, char *key_out, size_t len);
+int mce_batch_shape_key(mce_batch_t b, char *key_out, size_t len);
+/* Set the tuned fields of *inout from the table's line for `key`;
+ * MCE_EIO: no table, MCE_ESTATE: no line for the class.                    */
+int mce_tune_lookup(const char *table_path, const char *key, mce_opts_t *inout);
+/* Tune the graph's class unless the table (nullable) has it already (force
+ * = 1: tune anyway); each setting is timed `reps` times (best kept) and
+ * must return the same count (else MCE_ESTATE).  The table is rewritten
+ * with the class's new line.                                               */
+int mce_autotune(mce_graph_t g, const mce_opts_t *base, const char *table_path, int32_t reps,
+                 int32_t force, mce_tune_result_t *out);
+int mce_batch_autotune(mce_batch_t b, const mce_opts_t *base, const char *table_path,
+                       int32_t reps, int32_t force, mce_tune_result_t *out);
+
 /* ---- serving ------------------------------------------------------------ */
 /* A serving session answers requests against a resident graph from one
  * persistent kernel (no counterpart in the reference, which runs one graph

@@ -270,6 +270,15 @@ int ensure_slab(mce_graph *g, size_t bytes) {
 }  // namespace
 
 namespace mce {
+// sizes of a graph handle and the union graph of a batch (autotuner)
+int graph_shape(const struct ::mce_graph *g, int64_t *n, int64_t *m) {
+  if (!g) return MCE_EINVAL;
+  *n = g->n;
+  *m = g->m;
+  return MCE_OK;
+}
+struct ::mce_graph *batch_union(struct ::mce_batch *b, int32_t *num_graphs);
+
 // device CSR of a graph handle, for the serving sessions (serve.cu)
 int graph_device_view(const struct ::mce_graph *g, const int32_t **rp, const int32_t **col,
                       int64_t *n, int *device) {
@@ -836,6 +845,18 @@ int mce_batch_reload(mce_batch_t b, const int32_t *row_ptr, const int32_t *col,
   return batch_load(b, row_ptr, col, vtx_offsets, arc_offsets, num_graphs, n, m,
                     pick_stream(b->g, stream));
 }
+
+}  // extern "C"
+
+namespace mce {
+struct ::mce_graph *batch_union(struct ::mce_batch *b, int32_t *num_graphs) {
+  if (!b) return nullptr;
+  if (num_graphs) *num_graphs = b->G;
+  return b->g;
+}
+}  // namespace mce
+
+extern "C" {
 
 int mce_batch_count(mce_batch_t b, const mce_opts_t *opts, uint64_t *per_graph_total,
                     uint64_t *total, uint64_t *hist, mce_stats_t *stats) {

@@ -1,0 +1,268 @@
+// Autotuner: per graph-shape class, the search settings that ran fastest.
+//
+// No counterpart in the reference, whose only per-graph choice is the
+// L1+IP / L1+IPX rule of thumb of its evaluation script (table.py:127).
+// A shape class buckets a graph (or a batch's disjoint union) by
+// floor(log2) of its vertex count, mean degree and degeneracy, plus the
+// batch size for batches.  Tuning walks the knobs one at a time (worker
+// list, donation gate, donation threshold, bitmap word width of narrow
+// roots, single-block peeling of small frontiers), times each value with
+// the device timers of mce_count / mce_batch_count, keeps a value only when
+// it is at least 2% faster, and checks that every trial returns the same
+// count.  The winner is stored in a text table, one line per class; later
+// runs of the same class read it back without trials.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/mce.h"
+
+namespace mce {
+int graph_shape(const struct ::mce_graph *g, int64_t *n, int64_t *m);
+struct ::mce_graph *batch_union(struct ::mce_batch *b, int32_t *num_graphs);
+}  // namespace mce
+
+namespace {
+
+struct Knobs {
+  int32_t worker_list, donate_after, donate_threshold, bitmap_width, peel_solo_max;
+};
+
+// the library's defaults, written out so that a table entry is explicit
+Knobs resolved(const mce_opts_t &o) {
+  Knobs k;
+  k.worker_list = o.worker_list ? o.worker_list : MCE_WL_ON;
+  k.donate_after = o.donate_after > 0 ? o.donate_after : 256;
+  k.donate_threshold = o.donate_threshold > 0 ? o.donate_threshold : 10;
+  k.bitmap_width = o.bitmap_width ? o.bitmap_width : 32;
+  k.peel_solo_max = o.peel_solo_max > 0 ? o.peel_solo_max : -1;
+  return k;
+}
+
+void apply(const Knobs &k, mce_opts_t *o) {
+  o->worker_list = k.worker_list;
+  o->donate_after = k.donate_after;
+  o->donate_threshold = k.donate_threshold;
+  o->bitmap_width = k.bitmap_width;
+  o->peel_solo_max = k.peel_solo_max;
+}
+
+int ilog2(double x) { return x < 1.0 ? 0 : (int)std::floor(std::log2(x)); }
+
+struct Entry {
+  Knobs k;
+  double best_ms, default_ms;
+};
+
+const char *kHeader =
+    "# mce autotune table v1: class worker_list donate_after donate_threshold bitmap_width "
+    "peel_solo_max best_ms default_ms";
+
+bool read_table(const char *path, std::map<std::string, Entry> *t) {
+  std::ifstream f(path);
+  if (!f) return false;
+  std::string line;
+  while (std::getline(f, line)) {
+    if (line.empty() || line[0] == '#') continue;
+    std::istringstream ss(line);
+    std::string key;
+    Entry e;
+    if (ss >> key >> e.k.worker_list >> e.k.donate_after >> e.k.donate_threshold >>
+        e.k.bitmap_width >> e.k.peel_solo_max >> e.best_ms >> e.default_ms)
+      (*t)[key] = e;
+  }
+  return true;
+}
+
+int write_table(const char *path, const std::map<std::string, Entry> &t) {
+  const std::string tmp = std::string(path) + ".tmp";
+  FILE *f = std::fopen(tmp.c_str(), "w");
+  if (!f) return MCE_EIO;
+  std::fprintf(f, "%s\n", kHeader);
+  for (const auto &kv : t) {
+    const Entry &e = kv.second;
+    std::fprintf(f, "%s %d %d %d %d %d %.4f %.4f\n", kv.first.c_str(), e.k.worker_list,
+                 e.k.donate_after, e.k.donate_threshold, e.k.bitmap_width, e.k.peel_solo_max,
+                 e.best_ms, e.default_ms);
+  }
+  if (std::fclose(f) != 0 || std::rename(tmp.c_str(), path) != 0) return MCE_EIO;
+  return MCE_OK;
+}
+
+int shape_key(struct ::mce_graph *g, int32_t num_graphs, char *key, size_t len) {
+  int64_t n = 0, m = 0;
+  int rc = mce::graph_shape(g, &n, &m);
+  if (rc) return rc;
+  int32_t dg = 0;
+  if ((rc = mce_degeneracy(g, nullptr, nullptr, &dg))) return rc;
+  char buf[64];
+  const int a = ilog2(n > 0 ? (double)m / (double)n : 0.0);
+  if (num_graphs > 0)
+    std::snprintf(buf, sizeof(buf), "b%d-n%d-a%d-k%d", ilog2(num_graphs), ilog2((double)n), a,
+                  ilog2(dg));
+  else
+    std::snprintf(buf, sizeof(buf), "n%d-a%d-k%d", ilog2((double)n), a, ilog2(dg));
+  if (std::strlen(buf) + 1 > len) return MCE_EINVAL;
+  std::strcpy(key, buf);
+  return MCE_OK;
+}
+
+// Run(opts, &ms, &total) -> status
+template <typename Run>
+int tune(const char *key, const mce_opts_t &base, const char *table_path, int32_t reps,
+         int32_t force, Run run, mce_tune_result_t *out) {
+  std::memset(out, 0, sizeof(*out));
+  std::snprintf(out->key, sizeof(out->key), "%s", key);
+  std::map<std::string, Entry> table;
+  if (table_path) read_table(table_path, &table);
+  out->best = base;
+  if (!force && table.count(key)) {
+    const Entry &e = table[key];
+    apply(e.k, &out->best);
+    out->best_ms = e.best_ms;
+    out->default_ms = e.default_ms;
+    out->from_table = 1;
+    return MCE_OK;
+  }
+  if (reps < 1) reps = 1;
+  uint64_t want = 0;
+  bool have = false;
+  auto timed = [&](const Knobs &k, double *ms) -> int {
+    mce_opts_t o = base;
+    apply(k, &o);
+    double best = 1e300;
+    for (int r = 0; r < reps; ++r) {
+      double t = 0;
+      uint64_t total = 0;
+      const int rc = run(o, &t, &total);
+      if (rc) return rc;
+      if (have && total != want) return MCE_ESTATE;  // a setting changed the count
+      want = total;
+      have = true;
+      best = std::min(best, t);
+      ++out->trials_run;
+    }
+    *ms = best;
+    return MCE_OK;
+  };
+  Knobs cur = resolved(base);
+  double cur_ms = 0;
+  int rc = timed(cur, &cur_ms);
+  if (rc) return rc;
+  out->default_ms = cur_ms;
+  struct Axis {
+    int32_t Knobs::*field;
+    std::vector<int32_t> values;
+  };
+  const Axis axes[] = {
+      {&Knobs::worker_list, {MCE_WL_ON, MCE_WL_OFF}},
+      {&Knobs::donate_after, {64, 256, 1024}},
+      {&Knobs::donate_threshold, {6, 10, 16}},
+      {&Knobs::bitmap_width, {32, 64}},
+      {&Knobs::peel_solo_max, {-1, 64}},
+  };
+  for (const Axis &ax : axes) {
+    if (ax.field != &Knobs::worker_list && cur.worker_list == MCE_WL_OFF &&
+        (ax.field == &Knobs::donate_after || ax.field == &Knobs::donate_threshold))
+      continue;  // no sharing: the donation knobs do nothing
+    Knobs best = cur;
+    double best_ms = cur_ms;
+    for (int32_t v : ax.values) {
+      if (v == cur.*(ax.field)) continue;
+      Knobs k = cur;
+      k.*(ax.field) = v;
+      double ms = 0;
+      if ((rc = timed(k, &ms))) return rc;
+      if (ms < best_ms * 0.98) {
+        best = k;
+        best_ms = ms;
+      }
+    }
+    cur = best;
+    cur_ms = best_ms;
+  }
+  apply(cur, &out->best);
+  out->best_ms = cur_ms;
+  if (table_path) {
+    table[key] = Entry{cur, cur_ms, out->default_ms};
+    if ((rc = write_table(table_path, table))) return rc;
+  }
+  return MCE_OK;
+}
+
+}  // namespace
+
+extern "C" int mce_shape_key(mce_graph_t g, char *key_out, size_t len) {
+  if (!g || !key_out) return MCE_EINVAL;
+  return shape_key(g, 0, key_out, len);
+}
+
+extern "C" int mce_batch_shape_key(mce_batch_t b, char *key_out, size_t len) {
+  if (!b || !key_out) return MCE_EINVAL;
+  int32_t G = 0;
+  struct ::mce_graph *g = mce::batch_union(b, &G);
+  return shape_key(g, G, key_out, len);
+}
+
+extern "C" int mce_tune_lookup(const char *table_path, const char *key, mce_opts_t *inout) {
+  if (!table_path || !key || !inout) return MCE_EINVAL;
+  std::map<std::string, Entry> t;
+  if (!read_table(table_path, &t)) return MCE_EIO;
+  auto it = t.find(key);
+  if (it == t.end()) return MCE_ESTATE;
+  apply(it->second.k, inout);
+  return MCE_OK;
+}
+
+extern "C" int mce_autotune(mce_graph_t g, const mce_opts_t *base, const char *table_path,
+                            int32_t reps, int32_t force, mce_tune_result_t *out) {
+  if (!g || !out) return MCE_EINVAL;
+  mce_opts_t b;
+  if (base)
+    b = *base;
+  else
+    mce_opts_default(&b);
+  char key[48];
+  int rc = mce_shape_key(g, key, sizeof(key));
+  if (rc) return rc;
+  return tune(key, b, table_path, reps, force,
+              [&](const mce_opts_t &o, double *ms, uint64_t *total) {
+                mce_stats_t st;
+                const int r = mce_count(g, &o, total, nullptr, &st);
+                *ms = st.total_ms;
+                return r;
+              },
+              out);
+}
+
+extern "C" int mce_batch_autotune(mce_batch_t bt, const mce_opts_t *base, const char *table_path,
+                                  int32_t reps, int32_t force, mce_tune_result_t *out) {
+  if (!bt || !out) return MCE_EINVAL;
+  mce_opts_t b;
+  if (base) {
+    b = *base;
+  } else {
+    mce_opts_default(&b);
+    b.cuda_graph = 1;
+  }
+  char key[48];
+  int rc = mce_batch_shape_key(bt, key, sizeof(key));
+  if (rc) return rc;
+  int32_t G = 0;
+  mce::batch_union(bt, &G);
+  std::vector<uint64_t> per((size_t)std::max(G, 1));
+  return tune(key, b, table_path, reps, force,
+              [&](const mce_opts_t &o, double *ms, uint64_t *total) {
+                mce_stats_t st;
+                const int r = mce_batch_count(bt, &o, per.data(), total, nullptr, &st);
+                *ms = st.total_ms;
+                return r;
+              },
+              out);
+}

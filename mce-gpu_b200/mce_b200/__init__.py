@@ -66,6 +66,24 @@ class _HGraph(C.Structure):
                 ("vtx_offsets", C.POINTER(C.c_int64)), ("arc_offsets", C.POINTER(C.c_int64))]
 
 
+class _TuneResult(C.Structure):
+    _fields_ = [("key", C.c_char * 48), ("best", _Opts), ("best_ms", C.c_double),
+                ("default_ms", C.c_double), ("trials_run", C.c_int32), ("from_table", C.c_int32)]
+
+
+TUNED_FIELDS = ("worker_list", "donate_after", "donate_threshold", "bitmap_width", "peel_solo_max")
+
+
+def _tune_dict(r: _TuneResult) -> dict:
+    return {"key": r.key.decode(), "best": {f: getattr(r.best, f) for f in TUNED_FIELDS},
+            "best_ms": r.best_ms, "default_ms": r.default_ms, "trials_run": r.trials_run,
+            "from_table": bool(r.from_table)}
+
+
+def _opts_kwargs(o: "_Opts") -> dict:
+    return {f: getattr(o, f) for f in TUNED_FIELDS}
+
+
 class _ServeOpts(C.Structure):
     _fields_ = [("ego_cap", C.c_int32), ("slots", C.c_int32), ("ring", C.c_uint32),
                 ("idle_ms", C.c_int32), ("max_arcs", C.c_int64), ("max_nodes", C.c_int64),
@@ -118,6 +136,11 @@ _sigs = {
     "mce_model_predict": (C.c_int, [_P, _P, _P]),
     "mce_model_eval": (C.c_int, [_P, _P, C.c_int64, _P]),
     "mce_model_grad": (C.c_int, [_P, _P, _P, C.c_int64, _P, _P]),
+    "mce_shape_key": (C.c_int, [_P, C.c_char_p, C.c_size_t]),
+    "mce_batch_shape_key": (C.c_int, [_P, C.c_char_p, C.c_size_t]),
+    "mce_tune_lookup": (C.c_int, [C.c_char_p, C.c_char_p, _P]),
+    "mce_autotune": (C.c_int, [_P, _P, C.c_char_p, C.c_int32, C.c_int32, _P]),
+    "mce_batch_autotune": (C.c_int, [_P, _P, C.c_char_p, C.c_int32, C.c_int32, _P]),
     "mce_serve_opts_default": (None, [_P]),
     "mce_serve_open": (C.c_int, [_P, _P, _P]),
     "mce_serve_submit": (C.c_int, [_P, C.c_int64, _P]),
@@ -383,6 +406,21 @@ class Graph:
                "count")
         return CountResult(int(total.value), hist, _stats_dict(st))
 
+    def shape_key(self) -> str:
+        buf = C.create_string_buffer(48)
+        _check(_lib.mce_shape_key(self._h, buf, 48), "shape_key")
+        return buf.value.decode()
+
+    def autotune(self, table: str | None = None, reps: int = 2, force: bool = False,
+                 **opts) -> dict:
+        """Tune this graph's shape class (or read it from `table`); returns the
+        result with `best` = the tuned option values (pass them to count)."""
+        o = make_opts(**opts)
+        r = _TuneResult()
+        _check(_lib.mce_autotune(self._h, C.byref(o), table.encode() if table else None, reps,
+                                 int(force), C.byref(r)), "autotune")
+        return _tune_dict(r)
+
     def degeneracy(self) -> tuple[np.ndarray, np.ndarray, int]:
         prio = np.zeros(max(self.n, 1), np.uint32)
         core = np.zeros(max(self.n, 1), np.int32)
@@ -440,6 +478,19 @@ class Batch:
                                      C.c_void_p(vo_addr), C.c_void_p(ao_addr), num_graphs,
                                      stream), "batch_reload")
         self.num_graphs = num_graphs
+
+    def shape_key(self) -> str:
+        buf = C.create_string_buffer(48)
+        _check(_lib.mce_batch_shape_key(self._h, buf, 48), "batch_shape_key")
+        return buf.value.decode()
+
+    def autotune(self, table: str | None = None, reps: int = 2, force: bool = False,
+                 cuda_graph=1, **opts) -> dict:
+        o = make_opts(cuda_graph=cuda_graph, **opts)
+        r = _TuneResult()
+        _check(_lib.mce_batch_autotune(self._h, C.byref(o), table.encode() if table else None,
+                                       reps, int(force), C.byref(r)), "batch_autotune")
+        return _tune_dict(r)
 
     def count(self, *, stream=None, cuda_graph=1, **opts) -> BatchResult:
         o = make_opts(stream=stream, cuda_graph=cuda_graph, **opts)
@@ -619,3 +670,14 @@ class Serve:
 
     def __exit__(self, *a):
         self.close()
+
+
+def tune_lookup(table: str, key: str) -> dict | None:
+    """The tuned option values stored for a shape class, or None."""
+    o = _Opts()
+    _lib.mce_opts_default(C.byref(o))
+    rc = _lib.mce_tune_lookup(table.encode(), key.encode(), C.byref(o))
+    if rc in (EIO, ESTATE):
+        return None
+    _check(rc, "tune_lookup")
+    return _opts_kwargs(o)

@@ -190,3 +190,15 @@ class TestCli:
         assert r.returncode == 0
         assert "Main Task = convert" in r.stdout and "n = 3 and m = 3" in r.stdout
         assert os.path.getsize(bel) == 6 * 24
+
+
+def test_tune_table_lookup(tmp_path):
+    t = tmp_path / "tune.txt"
+    assert mce.tune_lookup(str(t), "n10-a3-k4") is None  # no table yet
+    t.write_text("# mce autotune table v1\n"
+                 "n10-a3-k4 1 1024 6 64 -1 1.5 2.0\n"
+                 "b12-n23-a4-k7 2 64 16 32 64 100.0 110.0\n")
+    assert mce.tune_lookup(str(t), "n10-a3-k4") == dict(
+        worker_list=1, donate_after=1024, donate_threshold=6, bitmap_width=64, peel_solo_max=-1)
+    assert mce.tune_lookup(str(t), "b12-n23-a4-k7")["peel_solo_max"] == 64
+    assert mce.tune_lookup(str(t), "n11-a3-k4") is None
