@@ -69,6 +69,10 @@ def parse_args():
                    help="root order (learned: the shipped cost model of the workload family; "
                         "the others are timed beside it unless --no-compare)")
     p.add_argument("--no-compare", action="store_true", help="skip the other schedules")
+    p.add_argument("--heavy-log2", type=int, default=0,
+                   help="cost schedules: roots predicted >= 2^k tree nodes run first (0: default)")
+    p.add_argument("--share-log2", type=int, default=0,
+                   help="learned schedule: roots predicted >= 2^k nodes share at once (0: default)")
     p.add_argument("--tune", choices=["table", "retune", "off"], default="table",
                    help="search settings: from the autotuner table (tuned and stored when the "
                         "shape class is missing), re-tuned, or the library defaults")
@@ -232,7 +236,8 @@ def run_mine(args, rank, world, local_rank):
     import torch
     import mce_b200 as mce
     kw = dict(worker_list=mce.WL_ON if args.wl == "on" else mce.WL_OFF,
-              donate_threshold=args.donate, peel_solo_max=args.solo, donate_after=args.after)
+              donate_threshold=args.donate, peel_solo_max=args.solo, donate_after=args.after,
+              heavy_log2=args.heavy_log2, share_log2=args.share_log2)
     scheds = {"plain": dict(sched=mce.SCHED_PLAIN), "degree": dict(sched=mce.SCHED_DEGREE)}
     wpath = os.path.join(ROOT, "mce-gpu_b200", "data", f"cost_mlp_{args.workload}.f32")
     model = None

@@ -85,7 +85,13 @@ typedef struct mce_opts {
                                root only after walking this many of its nodes */
   int32_t cuda_graph;       /* 1 = capture the search launches in a CUDA graph
                                once and replay it (default for batches)      */
-  int32_t reserved[4];
+  int32_t heavy_log2;       /* 0 = default (12): with a cost schedule, roots
+                               whose predicted tree has at least 2^heavy_log2
+                               nodes run first, largest first                */
+  int32_t share_log2;       /* 0 = default (16): with MCE_SCHED_LEARNED, roots
+                               predicted at least 2^share_log2 nodes share
+                               subtrees from their first node on             */
+  int32_t reserved[2];
   void *stream;             /* cudaStream_t to queue work on; NULL = own      */
   void *model;              /* mce_model_t for MCE_SCHED_LEARNED (NULL: the
                                degree heuristic is used instead)              */
@@ -321,8 +327,8 @@ int mce_count_oriented_noalloc(const int32_t *d_row_ptr, const int32_t *d_split,
                                int64_t num_roots, uint64_t *d_hist, void *stream);
 
 /* ---- autotuner ------------------------------------------------------------ */
-/* Per graph-shape class, the search settings (worker list, donation gate and
- * threshold, bitmap word width of narrow roots, single-block peeling of small
+/* Per graph-shape class, the search settings (donation gate and threshold,
+ * bitmap word width of narrow roots, single-block peeling of small
  * frontiers) that ran fastest in timed trials, kept in a text table with one
  * line per class.  A class is floor(log2) of the vertex count, mean degree
  * and degeneracy (and of the graph count for a batch), e.g. "n23-a4-k5" or

@@ -439,8 +439,8 @@ struct mce_model {
 
 namespace {
 
-constexpr float HEAVY_COST = 10.0f;   // predicted log2(tree nodes): run first, share at once
-constexpr float DEGREE_HEAVY = 12.0f; // degree-heuristic cost above which a root runs first
+constexpr int DEFAULT_HEAVY_LOG2 = 12;  // predicted log2(tree nodes) from which a root runs first
+constexpr int DEFAULT_SHARE_LOG2 = 16;  // ... and (learned schedule) shares from its first node
 
 int ensure_feat(mce_graph *g) {
   int rc;
@@ -477,8 +477,10 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   const int sched = o.sched == MCE_SCHED_LEARNED && !model ? MCE_SCHED_DEGREE : o.sched;
   if ((rc = run_orient(g, s, &launches, sched != MCE_SCHED_PLAIN))) return rc;
   const uint8_t *policy = nullptr;
+  const float heavy = (float)(o.heavy_log2 > 0 ? o.heavy_log2 : DEFAULT_HEAVY_LOG2);
+  const float share_cost = (float)(o.share_log2 > 0 ? o.share_log2 : DEFAULT_SHARE_LOG2);
   if (sched == MCE_SCHED_DEGREE && g->n > 0) {
-    if ((rc = rekey_launch(g->n, g->keys_in, nullptr, g->rp, g->split, nullptr, DEGREE_HEAVY,
+    if ((rc = rekey_launch(g->n, g->keys_in, nullptr, g->rp, g->split, nullptr, heavy, heavy,
                            g->sms, s, &launches)) ||
         (rc = run_sort(g, 32, s, &launches)))
       return rc;
@@ -487,7 +489,7 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
     if ((rc = compute_features(g, s, &launches)) ||
         (rc = mlp_forward_launch(model->wh, g->feat, nullptr, g->n, g->pred, g->sms, s,
                                  &launches)) ||
-        (rc = rekey_launch(g->n, g->keys_in, g->pred, g->rp, g->split, g->policy, HEAVY_COST,
+        (rc = rekey_launch(g->n, g->keys_in, g->pred, g->rp, g->split, g->policy, heavy, share_cost,
                            g->sms, s, &launches)) ||
         (rc = run_sort(g, 32, s, &launches)))
       return rc;

@@ -110,7 +110,8 @@ int mlp_grad_launch(const void *wh, const float *X, const float *Y, const int32_
 int mlp_adam_launch(float *master, void *wh, float *grad, float *m1, float *m2, float lr,
                     int step, cudaStream_t s);
 int rekey_launch(int64_t n, uint32_t *keys, const float *cost, const int32_t *rp,
-                 const int32_t *split, uint8_t *policy, float heavy_cost, int sms, cudaStream_t s,
+                 const int32_t *split, uint8_t *policy, float heavy_cost, float share_cost,
+                 int sms, cudaStream_t s,
                  int *launches);
 
 // ---- batches ------------------------------------------------------------------

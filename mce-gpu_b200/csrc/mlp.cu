@@ -272,7 +272,7 @@ __global__ void adam_kernel(float *__restrict__ master, __half *__restrict__ wh,
 // lists, and in a batch each graph stays together in L2).
 __global__ void rekey_kernel(int64_t n, uint32_t *keys, const float *__restrict__ cost,
                              const int32_t *__restrict__ rp, const int32_t *__restrict__ split,
-                             uint8_t *policy, float heavy_cost) {
+                             uint8_t *policy, float heavy_cost, float share_cost) {
   for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n;
        v += (int64_t)gridDim.x * blockDim.x) {
     const uint32_t cls = keys[v] & 0xF;
@@ -287,7 +287,7 @@ __global__ void rekey_kernel(int64_t n, uint32_t *keys, const float *__restrict_
     const bool heavy = c >= heavy_cost;
     const uint32_t q = heavy ? (uint32_t)(c * (float)(1 << 22)) : 0u;  // < 2^28
     keys[v] = (cls << 28) | (0x0FFFFFFFu - q);
-    if (policy) policy[v] = cost && heavy ? 1 : 0;
+    if (policy) policy[v] = cost && c >= share_cost ? 1 : 0;
   }
 }
 
@@ -342,10 +342,11 @@ int mlp_adam_launch(float *master, void *wh, float *grad, float *m1, float *m2, 
 }
 
 int rekey_launch(int64_t n, uint32_t *keys, const float *cost, const int32_t *rp,
-                 const int32_t *split, uint8_t *policy, float heavy_cost, int sms, cudaStream_t s,
+                 const int32_t *split, uint8_t *policy, float heavy_cost, float share_cost,
+                 int sms, cudaStream_t s,
                  int *launches) {
   if (n == 0) return MCE_OK;
-  rekey_kernel<<<sms * 8, 256, 0, s>>>(n, keys, cost, rp, split, policy, heavy_cost);
+  rekey_kernel<<<sms * 8, 256, 0, s>>>(n, keys, cost, rp, split, policy, heavy_cost, share_cost);
   MCE_CUDA(cudaGetLastError());
   if (launches) *launches += 1;
   return MCE_OK;

@@ -4,9 +4,10 @@
 // L1+IP / L1+IPX rule of thumb of its evaluation script (table.py:127).
 // A shape class buckets a graph (or a batch's disjoint union) by
 // floor(log2) of its vertex count, mean degree and degeneracy, plus the
-// batch size for batches.  Tuning walks the knobs one at a time (worker
-// list, donation gate, donation threshold, bitmap word width of narrow
-// roots, single-block peeling of small frontiers), times each value with
+// batch size for batches.  Tuning walks the knobs one at a time (donation
+// gate, donation threshold, bitmap word width of narrow roots, single-block
+// peeling of small frontiers; subtree sharing itself stays as given, since
+// without it one heavy root can run for minutes), times each value with
 // the device timers of mce_count / mce_batch_count, keeps a value only when
 // it is at least 2% faster, and checks that every trial returns the same
 // count.  The winner is stored in a text table, one line per class; later
@@ -161,14 +162,13 @@ int tune(const char *key, const mce_opts_t &base, const char *table_path, int32_
     std::vector<int32_t> values;
   };
   const Axis axes[] = {
-      {&Knobs::worker_list, {MCE_WL_ON, MCE_WL_OFF}},
       {&Knobs::donate_after, {64, 256, 1024}},
       {&Knobs::donate_threshold, {6, 10, 16}},
       {&Knobs::bitmap_width, {32, 64}},
       {&Knobs::peel_solo_max, {-1, 64}},
   };
   for (const Axis &ax : axes) {
-    if (ax.field != &Knobs::worker_list && cur.worker_list == MCE_WL_OFF &&
+    if (cur.worker_list == MCE_WL_OFF &&
         (ax.field == &Knobs::donate_after || ax.field == &Knobs::donate_threshold))
       continue;  // no sharing: the donation knobs do nothing
     Knobs best = cur;

@@ -45,7 +45,8 @@ class _Opts(C.Structure):
                 ("warps_per_root", C.c_int32), ("donate_threshold", C.c_int32),
                 ("log_roots", C.c_int32), ("x_pivot", C.c_int32),
                 ("peel_solo_max", C.c_int32), ("donate_after", C.c_int32),
-                ("cuda_graph", C.c_int32), ("reserved", C.c_int32 * 4),
+                ("cuda_graph", C.c_int32), ("heavy_log2", C.c_int32),
+                ("share_log2", C.c_int32), ("reserved", C.c_int32 * 2),
                 ("stream", C.c_void_p), ("model", C.c_void_p)]
 
 
@@ -346,13 +347,15 @@ def _stats_dict(st: _Stats) -> dict:
 
 def make_opts(*, sched=SCHED_PLAIN, bitmap_width=0, log_roots=False, level=LEVEL_L1,
               induced=INDUCED_P, worker_list=WL_ON, donate_threshold=0, x_pivot=0,
-              peel_solo_max=0, donate_after=0, cuda_graph=0, model=None, stream=None) -> _Opts:
+              peel_solo_max=0, donate_after=0, cuda_graph=0, heavy_log2=0, share_log2=0,
+              model=None, stream=None) -> _Opts:
     o = _Opts()
     _lib.mce_opts_default(C.byref(o))
     o.sched, o.bitmap_width, o.log_roots = sched, bitmap_width, int(bool(log_roots))
     o.level, o.induced, o.worker_list = level, induced, worker_list
     o.donate_threshold, o.x_pivot = donate_threshold, x_pivot
     o.peel_solo_max, o.donate_after, o.cuda_graph = peel_solo_max, donate_after, cuda_graph
+    o.heavy_log2, o.share_log2 = heavy_log2, share_log2
     o.stream = stream
     o.model = model._h if model is not None else None
     return o
