@@ -514,6 +514,9 @@ def run_serve(args, rank, world, local_rank):
             "latency_ms": {"p50": pct(lat, 50), "p90": pct(lat, 90), "p99": pct(lat, 99),
                            "max": float(lat.max())},
             "device_ms": {"p50": pct(dev_ms, 50), "p99": pct(dev_ms, 99)},
+            "slowest_1pct_phase_ms": {  # where the tail requests spend their slot time
+                ph: float(np.mean(res[ph + "_ns"][ok][np.argsort(dev_ms)[-max(1, len(dev_ms) // 100):]]) / 1e6)
+                for ph in ("extract", "order", "search")},
             "ego_n": {"p50": pct(res["ego_n"], 50), "max": int(res["ego_n"].max())},
             "ego_arcs": {"p50": pct(res["ego_arcs"], 50), "max": int(res["ego_arcs"].max())},
             "cliques_per_request": {"p50": pct(res["count"][ok], 50),

@@ -91,7 +91,9 @@ typedef struct mce_opts {
   int32_t share_log2;       /* 0 = default (16): with MCE_SCHED_LEARNED, roots
                                predicted at least 2^share_log2 nodes share
                                subtrees from their first node on             */
-  int32_t reserved[2];
+  int32_t warp_log;         /* 1 = record per search warp its SM, tree nodes
+                               and donations (read with mce_warp_log)        */
+  int32_t reserved[1];
   void *stream;             /* cudaStream_t to queue work on; NULL = own      */
   void *model;              /* mce_model_t for MCE_SCHED_LEARNED (NULL: the
                                degree heuristic is used instead)              */
@@ -223,6 +225,17 @@ int mce_root_log(mce_graph_t g, uint64_t *nodes_out);
 /* Per-root maximal-clique counts of the last mce_count that ran with
  * opts.log_roots = 1 (n entries, 0 for non-roots).                          */
 int mce_root_counts(mce_graph_t g, uint64_t *count_out);
+
+/* Per-warp load of the last mce_count that ran with opts.warp_log = 1: for
+ * every search warp (all engine classes, widest class first) the SM it ran
+ * on, the search-tree nodes it walked (its roots and the subtrees it took)
+ * and the subtrees it handed to other warps.  The counterpart of the
+ * reference's -m mce-lb-eval / mce-donor-eval per-block lines
+ * (mce/mce_kernel_wl_lb.cuh:157, mce/mce_kernel_wl_donor.cuh:157), with a
+ * warp as the unit of work.  Arrays (nullable) take up to `cap` entries;
+ * *count_out gets the number of warps.                                      */
+int mce_warp_log(mce_graph_t g, uint32_t *sm_out, uint64_t *nodes_out, uint64_t *donations_out,
+                 int64_t cap, int64_t *count_out);
 
 /* ---- batches of graphs ------------------------------------------------------ */
 typedef struct mce_batch *mce_batch_t;
@@ -394,6 +407,10 @@ typedef struct mce_serve_result {
   int32_t ego_arcs;   /* ego-graph arcs (2 x edges)                         */
   uint32_t limits;    /* MCE_SERVE_* bits of the limits a request hit       */
   uint64_t device_ns; /* time the slot spent on the request                 */
+  uint32_t extract_ns; /* ... building the ego graph                        */
+  uint32_t order_ns;   /* ... peeling and orienting it                      */
+  uint32_t search_ns;  /* ... searching its roots                           */
+  uint32_t pad2;
 } mce_serve_result_t;
 
 #define MCE_SERVE_OVER_BUDGET 0x20u /* search passed max_nodes             */

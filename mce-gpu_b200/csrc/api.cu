@@ -64,6 +64,8 @@ struct mce_graph {
   uint32_t *fetch = nullptr, *err = nullptr;
   unsigned long long *hist = nullptr, *nodes = nullptr;
   unsigned long long *root_nodes = nullptr, *root_count = nullptr;
+  unsigned long long *wlog = nullptr;     // per-warp {SM, nodes, donations} (opts.warp_log)
+  int64_t wlog_cap = 0, wlog_count = 0;
   float *feat = nullptr, *pred = nullptr;  // per-vertex features (n x 8) and predicted cost
   uint8_t *policy = nullptr;              // per-root sharing policy from the model
   unsigned long long *slab = nullptr;
@@ -96,7 +98,7 @@ void free_graph_bufs(mce_graph *g) {
   dfree(g->hb0); dfree(g->hb1); dfree(g->hb2);
   dfree(g->keys_in); dfree(g->keys_out); dfree(g->vals_in); dfree(g->roots);
   dfree(g->root_nodes); dfree(g->root_count);
-  dfree(g->feat); dfree(g->pred); dfree(g->policy);
+  dfree(g->feat); dfree(g->pred); dfree(g->policy); dfree(g->wlog);
   g->cap_n = g->cap_m = -1;
 }
 
@@ -524,6 +526,17 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
     if ((rc = dalloc(&g->root_nodes, (size_t)g->cap_n + 1))) return rc;
     if ((rc = dalloc(&g->root_count, (size_t)g->cap_n + 1))) return rc;
   }
+  int64_t wlog_base[NCLS] = {0}, wlog_total = 0;
+  for (int c : {CLS_MEM, CLS_R64, CLS_R32}) {  // the launch order below
+    wlog_base[c] = wlog_total;
+    if (grid[c]) wlog_total += (int64_t)grid[c] * (block[c] / 32);
+  }
+  if (o.warp_log && wlog_total > g->wlog_cap) {
+    dfree(g->wlog);
+    if ((rc = dalloc(&g->wlog, 3 * (size_t)wlog_total))) return rc;
+    g->wlog_cap = wlog_total;
+  }
+  g->wlog_count = o.warp_log ? wlog_total : 0;
   BKArgs a;
   std::memset(&a, 0, sizeof(a));
   a.rp = g->rp;
@@ -557,7 +570,7 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
     int grid[NCLS], block[NCLS];
     int dcap, xcap, wbits, share, dmin, log;
     uint32_t dafter;
-    const void *slab, *graph_count, *graph_of, *root_nodes, *policy, *q[NCLS], *bufs[4];
+    const void *slab, *graph_count, *graph_of, *root_nodes, *policy, *q[NCLS], *bufs[4], *wlog;
     int64_t n, G;
   } key;
   std::memset(&key, 0, sizeof(key));
@@ -578,6 +591,7 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   key.root_nodes = a.root_nodes;
   key.graph_of = a.graph_of;
   key.policy = a.policy;
+  key.wlog = o.warp_log ? g->wlog : nullptr;
   key.bufs[0] = g->rp;
   key.bufs[1] = g->split;
   key.bufs[2] = g->cs;
@@ -596,12 +610,15 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
     MCE_CUDA(cudaMemsetAsync(g->err, 0, sizeof(uint32_t) * 4, s));
     MCE_CUDA(cudaMemsetAsync(g->hist, 0, sizeof(unsigned long long) * MCE_HIST_MAX, s));
     MCE_CUDA(cudaMemsetAsync(g->nodes, 0, sizeof(unsigned long long) * 4, s));
+    if (o.warp_log)
+      MCE_CUDA(cudaMemsetAsync(g->wlog, 0, sizeof(unsigned long long) * 3 * (size_t)wlog_total, s));
     // widest roots first so the long trees start early
     const int order[3] = {CLS_MEM, CLS_R64, CLS_R32};
     for (int c : order) {
       if (!grid[c]) continue;
       a.slab_words = bk_slab_words(c, dcap, xcap);
       a.q = share ? qv[c] : QueueView();
+      a.warp_log = o.warp_log ? g->wlog + 3 * wlog_base[c] : nullptr;
       if (share && (r2 = queue_launch_init(a.q, s, &launches))) return r2;
       if ((r2 = bk_launch(c, wbits, a, grid[c], block[c], smem[c], s, &launches))) return r2;
     }
@@ -720,6 +737,24 @@ int mce_root_log(mce_graph_t g, uint64_t *nodes_out) {
   MCE_CUDA(cudaSetDevice(g->device));
   MCE_CUDA(cudaMemcpy(nodes_out, g->root_nodes, sizeof(uint64_t) * (size_t)g->n,
                       cudaMemcpyDeviceToHost));
+  return MCE_OK;
+}
+
+int mce_warp_log(mce_graph_t g, uint32_t *sm_out, uint64_t *nodes_out, uint64_t *donations_out,
+                 int64_t cap, int64_t *count_out) {
+  if (!g || cap < 0) return MCE_EINVAL;
+  if (count_out) *count_out = g->wlog_count;
+  const int64_t k = cap < g->wlog_count ? cap : g->wlog_count;
+  if (k == 0) return MCE_OK;
+  MCE_CUDA(cudaSetDevice(g->device));
+  std::vector<unsigned long long> h(3 * (size_t)k);
+  MCE_CUDA(cudaMemcpy(h.data(), g->wlog, sizeof(unsigned long long) * 3 * (size_t)k,
+                      cudaMemcpyDeviceToHost));
+  for (int64_t i = 0; i < k; ++i) {
+    if (sm_out) sm_out[i] = (uint32_t)h[3 * i];
+    if (nodes_out) nodes_out[i] = h[3 * i + 1];
+    if (donations_out) donations_out[i] = h[3 * i + 2];
+  }
   return MCE_OK;
 }
 

@@ -40,7 +40,7 @@ __global__ void queue_init_kernel(QueueView q) {
 
 namespace {
 
-template <typename Word, int NR>
+template <typename Word, int NR, bool Log = false>
 __global__ void __launch_bounds__(REG_BLOCK) bk_reg_kernel(BKArgs a, int cls) {
   __shared__ RegSmem<Word, NR> sm_all[REG_BLOCK / 32];
   RegSmem<Word, NR> &sm = sm_all[threadIdx.x >> 5];
@@ -63,7 +63,8 @@ __global__ void __launch_bounds__(REG_BLOCK) bk_reg_kernel(BKArgs a, int cls) {
       const int32_t r = a.roots[idx];
       reg_encode<Word, NR>(a, sm, sl, r, rt);
       u64 nd = 0, cnt = 0;
-      reg_tree<Word, NR>(a, sm, sl, rt, WOps<Word>::low(rt.d), (Word)0, (Word)0, h0, h1, nd, cnt);
+      reg_tree<Word, NR, false, Log>(a, sm, sl, rt, WOps<Word>::low(rt.d), (Word)0, (Word)0, h0, h1, nd,
+                                      cnt);
       nodes += nd;
       root_done(a, r, nd, cnt);
     }
@@ -90,7 +91,7 @@ __global__ void __launch_bounds__(REG_BLOCK) bk_reg_kernel(BKArgs a, int cls) {
           const Word S = (Word)__shfl_sync(MCE_FULL, t3, 3);
           if (r != rt.r) reg_encode<Word, NR>(a, sm, sl, r, rt);
           u64 nd = 0, cnt = 0;
-          reg_tree<Word, NR>(a, sm, sl, rt, P, X, S, h0, h1, nd, cnt);
+          reg_tree<Word, NR, false, Log>(a, sm, sl, rt, P, X, S, h0, h1, nd, cnt);
           nodes += nd;
           root_done(a, r, nd, cnt);
         });
@@ -98,8 +99,14 @@ __global__ void __launch_bounds__(REG_BLOCK) bk_reg_kernel(BKArgs a, int cls) {
   if (h0) atomicAdd(&a.hist[lane + 2], h0);
   if (h1) atomicAdd(&a.hist[lane + 34], h1);
   if (lane == 0 && nodes) atomicAdd(a.nodes, nodes);  // warp-uniform count
+  if (Log && lane == 0) {  // opts.warp_log
+    u64 *w = warp_record(a);
+    w[0] = sm_id();
+    w[1] = nodes;
+  }
 }
 
+template <bool Log = false>
 __global__ void __launch_bounds__(MEM_BLOCK) bk_mem_kernel(BKArgs a, int cls) {
   __shared__ MemSmem sm_all[MEM_BLOCK / 32];
   MemSmem &sm = sm_all[threadIdx.x >> 5];
@@ -128,7 +135,7 @@ __global__ void __launch_bounds__(MEM_BLOCK) bk_mem_kernel(BKArgs a, int cls) {
     }
     __syncwarp();
     u64 nd = 0, cnt = 0;
-    mem_tree(a, sl, rt, h0, h1, nd, cnt);
+    mem_tree<false, Log>(a, sl, rt, h0, h1, nd, cnt);
     nodes += nd;
     root_done(a, r, nd, cnt);
   }
@@ -170,7 +177,7 @@ __global__ void __launch_bounds__(MEM_BLOCK) bk_mem_kernel(BKArgs a, int cls) {
           }
           __syncwarp();
           u64 nd = 0, cnt = 0;
-          mem_tree(a, sl, rt, h0, h1, nd, cnt);
+          mem_tree<false, Log>(a, sl, rt, h0, h1, nd, cnt);
           nodes += nd;
           root_done(a, r, nd, cnt);
         });
@@ -178,6 +185,11 @@ __global__ void __launch_bounds__(MEM_BLOCK) bk_mem_kernel(BKArgs a, int cls) {
   if (h0) atomicAdd(&a.hist[lane + 2], h0);
   if (h1) atomicAdd(&a.hist[lane + 34], h1);
   if (lane == 0 && nodes) atomicAdd(a.nodes, nodes);  // warp-uniform count
+  if (Log && lane == 0) {  // opts.warp_log
+    u64 *w = warp_record(a);
+    w[0] = sm_id();
+    w[1] = nodes;
+  }
 }
 
 }  // namespace
@@ -221,18 +233,32 @@ int bk_warps_for_class(int cls, int sms, int *warps, int *block, int *smem) {
 int bk_launch(int cls, int word_bits, const BKArgs &a, int grid, int block, int smem,
               cudaStream_t s, int *launches) {
   if (grid <= 0) return MCE_OK;
+  const bool log = a.warp_log != nullptr;  // the evaluation variants record per-warp load
   switch (cls) {
     case CLS_R32:
-      if (word_bits == 64)
-        bk_reg_kernel<u64, 1><<<grid, block, smem, s>>>(a, cls);
-      else
-        bk_reg_kernel<uint32_t, 1><<<grid, block, smem, s>>>(a, cls);
+      if (word_bits == 64) {
+        if (log)
+          bk_reg_kernel<u64, 1, true><<<grid, block, smem, s>>>(a, cls);
+        else
+          bk_reg_kernel<u64, 1><<<grid, block, smem, s>>>(a, cls);
+      } else {
+        if (log)
+          bk_reg_kernel<uint32_t, 1, true><<<grid, block, smem, s>>>(a, cls);
+        else
+          bk_reg_kernel<uint32_t, 1><<<grid, block, smem, s>>>(a, cls);
+      }
       break;
     case CLS_R64:
-      bk_reg_kernel<u64, 2><<<grid, block, smem, s>>>(a, cls);
+      if (log)
+        bk_reg_kernel<u64, 2, true><<<grid, block, smem, s>>>(a, cls);
+      else
+        bk_reg_kernel<u64, 2><<<grid, block, smem, s>>>(a, cls);
       break;
     case CLS_MEM:
-      bk_mem_kernel<<<grid, block, smem, s>>>(a, cls);
+      if (log)
+        bk_mem_kernel<true><<<grid, block, smem, s>>>(a, cls);
+      else
+        bk_mem_kernel<><<<grid, block, smem, s>>>(a, cls);
       break;
     default:
       return MCE_EINVAL;

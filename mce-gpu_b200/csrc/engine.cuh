@@ -83,6 +83,17 @@ __device__ __forceinline__ bool wants_task(const QueueView &q) {
   return __shfl_sync(MCE_FULL, w, 0) != 0;
 }
 
+// Per-warp evaluation log (opts.warp_log): this warp's record in the launch.
+__device__ __forceinline__ u64 *warp_record(const BKArgs &a) {
+  return a.warp_log + 3 * (((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+}
+
+__device__ __forceinline__ uint32_t sm_id() {
+  uint32_t id;
+  asm volatile("mov.u32 %0, %%smid;" : "=r"(id));
+  return id;
+}
+
 // Per-root outputs shared by donor and takers: accumulate.
 __device__ __forceinline__ void root_done(const BKArgs &a, int32_t r, u64 nodes, u64 cnt) {
   if (lane_id() != 0) return;
@@ -292,8 +303,9 @@ __device__ void reg_encode(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab
 
 // Walk the subtree under node (P, X, S) of root rt.r.  For the root itself
 // S = 0; for a task S holds the vertices chosen above the node.  With
-// Budget, the walk stops once it has visited a.node_budget nodes.
-template <typename Word, int NR, bool Budget = false>
+// Budget, the walk stops once it has visited a.node_budget nodes; with Log,
+// the warp's donations are counted in its a.warp_log record.
+template <typename Word, int NR, bool Budget = false, bool Log = false>
 __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<Word> &sl,
                          const RegRoot<Word> &rt, Word P, Word X, Word S, u64 &h0, u64 &h1,
                          u64 &nodes, u64 &cnt) {
@@ -437,8 +449,10 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
       }
       if (want) {
         const u64 w0 = (u64)(uint32_t)rt.r, w1 = (u64)Pc, w2 = (u64)Xc, w3 = (u64)Sc;
-        if (q_push(a.q, [&](uint32_t k2) { return k2 == 0 ? w0 : k2 == 1 ? w1 : k2 == 2 ? w2 : w3; }))
+        if (q_push(a.q, [&](uint32_t k2) { return k2 == 0 ? w0 : k2 == 1 ? w1 : k2 == 2 ? w2 : w3; })) {
+          if (Log && lane == 0) warp_record(a)[2] += 1;  // opts.warp_log
           continue;
+        }
         want = false;
       }
     }
@@ -602,7 +616,7 @@ __device__ void mem_encode(const BKArgs &a, MemSmem &sm, const Slab &sl, int32_t
 }
 
 // Walk the subtree under frame 0 of the slab stack (P, X, S already there).
-template <bool Budget = false>
+template <bool Budget = false, bool Log = false>
 __device__ void mem_tree(const BKArgs &a, const Slab &sl, const MemRoot &rt, u64 &h0, u64 &h1,
                          u64 &nodes, u64 &cnt) {
   const int lane = (int)lane_id();
@@ -769,8 +783,10 @@ __device__ void mem_tree(const BKArgs &a, const Slab &sl, const MemRoot &rt, u64
             const uint32_t part = (k2 - 1) / WM, w = (k2 - 1) % WM;
             if ((int)w >= Wr) return 0ull;
             return part == 0 ? Cp[w] : part == 1 ? Cx[w] : Cs[w];
-          }))
+          })) {
+        if (Log && lane == 0) warp_record(a)[2] += 1;  // opts.warp_log
         continue;
+      }
       want = false;
     }
     k = (int)__reduce_max_sync(MCE_FULL, (unsigned)k);

@@ -88,6 +88,7 @@ struct BKArgs {
   uint64_t wait_limit_ns;        // an idle warp gives up after this long without progress
   const uint8_t *policy;         // nullable [n]: 1 = root may share subtrees at once
   unsigned long long node_budget;  // 0: none; else a tree stops past this many nodes
+  unsigned long long *warp_log;  // nullable: per warp of the launch {SM id, tree nodes, donations}
 };
 
 // Launch the engine of one class.  warps_out: number of warps launched (slab sizing).

@@ -52,7 +52,7 @@ struct SvEntry {             // one request, in mapped host memory
   int32_t status, ego_n, ego_arcs;
   uint32_t limits;           // MCE_ERR_* bits of the limits the request hit
   uint32_t done;             // id + 1 once the answer is written
-  uint32_t pad;
+  uint32_t extract_ns, order_ns, search_ns;  // the request's phases on the slot
 };
 
 struct SvHostHdr {           // mapped host memory, host-written
@@ -504,6 +504,7 @@ __global__ void __launch_bounds__(SV_BLOCK) serve_kernel(ServeArgs S) {
     const uint32_t req = sh.req;
     if (req == SV_EXIT) break;
     const uint64_t t0 = globaltimer_ns();
+    uint64_t t1 = t0, t2 = t0;
     SvEntry *E = S.ent + (req % S.ring);
     const int64_t seed = *(volatile int64_t *)&E->seed;
     int32_t status = MCE_OK;
@@ -513,6 +514,7 @@ __global__ void __launch_bounds__(SV_BLOCK) serve_kernel(ServeArgs S) {
       status = MCE_EINVAL;
     } else {
       n = ego_extract(S, A, seed, sortbuf, sh);
+      t1 = t2 = globaltimer_ns();
       if (n < 0) {
         status = MCE_ELIMIT;
         limits = MCE_ERR_ARCS;
@@ -522,6 +524,7 @@ __global__ void __launch_bounds__(SV_BLOCK) serve_kernel(ServeArgs S) {
     if (status == MCE_OK) {
       ego_peel(A, n, sh);
       ego_orient(A, n);
+      t2 = globaltimer_ns();
       unsigned long long mine = 0, h0 = 0, h1 = 0;
       RegRoot<uint32_t> rt32;
       RegRoot<u64> rt64;
@@ -571,7 +574,12 @@ __global__ void __launch_bounds__(SV_BLOCK) serve_kernel(ServeArgs S) {
     __syncthreads();
     if (threadIdx.x == 0) {
       E->count = status == MCE_OK ? sh.total : 0ull;
-      E->device_ns = globaltimer_ns() - t0;
+      const uint64_t t3 = globaltimer_ns();
+      E->device_ns = t3 - t0;
+      auto clamp32 = [](uint64_t x) { return (uint32_t)(x > 0xFFFFFFFFull ? 0xFFFFFFFFull : x); };
+      E->extract_ns = clamp32(t1 - t0);
+      E->order_ns = clamp32(t2 - t1);
+      E->search_ns = clamp32(t2 > t0 ? t3 - t2 : 0ull);
       E->status = status;
       E->limits = limits;
       E->ego_n = n;
@@ -785,6 +793,9 @@ extern "C" int mce_serve_poll(mce_serve_t s, uint64_t id, mce_serve_result_t *re
   res->ego_arcs = e.ego_arcs;
   res->limits = e.limits;
   res->device_ns = e.device_ns;
+  res->extract_ns = e.extract_ns;
+  res->order_ns = e.order_ns;
+  res->search_ns = e.search_ns;
   s->taken[i % s->ring] = 1;
   sv_retire(s);
   return MCE_OK;

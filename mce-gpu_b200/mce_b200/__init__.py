@@ -46,7 +46,7 @@ class _Opts(C.Structure):
                 ("log_roots", C.c_int32), ("x_pivot", C.c_int32),
                 ("peel_solo_max", C.c_int32), ("donate_after", C.c_int32),
                 ("cuda_graph", C.c_int32), ("heavy_log2", C.c_int32),
-                ("share_log2", C.c_int32), ("reserved", C.c_int32 * 2),
+                ("share_log2", C.c_int32), ("warp_log", C.c_int32), ("reserved", C.c_int32 * 1),
                 ("stream", C.c_void_p), ("model", C.c_void_p)]
 
 
@@ -94,7 +94,8 @@ class _ServeOpts(C.Structure):
 class _ServeResult(C.Structure):
     _fields_ = [("count", C.c_uint64), ("seed", C.c_int64), ("status", C.c_int32),
                 ("ego_n", C.c_int32), ("ego_arcs", C.c_int32), ("limits", C.c_uint32),
-                ("device_ns", C.c_uint64)]
+                ("device_ns", C.c_uint64), ("extract_ns", C.c_uint32), ("order_ns", C.c_uint32),
+                ("search_ns", C.c_uint32), ("pad2", C.c_uint32)]
 
 
 class _ServeStats(C.Structure):
@@ -123,6 +124,7 @@ _sigs = {
     "mce_count": (C.c_int, [_P, _P, _P, _P, _P]),
     "mce_root_log": (C.c_int, [_P, _P]),
     "mce_root_counts": (C.c_int, [_P, _P]),
+    "mce_warp_log": (C.c_int, [_P, _P, _P, _P, C.c_int64, _P]),
     "mce_count_oriented_noalloc": (C.c_int, [_P, _P, _P, _P, C.c_int64, _P, _P]),
     "mce_batch_upload": (C.c_int, [_P, _P, _P, _P, C.c_int32, C.c_int32, _P, _P]),
     "mce_batch_reload": (C.c_int, [_P, _P, _P, _P, _P, C.c_int32, _P]),
@@ -348,14 +350,14 @@ def _stats_dict(st: _Stats) -> dict:
 def make_opts(*, sched=SCHED_PLAIN, bitmap_width=0, log_roots=False, level=LEVEL_L1,
               induced=INDUCED_P, worker_list=WL_ON, donate_threshold=0, x_pivot=0,
               peel_solo_max=0, donate_after=0, cuda_graph=0, heavy_log2=0, share_log2=0,
-              model=None, stream=None) -> _Opts:
+              warp_log=False, model=None, stream=None) -> _Opts:
     o = _Opts()
     _lib.mce_opts_default(C.byref(o))
     o.sched, o.bitmap_width, o.log_roots = sched, bitmap_width, int(bool(log_roots))
     o.level, o.induced, o.worker_list = level, induced, worker_list
     o.donate_threshold, o.x_pivot = donate_threshold, x_pivot
     o.peel_solo_max, o.donate_after, o.cuda_graph = peel_solo_max, donate_after, cuda_graph
-    o.heavy_log2, o.share_log2 = heavy_log2, share_log2
+    o.heavy_log2, o.share_log2, o.warp_log = heavy_log2, share_log2, int(bool(warp_log))
     o.stream = stream
     o.model = model._h if model is not None else None
     return o
@@ -441,6 +443,17 @@ class Graph:
         out = np.zeros(max(self.n, 1), np.uint64)
         _check(_lib.mce_root_log(self._h, _ptr(out)), "root_log")
         return out[:self.n]
+
+    def warp_log(self) -> dict:
+        """Per search warp of the last count(warp_log=True): SM id, tree nodes, donations."""
+        k = C.c_int64()
+        _check(_lib.mce_warp_log(self._h, None, None, None, 0, C.byref(k)), "warp_log")
+        sm = np.zeros(max(k.value, 1), np.uint32)
+        nodes = np.zeros(max(k.value, 1), np.uint64)
+        don = np.zeros(max(k.value, 1), np.uint64)
+        _check(_lib.mce_warp_log(self._h, _ptr(sm), _ptr(nodes), _ptr(don), k.value, C.byref(k)),
+               "warp_log")
+        return {"sm": sm[:k.value], "nodes": nodes[:k.value], "donations": don[:k.value]}
 
     def root_counts(self) -> np.ndarray:
         out = np.zeros(max(self.n, 1), np.uint64)
@@ -599,12 +612,14 @@ def root_features(g: "Graph") -> np.ndarray:
 # ---------------------------------------------------------------------------
 SERVE_RESULT_DTYPE = np.dtype([("count", np.uint64), ("seed", np.int64), ("status", np.int32),
                                ("ego_n", np.int32), ("ego_arcs", np.int32), ("limits", np.uint32),
-                               ("device_ns", np.uint64)])
+                               ("device_ns", np.uint64), ("extract_ns", np.uint32),
+                               ("order_ns", np.uint32), ("search_ns", np.uint32),
+                               ("pad2", np.uint32)])
 assert SERVE_RESULT_DTYPE.itemsize == C.sizeof(_ServeResult)
 
 
 def _result_dict(r: _ServeResult) -> dict:
-    return {k: getattr(r, k) for k, _ in _ServeResult._fields_}
+    return {k: getattr(r, k) for k, _ in _ServeResult._fields_ if k != "pad2"}
 
 
 class Serve:
