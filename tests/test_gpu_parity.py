@@ -200,3 +200,33 @@ def test_worker_list_on_off_identical(maker):
         assert tot == t and np.array_equal(hist, h)
         assert np.array_equal(rc, rc_o)
         assert np.array_equal(rn, rn_o)  # donation moves subtrees, never changes them
+
+
+def test_warp_log_accounts_for_every_node_and_donation():
+    hg = mce.gen_rmat(12, 16, 0.57, 0.19, 0.19, 7)
+    with mce.Graph.from_host(hg) as g:
+        r = g.count(warp_log=True, donate_after=1)
+        log = g.warp_log()
+        plain = g.count()
+    assert r.total == plain.total
+    assert len(log["sm"]) > 0 and int(log["sm"].max()) < 1024
+    assert int(log["nodes"].sum()) == r.stats["tree_nodes"]
+    assert int(log["donations"].sum()) == r.stats["donations"] and r.stats["donations"] > 0
+
+
+@pytest.mark.skipif(not os.path.exists(CLI), reason="CLI not built")
+@pytest.mark.parametrize("task,header", [("mce-lb-eval", "Number of traversed nodes"),
+                                         ("mce-donor-eval", "Number of donations")])
+def test_cli_eval_lines(tmp_path, task, header):
+    import re
+    import subprocess
+    hg = mce.gen_rmat(11, 16, 0.57, 0.19, 0.19, 7)
+    bel = str(tmp_path / "g.bel")
+    mce.bel_write(bel, hg)
+    out = subprocess.run([CLI, "-m", task, "-g", bel, "-d", "0", "-p", "l1", "-i", "p", "-w", "wl"],
+                         capture_output=True, text=True, timeout=120).stdout
+    assert header in out
+    found = int(re.findall(r"Found (.*) maximal cliques in total", out)[0].replace(",", ""))
+    assert found == oracle.count(hg)[0]
+    rows = re.findall(r"([0-9]+), ([0-9]+), ([0-9]+)", out)  # the reference's plot.py pattern
+    assert len(rows) > 0 and all(int(sm) < 1024 for _, sm, _ in rows)
