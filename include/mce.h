@@ -191,8 +191,19 @@ int mce_graph_upload(const int32_t *row_ptr, const int32_t *col, int64_t n, int6
 int mce_graph_reload(mce_graph_t g, const int32_t *row_ptr, const int32_t *col, int64_t n,
                      int64_t m, void *stream);
 
+/* Vertex and arc count of a handle. */
+int mce_graph_size(mce_graph_t g, int64_t *n, int64_t *m);
+
 /* Free a handle and every device buffer it owns. */
 int mce_graph_free(mce_graph_t g);
+
+/* Read a .bel file straight into a device handle: the records stream
+ * through pinned staging buffers to the device, where they are decoded and
+ * checked and the row offsets are built (the host reader's checks, same
+ * MCE_EFORMAT cases).  Replaces read_bel + from_edgelist + the upload
+ * (include/fileop.h:81-129, include/csrcoo.cuh:41-81, src/main.cu:53-93)
+ * for callers that do not need the graph on the host.                      */
+int mce_bel_load(const char *path, int32_t device, void *stream, mce_graph_t *out);
 
 /* Degeneracy order of the uploaded graph.  Replaces
  * graph::SingleGPU_Kcore::findKcoreIncremental_async (include/kcore.cuh:233-316).

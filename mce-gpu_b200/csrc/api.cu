@@ -139,6 +139,8 @@ struct BatchCtx {
   unsigned long long *graph_count;     // device, G
   uint64_t *per_graph_out;             // host, G
   int64_t G;
+  const int64_t *vtx_off, *arc_off;    // device, G + 1: the uploaded layout
+  const int32_t *order;                // device, G: graphs largest first
 };
 
 int check_args(const int32_t *row_ptr, const int32_t *col, int64_t n, int64_t m) {
@@ -165,7 +167,8 @@ int upload_csr(mce_graph *g, const int32_t *row_ptr, const int32_t *col, int64_t
 }
 
 // Stage 1: peel -> prio, core.
-int run_peel(mce_graph *g, cudaStream_t s, int *launches, int solo_opt = 0) {
+int run_peel(mce_graph *g, cudaStream_t s, int *launches, int solo_opt = 0,
+             const BatchCtx *bc = nullptr) {
   if (g->n == 0) return MCE_OK;
   PeelArgs pa;
   pa.n = g->n;
@@ -186,6 +189,9 @@ int run_peel(mce_graph *g, cudaStream_t s, int *launches, int solo_opt = 0) {
   pa.ctl = g->peel_ctl;
   pa.wait_limit_ns = WAIT_LIMIT_NS;
   pa.solo_max = solo_opt < 0 ? 0u : solo_opt == 0 ? DEFAULT_SOLO_MAX : (uint32_t)solo_opt;
+  if (bc)  // a batch: every graph peeled by one block, no grid-wide rounds
+    return peel_segments_launch(pa, bc->vtx_off, bc->arc_off, bc->order, (int32_t)bc->G, s,
+                                launches);
   return peel_launch(pa, s, launches);
 }
 
@@ -272,6 +278,29 @@ int ensure_slab(mce_graph *g, size_t bytes) {
 }  // namespace
 
 namespace mce {
+// A new handle sized for n vertices and m arcs whose CSR the caller writes
+// on the device (the .bel loader): row_ptr, col, and the m-entry split-CSR
+// array as scratch (orientation rewrites it).
+int graph_adopt(int32_t device, int64_t n, int64_t m, struct ::mce_graph **out, int32_t **rp,
+                int32_t **col, int32_t **scratch, cudaStream_t *own) {
+  int rc;
+  if (n < 0 || m < 0 || n >= ((int64_t)1 << 31) - 1 || m >= ((int64_t)1 << 31)) return MCE_ELIMIT;
+  mce_graph *g = nullptr;
+  if ((rc = graph_create(device, &g))) return rc;
+  if ((rc = alloc_graph_bufs(g, n, m))) {
+    mce_graph_free(g);
+    return rc;
+  }
+  g->n = n;
+  g->m = m;
+  *out = g;
+  *rp = g->rp;
+  *col = g->col;
+  *scratch = g->cs;
+  *own = g->own;
+  return MCE_OK;
+}
+
 // sizes of a graph handle and the union graph of a batch (autotuner)
 int graph_shape(const struct ::mce_graph *g, int64_t *n, int64_t *m) {
   if (!g) return MCE_EINVAL;
@@ -357,6 +386,13 @@ int mce_graph_reload(mce_graph_t g, const int32_t *row_ptr, const int32_t *col, 
   if (rc) return rc;
   MCE_CUDA(cudaSetDevice(g->device));
   return upload_csr(g, row_ptr, col, n, m, pick_stream(g, stream));
+}
+
+int mce_graph_size(mce_graph_t g, int64_t *n, int64_t *m) {
+  if (!g || !n || !m) return MCE_EINVAL;
+  *n = g->n;
+  *m = g->m;
+  return MCE_OK;
 }
 
 int mce_graph_free(mce_graph_t g) {
@@ -470,7 +506,7 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   mce_stats_t st;
   std::memset(&st, 0, sizeof(st));
   MCE_CUDA(cudaEventRecord(g->ev[0], s));
-  if ((rc = run_peel(g, s, &launches, o.peel_solo_max))) return rc;
+  if ((rc = run_peel(g, s, &launches, o.peel_solo_max, bc))) return rc;
   MCE_CUDA(cudaEventRecord(g->ev[1], s));
   // Root order: plain = vertex id within each engine class; degree = a
   // degree-based cost; learned = the model's predicted tree size.  Larger
@@ -779,6 +815,8 @@ struct mce_batch {
   unsigned long long *graph_count = nullptr;
   int32_t *rp_local = nullptr, *col_local = nullptr;  // uploaded concatenations
   int64_t *vtx_off = nullptr, *arc_off = nullptr;
+  int32_t *order = nullptr;    // graph ids by arc count, largest first (per-graph peel)
+  int32_t *order_h = nullptr;  // its pinned host staging copy
   int64_t cap_rows = -1, cap_m = -1, cap_g = -1;
 };
 
@@ -804,6 +842,9 @@ void batch_free_bufs(mce_batch *b) {
   dfree(b->col_local);
   dfree(b->vtx_off);
   dfree(b->arc_off);
+  dfree(b->order);
+  if (b->order_h) cudaFreeHost(b->order_h);
+  b->order_h = nullptr;
   b->cap_rows = b->cap_m = b->cap_g = -1;
 }
 
@@ -819,8 +860,12 @@ int batch_load(mce_batch *b, const int32_t *row_ptr, const int32_t *col, const i
     batch_free_bufs(b);
     if ((rc = dalloc(&b->graph_of, (size_t)n + 1)) || (rc = dalloc(&b->graph_count, (size_t)G)) ||
         (rc = dalloc(&b->rp_local, (size_t)rows)) || (rc = dalloc(&b->col_local, (size_t)m)) ||
-        (rc = dalloc(&b->vtx_off, (size_t)G + 1)) || (rc = dalloc(&b->arc_off, (size_t)G + 1)))
+        (rc = dalloc(&b->vtx_off, (size_t)G + 1)) || (rc = dalloc(&b->arc_off, (size_t)G + 1)) ||
+        (rc = dalloc(&b->order, (size_t)G)))
       return rc;
+    if (cudaHostAlloc((void **)&b->order_h, sizeof(int32_t) * (size_t)G, cudaHostAllocDefault) !=
+        cudaSuccess)
+      return MCE_ENOMEM;
     b->cap_rows = rows;
     b->cap_m = m;
     b->cap_g = G;
@@ -838,6 +883,14 @@ int batch_load(mce_batch *b, const int32_t *row_ptr, const int32_t *col, const i
                            cudaMemcpyHostToDevice, s));
   MCE_CUDA(cudaMemcpyAsync(b->arc_off, ao, sizeof(int64_t) * (size_t)(G + 1),
                            cudaMemcpyHostToDevice, s));
+  // the previous call's copy out of order_h finished before that call returned
+  int32_t *order = b->order_h;
+  for (int32_t i = 0; i < G; ++i) order[i] = i;
+  std::stable_sort(order, order + G, [&](int32_t x, int32_t y) {
+    return ao[x + 1] - ao[x] > ao[y + 1] - ao[y];
+  });
+  MCE_CUDA(cudaMemcpyAsync(b->order, order, sizeof(int32_t) * (size_t)G, cudaMemcpyHostToDevice,
+                           s));
   return batch_rebase_launch(b->rp_local, b->col_local, b->vtx_off, b->arc_off, G, n, m, g->rp,
                              g->col, b->graph_of, g->sms, s, nullptr);
 }
@@ -905,7 +958,7 @@ int mce_batch_count(mce_batch_t b, const mce_opts_t *opts, uint64_t *per_graph_t
     mce_opts_default(&o);
     o.cuda_graph = 1;
   }
-  BatchCtx bc{b->graph_of, b->graph_count, per_graph_total, b->G};
+  BatchCtx bc{b->graph_of, b->graph_count, per_graph_total, b->G, b->vtx_off, b->arc_off, b->order};
   return count_impl(b->g, o, total, hist, stats, &bc);
 }
 

@@ -23,6 +23,10 @@ struct PeelArgs {
 };
 size_t peel_ctl_bytes();
 int peel_launch(const PeelArgs &a, cudaStream_t s, int *launches);
+// Batches: each graph of the disjoint union peeled by one block (order:
+// graph ids, largest first).
+int peel_segments_launch(const PeelArgs &a, const int64_t *vtx_off, const int64_t *arc_off,
+                         const int32_t *order, int32_t G, cudaStream_t s, int *launches);
 int peel_read(const void *ctl_dev, int32_t *degeneracy, uint32_t *err, uint32_t *rounds,
               uint32_t *solo_sections, cudaStream_t s, double *phase_ms = nullptr);
 

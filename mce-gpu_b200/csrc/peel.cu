@@ -20,6 +20,8 @@
 //    same way).
 // Decrements of a vertex that is already removed or queued are skipped;
 // they cannot change any round's membership.
+#include <climits>
+
 #include <cooperative_groups.h>
 
 #include "common.cuh"
@@ -43,6 +45,7 @@ struct PeelCtl {
   int32_t solo_degen;
   uint32_t solo_sections;
   unsigned long long t_scan, t_round, t_wait;  // ns seen by block 0 (diagnostics)
+  uint32_t seg_next;   // batches: next graph to peel
 };
 
 namespace {
@@ -378,6 +381,146 @@ __global__ void __launch_bounds__(PEEL_BLOCK)
 }
 
 }  // namespace
+
+// ---------------------------------------------------------------------------
+// Batches: one block peels one graph of the disjoint union at a time.
+//
+// The graphs of a batch share no edge, so each can be peeled alone; a block
+// runs a graph's synchronous rounds with __syncthreads between them instead
+// of grid barriers, and blocks take graphs largest first.  Rounds are
+// numbered per graph and a graph's final round keeps priority m_g (its own
+// arc count): each graph gets the numbering the reference gives it when it
+// is the whole input.  Orientation only compares vertices of one graph.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int SEG_BLOCK = 256;
+
+struct SegShared {
+  int32_t todo, level, minv, fcnt, ncnt;
+  uint32_t g;
+};
+
+__global__ void __launch_bounds__(SEG_BLOCK)
+    peel_segments_kernel(const int32_t *__restrict__ rp, const int32_t *__restrict__ col,
+                         int32_t *deg, int32_t *core, uint32_t *prio, int32_t *fa, int32_t *fb,
+                         const int64_t *__restrict__ vtx_off, const int64_t *__restrict__ arc_off,
+                         const int32_t *__restrict__ order, int32_t G, PeelCtl *ctl) {
+  __shared__ SegShared sh;
+  const int lane = (int)lane_id(), w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (;;) {
+    if (threadIdx.x == 0) sh.g = atomicAdd(&ctl->seg_next, 1u);  // next graph, largest first
+    __syncthreads();
+    const uint32_t gi = sh.g;
+    if (gi >= (uint32_t)G) break;
+    const int32_t gr = order[gi];
+    const int64_t vb = vtx_off[gr] - gr, n = vtx_off[gr + 1] - vtx_off[gr] - 1;
+    const uint32_t mg = (uint32_t)(arc_off[gr + 1] - arc_off[gr]);
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+      const int64_t v = vb + i;
+      deg[v] = rp[v + 1] - rp[v];
+      core[v] = -1;
+      prio[v] = mg;
+    }
+    if (threadIdx.x == 0) {
+      sh.todo = (int32_t)n;
+      sh.level = 0;
+    }
+    __syncthreads();
+    int32_t *F0 = fa + vb, *G0 = fb + vb;  // this graph's slice of the frontier buffers
+    uint32_t priority = 0;
+    int last_level = -1;
+    while (sh.todo > 0) {
+      const int level = sh.level;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        sh.fcnt = 0;
+        sh.minv = INT_MAX;
+      }
+      __syncthreads();
+      for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const int64_t v = vb + i;
+        if (core[v] == -1) {
+          if (deg[v] <= level) {  // == level: a remaining vertex never has less
+            core[v] = level;
+            F0[atomicAdd(&sh.fcnt, 1)] = (int32_t)v;
+          } else {
+            atomicMin(&sh.minv, deg[v]);
+          }
+        }
+      }
+      __syncthreads();
+      if (sh.fcnt == 0) {  // no vertex at this level: go to the lowest remaining degree
+        __syncthreads();
+        if (threadIdx.x == 0) sh.level = sh.minv;
+        __syncthreads();
+        continue;
+      }
+      int32_t *F = F0, *Gq = G0;
+      for (;;) {
+        const int cnt = sh.fcnt;
+        __syncthreads();
+        if (cnt == 0) break;
+        last_level = level;
+        if (threadIdx.x == 0) {
+          sh.todo -= cnt;
+          sh.ncnt = 0;
+        }
+        __syncthreads();
+        if (sh.todo == 0) break;  // the final round keeps priority m_g
+        for (int i = threadIdx.x; i < cnt; i += blockDim.x) prio[F[i]] = priority;
+        for (int i = w; i < cnt; i += nw) {
+          const int32_t v = F[i];
+          for (int32_t j = rp[v] + lane; j < rp[v + 1]; j += 32) {
+            const int32_t u = col[j];
+            if (*(volatile int32_t *)&core[u] == -1) {
+              const int old = atomicSub(&deg[u], 1);
+              if (old == level + 1) {
+                core[u] = level;
+                Gq[atomicAdd(&sh.ncnt, 1)] = u;
+              }
+            }
+          }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) sh.fcnt = sh.ncnt;
+        int32_t *t = F;
+        F = Gq;
+        Gq = t;
+        ++priority;
+        __syncthreads();
+      }
+      if (threadIdx.x == 0) sh.level = level + 1;
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      atomicMax(&ctl->rounds, priority);
+      atomicMax(&ctl->degeneracy, last_level < 0 ? 0 : last_level);
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace
+
+int peel_segments_launch(const PeelArgs &a, const int64_t *vtx_off, const int64_t *arc_off,
+                         const int32_t *order, int32_t G, cudaStream_t s, int *launches) {
+  int dev = 0, sms = 0, per_sm = 0;
+  MCE_CUDA(cudaGetDevice(&dev));
+  MCE_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  MCE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, peel_segments_kernel, SEG_BLOCK, 0));
+  if (per_sm < 1) return MCE_ECUDA;
+  PeelCtl *ctl = (PeelCtl *)a.ctl;
+  MCE_CUDA(cudaMemsetAsync(ctl, 0, sizeof(PeelCtl), s));
+  int blocks = sms * per_sm;
+  if (blocks > G) blocks = G;
+  if (blocks < 1) return MCE_OK;
+  peel_segments_kernel<<<blocks, SEG_BLOCK, 0, s>>>(a.rp, a.col, a.deg, a.core, a.prio, a.front0,
+                                                    a.front1, vtx_off, arc_off, order, G, ctl);
+  MCE_CUDA(cudaGetLastError());
+  if (launches) *launches += 1;
+  return MCE_OK;
+}
 
 size_t peel_ctl_bytes() { return sizeof(PeelCtl); }
 

@@ -119,6 +119,8 @@ _sigs = {
     "mce_graph_upload": (C.c_int, [_P, _P, C.c_int64, C.c_int64, C.c_int32, _P, _P]),
     "mce_graph_reload": (C.c_int, [_P, _P, _P, C.c_int64, C.c_int64, _P]),
     "mce_graph_free": (C.c_int, [_P]),
+    "mce_bel_load": (C.c_int, [C.c_char_p, C.c_int32, _P, _P]),
+    "mce_graph_size": (C.c_int, [_P, _P, _P]),
     "mce_degeneracy": (C.c_int, [_P, _P, _P, _P]),
     "mce_split_csr": (C.c_int, [_P, _P, _P]),
     "mce_count": (C.c_int, [_P, _P, _P, _P, _P]),
@@ -378,6 +380,18 @@ class Graph:
     @classmethod
     def from_host(cls, g: HostGraph, device: int = 0, stream=None) -> "Graph":
         return cls(g.row_ptr[:g.n + 1], g.col, device, stream)
+
+    @classmethod
+    def load_bel(cls, path: str, device: int = 0, stream=None) -> "Graph":
+        """A .bel file read straight into device memory (mce_bel_load)."""
+        self = cls.__new__(cls)
+        self._h = C.c_void_p()
+        _check(_lib.mce_bel_load(path.encode(), device, stream, C.byref(self._h)), "bel_load")
+        self.row_ptr = self.col = None
+        n, m = C.c_int64(), C.c_int64()
+        _check(_lib.mce_graph_size(self._h, C.byref(n), C.byref(m)), "graph_size")
+        self.n, self.m = n.value, m.value
+        return self
 
     def reload_ptr(self, row_ptr_addr: int, col_addr: int, n: int, m: int, stream=None) -> None:
         """Re-upload from raw host addresses (e.g. pinned buffers), no copy in Python."""
