@@ -92,8 +92,10 @@ typedef struct mce_opts {
                                predicted at least 2^share_log2 nodes share
                                subtrees from their first node on             */
   int32_t warp_log;         /* 1 = record per search warp its SM, tree nodes
-                               and donations (read with mce_warp_log)        */
-  int32_t reserved[1];
+                               and donations; 2 = also its clock cycles per
+                               phase (read both with mce_warp_log)           */
+  int32_t wide_blocks;      /* 0 = default (4): blocks per SM of the wide
+                               engine (d+ > 64); 8 = its 64-register variant */
   void *stream;             /* cudaStream_t to queue work on; NULL = own      */
   void *model;              /* mce_model_t for MCE_SCHED_LEARNED (NULL: the
                                degree heuristic is used instead)              */
@@ -237,16 +239,20 @@ int mce_root_log(mce_graph_t g, uint64_t *nodes_out);
  * opts.log_roots = 1 (n entries, 0 for non-roots).                          */
 int mce_root_counts(mce_graph_t g, uint64_t *count_out);
 
-/* Per-warp load of the last mce_count that ran with opts.warp_log = 1: for
+/* Per-warp load of the last mce_count that ran with opts.warp_log >= 1: for
  * every search warp (all engine classes, widest class first) the SM it ran
  * on, the search-tree nodes it walked (its roots and the subtrees it took)
- * and the subtrees it handed to other warps.  The counterpart of the
- * reference's -m mce-lb-eval / mce-donor-eval per-block lines
- * (mce/mce_kernel_wl_lb.cuh:157, mce/mce_kernel_wl_donor.cuh:157), with a
- * warp as the unit of work.  Arrays (nullable) take up to `cap` entries;
+ * and the subtrees it handed to other warps; with warp_log = 2 also its
+ * clock cycles in the seven phases of the reference's breakdown, in its
+ * order (other, building induced subgraphs, worker list, selecting pivots,
+ * set operations, testing maximality, branching and backtracking; 7 per
+ * warp in cycles_out).  The counterpart of the reference's -m mce-lb-eval /
+ * mce-donor-eval / mce-bd-eval per-block lines (mce/mce_kernel_wl_lb.cuh:157,
+ * mce/mce_kernel_wl_donor.cuh:157, mce/mce_kernel_wl_bd.cuh:270), with a
+ * warp as the unit of work.  Arrays (nullable) take up to `cap` warps;
  * *count_out gets the number of warps.                                      */
 int mce_warp_log(mce_graph_t g, uint32_t *sm_out, uint64_t *nodes_out, uint64_t *donations_out,
-                 int64_t cap, int64_t *count_out);
+                 uint64_t *cycles_out, int64_t cap, int64_t *count_out);
 
 /* ---- batches of graphs ------------------------------------------------------ */
 typedef struct mce_batch *mce_batch_t;
@@ -353,7 +359,8 @@ int mce_count_oriented_noalloc(const int32_t *d_row_ptr, const int32_t *d_split,
 /* ---- autotuner ------------------------------------------------------------ */
 /* Per graph-shape class, the search settings (donation gate and threshold,
  * bitmap word width of narrow roots, single-block peeling of small
- * frontiers) that ran fastest in timed trials, kept in a text table with one
+ * frontiers, blocks per SM of the wide engine) that ran fastest in timed
+ * trials, kept in a text table with one
  * line per class.  A class is floor(log2) of the vertex count, mean degree
  * and degeneracy (and of the graph count for a batch), e.g. "n23-a4-k5" or
  * "b12-n23-a4-k7".  No counterpart in the reference (its per-graph variant

@@ -477,6 +477,7 @@ struct mce_model {
 
 namespace {
 
+constexpr int WLOG_WORDS = 10;  // per-warp log record: SM, nodes, donations, 7 phase cycles
 constexpr int DEFAULT_HEAVY_LOG2 = 12;  // predicted log2(tree nodes) from which a root runs first
 constexpr int DEFAULT_SHARE_LOG2 = 16;  // ... and (learned schedule) shares from its first node
 
@@ -500,6 +501,7 @@ int compute_features(mce_graph *g, cudaStream_t s, int *launches) {
 int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *hist,
                mce_stats_t *stats, const BatchCtx *bc) {
   if (o.bitmap_width != 0 && o.bitmap_width != 32 && o.bitmap_width != 64) return MCE_EINVAL;
+  if (o.wide_blocks != 0 && o.wide_blocks != 4 && o.wide_blocks != 8) return MCE_EINVAL;
   MCE_CUDA(cudaSetDevice(g->device));
   cudaStream_t s = pick_stream(g, o.stream);
   int launches = 0, rc;
@@ -546,11 +548,11 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   for (int c = CLS_R32; c <= CLS_MEM; ++c) {
     if (!sh.cls_cnt[c]) continue;
     int warps = 0;
-    if ((rc = bk_warps_for_class(c, g->sms, &warps, &block[c], &smem[c]))) return rc;
+    if ((rc = bk_warps_for_class(c, g->sms, o.wide_blocks, &warps, &block[c], &smem[c]))) return rc;
     // never more warps than roots (rounded up to whole blocks); with task
     // sharing keep at least a full wave so idle warps can take subtrees
     const int wpb = block[c] / 32;
-    int64_t want = c == CLS_MEM ? (int64_t)sh.cls_cnt[c] : ((int64_t)sh.cls_cnt[c] + 3) / 4;
+    int64_t want = (int64_t)sh.cls_cnt[c];
     if (share) want = want > warps ? want : warps;
     if (want < warps) warps = (int)((want + wpb - 1) / wpb) * wpb;
     grid[c] = warps / wpb;
@@ -569,7 +571,7 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   }
   if (o.warp_log && wlog_total > g->wlog_cap) {
     dfree(g->wlog);
-    if ((rc = dalloc(&g->wlog, 3 * (size_t)wlog_total))) return rc;
+    if ((rc = dalloc(&g->wlog, WLOG_WORDS * (size_t)wlog_total))) return rc;
     g->wlog_cap = wlog_total;
   }
   g->wlog_count = o.warp_log ? wlog_total : 0;
@@ -595,6 +597,7 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   a.donate_after = o.donate_after > 0 ? (uint32_t)o.donate_after : DEFAULT_DONATE_AFTER;
   a.wait_limit_ns = IDLE_LIMIT_NS;
   a.policy = policy;
+  a.wide8 = o.wide_blocks == 8 ? 1 : 0;
   const int wbits = o.bitmap_width == 64 ? 64 : 32;
   QueueView qv[NCLS];
   for (int c = CLS_R32; c <= CLS_MEM; ++c)
@@ -604,7 +607,7 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   // opts.cuda_graph it is captured once and replayed.
   struct SearchKey {
     int grid[NCLS], block[NCLS];
-    int dcap, xcap, wbits, share, dmin, log;
+    int dcap, xcap, wbits, share, dmin, log, wide8;
     uint32_t dafter;
     const void *slab, *graph_count, *graph_of, *root_nodes, *policy, *q[NCLS], *bufs[4], *wlog;
     int64_t n, G;
@@ -622,6 +625,7 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   key.dmin = a.donate_min;
   key.dafter = a.donate_after;
   key.log = o.log_roots != 0;
+  key.wide8 = a.wide8;
   key.slab = g->slab;
   key.graph_count = a.graph_count;
   key.root_nodes = a.root_nodes;
@@ -647,14 +651,16 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
     MCE_CUDA(cudaMemsetAsync(g->hist, 0, sizeof(unsigned long long) * MCE_HIST_MAX, s));
     MCE_CUDA(cudaMemsetAsync(g->nodes, 0, sizeof(unsigned long long) * 4, s));
     if (o.warp_log)
-      MCE_CUDA(cudaMemsetAsync(g->wlog, 0, sizeof(unsigned long long) * 3 * (size_t)wlog_total, s));
+      MCE_CUDA(cudaMemsetAsync(g->wlog, 0, sizeof(unsigned long long) * WLOG_WORDS * (size_t)wlog_total,
+                               s));
     // widest roots first so the long trees start early
     const int order[3] = {CLS_MEM, CLS_R64, CLS_R32};
     for (int c : order) {
       if (!grid[c]) continue;
       a.slab_words = bk_slab_words(c, dcap, xcap);
       a.q = share ? qv[c] : QueueView();
-      a.warp_log = o.warp_log ? g->wlog + 3 * wlog_base[c] : nullptr;
+      a.warp_log = o.warp_log ? g->wlog + WLOG_WORDS * wlog_base[c] : nullptr;
+      a.warp_cycles = o.warp_log == 2 ? 1 : 0;
       if (share && (r2 = queue_launch_init(a.q, s, &launches))) return r2;
       if ((r2 = bk_launch(c, wbits, a, grid[c], block[c], smem[c], s, &launches))) return r2;
     }
@@ -777,19 +783,22 @@ int mce_root_log(mce_graph_t g, uint64_t *nodes_out) {
 }
 
 int mce_warp_log(mce_graph_t g, uint32_t *sm_out, uint64_t *nodes_out, uint64_t *donations_out,
-                 int64_t cap, int64_t *count_out) {
+                 uint64_t *cycles_out, int64_t cap, int64_t *count_out) {
   if (!g || cap < 0) return MCE_EINVAL;
   if (count_out) *count_out = g->wlog_count;
   const int64_t k = cap < g->wlog_count ? cap : g->wlog_count;
   if (k == 0) return MCE_OK;
   MCE_CUDA(cudaSetDevice(g->device));
-  std::vector<unsigned long long> h(3 * (size_t)k);
-  MCE_CUDA(cudaMemcpy(h.data(), g->wlog, sizeof(unsigned long long) * 3 * (size_t)k,
+  std::vector<unsigned long long> h(WLOG_WORDS * (size_t)k);
+  MCE_CUDA(cudaMemcpy(h.data(), g->wlog, sizeof(unsigned long long) * WLOG_WORDS * (size_t)k,
                       cudaMemcpyDeviceToHost));
   for (int64_t i = 0; i < k; ++i) {
-    if (sm_out) sm_out[i] = (uint32_t)h[3 * i];
-    if (nodes_out) nodes_out[i] = h[3 * i + 1];
-    if (donations_out) donations_out[i] = h[3 * i + 2];
+    const unsigned long long *r = &h[WLOG_WORDS * (size_t)i];
+    if (sm_out) sm_out[i] = (uint32_t)r[0];
+    if (nodes_out) nodes_out[i] = r[1];
+    if (donations_out) donations_out[i] = r[2];
+    if (cycles_out)
+      for (int p = 0; p < 7; ++p) cycles_out[7 * i + p] = r[3 + p];
   }
   return MCE_OK;
 }

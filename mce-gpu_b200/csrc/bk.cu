@@ -40,8 +40,14 @@ __global__ void queue_init_kernel(QueueView q) {
 
 namespace {
 
-template <typename Word, int NR, bool Log = false>
-__global__ void __launch_bounds__(REG_BLOCK) bk_reg_kernel(BKArgs a, int cls) {
+// Blocks per SM: the 32-bit engine runs 6 (48 warps: more warps hide the
+// encode's memory latency better than the registers they give up), the
+// 64-bit engine 4.
+// EV (opts.warp_log): 0 none, 1 per-warp load and donations, 2 plus the
+// per-phase cycle breakdown.
+template <typename Word, int NR, int EV = 0>
+__global__ void __launch_bounds__(REG_BLOCK, (NR == 1 && sizeof(Word) == 4) ? 6 : (NR == 2 ? 4 : 1))
+    bk_reg_kernel(BKArgs a, int cls) {
   __shared__ RegSmem<Word, NR> sm_all[REG_BLOCK / 32];
   RegSmem<Word, NR> &sm = sm_all[threadIdx.x >> 5];
   const int lane = (int)lane_id();
@@ -51,6 +57,8 @@ __global__ void __launch_bounds__(REG_BLOCK) bk_reg_kernel(BKArgs a, int cls) {
   const bool share = a.q.hdr != nullptr;
   u64 h0 = 0, h1 = 0, nodes = 0;
   RegRoot<Word> rt;
+  Bd bdv, *bd = &bdv;
+  if constexpr (EV == 2) bdv.start();
   if (share && lane == 0) atomicAdd(&a.q.hdr->work, 1u);
   for (;;) {
     uint32_t i0 = 0;
@@ -61,10 +69,12 @@ __global__ void __launch_bounds__(REG_BLOCK) bk_reg_kernel(BKArgs a, int cls) {
       const uint32_t idx = beg + i0 + k;
       if (idx >= end) break;
       const int32_t r = a.roots[idx];
+      MCE_BD(BD_ENCODE);
       reg_encode<Word, NR>(a, sm, sl, r, rt);
+      MCE_BD(BD_OTHER);
       u64 nd = 0, cnt = 0;
-      reg_tree<Word, NR, false, Log>(a, sm, sl, rt, WOps<Word>::low(rt.d), (Word)0, (Word)0, h0, h1, nd,
-                                      cnt);
+      reg_tree<Word, NR, false, EV>(a, sm, sl, rt, WOps<Word>::low(rt.d), (Word)0, (Word)0, h0, h1,
+                                     nd, cnt, bd);
       nodes += nd;
       root_done(a, r, nd, cnt);
     }
@@ -75,6 +85,7 @@ __global__ void __launch_bounds__(REG_BLOCK) bk_reg_kernel(BKArgs a, int cls) {
       atomicAdd(&a.q.hdr->epoch, 1u);
     }
     u64 t0 = 0, t1 = 0, t2 = 0, t3 = 0;
+    MCE_BD(BD_QUEUE);
     idle_phase(
         a,
         [&](uint32_t k, u64 w) {  // lane k receives word k
@@ -89,25 +100,33 @@ __global__ void __launch_bounds__(REG_BLOCK) bk_reg_kernel(BKArgs a, int cls) {
           const Word P = (Word)__shfl_sync(MCE_FULL, t1, 1);
           const Word X = (Word)__shfl_sync(MCE_FULL, t2, 2);
           const Word S = (Word)__shfl_sync(MCE_FULL, t3, 3);
+          MCE_BD(BD_ENCODE);
           if (r != rt.r) reg_encode<Word, NR>(a, sm, sl, r, rt);
           u64 nd = 0, cnt = 0;
-          reg_tree<Word, NR, false, Log>(a, sm, sl, rt, P, X, S, h0, h1, nd, cnt);
+          reg_tree<Word, NR, false, EV>(a, sm, sl, rt, P, X, S, h0, h1, nd, cnt, bd);
           nodes += nd;
           root_done(a, r, nd, cnt);
+          MCE_BD(BD_QUEUE);
         });
   }
+  MCE_BD(BD_OTHER);
   if (h0) atomicAdd(&a.hist[lane + 2], h0);
   if (h1) atomicAdd(&a.hist[lane + 34], h1);
   if (lane == 0 && nodes) atomicAdd(a.nodes, nodes);  // warp-uniform count
-  if (Log && lane == 0) {  // opts.warp_log
+  if (EV && lane == 0) {  // opts.warp_log
     u64 *w = warp_record(a);
     w[0] = sm_id();
     w[1] = nodes;
+    if constexpr (EV == 2)
+      for (int i = 0; i < 7; ++i) w[3 + i] = bdv.acc[i];
   }
 }
 
-template <bool Log = false>
-__global__ void __launch_bounds__(MEM_BLOCK) bk_mem_kernel(BKArgs a, int cls) {
+// The wide engine at 4 blocks per SM (96 registers) or, with
+// opts.wide_blocks = 8, at 8 (64 registers): more warps pay on graphs whose
+// wide roots have large shared subtrees (R-MAT), fewer on many small ones.
+template <int EV = 0, int MINB = 1>
+__global__ void __launch_bounds__(MEM_BLOCK, MINB) bk_mem_kernel(BKArgs a, int cls) {
   __shared__ MemSmem sm_all[MEM_BLOCK / 32];
   MemSmem &sm = sm_all[threadIdx.x >> 5];
   const int lane = (int)lane_id();
@@ -117,6 +136,8 @@ __global__ void __launch_bounds__(MEM_BLOCK) bk_mem_kernel(BKArgs a, int cls) {
   const bool share = a.q.hdr != nullptr;
   u64 h0 = 0, h1 = 0, nodes = 0;
   MemRoot rt;
+  Bd bdv, *bd = &bdv;
+  if constexpr (EV == 2) bdv.start();
   if (share && lane == 0) atomicAdd(&a.q.hdr->work, 1u);
   for (;;) {
     uint32_t i0 = 0;
@@ -124,7 +145,9 @@ __global__ void __launch_bounds__(MEM_BLOCK) bk_mem_kernel(BKArgs a, int cls) {
     i0 = __shfl_sync(MCE_FULL, i0, 0);
     if (i0 >= end - beg) break;
     const int32_t r = a.roots[beg + i0];
+    MCE_BD(BD_ENCODE);
     mem_encode(a, sm, sl, r, rt);
+    MCE_BD(BD_OTHER);
     if (rt.d == 0) continue;
     const int Wr = rt.Wr;
     if (lane < Wr) {  // root frame: P = all of N+(r), X = 0, S = 0
@@ -135,7 +158,7 @@ __global__ void __launch_bounds__(MEM_BLOCK) bk_mem_kernel(BKArgs a, int cls) {
     }
     __syncwarp();
     u64 nd = 0, cnt = 0;
-    mem_tree<false, Log>(a, sl, rt, h0, h1, nd, cnt);
+    mem_tree<false, EV>(a, sl, rt, h0, h1, nd, cnt, bd);
     nodes += nd;
     root_done(a, r, nd, cnt);
   }
@@ -146,6 +169,7 @@ __global__ void __launch_bounds__(MEM_BLOCK) bk_mem_kernel(BKArgs a, int cls) {
     }
     const int WM = (a.dcap + 63) >> 6;
     int32_t task_root = -1;
+    MCE_BD(BD_QUEUE);
     idle_phase(
         a,
         [&](uint32_t k, u64 w) {
@@ -167,7 +191,9 @@ __global__ void __launch_bounds__(MEM_BLOCK) bk_mem_kernel(BKArgs a, int cls) {
             ts = sl.xs[2 * WM + lane];
           }
           __syncwarp();
+          MCE_BD(BD_ENCODE);
           if (r != rt.r) mem_encode(a, sm, sl, r, rt);
+          MCE_BD(BD_QUEUE);
           if (rt.d == 0) return;
           const int Wr = rt.Wr;
           if (lane < Wr) {
@@ -177,18 +203,22 @@ __global__ void __launch_bounds__(MEM_BLOCK) bk_mem_kernel(BKArgs a, int cls) {
           }
           __syncwarp();
           u64 nd = 0, cnt = 0;
-          mem_tree<false, Log>(a, sl, rt, h0, h1, nd, cnt);
+          mem_tree<false, EV>(a, sl, rt, h0, h1, nd, cnt, bd);
           nodes += nd;
           root_done(a, r, nd, cnt);
+          MCE_BD(BD_QUEUE);
         });
   }
+  MCE_BD(BD_OTHER);
   if (h0) atomicAdd(&a.hist[lane + 2], h0);
   if (h1) atomicAdd(&a.hist[lane + 34], h1);
   if (lane == 0 && nodes) atomicAdd(a.nodes, nodes);  // warp-uniform count
-  if (Log && lane == 0) {  // opts.warp_log
+  if (EV && lane == 0) {  // opts.warp_log
     u64 *w = warp_record(a);
     w[0] = sm_id();
     w[1] = nodes;
+    if constexpr (EV == 2)
+      for (int i = 0; i < 7; ++i) w[3 + i] = bdv.acc[i];
   }
 }
 
@@ -201,6 +231,7 @@ size_t bk_slab_words(int cls, int dcap, int xcap) {
   size_t w = (size_t)dcap * WM + (size_t)(dcap + 1) * 4 * WM + 32 * WM + (size_t)xcap * WM;
   w += (size_t)hash_cap(xcap);                      // hash set (one-word rows)
   w += ((size_t)dcap + (size_t)xcap + 1) / 2 + 1;  // pl and xl (int32)
+  w += (size_t)p_cap(dcap);                         // hash of P: keys and indices (int32)
   w = w > 3 * WM + 1 ? w : 3 * WM + 1;
   return (w + 31) & ~(size_t)31;                    // 256-byte aligned slabs
 }
@@ -210,7 +241,7 @@ uint32_t bk_task_words(int cls, int dcap) {
   return 1 + 3 * (uint32_t)((dcap + 63) / 64);
 }
 
-int bk_warps_for_class(int cls, int sms, int *warps, int *block, int *smem) {
+int bk_warps_for_class(int cls, int sms, int wide_blocks, int *warps, int *block, int *smem) {
   int per_sm = 0;
   if (cls == CLS_R32 || cls == CLS_R64) {
     *block = REG_BLOCK;
@@ -224,7 +255,7 @@ int bk_warps_for_class(int cls, int sms, int *warps, int *block, int *smem) {
   } else {
     *block = MEM_BLOCK;
     *smem = 0;
-    per_sm = 4;
+    per_sm = wide_blocks == 8 ? 8 : 4;
     *warps = sms * per_sm * (MEM_BLOCK / 32);
   }
   return MCE_OK;
@@ -233,30 +264,41 @@ int bk_warps_for_class(int cls, int sms, int *warps, int *block, int *smem) {
 int bk_launch(int cls, int word_bits, const BKArgs &a, int grid, int block, int smem,
               cudaStream_t s, int *launches) {
   if (grid <= 0) return MCE_OK;
-  const bool log = a.warp_log != nullptr;  // the evaluation variants record per-warp load
+  // the evaluation variants record per-warp load (1) and cycles (2)
+  const int ev = a.warp_log == nullptr ? 0 : (a.warp_cycles ? 2 : 1);
   switch (cls) {
     case CLS_R32:
       if (word_bits == 64) {
-        if (log)
-          bk_reg_kernel<u64, 1, true><<<grid, block, smem, s>>>(a, cls);
+        if (ev == 2)
+          bk_reg_kernel<u64, 1, 2><<<grid, block, smem, s>>>(a, cls);
+        else if (ev == 1)
+          bk_reg_kernel<u64, 1, 1><<<grid, block, smem, s>>>(a, cls);
         else
           bk_reg_kernel<u64, 1><<<grid, block, smem, s>>>(a, cls);
       } else {
-        if (log)
-          bk_reg_kernel<uint32_t, 1, true><<<grid, block, smem, s>>>(a, cls);
+        if (ev == 2)
+          bk_reg_kernel<uint32_t, 1, 2><<<grid, block, smem, s>>>(a, cls);
+        else if (ev == 1)
+          bk_reg_kernel<uint32_t, 1, 1><<<grid, block, smem, s>>>(a, cls);
         else
           bk_reg_kernel<uint32_t, 1><<<grid, block, smem, s>>>(a, cls);
       }
       break;
     case CLS_R64:
-      if (log)
-        bk_reg_kernel<u64, 2, true><<<grid, block, smem, s>>>(a, cls);
+      if (ev == 2)
+        bk_reg_kernel<u64, 2, 2><<<grid, block, smem, s>>>(a, cls);
+      else if (ev == 1)
+        bk_reg_kernel<u64, 2, 1><<<grid, block, smem, s>>>(a, cls);
       else
         bk_reg_kernel<u64, 2><<<grid, block, smem, s>>>(a, cls);
       break;
     case CLS_MEM:
-      if (log)
-        bk_mem_kernel<true><<<grid, block, smem, s>>>(a, cls);
+      if (ev == 2)
+        bk_mem_kernel<2><<<grid, block, smem, s>>>(a, cls);
+      else if (ev == 1)
+        bk_mem_kernel<1><<<grid, block, smem, s>>>(a, cls);
+      else if (a.wide8)
+        bk_mem_kernel<0, 8><<<grid, block, smem, s>>>(a, cls);
       else
         bk_mem_kernel<><<<grid, block, smem, s>>>(a, cls);
       break;

@@ -35,7 +35,7 @@ struct WOps<u64> {
 
 constexpr int REG_BLOCK = 256;  // 8 warps
 constexpr int MEM_BLOCK = 128;  // 4 warps
-constexpr int REG_CHUNK = 4;    // roots fetched per atomic by the register engine
+constexpr int REG_CHUNK = 1;    // roots fetched per atomic by the register engine
 
 __device__ __forceinline__ int warp_incl_scan(int x) {
   const int lane = (int)lane_id();
@@ -45,31 +45,6 @@ __device__ __forceinline__ int warp_incl_scan(int x) {
     if (lane >= o) x += y;
   }
   return x;
-}
-
-// index t of the chunk item owning flattened element e: the last t with
-// off[t] <= e (off is the exclusive prefix of the items' list lengths).
-__device__ __forceinline__ int chunk_owner(const int32_t *off, int e) {
-  int lo = 0, hi = 32;
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if (off[mid] <= e)
-      lo = mid + 1;
-    else
-      hi = mid;
-  }
-  return lo - 1;
-}
-
-__device__ __forceinline__ int lower_bound_g(const int32_t *a, int n, int32_t key) {
-  int lo = 0, len = n;
-  while (len > 0) {
-    const int half = len >> 1;
-    const bool right = a[lo + half] < key;
-    lo = right ? lo + half + 1 : lo;
-    len = right ? len - half - 1 : half;
-  }
-  return lo;
 }
 
 __device__ __forceinline__ uint32_t hash_word(u64 x) {
@@ -83,10 +58,37 @@ __device__ __forceinline__ bool wants_task(const QueueView &q) {
   return __shfl_sync(MCE_FULL, w, 0) != 0;
 }
 
-// Per-warp evaluation log (opts.warp_log): this warp's record in the launch.
+// Per-warp evaluation log (opts.warp_log): this warp's record in the launch:
+// {SM, tree nodes, donations, cycles per phase[7]}.
+constexpr int WLOG_WORDS = 10;
 __device__ __forceinline__ u64 *warp_record(const BKArgs &a) {
-  return a.warp_log + 3 * (((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  return a.warp_log + WLOG_WORDS * (((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
 }
+
+// Cycle breakdown of a warp (opts.warp_log = 2) in the categories of the
+// reference's -m mce-bd-eval (mce/mce.cuh:385-390): time is charged to the
+// current phase whenever the warp switches to another one.
+enum BdPhase { BD_OTHER, BD_ENCODE, BD_QUEUE, BD_PIVOT, BD_SETS, BD_MAXIMAL, BD_BRANCH };
+struct Bd {
+  u64 acc[7];
+  u64 last;
+  int cur;
+  __device__ void start() {
+    for (int i = 0; i < 7; ++i) acc[i] = 0;
+    last = clock64();
+    cur = BD_OTHER;
+  }
+  __device__ void to(int k) {
+    const u64 t = clock64();
+    acc[cur] += t - last;
+    last = t;
+    cur = k;
+  }
+};
+#define MCE_BD(k)                    \
+  do {                               \
+    if constexpr (EV == 2) bd->to(k); \
+  } while (0)
 
 __device__ __forceinline__ uint32_t sm_id() {
   uint32_t id;
@@ -161,9 +163,79 @@ struct RegSmem {
   Word xs[32];              // earlier-neighbour rows while they are built
   Word stk[32 * NR + 1][4]; // DFS frames: P, X, branch set, chosen set
   int32_t pl[32 * NR];      // the root's later neighbours (sorted ids), padded
-  int32_t off[32];          // chunk prefix offsets
-  int32_t beg[32];          // chunk list starts
+  int32_t off[32];          // flattened-walk prefix offsets of the items' lists
+  int32_t beg[32];          // ... and the lists' starts
+  int32_t own[32];          // ... and the item whose list starts at a window position
+  int32_t hkey[64 * NR];    // hash of P: vertex id (-1: empty) ...
+  uint8_t hidx[64 * NR];    // ... and its index in P
+  Word xl0[32];             // the first 32 leaf-filter rows (the rest: slab xl)
 };
+
+// Flattened walk over the concatenated lists of up to 32 items (lane t
+// holds item t's list start b and length len; the lists live in cs): calls
+// f(t, element) for every element, 32 at a time.  The owner of a position
+// is the last item whose list starts at or before it, read from a bitmask
+// of the list starts inside the current window.
+template <typename F>
+__device__ __forceinline__ void flat_walk(const int32_t *__restrict__ cs, int32_t b, int len,
+                                          int32_t *off_sm, int32_t *beg_sm, int32_t *own_sm,
+                                          F f) {
+  const int lane = (int)lane_id();
+  const int incl = warp_incl_scan(len);
+  const int T = __shfl_sync(MCE_FULL, incl, 31);
+  const int off = incl - len;
+  off_sm[lane] = off;
+  beg_sm[lane] = b;
+  int carry = 0;
+  for (int e0 = 0; e0 < T; e0 += 32) {
+    const bool st = len > 0 && off >= e0 && off < e0 + 32;
+    if (st) own_sm[off - e0] = lane;
+    const uint32_t mask = __reduce_or_sync(MCE_FULL, st ? 1u << (off - e0) : 0u);
+    __syncwarp();
+    const uint32_t below = mask & (0xFFFFFFFFu >> (31 - lane));
+    const int t = below ? own_sm[31 - __clz(below)] : carry;
+    carry = __shfl_sync(MCE_FULL, t, 31);
+    const int e = e0 + lane;
+    if (e < T) f(t, cs[beg_sm[t] + (e - off_sm[t])]);
+    __syncwarp();
+  }
+}
+
+// Hash of the root's later neighbours (ids are distinct): 2x slots.
+template <typename Word, int NR>
+__device__ __forceinline__ uint32_t p_slot(int32_t w) {
+  return ((uint32_t)w * 0x9E3779B1u) >> (NR == 2 ? 25 : 26);
+}
+
+template <typename Word, int NR>
+__device__ __forceinline__ void p_hash_build(RegSmem<Word, NR> &sm, int d) {
+  const int lane = (int)lane_id();
+  for (int i = lane; i < 64 * NR; i += 32) sm.hkey[i] = -1;
+  __syncwarp();
+#pragma unroll
+  for (int k = 0; k < NR; ++k) {
+    const int i = lane + 32 * k;
+    if (i < d) {
+      const int32_t w = sm.pl[i];
+      uint32_t h = p_slot<Word, NR>(w);
+      while (atomicCAS(&sm.hkey[h], -1, w) != -1) h = (h + 1) & (64 * NR - 1);
+      sm.hidx[h] = (uint8_t)i;
+    }
+  }
+  __syncwarp();
+}
+
+// index of w in P, or -1
+template <typename Word, int NR>
+__device__ __forceinline__ int p_find(const RegSmem<Word, NR> &sm, int32_t w) {
+  uint32_t h = p_slot<Word, NR>(w);
+  for (;;) {
+    const int32_t k = sm.hkey[h];
+    if (k == w) return sm.hidx[h];
+    if (k == -1) return -1;
+    h = (h + 1) & (64 * NR - 1);
+  }
+}
 
 // Per-warp slab of the register engine, in Words: a hash set used while the
 // earlier-neighbour rows are built (2 * REG_XCAP), the distinct rows
@@ -214,6 +286,8 @@ __device__ void reg_encode(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab
   }
   __syncwarp();
 
+  p_hash_build(sm, d);
+
   // warp_sorted_count_and_encode_full (mce/mce_utils.cuh:90-117): bit (j, i)
   // and (i, j) for every later neighbour w = P[i] of v = P[j].  The later
   // lists of 32 P vertices are flattened over the lanes.
@@ -225,21 +299,14 @@ __device__ void reg_encode(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab
       vb = a.split[v];
       vlen = a.rp[v + 1] - vb;
     }
-    const int incl = warp_incl_scan(vlen);
-    const int T = __shfl_sync(MCE_FULL, incl, 31);
-    sm.off[lane] = incl - vlen;
-    sm.beg[lane] = vb;
-    __syncwarp();
-    for (int e = lane; e < T; e += 32) {
-      const int t = chunk_owner(sm.off, e);
-      const int32_t w = a.cs[sm.beg[t] + (e - sm.off[t])];
-      const int i = lower_bound_g(sm.pl, 32 * NR, w);
-      if (i < d && sm.pl[i] == w) {
+    flat_walk(a.cs, vb, vlen, sm.off, sm.beg, sm.own, [&](int t, int32_t w) {
+      const int i = p_find(sm, w);
+      if (i >= 0) {
         const int j = c * 32 + t;
         atomicOr(&sm.rows[j], O::bit(i));
         atomicOr(&sm.rows[i], O::bit(j));
       }
-    }
+    });
     __syncwarp();
   }
   rt.r0 = sm.rows[lane];
@@ -248,13 +315,16 @@ __device__ void reg_encode(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab
 
   // Earlier neighbours x of r: row(x) = N(x) & P, kept once per distinct
   // non-empty value; x is earlier than every vertex of P, so N(x) & P lies
-  // in N+(x).
+  // in N+(x).  Up to 32 of them are deduplicated with one match over the
+  // warp; more go through a hash set in the slab.
   int nX = 0;
   if (u > 0) {
+    const bool hashed = u > 32;
     int hc = 32;
-    while (hc < 2 * u && hc < 2 * REG_XCAP) hc <<= 1;
-    for (int i = lane; i < hc; i += 32) sl.hash[i] = 0;
-    __syncwarp();
+    if (hashed) {
+      while (hc < 2 * u && hc < 2 * REG_XCAP) hc <<= 1;
+      for (int i = lane; i < hc; i += 32) sl.hash[i] = 0;
+    }
     for (int c = 0; c * 32 < u; ++c) {
       const int items = min(32, u - c * 32);
       int xb = 0, xlen = 0;
@@ -264,21 +334,18 @@ __device__ void reg_encode(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab
         xlen = a.rp[x + 1] - xb;
       }
       sm.xs[lane] = 0;
-      const int incl = warp_incl_scan(xlen);
-      const int T = __shfl_sync(MCE_FULL, incl, 31);
-      sm.off[lane] = incl - xlen;
-      sm.beg[lane] = xb;
       __syncwarp();
-      for (int e = lane; e < T; e += 32) {
-        const int t = chunk_owner(sm.off, e);
-        const int32_t w = a.cs[sm.beg[t] + (e - sm.off[t])];
-        const int i = lower_bound_g(sm.pl, 32 * NR, w);
-        if (i < d && sm.pl[i] == w) atomicOr(&sm.xs[t], O::bit(i));
-      }
+      flat_walk(a.cs, xb, xlen, sm.off, sm.beg, sm.own, [&](int t, int32_t w) {
+        const int i = p_find(sm, w);
+        if (i >= 0) atomicOr(&sm.xs[t], O::bit(i));
+      });
       __syncwarp();
       const Word row = sm.xs[lane];
       bool fresh = false;
-      if (lane < items && row != 0) {
+      if (!hashed) {
+        const uint32_t same = __match_any_sync(MCE_FULL, row);
+        fresh = lane < items && row != 0 && (same & lt) == 0;  // first lane of its value
+      } else if (lane < items && row != 0) {
         uint32_t h = hash_word((u64)row) & (uint32_t)(hc - 1);
         for (int probe = 0; probe < hc; ++probe) {
           const Word old = atomicCAS(&sl.hash[h], (Word)0, row);
@@ -303,13 +370,15 @@ __device__ void reg_encode(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab
 
 // Walk the subtree under node (P, X, S) of root rt.r.  For the root itself
 // S = 0; for a task S holds the vertices chosen above the node.  With
-// Budget, the walk stops once it has visited a.node_budget nodes; with Log,
-// the warp's donations are counted in its a.warp_log record.
-template <typename Word, int NR, bool Budget = false, bool Log = false>
+// Budget, the walk stops once it has visited a.node_budget nodes; with EV
+// (opts.warp_log) >= 1 the warp's donations are counted in its a.warp_log
+// record, with EV == 2 its cycles are charged to *bd by phase.
+template <typename Word, int NR, bool Budget = false, int EV = 0>
 __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<Word> &sl,
                          const RegRoot<Word> &rt, Word P, Word X, Word S, u64 &h0, u64 &h1,
-                         u64 &nodes, u64 &cnt) {
+                         u64 &nodes, u64 &cnt, Bd *bd = nullptr) {
   using O = WOps<Word>;
+  MCE_BD(BD_PIVOT);
   const int lane = (int)lane_id();
   const uint32_t lt = (1u << lane) - 1u;
   const Word r0 = rt.r0, r1 = rt.r1;
@@ -334,10 +403,14 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
         el = el || (((X >> (lane + 32)) & 1) && s == pc);
       }
     }
-    if (__any_sync(MCE_FULL, el) || P == 0) return;
+    if (__any_sync(MCE_FULL, el) || P == 0) {
+      MCE_BD(BD_OTHER);
+      return;
+    }
     k = (int)__reduce_max_sync(MCE_FULL, (unsigned)k);
     start_k = k;
   }
+  MCE_BD(BD_SETS);
   // apply_pivot_to_first_level (:204-216) / apply_pivot_to_next_level (:218-239)
   Word B = P & ~row_of<Word, NR>(r0, r1, 127 - (start_k & 127));
   // Leaf filter: for the root it is rebuilt at every depth-0 branch (rows
@@ -351,7 +424,10 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
       const Word row = i < nX ? sl.xr[i] : (Word)0;
       const bool has = i < nX && (row & S) == S;
       const uint32_t mk = __ballot_sync(MCE_FULL, has);
-      if (has) sl.xl[nL + __popc(mk & lt)] = row;
+      if (has) {
+        const int at = nL + __popc(mk & lt);
+        (at < 32 ? sm.xl0 : sl.xl)[at] = row;
+      }
       nL += __popc(mk);
     }
     __syncwarp();
@@ -359,6 +435,7 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
   int depth = 0, recheck = 0;
   bool want = false;
   for (;;) {
+    MCE_BD(BD_BRANCH);
     if (B == 0) {  // get_next_candidate found nothing: backtrack (:526-563)
       if (depth == 0) break;
       --depth;
@@ -372,6 +449,7 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
     B &= B - 1;
     const Word vb = O::bit(v);
     const Word rv = row_of<Word, NR>(r0, r1, v);
+    MCE_BD(BD_SETS);
     // populate_xl_and_cl (:321-336): child P' = P & N(v), X' = X & N(v);
     // v leaves P for X in this frame.
     const Word Pc = P & rv, Xc = X & rv, Sc = S | vb;
@@ -389,23 +467,23 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
         const Word row = i < nX ? sl.xr[i] : (Word)0;
         const bool has = (row & vb) != 0;
         const uint32_t mk = __ballot_sync(MCE_FULL, has);
-        if (has) sl.xl[nL + __popc(mk & lt)] = row;
+        if (has) {
+          const int at = nL + __popc(mk & lt);
+          (at < 32 ? sm.xl0 : sl.xl)[at] = row;
+        }
         nL += __popc(mk);
       }
       __syncwarp();
     }
     if (Pc == 0) {
+      MCE_BD(BD_MAXIMAL);
       // test_maximality (:507-524): P' and X' empty and no earlier
       // neighbour of the root adjacent to the whole clique.
       if (Xc == 0) {
-        bool covered = false;
-        for (int i0 = 0; i0 < nL; i0 += 32) {
+        bool covered = __any_sync(MCE_FULL, lane < nL && (sm.xl0[lane] & Sc) == Sc);
+        for (int i0 = 32; !covered && i0 < nL; i0 += 32) {
           const int i = i0 + lane;
-          const bool hit = i < nL && (sl.xl[i] & Sc) == Sc;
-          if (__any_sync(MCE_FULL, hit)) {
-            covered = true;
-            break;
-          }
+          covered = __any_sync(MCE_FULL, i < nL && (sl.xl[i] & Sc) == Sc);
         }
         if (!covered) {
           ++cnt;
@@ -420,6 +498,7 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
       }
       continue;
     }
+    MCE_BD(BD_PIVOT);
     // select_pivot_from_P_and_Xp (:366-402): pivot over P' | X'; an X'
     // vertex adjacent to all of P' ends the path.
     const Word cand = Pc | Xc;
@@ -443,6 +522,7 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
     // mce/mce_utils.cuh:872-880,1063-1113)
     if (share && pc >= a.donate_min &&
         (nodes >= a.donate_after || (a.policy && a.policy[rt.r]))) {
+      MCE_BD(BD_QUEUE);
       if (--recheck <= 0) {  // the queue state is read every 32 candidate nodes
         want = wants_task(a.q);
         recheck = 32;
@@ -450,13 +530,15 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
       if (want) {
         const u64 w0 = (u64)(uint32_t)rt.r, w1 = (u64)Pc, w2 = (u64)Xc, w3 = (u64)Sc;
         if (q_push(a.q, [&](uint32_t k2) { return k2 == 0 ? w0 : k2 == 1 ? w1 : k2 == 2 ? w2 : w3; })) {
-          if (Log && lane == 0) warp_record(a)[2] += 1;  // opts.warp_log
+          if (EV && lane == 0) warp_record(a)[2] += 1;  // opts.warp_log
           continue;
         }
         want = false;
       }
     }
+    MCE_BD(BD_PIVOT);
     k = (int)__reduce_max_sync(MCE_FULL, (unsigned)k);
+    MCE_BD(BD_BRANCH);
     if (lane == 0) {
       sm.stk[depth][0] = P;
       sm.stk[depth][1] = X;
@@ -471,6 +553,7 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
     // apply_pivot_to_next_level (:218-239)
     B = Pc & ~row_of<Word, NR>(r0, r1, 127 - (k & 127));
   }
+  MCE_BD(BD_OTHER);
 }
 
 // ---------------------------------------------------------------------------
@@ -479,18 +562,27 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
 struct MemSmem {
   int32_t off[32];
   int32_t beg[32];
+  int32_t own[32];
 };
 
 struct Slab {
   int32_t *pl;
   u64 *rows, *stk, *xs, *xr, *hash;
   int32_t *xl;
+  int32_t *pkey, *pidx;  // hash of P: vertex id (-1: empty) and its index in P
   int hcap;  // hash set entries: a power of two >= 2 * xcap
 };
 
 __host__ __device__ __forceinline__ int hash_cap(int xcap) {
   int h = 32;
   while (h < 2 * xcap) h <<= 1;
+  return h;
+}
+
+// slots of the hash of P for d later neighbours: a power of two >= 2 d
+__host__ __device__ __forceinline__ int p_cap(int d) {
+  int h = 64;
+  while (h < 2 * d) h <<= 1;
   return h;
 }
 
@@ -506,7 +598,24 @@ __device__ __forceinline__ Slab slab_of(const BKArgs &a, int64_t gw) {
   s.hcap = hash_cap(XC);
   s.pl = (int32_t *)(s.hash + (size_t)s.hcap);
   s.xl = s.pl + D;
+  s.pkey = s.xl + XC;
+  s.pidx = s.pkey + p_cap(D);
   return s;
+}
+
+__device__ __forceinline__ uint32_t wide_slot(int32_t w, int pc) {
+  return (((uint32_t)w * 0x9E3779B1u) >> 12) & (uint32_t)(pc - 1);
+}
+
+// index of w in P (hash of pc slots), or -1
+__device__ __forceinline__ int wide_find(const Slab &sl, int pc, int32_t w) {
+  uint32_t h = wide_slot(w, pc);
+  for (;;) {
+    const int32_t k = sl.pkey[h];
+    if (k == w) return sl.pidx[h];
+    if (k == -1) return -1;
+    h = (h + 1) & (uint32_t)(pc - 1);
+  }
 }
 
 struct MemRoot {
@@ -530,8 +639,17 @@ __device__ void mem_encode(const BKArgs &a, MemSmem &sm, const Slab &sl, int32_t
   rt.Wr = Wr;
   int32_t *pl = sl.pl;
   u64 *rows = sl.rows;
+  const int pc = p_cap(d);
   for (int i = lane; i < d; i += 32) pl[i] = a.cs[sb + i];
   for (int i = lane; i < d * Wr; i += 32) rows[i] = 0;
+  for (int i = lane; i < pc; i += 32) sl.pkey[i] = -1;
+  __syncwarp();
+  for (int i = lane; i < d; i += 32) {  // P's ids are distinct
+    const int32_t w = pl[i];
+    uint32_t h = wide_slot(w, pc);
+    while (atomicCAS(&sl.pkey[h], -1, w) != -1) h = (h + 1) & (uint32_t)(pc - 1);
+    sl.pidx[h] = i;
+  }
   __syncwarp();
   for (int c = 0; c * 32 < d; ++c) {
     const int items = min(32, d - c * 32);
@@ -541,21 +659,14 @@ __device__ void mem_encode(const BKArgs &a, MemSmem &sm, const Slab &sl, int32_t
       vb = a.split[v];
       vlen = a.rp[v + 1] - vb;
     }
-    const int incl = warp_incl_scan(vlen);
-    const int T = __shfl_sync(MCE_FULL, incl, 31);
-    sm.off[lane] = incl - vlen;
-    sm.beg[lane] = vb;
-    __syncwarp();
-    for (int e = lane; e < T; e += 32) {
-      const int t = chunk_owner(sm.off, e);
-      const int32_t w = a.cs[sm.beg[t] + (e - sm.off[t])];
-      const int i = lower_bound_g(pl, d, w);
-      if (i < d && pl[i] == w) {
+    flat_walk(a.cs, vb, vlen, sm.off, sm.beg, sm.own, [&](int t, int32_t w) {
+      const int i = wide_find(sl, pc, w);
+      if (i >= 0) {
         const int j = c * 32 + t;
         atomicOr(&rows[(size_t)j * Wr + (i >> 6)], 1ull << (i & 63));
         atomicOr(&rows[(size_t)i * Wr + (j >> 6)], 1ull << (j & 63));
       }
-    }
+    });
     __syncwarp();
   }
   // earlier-neighbour rows: non-empty ones, distinct when one word wide
@@ -574,17 +685,11 @@ __device__ void mem_encode(const BKArgs &a, MemSmem &sm, const Slab &sl, int32_t
       xlen = a.rp[x + 1] - xb;
     }
     for (int i = lane; i < 32 * Wr; i += 32) sl.xs[i] = 0;
-    const int incl = warp_incl_scan(xlen);
-    const int T = __shfl_sync(MCE_FULL, incl, 31);
-    sm.off[lane] = incl - xlen;
-    sm.beg[lane] = xb;
     __syncwarp();
-    for (int e = lane; e < T; e += 32) {
-      const int t = chunk_owner(sm.off, e);
-      const int32_t w = a.cs[sm.beg[t] + (e - sm.off[t])];
-      const int i = lower_bound_g(pl, d, w);
-      if (i < d && pl[i] == w) atomicOr(&sl.xs[(size_t)t * Wr + (i >> 6)], 1ull << (i & 63));
-    }
+    flat_walk(a.cs, xb, xlen, sm.off, sm.beg, sm.own, [&](int t, int32_t w) {
+      const int i = wide_find(sl, pc, w);
+      if (i >= 0) atomicOr(&sl.xs[(size_t)t * Wr + (i >> 6)], 1ull << (i & 63));
+    });
     __syncwarp();
     bool keep = false;
     if (lane < items) {
@@ -616,9 +721,10 @@ __device__ void mem_encode(const BKArgs &a, MemSmem &sm, const Slab &sl, int32_t
 }
 
 // Walk the subtree under frame 0 of the slab stack (P, X, S already there).
-template <bool Budget = false, bool Log = false>
+template <bool Budget = false, int EV = 0>
 __device__ void mem_tree(const BKArgs &a, const Slab &sl, const MemRoot &rt, u64 &h0, u64 &h1,
-                         u64 &nodes, u64 &cnt) {
+                         u64 &nodes, u64 &cnt, Bd *bd = nullptr) {
+  MCE_BD(BD_PIVOT);
   const int lane = (int)lane_id();
   const uint32_t lt = (1u << lane) - 1u;
   const int d = rt.d, Wr = rt.Wr, nX = rt.nX;
@@ -648,7 +754,10 @@ __device__ void mem_tree(const BKArgs &a, const Slab &sl, const MemRoot &rt, u64
       k = max(k, ((s + 1) << 11) | (2047 - uu));
       el = el || (inX && s == pc);
     }
-    if (__any_sync(MCE_FULL, el) || pc == 0) return;
+    if (__any_sync(MCE_FULL, el) || pc == 0) {
+      MCE_BD(BD_OTHER);
+      return;
+    }
     k = (int)__reduce_max_sync(MCE_FULL, (unsigned)k);
     const int piv = 2047 - (k & 2047);
     if (lane < Wr) F0[2 * Wr + lane] = F0[lane] & ~rows[(size_t)piv * Wr + lane];
@@ -674,6 +783,7 @@ __device__ void mem_tree(const BKArgs &a, const Slab &sl, const MemRoot &rt, u64
   int depth = 0, recheck = 0;
   bool want = false;
   for (;;) {
+    MCE_BD(BD_BRANCH);
     u64 *F = sl.stk + (size_t)depth * 4 * Wr;
     u64 *Fp = F, *Fx = F + Wr, *Fb = F + 2 * Wr, *Fs = F + 3 * Wr;
     // lowest set bit of the branch set
@@ -689,6 +799,7 @@ __device__ void mem_tree(const BKArgs &a, const Slab &sl, const MemRoot &rt, u64
     const int v = wl * 64 + __ffsll((long long)word) - 1;
     const int vw = v >> 6;
     const u64 vbit = 1ull << (v & 63);
+    MCE_BD(BD_SETS);
     if (lane == 0) {
       Fb[vw] &= ~vbit;
       Fp[vw] &= ~vbit;
@@ -726,6 +837,7 @@ __device__ void mem_tree(const BKArgs &a, const Slab &sl, const MemRoot &rt, u64
     }
     __syncwarp();
     if (pc == 0) {
+      MCE_BD(BD_MAXIMAL);
       if (!xnz) {
         const u64 *Cs = C + 3 * Wr;
         bool covered = false;
@@ -759,6 +871,7 @@ __device__ void mem_tree(const BKArgs &a, const Slab &sl, const MemRoot &rt, u64
       }
       continue;
     }
+    MCE_BD(BD_PIVOT);
     int k = 0;
     bool el = false;
     for (int uu = lane; uu < d; uu += 32) {
@@ -776,6 +889,7 @@ __device__ void mem_tree(const BKArgs &a, const Slab &sl, const MemRoot &rt, u64
     if (share && pc >= a.donate_min &&
         (nodes >= a.donate_after || (a.policy && a.policy[rt.r])) &&
         (--recheck <= 0 ? (recheck = 32, want = wants_task(a.q)) : want)) {
+      MCE_BD(BD_QUEUE);
       const int WM = (a.dcap + 63) >> 6;
       const u64 *Cp = C, *Cx = C + Wr, *Cs = C + 3 * Wr;
       if (q_push(a.q, [&](uint32_t k2) -> u64 {
@@ -784,17 +898,20 @@ __device__ void mem_tree(const BKArgs &a, const Slab &sl, const MemRoot &rt, u64
             if ((int)w >= Wr) return 0ull;
             return part == 0 ? Cp[w] : part == 1 ? Cx[w] : Cs[w];
           })) {
-        if (Log && lane == 0) warp_record(a)[2] += 1;  // opts.warp_log
+        if (EV && lane == 0) warp_record(a)[2] += 1;  // opts.warp_log
         continue;
       }
       want = false;
     }
+    MCE_BD(BD_PIVOT);
     k = (int)__reduce_max_sync(MCE_FULL, (unsigned)k);
     const int up = 2047 - (k & 2047);
+    MCE_BD(BD_BRANCH);
     if (lane < Wr) C[2 * Wr + lane] = C[lane] & ~rows[(size_t)up * Wr + lane];
     __syncwarp();
     ++depth;
   }
+  MCE_BD(BD_OTHER);
 }
 
 }  // namespace

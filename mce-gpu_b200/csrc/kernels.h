@@ -92,11 +92,14 @@ struct BKArgs {
   uint64_t wait_limit_ns;        // an idle warp gives up after this long without progress
   const uint8_t *policy;         // nullable [n]: 1 = root may share subtrees at once
   unsigned long long node_budget;  // 0: none; else a tree stops past this many nodes
-  unsigned long long *warp_log;  // nullable: per warp of the launch {SM id, tree nodes, donations}
+  unsigned long long *warp_log;  // nullable: per warp of the launch {SM id, tree nodes, donations,
+                                 // cycles per phase[7]}
+  int32_t warp_cycles;           // 1: also the per-phase cycle breakdown
+  int32_t wide8;                 // 1: the wide engine's 8-blocks-per-SM variant
 };
 
 // Launch the engine of one class.  warps_out: number of warps launched (slab sizing).
-int bk_warps_for_class(int cls, int sms, int *warps, int *block, int *smem);
+int bk_warps_for_class(int cls, int sms, int wide_blocks, int *warps, int *block, int *smem);
 size_t bk_slab_words(int cls, int dcap, int xcap);
 uint32_t bk_task_words(int cls, int dcap);
 int queue_launch_init(const QueueView &q, cudaStream_t s, int *launches);

@@ -246,7 +246,7 @@ int main(int argc, char **argv) {
   o.worker_list = c.wl;
   o.bitmap_width = c.bitmap_width;
   o.sched = c.sched;
-  o.warp_log = (c.task == TASK_LB || c.task == TASK_DONOR) ? 1 : 0;
+  o.warp_log = (c.task == TASK_LB || c.task == TASK_DONOR) ? 1 : c.task == TASK_BD ? 2 : 0;
   uint64_t total = 0;
   std::vector<uint64_t> hist(MCE_HIST_MAX, 0);
   mce_stats_t st;
@@ -260,16 +260,27 @@ int main(int argc, char **argv) {
     // per-unit load lines as the reference's evaluation kernels print them
     // (mce/mce.cuh:385-390); the unit here is a search warp
     int64_t k = 0;
-    rc = mce_warp_log(g, nullptr, nullptr, nullptr, 0, &k);
+    rc = mce_warp_log(g, nullptr, nullptr, nullptr, nullptr, 0, &k);
     std::vector<uint32_t> sm((size_t)k);
-    std::vector<uint64_t> nodes((size_t)k), don((size_t)k);
-    if (!rc) rc = mce_warp_log(g, sm.data(), nodes.data(), don.data(), k, &k);
+    std::vector<uint64_t> nodes((size_t)k), don((size_t)k), cyc(7 * (size_t)k);
+    if (!rc) rc = mce_warp_log(g, sm.data(), nodes.data(), don.data(), cyc.data(), k, &k);
     if (rc) fail("warp_log", rc);
-    std::printf(c.task == TASK_LB ? "BLOCK ID, SM ID, Number of traversed nodes\n"
-                                  : "BLOCK ID, SM ID, Number of donations\n");
-    for (int64_t i = 0; i < k; ++i)
-      std::printf("%lld, %u, %llu\n", (long long)i, sm[(size_t)i],
-                  (unsigned long long)(c.task == TASK_LB ? nodes[(size_t)i] : don[(size_t)i]));
+    if (c.task == TASK_BD) {
+      std::printf("OTHER, BUILDING INDUCED SUBGRAPHS, WORKER LIST, SELECTING PIVOTS, SET "
+                  "OPERATIONS, TESTING MAXIMALITY, BRANCHING AND BACKTRACKING\n");
+      for (int64_t i = 0; i < k; ++i) {
+        const uint64_t *r = &cyc[7 * (size_t)i];
+        std::printf("%llu, %llu, %llu, %llu, %llu, %llu, %llu\n", (unsigned long long)r[0],
+                    (unsigned long long)r[1], (unsigned long long)r[2], (unsigned long long)r[3],
+                    (unsigned long long)r[4], (unsigned long long)r[5], (unsigned long long)r[6]);
+      }
+    } else {
+      std::printf(c.task == TASK_LB ? "BLOCK ID, SM ID, Number of traversed nodes\n"
+                                    : "BLOCK ID, SM ID, Number of donations\n");
+      for (int64_t i = 0; i < k; ++i)
+        std::printf("%lld, %u, %llu\n", (long long)i, sm[(size_t)i],
+                    (unsigned long long)(c.task == TASK_LB ? nodes[(size_t)i] : don[(size_t)i]));
+    }
   }
   std::printf("Finished Launching Instance 0.\n");
   log_info("count time %f s", st.count_ms / 1e3);

@@ -6,7 +6,8 @@
 // floor(log2) of its vertex count, mean degree and degeneracy, plus the
 // batch size for batches.  Tuning walks the knobs one at a time (donation
 // gate, donation threshold, bitmap word width of narrow roots, single-block
-// peeling of small frontiers; subtree sharing itself stays as given, since
+// peeling of small frontiers, blocks per SM of the wide engine; subtree
+// sharing itself stays as given, since
 // without it one heavy root can run for minutes), times each value with
 // the device timers of mce_count / mce_batch_count, keeps a value only when
 // it is at least 2% faster, and checks that every trial returns the same
@@ -32,7 +33,7 @@ struct ::mce_graph *batch_union(struct ::mce_batch *b, int32_t *num_graphs);
 namespace {
 
 struct Knobs {
-  int32_t worker_list, donate_after, donate_threshold, bitmap_width, peel_solo_max;
+  int32_t worker_list, donate_after, donate_threshold, bitmap_width, peel_solo_max, wide_blocks;
 };
 
 // the library's defaults, written out so that a table entry is explicit
@@ -43,6 +44,7 @@ Knobs resolved(const mce_opts_t &o) {
   k.donate_threshold = o.donate_threshold > 0 ? o.donate_threshold : 10;
   k.bitmap_width = o.bitmap_width ? o.bitmap_width : 32;
   k.peel_solo_max = o.peel_solo_max > 0 ? o.peel_solo_max : -1;
+  k.wide_blocks = o.wide_blocks ? o.wide_blocks : 4;
   return k;
 }
 
@@ -52,6 +54,7 @@ void apply(const Knobs &k, mce_opts_t *o) {
   o->donate_threshold = k.donate_threshold;
   o->bitmap_width = k.bitmap_width;
   o->peel_solo_max = k.peel_solo_max;
+  o->wide_blocks = k.wide_blocks;
 }
 
 int ilog2(double x) { return x < 1.0 ? 0 : (int)std::floor(std::log2(x)); }
@@ -62,9 +65,10 @@ struct Entry {
 };
 
 const char *kHeader =
-    "# mce autotune table v1: class worker_list donate_after donate_threshold bitmap_width "
-    "peel_solo_max best_ms default_ms";
+    "# mce autotune table v2: class worker_list donate_after donate_threshold bitmap_width "
+    "peel_solo_max wide_blocks best_ms default_ms";
 
+// v2 lines have 9 fields; v1 lines (8, no wide_blocks) read as wide_blocks 4
 bool read_table(const char *path, std::map<std::string, Entry> *t) {
   std::ifstream f(path);
   if (!f) return false;
@@ -73,10 +77,22 @@ bool read_table(const char *path, std::map<std::string, Entry> *t) {
     if (line.empty() || line[0] == '#') continue;
     std::istringstream ss(line);
     std::string key;
+    std::vector<double> v;
+    double x;
+    ss >> key;
+    while (ss >> x) v.push_back(x);
+    if (v.size() != 7 && v.size() != 8) continue;
+    const bool v2 = v.size() == 8;
     Entry e;
-    if (ss >> key >> e.k.worker_list >> e.k.donate_after >> e.k.donate_threshold >>
-        e.k.bitmap_width >> e.k.peel_solo_max >> e.best_ms >> e.default_ms)
-      (*t)[key] = e;
+    e.k.worker_list = (int32_t)v[0];
+    e.k.donate_after = (int32_t)v[1];
+    e.k.donate_threshold = (int32_t)v[2];
+    e.k.bitmap_width = (int32_t)v[3];
+    e.k.peel_solo_max = (int32_t)v[4];
+    e.k.wide_blocks = v2 ? (int32_t)v[5] : 4;
+    e.best_ms = v[v2 ? 6 : 5];
+    e.default_ms = v[v2 ? 7 : 6];
+    (*t)[key] = e;
   }
   return true;
 }
@@ -88,9 +104,9 @@ int write_table(const char *path, const std::map<std::string, Entry> &t) {
   std::fprintf(f, "%s\n", kHeader);
   for (const auto &kv : t) {
     const Entry &e = kv.second;
-    std::fprintf(f, "%s %d %d %d %d %d %.4f %.4f\n", kv.first.c_str(), e.k.worker_list,
+    std::fprintf(f, "%s %d %d %d %d %d %d %.4f %.4f\n", kv.first.c_str(), e.k.worker_list,
                  e.k.donate_after, e.k.donate_threshold, e.k.bitmap_width, e.k.peel_solo_max,
-                 e.best_ms, e.default_ms);
+                 e.k.wide_blocks, e.best_ms, e.default_ms);
   }
   if (std::fclose(f) != 0 || std::rename(tmp.c_str(), path) != 0) return MCE_EIO;
   return MCE_OK;
@@ -166,6 +182,7 @@ int tune(const char *key, const mce_opts_t &base, const char *table_path, int32_
       {&Knobs::donate_threshold, {6, 10, 16}},
       {&Knobs::bitmap_width, {32, 64}},
       {&Knobs::peel_solo_max, {-1, 64}},
+      {&Knobs::wide_blocks, {4, 8}},
   };
   for (const Axis &ax : axes) {
     if (cur.worker_list == MCE_WL_OFF &&

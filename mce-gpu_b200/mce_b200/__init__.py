@@ -46,7 +46,7 @@ class _Opts(C.Structure):
                 ("log_roots", C.c_int32), ("x_pivot", C.c_int32),
                 ("peel_solo_max", C.c_int32), ("donate_after", C.c_int32),
                 ("cuda_graph", C.c_int32), ("heavy_log2", C.c_int32),
-                ("share_log2", C.c_int32), ("warp_log", C.c_int32), ("reserved", C.c_int32 * 1),
+                ("share_log2", C.c_int32), ("warp_log", C.c_int32), ("wide_blocks", C.c_int32),
                 ("stream", C.c_void_p), ("model", C.c_void_p)]
 
 
@@ -72,7 +72,8 @@ class _TuneResult(C.Structure):
                 ("default_ms", C.c_double), ("trials_run", C.c_int32), ("from_table", C.c_int32)]
 
 
-TUNED_FIELDS = ("worker_list", "donate_after", "donate_threshold", "bitmap_width", "peel_solo_max")
+TUNED_FIELDS = ("worker_list", "donate_after", "donate_threshold", "bitmap_width", "peel_solo_max",
+                "wide_blocks")
 
 
 def _tune_dict(r: _TuneResult) -> dict:
@@ -126,7 +127,7 @@ _sigs = {
     "mce_count": (C.c_int, [_P, _P, _P, _P, _P]),
     "mce_root_log": (C.c_int, [_P, _P]),
     "mce_root_counts": (C.c_int, [_P, _P]),
-    "mce_warp_log": (C.c_int, [_P, _P, _P, _P, C.c_int64, _P]),
+    "mce_warp_log": (C.c_int, [_P, _P, _P, _P, _P, C.c_int64, _P]),
     "mce_count_oriented_noalloc": (C.c_int, [_P, _P, _P, _P, C.c_int64, _P, _P]),
     "mce_batch_upload": (C.c_int, [_P, _P, _P, _P, C.c_int32, C.c_int32, _P, _P]),
     "mce_batch_reload": (C.c_int, [_P, _P, _P, _P, _P, C.c_int32, _P]),
@@ -352,14 +353,15 @@ def _stats_dict(st: _Stats) -> dict:
 def make_opts(*, sched=SCHED_PLAIN, bitmap_width=0, log_roots=False, level=LEVEL_L1,
               induced=INDUCED_P, worker_list=WL_ON, donate_threshold=0, x_pivot=0,
               peel_solo_max=0, donate_after=0, cuda_graph=0, heavy_log2=0, share_log2=0,
-              warp_log=False, model=None, stream=None) -> _Opts:
+              warp_log=False, wide_blocks=0, model=None, stream=None) -> _Opts:
     o = _Opts()
     _lib.mce_opts_default(C.byref(o))
     o.sched, o.bitmap_width, o.log_roots = sched, bitmap_width, int(bool(log_roots))
     o.level, o.induced, o.worker_list = level, induced, worker_list
     o.donate_threshold, o.x_pivot = donate_threshold, x_pivot
     o.peel_solo_max, o.donate_after, o.cuda_graph = peel_solo_max, donate_after, cuda_graph
-    o.heavy_log2, o.share_log2, o.warp_log = heavy_log2, share_log2, int(bool(warp_log))
+    o.heavy_log2, o.share_log2, o.warp_log = heavy_log2, share_log2, int(warp_log)
+    o.wide_blocks = wide_blocks
     o.stream = stream
     o.model = model._h if model is not None else None
     return o
@@ -459,15 +461,19 @@ class Graph:
         return out[:self.n]
 
     def warp_log(self) -> dict:
-        """Per search warp of the last count(warp_log=True): SM id, tree nodes, donations."""
+        """Per search warp of the last count(warp_log=1 or 2): SM id, tree nodes,
+        donations and (warp_log=2) clock cycles per phase (warps x 7)."""
         k = C.c_int64()
-        _check(_lib.mce_warp_log(self._h, None, None, None, 0, C.byref(k)), "warp_log")
-        sm = np.zeros(max(k.value, 1), np.uint32)
-        nodes = np.zeros(max(k.value, 1), np.uint64)
-        don = np.zeros(max(k.value, 1), np.uint64)
-        _check(_lib.mce_warp_log(self._h, _ptr(sm), _ptr(nodes), _ptr(don), k.value, C.byref(k)),
-               "warp_log")
-        return {"sm": sm[:k.value], "nodes": nodes[:k.value], "donations": don[:k.value]}
+        _check(_lib.mce_warp_log(self._h, None, None, None, None, 0, C.byref(k)), "warp_log")
+        n = max(k.value, 1)
+        sm = np.zeros(n, np.uint32)
+        nodes = np.zeros(n, np.uint64)
+        don = np.zeros(n, np.uint64)
+        cyc = np.zeros((n, 7), np.uint64)
+        _check(_lib.mce_warp_log(self._h, _ptr(sm), _ptr(nodes), _ptr(don), _ptr(cyc), k.value,
+                                 C.byref(k)), "warp_log")
+        return {"sm": sm[:k.value], "nodes": nodes[:k.value], "donations": don[:k.value],
+                "cycles": cyc[:k.value]}
 
     def root_counts(self) -> np.ndarray:
         out = np.zeros(max(self.n, 1), np.uint64)

@@ -214,9 +214,24 @@ def test_warp_log_accounts_for_every_node_and_donation():
     assert int(log["donations"].sum()) == r.stats["donations"] and r.stats["donations"] > 0
 
 
+def test_warp_cycle_breakdown():
+    hg = mce.gen_rmat(12, 16, 0.57, 0.19, 0.19, 7)
+    with mce.Graph.from_host(hg) as g:
+        r = g.count(warp_log=2)
+        log = g.warp_log()
+    assert r.total == oracle.count(hg)[0]
+    cyc = log["cycles"].astype(np.float64)
+    assert cyc.shape == (len(log["sm"]), 7)
+    busy = cyc.sum(axis=0)
+    # every warp encodes, pivots, branches and tests leaves
+    assert busy[1] > 0 and busy[3] > 0 and busy[5] > 0 and busy[6] > 0
+    assert int(log["nodes"].sum()) == r.stats["tree_nodes"]
+
+
 @pytest.mark.skipif(not os.path.exists(CLI), reason="CLI not built")
 @pytest.mark.parametrize("task,header", [("mce-lb-eval", "Number of traversed nodes"),
-                                         ("mce-donor-eval", "Number of donations")])
+                                         ("mce-donor-eval", "Number of donations"),
+                                         ("mce-bd-eval", "TESTING MAXIMALITY")])
 def test_cli_eval_lines(tmp_path, task, header):
     import re
     import subprocess
@@ -228,5 +243,21 @@ def test_cli_eval_lines(tmp_path, task, header):
     assert header in out
     found = int(re.findall(r"Found (.*) maximal cliques in total", out)[0].replace(",", ""))
     assert found == oracle.count(hg)[0]
-    rows = re.findall(r"([0-9]+), ([0-9]+), ([0-9]+)", out)  # the reference's plot.py pattern
-    assert len(rows) > 0 and all(int(sm) < 1024 for _, sm, _ in rows)
+    if task == "mce-bd-eval":  # plot.py's parse_mce_bd pattern: seven columns
+        rows = re.findall(r"([0-9]+)" + r", ([0-9]+)" * 6, out)
+        assert len(rows) > 0 and sum(int(x) for row in rows for x in row) > 0
+    else:  # plot.py's parse_mce_lb pattern
+        rows = re.findall(r"([0-9]+), ([0-9]+), ([0-9]+)", out)
+        assert len(rows) > 0 and all(int(sm) < 1024 for _, sm, _ in rows)
+
+
+@pytest.mark.parametrize("wide_blocks", [4, 8])
+def test_wide_engine_occupancy_variants(wide_blocks):
+    g = mce.gen_er(2000, 0.005, 21, planted=6, cmin=70, cmax=300)  # roots in the wide engine
+    t, h, _ = oracle.count(g)
+    with mce.Graph.from_host(g) as dg:
+        r = dg.count(wide_blocks=wide_blocks, log_roots=True)
+        nodes = dg.root_log()
+    assert r.stats["class_roots"][2] > 0
+    assert r.total == t and np.array_equal(r.hist, h)
+    assert np.array_equal(nodes, oracle.roots(g)[3])
