@@ -231,6 +231,17 @@ int mce_split_csr(mce_graph_t g, int32_t *split_out, int32_t *col_out);
 int mce_count(mce_graph_t g, const mce_opts_t *opts, uint64_t *total, uint64_t *hist,
               mce_stats_t *stats);
 
+/* List the maximal cliques (size >= 2): clique k is
+ * ids_out[offsets_out[k] .. offsets_out[k+1]), the root first, k <
+ * *count_out, in no particular order (the search's leaves are reached in
+ * parallel).  offsets_out holds cliques_cap + 1 entries.  If the listing
+ * does not fit (more than ids_cap ids or cliques_cap cliques), nothing is
+ * written, *count_out and *ids_needed (nullable) get the sizes it needs and
+ * MCE_ELIMIT is returned.  No counterpart in the reference, which only
+ * counts (mce/mce_utils.cuh:522-523).                                      */
+int mce_list(mce_graph_t g, const mce_opts_t *opts, int32_t *ids_out, int64_t ids_cap,
+             int64_t *offsets_out, int64_t cliques_cap, uint64_t *count_out, int64_t *ids_needed);
+
 /* Per-root search-tree node counts of the last mce_count that ran with
  * opts.log_roots = 1 (n entries, 0 for non-roots).                          */
 int mce_root_log(mce_graph_t g, uint64_t *nodes_out);
@@ -398,6 +409,9 @@ int mce_batch_autotune(mce_batch_t b, const mce_opts_t *base, const char *table_
  * block (a slot) takes one request at a time; requests are admitted as
  * slots free up, so a request never waits for a batch to fill.  The graph
  * handle must outlive the session and must not be reloaded meanwhile.
+ * A request whose ego graph has at least 1,024 vertices opens its root
+ * search to slots that have nothing to do, so a large request does not
+ * run on one block alone while the GPU idles.
  * While requests keep coming the kernel stays resident on every SM; a
  * cudaDeviceSynchronize by the caller returns only after the slots have
  * been idle for idle_ms (or after mce_serve_close).                       */
@@ -442,6 +456,7 @@ typedef struct mce_serve_stats {
   uint64_t submitted, served, tree_nodes;
   int64_t kernel_launches;
   uint64_t arena_bytes, slab_bytes;
+  uint64_t helps;     /* times an idle slot joined another slot's search    */
 } mce_serve_stats_t;
 
 void mce_serve_opts_default(mce_serve_opts_t *o);

@@ -498,8 +498,15 @@ int compute_features(mce_graph *g, cudaStream_t s, int *launches) {
 
 // The counting pipeline shared by mce_count and mce_batch_count.  With a
 // batch context, each root's count also goes to its graph's counter.
+// Clique listing: device buffer for the {size, root, members...} records.
+struct ListCtx {
+  int32_t *buf;
+  unsigned long long *words;
+  unsigned long long cap;
+};
+
 int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *hist,
-               mce_stats_t *stats, const BatchCtx *bc) {
+               mce_stats_t *stats, const BatchCtx *bc, const ListCtx *lc = nullptr) {
   if (o.bitmap_width != 0 && o.bitmap_width != 32 && o.bitmap_width != 64) return MCE_EINVAL;
   if (o.wide_blocks != 0 && o.wide_blocks != 4 && o.wide_blocks != 8) return MCE_EINVAL;
   MCE_CUDA(cudaSetDevice(g->device));
@@ -598,6 +605,11 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   a.wait_limit_ns = IDLE_LIMIT_NS;
   a.policy = policy;
   a.wide8 = o.wide_blocks == 8 ? 1 : 0;
+  if (lc) {
+    a.list_buf = lc->buf;
+    a.list_words = lc->words;
+    a.list_cap = lc->cap;
+  }
   const int wbits = o.bitmap_width == 64 ? 64 : 32;
   QueueView qv[NCLS];
   for (int c = CLS_R32; c <= CLS_MEM; ++c)
@@ -653,6 +665,7 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
     if (o.warp_log)
       MCE_CUDA(cudaMemsetAsync(g->wlog, 0, sizeof(unsigned long long) * WLOG_WORDS * (size_t)wlog_total,
                                s));
+    if (lc) MCE_CUDA(cudaMemsetAsync(lc->words, 0, sizeof(unsigned long long), s));
     // widest roots first so the long trees start early
     const int order[3] = {CLS_MEM, CLS_R64, CLS_R32};
     for (int c : order) {
@@ -666,7 +679,7 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
     }
     return MCE_OK;
   };
-  if (o.cuda_graph) {
+  if (o.cuda_graph && !lc) {
     if (!g->search_exec || std::memcmp(g->search_key, &key, sizeof(key)) != 0) {
       if (g->search_exec) {
         cudaGraphExecDestroy(g->search_exec);
@@ -771,6 +784,50 @@ int mce_count(mce_graph_t g, const mce_opts_t *opts, uint64_t *total, uint64_t *
   else
     mce_opts_default(&o);
   return count_impl(g, o, total, hist, stats, nullptr);
+}
+
+int mce_list(mce_graph_t g, const mce_opts_t *opts, int32_t *ids_out, int64_t ids_cap,
+             int64_t *offsets_out, int64_t cliques_cap, uint64_t *count_out, int64_t *ids_needed) {
+  if (!g || !count_out || ids_cap < 0 || cliques_cap < 0 || (ids_cap > 0 && !ids_out) ||
+      !offsets_out)
+    return MCE_EINVAL;
+  mce_opts_t o;
+  if (opts)
+    o = *opts;
+  else
+    mce_opts_default(&o);
+  MCE_CUDA(cudaSetDevice(g->device));
+  // the records hold a size word per clique beside the ids
+  const unsigned long long cap = (unsigned long long)ids_cap + (unsigned long long)cliques_cap;
+  ListCtx lc{nullptr, nullptr, cap};
+  int rc = dalloc(&lc.buf, (size_t)(cap > 0 ? cap : 1));
+  if (!rc) rc = dalloc(&lc.words, 1);
+  uint64_t total = 0;
+  if (!rc) rc = count_impl(g, o, &total, nullptr, nullptr, nullptr, &lc);
+  unsigned long long words = 0;
+  if (!rc && cudaMemcpy(&words, lc.words, sizeof(words), cudaMemcpyDeviceToHost) != cudaSuccess)
+    rc = MCE_ECUDA;
+  *count_out = total;
+  if (ids_needed) *ids_needed = (int64_t)(words - total);
+  if (!rc && (words > cap || total > (uint64_t)cliques_cap)) rc = MCE_ELIMIT;
+  if (!rc) {
+    std::vector<int32_t> h((size_t)words);
+    if (words && cudaMemcpy(h.data(), lc.buf, sizeof(int32_t) * (size_t)words,
+                            cudaMemcpyDeviceToHost) != cudaSuccess)
+      rc = MCE_ECUDA;
+    int64_t pos = 0, k = 0;
+    for (size_t w = 0; !rc && w < (size_t)words; ++k) {
+      const int32_t sz = h[w];
+      offsets_out[k] = pos;
+      std::memcpy(ids_out + pos, &h[w + 1], sizeof(int32_t) * (size_t)sz);
+      pos += sz;
+      w += (size_t)sz + 1;
+    }
+    if (!rc) offsets_out[k] = pos;
+  }
+  dfree(lc.buf);
+  dfree(lc.words);
+  return rc;
 }
 
 int mce_root_log(mce_graph_t g, uint64_t *nodes_out) {

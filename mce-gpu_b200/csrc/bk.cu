@@ -45,7 +45,7 @@ namespace {
 // 64-bit engine 4.
 // EV (opts.warp_log): 0 none, 1 per-warp load and donations, 2 plus the
 // per-phase cycle breakdown.
-template <typename Word, int NR, int EV = 0>
+template <typename Word, int NR, int EV = 0, bool LIST = false>
 __global__ void __launch_bounds__(REG_BLOCK, (NR == 1 && sizeof(Word) == 4) ? 6 : (NR == 2 ? 4 : 1))
     bk_reg_kernel(BKArgs a, int cls) {
   __shared__ RegSmem<Word, NR> sm_all[REG_BLOCK / 32];
@@ -73,8 +73,8 @@ __global__ void __launch_bounds__(REG_BLOCK, (NR == 1 && sizeof(Word) == 4) ? 6 
       reg_encode<Word, NR>(a, sm, sl, r, rt);
       MCE_BD(BD_OTHER);
       u64 nd = 0, cnt = 0;
-      reg_tree<Word, NR, false, EV>(a, sm, sl, rt, WOps<Word>::low(rt.d), (Word)0, (Word)0, h0, h1,
-                                     nd, cnt, bd);
+      reg_tree<Word, NR, false, EV, LIST>(a, sm, sl, rt, WOps<Word>::low(rt.d), (Word)0, (Word)0,
+                                           h0, h1, nd, cnt, bd);
       nodes += nd;
       root_done(a, r, nd, cnt);
     }
@@ -103,7 +103,7 @@ __global__ void __launch_bounds__(REG_BLOCK, (NR == 1 && sizeof(Word) == 4) ? 6 
           MCE_BD(BD_ENCODE);
           if (r != rt.r) reg_encode<Word, NR>(a, sm, sl, r, rt);
           u64 nd = 0, cnt = 0;
-          reg_tree<Word, NR, false, EV>(a, sm, sl, rt, P, X, S, h0, h1, nd, cnt, bd);
+          reg_tree<Word, NR, false, EV, LIST>(a, sm, sl, rt, P, X, S, h0, h1, nd, cnt, bd);
           nodes += nd;
           root_done(a, r, nd, cnt);
           MCE_BD(BD_QUEUE);
@@ -125,7 +125,7 @@ __global__ void __launch_bounds__(REG_BLOCK, (NR == 1 && sizeof(Word) == 4) ? 6 
 // The wide engine at 4 blocks per SM (96 registers) or, with
 // opts.wide_blocks = 8, at 8 (64 registers): more warps pay on graphs whose
 // wide roots have large shared subtrees (R-MAT), fewer on many small ones.
-template <int EV = 0, int MINB = 1>
+template <int EV = 0, int MINB = 1, bool LIST = false>
 __global__ void __launch_bounds__(MEM_BLOCK, MINB) bk_mem_kernel(BKArgs a, int cls) {
   __shared__ MemSmem sm_all[MEM_BLOCK / 32];
   MemSmem &sm = sm_all[threadIdx.x >> 5];
@@ -158,7 +158,7 @@ __global__ void __launch_bounds__(MEM_BLOCK, MINB) bk_mem_kernel(BKArgs a, int c
     }
     __syncwarp();
     u64 nd = 0, cnt = 0;
-    mem_tree<false, EV>(a, sl, rt, h0, h1, nd, cnt, bd);
+    mem_tree<false, EV, LIST>(a, sl, rt, h0, h1, nd, cnt, bd);
     nodes += nd;
     root_done(a, r, nd, cnt);
   }
@@ -203,7 +203,7 @@ __global__ void __launch_bounds__(MEM_BLOCK, MINB) bk_mem_kernel(BKArgs a, int c
           }
           __syncwarp();
           u64 nd = 0, cnt = 0;
-          mem_tree<false, EV>(a, sl, rt, h0, h1, nd, cnt, bd);
+          mem_tree<false, EV, LIST>(a, sl, rt, h0, h1, nd, cnt, bd);
           nodes += nd;
           root_done(a, r, nd, cnt);
           MCE_BD(BD_QUEUE);
@@ -264,8 +264,26 @@ int bk_warps_for_class(int cls, int sms, int wide_blocks, int *warps, int *block
 int bk_launch(int cls, int word_bits, const BKArgs &a, int grid, int block, int smem,
               cudaStream_t s, int *launches) {
   if (grid <= 0) return MCE_OK;
-  // the evaluation variants record per-warp load (1) and cycles (2)
+  // the evaluation variants record per-warp load (1) and cycles (2); the
+  // listing variants write every clique
   const int ev = a.warp_log == nullptr ? 0 : (a.warp_cycles ? 2 : 1);
+  if (a.list_buf) {
+    if (cls == CLS_R32 && word_bits == 64)
+      bk_reg_kernel<u64, 1, 0, true><<<grid, block, smem, s>>>(a, cls);
+    else if (cls == CLS_R32)
+      bk_reg_kernel<uint32_t, 1, 0, true><<<grid, block, smem, s>>>(a, cls);
+    else if (cls == CLS_R64)
+      bk_reg_kernel<u64, 2, 0, true><<<grid, block, smem, s>>>(a, cls);
+    else if (cls == CLS_MEM && a.wide8)
+      bk_mem_kernel<0, 8, true><<<grid, block, smem, s>>>(a, cls);
+    else if (cls == CLS_MEM)
+      bk_mem_kernel<0, 1, true><<<grid, block, smem, s>>>(a, cls);
+    else
+      return MCE_EINVAL;
+    MCE_CUDA(cudaGetLastError());
+    if (launches) *launches += 1;
+    return MCE_OK;
+  }
   switch (cls) {
     case CLS_R32:
       if (word_bits == 64) {

@@ -368,12 +368,36 @@ __device__ void reg_encode(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab
   rt.nX = nX;
 }
 
+// Clique listing (mce_list): each maximal clique becomes the record
+// {size, root, members...} at a position of a.list_buf taken with one
+// atomicAdd; a record past a.list_cap is counted but not written.
+template <typename Word, int NR>
+__device__ __forceinline__ void reg_emit(const BKArgs &a, const RegSmem<Word, NR> &sm, int32_t r,
+                                         Word Sc) {
+  const int lane = (int)lane_id();
+  const int sz = WOps<Word>::popc(Sc) + 1;
+  unsigned long long base = 0;
+  if (lane == 0) base = atomicAdd(a.list_words, (unsigned long long)(sz + 1));
+  base = __shfl_sync(MCE_FULL, base, 0);
+  if (base + (unsigned long long)sz + 1 > a.list_cap) return;
+  if (lane == 0) {
+    a.list_buf[base] = sz;
+    a.list_buf[base + 1] = r;
+  }
+#pragma unroll
+  for (int k = 0; k < NR; ++k) {
+    const int i = lane + 32 * k;
+    if ((Sc >> i) & 1)
+      a.list_buf[base + 2 + WOps<Word>::popc(Sc & WOps<Word>::low(i))] = sm.pl[i];
+  }
+}
+
 // Walk the subtree under node (P, X, S) of root rt.r.  For the root itself
 // S = 0; for a task S holds the vertices chosen above the node.  With
 // Budget, the walk stops once it has visited a.node_budget nodes; with EV
 // (opts.warp_log) >= 1 the warp's donations are counted in its a.warp_log
 // record, with EV == 2 its cycles are charged to *bd by phase.
-template <typename Word, int NR, bool Budget = false, int EV = 0>
+template <typename Word, int NR, bool Budget = false, int EV = 0, bool LIST = false>
 __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<Word> &sl,
                          const RegRoot<Word> &rt, Word P, Word X, Word S, u64 &h0, u64 &h1,
                          u64 &nodes, u64 &cnt, Bd *bd = nullptr) {
@@ -487,6 +511,7 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
         }
         if (!covered) {
           ++cnt;
+          if constexpr (LIST) reg_emit<Word, NR>(a, sm, rt.r, Sc);
           const int bin = O::popc(Sc) - 1;  // clique size - 2
           if (lane == (bin & 31)) {
             if (bin < 32)
@@ -721,7 +746,7 @@ __device__ void mem_encode(const BKArgs &a, MemSmem &sm, const Slab &sl, int32_t
 }
 
 // Walk the subtree under frame 0 of the slab stack (P, X, S already there).
-template <bool Budget = false, int EV = 0>
+template <bool Budget = false, int EV = 0, bool LIST = false>
 __device__ void mem_tree(const BKArgs &a, const Slab &sl, const MemRoot &rt, u64 &h0, u64 &h1,
                          u64 &nodes, u64 &cnt, Bd *bd = nullptr) {
   MCE_BD(BD_PIVOT);
@@ -857,6 +882,26 @@ __device__ void mem_tree(const BKArgs &a, const Slab &sl, const MemRoot &rt, u64
         if (!covered) {
           ++cnt;
           const int bin = s_base + depth;  // clique size - 2
+          if constexpr (LIST) {  // record {size, root, members...}, as reg_emit
+            const int sz = bin + 2;
+            unsigned long long base = 0;
+            if (lane == 0) base = atomicAdd(a.list_words, (unsigned long long)(sz + 1));
+            base = __shfl_sync(MCE_FULL, base, 0);
+            if (base + (unsigned long long)sz + 1 <= a.list_cap) {
+              if (lane == 0) {
+                a.list_buf[base] = sz;
+                a.list_buf[base + 1] = rt.r;
+              }
+              u64 word = lane < Wr ? Cs[lane] : 0ull;  // Wr <= 32 words
+              const int c = __popcll(word);
+              unsigned long long pos = base + 2 + (warp_incl_scan(c) - c);
+              while (word) {
+                const int b = __ffsll((long long)word) - 1;
+                word &= word - 1;
+                a.list_buf[pos++] = sl.pl[lane * 64 + b];
+              }
+            }
+          }
           if (bin < 64) {
             if (lane == (bin & 31)) {
               if (bin < 32)

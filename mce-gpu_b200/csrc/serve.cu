@@ -64,8 +64,22 @@ struct SvHostHdr {           // mapped host memory, host-written
 
 struct SvCtl {               // device memory
   uint32_t next, dtail, dstop, pad;
-  unsigned long long poll_ns, served, nodes;
+  unsigned long long poll_ns, served, nodes, helped;
 };
+
+// The root work of a slot's current request, shared with helping slots.
+struct SvHelp {
+  uint32_t state;            // SV_OPEN | number of helping slots inside
+  uint32_t rootnext;         // next root (ego vertex) to search
+  int32_t n;                 // roots
+  uint32_t pad;
+  unsigned long long total, nodes;
+};
+constexpr uint32_t SV_OPEN = 0x80000000u;
+constexpr int SV_BOARD = 64;                  // requests open for help at a time
+constexpr int SV_HELP_MIN = 1024;             // roots from which a request takes helpers
+constexpr uint32_t SV_HELP = 0x40000000u;     // claim(): help slot (value & 0xFFFFFF)
+constexpr uint64_t SV_HELP_WAIT_NS = 60ull * 1000 * 1000 * 1000;
 
 struct ServeArgs {
   const int32_t *grp, *gcol;  // resident graph
@@ -81,6 +95,8 @@ struct ServeArgs {
   size_t slab_words, reg_words;
   uint64_t idle_ns;
   unsigned long long node_budget;  // per request; 0: none
+  SvHelp *help;                    // per slot
+  uint32_t *board;                 // slot + 1 of requests open for help (0: empty)
 };
 
 struct Arena {
@@ -192,8 +208,8 @@ __device__ void block_sort(int32_t *buf, int n_pow2) {
 
 struct SvShared {
   uint32_t req;
+  int32_t posted, broken;
   int32_t k, fcnt, ncnt, todo, level, minv, acnt;
-  uint32_t rootnext;
   unsigned long long total, nodes;
   int ws[SV_WARPS];
 };
@@ -460,9 +476,76 @@ __device__ uint32_t claim(const ServeArgs &S) {
     }
     if (stop) return SV_EXIT;
     if (now - t_idle > S.idle_ns) return SV_EXIT;
+    // no new request: join the search of a large one another slot runs
+    for (int e = 0; e < SV_BOARD; ++e) {
+      const uint32_t j1 = ld_volatile(&S.board[e]);
+      if (j1 == 0) continue;
+      SvHelp *h = &S.help[j1 - 1];
+      uint32_t st = ld_volatile(&h->state);
+      while ((st & SV_OPEN) && ld_volatile(&h->rootnext) < (uint32_t)ld_volatile((uint32_t *)&h->n)) {
+        const uint32_t prev = atomicCAS(&h->state, st, st + 1);
+        if (prev == st) {
+          __threadfence();  // the owner's arena was written before it opened
+          return SV_HELP | (j1 - 1);
+        }
+        st = prev;
+      }
+    }
     __nanosleep(ns);
     if (ns < 1024) ns <<= 1;
   }
+}
+
+// The warps of a block search roots of the request whose shared state is h
+// (the block's own or, when helping, another slot's): a holds the request's
+// arena for the wide engine, ar for the register engines; slabs and shared
+// memory are the block's own.
+__device__ void search_roots(const ServeArgs &S, const BKArgs &a, const BKArgs &ar,
+                             const Slab &msl, const RegSlab<uint32_t> &rs32,
+                             const RegSlab<u64> &rs64, WarpSmem &sm, SvHelp *h) {
+  const int lane = (int)lane_id();
+  const int n = (int)ld_volatile((const uint32_t *)&h->n);
+  unsigned long long mine = 0, h0 = 0, h1 = 0;
+  RegRoot<uint32_t> rt32;
+  RegRoot<u64> rt64;
+  MemRoot rtm;
+  for (;;) {  // warps take roots in id order until done or over a limit
+    uint32_t r = 0;
+    if (lane == 0) {
+      const bool over = S.node_budget && ld_volatile(&h->nodes) > S.node_budget;
+      if (over) atomicOr(a.err, MCE_ERR_BUDGET);
+      r = (over || ld_volatile(a.err)) ? 0xFFFFFFFFu : atomicAdd(&h->rootnext, 1u);
+    }
+    r = __shfl_sync(MCE_FULL, r, 0);
+    if (r >= (uint32_t)n) break;
+    const int dp = a.rp[r + 1] - a.split[r], dm = a.split[r] - a.rp[r];
+    if (dp == 0) continue;
+    unsigned long long nd = 0, cnt = 0;
+    if (dp <= 32 && dm <= REG_XCAP) {
+      reg_encode<uint32_t, 1>(ar, sm.r32, rs32, (int32_t)r, rt32);
+      reg_tree<uint32_t, 1, true>(ar, sm.r32, rs32, rt32, WOps<uint32_t>::low(dp), 0u, 0u, h0, h1,
+                                  nd, cnt);
+    } else if (dp <= 64 && dm <= REG_XCAP) {
+      reg_encode<u64, 2>(ar, sm.r64, rs64, (int32_t)r, rt64);
+      reg_tree<u64, 2, true>(ar, sm.r64, rs64, rt64, WOps<u64>::low(dp), 0ull, 0ull, h0, h1, nd,
+                             cnt);
+    } else {  // mem_encode flags roots wider than SV_DCAP
+      mem_encode(a, sm.mem, msl, (int32_t)r, rtm);
+      if (rtm.d > 0) {
+        const int Wr = rtm.Wr;
+        if (lane < Wr) {  // root frame: P = all of N+(r), X = 0, S = 0
+          msl.stk[lane] = (lane == Wr - 1 && (dp & 63)) ? ((1ull << (dp & 63)) - 1ull) : ~0ull;
+          msl.stk[Wr + lane] = 0;
+          msl.stk[3 * Wr + lane] = 0;
+        }
+        __syncwarp();
+        mem_tree<true>(a, msl, rtm, h0, h1, nd, cnt);
+      }
+    }
+    mine += cnt;
+    if (lane == 0 && nd) atomicAdd(&h->nodes, nd);
+  }
+  if (lane == 0 && mine) atomicAdd(&h->total, mine);
 }
 
 __global__ void __launch_bounds__(SV_BLOCK) serve_kernel(ServeArgs S) {
@@ -492,17 +575,37 @@ __global__ void __launch_bounds__(SV_BLOCK) serve_kernel(ServeArgs S) {
   ar.slab = wslab;
   const RegSlab<uint32_t> rs32 = reg_slab<uint32_t>(ar, 0);
   const RegSlab<u64> rs64 = reg_slab<u64>(ar, 0);
+  SvHelp *own = &S.help[blockIdx.x];
   for (;;) {
-    if (threadIdx.x == 0) {
-      sh.req = claim(S);
-      sh.total = 0;
-      sh.nodes = 0;
-      sh.rootnext = 0;
-      *A.err = 0;
-    }
+    if (threadIdx.x == 0) sh.req = claim(S);
     __syncthreads();
     const uint32_t req = sh.req;
     if (req == SV_EXIT) break;
+    if (req & SV_HELP) {  // search roots of another slot's request in its arena
+      const uint32_t j = req & 0xFFFFFFu;
+      Arena B;
+      arena_layout(S.ego_cap, S.arc_cap, S.hcap, S.arena + (size_t)j * S.arena_bytes, &B);
+      BKArgs hb = a, hr = ar;
+      hb.rp = hr.rp = B.rp;
+      hb.split = hr.split = B.split;
+      hb.cs = hr.cs = B.cs;
+      hb.hist = hr.hist = B.hist;
+      hb.err = hr.err = B.err;
+      search_roots(S, hb, hr, msl, rs32, rs64, wsm[w], &S.help[j]);
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        __threadfence();  // this block's counts land before it leaves
+        atomicSub(&S.help[j].state, 1u);
+        atomicAdd(&S.ctl->helped, 1ull);
+      }
+      continue;
+    }
+    if (threadIdx.x == 0) {
+      *A.err = 0;
+      sh.posted = -1;
+      sh.broken = 0;
+    }
+    __syncthreads();
     const uint64_t t0 = globaltimer_ns();
     uint64_t t1 = t0, t2 = t0;
     SvEntry *E = S.ent + (req % S.ring);
@@ -521,55 +624,51 @@ __global__ void __launch_bounds__(SV_BLOCK) serve_kernel(ServeArgs S) {
         n = 0;
       }
     }
+    if (threadIdx.x == 0) {
+      sh.total = 0;
+      sh.nodes = 0;
+    }
     if (status == MCE_OK) {
       ego_peel(A, n, sh);
       ego_orient(A, n);
       t2 = globaltimer_ns();
-      unsigned long long mine = 0, h0 = 0, h1 = 0;
-      RegRoot<uint32_t> rt32;
-      RegRoot<u64> rt64;
-      MemRoot rtm;
-      WarpSmem &sm = wsm[w];
-      for (;;) {  // warps take roots in id order until done or over a limit
-        uint32_t r = 0;
-        if (lane == 0) {
-          const bool over = S.node_budget && ld_volatile(&sh.nodes) > S.node_budget;
-          if (over) atomicOr(A.err, MCE_ERR_BUDGET);
-          r = (over || ld_volatile(A.err)) ? 0xFFFFFFFFu : atomicAdd(&sh.rootnext, 1u);
-        }
-        r = __shfl_sync(MCE_FULL, r, 0);
-        if (r >= (uint32_t)n) break;
-        const int dp = A.rp[r + 1] - A.split[r], dm = A.split[r] - A.rp[r];
-        if (dp == 0) continue;
-        unsigned long long nd = 0, cnt = 0;
-        if (dp <= 32 && dm <= REG_XCAP) {
-          reg_encode<uint32_t, 1>(ar, sm.r32, rs32, (int32_t)r, rt32);
-          reg_tree<uint32_t, 1, true>(ar, sm.r32, rs32, rt32, WOps<uint32_t>::low(dp), 0u, 0u, h0, h1,
-                                nd, cnt);
-        } else if (dp <= 64 && dm <= REG_XCAP) {
-          reg_encode<u64, 2>(ar, sm.r64, rs64, (int32_t)r, rt64);
-          reg_tree<u64, 2, true>(ar, sm.r64, rs64, rt64, WOps<u64>::low(dp), 0ull, 0ull, h0, h1, nd,
-                           cnt);
-        } else {  // mem_encode flags roots wider than SV_DCAP
-          mem_encode(a, sm.mem, msl, (int32_t)r, rtm);
-          if (rtm.d > 0) {
-            const int Wr = rtm.Wr;
-            if (lane < Wr) {  // root frame: P = all of N+(r), X = 0, S = 0
-              msl.stk[lane] = (lane == Wr - 1 && (dp & 63)) ? ((1ull << (dp & 63)) - 1ull) : ~0ull;
-              msl.stk[Wr + lane] = 0;
-              msl.stk[3 * Wr + lane] = 0;
+      if (threadIdx.x == 0) {  // open the roots; large requests also to helping slots
+        own->rootnext = 0;
+        own->n = n;
+        own->total = 0;
+        own->nodes = 0;
+        __threadfence();  // the arena and the fields above before the opening
+        if (n >= SV_HELP_MIN) {
+          atomicExch(&own->state, SV_OPEN);
+          for (int e = 0; e < SV_BOARD; ++e)
+            if (atomicCAS(&S.board[e], 0u, blockIdx.x + 1) == 0u) {
+              sh.posted = e;
+              break;
             }
-            __syncwarp();
-            mem_tree<true>(a, msl, rtm, h0, h1, nd, cnt);
-          }
         }
-        mine += cnt;
-        if (lane == 0 && nd) atomicAdd(&sh.nodes, nd);
       }
-      if (lane == 0 && mine) atomicAdd(&sh.total, mine);
+      __syncthreads();
+      search_roots(S, a, ar, msl, rs32, rs64, wsm[w], own);
+      __syncthreads();
+      if (threadIdx.x == 0) {  // close, then wait (bounded) for the helpers to leave
+        if (sh.posted >= 0) atomicExch(&S.board[sh.posted], 0u);
+        atomicAnd(&own->state, ~SV_OPEN);
+        const uint64_t tw = globaltimer_ns();
+        while ((ld_volatile(&own->state) & 0xFFFFFFu) != 0) {
+          if (globaltimer_ns() - tw > SV_HELP_WAIT_NS) {
+            sh.broken = 1;
+            break;
+          }
+          __nanosleep(256);
+        }
+        __threadfence();
+        sh.total = ld_volatile(&own->total);
+        sh.nodes = ld_volatile(&own->nodes);
+      }
       __syncthreads();
       limits = ld_volatile(A.err);
       if (limits) status = MCE_ELIMIT;
+      if (sh.broken) status = MCE_ETIMEOUT;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -590,6 +689,8 @@ __global__ void __launch_bounds__(SV_BLOCK) serve_kernel(ServeArgs S) {
       atomicAdd(&S.ctl->nodes, sh.nodes);
     }
     __syncthreads();
+    // a helper that never left may still read the arena: the slot retires
+    if (sh.broken) break;
   }
 }
 
@@ -620,6 +721,8 @@ struct mce_serve {
   char *arena = nullptr;
   unsigned long long *slab = nullptr;
   SvCtl *ctl = nullptr;
+  SvHelp *help = nullptr;
+  uint32_t *board = nullptr;
   int64_t launches = 0;
   bool closed = false;
 };
@@ -662,6 +765,8 @@ void sv_free(mce_serve *s) {
   if (s->arena) cudaFree(s->arena);
   if (s->slab) cudaFree(s->slab);
   if (s->ctl) cudaFree(s->ctl);
+  if (s->help) cudaFree(s->help);
+  if (s->board) cudaFree(s->board);
   delete s;
 }
 
@@ -748,9 +853,16 @@ extern "C" int mce_serve_open(mce_graph_t g, const mce_serve_opts_t *opts, mce_s
   if (cudaMalloc((void **)&s->arena, A.arena_bytes * s->slots) != cudaSuccess ||
       cudaMalloc((void **)&s->slab, A.slab_words * 8 * (size_t)s->slots * SV_WARPS) !=
           cudaSuccess ||
-      cudaMalloc((void **)&s->ctl, sizeof(SvCtl)) != cudaSuccess)
+      cudaMalloc((void **)&s->ctl, sizeof(SvCtl)) != cudaSuccess ||
+      cudaMalloc((void **)&s->help, sizeof(SvHelp) * s->slots) != cudaSuccess ||
+      cudaMalloc((void **)&s->board, sizeof(uint32_t) * SV_BOARD) != cudaSuccess)
     return fail(MCE_ENOMEM);
-  if (cudaMemset(s->ctl, 0, sizeof(SvCtl)) != cudaSuccess) return fail(MCE_ECUDA);
+  if (cudaMemset(s->ctl, 0, sizeof(SvCtl)) != cudaSuccess ||
+      cudaMemset(s->help, 0, sizeof(SvHelp) * s->slots) != cudaSuccess ||
+      cudaMemset(s->board, 0, sizeof(uint32_t) * SV_BOARD) != cudaSuccess)
+    return fail(MCE_ECUDA);
+  A.help = s->help;
+  A.board = s->board;
   A.arena = s->arena;
   A.slab = s->slab;
   A.ctl = s->ctl;
@@ -766,7 +878,7 @@ extern "C" int mce_serve_submit(mce_serve_t s, int64_t seed, uint64_t *id_out) {
   if (s->closed) return MCE_ESTATE;
   sv_retire(s);
   if (s->tail - s->low >= s->ring) return MCE_ELIMIT;  // ring full: take answers first
-  if (s->tail == 0xFFFFFFF0u) return MCE_ELIMIT;       // ids exhausted
+  if (s->tail >= 0x3FFFFFF0u) return MCE_ELIMIT;       // ids exhausted (below SV_HELP)
   const uint32_t id = s->tail;
   SvEntry &e = s->ent[id % s->ring];
   e.seed = seed;
@@ -869,6 +981,7 @@ extern "C" int mce_serve_stats(mce_serve_t s, mce_serve_stats_t *st) {
   st->kernel_launches = s->launches;
   st->arena_bytes = (uint64_t)s->args.arena_bytes * s->slots;
   st->slab_bytes = (uint64_t)s->args.slab_words * 8 * s->slots * SV_WARPS;
+  st->helps = c.helped;
   st->running = cudaStreamQuery(s->stream) == cudaErrorNotReady ? 1 : 0;
   return MCE_OK;
 }

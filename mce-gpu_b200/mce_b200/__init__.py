@@ -103,7 +103,7 @@ class _ServeStats(C.Structure):
     _fields_ = [("slots", C.c_int32), ("running", C.c_int32), ("ring", C.c_uint32),
                 ("pad", C.c_uint32), ("submitted", C.c_uint64), ("served", C.c_uint64),
                 ("tree_nodes", C.c_uint64), ("kernel_launches", C.c_int64),
-                ("arena_bytes", C.c_uint64), ("slab_bytes", C.c_uint64)]
+                ("arena_bytes", C.c_uint64), ("slab_bytes", C.c_uint64), ("helps", C.c_uint64)]
 
 
 _P = C.c_void_p
@@ -127,6 +127,7 @@ _sigs = {
     "mce_count": (C.c_int, [_P, _P, _P, _P, _P]),
     "mce_root_log": (C.c_int, [_P, _P]),
     "mce_root_counts": (C.c_int, [_P, _P]),
+    "mce_list": (C.c_int, [_P, _P, _P, C.c_int64, _P, C.c_int64, _P, _P]),
     "mce_warp_log": (C.c_int, [_P, _P, _P, _P, _P, C.c_int64, _P]),
     "mce_count_oriented_noalloc": (C.c_int, [_P, _P, _P, _P, C.c_int64, _P, _P]),
     "mce_batch_upload": (C.c_int, [_P, _P, _P, _P, C.c_int32, C.c_int32, _P, _P]),
@@ -459,6 +460,25 @@ class Graph:
         out = np.zeros(max(self.n, 1), np.uint64)
         _check(_lib.mce_root_log(self._h, _ptr(out)), "root_log")
         return out[:self.n]
+
+    def list_cliques(self, ids_cap: int = 1 << 22, cliques_cap: int = 1 << 20,
+                     **opts) -> list[np.ndarray]:
+        """Every maximal clique as an array of vertex ids (root first);
+        grows the buffers once if the first caps are too small."""
+        for _ in range(2):
+            ids = np.zeros(max(ids_cap, 1), np.int32)
+            off = np.zeros(cliques_cap + 1, np.int64)
+            cnt, need = C.c_uint64(), C.c_int64()
+            o = make_opts(**opts)
+            rc = _lib.mce_list(self._h, C.byref(o), _ptr(ids), ids_cap, _ptr(off), cliques_cap,
+                               C.byref(cnt), C.byref(need))
+            if rc == ELIMIT:
+                ids_cap, cliques_cap = max(ids_cap, need.value), max(cliques_cap, cnt.value)
+                continue
+            _check(rc, "list")
+            k = cnt.value
+            return [ids[off[i]:off[i + 1]].copy() for i in range(k)]
+        raise MceError(ELIMIT, "list")
 
     def warp_log(self) -> dict:
         """Per search warp of the last count(warp_log=1 or 2): SM id, tree nodes,
