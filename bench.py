@@ -436,6 +436,10 @@ def serve_trace(n, count, rate, seed):
     return seeds, arrival
 
 
+def log(msg):
+    print(f"[{time.strftime('%H:%M:%S')}] {msg}", file=sys.stderr, flush=True)
+
+
 def pct(x, q):
     return float(np.percentile(np.asarray(x, np.float64), q)) if len(x) else None
 
@@ -448,6 +452,7 @@ def run_serve(args, rank, world, local_rank):
     import oracle
     torch.cuda.set_device(local_rank)
     hg, desc = serve_graph(args)
+    log(f"serve: resident graph n={hg.n} arcs={hg.m}")
     g = mce.Graph.from_host(hg, device=local_rank)
     s = mce.Serve(g, ego_cap=args.ego_cap, max_nodes=args.max_nodes)
     try:
@@ -458,10 +463,11 @@ def run_serve(args, rank, world, local_rank):
             if world > 1:
                 torch.distributed.barrier()
             res_all, lat_all, makespans = [], [], []
+            log("serve: warm-up done")
             for k in range(args.steps):
                 seeds, arr = serve_trace(hg.n, args.requests, args.rate, 31 + 1000 * rank + k)
                 t0 = time.perf_counter()
-                res, lat = s.run(seeds, arr)
+                res, lat = s.run(seeds, arr, timeout_ms=300000)
                 makespans.append(time.perf_counter() - t0)
                 res_all.append(res)
                 lat_all.append(lat)
@@ -475,17 +481,22 @@ def run_serve(args, rank, world, local_rank):
         # capacity: every request of one trace admitted at once
         seeds_b, _ = serve_trace(hg.n, args.requests, 0, 77 + rank)
         t0 = time.perf_counter()
-        res_b, lat_b = s.run(seeds_b, None)
+        res_b, lat_b = s.run(seeds_b, None, timeout_ms=300000)
         burst_s = time.perf_counter() - t0
         st = s.stats()
-        # oracle check on a sample of the timed requests
+        # oracle check on a sample of the timed requests (smallest first, at
+        # most about a minute of CPU time)
+        log(f"serve: {len(res)} requests timed; oracle sample")
         rng = np.random.default_rng(5)
         pick = rng.choice(len(res), size=min(24, len(res)), replace=False)
-        mism, checked = 0, 0
+        pick = sorted(pick, key=lambda i: int(res[i]["count"]))
+        mism, checked, t_or = 0, 0, time.perf_counter()
         for i in pick:
             r = res[i]
             if r["status"] != mce.OK:
                 continue
+            if time.perf_counter() - t_or > 60:
+                break
             eg, _ = mce.ego_subgraph(hg, int(r["seed"]), args.ego_cap)
             checked += 1
             mism += int(oracle.count(eg)[0] != int(r["count"]))

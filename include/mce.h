@@ -51,7 +51,11 @@ extern "C" {
 #define MCE_MAX_LATER_DEGREE 2048
 
 /* ---- options ------------------------------------------------------------ */
-/* -p (include/config.h:52-61): level of the subtrees that are parallelised */
+/* -p (include/config.h:52-61): level of the subtrees that are parallelised.
+ * L1: a root's subtrees go to idle warps once its walk is under way
+ * (donate_after nodes); L2: its first-level subtrees (one per edge from the
+ * root, the reference's edge-rooted L2 instances) are offered to idle warps
+ * at once.                                                                  */
 #define MCE_LEVEL_L1 1
 #define MCE_LEVEL_L2 2
 /* -i (include/config.h:72-81): which sets the induced subgraph is built on */

@@ -546,7 +546,7 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
     // hand the child to an idle warp (try_dequeue / do_fork_L1,
     // mce/mce_utils.cuh:872-880,1063-1113)
     if (share && pc >= a.donate_min &&
-        (nodes >= a.donate_after || (a.policy && a.policy[rt.r]))) {
+        (nodes >= a.donate_after || (a.policy && a.policy[rt.r]) || (a.level2 && depth == 0))) {
       MCE_BD(BD_QUEUE);
       if (--recheck <= 0) {  // the queue state is read every 32 candidate nodes
         want = wants_task(a.q);
@@ -932,7 +932,7 @@ __device__ void mem_tree(const BKArgs &a, const Slab &sl, const MemRoot &rt, u64
     }
     if (__any_sync(MCE_FULL, el)) continue;
     if (share && pc >= a.donate_min &&
-        (nodes >= a.donate_after || (a.policy && a.policy[rt.r])) &&
+        (nodes >= a.donate_after || (a.policy && a.policy[rt.r]) || (a.level2 && depth == 0)) &&
         (--recheck <= 0 ? (recheck = 32, want = wants_task(a.q)) : want)) {
       MCE_BD(BD_QUEUE);
       const int WM = (a.dcap + 63) >> 6;

@@ -261,3 +261,15 @@ def test_wide_engine_occupancy_variants(wide_blocks):
     assert r.stats["class_roots"][2] > 0
     assert r.total == t and np.array_equal(r.hist, h)
     assert np.array_equal(nodes, oracle.roots(g)[3])
+
+
+def test_level2_offers_first_level_subtrees():
+    g = mce.gen_rmat(12, 16, 0.57, 0.19, 0.19, 7)
+    t, h, _ = oracle.count(g)
+    _, _, rc, rn = oracle.roots(g)
+    with mce.Graph.from_host(g) as dg:
+        r = dg.count(level=mce.LEVEL_L2, log_roots=True)
+        counts, nodes = dg.root_counts(), dg.root_log()
+    assert r.total == t and np.array_equal(r.hist, h)
+    assert np.array_equal(counts, rc) and np.array_equal(nodes, rn)  # same trees, shared sooner
+    assert r.stats["donations"] > 0

@@ -126,3 +126,17 @@ def test_serve_poll_contract():
             pending = [s.submit(i) for i in range(20)]
         # closing with unpolled requests finishes them and frees the session
         assert len(pending) == 20
+
+
+def test_serve_idle_slots_help_large_requests(ba):
+    hg, g = ba
+    deg = np.diff(hg.row_ptr[:hg.n + 1])
+    seeds = [int(x) for x in np.argsort(deg)[-8:]]  # hubs: ego graphs at the cap
+    with mce.Serve(g, ego_cap=4096) as s:
+        got = [s.wait(s.submit(x)) for x in seeds]  # one at a time: the other slots idle
+        st = s.stats()
+    for r, x in zip(got, seeds):
+        want, n, m = ego_count(hg, x, 4096)
+        assert r["status"] == mce.OK and n >= 1024
+        assert (int(r["count"]), int(r["ego_n"])) == (want, n)
+    assert st["helps"] > 0
