@@ -100,7 +100,7 @@ struct ServeArgs {
 };
 
 struct Arena {
-  int32_t *hkey, *hval, *V, *rp, *col, *split, *cs, *deg, *core, *fa, *fb, *cnt;
+  int32_t *hkey, *hval, *hfirst, *V, *rp, *col, *split, *cs, *deg, *core, *fa, *fb, *off;
   uint32_t *prio, *err;
   unsigned long long *hist;  // clique sizes above the engines' register bins
 };
@@ -116,6 +116,7 @@ __host__ __device__ inline size_t arena_layout(int ego_cap, int arc_cap, int hca
   Arena x;
   x.hkey = (int32_t *)take(4 * (size_t)hcap);
   x.hval = (int32_t *)take(4 * (size_t)hcap);
+  x.hfirst = (int32_t *)take(4 * (size_t)hcap);
   x.V = (int32_t *)take(4 * (size_t)ego_cap);
   x.rp = (int32_t *)take(4 * ((size_t)ego_cap + 1));
   x.col = (int32_t *)take(4 * (size_t)arc_cap);
@@ -125,7 +126,7 @@ __host__ __device__ inline size_t arena_layout(int ego_cap, int arc_cap, int hca
   x.core = (int32_t *)take(4 * (size_t)ego_cap);
   x.fa = (int32_t *)take(4 * (size_t)ego_cap);
   x.fb = (int32_t *)take(4 * (size_t)ego_cap);
-  x.cnt = (int32_t *)take(4 * (size_t)ego_cap);
+  x.off = (int32_t *)take(4 * ((size_t)ego_cap + 1));
   x.prio = (uint32_t *)take(4 * (size_t)ego_cap);
   x.err = (uint32_t *)take(4);
   x.hist = (unsigned long long *)take(8 * (size_t)MCE_HIST_MAX);
@@ -155,19 +156,18 @@ __device__ __forceinline__ int32_t hget(const Arena &A, int hcap, int32_t key) {
   return -1;
 }
 
-// insert key; true if it was absent (then *slot holds its entry)
+// insert key if absent; *slot receives its entry; true if this call inserted it
 __device__ __forceinline__ bool hput(const Arena &A, int hcap, int32_t key, uint32_t *slot) {
   uint32_t h = hslot(key, hcap);
   for (int p = 0; p < hcap; ++p) {
     const int32_t old = atomicCAS(&A.hkey[h], -1, key);
-    if (old == -1) {
+    if (old == -1 || old == key) {
       *slot = h;
-      return true;
+      return old == -1;
     }
-    if (old == key) return false;
     h = (h + 1) & (uint32_t)(hcap - 1);
   }
-  return false;  // cannot happen: the table has twice the cap's entries
+  return false;  // cannot happen: the table has twice the keys it can receive
 }
 
 // exclusive scan of one value per thread over the block; returns the total
@@ -209,44 +209,140 @@ __device__ void block_sort(int32_t *buf, int n_pow2) {
 struct SvShared {
   uint32_t req;
   int32_t posted, broken;
-  int32_t k, fcnt, ncnt, todo, level, minv, acnt;
+  int32_t k, fcnt, ncnt, todo, level, minv, acnt, ia, ib, carry;
   unsigned long long total, nodes;
   int ws[SV_WARPS];
 };
 
-// Append the not-yet-seen vertices of row [b, e) of the resident graph to
-// the ego list in row order, stopping at the cap.
-__device__ void ego_append_row(const ServeArgs &S, const Arena &A, int32_t b, int32_t e,
-                               SvShared &sh) {
+constexpr int32_t SV_PENDING = -3;  // hval of a vertex first seen in the current window
+
+// inclusive max over the block (one value per thread)
+__device__ __forceinline__ int block_max_scan(int x, int *ws) {
+  const int lane = (int)lane_id(), w = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(MCE_FULL, x, o);
+    if (lane >= o) x = max(x, y);
+  }
+  if (lane == 31) ws[w] = x;
+  __syncthreads();
+  int before = -1;
+  for (int i = 0; i < w; ++i) before = max(before, ws[i]);
+  __syncthreads();
+  return max(x, before);
+}
+
+// first i in [0, n) with a[i] >= key (n if none)
+__device__ __forceinline__ int lower_bound_i(const int32_t *a, int n, int32_t key) {
+  int lo = 0, len = n;
+  while (len > 0) {
+    const int half = len >> 1;
+    if (a[lo + half] < key) {
+      lo += half + 1;
+      len -= half + 1;
+    } else {
+      len = half;
+    }
+  }
+  return lo;
+}
+
+// off[0 .. nrows] = exclusive prefix of the resident-row lengths of the
+// vertices list[0 .. nrows); returns the total.
+__device__ int row_offsets(const ServeArgs &S, const int32_t *list, int nrows, int32_t *off,
+                           SvShared &sh) {
+  int base = 0;
+  for (int i0 = 0; i0 < nrows; i0 += blockDim.x) {
+    const int i = i0 + (int)threadIdx.x;
+    int len = 0;
+    if (i < nrows) {
+      const int32_t g = list[i];
+      len = S.grp[g + 1] - S.grp[g];
+    }
+    int ex;
+    const int tot = block_scan(len, &ex, sh.ws);
+    if (i < nrows) off[i] = base + ex;
+    base += tot;
+  }
+  if (threadIdx.x == 0) off[nrows] = base;
+  __syncthreads();
+  return base;
+}
+
+// The rows list[0 .. nrows) of the resident graph are walked as one
+// flattened sequence, blockDim elements per window.  This returns the row
+// that owns position e0 + threadIdx.x: the last row starting at or before
+// it (`carry`, the owner of the previous window's last position, covers a
+// window in which no row starts before a thread's position).
+__device__ int window_owner(const int32_t *off, int nrows, int e0, int carry, int32_t *own_sm,
+                            SvShared &sh) {
+  own_sm[threadIdx.x] = -1;
+  if (threadIdx.x == 0) {
+    sh.ia = lower_bound_i(off, nrows, e0);
+    sh.ib = lower_bound_i(off, nrows, e0 + (int)blockDim.x);
+  }
+  __syncthreads();
+  // rows of length 0 start where the next row starts: the larger index wins
+  for (int i = sh.ia + (int)threadIdx.x; i < sh.ib; i += blockDim.x)
+    atomicMax(&own_sm[off[i] - e0], i);
+  __syncthreads();
+  return max(block_max_scan(own_sm[threadIdx.x], sh.ws), carry);
+}
+
+// Append the vertices first met in the rows of list[0 .. nrows) (row order,
+// then position: discovery order) to the ego list, up to the cap.  A vertex
+// seen at several positions of one window is appended at the first.
+__device__ void ego_discover(const ServeArgs &S, const Arena &A, const int32_t *list, int nrows,
+                             int32_t *own_sm, SvShared &sh) {
   const int cap = S.ego_cap, hc = S.hcap;
-  for (int32_t j0 = b; j0 < e; j0 += (int32_t)blockDim.x) {
+  const int T = row_offsets(S, list, nrows, A.off, sh);
+  int carry = -1;
+  for (int e0 = 0; e0 < T; e0 += blockDim.x) {
     const int k = sh.k;  // read by all before thread 0 updates it below
     if (k >= cap) break;
-    const int32_t j = j0 + (int32_t)threadIdx.x;
-    bool fresh = false;
+    const int o = window_owner(A.off, nrows, e0, carry, own_sm, sh);
+    const int e = e0 + (int)threadIdx.x;
+    int32_t w = -1;
     uint32_t slot = 0;
-    if (j < e) fresh = hput(A, hc, S.gcol[j], &slot);
+    bool cand = false;
+    if (e < T) {
+      const int32_t g = list[o];
+      w = S.gcol[S.grp[g] + (e - A.off[o])];
+      hput(A, hc, w, &slot);  // inserts or finds the vertex
+      cand = A.hval[slot] == SV_PENDING;
+      if (cand) atomicMin(&A.hfirst[slot], e);
+    }
+    __syncthreads();
+    const bool fresh = cand && A.hfirst[slot] == e;
     int pos;
     const int tot = block_scan(fresh ? 1 : 0, &pos, sh.ws);
     if (fresh) {
       if (k + pos < cap) {
         A.hval[slot] = k + pos;
-        A.V[k + pos] = S.gcol[j];
+        A.V[k + pos] = w;
       } else {
         A.hval[slot] = -1;  // beyond the cap: not in the ego graph
       }
     }
-    if (threadIdx.x == 0) sh.k = min(cap, k + tot);
+    if (threadIdx.x == blockDim.x - 1) {
+      sh.k = min(cap, k + tot);
+      sh.carry = o;
+    }
     __syncthreads();
+    carry = sh.carry;
   }
 }
 
 // Build the ego graph of `seed` in the arena: sorted local CSR in rp/col.
 // Returns its vertex count, or -1 if it has more arcs than the arena holds.
 __device__ int ego_extract(const ServeArgs &S, const Arena &A, int64_t seed, int32_t *sortbuf,
-                           SvShared &sh) {
+                           int32_t *own_sm, SvShared &sh) {
   const int hc = S.hcap;
-  for (int i = threadIdx.x; i < hc; i += blockDim.x) A.hkey[i] = -1;
+  for (int i = threadIdx.x; i < hc; i += blockDim.x) {
+    A.hkey[i] = -1;
+    A.hval[i] = SV_PENDING;
+    A.hfirst[i] = INT_MAX;
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
     uint32_t slot = 0;
@@ -256,13 +352,9 @@ __device__ int ego_extract(const ServeArgs &S, const Arena &A, int64_t seed, int
     sh.k = 1;
   }
   __syncthreads();
-  ego_append_row(S, A, S.grp[seed], S.grp[seed + 1], sh);  // 1-hop
+  ego_discover(S, A, A.V, 1, own_sm, sh);  // 1-hop: the seed's row
   const int k1 = sh.k;
-  for (int i = 1; i < k1; ++i) {  // 2-hop, in discovery order
-    if (sh.k >= S.ego_cap) break;
-    const int32_t u = A.V[i];
-    ego_append_row(S, A, S.grp[u], S.grp[u + 1], sh);
-  }
+  if (k1 < S.ego_cap && k1 > 1) ego_discover(S, A, A.V + 1, k1 - 1, own_sm, sh);  // 2-hop
   const int n = sh.k;
   // local ids in ascending resident-graph id
   int np2 = 1;
@@ -278,45 +370,35 @@ __device__ int ego_extract(const ServeArgs &S, const Arena &A, int64_t seed, int
     A.hval[h] = i;
   }
   __syncthreads();
-  // induced rows: count, scan, fill (filtering a sorted row keeps it sorted)
-  const int lane = (int)lane_id(), w = threadIdx.x >> 5;
-  for (int i = w; i < n; i += SV_WARPS) {
-    const int32_t g = A.V[i], gb = S.grp[g], ge = S.grp[g + 1];
-    int c = 0;
-    for (int32_t j0 = gb; j0 < ge; j0 += 32) {
-      const int32_t j = j0 + lane;
-      const bool in = j < ge && hget(A, hc, S.gcol[j]) >= 0;
-      c += __popc(__ballot_sync(MCE_FULL, in));
+  // induced rows in one flattened pass: the i-th kept element overall is
+  // col[i] (rows in order, each filtered row stays sorted), and a row starts
+  // at the count of kept elements before its first one
+  const int T = row_offsets(S, A.V, n, A.off, sh);
+  int carry = -1, kept = 0;
+  for (int e0 = 0; e0 < T; e0 += blockDim.x) {
+    const int o = window_owner(A.off, n, e0, carry, own_sm, sh);
+    const int e = e0 + (int)threadIdx.x;
+    int32_t loc = -1;
+    if (e < T) {
+      const int32_t g = A.V[o];
+      loc = hget(A, hc, S.gcol[S.grp[g] + (e - A.off[o])]);
     }
-    if (lane == 0) A.cnt[i] = c;
-  }
-  if (threadIdx.x == 0) sh.acnt = 0;
-  __syncthreads();
-  for (int i0 = 0; i0 < n; i0 += blockDim.x) {
-    const int i = i0 + (int)threadIdx.x;
-    const int base = sh.acnt;
-    int ex;
-    const int tot = block_scan(i < n ? A.cnt[i] : 0, &ex, sh.ws);
-    if (i < n) A.rp[i] = base + ex;
-    if (threadIdx.x == 0) sh.acnt = base + tot;
+    int pos;
+    const int tot = block_scan(loc >= 0 ? 1 : 0, &pos, sh.ws);
+    if (loc >= 0 && kept + pos < S.arc_cap) A.col[kept + pos] = loc;
+    own_sm[threadIdx.x] = pos;  // kept elements of this window before each position
     __syncthreads();
+    for (int i = sh.ia + (int)threadIdx.x; i < sh.ib; i += blockDim.x)  // rows starting here
+      A.rp[i] = kept + own_sm[A.off[i] - e0];
+    if (threadIdx.x == blockDim.x - 1) sh.carry = o;
+    __syncthreads();
+    carry = sh.carry;
+    kept += tot;
   }
-  const int m = sh.acnt;
-  if (m > S.arc_cap) return -1;
-  if (threadIdx.x == 0) A.rp[n] = m;
-  for (int i = w; i < n; i += SV_WARPS) {
-    const int32_t g = A.V[i], gb = S.grp[g], ge = S.grp[g + 1];
-    int out = A.rp[i];
-    for (int32_t j0 = gb; j0 < ge; j0 += 32) {
-      const int32_t j = j0 + lane;
-      const int32_t loc = j < ge ? hget(A, hc, S.gcol[j]) : -1;
-      const uint32_t mk = __ballot_sync(MCE_FULL, loc >= 0);
-      if (loc >= 0) A.col[out + __popc(mk & ((1u << lane) - 1u))] = loc;
-      out += __popc(mk);
-    }
-  }
+  for (int i = threadIdx.x; i <= n; i += blockDim.x)  // rows starting at the end (empty)
+    if (A.off[i] == T) A.rp[i] = kept;
   __syncthreads();
-  return n;
+  return kept > S.arc_cap ? -1 : n;
 }
 
 // Degeneracy priorities of the ego graph: synchronous peeling rounds over
@@ -552,6 +634,7 @@ __global__ void __launch_bounds__(SV_BLOCK) serve_kernel(ServeArgs S) {
   extern __shared__ int32_t sortbuf[];  // next power of two >= ego_cap ints
   __shared__ SvShared sh;
   __shared__ WarpSmem wsm[SV_WARPS];
+  __shared__ int32_t own_sm[SV_BLOCK];
   const int lane = (int)lane_id(), w = threadIdx.x >> 5;
   Arena A;
   arena_layout(S.ego_cap, S.arc_cap, S.hcap, S.arena + (size_t)blockIdx.x * S.arena_bytes, &A);
@@ -616,7 +699,7 @@ __global__ void __launch_bounds__(SV_BLOCK) serve_kernel(ServeArgs S) {
     if (seed < 0 || seed >= S.gn) {
       status = MCE_EINVAL;
     } else {
-      n = ego_extract(S, A, seed, sortbuf, sh);
+      n = ego_extract(S, A, seed, sortbuf, own_sm, sh);
       t1 = t2 = globaltimer_ns();
       if (n < 0) {
         status = MCE_ELIMIT;
