@@ -209,7 +209,7 @@ __device__ void block_sort(int32_t *buf, int n_pow2) {
 struct SvShared {
   uint32_t req;
   int32_t posted, broken;
-  int32_t k, fcnt, ncnt, todo, level, minv, acnt, ia, ib, carry;
+  int32_t k, fcnt, ncnt, todo, level, minv, acnt, carry;
   unsigned long long total, nodes;
   int ws[SV_WARPS];
 };
@@ -230,21 +230,6 @@ __device__ __forceinline__ int block_max_scan(int x, int *ws) {
   for (int i = 0; i < w; ++i) before = max(before, ws[i]);
   __syncthreads();
   return max(x, before);
-}
-
-// first i in [0, n) with a[i] >= key (n if none)
-__device__ __forceinline__ int lower_bound_i(const int32_t *a, int n, int32_t key) {
-  int lo = 0, len = n;
-  while (len > 0) {
-    const int half = len >> 1;
-    if (a[lo + half] < key) {
-      lo += half + 1;
-      len -= half + 1;
-    } else {
-      len = half;
-    }
-  }
-  return lo;
 }
 
 // off[0 .. nrows] = exclusive prefix of the resident-row lengths of the
@@ -273,19 +258,26 @@ __device__ int row_offsets(const ServeArgs &S, const int32_t *list, int nrows, i
 // flattened sequence, blockDim elements per window.  This returns the row
 // that owns position e0 + threadIdx.x: the last row starting at or before
 // it (`carry`, the owner of the previous window's last position, covers a
-// window in which no row starts before a thread's position).
-__device__ int window_owner(const int32_t *off, int nrows, int e0, int carry, int32_t *own_sm,
-                            SvShared &sh) {
+// window in which no row starts before a thread's position).  [ia, ib) are
+// the rows starting in the window; ia comes in as the previous window's ib
+// (0 at the start): starts are ascending, so they are found by one pass of
+// coalesced loads, not a search.
+__device__ int window_owner(const int32_t *off, int nrows, int e0, int carry, int &ia, int &ib,
+                            int32_t *own_sm, SvShared &sh) {
   own_sm[threadIdx.x] = -1;
-  if (threadIdx.x == 0) {
-    sh.ia = lower_bound_i(off, nrows, e0);
-    sh.ib = lower_bound_i(off, nrows, e0 + (int)blockDim.x);
+  __syncthreads();
+  const int B = (int)blockDim.x;
+  int count = 0;
+  for (;;) {
+    const int i = ia + count + (int)threadIdx.x;
+    const bool in = i < nrows && off[i] < e0 + B;
+    // rows of length 0 start where the next row starts: the larger index wins
+    if (in) atomicMax(&own_sm[off[i] - e0], i);
+    const int c = __syncthreads_count(in);
+    count += c;
+    if (c < B) break;
   }
-  __syncthreads();
-  // rows of length 0 start where the next row starts: the larger index wins
-  for (int i = sh.ia + (int)threadIdx.x; i < sh.ib; i += blockDim.x)
-    atomicMax(&own_sm[off[i] - e0], i);
-  __syncthreads();
+  ib = ia + count;
   return max(block_max_scan(own_sm[threadIdx.x], sh.ws), carry);
 }
 
@@ -296,11 +288,11 @@ __device__ void ego_discover(const ServeArgs &S, const Arena &A, const int32_t *
                              int32_t *own_sm, SvShared &sh) {
   const int cap = S.ego_cap, hc = S.hcap;
   const int T = row_offsets(S, list, nrows, A.off, sh);
-  int carry = -1;
-  for (int e0 = 0; e0 < T; e0 += blockDim.x) {
+  int carry = -1, ia = 0, ib = 0;
+  for (int e0 = 0; e0 < T; e0 += blockDim.x, ia = ib) {
     const int k = sh.k;  // read by all before thread 0 updates it below
     if (k >= cap) break;
-    const int o = window_owner(A.off, nrows, e0, carry, own_sm, sh);
+    const int o = window_owner(A.off, nrows, e0, carry, ia, ib, own_sm, sh);
     const int e = e0 + (int)threadIdx.x;
     int32_t w = -1;
     uint32_t slot = 0;
@@ -374,9 +366,9 @@ __device__ int ego_extract(const ServeArgs &S, const Arena &A, int64_t seed, int
   // col[i] (rows in order, each filtered row stays sorted), and a row starts
   // at the count of kept elements before its first one
   const int T = row_offsets(S, A.V, n, A.off, sh);
-  int carry = -1, kept = 0;
-  for (int e0 = 0; e0 < T; e0 += blockDim.x) {
-    const int o = window_owner(A.off, n, e0, carry, own_sm, sh);
+  int carry = -1, kept = 0, ia = 0, ib = 0;
+  for (int e0 = 0; e0 < T; e0 += blockDim.x, ia = ib) {
+    const int o = window_owner(A.off, n, e0, carry, ia, ib, own_sm, sh);
     const int e = e0 + (int)threadIdx.x;
     int32_t loc = -1;
     if (e < T) {
@@ -388,7 +380,7 @@ __device__ int ego_extract(const ServeArgs &S, const Arena &A, int64_t seed, int
     if (loc >= 0 && kept + pos < S.arc_cap) A.col[kept + pos] = loc;
     own_sm[threadIdx.x] = pos;  // kept elements of this window before each position
     __syncthreads();
-    for (int i = sh.ia + (int)threadIdx.x; i < sh.ib; i += blockDim.x)  // rows starting here
+    for (int i = ia + (int)threadIdx.x; i < ib; i += blockDim.x)  // rows starting here
       A.rp[i] = kept + own_sm[A.off[i] - e0];
     if (threadIdx.x == blockDim.x - 1) sh.carry = o;
     __syncthreads();
