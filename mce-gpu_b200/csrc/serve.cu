@@ -39,7 +39,7 @@ namespace mce {
 
 namespace {
 
-constexpr int SV_BLOCK = 256;
+constexpr int SV_BLOCK = 512;  // 16 warps: halves the block-wide phases of a large request
 constexpr int SV_WARPS = SV_BLOCK / 32;
 constexpr int SV_DCAP = 256;            // widest root (later neighbours) a slot searches
 constexpr uint64_t SV_POLL_NS = 500;    // host tail read at most this often
@@ -623,9 +623,12 @@ __device__ void search_roots(const ServeArgs &S, const BKArgs &a, const BKArgs &
 }
 
 __global__ void __launch_bounds__(SV_BLOCK) serve_kernel(ServeArgs S) {
-  extern __shared__ int32_t sortbuf[];  // next power of two >= ego_cap ints
+  // dynamic: the warps' engine state, then the sort buffer (next power of
+  // two >= ego_cap ints)
+  extern __shared__ __align__(16) unsigned char sv_dyn[];
+  WarpSmem *wsm = (WarpSmem *)sv_dyn;
+  int32_t *sortbuf = (int32_t *)(sv_dyn + sizeof(WarpSmem) * SV_WARPS);
   __shared__ SvShared sh;
-  __shared__ WarpSmem wsm[SV_WARPS];
   __shared__ int32_t own_sm[SV_BLOCK];
   const int lane = (int)lane_id(), w = threadIdx.x >> 5;
   Arena A;
@@ -878,7 +881,7 @@ extern "C" int mce_serve_open(mce_graph_t g, const mce_serve_opts_t *opts, mce_s
   s->ring = o.ring;
   int np2 = 1;
   while (np2 < o.ego_cap) np2 <<= 1;
-  s->smem = sizeof(int32_t) * (size_t)np2;
+  s->smem = sizeof(WarpSmem) * SV_WARPS + sizeof(int32_t) * (size_t)np2;
   auto fail = [&](int code) {
     sv_free(s);
     return code;
