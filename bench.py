@@ -401,7 +401,11 @@ def run_mine(args, rank, world, local_rank):
                 assert r.total == total, f"{name} schedule changed the count"
                 ts.append(e0.elapsed_time(e1))
             ms = sum(ts) / len(ts)
-            cmp[name] = {"ms_per_step": round(ms, 3), "value": total / (ms / 1e3)}
+            cmp[name] = {"ms_per_step": round(ms, 3), "value": total / (ms / 1e3),
+                         "phases_ms": {"search": round(r.stats["count_ms"], 3),
+                                       "peel": round(r.stats["peel_ms"], 3),
+                                       "orient": round(r.stats["orient_ms"], 3)},
+                         "tasks_shared": r.stats["donations"]}
         line["config"]["other_schedules"] = cmp
     if hb is not None and not args.no_plain:
         kw_plain = {k: v for k, v in kw.items() if k not in ("cuda_graph", "model", "sched")}

@@ -82,7 +82,11 @@ typedef struct mce_opts {
                                subtree must have to be donated                 */
   int32_t log_roots;        /* 1 = record per-root search-tree node counts    */
   int32_t x_pivot;          /* 1 = also take pivots from the root's earlier
-                               neighbours (the -i px pivot rule)               */
+                               neighbours adjacent to the chosen set, and prune
+                               a subtree when one of them covers P (the -i px
+                               rule; also set by induced = MCE_INDUCED_PX).
+                               Register engines only; the count is unchanged,
+                               the search trees are not                      */
   int32_t peel_solo_max;    /* 0 = default (off); < 0 = off; > 0: frontiers of at most
                                this many vertices are peeled by one block           */
   int32_t donate_after;     /* 0 = default (256): a warp shares subtrees of a
@@ -374,8 +378,8 @@ int mce_count_oriented_noalloc(const int32_t *d_row_ptr, const int32_t *d_split,
 /* ---- autotuner ------------------------------------------------------------ */
 /* Per graph-shape class, the search settings (donation gate and threshold,
  * bitmap word width of narrow roots, single-block peeling of small
- * frontiers, blocks per SM of the wide engine) that ran fastest in timed
- * trials, kept in a text table with one
+ * frontiers, blocks per SM of the wide engine, X-in-subgraph pivots) that
+ * ran fastest in timed trials, kept in a text table with one
  * line per class.  A class is floor(log2) of the vertex count, mean degree
  * and degeneracy (and of the graph count for a batch), e.g. "n23-a4-k5" or
  * "b12-n23-a4-k7".  No counterpart in the reference (its per-graph variant

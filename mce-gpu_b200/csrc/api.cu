@@ -606,6 +606,7 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   a.policy = policy;
   a.wide8 = o.wide_blocks == 8 ? 1 : 0;
   a.level2 = o.level == MCE_LEVEL_L2 ? 1 : 0;
+  a.x_pivot = (o.x_pivot || o.induced == MCE_INDUCED_PX) ? 1 : 0;
   if (lc) {
     a.list_buf = lc->buf;
     a.list_words = lc->words;
@@ -620,7 +621,7 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   // opts.cuda_graph it is captured once and replayed.
   struct SearchKey {
     int grid[NCLS], block[NCLS];
-    int dcap, xcap, wbits, share, dmin, log, wide8, level2;
+    int dcap, xcap, wbits, share, dmin, log, wide8, level2, xpiv;
     uint32_t dafter;
     const void *slab, *graph_count, *graph_of, *root_nodes, *policy, *q[NCLS], *bufs[4], *wlog;
     int64_t n, G;
@@ -640,6 +641,7 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   key.log = o.log_roots != 0;
   key.wide8 = a.wide8;
   key.level2 = a.level2;
+  key.xpiv = a.x_pivot;
   key.slab = g->slab;
   key.graph_count = a.graph_count;
   key.root_nodes = a.root_nodes;

@@ -45,7 +45,7 @@ namespace {
 // 64-bit engine 4.
 // EV (opts.warp_log): 0 none, 1 per-warp load and donations, 2 plus the
 // per-phase cycle breakdown.
-template <typename Word, int NR, int EV = 0, bool LIST = false>
+template <typename Word, int NR, int EV = 0, bool LIST = false, bool XP = false>
 __global__ void __launch_bounds__(REG_BLOCK, (NR == 1 && sizeof(Word) == 4) ? 6 : (NR == 2 ? 4 : 1))
     bk_reg_kernel(BKArgs a, int cls) {
   __shared__ RegSmem<Word, NR> sm_all[REG_BLOCK / 32];
@@ -73,8 +73,8 @@ __global__ void __launch_bounds__(REG_BLOCK, (NR == 1 && sizeof(Word) == 4) ? 6 
       reg_encode<Word, NR>(a, sm, sl, r, rt);
       MCE_BD(BD_OTHER);
       u64 nd = 0, cnt = 0;
-      reg_tree<Word, NR, false, EV, LIST>(a, sm, sl, rt, WOps<Word>::low(rt.d), (Word)0, (Word)0,
-                                           h0, h1, nd, cnt, bd);
+      reg_tree<Word, NR, false, EV, LIST, XP>(a, sm, sl, rt, WOps<Word>::low(rt.d), (Word)0,
+                                               (Word)0, h0, h1, nd, cnt, bd);
       nodes += nd;
       root_done(a, r, nd, cnt);
     }
@@ -103,7 +103,7 @@ __global__ void __launch_bounds__(REG_BLOCK, (NR == 1 && sizeof(Word) == 4) ? 6 
           MCE_BD(BD_ENCODE);
           if (r != rt.r) reg_encode<Word, NR>(a, sm, sl, r, rt);
           u64 nd = 0, cnt = 0;
-          reg_tree<Word, NR, false, EV, LIST>(a, sm, sl, rt, P, X, S, h0, h1, nd, cnt, bd);
+          reg_tree<Word, NR, false, EV, LIST, XP>(a, sm, sl, rt, P, X, S, h0, h1, nd, cnt, bd);
           nodes += nd;
           root_done(a, r, nd, cnt);
           MCE_BD(BD_QUEUE);
@@ -280,6 +280,17 @@ int bk_launch(int cls, int word_bits, const BKArgs &a, int grid, int block, int 
       bk_mem_kernel<0, 1, true><<<grid, block, smem, s>>>(a, cls);
     else
       return MCE_EINVAL;
+    MCE_CUDA(cudaGetLastError());
+    if (launches) *launches += 1;
+    return MCE_OK;
+  }
+  if (a.x_pivot && ev == 0 && cls != CLS_MEM) {  // -i px: pivots also from earlier neighbours
+    if (cls == CLS_R32 && word_bits == 64)
+      bk_reg_kernel<u64, 1, 0, false, true><<<grid, block, smem, s>>>(a, cls);
+    else if (cls == CLS_R32)
+      bk_reg_kernel<uint32_t, 1, 0, false, true><<<grid, block, smem, s>>>(a, cls);
+    else
+      bk_reg_kernel<u64, 2, 0, false, true><<<grid, block, smem, s>>>(a, cls);
     MCE_CUDA(cudaGetLastError());
     if (launches) *launches += 1;
     return MCE_OK;

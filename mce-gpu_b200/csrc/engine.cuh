@@ -368,6 +368,39 @@ __device__ void reg_encode(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab
   rt.nX = nX;
 }
 
+// Leaf-filter row i: the first 32 in shared memory, the rest in the slab.
+template <typename Word>
+__device__ __forceinline__ Word xrow(const Word *first32, const Word *rest, int i) {
+  return i < 32 ? first32[i] : rest[i];
+}
+
+// X-in-subgraph pivoting (-i px, opts.x_pivot): among the root's earlier
+// neighbours adjacent to the whole chosen set (rows[0 .. cnt) containing
+// `chosen`), the one with the most neighbours in Pn - the reference's
+// select_pivot_from_Xx (mce/mce_utils.cuh:404-472).  Returns the key
+// ((score + 1) << 11 | (2047 - row)) or 0; *elim: one of them is adjacent to
+// all of Pn, so no clique below is maximal.
+template <typename Word>
+__device__ __forceinline__ int outside_pivot(const Word *first32, const Word *rest, int cnt,
+                                             Word chosen, Word Pn, int pcn, bool *elim) {
+  const int lane = (int)lane_id();
+  int k = 0;
+  bool el = false;
+  for (int i0 = 0; i0 < cnt; i0 += 32) {
+    const int i = i0 + lane;
+    if (i < cnt) {
+      const Word row = xrow(first32, rest, i);
+      if ((row & chosen) == chosen) {
+        const int sc = WOps<Word>::popc(Pn & row);
+        el |= sc == pcn;
+        k = max(k, ((sc + 1) << 11) | (2047 - i));
+      }
+    }
+  }
+  *elim = __any_sync(MCE_FULL, el);
+  return (int)__reduce_max_sync(MCE_FULL, (unsigned)k);
+}
+
 // Clique listing (mce_list): each maximal clique becomes the record
 // {size, root, members...} at a position of a.list_buf taken with one
 // atomicAdd; a record past a.list_cap is counted but not written.
@@ -397,7 +430,8 @@ __device__ __forceinline__ void reg_emit(const BKArgs &a, const RegSmem<Word, NR
 // Budget, the walk stops once it has visited a.node_budget nodes; with EV
 // (opts.warp_log) >= 1 the warp's donations are counted in its a.warp_log
 // record, with EV == 2 its cycles are charged to *bd by phase.
-template <typename Word, int NR, bool Budget = false, int EV = 0, bool LIST = false>
+template <typename Word, int NR, bool Budget = false, int EV = 0, bool LIST = false,
+          bool XP = false>
 __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<Word> &sl,
                          const RegRoot<Word> &rt, Word P, Word X, Word S, u64 &h0, u64 &h1,
                          u64 &nodes, u64 &cnt, Bd *bd = nullptr) {
@@ -408,35 +442,6 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
   const Word r0 = rt.r0, r1 = rt.r1;
   const int nX = rt.nX;
   const bool share = a.q.hdr != nullptr;
-  // pivot of the start node (select_pivot_from_P / _and_Xp, mce/mce_utils.cuh:338-402)
-  int start_k = 0;
-  {
-    const Word cand = P | X;
-    const int pc = O::popc(P);
-    int k = 0;
-    bool el = false;
-    if ((cand >> lane) & 1) {
-      const int s = O::popc(P & r0);
-      k = ((s + 1) << 7) | (127 - lane);
-      el = ((X >> lane) & 1) && s == pc;
-    }
-    if constexpr (NR == 2) {
-      if ((cand >> (lane + 32)) & 1) {
-        const int s = O::popc(P & r1);
-        k = max(k, ((s + 1) << 7) | (127 - (lane + 32)));
-        el = el || (((X >> (lane + 32)) & 1) && s == pc);
-      }
-    }
-    if (__any_sync(MCE_FULL, el) || P == 0) {
-      MCE_BD(BD_OTHER);
-      return;
-    }
-    k = (int)__reduce_max_sync(MCE_FULL, (unsigned)k);
-    start_k = k;
-  }
-  MCE_BD(BD_SETS);
-  // apply_pivot_to_first_level (:204-216) / apply_pivot_to_next_level (:218-239)
-  Word B = P & ~row_of<Word, NR>(r0, r1, 127 - (start_k & 127));
   // Leaf filter: for the root it is rebuilt at every depth-0 branch (rows
   // adjacent to that branch vertex); for a task it is built once (rows
   // containing the whole chosen set).
@@ -456,6 +461,50 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
     }
     __syncwarp();
   }
+  // pivot of the start node (select_pivot_from_P / _and_Xp, mce/mce_utils.cuh:338-402)
+  int start_k = 0;
+  Word start_row = 0;
+  bool start_out = false;
+  {
+    const Word cand = P | X;
+    const int pc = O::popc(P);
+    int k = 0;
+    bool el = false;
+    if ((cand >> lane) & 1) {
+      const int s = O::popc(P & r0);
+      k = ((s + 1) << 7) | (127 - lane);
+      el = ((X >> lane) & 1) && s == pc;
+    }
+    if constexpr (NR == 2) {
+      if ((cand >> (lane + 32)) & 1) {
+        const int s = O::popc(P & r1);
+        k = max(k, ((s + 1) << 7) | (127 - (lane + 32)));
+        el = el || (((X >> (lane + 32)) & 1) && s == pc);
+      }
+    }
+    bool elo = false;
+    int ko = 0;
+    if constexpr (XP) {  // the root's rows all contain S = 0; a task's are in the filter
+      if (per_branch && nX > 0)
+        ko = outside_pivot(sl.xr, sl.xr, nX, (Word)0, P, pc, &elo);
+      else if (nL > 0)
+        ko = outside_pivot(sm.xl0, sl.xl, nL, S, P, pc, &elo);
+    }
+    if (__any_sync(MCE_FULL, el) || elo || P == 0) {
+      MCE_BD(BD_OTHER);
+      return;
+    }
+    k = (int)__reduce_max_sync(MCE_FULL, (unsigned)k);
+    start_k = k;
+    if (XP && (ko >> 11) > (k >> 7)) {  // an earlier neighbour covers more of P
+      const int i = 2047 - (ko & 2047);
+      start_row = (per_branch ? sl.xr[i] : xrow(sm.xl0, sl.xl, i));
+      start_out = true;
+    }
+  }
+  MCE_BD(BD_SETS);
+  // apply_pivot_to_first_level (:204-216) / apply_pivot_to_next_level (:218-239)
+  Word B = P & ~(start_out ? start_row : row_of<Word, NR>(r0, r1, 127 - (start_k & 127)));
   int depth = 0, recheck = 0;
   bool want = false;
   for (;;) {
@@ -543,6 +592,14 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
       }
     }
     if (__any_sync(MCE_FULL, el)) continue;
+    int ko = 0;
+    if constexpr (XP) {  // earlier neighbours adjacent to the whole chosen set
+      if (nL > 0) {
+        bool elo;
+        ko = outside_pivot(sm.xl0, sl.xl, nL, Sc, Pc, pc, &elo);
+        if (elo) continue;
+      }
+    }
     // hand the child to an idle warp (try_dequeue / do_fork_L1,
     // mce/mce_utils.cuh:872-880,1063-1113)
     if (share && pc >= a.donate_min &&
@@ -576,7 +633,10 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
     X = Xc;
     S = Sc;
     // apply_pivot_to_next_level (:218-239)
-    B = Pc & ~row_of<Word, NR>(r0, r1, 127 - (k & 127));
+    if (XP && (ko >> 11) > (k >> 7))
+      B = Pc & ~xrow(sm.xl0, sl.xl, 2047 - (ko & 2047));
+    else
+      B = Pc & ~row_of<Word, NR>(r0, r1, 127 - (k & 127));
   }
   MCE_BD(BD_OTHER);
 }

@@ -97,6 +97,7 @@ struct BKArgs {
   int32_t warp_cycles;           // 1: also the per-phase cycle breakdown
   int32_t wide8;                 // 1: the wide engine's 8-blocks-per-SM variant
   int32_t level2;                // 1 (-p l2): first-level subtrees go to idle warps at once
+  int32_t x_pivot;               // 1 (-i px): register engines also pivot on earlier neighbours
   int32_t *list_buf;             // nullable: clique records {size, root, members...}
   unsigned long long *list_words;  // words taken in list_buf (also past list_cap)
   unsigned long long list_cap;   // words list_buf holds

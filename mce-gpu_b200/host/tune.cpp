@@ -6,7 +6,8 @@
 // floor(log2) of its vertex count, mean degree and degeneracy, plus the
 // batch size for batches.  Tuning walks the knobs one at a time (donation
 // gate, donation threshold, bitmap word width of narrow roots, single-block
-// peeling of small frontiers, blocks per SM of the wide engine; subtree
+// peeling of small frontiers, blocks per SM of the wide engine, pivots from
+// the root's earlier neighbours (-i px); subtree
 // sharing itself stays as given, since
 // without it one heavy root can run for minutes), times each value with
 // the device timers of mce_count / mce_batch_count, keeps a value only when
@@ -33,7 +34,8 @@ struct ::mce_graph *batch_union(struct ::mce_batch *b, int32_t *num_graphs);
 namespace {
 
 struct Knobs {
-  int32_t worker_list, donate_after, donate_threshold, bitmap_width, peel_solo_max, wide_blocks;
+  int32_t worker_list, donate_after, donate_threshold, bitmap_width, peel_solo_max, wide_blocks,
+      x_pivot;
 };
 
 // the library's defaults, written out so that a table entry is explicit
@@ -45,6 +47,7 @@ Knobs resolved(const mce_opts_t &o) {
   k.bitmap_width = o.bitmap_width ? o.bitmap_width : 32;
   k.peel_solo_max = o.peel_solo_max > 0 ? o.peel_solo_max : -1;
   k.wide_blocks = o.wide_blocks ? o.wide_blocks : 4;
+  k.x_pivot = o.x_pivot ? 1 : 0;
   return k;
 }
 
@@ -55,6 +58,7 @@ void apply(const Knobs &k, mce_opts_t *o) {
   o->bitmap_width = k.bitmap_width;
   o->peel_solo_max = k.peel_solo_max;
   o->wide_blocks = k.wide_blocks;
+  o->x_pivot = k.x_pivot;
 }
 
 int ilog2(double x) { return x < 1.0 ? 0 : (int)std::floor(std::log2(x)); }
@@ -65,10 +69,11 @@ struct Entry {
 };
 
 const char *kHeader =
-    "# mce autotune table v2: class worker_list donate_after donate_threshold bitmap_width "
-    "peel_solo_max wide_blocks best_ms default_ms";
+    "# mce autotune table v3: class worker_list donate_after donate_threshold bitmap_width "
+    "peel_solo_max wide_blocks x_pivot best_ms default_ms";
 
-// v2 lines have 9 fields; v1 lines (8, no wide_blocks) read as wide_blocks 4
+// v3 lines have 10 fields; v2 lines (9, no x_pivot) read as x_pivot 0 and
+// v1 lines (8, no wide_blocks either) as wide_blocks 4
 bool read_table(const char *path, std::map<std::string, Entry> *t) {
   std::ifstream f(path);
   if (!f) return false;
@@ -81,17 +86,18 @@ bool read_table(const char *path, std::map<std::string, Entry> *t) {
     double x;
     ss >> key;
     while (ss >> x) v.push_back(x);
-    if (v.size() != 7 && v.size() != 8) continue;
-    const bool v2 = v.size() == 8;
+    if (v.size() < 7 || v.size() > 9) continue;
+    const size_t knobs = v.size() - 2;  // 5, 6 or 7
     Entry e;
     e.k.worker_list = (int32_t)v[0];
     e.k.donate_after = (int32_t)v[1];
     e.k.donate_threshold = (int32_t)v[2];
     e.k.bitmap_width = (int32_t)v[3];
     e.k.peel_solo_max = (int32_t)v[4];
-    e.k.wide_blocks = v2 ? (int32_t)v[5] : 4;
-    e.best_ms = v[v2 ? 6 : 5];
-    e.default_ms = v[v2 ? 7 : 6];
+    e.k.wide_blocks = knobs >= 6 ? (int32_t)v[5] : 4;
+    e.k.x_pivot = knobs >= 7 ? (int32_t)v[6] : 0;
+    e.best_ms = v[knobs];
+    e.default_ms = v[knobs + 1];
     (*t)[key] = e;
   }
   return true;
@@ -104,9 +110,9 @@ int write_table(const char *path, const std::map<std::string, Entry> &t) {
   std::fprintf(f, "%s\n", kHeader);
   for (const auto &kv : t) {
     const Entry &e = kv.second;
-    std::fprintf(f, "%s %d %d %d %d %d %d %.4f %.4f\n", kv.first.c_str(), e.k.worker_list,
+    std::fprintf(f, "%s %d %d %d %d %d %d %d %.4f %.4f\n", kv.first.c_str(), e.k.worker_list,
                  e.k.donate_after, e.k.donate_threshold, e.k.bitmap_width, e.k.peel_solo_max,
-                 e.k.wide_blocks, e.best_ms, e.default_ms);
+                 e.k.wide_blocks, e.k.x_pivot, e.best_ms, e.default_ms);
   }
   if (std::fclose(f) != 0 || std::rename(tmp.c_str(), path) != 0) return MCE_EIO;
   return MCE_OK;
@@ -183,6 +189,7 @@ int tune(const char *key, const mce_opts_t &base, const char *table_path, int32_
       {&Knobs::bitmap_width, {32, 64}},
       {&Knobs::peel_solo_max, {-1, 64}},
       {&Knobs::wide_blocks, {4, 8}},
+      {&Knobs::x_pivot, {0, 1}},
   };
   for (const Axis &ax : axes) {
     if (cur.worker_list == MCE_WL_OFF &&

@@ -73,7 +73,7 @@ class _TuneResult(C.Structure):
 
 
 TUNED_FIELDS = ("worker_list", "donate_after", "donate_threshold", "bitmap_width", "peel_solo_max",
-                "wide_blocks")
+                "wide_blocks", "x_pivot")
 
 
 def _tune_dict(r: _TuneResult) -> dict:

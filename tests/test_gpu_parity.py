@@ -273,3 +273,21 @@ def test_level2_offers_first_level_subtrees():
     assert r.total == t and np.array_equal(r.hist, h)
     assert np.array_equal(counts, rc) and np.array_equal(nodes, rn)  # same trees, shared sooner
     assert r.stats["donations"] > 0
+
+
+@pytest.mark.parametrize("maker", [
+    lambda: mce.gen_rmat(12, 16, 0.57, 0.19, 0.19, 7),
+    lambda: mce.gen_ba(40000, 8, 9, 20, 20, 60),
+    lambda: mce.union(mce.gen_chung_lu_batch(32, 64, 4096, 2.3, 8, 32, 5, 5, 40, 13)),
+])
+def test_x_pivot_changes_trees_not_counts(maker):
+    g = maker()
+    t, h, _ = oracle.count(g)
+    _, _, rc, _ = oracle.roots(g)
+    with mce.Graph.from_host(g) as dg:
+        ip = dg.count()
+        px = dg.count(induced=mce.INDUCED_PX, log_roots=True)
+        counts = dg.root_counts()
+    assert px.total == t and np.array_equal(px.hist, h)
+    assert np.array_equal(counts, rc)  # a root's cliques do not depend on its pivots
+    assert px.stats["tree_nodes"] <= ip.stats["tree_nodes"]

@@ -200,8 +200,10 @@ def test_tune_table_lookup(tmp_path):
                  "b12-n23-a4-k7 2 64 16 32 64 100.0 110.0\n")
     assert mce.tune_lookup(str(t), "n10-a3-k4") == dict(
         worker_list=1, donate_after=1024, donate_threshold=6, bitmap_width=64, peel_solo_max=-1,
-        wide_blocks=4)  # a v1 line: no wide_blocks column
+        wide_blocks=4, x_pivot=0)  # a v1 line: no wide_blocks or x_pivot column
     assert mce.tune_lookup(str(t), "b12-n23-a4-k7")["peel_solo_max"] == 64
     assert mce.tune_lookup(str(t), "n11-a3-k4") is None
     t.write_text("# mce autotune table v2\nn14-a4-k6 2 1024 10 32 -1 8 900.0 1100.0\n")
     assert mce.tune_lookup(str(t), "n14-a4-k6")["wide_blocks"] == 8
+    t.write_text("# mce autotune table v3\nn14-a4-k6 2 1024 10 32 -1 8 1 800.0 1100.0\n")
+    assert mce.tune_lookup(str(t), "n14-a4-k6")["x_pivot"] == 1
