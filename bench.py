@@ -341,10 +341,12 @@ def run_mine(args, rank, world, local_rank):
     phases = {"search": count_ms, "peel": peel_ms, "orient": orient_ms}
     dom = max(phases, key=phases.get)
     achieved = ab[dom] / (phases[dom] / 1e3) / 1e9
-    traffic = None
+    traffic, inst = None, None
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
-            traffic = json.load(f).get(f"{args.workload}:{dom}")
+            tj = json.load(f)
+        traffic = tj.get(f"{args.workload}:{dom}")
+        inst = tj.get(f"{args.workload}:search_inst")
     except Exception:
         pass
     line = {
@@ -379,6 +381,17 @@ def run_mine(args, rank, world, local_rank):
                      "algorithmic_bytes": ab[dom], "peak_source": peak_kind},
         "clocks": clocks,
     }
+    if inst and clocks.get("sm_mhz"):
+        # the search is issue-bound, not HBM-bound: its warp-instructions per
+        # call (ncu, profiles/) over its event time, against 4 issue slots per
+        # SM per cycle at the sampled clock
+        sms = torch.cuda.get_device_properties(local_rank).multi_processor_count
+        peak = 4 * sms * clocks["sm_mhz"] * 1e6 / 1e9
+        ach = inst / (count_ms / 1e3) / 1e9
+        line["roofline_issue"] = {"bound": "issue", "kernel": "search", "achieved": ach,
+                                  "peak": peak, "unit": "G warp-instructions/s",
+                                  "frac": ach / peak, "instructions": inst,
+                                  "peak_source": "4 x SMs x sampled SM clock"}
     if not args.no_compare:  # the other root orders on the same resident graph
         cmp = {}
         for name, extra in scheds.items():
