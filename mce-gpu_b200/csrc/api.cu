@@ -67,6 +67,8 @@ struct mce_graph {
   unsigned long long *wlog = nullptr;     // per-warp {SM, nodes, donations} (opts.warp_log)
   int64_t wlog_cap = 0, wlog_count = 0;
   float *feat = nullptr, *pred = nullptr;  // per-vertex features (n x 8) and predicted cost
+  int32_t *cand = nullptr;                // the roots the model scores ...
+  uint32_t *cand_n = nullptr;             // ... and their number (device)
   uint8_t *policy = nullptr;              // per-root sharing policy from the model
   unsigned long long *slab = nullptr;
   size_t slab_bytes = 0;
@@ -98,7 +100,8 @@ void free_graph_bufs(mce_graph *g) {
   dfree(g->hb0); dfree(g->hb1); dfree(g->hb2);
   dfree(g->keys_in); dfree(g->keys_out); dfree(g->vals_in); dfree(g->roots);
   dfree(g->root_nodes); dfree(g->root_count);
-  dfree(g->feat); dfree(g->pred); dfree(g->policy); dfree(g->wlog);
+  dfree(g->feat); dfree(g->pred); dfree(g->policy); dfree(g->wlog); dfree(g->cand);
+  dfree(g->cand_n);
   g->cap_n = g->cap_m = -1;
 }
 
@@ -486,14 +489,29 @@ int ensure_feat(mce_graph *g) {
   if (!g->feat && (rc = dalloc(&g->feat, (size_t)(g->cap_n + 1) * MLP_IN))) return rc;
   if (!g->pred && (rc = dalloc(&g->pred, (size_t)g->cap_n + 1))) return rc;
   if (!g->policy && (rc = dalloc(&g->policy, (size_t)g->cap_n + 1))) return rc;
+  if (!g->cand && (rc = dalloc(&g->cand, (size_t)g->cap_n + 1))) return rc;
+  if (!g->cand_n && (rc = dalloc(&g->cand_n, 1))) return rc;
   return MCE_OK;
 }
 
-// Features of every vertex of the (peeled, oriented) graph into g->feat.
-int compute_features(mce_graph *g, cudaStream_t s, int *launches) {
+// Features of the candidate roots (at least MLP_MIN_LATER later neighbours)
+// of the peeled, oriented graph into g->feat, their list into g->cand; with
+// zero_rest the other rows are zeroed too (mce_root_features returns them).
+int compute_features(mce_graph *g, cudaStream_t s, int *launches, bool zero_rest) {
   int rc = ensure_feat(g);
   if (rc) return rc;
-  return features_launch(g->n, g->rp, g->split, g->cs, g->core, g->feat, g->sms, s, launches);
+  if (zero_rest && g->n)
+    MCE_CUDA(cudaMemsetAsync(g->feat, 0, sizeof(float) * MLP_IN * (size_t)g->n, s));
+  return features_launch(g->n, g->rp, g->split, g->cs, g->core, g->feat, g->cand, g->cand_n,
+                         g->sms, s, launches);
+}
+
+// Predicted cost of every vertex into g->pred: the model on the candidate
+// roots, 0 (light) elsewhere.
+int predict_candidates(mce_graph *g, const void *wh, cudaStream_t s, int *launches) {
+  if (g->n == 0) return MCE_OK;
+  MCE_CUDA(cudaMemsetAsync(g->pred, 0, sizeof(float) * (size_t)g->n, s));
+  return mlp_forward_launch(wh, g->feat, g->cand, g->cand_n, g->n, g->pred, g->sms, s, launches);
 }
 
 // The counting pipeline shared by mce_count and mce_batch_count.  With a
@@ -533,9 +551,8 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
       return rc;
   } else if (sched == MCE_SCHED_LEARNED && g->n > 0) {
     if (model->device != g->device) return MCE_EINVAL;
-    if ((rc = compute_features(g, s, &launches)) ||
-        (rc = mlp_forward_launch(model->wh, g->feat, nullptr, g->n, g->pred, g->sms, s,
-                                 &launches)) ||
+    if ((rc = compute_features(g, s, &launches, false)) ||
+        (rc = predict_candidates(g, model->wh, s, &launches)) ||
         (rc = rekey_launch(g->n, g->keys_in, g->pred, g->rp, g->split, g->policy, heavy, share_cost,
                            g->sms, s, &launches)) ||
         (rc = run_sort(g, 32, s, &launches)))
@@ -1151,7 +1168,7 @@ int mce_root_features(mce_graph_t g, float *features_out) {
   cudaStream_t s = g->own;
   int launches = 0, rc;
   if ((rc = run_peel(g, s, &launches)) || (rc = run_orient(g, s, &launches)) ||
-      (rc = compute_features(g, s, &launches)))
+      (rc = compute_features(g, s, &launches, true)))
     return rc;
   if (features_out && g->n)
     MCE_CUDA(cudaMemcpyAsync(features_out, g->feat, sizeof(float) * MLP_IN * (size_t)g->n,
@@ -1228,8 +1245,7 @@ int mce_model_predict(mce_model_t m, mce_graph_t g, float *pred_out) {
   int rc = mce_root_features(g, nullptr);
   if (rc) return rc;
   cudaStream_t s = g->own;
-  if ((rc = mlp_forward_launch(m->wh, g->feat, nullptr, g->n, g->pred, g->sms, s, nullptr)))
-    return rc;
+  if ((rc = predict_candidates(g, m->wh, s, nullptr))) return rc;
   if (pred_out && g->n)
     MCE_CUDA(cudaMemcpyAsync(pred_out, g->pred, sizeof(float) * (size_t)g->n,
                              cudaMemcpyDeviceToHost, s));
@@ -1251,7 +1267,7 @@ int mce_model_eval(mce_model_t m, const float *X, int64_t count, float *out) {
   if (cudaMemcpyAsync(dx, X, sizeof(float) * MLP_IN * (size_t)count, cudaMemcpyHostToDevice, s) !=
       cudaSuccess)
     rc = MCE_ECUDA;
-  if (!rc) rc = mlp_forward_launch(m->wh, dx, nullptr, count, dout, m->sms, s, nullptr);
+  if (!rc) rc = mlp_forward_launch(m->wh, dx, nullptr, nullptr, count, dout, m->sms, s, nullptr);
   if (!rc && (cudaMemcpyAsync(out, dout, sizeof(float) * (size_t)count, cudaMemcpyDeviceToHost,
                               s) != cudaSuccess ||
               cudaStreamSynchronize(s) != cudaSuccess))

@@ -115,9 +115,10 @@ constexpr int MLP_MIN_LATER = 16;  // roots the model sees: at least this many l
 constexpr int MLP_PARAMS = MLP_HIDDEN * MLP_IN + MLP_HIDDEN + MLP_HIDDEN * MLP_HIDDEN + MLP_HIDDEN +
                            MLP_HIDDEN + 1;
 int features_launch(int64_t n, const int32_t *rp, const int32_t *split, const int32_t *cs,
-                    const int32_t *core, float *out, int sms, cudaStream_t s, int *launches);
-int mlp_forward_launch(const void *wh, const float *X, const int32_t *idx, int64_t count,
-                       float *out, int sms, cudaStream_t s, int *launches);
+                    const int32_t *core, float *out, int32_t *cand, uint32_t *cand_count, int sms,
+                    cudaStream_t s, int *launches);
+int mlp_forward_launch(const void *wh, const float *X, const int32_t *idx, const uint32_t *idx_count,
+                       int64_t count, float *out, int sms, cudaStream_t s, int *launches);
 int mlp_grad_launch(const void *wh, const float *X, const float *Y, const int32_t *idx,
                     int64_t begin, int64_t end, float *grad, float *loss, cudaStream_t s);
 int mlp_adam_launch(float *master, void *wh, float *grad, float *m1, float *m2, float lr,

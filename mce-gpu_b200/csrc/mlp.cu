@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "engine.cuh"
 #include "kernels.h"
 
 namespace mce {
@@ -46,50 +47,85 @@ constexpr int FEAT_CAP = 64;
 // scheduling: their features stay zero and the model is not run on them.
 constexpr int FEAT_MIN = MLP_MIN_LATER;
 
-__global__ void features_kernel(int64_t n, const int32_t *__restrict__ rp,
-                                const int32_t *__restrict__ split, const int32_t *__restrict__ cs,
-                                const int32_t *__restrict__ core, float *__restrict__ out) {
+// The roots with at least FEAT_MIN later neighbours (warp-aggregated append;
+// their order does not matter).
+__global__ void cand_list_kernel(int64_t n, const int32_t *__restrict__ rp,
+                                 const int32_t *__restrict__ split, int32_t *list,
+                                 uint32_t *count) {
+  const int lane = (int)lane_id();
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v - lane < n; v += stride) {
+    const bool c = v < n && rp[v + 1] - split[v] >= FEAT_MIN;
+    const uint32_t mk = __ballot_sync(MCE_FULL, c);
+    if (!mk) continue;
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(count, (uint32_t)__popc(mk));
+    base = __shfl_sync(MCE_FULL, base, 0);
+    if (c) list[base + __popc(mk & ((1u << lane) - 1u))] = (int32_t)v;
+  }
+}
+
+// Features of the listed roots, one warp each.  The later lists of the
+// first d later neighbours are walked flattened over the lanes, each element
+// tested against a hash of those neighbours' ids.
+__global__ void features_kernel(const int32_t *__restrict__ list, const uint32_t *count,
+                                const int32_t *__restrict__ rp, const int32_t *__restrict__ split,
+                                const int32_t *__restrict__ cs, const int32_t *__restrict__ core,
+                                float *__restrict__ out) {
   __shared__ int32_t s_p[8][FEAT_CAP];
   __shared__ int32_t s_deg[8][FEAT_CAP];
+  __shared__ int32_t s_key[8][2 * FEAT_CAP];
+  __shared__ uint8_t s_idx[8][2 * FEAT_CAP];
+  __shared__ int32_t s_off[8][32], s_beg[8][32], s_own[8][32];
   const int lane = (int)lane_id(), wib = threadIdx.x >> 5;
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t vv = gw; vv < n; vv += nw) {
-    const int32_t v = (int32_t)vv;
+  const int64_t cnt = (int64_t)*count;
+  auto slot = [](int32_t w) { return ((uint32_t)w * 0x9E3779B1u) >> 25; };  // 128 slots
+  for (int64_t t = gw; t < cnt; t += nw) {
+    const int32_t v = list[t];
     const int32_t sb = split[v], dp = rp[v + 1] - sb, dm = sb - rp[v];
     float *o = out + (size_t)v * F;
-    if (dp < FEAT_MIN) {
-      if (lane < F) o[lane] = 0.f;
-      continue;
-    }
     const int d = dp < FEAT_CAP ? dp : FEAT_CAP;
     for (int i = lane; i < FEAT_CAP; i += 32) {
       s_p[wib][i] = i < d ? cs[sb + i] : 0x7FFFFFFF;
       s_deg[wib][i] = 0;
     }
+    for (int i = lane; i < 2 * FEAT_CAP; i += 32) s_key[wib][i] = -1;
+    __syncwarp();
+    for (int i = lane; i < d; i += 32) {  // the ids are distinct
+      const int32_t w = s_p[wib][i];
+      uint32_t h = slot(w);
+      while (atomicCAS(&s_key[wib][h], -1, w) != -1) h = (h + 1) & (2 * FEAT_CAP - 1);
+      s_idx[wib][h] = (uint8_t)i;
+    }
     __syncwarp();
     // induced edges among the first d later neighbours; later-list mass
     long long mass = 0;
     int edges = 0;
-    for (int j = lane; j < d; j += 32) {
-      const int32_t u = s_p[wib][j];
-      const int32_t ub = split[u], ue = rp[u + 1];
-      mass += ue - ub;
-      for (int32_t k = ub; k < ue; ++k) {
-        const int32_t w = cs[k];
-        int lo = 0, len = FEAT_CAP;  // lower bound in the padded list
-        while (len > 0) {
-          const int half = len >> 1;
-          const bool right = s_p[wib][lo + half] < w;
-          lo = right ? lo + half + 1 : lo;
-          len = right ? len - half - 1 : half;
-        }
-        if (lo < d && s_p[wib][lo] == w) {
-          ++edges;
-          atomicAdd(&s_deg[wib][j], 1);
-          atomicAdd(&s_deg[wib][lo], 1);
-        }
+    for (int c = 0; c * 32 < d; ++c) {
+      const int items = min(32, d - c * 32);
+      int ub = 0, ulen = 0;
+      if (lane < items) {
+        const int32_t u = s_p[wib][c * 32 + lane];
+        ub = split[u];
+        ulen = rp[u + 1] - ub;
       }
+      mass += ulen;
+      flat_walk(cs, ub, ulen, s_off[wib], s_beg[wib], s_own[wib], [&](int tt, int32_t w) {
+        uint32_t h = slot(w);
+        for (;;) {
+          const int32_t k = s_key[wib][h];
+          if (k == w) {
+            ++edges;
+            atomicAdd(&s_deg[wib][c * 32 + tt], 1);
+            atomicAdd(&s_deg[wib][s_idx[wib][h]], 1);
+            break;
+          }
+          if (k == -1) break;
+          h = (h + 1) & (2 * FEAT_CAP - 1);
+        }
+      });
     }
     __syncwarp();
     edges = __reduce_add_sync(MCE_FULL, edges);
@@ -135,19 +171,22 @@ __device__ __forceinline__ float mlp_eval(const float *w, const float *x) {
   return out;
 }
 
+// idx null: out[t] for rows t < count of X; else out[idx[t]] for t < *idx_count
+// (the candidate list), the other entries of out untouched.
 __global__ void mlp_forward_kernel(const __half *__restrict__ wh, const float *__restrict__ X,
-                                   const int32_t *__restrict__ idx, int64_t count,
-                                   float *__restrict__ out) {
+                                   const int32_t *__restrict__ idx, const uint32_t *idx_count,
+                                   int64_t count, float *__restrict__ out) {
   __shared__ float w[NPARAM];
   for (int i = threadIdx.x; i < NPARAM; i += blockDim.x) w[i] = __half2float(wh[i]);
   __syncthreads();
+  if (idx) count = (int64_t)*idx_count;
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < count;
        t += (int64_t)gridDim.x * blockDim.x) {
     const int64_t s = idx ? idx[t] : t;
     float x[F];
 #pragma unroll
     for (int i = 0; i < F; ++i) x[i] = X[(size_t)s * F + i];
-    out[t] = x[0] > 0.f ? mlp_eval(w, x) : 0.f;  // all-zero features: not a candidate
+    out[s] = x[0] > 0.f ? mlp_eval(w, x) : 0.f;  // all-zero features: not a candidate
   }
 }
 
@@ -294,20 +333,25 @@ __global__ void rekey_kernel(int64_t n, uint32_t *keys, const float *__restrict_
 }  // namespace
 
 int features_launch(int64_t n, const int32_t *rp, const int32_t *split, const int32_t *cs,
-                    const int32_t *core, float *out, int sms, cudaStream_t s, int *launches) {
+                    const int32_t *core, float *out, int32_t *cand, uint32_t *cand_count, int sms,
+                    cudaStream_t s, int *launches) {
   if (n == 0) return MCE_OK;
-  features_kernel<<<sms * 8, 256, 0, s>>>(n, rp, split, cs, core, out);
+  MCE_CUDA(cudaMemsetAsync(cand_count, 0, sizeof(uint32_t), s));
+  cand_list_kernel<<<sms * 8, 256, 0, s>>>(n, rp, split, cand, cand_count);
   MCE_CUDA(cudaGetLastError());
-  if (launches) *launches += 1;
+  features_kernel<<<sms * 8, 256, 0, s>>>(cand, cand_count, rp, split, cs, core, out);
+  MCE_CUDA(cudaGetLastError());
+  if (launches) *launches += 2;
   return MCE_OK;
 }
 
-int mlp_forward_launch(const void *wh, const float *X, const int32_t *idx, int64_t count,
-                       float *out, int sms, cudaStream_t s, int *launches) {
+int mlp_forward_launch(const void *wh, const float *X, const int32_t *idx, const uint32_t *idx_count,
+                       int64_t count, float *out, int sms, cudaStream_t s, int *launches) {
   if (count == 0) return MCE_OK;
   int64_t blocks = (count + 127) / 128;
   if (blocks > (int64_t)sms * 16) blocks = (int64_t)sms * 16;
-  mlp_forward_kernel<<<(unsigned)blocks, 128, 0, s>>>((const __half *)wh, X, idx, count, out);
+  mlp_forward_kernel<<<(unsigned)blocks, 128, 0, s>>>((const __half *)wh, X, idx, idx_count, count,
+                                                       out);
   MCE_CUDA(cudaGetLastError());
   if (launches) *launches += 1;
   return MCE_OK;

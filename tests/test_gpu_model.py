@@ -113,3 +113,39 @@ def test_schedules_change_order_never_results(maker):
     for t, h, c, n in runs[1:]:
         assert t == t0 and np.array_equal(h, h0)
         assert np.array_equal(c, c0) and np.array_equal(n, n0)
+
+
+def test_root_features_match_restatement():
+    g = mce.gen_ba(20000, 12, 5, 20, 20, 60)
+    with mce.Graph.from_host(g) as dg:
+        feat = mce.root_features(dg)
+    split, cs = oracle.prepare(g)
+    _, core, _ = oracle.peel(g)
+    rp = g.row_ptr[:g.n + 1].astype(np.int64)
+    lg = lambda x: np.log2(1.0 + np.float64(x))
+    checked = 0
+    for v in range(g.n):
+        dp, dm = rp[v + 1] - split[v], split[v] - rp[v]
+        if dp < 16:
+            assert not feat[v].any()
+            continue
+        d = min(dp, 64)
+        P = cs[split[v]:split[v] + d]
+        idx = {int(w): i for i, w in enumerate(P)}
+        deg = np.zeros(d, np.int64)
+        edges, mass = 0, 0
+        for j, u in enumerate(P):
+            later = cs[split[u]:rp[u + 1]]
+            mass += len(later)
+            for w in later:
+                i = idx.get(int(w))
+                if i is not None:
+                    edges += 1
+                    deg[j] += 1
+                    deg[i] += 1
+        mx = int(deg.max())
+        want = [lg(dp), lg(dm), lg(core[v]), lg(rp[v + 1] - rp[v]), edges / (0.5 * d * (d - 1)),
+                lg(d - mx), lg(mass), lg(mx)]
+        np.testing.assert_allclose(feat[v], want, rtol=1e-5, atol=1e-6)
+        checked += 1
+    assert checked > 100
