@@ -78,8 +78,6 @@ def parse_args():
                         "shape class is missing), re-tuned, or the library defaults")
     p.add_argument("--tune-table", default=os.path.join(ROOT, "mce-gpu_b200", "data",
                                                         "tune_table.txt"))
-    p.add_argument("--pipe-parts", type=int, default=6,
-                   help="batch e2e: parts whose uploads overlap the counts (1: one upload)")
     p.add_argument("--no-plain", action="store_true",
                    help="skip the per-graph plain-path comparison (batch workload)")
     return p.parse_args()
@@ -324,33 +322,8 @@ def run_mine(args, rank, world, local_rank):
         e2e_times.append(e0.elapsed_time(e1))
     barrier()
     e2e_ms = sum(e2e_times) / len(e2e_times)
-    e2e_single_ms, e2e_path = e2e_ms, "mce_batch_reload + mce_batch_count" if hb is not None \
-        else "mce_graph_reload + mce_count"
-    if hb is not None and args.pipe_parts > 1:
-        # the batch from pinned host memory in parts: each part's upload overlaps
-        # the previous part's count (mce_pipe_count returns with the counts)
-        kp = {k: v for k, v in kw.items() if k not in ("cuda_graph",)}
-        with mce.Pipe(device=local_rank, parts=args.pipe_parts) as pipe:
-            for _ in range(2):  # first calls allocate the two device batches
-                pipe.count_ptr(rp_h.data_ptr(), col_h.data_ptr(), vo_h.data_ptr(),
-                               ao_h.data_ptr(), hb.num_graphs, **kp)
-            pipe_times = []
-            barrier()
-            for _ in range(args.steps):
-                flush.zero_()
-                torch.cuda.synchronize()
-                e0 = torch.cuda.Event(enable_timing=True)
-                e1 = torch.cuda.Event(enable_timing=True)
-                e0.record(stream)  # the call is synchronous: e1 follows all its work
-                r = pipe.count_ptr(rp_h.data_ptr(), col_h.data_ptr(), vo_h.data_ptr(),
-                                   ao_h.data_ptr(), hb.num_graphs, **kp)
-                e1.record(stream)
-                e1.synchronize()
-                assert r.total == total, "pipelined count differs"
-                pipe_times.append(e0.elapsed_time(e1))
-            barrier()
-        e2e_ms = sum(pipe_times) / len(pipe_times)
-        e2e_path = f"mce_pipe_count ({args.pipe_parts} parts, upload of a part overlaps the previous count)"
+    e2e_path = ("mce_batch_reload + mce_batch_count" if hb is not None
+                else "mce_graph_reload + mce_count")
 
     # max over ranks
     if world > 1:
@@ -402,8 +375,7 @@ def run_mine(args, rank, world, local_rank):
         "e2e": {"value": world * total / (e2e_ms / 1e3), "unit": "maximal cliques/s",
                 "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h + 8 * 4096 + 64 + 8 + 4 + 128),
-                "ms_per_step": e2e_ms, "path": e2e_path,
-                "single_upload_ms_per_step": e2e_single_ms},
+                "ms_per_step": e2e_ms, "path": e2e_path},
         "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved,
                      "peak": peaks["hbm_gbs"], "unit": "GB/s",

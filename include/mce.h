@@ -302,19 +302,6 @@ int mce_batch_count(mce_batch_t b, const mce_opts_t *opts, uint64_t *per_graph_t
 
 int mce_batch_free(mce_batch_t b);
 
-/* A batch in host memory (preferably pinned), counted in `parts` runs of
- * consecutive graphs of about equal arcs through two device batches that
- * alternate, each on its own stream: the host-to-device copy of one part
- * overlaps the count of the previous one.  Results as mce_batch_count
- * (hist nullable).  The handle keeps the two device batches between calls;
- * the host arrays must stay unchanged until the call returns.             */
-typedef struct mce_pipe *mce_pipe_t;
-int mce_pipe_create(int32_t device, int32_t parts, mce_pipe_t *out);
-int mce_pipe_count(mce_pipe_t p, const int32_t *row_ptr, const int32_t *col,
-                   const int64_t *vtx_offsets, const int64_t *arc_offsets, int32_t num_graphs,
-                   const mce_opts_t *opts, uint64_t *per_graph_total, uint64_t *total,
-                   uint64_t *hist);
-int mce_pipe_free(mce_pipe_t p);
 
 /* ---- learned scheduling ------------------------------------------------------ */
 /* A cost model predicts each root's search-tree size (log2(1 + nodes)) from

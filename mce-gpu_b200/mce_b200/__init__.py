@@ -134,9 +134,6 @@ _sigs = {
     "mce_batch_reload": (C.c_int, [_P, _P, _P, _P, _P, C.c_int32, _P]),
     "mce_batch_count": (C.c_int, [_P, _P, _P, _P, _P, _P]),
     "mce_batch_free": (C.c_int, [_P]),
-    "mce_pipe_create": (C.c_int, [C.c_int32, C.c_int32, _P]),
-    "mce_pipe_count": (C.c_int, [_P, _P, _P, _P, _P, C.c_int32, _P, _P, _P, _P]),
-    "mce_pipe_free": (C.c_int, [_P]),
     "mce_model_create": (C.c_int, [C.c_int32, C.c_uint64, _P]),
     "mce_model_free": (C.c_int, [_P]),
     "mce_model_set": (C.c_int, [_P, _P]),
@@ -743,46 +740,3 @@ def tune_lookup(table: str, key: str) -> dict | None:
     _check(rc, "tune_lookup")
     return _opts_kwargs(o)
 
-
-class Pipe:
-    """Counts batches held in host memory, overlapping each part's upload with
-    the previous part's count (wraps mce_pipe_t)."""
-
-    def __init__(self, device: int = 0, parts: int = 4):
-        self._h = C.c_void_p()
-        _check(_lib.mce_pipe_create(device, parts, C.byref(self._h)), "pipe_create")
-
-    def count_ptr(self, rp_addr, col_addr, vo_addr, ao_addr, num_graphs, cuda_graph=1,
-                  **opts) -> BatchResult:
-        """Raw host addresses (e.g. pinned torch tensors); no copy in Python."""
-        o = make_opts(cuda_graph=cuda_graph, **opts)
-        per = np.zeros(num_graphs, np.uint64)
-        total = C.c_uint64()
-        hist = np.zeros(HIST_MAX, np.uint64)
-        _check(_lib.mce_pipe_count(self._h, C.c_void_p(rp_addr), C.c_void_p(col_addr),
-                                   C.c_void_p(vo_addr), C.c_void_p(ao_addr), num_graphs,
-                                   C.byref(o), _ptr(per), C.byref(total), _ptr(hist)),
-               "pipe_count")
-        return BatchResult(int(total.value), per, hist, {})
-
-    def count(self, hg: HostGraph, **opts) -> BatchResult:
-        rp, col, vo, ao = Batch._arrays(hg)
-        return self.count_ptr(rp.ctypes.data, col.ctypes.data, vo.ctypes.data, ao.ctypes.data,
-                              hg.num_graphs, **opts)
-
-    def close(self) -> None:
-        if self._h:
-            _lib.mce_pipe_free(self._h)
-            self._h = C.c_void_p()
-
-    def __del__(self):
-        try:
-            self.close()
-        except Exception:
-            pass
-
-    def __enter__(self):
-        return self
-
-    def __exit__(self, *a):
-        self.close()

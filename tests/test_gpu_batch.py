@@ -59,17 +59,3 @@ def test_batch_with_empty_and_tiny_graphs():
         r = db.count()
     assert list(r.per_graph) == [0, 1, oracle.count(graphs[2])[0]]
 
-
-@pytest.mark.parametrize("parts", [1, 3, 7])
-def test_pipe_counts_host_batches_in_parts(parts):
-    b = mce.gen_chung_lu_batch(40, 64, 2048, 2.3, 8, 32, 5, 5, 40, 5)
-    want = per_graph_oracle(b)
-    _, h_union, _ = oracle.count(mce.union(b))
-    with mce.Pipe(parts=parts) as p:
-        r1 = p.count(b)
-        r2 = p.count(b)  # the device batches are reused
-        b2 = mce.gen_chung_lu_batch(9, 64, 1024, 2.3, 8, 32, 5, 5, 40, 6)
-        r3 = p.count(b2)
-    assert np.array_equal(r1.per_graph, want) and np.array_equal(r2.per_graph, want)
-    assert r1.total == int(want.sum()) and np.array_equal(r1.hist, h_union)
-    assert np.array_equal(r3.per_graph, per_graph_oracle(b2))
