@@ -288,6 +288,45 @@ __device__ void reg_encode(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab
 
   p_hash_build(sm, d);
 
+  if (d + u <= 32) {
+    // Small root: one flattened walk over the later lists of the P vertices
+    // (lanes [0, d)) and of the earlier neighbours (lanes [d, d + u)).
+    int b = 0, len = 0;
+    if (lane < d + u) {
+      const int32_t item = lane < d ? sm.pl[lane] : a.cs[ub + lane - d];
+      b = a.split[item];
+      len = a.rp[item + 1] - b;
+    }
+    sm.xs[lane] = 0;
+    __syncwarp();
+    flat_walk(a.cs, b, len, sm.off, sm.beg, sm.own, [&](int t, int32_t w) {
+      const int i = p_find(sm, w);
+      if (i >= 0) {
+        if (t < d) {
+          atomicOr(&sm.rows[t], O::bit(i));
+          atomicOr(&sm.rows[i], O::bit(t));
+        } else {
+          atomicOr(&sm.xs[t - d], O::bit(i));
+        }
+      }
+    });
+    __syncwarp();
+    rt.r0 = sm.rows[lane];
+    rt.r1 = 0;
+    if constexpr (NR == 2) rt.r1 = sm.rows[lane + 32];
+    // the distinct non-empty earlier-neighbour rows, in lane order
+    const Word row = lane < u ? sm.xs[lane] : (Word)0;
+    const uint32_t same = __match_any_sync(MCE_FULL, row);
+    const bool fresh = lane < u && row != 0 && (same & lt) == 0;
+    const uint32_t mk = __ballot_sync(MCE_FULL, fresh);
+    if (fresh) sl.xr[__popc(mk & lt)] = row;
+    __syncwarp();
+    rt.r = r;
+    rt.d = d;
+    rt.nX = __popc(mk);
+    return;
+  }
+
   // warp_sorted_count_and_encode_full (mce/mce_utils.cuh:90-117): bit (j, i)
   // and (i, j) for every later neighbour w = P[i] of v = P[j].  The later
   // lists of 32 P vertices are flattened over the lanes.
@@ -442,6 +481,38 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
   const Word r0 = rt.r0, r1 = rt.r1;
   const int nX = rt.nX;
   const bool share = a.q.hdr != nullptr;
+  // A root whose later neighbours are pairwise adjacent: Tomita's walk is one
+  // path of d nodes (every pivot leaves exactly itself to branch on) ending
+  // in the clique P, which is maximal unless an earlier neighbour of the
+  // root is adjacent to all of it.  Same nodes and count, no walk.
+  if constexpr (!XP) {
+    const int d = rt.d;
+    if (S == 0 && X == 0 && P == O::low(d) && d > 0) {
+      bool full = lane >= d || ((r0 | O::bit(lane)) & P) == P;
+      if constexpr (NR == 2) full = full && (lane + 32 >= d || ((r1 | O::bit(lane + 32)) & P) == P);
+      if (__all_sync(MCE_FULL, full)) {
+        bool covered = false;
+        for (int i0 = 0; !covered && i0 < nX; i0 += 32) {
+          const int i = i0 + lane;
+          covered = __any_sync(MCE_FULL, i < nX && (sl.xr[i] & P) == P);
+        }
+        nodes += (u64)d;
+        if (!covered) {
+          ++cnt;
+          if constexpr (LIST) reg_emit<Word, NR>(a, sm, rt.r, P);
+          const int bin = d - 1;  // clique size - 2
+          if (lane == (bin & 31)) {
+            if (bin < 32)
+              ++h0;
+            else
+              ++h1;
+          }
+        }
+        MCE_BD(BD_OTHER);
+        return;
+      }
+    }
+  }
   // Leaf filter: for the root it is rebuilt at every depth-0 branch (rows
   // adjacent to that branch vertex); for a task it is built once (rows
   // containing the whole chosen set).
