@@ -79,9 +79,6 @@ struct mce_graph {
   ShapeInfo shape_h{};
   int32_t degeneracy = 0;
   cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
-  // the wide and 64-bit engines run beside the 32-bit one on these streams
-  cudaStream_t side[2] = {nullptr, nullptr};
-  cudaEvent_t fork = nullptr, join[2] = {nullptr, nullptr};
   // search launches captured as a CUDA graph, replayed while the key matches
   cudaGraphExec_t search_exec = nullptr;
   unsigned char search_key[256] = {0};
@@ -134,9 +131,6 @@ int alloc_fixed_bufs(mce_graph *g) {
       (rc = dalloc(&g->hist, MCE_HIST_MAX)) || (rc = dalloc(&g->nodes, 4)))
     return rc;
   for (auto &e : g->ev) MCE_CUDA(cudaEventCreate(&e));
-  for (auto &st : g->side) MCE_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-  MCE_CUDA(cudaEventCreateWithFlags(&g->fork, cudaEventDisableTiming));
-  for (auto &e : g->join) MCE_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   return MCE_OK;
 }
 
@@ -421,11 +415,6 @@ int mce_graph_free(mce_graph_t g) {
   if (g->search_exec) cudaGraphExecDestroy(g->search_exec);
   for (auto &e : g->ev)
     if (e) cudaEventDestroy(e);
-  for (auto &st : g->side)
-    if (st) cudaStreamDestroy(st);
-  if (g->fork) cudaEventDestroy(g->fork);
-  for (auto &e : g->join)
-    if (e) cudaEventDestroy(e);
   if (g->own) cudaStreamDestroy(g->own);
   delete g;
   return MCE_OK;
@@ -579,7 +568,7 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   int grid[NCLS] = {0}, block[NCLS] = {0}, smem[NCLS] = {0};
   const int dcap = (int)(sh.max_dplus > 0 ? sh.max_dplus : 1);
   const int xcap = (int)(sh.max_dminus_mem > 0 ? sh.max_dminus_mem : 1);
-  size_t slab_need = 0, slab_off[NCLS] = {0};  // the classes run at once: one region each
+  size_t slab_need = 0;
   for (int c = CLS_R32; c <= CLS_MEM; ++c) {
     if (!sh.cls_cnt[c]) continue;
     int warps = 0;
@@ -591,8 +580,8 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
     if (share) want = want > warps ? want : warps;
     if (want < warps) warps = (int)((want + wpb - 1) / wpb) * wpb;
     grid[c] = warps / wpb;
-    slab_off[c] = slab_need / 8;
-    slab_need += (size_t)warps * bk_slab_words(c, dcap, xcap) * 8;
+    const size_t need = (size_t)warps * bk_slab_words(c, dcap, xcap) * 8;
+    if (need > slab_need) slab_need = need;
   }
   if ((rc = ensure_slab(g, slab_need))) return rc;
   if (o.log_roots && !g->root_nodes) {
@@ -698,30 +687,17 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
       MCE_CUDA(cudaMemsetAsync(g->wlog, 0, sizeof(unsigned long long) * WLOG_WORDS * (size_t)wlog_total,
                                s));
     if (lc) MCE_CUDA(cudaMemsetAsync(lc->words, 0, sizeof(unsigned long long), s));
-    // The three engine classes run at once: the wide and 64-bit ones (few,
-    // long roots) on side streams started first, the 32-bit one (many short
-    // roots) on the main stream, so its roots fill the SMs that the other
-    // classes' long tails leave idle.
-    MCE_CUDA(cudaEventRecord(g->fork, s));
+    // widest roots first so the long trees start early
     const int order[3] = {CLS_MEM, CLS_R64, CLS_R32};
-    int nside = 0;
     for (int c : order) {
       if (!grid[c]) continue;
-      cudaStream_t cs = s;
-      if (c != CLS_R32) {
-        cs = g->side[nside];
-        MCE_CUDA(cudaStreamWaitEvent(cs, g->fork, 0));
-      }
-      a.slab = g->slab + slab_off[c];
       a.slab_words = bk_slab_words(c, dcap, xcap);
       a.q = share ? qv[c] : QueueView();
       a.warp_log = o.warp_log ? g->wlog + WLOG_WORDS * wlog_base[c] : nullptr;
       a.warp_cycles = o.warp_log == 2 ? 1 : 0;
-      if (share && (r2 = queue_launch_init(a.q, cs, &launches))) return r2;
-      if ((r2 = bk_launch(c, wbits, a, grid[c], block[c], smem[c], cs, &launches))) return r2;
-      if (c != CLS_R32) MCE_CUDA(cudaEventRecord(g->join[nside++], cs));
+      if (share && (r2 = queue_launch_init(a.q, s, &launches))) return r2;
+      if ((r2 = bk_launch(c, wbits, a, grid[c], block[c], smem[c], s, &launches))) return r2;
     }
-    for (int i = 0; i < nside; ++i) MCE_CUDA(cudaStreamWaitEvent(s, g->join[i], 0));
     return MCE_OK;
   };
   if (o.cuda_graph && !lc) {
