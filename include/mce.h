@@ -187,6 +187,15 @@ int mce_bel_write(const char *path, const mce_hgraph_t *g);
 int mce_convert_to_bel(const char *txt_path, const char *bel_path, int64_t *n_out,
                        int64_t *undirected_edges_out);
 
+/* The same conversion on device `device`: the text is parsed, and the arcs
+ * sorted and deduplicated, on the GPU; the output file and the two numbers
+ * are those of mce_convert_to_bel, byte for byte (lines are read up to
+ * 65,535 bytes by both).  Replaces graph::convert_to_bel
+ * (include/fileop.h:13-79).  `stream` may be NULL (a stream of the call's
+ * own).                                                                    */
+int mce_convert_to_bel_device(const char *txt_path, const char *bel_path, int32_t device,
+                              void *stream, int64_t *n_out, int64_t *undirected_edges_out);
+
 /* ---- device graphs -------------------------------------------------------- */
 typedef struct mce_graph *mce_graph_t;
 
@@ -214,6 +223,14 @@ int mce_graph_free(mce_graph_t g);
  * (include/fileop.h:81-129, include/csrcoo.cuh:41-81, src/main.cu:53-93)
  * for callers that do not need the graph on the host.                      */
 int mce_bel_load(const char *path, int32_t device, void *stream, mce_graph_t *out);
+
+/* Read a text edge list straight into a device handle, without a .bel file:
+ * the graph mce_bel_load builds from mce_convert_to_bel's output
+ * (include/fileop.h:13-79 followed by :81-129 and include/csrcoo.cuh:41-81).
+ * MCE_ELIMIT when a narrowed id is above the int32 CSR's range, MCE_EFORMAT
+ * when two ids narrow to the same vertex (a self-loop the .bel reader
+ * rejects).                                                                */
+int mce_text_load(const char *txt_path, int32_t device, void *stream, mce_graph_t *out);
 
 /* Degeneracy order of the uploaded graph.  Replaces
  * graph::SingleGPU_Kcore::findKcoreIncremental_async (include/kcore.cuh:233-316).

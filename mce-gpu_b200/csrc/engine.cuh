@@ -649,20 +649,53 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
     const Word cand = Pc | Xc;
     const int pc = O::popc(Pc);
     int k = 0;
-    bool el = false;
+    uint32_t vote = 0;  // bit 0: an X' vertex covers P'; bit 1: P' is not a clique
     if ((cand >> lane) & 1) {
       const int s = O::popc(Pc & r0);
       k = ((s + 1) << 7) | (127 - lane);
-      el = ((Xc >> lane) & 1) && s == pc;
+      vote = (((Xc >> lane) & 1) && s == pc) | ((((Pc >> lane) & 1) && s != pc - 1) << 1);
     }
     if constexpr (NR == 2) {
       if ((cand >> (lane + 32)) & 1) {
         const int s = O::popc(Pc & r1);
         k = max(k, ((s + 1) << 7) | (127 - (lane + 32)));
-        el = el || (((Xc >> (lane + 32)) & 1) && s == pc);
+        vote |= (((Xc >> (lane + 32)) & 1) && s == pc) |
+                ((((Pc >> (lane + 32)) & 1) && s != pc - 1) << 1);
       }
     }
-    if (__any_sync(MCE_FULL, el)) continue;
+    vote = __reduce_or_sync(MCE_FULL, vote);
+    if (vote & 1u) continue;
+    if (vote == 0) {
+      // P' is a clique and no X' vertex covers it: below this node the walk
+      // is one path of |P'| nodes (each pivot leaves one vertex to branch
+      // on; X' never covers the shrinking P') ending in S' | P', maximal
+      // unless an earlier neighbour of the root covers it - the condition
+      // under which the outside pivot (XP) ends the walk here instead.
+      const Word Sl = Sc | Pc;
+      bool covered = __any_sync(MCE_FULL, lane < nL && (sm.xl0[lane] & Sl) == Sl);
+      for (int i0 = 32; !covered && i0 < nL; i0 += 32) {
+        const int i = i0 + lane;
+        covered = __any_sync(MCE_FULL, i < nL && (sl.xl[i] & Sl) == Sl);
+      }
+      if (XP && covered) continue;
+      nodes += (u64)pc;
+      if (Budget && a.node_budget && nodes > a.node_budget) {
+        if (lane == 0) atomicOr(a.err, MCE_ERR_BUDGET);
+        break;
+      }
+      if (!covered) {
+        ++cnt;
+        if constexpr (LIST) reg_emit<Word, NR>(a, sm, rt.r, Sl);
+        const int bin = O::popc(Sl) - 1;  // clique size - 2
+        if (lane == (bin & 31)) {
+          if (bin < 32)
+            ++h0;
+          else
+            ++h1;
+        }
+      }
+      continue;
+    }
     int ko = 0;
     if constexpr (XP) {  // earlier neighbours adjacent to the whole chosen set
       if (nL > 0) {
@@ -877,6 +910,61 @@ __device__ void mem_encode(const BKArgs &a, MemSmem &sm, const Slab &sl, int32_t
 }
 
 // Walk the subtree under frame 0 of the slab stack (P, X, S already there).
+// Whether one of the nL filtered earlier-neighbour rows contains the chosen
+// set Cs (Wr words in the slab): the leaf's clique is then not maximal.
+__device__ __forceinline__ bool mem_covered(const Slab &sl, int nL, int Wr, const u64 *Cs) {
+  const int lane = (int)lane_id();
+  for (int i0 = 0; i0 < nL; i0 += 32) {
+    const int i = i0 + lane;
+    bool hit = false;
+    if (i < nL) {
+      const u64 *xrow = sl.xr + (size_t)sl.xl[i] * Wr;
+      hit = true;
+      for (int w = 0; w < Wr && hit; ++w) hit = (xrow[w] & Cs[w]) == Cs[w];
+    }
+    if (__any_sync(MCE_FULL, hit)) return true;
+  }
+  return false;
+}
+
+// A maximal clique: the root and the set bits of Cs; bin = its size - 2.
+template <bool LIST>
+__device__ __forceinline__ void mem_leaf(const BKArgs &a, const Slab &sl, int32_t r, int Wr,
+                                         const u64 *Cs, int bin, u64 &h0, u64 &h1, u64 &cnt) {
+  const int lane = (int)lane_id();
+  ++cnt;
+  if constexpr (LIST) {  // record {size, root, members...}, as reg_emit
+    const int sz = bin + 2;
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(a.list_words, (unsigned long long)(sz + 1));
+    base = __shfl_sync(MCE_FULL, base, 0);
+    if (base + (unsigned long long)sz + 1 <= a.list_cap) {
+      if (lane == 0) {
+        a.list_buf[base] = sz;
+        a.list_buf[base + 1] = r;
+      }
+      u64 word = lane < Wr ? Cs[lane] : 0ull;  // Wr <= 32 words
+      const int c = __popcll(word);
+      unsigned long long pos = base + 2 + (warp_incl_scan(c) - c);
+      while (word) {
+        const int b = __ffsll((long long)word) - 1;
+        word &= word - 1;
+        a.list_buf[pos++] = sl.pl[lane * 64 + b];
+      }
+    }
+  }
+  if (bin < 64) {
+    if (lane == (bin & 31)) {
+      if (bin < 32)
+        ++h0;
+      else
+        ++h1;
+    }
+  } else if (lane == 0 && bin + 2 < MCE_HIST_MAX) {
+    atomicAdd(&a.hist[bin + 2], 1ull);
+  }
+}
+
 template <bool Budget = false, int EV = 0, bool LIST = false>
 __device__ void mem_tree(const BKArgs &a, const Slab &sl, const MemRoot &rt, u64 &h0, u64 &h1,
                          u64 &nodes, u64 &cnt, Bd *bd = nullptr) {
@@ -994,62 +1082,14 @@ __device__ void mem_tree(const BKArgs &a, const Slab &sl, const MemRoot &rt, u64
     __syncwarp();
     if (pc == 0) {
       MCE_BD(BD_MAXIMAL);
-      if (!xnz) {
-        const u64 *Cs = C + 3 * Wr;
-        bool covered = false;
-        for (int i0 = 0; i0 < nL; i0 += 32) {
-          const int i = i0 + lane;
-          bool hit = false;
-          if (i < nL) {
-            const u64 *xrow = sl.xr + (size_t)sl.xl[i] * Wr;
-            hit = true;
-            for (int w = 0; w < Wr && hit; ++w) hit = (xrow[w] & Cs[w]) == Cs[w];
-          }
-          if (__any_sync(MCE_FULL, hit)) {
-            covered = true;
-            break;
-          }
-        }
-        if (!covered) {
-          ++cnt;
-          const int bin = s_base + depth;  // clique size - 2
-          if constexpr (LIST) {  // record {size, root, members...}, as reg_emit
-            const int sz = bin + 2;
-            unsigned long long base = 0;
-            if (lane == 0) base = atomicAdd(a.list_words, (unsigned long long)(sz + 1));
-            base = __shfl_sync(MCE_FULL, base, 0);
-            if (base + (unsigned long long)sz + 1 <= a.list_cap) {
-              if (lane == 0) {
-                a.list_buf[base] = sz;
-                a.list_buf[base + 1] = rt.r;
-              }
-              u64 word = lane < Wr ? Cs[lane] : 0ull;  // Wr <= 32 words
-              const int c = __popcll(word);
-              unsigned long long pos = base + 2 + (warp_incl_scan(c) - c);
-              while (word) {
-                const int b = __ffsll((long long)word) - 1;
-                word &= word - 1;
-                a.list_buf[pos++] = sl.pl[lane * 64 + b];
-              }
-            }
-          }
-          if (bin < 64) {
-            if (lane == (bin & 31)) {
-              if (bin < 32)
-                ++h0;
-              else
-                ++h1;
-            }
-          } else if (lane == 0 && bin + 2 < MCE_HIST_MAX) {
-            atomicAdd(&a.hist[bin + 2], 1ull);
-          }
-        }
-      }
+      const u64 *Cs = C + 3 * Wr;
+      if (!xnz && !mem_covered(sl, nL, Wr, Cs))
+        mem_leaf<LIST>(a, sl, rt.r, Wr, Cs, s_base + depth, h0, h1, cnt);
       continue;
     }
     MCE_BD(BD_PIVOT);
     int k = 0;
-    bool el = false;
+    bool el = false, nc = false;  // nc: a vertex of P' misses another one
     for (int uu = lane; uu < d; uu += 32) {
       const int uw = uu >> 6;
       const u64 ub2 = 1ull << (uu & 63);
@@ -1060,8 +1100,26 @@ __device__ void mem_tree(const BKArgs &a, const Slab &sl, const MemRoot &rt, u64
       for (int w = 0; w < Wr; ++w) s += __popcll(C[w] & ru[w]);
       k = max(k, ((s + 1) << 11) | (2047 - uu));
       el = el || (inX && s == pc);
+      nc = nc || (inP && s != pc - 1);
     }
-    if (__any_sync(MCE_FULL, el)) continue;
+    const uint32_t vote = __reduce_or_sync(MCE_FULL, (el ? 1u : 0u) | (nc ? 2u : 0u));
+    if (vote & 1u) continue;
+    if (vote == 0) {
+      // P' is a clique and no X' vertex covers it: one path of |P'| nodes
+      // below ends in S' | P' (the register engine's shortcut); the union
+      // goes into the child's unused branch words.
+      u64 *Cl = C + 2 * Wr;
+      if (lane < Wr) Cl[lane] = C[3 * Wr + lane] | C[lane];
+      __syncwarp();
+      nodes += (u64)pc;
+      if (Budget && a.node_budget && nodes > a.node_budget) {
+        if (lane == 0) atomicOr(a.err, MCE_ERR_BUDGET);
+        break;
+      }
+      if (!mem_covered(sl, nL, Wr, Cl))
+        mem_leaf<LIST>(a, sl, rt.r, Wr, Cl, s_base + depth + pc, h0, h1, cnt);
+      continue;
+    }
     if (share && pc >= a.donate_min &&
         (nodes >= a.donate_after || (a.policy && a.policy[rt.r]) || (a.level2 && depth == 0)) &&
         (--recheck <= 0 ? (recheck = 32, want = wants_task(a.q)) : want)) {

@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <cctype>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -96,9 +97,10 @@ extern "C" int mce_bel_write(const char *path, const mce_hgraph_t *g) {
   return rc;
 }
 
-// graph::convert_to_bel (include/fileop.h:13-79).  One deviation: an empty
-// line is skipped here; the reference's fscanf("%[^\n]%*c") loop never
-// advances past it.
+// graph::convert_to_bel (include/fileop.h:13-79).  The parse sees the
+// first 65,535 bytes of each line (a NUL byte ends it earlier), the window
+// the device converter uses too.  One deviation: an empty line is skipped
+// here; the reference's fscanf("%[^\n]%*c") loop never advances past it.
 extern "C" int mce_convert_to_bel(const char *txt_path, const char *bel_path, int64_t *n_out,
                                   int64_t *undirected_edges_out) {
   if (!txt_path || !bel_path) return MCE_EINVAL;
@@ -107,34 +109,22 @@ extern "C" int mce_convert_to_bel(const char *txt_path, const char *bel_path, in
   std::vector<std::pair<uint32_t, uint32_t>> edges;
   unsigned long long maxnode = 0;
   bool any = false;
-  std::vector<char> line(1 << 16);
-  while (std::fgets(line.data(), (int)line.size(), fp)) {
-    // a line longer than the buffer continues in the next read; its tail
-    // does not start with a digit in general, exactly one record per line
-    size_t len = std::strlen(line.data());
-    const bool whole = len > 0 && line[len - 1] == '\n';
-    if (!std::isdigit((unsigned char)line[0])) {
-      if (!whole) {  // drain the rest of an over-long non-edge line
-        int ch;
-        while ((ch = std::fgetc(fp)) != EOF && ch != '\n') {
-        }
-      }
-      continue;
-    }
+  char *line = nullptr;
+  size_t cap = 0;
+  ssize_t len;
+  while ((len = getline(&line, &cap, fp)) != -1) {
+    if (len > 65535) line[65535] = '\0';
+    if (!std::isdigit((unsigned char)line[0])) continue;
     unsigned long long s = 0, d = 0;
-    if (std::sscanf(line.data(), "%llu %llu", &s, &d) == 2 && s != d) {
+    if (std::sscanf(line, "%llu %llu", &s, &d) == 2 && s != d) {
       // ids narrowed to 32 bits, as T(src) does in the reference
       edges.push_back({(uint32_t)s, (uint32_t)d});
       edges.push_back({(uint32_t)d, (uint32_t)s});
       maxnode = std::max({maxnode, s, d});
       any = true;
     }
-    if (!whole) {
-      int ch;
-      while ((ch = std::fgetc(fp)) != EOF && ch != '\n') {
-      }
-    }
   }
+  std::free(line);
   std::fclose(fp);
   std::sort(edges.begin(), edges.end());
   edges.erase(std::unique(edges.begin(), edges.end()), edges.end());

@@ -216,8 +216,12 @@ int main(int argc, char **argv) {
   print_config(c);
 
   if (c.task == TASK_CONVERT) {
+    // on the first device when there is one; the host converter (the
+    // reference's own path, include/fileop.h:13-79) writes the same file
     int64_t n = 0, e = 0;
-    int rc = mce_convert_to_bel(c.src.c_str(), c.dst.c_str(), &n, &e);
+    int rc = mce_convert_to_bel_device(c.src.c_str(), c.dst.c_str(), c.gpus.empty() ? 0 : c.gpus[0],
+                                       nullptr, &n, &e);
+    if (rc == MCE_ENODEV) rc = mce_convert_to_bel(c.src.c_str(), c.dst.c_str(), &n, &e);
     if (rc) fail("convert", rc);
     std::printf("n = %lld and m = %lld\n", (long long)n, (long long)e);
     return 0;

@@ -121,6 +121,8 @@ _sigs = {
     "mce_graph_reload": (C.c_int, [_P, _P, _P, C.c_int64, C.c_int64, _P]),
     "mce_graph_free": (C.c_int, [_P]),
     "mce_bel_load": (C.c_int, [C.c_char_p, C.c_int32, _P, _P]),
+    "mce_text_load": (C.c_int, [C.c_char_p, C.c_int32, _P, _P]),
+    "mce_convert_to_bel_device": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int32, _P, _P, _P]),
     "mce_graph_size": (C.c_int, [_P, _P, _P]),
     "mce_degeneracy": (C.c_int, [_P, _P, _P, _P]),
     "mce_split_csr": (C.c_int, [_P, _P, _P]),
@@ -327,11 +329,17 @@ def bel_write(path: str, g: HostGraph) -> None:
     _check(_lib.mce_bel_write(path.encode(), C.byref(s)), f"bel_write({path})")
 
 
-def convert_to_bel(txt: str, bel: str) -> tuple[int, int]:
+def convert_to_bel(txt: str, bel: str, device: int | None = None) -> tuple[int, int]:
+    """Text edge list -> .bel; (n, undirected edges) as the reference prints
+    them.  device=None converts on the host, an index on that GPU."""
     n = C.c_int64()
     e = C.c_int64()
-    _check(_lib.mce_convert_to_bel(txt.encode(), bel.encode(), C.byref(n), C.byref(e)),
-           "convert_to_bel")
+    if device is None:
+        rc = _lib.mce_convert_to_bel(txt.encode(), bel.encode(), C.byref(n), C.byref(e))
+    else:
+        rc = _lib.mce_convert_to_bel_device(txt.encode(), bel.encode(), device, None,
+                                            C.byref(n), C.byref(e))
+    _check(rc, "convert_to_bel")
     return n.value, e.value
 
 
@@ -390,6 +398,19 @@ class Graph:
         self = cls.__new__(cls)
         self._h = C.c_void_p()
         _check(_lib.mce_bel_load(path.encode(), device, stream, C.byref(self._h)), "bel_load")
+        self.row_ptr = self.col = None
+        n, m = C.c_int64(), C.c_int64()
+        _check(_lib.mce_graph_size(self._h, C.byref(n), C.byref(m)), "graph_size")
+        self.n, self.m = n.value, m.value
+        return self
+
+    @classmethod
+    def load_text(cls, path: str, device: int = 0, stream=None) -> "Graph":
+        """A text edge list parsed, sorted and deduplicated on the device
+        (mce_text_load); the graph load_bel builds from its .bel file."""
+        self = cls.__new__(cls)
+        self._h = C.c_void_p()
+        _check(_lib.mce_text_load(path.encode(), device, stream, C.byref(self._h)), "text_load")
         self.row_ptr = self.col = None
         n, m = C.c_int64(), C.c_int64()
         _check(_lib.mce_graph_size(self._h, C.byref(n), C.byref(m)), "graph_size")
