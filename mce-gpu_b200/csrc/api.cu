@@ -57,6 +57,10 @@ struct mce_graph {
   // roots
   uint32_t *keys_in = nullptr, *keys_out = nullptr;
   int32_t *vals_in = nullptr, *roots = nullptr;
+  int32_t *hub_of = nullptr, *hub_list = nullptr;  // roots with many earlier neighbours
+  int64_t *hub_off = nullptr;                      // ... their first precomputed row
+  unsigned long long *hub_rows = nullptr;          // ... and the rows
+  int64_t hub_off_cap = 0, hub_rows_cap = 0;
   ShapeInfo *shape = nullptr;
   void *sort_tmp = nullptr;
   size_t sort_tmp_bytes = 0;
@@ -99,6 +103,8 @@ void free_graph_bufs(mce_graph *g) {
   dfree(g->f0); dfree(g->f1); dfree(g->f2);
   dfree(g->hb0); dfree(g->hb1); dfree(g->hb2);
   dfree(g->keys_in); dfree(g->keys_out); dfree(g->vals_in); dfree(g->roots);
+  dfree(g->hub_of); dfree(g->hub_list); dfree(g->hub_off); dfree(g->hub_rows);
+  g->hub_off_cap = g->hub_rows_cap = 0;
   dfree(g->root_nodes); dfree(g->root_count);
   dfree(g->feat); dfree(g->pred); dfree(g->policy); dfree(g->wlog); dfree(g->cand);
   dfree(g->cand_n);
@@ -115,7 +121,8 @@ int alloc_graph_bufs(mce_graph *g, int64_t n, int64_t m) {
       (rc = dalloc(&g->f0, N)) || (rc = dalloc(&g->f1, N)) || (rc = dalloc(&g->f2, N)) ||
       (rc = dalloc(&g->hb0, N)) || (rc = dalloc(&g->hb1, N)) || (rc = dalloc(&g->hb2, N)) ||
       (rc = dalloc(&g->keys_in, N)) || (rc = dalloc(&g->keys_out, N)) ||
-      (rc = dalloc(&g->vals_in, N)) || (rc = dalloc(&g->roots, N))) {
+      (rc = dalloc(&g->vals_in, N)) || (rc = dalloc(&g->roots, N)) ||
+      (rc = dalloc(&g->hub_of, N)) || (rc = dalloc(&g->hub_list, N))) {
     free_graph_bufs(g);
     return rc;
   }
@@ -217,6 +224,8 @@ int run_orient(mce_graph *g, cudaStream_t s, int *launches, bool skip_sort = fal
   oa.shape = g->shape;
   oa.cost = nullptr;
   oa.sched = MCE_SCHED_PLAIN;
+  oa.hub_of = g->hub_of;
+  oa.hub_list = g->hub_list;
   int rc = orient_launch(oa, s, launches);
   if (rc) return rc;
   return skip_sort ? MCE_OK : run_sort(g, 3, s, launches);  // keys: class only
@@ -563,11 +572,32 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   if ((rc = read_shape(g, s))) return rc;
   const ShapeInfo &sh = g->shape_h;
   if (sh.cls_cnt[CLS_BIG]) return MCE_ELIMIT;
+  // earlier-neighbour rows of the hub roots, built by many warps at once
+  if (sh.hub_cnt > 0) {
+    const int64_t need_off = (int64_t)sh.hub_cnt + 1, need_rows = (int64_t)sh.hub_rows;
+    if (need_off > g->hub_off_cap) {
+      dfree(g->hub_off);
+      g->hub_off_cap = 0;
+      if ((rc = dalloc(&g->hub_off, (size_t)need_off))) return rc;
+      g->hub_off_cap = need_off;
+    }
+    if (need_rows > g->hub_rows_cap) {
+      dfree(g->hub_rows);
+      g->hub_rows_cap = 0;
+      if ((rc = dalloc(&g->hub_rows, (size_t)need_rows))) return rc;
+      g->hub_rows_cap = need_rows;
+    }
+    if ((rc = hub_rows_launch(g->rp, g->split, g->cs, g->hub_list, sh.hub_cnt, need_rows,
+                              g->hub_off, g->hub_rows, g->sms, s, &launches)))
+      return rc;
+  }
   // search scratch
   const bool share = o.worker_list != MCE_WL_OFF;
   int grid[NCLS] = {0}, block[NCLS] = {0}, smem[NCLS] = {0};
   const int dcap = (int)(sh.max_dplus > 0 ? sh.max_dplus : 1);
   const int xcap = (int)(sh.max_dminus_mem > 0 ? sh.max_dminus_mem : 1);
+  int rxcap = REG_XCAP;  // a power of two covering the register classes' earlier degrees
+  while (rxcap < (int)sh.max_dminus_reg && rxcap < REG_XCAP_MAX) rxcap <<= 1;
   size_t slab_need = 0;
   for (int c = CLS_R32; c <= CLS_MEM; ++c) {
     if (!sh.cls_cnt[c]) continue;
@@ -580,7 +610,7 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
     if (share) want = want > warps ? want : warps;
     if (want < warps) warps = (int)((want + wpb - 1) / wpb) * wpb;
     grid[c] = warps / wpb;
-    const size_t need = (size_t)warps * bk_slab_words(c, dcap, xcap) * 8;
+    const size_t need = (size_t)warps * bk_slab_words(c, dcap, xcap, rxcap) * 8;
     if (need > slab_need) slab_need = need;
   }
   if ((rc = ensure_slab(g, slab_need))) return rc;
@@ -617,6 +647,10 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   a.slab = g->slab;
   a.dcap = dcap;
   a.xcap = xcap;
+  a.rxcap = rxcap;
+  a.hub_of = sh.hub_cnt > 0 ? g->hub_of : nullptr;
+  a.hub_off = g->hub_off;
+  a.hub_rows = g->hub_rows;
   a.donate_min = o.donate_threshold > 0 ? o.donate_threshold : DEFAULT_DONATE_MIN;
   a.donate_after = o.donate_after > 0 ? (uint32_t)o.donate_after : DEFAULT_DONATE_AFTER;
   a.wait_limit_ns = IDLE_LIMIT_NS;
@@ -638,9 +672,10 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   // opts.cuda_graph it is captured once and replayed.
   struct SearchKey {
     int grid[NCLS], block[NCLS];
-    int dcap, xcap, wbits, share, dmin, log, wide8, level2, xpiv;
+    int dcap, xcap, rxcap, wbits, share, dmin, log, wide8, level2, xpiv;
     uint32_t dafter;
     const void *slab, *graph_count, *graph_of, *root_nodes, *policy, *q[NCLS], *bufs[4], *wlog;
+    const void *hub[3];
     int64_t n, G;
   } key;
   std::memset(&key, 0, sizeof(key));
@@ -651,6 +686,7 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   }
   key.dcap = dcap;
   key.xcap = xcap;
+  key.rxcap = rxcap;
   key.wbits = wbits;
   key.share = share;
   key.dmin = a.donate_min;
@@ -669,6 +705,9 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   key.bufs[1] = g->split;
   key.bufs[2] = g->cs;
   key.bufs[3] = g->roots;
+  key.hub[0] = a.hub_of;
+  key.hub[1] = a.hub_off;
+  key.hub[2] = a.hub_rows;
   key.n = g->n;
   key.G = bc ? bc->G : 0;
   static_assert(sizeof(SearchKey) <= sizeof(g->search_key), "search key");
@@ -691,7 +730,7 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
     const int order[3] = {CLS_MEM, CLS_R64, CLS_R32};
     for (int c : order) {
       if (!grid[c]) continue;
-      a.slab_words = bk_slab_words(c, dcap, xcap);
+      a.slab_words = bk_slab_words(c, dcap, xcap, rxcap);
       a.q = share ? qv[c] : QueueView();
       a.warp_log = o.warp_log ? g->wlog + WLOG_WORDS * wlog_base[c] : nullptr;
       a.warp_cycles = o.warp_log == 2 ? 1 : 0;

@@ -222,11 +222,145 @@ __global__ void __launch_bounds__(MEM_BLOCK, MINB) bk_mem_kernel(BKArgs a, int c
   }
 }
 
+// ---------------------------------------------------------------------------
+// Hub rows: the earlier-neighbour rows of roots with d- > HUB_XMIN, built
+// before the search by many warps at once (the root's own warp would walk
+// thousands of later lists one window at a time, a chain of dependent
+// loads that leaves the rest of its class idle at the end).
+// ---------------------------------------------------------------------------
+constexpr int HUB_BLOCK = 256;
+
+// off[j] = sum over k < j of hub k's earlier degree rounded up to 32; one
+// block walks the list in tiles of HUB_BLOCK.
+__global__ void __launch_bounds__(HUB_BLOCK) hub_offsets_kernel(
+    const int32_t *__restrict__ rp, const int32_t *__restrict__ split,
+    const int32_t *__restrict__ hub_list, uint32_t cnt, int64_t *__restrict__ off) {
+  __shared__ long long wsum[HUB_BLOCK / 32];
+  __shared__ long long carry;
+  const int lane = (int)lane_id(), wid = (int)(threadIdx.x >> 5);
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (uint32_t base = 0; base < cnt; base += HUB_BLOCK) {
+    const uint32_t j = base + threadIdx.x;
+    long long v = 0;
+    if (j < cnt) {
+      const int32_t r = hub_list[j];
+      v = (long long)(((uint32_t)(split[r] - rp[r]) + 31u) & ~31u);
+    }
+    long long x = v;  // inclusive scan in the warp
+    for (int o = 1; o < 32; o <<= 1) {
+      const long long y = __shfl_up_sync(MCE_FULL, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[wid] = x;
+    __syncthreads();
+    long long before = carry;
+    for (int w = 0; w < wid; ++w) before += wsum[w];
+    if (j < cnt) off[j] = (int64_t)(before + x - v);
+    __syncthreads();
+    if (threadIdx.x == HUB_BLOCK - 1) carry = before + x;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) off[cnt] = (int64_t)carry;
+}
+
+struct HubSmem {
+  int32_t hkey[128];  // hash of the hub's later list: vertex id (-1: empty) ...
+  uint8_t hidx[128];  // ... and its index in the list
+  u64 xs[32];         // the rows of the current 32 earlier neighbours
+  int32_t off[32], beg[32], own[32];  // flat_walk scratch
+};
+
+__device__ __forceinline__ uint32_t hub_slot(int32_t w) { return ((uint32_t)w * 0x9E3779B1u) >> 25; }
+
+// Each warp takes a contiguous range of 32-row chunks; the hash of a hub's
+// later list (d+ <= 64) is rebuilt when the range moves to the next hub.
+__global__ void __launch_bounds__(HUB_BLOCK) hub_rows_kernel(
+    const int32_t *__restrict__ rp, const int32_t *__restrict__ split,
+    const int32_t *__restrict__ cs, const int32_t *__restrict__ hub_list, uint32_t cnt,
+    const int64_t *__restrict__ off, int64_t chunks, unsigned long long *__restrict__ rows) {
+  __shared__ HubSmem sm_all[HUB_BLOCK / 32];
+  HubSmem &sm = sm_all[threadIdx.x >> 5];
+  const int lane = (int)lane_id();
+  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int64_t per = (chunks + nw - 1) / nw;
+  const int64_t c0 = gw * per, c1 = min(chunks, c0 + per);
+  int32_t cur = -1;  // hub whose hash is built
+  uint32_t j = 0;
+  for (int64_t c = c0; c < c1; ++c) {
+    const int64_t row0 = 32 * c;
+    if (cur < 0 || row0 >= off[j + 1]) {  // first chunk, or the next hub: last j with off[j] <= row0
+      uint32_t lo = 0, hi = cnt - 1;
+      while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= row0) lo = mid; else hi = mid - 1;
+      }
+      j = lo;
+      cur = hub_list[j];
+      const int32_t sb = split[cur], d = rp[cur + 1] - sb;
+      for (int i = lane; i < 128; i += 32) sm.hkey[i] = -1;
+      __syncwarp();
+      for (int i = lane; i < d; i += 32) {  // the later list's ids are distinct
+        const int32_t w = cs[sb + i];
+        uint32_t h = hub_slot(w);
+        while (atomicCAS(&sm.hkey[h], -1, w) != -1) h = (h + 1) & 127u;
+        sm.hidx[h] = (uint8_t)i;
+      }
+      __syncwarp();
+    }
+    const int32_t ub = rp[cur], u = split[cur] - ub;
+    const int64_t i0 = row0 - off[j];
+    const int items = (int)min((int64_t)32, (int64_t)u - i0);
+    int xb = 0, xlen = 0;
+    if (lane < items) {
+      const int32_t x = cs[ub + i0 + lane];
+      xb = split[x];
+      xlen = rp[x + 1] - xb;
+    }
+    sm.xs[lane] = 0;
+    __syncwarp();
+    flat_walk(cs, xb, xlen, sm.off, sm.beg, sm.own, [&](int t, int32_t w) {
+      uint32_t h = hub_slot(w);
+      for (;;) {
+        const int32_t k = sm.hkey[h];
+        if (k == w) {
+          atomicOr(&sm.xs[t], 1ull << sm.hidx[h]);
+          break;
+        }
+        if (k == -1) break;
+        h = (h + 1) & 127u;
+      }
+    });
+    __syncwarp();
+    rows[row0 + lane] = sm.xs[lane];  // lanes past the hub's list write its zero padding
+    __syncwarp();
+  }
+}
+
 }  // namespace
 
 
-size_t bk_slab_words(int cls, int dcap, int xcap) {
-  if (cls == CLS_R32 || cls == CLS_R64) return 4 * (size_t)REG_XCAP;  // hash, rows, leaf list
+int hub_rows_launch(const int32_t *rp, const int32_t *split, const int32_t *cs,
+                    const int32_t *hub_list, uint32_t cnt, int64_t total_rows, int64_t *off,
+                    unsigned long long *rows, int sms, cudaStream_t s, int *launches) {
+  if (cnt == 0) return MCE_OK;
+  hub_offsets_kernel<<<1, HUB_BLOCK, 0, s>>>(rp, split, hub_list, cnt, off);
+  MCE_CUDA(cudaGetLastError());
+  const int64_t chunks = total_rows / 32;
+  int64_t blocks = ((chunks + 7) / 8 + 0);  // up to one chunk per warp
+  const int64_t cap = (int64_t)sms * 8;
+  if (blocks > cap) blocks = cap;
+  if (blocks < 1) blocks = 1;
+  hub_rows_kernel<<<(unsigned)blocks, HUB_BLOCK, 0, s>>>(rp, split, cs, hub_list, cnt, off, chunks,
+                                                        rows);
+  MCE_CUDA(cudaGetLastError());
+  if (launches) *launches += 2;
+  return MCE_OK;
+}
+
+size_t bk_slab_words(int cls, int dcap, int xcap, int rxcap) {
+  if (cls == CLS_R32 || cls == CLS_R64) return 4 * (size_t)rxcap;  // hash, rows, leaf list
   const size_t WM = (size_t)(dcap + 63) / 64;
   size_t w = (size_t)dcap * WM + (size_t)(dcap + 1) * 4 * WM + 32 * WM + (size_t)xcap * WM;
   w += (size_t)hash_cap(xcap);                      // hash set (one-word rows)
@@ -465,6 +599,7 @@ extern "C" int mce_count_oriented_noalloc(const int32_t *d_row_ptr, const int32_
   a.slab_words = NOALLOC_SLAB_WORDS;
   a.dcap = 32;
   a.xcap = REG_XCAP;
+  a.rxcap = REG_XCAP;
   bk_reg_kernel<uint32_t, 1><<<(unsigned)blocks, REG_BLOCK, 0, s>>>(a, CLS_R32);
   MCE_CUDA(cudaGetLastError());
   MCE_CUDA(cudaMemcpyAsync(&err, &ctl->err[1], sizeof(err), cudaMemcpyDeviceToHost, s));

@@ -237,21 +237,26 @@ __device__ __forceinline__ int p_find(const RegSmem<Word, NR> &sm, int32_t w) {
   }
 }
 
-// Per-warp slab of the register engine, in Words: a hash set used while the
-// earlier-neighbour rows are built (2 * REG_XCAP), the distinct rows
-// (REG_XCAP) and the rows adjacent to the current branch (REG_XCAP).
+// Per-warp slab of the register engine, in Words, for xc = the x-row
+// capacity (a power of two): a hash set used while the earlier-neighbour
+// rows are built (2 xc), the distinct rows (xc) and the rows adjacent to the
+// current branch (xc).
 template <typename Word>
 struct RegSlab {
   Word *hash, *xr, *xl;
+  int xc;
 };
+
+__device__ __forceinline__ int reg_xcap(const BKArgs &a) { return a.rxcap ? a.rxcap : REG_XCAP; }
 
 template <typename Word>
 __device__ __forceinline__ RegSlab<Word> reg_slab(const BKArgs &a, int64_t gw) {
   Word *base = (Word *)(a.slab + (size_t)gw * a.slab_words);
   RegSlab<Word> s;
+  s.xc = reg_xcap(a);
   s.hash = base;
-  s.xr = base + 2 * REG_XCAP;
-  s.xl = s.xr + REG_XCAP;
+  s.xr = base + 2 * s.xc;
+  s.xl = s.xr + s.xc;
   return s;
 }
 
@@ -276,6 +281,13 @@ __device__ void reg_encode(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab
   const int lane = (int)lane_id();
   const uint32_t lt = (1u << lane) - 1u;
   const int32_t sb = a.split[r], d = a.rp[r + 1] - sb, ub = a.rp[r], u = sb - ub;
+  if (u > sl.xc) {  // more earlier neighbours than the slab's rows (classification bounds it)
+    if (lane == 0) atomicOr(a.err, MCE_ERR_XROWS);
+    rt.r = r;
+    rt.d = 0;
+    rt.nX = 0;
+    return;
+  }
 
   // setup_stack_original_L1_IP (mce/mce_utils.cuh:565-611): P = N+(r)
 #pragma unroll
@@ -361,25 +373,33 @@ __device__ void reg_encode(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab
     const bool hashed = u > 32;
     int hc = 32;
     if (hashed) {
-      while (hc < 2 * u && hc < 2 * REG_XCAP) hc <<= 1;
+      while (hc < 2 * u && hc < 2 * sl.xc) hc <<= 1;
       for (int i = lane; i < hc; i += 32) sl.hash[i] = 0;
     }
+    // a hub's rows were built before the search (hub_rows_launch)
+    const int32_t hub = a.hub_of ? a.hub_of[r] : -1;
+    const unsigned long long *hrows = hub >= 0 ? a.hub_rows + a.hub_off[hub] : nullptr;
     for (int c = 0; c * 32 < u; ++c) {
       const int items = min(32, u - c * 32);
-      int xb = 0, xlen = 0;
-      if (lane < items) {
-        const int32_t x = a.cs[ub + c * 32 + lane];
-        xb = a.split[x];
-        xlen = a.rp[x + 1] - xb;
+      Word row;
+      if (hrows) {
+        row = (Word)hrows[c * 32 + lane];  // zero past the list (padding)
+      } else {
+        int xb = 0, xlen = 0;
+        if (lane < items) {
+          const int32_t x = a.cs[ub + c * 32 + lane];
+          xb = a.split[x];
+          xlen = a.rp[x + 1] - xb;
+        }
+        sm.xs[lane] = 0;
+        __syncwarp();
+        flat_walk(a.cs, xb, xlen, sm.off, sm.beg, sm.own, [&](int t, int32_t w) {
+          const int i = p_find(sm, w);
+          if (i >= 0) atomicOr(&sm.xs[t], O::bit(i));
+        });
+        __syncwarp();
+        row = sm.xs[lane];
       }
-      sm.xs[lane] = 0;
-      __syncwarp();
-      flat_walk(a.cs, xb, xlen, sm.off, sm.beg, sm.own, [&](int t, int32_t w) {
-        const int i = p_find(sm, w);
-        if (i >= 0) atomicOr(&sm.xs[t], O::bit(i));
-      });
-      __syncwarp();
-      const Word row = sm.xs[lane];
       bool fresh = false;
       if (!hashed) {
         const uint32_t same = __match_any_sync(MCE_FULL, row);

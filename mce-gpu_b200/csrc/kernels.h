@@ -33,14 +33,24 @@ int peel_read(const void *ctl_dev, int32_t *degeneracy, uint32_t *err, uint32_t 
 // ---- orientation + root classes ------------------------------------------------
 // Engine classes of a root (by later degree d+ and earlier degree d-).
 enum RootClass : uint32_t {
-  CLS_R32 = 0,   // 1 <= d+ <= 32, d- <= REG_XCAP: warp engine, rows in registers
-  CLS_R64 = 1,   // 33 <= d+ <= 64, d- <= REG_XCAP: warp engine, two rows per lane
+  CLS_R32 = 0,   // 1 <= d+ <= 32, d- <= REG_XCAP_MAX: warp engine, rows in registers
+  CLS_R64 = 1,   // 33 <= d+ <= 64, d- <= REG_XCAP_MAX: warp engine, two rows per lane
   CLS_MEM = 2,   // any other root with d+ <= 2048: warp engine, rows in a slab
   CLS_NONE = 3,  // d+ == 0: not a root
   CLS_BIG = 4,   // d+ > 2048: rejected (the reference's MAX_DEGEN)
   NCLS = 5
 };
-constexpr int REG_XCAP = 1024;  // earlier-neighbour rows a register-engine warp keeps
+// Earlier-neighbour rows a register-engine warp keeps: REG_XCAP in the
+// serving slots and the allocation-free entry point; in mce_count and
+// mce_batch_count the slab is sized per graph (BKArgs::rxcap, a power of two
+// from REG_XCAP up to REG_XCAP_MAX covering the largest d- of those roots),
+// so hubs with few later neighbours stay in the register engines.
+constexpr int REG_XCAP = 1024;
+constexpr int REG_XCAP_MAX = 16384;
+// Register-class roots with more earlier neighbours than this ("hubs") get
+// their earlier-neighbour rows from a parallel pass before the search, one
+// warp per 32 of them, instead of walking them serially in the root's warp.
+constexpr int HUB_XMIN = 256;
 
 // Per-call summary the device writes and the host reads once.
 struct ShapeInfo {
@@ -49,7 +59,10 @@ struct ShapeInfo {
   uint32_t max_dplus;      // over all roots
   uint32_t max_dminus_mem; // over roots of CLS_MEM
   uint32_t max_deg;
+  uint32_t max_dminus_reg; // over roots of CLS_R32 and CLS_R64
+  uint32_t hub_cnt;        // register-class roots with d- > HUB_XMIN
   uint32_t pad;
+  unsigned long long hub_rows;  // their earlier degrees, each rounded up to 32
 };
 
 struct OrientArgs {
@@ -62,8 +75,17 @@ struct OrientArgs {
   ShapeInfo *shape;     // zeroed by the launcher
   const float *cost;    // nullable: per-vertex cost estimate (larger first)
   int sched;
+  int32_t *hub_of;      // nullable, n: index of the vertex in hub_list, or -1
+  int32_t *hub_list;    // n: the hub roots, in no particular order
 };
 int orient_launch(const OrientArgs &a, cudaStream_t s, int *launches);
+
+// Earlier-neighbour rows of the hub roots (orient's hub_list, cnt of them):
+// off[j] = first row of hub j (rows padded to 32 per hub), rows[k] = the
+// bitmap over the hub's later list of one earlier neighbour's later list.
+int hub_rows_launch(const int32_t *rp, const int32_t *split, const int32_t *cs,
+                    const int32_t *hub_list, uint32_t cnt, int64_t total_rows, int64_t *off,
+                    unsigned long long *rows, int sms, cudaStream_t s, int *launches);
 
 // Sort roots by key (stable) and compute class offsets.  temp grows on demand.
 int roots_sort(int64_t n, const uint32_t *keys_in, uint32_t *keys_out, const int32_t *vals_in,
@@ -86,6 +108,10 @@ struct BKArgs {
   unsigned long long *slab;      // per-warp scratch
   size_t slab_words;             // u64 words per warp
   int32_t dcap, xcap;            // slab capacities (later degree, x rows)
+  int32_t rxcap;                 // register engines' x rows (0: REG_XCAP)
+  const int32_t *hub_of;         // nullable, n: hub index of a root (-1: none) ...
+  const int64_t *hub_off;        // ... its first precomputed earlier-neighbour row ...
+  const unsigned long long *hub_rows;  // ... in these rows (hub_rows_launch)
   QueueView q;                   // task queue (q.hdr == nullptr: no sharing)
   int32_t donate_min;            // hand off children with at least this many candidates
   uint32_t donate_after;         // ... once this many nodes of the root/task were walked
@@ -105,7 +131,7 @@ struct BKArgs {
 
 // Launch the engine of one class.  warps_out: number of warps launched (slab sizing).
 int bk_warps_for_class(int cls, int sms, int wide_blocks, int *warps, int *block, int *smem);
-size_t bk_slab_words(int cls, int dcap, int xcap);
+size_t bk_slab_words(int cls, int dcap, int xcap, int rxcap = REG_XCAP);
 uint32_t bk_task_words(int cls, int dcap);
 int queue_launch_init(const QueueView &q, cudaStream_t s, int *launches);
 

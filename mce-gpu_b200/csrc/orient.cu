@@ -25,7 +25,7 @@ constexpr int ORIENT_BLOCK = 256;
 __device__ __forceinline__ uint32_t classify(uint32_t dplus, uint32_t dminus) {
   if (dplus == 0) return CLS_NONE;
   if (dplus > MCE_MAX_LATER_DEGREE) return CLS_BIG;
-  if (dminus <= (uint32_t)REG_XCAP) {
+  if (dminus <= (uint32_t)REG_XCAP_MAX) {
     if (dplus <= 32) return CLS_R32;
     if (dplus <= 64) return CLS_R64;
   }
@@ -34,9 +34,9 @@ __device__ __forceinline__ uint32_t classify(uint32_t dplus, uint32_t dminus) {
 
 __global__ void __launch_bounds__(ORIENT_BLOCK) orient_kernel(OrientArgs a) {
   __shared__ uint32_t s_cls[8];
-  __shared__ uint32_t s_maxd, s_maxdm, s_maxdeg;
+  __shared__ uint32_t s_maxd, s_maxdm, s_maxdeg, s_maxdr;
   if (threadIdx.x < 8) s_cls[threadIdx.x] = 0;
-  if (threadIdx.x == 0) s_maxd = s_maxdm = s_maxdeg = 0;
+  if (threadIdx.x == 0) s_maxd = s_maxdm = s_maxdeg = s_maxdr = 0;
   __syncthreads();
   const uint32_t lane = lane_id();
   const uint32_t lt = (1u << lane) - 1u;
@@ -94,6 +94,16 @@ __global__ void __launch_bounds__(ORIENT_BLOCK) orient_kernel(OrientArgs a) {
       atomicAdd(&s_cls[cls], 1u);
       if (cls != CLS_NONE) atomicMax(&s_maxd, dplus);
       if (cls == CLS_MEM) atomicMax(&s_maxdm, dminus);
+      if (cls == CLS_R32 || cls == CLS_R64) atomicMax(&s_maxdr, dminus);
+      if (a.hub_of) {
+        int32_t hi = -1;
+        if ((cls == CLS_R32 || cls == CLS_R64) && dminus > (uint32_t)HUB_XMIN) {
+          hi = (int32_t)atomicAdd(&a.shape->hub_cnt, 1u);
+          a.hub_list[hi] = v;
+          atomicAdd(&a.shape->hub_rows, (unsigned long long)((dminus + 31u) & ~31u));
+        }
+        a.hub_of[v] = hi;
+      }
       atomicMax(&s_maxdeg, (uint32_t)(e - b));
     }
   }
@@ -103,6 +113,7 @@ __global__ void __launch_bounds__(ORIENT_BLOCK) orient_kernel(OrientArgs a) {
     atomicMax(&a.shape->max_dplus, s_maxd);
     atomicMax(&a.shape->max_dminus_mem, s_maxdm);
     atomicMax(&a.shape->max_deg, s_maxdeg);
+    atomicMax(&a.shape->max_dminus_reg, s_maxdr);
   }
 }
 

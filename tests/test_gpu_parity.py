@@ -95,19 +95,27 @@ def test_rmat_scale13_wide_roots():
     assert r.stats["class_roots"][2] > 0  # wide-engine roots exercised
 
 
-def test_hub_with_many_earlier_neighbours():
-    """A hub of degree 4999 lands in the wide engine through its earlier list."""
-    base = mce.gen_er(5000, 0.002, 11, 5, 5, 12)
+@pytest.mark.parametrize("n", [5000, 18000])
+def test_hub_with_many_earlier_neighbours(n):
+    """Vertex 0 is adjacent to every vertex and sits in a K8 on 0..7, which
+    is peeled last (the sparse rest has a smaller core): its earlier list
+    holds n - 8 vertices, its later list 7.  Up to 16,384 earlier neighbours
+    such a root stays in a register engine (whose slab grows to a power of
+    two covering them); beyond that it lands in the wide engine."""
+    base = mce.gen_er(n, 6.0 / n, 11)
     s, d = [], []
     for v in range(base.n):
         for w in base.col[base.row_ptr[v]:base.row_ptr[v + 1]]:
             if v < w:
                 s.append(v); d.append(int(w))
-    s += [0] * 4999
-    d += list(range(1, 5000))
-    g = mce.from_edges(np.array(s), np.array(d), 5000)
+    s += [0] * (n - 1)
+    d += list(range(1, n))
+    for v in range(1, 8):
+        for w in range(v + 1, 8):
+            s.append(v); d.append(w)
+    g = mce.from_edges(np.array(s), np.array(d), n)
     r = assert_same(g)
-    assert r.stats["class_roots"][2] >= 1
+    assert r.stats["class_roots"][2] == (0 if n - 8 <= 16384 else 1)
 
 
 def test_cliques_wider_than_64():
