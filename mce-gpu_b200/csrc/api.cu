@@ -59,6 +59,7 @@ struct mce_graph {
   int32_t *vals_in = nullptr, *roots = nullptr;
   int32_t *hub_of = nullptr, *hub_list = nullptr;  // roots with many earlier neighbours
   int64_t *hub_off = nullptr;                      // ... their first precomputed row
+  int32_t *hub_nx = nullptr;                       // ... and their number of distinct rows
   unsigned long long *hub_rows = nullptr;          // ... and the rows
   int64_t hub_off_cap = 0, hub_rows_cap = 0;
   ShapeInfo *shape = nullptr;
@@ -103,7 +104,7 @@ void free_graph_bufs(mce_graph *g) {
   dfree(g->f0); dfree(g->f1); dfree(g->f2);
   dfree(g->hb0); dfree(g->hb1); dfree(g->hb2);
   dfree(g->keys_in); dfree(g->keys_out); dfree(g->vals_in); dfree(g->roots);
-  dfree(g->hub_of); dfree(g->hub_list); dfree(g->hub_off); dfree(g->hub_rows);
+  dfree(g->hub_of); dfree(g->hub_list); dfree(g->hub_off); dfree(g->hub_rows); dfree(g->hub_nx);
   g->hub_off_cap = g->hub_rows_cap = 0;
   dfree(g->root_nodes); dfree(g->root_count);
   dfree(g->feat); dfree(g->pred); dfree(g->policy); dfree(g->wlog); dfree(g->cand);
@@ -577,8 +578,10 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
     const int64_t need_off = (int64_t)sh.hub_cnt + 1, need_rows = (int64_t)sh.hub_rows;
     if (need_off > g->hub_off_cap) {
       dfree(g->hub_off);
+      dfree(g->hub_nx);
       g->hub_off_cap = 0;
-      if ((rc = dalloc(&g->hub_off, (size_t)need_off))) return rc;
+      if ((rc = dalloc(&g->hub_off, (size_t)need_off)) || (rc = dalloc(&g->hub_nx, (size_t)need_off)))
+        return rc;
       g->hub_off_cap = need_off;
     }
     if (need_rows > g->hub_rows_cap) {
@@ -588,7 +591,7 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
       g->hub_rows_cap = need_rows;
     }
     if ((rc = hub_rows_launch(g->rp, g->split, g->cs, g->hub_list, sh.hub_cnt, need_rows,
-                              g->hub_off, g->hub_rows, g->sms, s, &launches)))
+                              g->hub_off, g->hub_nx, g->hub_rows, g->sms, s, &launches)))
       return rc;
   }
   // search scratch
@@ -651,6 +654,7 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   a.hub_of = sh.hub_cnt > 0 ? g->hub_of : nullptr;
   a.hub_off = g->hub_off;
   a.hub_rows = g->hub_rows;
+  a.hub_nx = g->hub_nx;
   a.donate_min = o.donate_threshold > 0 ? o.donate_threshold : DEFAULT_DONATE_MIN;
   a.donate_after = o.donate_after > 0 ? (uint32_t)o.donate_after : DEFAULT_DONATE_AFTER;
   a.wait_limit_ns = IDLE_LIMIT_NS;
@@ -675,7 +679,7 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
     int dcap, xcap, rxcap, wbits, share, dmin, log, wide8, level2, xpiv;
     uint32_t dafter;
     const void *slab, *graph_count, *graph_of, *root_nodes, *policy, *q[NCLS], *bufs[4], *wlog;
-    const void *hub[3];
+    const void *hub[4];
     int64_t n, G;
   } key;
   std::memset(&key, 0, sizeof(key));
@@ -708,6 +712,7 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   key.hub[0] = a.hub_of;
   key.hub[1] = a.hub_off;
   key.hub[2] = a.hub_rows;
+  key.hub[3] = a.hub_nx;
   key.n = g->n;
   key.G = bc ? bc->G : 0;
   static_assert(sizeof(SearchKey) <= sizeof(g->search_key), "search key");

@@ -234,7 +234,8 @@ constexpr int HUB_BLOCK = 256;
 // block walks the list in tiles of HUB_BLOCK.
 __global__ void __launch_bounds__(HUB_BLOCK) hub_offsets_kernel(
     const int32_t *__restrict__ rp, const int32_t *__restrict__ split,
-    const int32_t *__restrict__ hub_list, uint32_t cnt, int64_t *__restrict__ off) {
+    const int32_t *__restrict__ hub_list, uint32_t cnt, int64_t *__restrict__ off,
+    int32_t *__restrict__ nx) {
   __shared__ long long wsum[HUB_BLOCK / 32];
   __shared__ long long carry;
   const int lane = (int)lane_id(), wid = (int)(threadIdx.x >> 5);
@@ -256,7 +257,10 @@ __global__ void __launch_bounds__(HUB_BLOCK) hub_offsets_kernel(
     __syncthreads();
     long long before = carry;
     for (int w = 0; w < wid; ++w) before += wsum[w];
-    if (j < cnt) off[j] = (int64_t)(before + x - v);
+    if (j < cnt) {
+      off[j] = (int64_t)(before + x - v);
+      nx[j] = -1;
+    }
     __syncthreads();
     if (threadIdx.x == HUB_BLOCK - 1) carry = before + x;
     __syncthreads();
@@ -343,9 +347,10 @@ __global__ void __launch_bounds__(HUB_BLOCK) hub_rows_kernel(
 
 int hub_rows_launch(const int32_t *rp, const int32_t *split, const int32_t *cs,
                     const int32_t *hub_list, uint32_t cnt, int64_t total_rows, int64_t *off,
-                    unsigned long long *rows, int sms, cudaStream_t s, int *launches) {
+                    int32_t *nx, unsigned long long *rows, int sms, cudaStream_t s,
+                    int *launches) {
   if (cnt == 0) return MCE_OK;
-  hub_offsets_kernel<<<1, HUB_BLOCK, 0, s>>>(rp, split, hub_list, cnt, off);
+  hub_offsets_kernel<<<1, HUB_BLOCK, 0, s>>>(rp, split, hub_list, cnt, off, nx);
   MCE_CUDA(cudaGetLastError());
   const int64_t chunks = total_rows / 32;
   int64_t blocks = ((chunks + 7) / 8 + 0);  // up to one chunk per warp

@@ -369,16 +369,28 @@ __device__ void reg_encode(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab
   // in N+(x).  Up to 32 of them are deduplicated with one match over the
   // warp; more go through a hash set in the slab.
   int nX = 0;
-  if (u > 0) {
+  // A hub's rows were built before the search (hub_rows_launch); its first
+  // encode writes the distinct ones back there and publishes their number
+  // (hub_nx), so the warps that take its subtrees later only copy them.
+  const int32_t hub = (u > 0 && a.hub_of) ? a.hub_of[r] : -1;
+  unsigned long long *hrows = hub >= 0 ? a.hub_rows + a.hub_off[hub] : nullptr;
+  int kept = -1;
+  if (hrows) {
+    if (lane == 0) kept = (int)ld_acquire(reinterpret_cast<const uint32_t *>(a.hub_nx + hub));
+    kept = __shfl_sync(MCE_FULL, kept, 0);
+    __syncwarp();  // the other lanes read after lane 0's acquire
+  }
+  if (kept >= 0) {
+    for (int i = lane; i < kept; i += 32) sl.xr[i] = (Word)__ldcg(hrows + i);  // from L2
+    __syncwarp();
+    nX = kept;
+  } else if (u > 0) {
     const bool hashed = u > 32;
     int hc = 32;
     if (hashed) {
       while (hc < 2 * u && hc < 2 * sl.xc) hc <<= 1;
       for (int i = lane; i < hc; i += 32) sl.hash[i] = 0;
     }
-    // a hub's rows were built before the search (hub_rows_launch)
-    const int32_t hub = a.hub_of ? a.hub_of[r] : -1;
-    const unsigned long long *hrows = hub >= 0 ? a.hub_rows + a.hub_off[hub] : nullptr;
     for (int c = 0; c * 32 < u; ++c) {
       const int items = min(32, u - c * 32);
       Word row;
@@ -421,10 +433,61 @@ __device__ void reg_encode(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab
       nX += __popc(mk);
       __syncwarp();
     }
+    if (hrows) {  // rows [0, nX) of the hub's region are no longer read as built
+      for (int i = lane; i < nX; i += 32) hrows[i] = (u64)sl.xr[i];
+      __threadfence();
+      __syncwarp();
+      if (lane == 0) st_release(reinterpret_cast<uint32_t *>(a.hub_nx + hub), (uint32_t)nX);
+    }
   }
   rt.r = r;
   rt.d = d;
   rt.nX = nX;
+}
+
+// Rows [32, nL) of the leaf filter (in the slab): does one contain S?  Four
+// windows of loads are in flight per step; hub roots keep thousands.
+template <typename Word>
+__device__ __forceinline__ bool xl_covers(const Word *xl, int nL, Word S) {
+  const int lane = (int)lane_id();
+  for (int i0 = 32; i0 < nL; i0 += 128) {
+    bool hit = false;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int i = i0 + 32 * q + lane;
+      if (i < nL) hit |= (xl[i] & S) == S;
+    }
+    if (__any_sync(MCE_FULL, hit)) return true;
+  }
+  return false;
+}
+
+// The leaf filter of a depth-0 branch: the rows of xr[0, nX) adjacent to
+// branch vertex vb, the first 32 into xl0 (shared memory), the rest into xl.
+template <typename Word>
+__device__ __forceinline__ int xl_filter(const Word *xr, int nX, Word vb, Word *xl0, Word *xl) {
+  const int lane = (int)lane_id();
+  const uint32_t lt = (1u << lane) - 1u;
+  int nL = 0;
+  for (int i0 = 0; i0 < nX; i0 += 128) {
+    Word rw[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int i = i0 + 32 * q + lane;
+      rw[q] = i < nX ? xr[i] : (Word)0;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const bool has = (rw[q] & vb) != 0;
+      const uint32_t mk = __ballot_sync(MCE_FULL, has);
+      if (has) {
+        const int at = nL + __popc(mk & lt);
+        (at < 32 ? xl0 : xl)[at] = rw[q];
+      }
+      nL += __popc(mk);
+    }
+  }
+  return nL;
 }
 
 // Leaf-filter row i: the first 32 in shared memory, the rest in the slab.
@@ -625,18 +688,7 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
       break;
     }
     if (per_branch && depth == 0 && nX > 0) {  // earlier neighbours adjacent to v
-      nL = 0;
-      for (int i0 = 0; i0 < nX; i0 += 32) {
-        const int i = i0 + lane;
-        const Word row = i < nX ? sl.xr[i] : (Word)0;
-        const bool has = (row & vb) != 0;
-        const uint32_t mk = __ballot_sync(MCE_FULL, has);
-        if (has) {
-          const int at = nL + __popc(mk & lt);
-          (at < 32 ? sm.xl0 : sl.xl)[at] = row;
-        }
-        nL += __popc(mk);
-      }
+      nL = xl_filter<Word>(sl.xr, nX, vb, sm.xl0, sl.xl);
       __syncwarp();
     }
     if (Pc == 0) {
@@ -645,10 +697,7 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
       // neighbour of the root adjacent to the whole clique.
       if (Xc == 0) {
         bool covered = __any_sync(MCE_FULL, lane < nL && (sm.xl0[lane] & Sc) == Sc);
-        for (int i0 = 32; !covered && i0 < nL; i0 += 32) {
-          const int i = i0 + lane;
-          covered = __any_sync(MCE_FULL, i < nL && (sl.xl[i] & Sc) == Sc);
-        }
+        if (!covered && nL > 32) covered = xl_covers<Word>(sl.xl, nL, Sc);
         if (!covered) {
           ++cnt;
           if constexpr (LIST) reg_emit<Word, NR>(a, sm, rt.r, Sc);
@@ -693,10 +742,7 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
       // under which the outside pivot (XP) ends the walk here instead.
       const Word Sl = Sc | Pc;
       bool covered = __any_sync(MCE_FULL, lane < nL && (sm.xl0[lane] & Sl) == Sl);
-      for (int i0 = 32; !covered && i0 < nL; i0 += 32) {
-        const int i = i0 + lane;
-        covered = __any_sync(MCE_FULL, i < nL && (sl.xl[i] & Sl) == Sl);
-      }
+      if (!covered && nL > 32) covered = xl_covers<Word>(sl.xl, nL, Sl);
       if (XP && covered) continue;
       nodes += (u64)pc;
       if (Budget && a.node_budget && nodes > a.node_budget) {

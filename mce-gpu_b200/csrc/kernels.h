@@ -83,9 +83,11 @@ int orient_launch(const OrientArgs &a, cudaStream_t s, int *launches);
 // Earlier-neighbour rows of the hub roots (orient's hub_list, cnt of them):
 // off[j] = first row of hub j (rows padded to 32 per hub), rows[k] = the
 // bitmap over the hub's later list of one earlier neighbour's later list.
+// nx[j] = -1: hub j's distinct rows are not known yet (the search sets it).
 int hub_rows_launch(const int32_t *rp, const int32_t *split, const int32_t *cs,
                     const int32_t *hub_list, uint32_t cnt, int64_t total_rows, int64_t *off,
-                    unsigned long long *rows, int sms, cudaStream_t s, int *launches);
+                    int32_t *nx, unsigned long long *rows, int sms, cudaStream_t s,
+                    int *launches);
 
 // Sort roots by key (stable) and compute class offsets.  temp grows on demand.
 int roots_sort(int64_t n, const uint32_t *keys_in, uint32_t *keys_out, const int32_t *vals_in,
@@ -111,7 +113,8 @@ struct BKArgs {
   int32_t rxcap;                 // register engines' x rows (0: REG_XCAP)
   const int32_t *hub_of;         // nullable, n: hub index of a root (-1: none) ...
   const int64_t *hub_off;        // ... its first precomputed earlier-neighbour row ...
-  const unsigned long long *hub_rows;  // ... in these rows (hub_rows_launch)
+  unsigned long long *hub_rows;  // ... in these rows (hub_rows_launch) ...
+  int32_t *hub_nx;               // ... of which the first hub_nx are distinct once >= 0
   QueueView q;                   // task queue (q.hdr == nullptr: no sharing)
   int32_t donate_min;            // hand off children with at least this many candidates
   uint32_t donate_after;         // ... once this many nodes of the root/task were walked
