@@ -317,6 +317,17 @@ int mce_batch_reload(mce_batch_t b, const int32_t *row_ptr, const int32_t *col,
 int mce_batch_count(mce_batch_t b, const mce_opts_t *opts, uint64_t *per_graph_total,
                     uint64_t *total, uint64_t *hist, mce_stats_t *stats);
 
+/* mce_batch_reload followed by mce_batch_count in one call, for a batch in
+ * host memory: batches of 2^20 arcs or more are copied in up to four parts
+ * of whole graphs on a stream of the handle's own, and each part is rebased,
+ * peeled and oriented as soon as it is on the device, while the next parts
+ * are still being copied; one search over the whole batch follows.  Same
+ * results as the two calls.  Pinned host memory lets the copies overlap. */
+int mce_batch_count_host(mce_batch_t b, const int32_t *row_ptr, const int32_t *col,
+                         const int64_t *vtx_offsets, const int64_t *arc_offsets,
+                         int32_t num_graphs, const mce_opts_t *opts, uint64_t *per_graph_total,
+                         uint64_t *total, uint64_t *hist, mce_stats_t *stats);
+
 int mce_batch_free(mce_batch_t b);
 
 

@@ -84,6 +84,10 @@ struct mce_graph {
   ShapeInfo shape_h{};
   int32_t degeneracy = 0;
   cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  // a batch arriving in parts: one stream per part, forked from and joined
+  // to the caller's stream
+  cudaStream_t part_s[4] = {nullptr};
+  cudaEvent_t part_fork = nullptr, part_done[4] = {nullptr};
   // search launches captured as a CUDA graph, replayed while the key matches
   cudaGraphExec_t search_exec = nullptr;
   unsigned char search_key[256] = {0};
@@ -95,6 +99,7 @@ constexpr uint64_t WAIT_LIMIT_NS = 20ull * 1000 * 1000 * 1000;  // 20 s per barr
 constexpr uint64_t IDLE_LIMIT_NS = 30ull * 1000 * 1000 * 1000;  // 30 s without any progress
 constexpr uint32_t QUEUE_CAP = 1u << 14;                        // tasks per class queue
 constexpr int DEFAULT_DONATE_MIN = 10;
+constexpr int64_t BATCH_PART_MIN_ARCS = 1 << 20;  // mce_batch_count_host: smaller batches in one part
 constexpr uint32_t DEFAULT_SOLO_MAX = 0;     // measured slower than grid-wide rounds
 constexpr uint32_t DEFAULT_DONATE_AFTER = 256;  // the reference's SZTH (mce/parameter.cuh:5)
 
@@ -145,13 +150,25 @@ int alloc_fixed_bufs(mce_graph *g) {
 cudaStream_t pick_stream(mce_graph *g, void *s) { return s ? (cudaStream_t)s : g->own; }
 
 // Per-graph counting of a batch handle.
+// A batch still arriving from the host in parts (mce_batch_count_host):
+// graphs [g[p], g[p+1]) are on the device once ready[p] has fired.
+constexpr int MAX_PARTS = 4;
+struct BatchParts {
+  int k;
+  int64_t g[MAX_PARTS + 1];
+  cudaEvent_t ready[MAX_PARTS];
+  const int32_t *rp_local, *col_local;  // device: the uploaded concatenations
+  const int64_t *vo_h, *ao_h;           // host: the layout
+};
+
 struct BatchCtx {
   const int32_t *graph_of;             // device, n
   unsigned long long *graph_count;     // device, G
   uint64_t *per_graph_out;             // host, G
   int64_t G;
   const int64_t *vtx_off, *arc_off;    // device, G + 1: the uploaded layout
-  const int32_t *order;                // device, G: graphs largest first
+  const int32_t *order;                // device, G: graphs largest first (within each part)
+  const BatchParts *parts = nullptr;   // nullable: rebase, peel and orient part by part
 };
 
 int check_args(const int32_t *row_ptr, const int32_t *col, int64_t n, int64_t m) {
@@ -178,9 +195,19 @@ int upload_csr(mce_graph *g, const int32_t *row_ptr, const int32_t *col, int64_t
 }
 
 // Stage 1: peel -> prio, core.
+PeelArgs peel_args(mce_graph *g, int solo_opt);
+
 int run_peel(mce_graph *g, cudaStream_t s, int *launches, int solo_opt = 0,
              const BatchCtx *bc = nullptr) {
   if (g->n == 0) return MCE_OK;
+  const PeelArgs pa = peel_args(g, solo_opt);
+  if (bc)  // a batch: every graph peeled by one block, no grid-wide rounds
+    return peel_segments_launch(pa, bc->vtx_off, bc->arc_off, bc->order, (int32_t)bc->G, s,
+                                launches);
+  return peel_launch(pa, s, launches);
+}
+
+PeelArgs peel_args(mce_graph *g, int solo_opt) {
   PeelArgs pa;
   pa.n = g->n;
   pa.m = g->m;
@@ -200,10 +227,7 @@ int run_peel(mce_graph *g, cudaStream_t s, int *launches, int solo_opt = 0,
   pa.ctl = g->peel_ctl;
   pa.wait_limit_ns = WAIT_LIMIT_NS;
   pa.solo_max = solo_opt < 0 ? 0u : solo_opt == 0 ? DEFAULT_SOLO_MAX : (uint32_t)solo_opt;
-  if (bc)  // a batch: every graph peeled by one block, no grid-wide rounds
-    return peel_segments_launch(pa, bc->vtx_off, bc->arc_off, bc->order, (int32_t)bc->G, s,
-                                launches);
-  return peel_launch(pa, s, launches);
+  return pa;
 }
 
 // Stage 2: orient + classify + sort roots (keys plain: class only).
@@ -212,7 +236,7 @@ int run_sort(mce_graph *g, int end_bit, cudaStream_t s, int *launches) {
                     &g->sort_tmp_bytes, g->shape, s, launches);
 }
 
-int run_orient(mce_graph *g, cudaStream_t s, int *launches, bool skip_sort = false) {
+OrientArgs orient_args(mce_graph *g) {
   OrientArgs oa;
   oa.n = g->n;
   oa.rp = g->rp;
@@ -227,9 +251,57 @@ int run_orient(mce_graph *g, cudaStream_t s, int *launches, bool skip_sort = fal
   oa.sched = MCE_SCHED_PLAIN;
   oa.hub_of = g->hub_of;
   oa.hub_list = g->hub_list;
-  int rc = orient_launch(oa, s, launches);
+  return oa;
+}
+
+int run_orient(mce_graph *g, cudaStream_t s, int *launches, bool skip_sort = false) {
+  int rc = orient_launch(orient_args(g), s, launches);
   if (rc) return rc;
   return skip_sort ? MCE_OK : run_sort(g, 3, s, launches);  // keys: class only
+}
+
+// A batch arriving in parts: as each part's copy lands, its graphs are
+// rebased, peeled (one block per graph) and their vertices oriented, on a
+// stream per part so that the parts' peels (each bound by its largest
+// graphs' round chains) overlap; the roots' summary accumulates over them.
+int run_parts(mce_graph *g, cudaStream_t s, int *launches, const BatchCtx *bc, int solo_opt) {
+  const BatchParts &P = *bc->parts;
+  static_assert(MAX_PARTS <= 4, "part streams");
+  const PeelArgs pa = peel_args(g, solo_opt);
+  for (int p = 0; p < P.k; ++p) {
+    if (!g->part_s[p]) MCE_CUDA(cudaStreamCreateWithFlags(&g->part_s[p], cudaStreamNonBlocking));
+    if (!g->part_done[p])
+      MCE_CUDA(cudaEventCreateWithFlags(&g->part_done[p], cudaEventDisableTiming));
+  }
+  if (!g->part_fork) MCE_CUDA(cudaEventCreateWithFlags(&g->part_fork, cudaEventDisableTiming));
+  // zeroed once for all parts: the peel's control block and the roots' summary
+  MCE_CUDA(cudaMemsetAsync(g->peel_ctl, 0, peel_ctl_bytes(), s));
+  MCE_CUDA(cudaMemsetAsync(g->shape, 0, sizeof(ShapeInfo), s));
+  MCE_CUDA(cudaEventRecord(g->part_fork, s));
+  for (int p = 0; p < P.k; ++p) {
+    cudaStream_t sp = g->part_s[p];
+    const int64_t g0 = P.g[p], g1 = P.g[p + 1];
+    const int64_t vbeg = P.vo_h[g0] - g0, vend = P.vo_h[g1] - g1;
+    MCE_CUDA(cudaStreamWaitEvent(sp, g->part_fork, 0));
+    MCE_CUDA(cudaStreamWaitEvent(sp, P.ready[p], 0));
+    int rc = batch_rebase_part_launch(P.rp_local, P.col_local, bc->vtx_off, bc->arc_off,
+                                      (int32_t)bc->G, P.vo_h[g0], P.vo_h[g1], P.ao_h[g0],
+                                      P.ao_h[g1], vend, (int32_t)P.ao_h[g1], g->rp, g->col,
+                                      const_cast<int32_t *>(bc->graph_of), g->sms, sp, launches);
+    if (rc) return rc;
+    if (vend > vbeg &&
+        (rc = peel_segments_launch(pa, bc->vtx_off, bc->arc_off, bc->order + g0,
+                                   (int32_t)(g1 - g0), sp, launches, p)))
+      return rc;
+    OrientArgs oa = orient_args(g);
+    oa.v0 = vbeg;
+    oa.n = vend;
+    oa.keep_shape = true;
+    if ((rc = orient_launch(oa, sp, launches))) return rc;
+    MCE_CUDA(cudaEventRecord(g->part_done[p], sp));
+  }
+  for (int p = 0; p < P.k; ++p) MCE_CUDA(cudaStreamWaitEvent(s, g->part_done[p], 0));
+  return MCE_OK;
 }
 
 int read_shape(mce_graph *g, cudaStream_t s) {
@@ -425,6 +497,11 @@ int mce_graph_free(mce_graph_t g) {
   if (g->search_exec) cudaGraphExecDestroy(g->search_exec);
   for (auto &e : g->ev)
     if (e) cudaEventDestroy(e);
+  for (int p = 0; p < 4; ++p) {
+    if (g->part_s[p]) cudaStreamDestroy(g->part_s[p]);
+    if (g->part_done[p]) cudaEventDestroy(g->part_done[p]);
+  }
+  if (g->part_fork) cudaEventDestroy(g->part_fork);
   if (g->own) cudaStreamDestroy(g->own);
   delete g;
   return MCE_OK;
@@ -543,14 +620,21 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   mce_stats_t st;
   std::memset(&st, 0, sizeof(st));
   MCE_CUDA(cudaEventRecord(g->ev[0], s));
-  if ((rc = run_peel(g, s, &launches, o.peel_solo_max, bc))) return rc;
+  const bool parted = bc && bc->parts;
+  if ((rc = parted ? run_parts(g, s, &launches, bc, o.peel_solo_max)
+                   : run_peel(g, s, &launches, o.peel_solo_max, bc)))
+    return rc;
   MCE_CUDA(cudaEventRecord(g->ev[1], s));
   // Root order: plain = vertex id within each engine class; degree = a
   // degree-based cost; learned = the model's predicted tree size.  Larger
   // costs first; the learned order also sets which roots share subtrees.
   const mce_model *model = (const mce_model *)o.model;
   const int sched = o.sched == MCE_SCHED_LEARNED && !model ? MCE_SCHED_DEGREE : o.sched;
-  if ((rc = run_orient(g, s, &launches, sched != MCE_SCHED_PLAIN))) return rc;
+  if (parted) {  // oriented part by part already; plain order sorts by class only
+    if (sched == MCE_SCHED_PLAIN && (rc = run_sort(g, 3, s, &launches))) return rc;
+  } else if ((rc = run_orient(g, s, &launches, sched != MCE_SCHED_PLAIN))) {
+    return rc;
+  }
   const uint8_t *policy = nullptr;
   const float heavy = (float)(o.heavy_log2 > 0 ? o.heavy_log2 : DEFAULT_HEAVY_LOG2);
   const float share_cost = (float)(o.share_log2 > 0 ? o.share_log2 : DEFAULT_SHARE_LOG2);
@@ -949,6 +1033,9 @@ struct mce_batch {
   int32_t *order = nullptr;    // graph ids by arc count, largest first (per-graph peel)
   int32_t *order_h = nullptr;  // its pinned host staging copy
   int64_t cap_rows = -1, cap_m = -1, cap_g = -1;
+  // mce_batch_count_host: copies on their own stream, one event per part
+  cudaStream_t copy = nullptr;
+  cudaEvent_t start = nullptr, ready[MAX_PARTS] = {nullptr};
 };
 
 namespace {
@@ -979,8 +1066,8 @@ void batch_free_bufs(mce_batch *b) {
   b->cap_rows = b->cap_m = b->cap_g = -1;
 }
 
-int batch_load(mce_batch *b, const int32_t *row_ptr, const int32_t *col, const int64_t *vo,
-               const int64_t *ao, int32_t G, int64_t n, int64_t m, cudaStream_t s) {
+// Device buffers for a batch of G graphs, n vertices and m arcs.
+int batch_alloc(mce_batch *b, int32_t G, int64_t n, int64_t m) {
   mce_graph *g = b->g;
   int rc;
   if (n > g->cap_n || m > g->cap_m) {
@@ -1005,6 +1092,15 @@ int batch_load(mce_batch *b, const int32_t *row_ptr, const int32_t *col, const i
   g->n = n;
   g->m = m;
   g->logged = false;
+  return MCE_OK;
+}
+
+int batch_load(mce_batch *b, const int32_t *row_ptr, const int32_t *col, const int64_t *vo,
+               const int64_t *ao, int32_t G, int64_t n, int64_t m, cudaStream_t s) {
+  mce_graph *g = b->g;
+  int rc = batch_alloc(b, G, n, m);
+  if (rc) return rc;
+  const int64_t rows = n + G;
   MCE_CUDA(cudaMemcpyAsync(b->rp_local, row_ptr, sizeof(int32_t) * (size_t)rows,
                            cudaMemcpyHostToDevice, s));
   if (m > 0)
@@ -1093,11 +1189,97 @@ int mce_batch_count(mce_batch_t b, const mce_opts_t *opts, uint64_t *per_graph_t
   return count_impl(b->g, o, total, hist, stats, &bc);
 }
 
+int mce_batch_count_host(mce_batch_t b, const int32_t *row_ptr, const int32_t *col,
+                         const int64_t *vtx_offsets, const int64_t *arc_offsets,
+                         int32_t num_graphs, const mce_opts_t *opts, uint64_t *per_graph_total,
+                         uint64_t *total, uint64_t *hist, mce_stats_t *stats) {
+  if (!b || !total || !per_graph_total) return MCE_EINVAL;
+  int64_t n = 0, m = 0;
+  int rc = batch_check(row_ptr, col, vtx_offsets, arc_offsets, num_graphs, &n, &m);
+  if (rc) return rc;
+  mce_opts_t o;
+  if (opts) {
+    o = *opts;
+  } else {
+    mce_opts_default(&o);
+    o.cuda_graph = 1;
+  }
+  const int32_t G = num_graphs;
+  const int64_t *vo = vtx_offsets, *ao = arc_offsets;
+  // parts of about equal arc count, whole graphs each; small batches in one
+  int k = m >= BATCH_PART_MIN_ARCS ? MAX_PARTS : 1;
+  if (k > G) k = G;
+  BatchParts P;
+  P.k = 0;
+  P.g[0] = 0;
+  for (int p = 1; p < k; ++p) {
+    int64_t gp = P.g[P.k];
+    const int64_t want = m * p / k;
+    while (gp < G && ao[gp] < want) ++gp;
+    if (gp > P.g[P.k] && gp < G) P.g[++P.k] = gp;
+  }
+  P.g[++P.k] = G;
+  if (P.k == 1)
+    return (rc = mce_batch_reload(b, row_ptr, col, vo, ao, G, o.stream)) ? rc
+           : mce_batch_count(b, &o, per_graph_total, total, hist, stats);
+  MCE_CUDA(cudaSetDevice(b->g->device));
+  cudaStream_t s = pick_stream(b->g, o.stream);
+  if ((rc = batch_alloc(b, G, n, m))) return rc;
+  if (!b->copy) MCE_CUDA(cudaStreamCreateWithFlags(&b->copy, cudaStreamNonBlocking));
+  if (!b->start) MCE_CUDA(cudaEventCreateWithFlags(&b->start, cudaEventDisableTiming));
+  for (int p = 0; p < MAX_PARTS; ++p)
+    if (!b->ready[p]) MCE_CUDA(cudaEventCreateWithFlags(&b->ready[p], cudaEventDisableTiming));
+  // graphs largest first within each part (the per-graph peel's order)
+  int32_t *order = b->order_h;
+  for (int32_t i = 0; i < G; ++i) order[i] = i;
+  for (int p = 0; p < P.k; ++p)
+    std::stable_sort(order + P.g[p], order + P.g[p + 1], [&](int32_t x, int32_t y) {
+      return ao[x + 1] - ao[x] > ao[y + 1] - ao[y];
+    });
+  // the copies wait for earlier work on the caller's stream, then run on
+  // their own stream while the caller's stream processes the parts already
+  // on the device
+  MCE_CUDA(cudaEventRecord(b->start, s));
+  MCE_CUDA(cudaStreamWaitEvent(b->copy, b->start, 0));
+  MCE_CUDA(cudaMemcpyAsync(b->vtx_off, vo, sizeof(int64_t) * (size_t)(G + 1),
+                           cudaMemcpyHostToDevice, b->copy));
+  MCE_CUDA(cudaMemcpyAsync(b->arc_off, ao, sizeof(int64_t) * (size_t)(G + 1),
+                           cudaMemcpyHostToDevice, b->copy));
+  MCE_CUDA(cudaMemcpyAsync(b->order, order, sizeof(int32_t) * (size_t)G, cudaMemcpyHostToDevice,
+                           b->copy));
+  for (int p = 0; p < P.k; ++p) {
+    const int64_t r0 = vo[P.g[p]], r1 = vo[P.g[p + 1]], a0 = ao[P.g[p]], a1 = ao[P.g[p + 1]];
+    MCE_CUDA(cudaMemcpyAsync(b->rp_local + r0, row_ptr + r0, sizeof(int32_t) * (size_t)(r1 - r0),
+                             cudaMemcpyHostToDevice, b->copy));
+    if (a1 > a0)
+      MCE_CUDA(cudaMemcpyAsync(b->col_local + a0, col + a0, sizeof(int32_t) * (size_t)(a1 - a0),
+                               cudaMemcpyHostToDevice, b->copy));
+    MCE_CUDA(cudaEventRecord(b->ready[p], b->copy));
+    P.ready[p] = b->ready[p];
+  }
+  P.rp_local = b->rp_local;
+  P.col_local = b->col_local;
+  P.vo_h = vo;
+  P.ao_h = ao;
+  BatchCtx bc{b->graph_of, b->graph_count, per_graph_total, b->G, b->vtx_off, b->arc_off, b->order};
+  bc.parts = &P;
+  rc = count_impl(b->g, o, total, hist, stats, &bc);
+  if (rc) cudaStreamSynchronize(b->copy);  // no copy outlives a failed call
+  return rc;
+}
+
 int mce_batch_free(mce_batch_t b) {
   if (!b) return MCE_OK;
   if (b->g) {
     cudaSetDevice(b->g->device);
     cudaStreamSynchronize(b->g->own);
+    if (b->copy) {
+      cudaStreamSynchronize(b->copy);
+      cudaStreamDestroy(b->copy);
+    }
+    if (b->start) cudaEventDestroy(b->start);
+    for (cudaEvent_t e : b->ready)
+      if (e) cudaEventDestroy(e);
   }
   batch_free_bufs(b);
   if (b->g) mce_graph_free(b->g);

@@ -25,8 +25,12 @@ size_t peel_ctl_bytes();
 int peel_launch(const PeelArgs &a, cudaStream_t s, int *launches);
 // Batches: each graph of the disjoint union peeled by one block (order:
 // graph ids, largest first).
+// part >= 0 (0..3): one part of a batch still arriving, peeled concurrently
+// with the others; the control block was zeroed before the first part and
+// each part takes graphs from its own counter.  part < 0: the whole batch.
 int peel_segments_launch(const PeelArgs &a, const int64_t *vtx_off, const int64_t *arc_off,
-                         const int32_t *order, int32_t G, cudaStream_t s, int *launches);
+                         const int32_t *order, int32_t G, cudaStream_t s, int *launches,
+                         int part = -1);
 int peel_read(const void *ctl_dev, int32_t *degeneracy, uint32_t *err, uint32_t *rounds,
               uint32_t *solo_sections, cudaStream_t s, double *phase_ms = nullptr);
 
@@ -77,6 +81,8 @@ struct OrientArgs {
   int sched;
   int32_t *hub_of;      // nullable, n: index of the vertex in hub_list, or -1
   int32_t *hub_list;    // n: the hub roots, in no particular order
+  int64_t v0 = 0;       // vertices [v0, n) are oriented (a batch part: its range)
+  bool keep_shape = false;  // add to the summary of earlier parts instead of zeroing it
 };
 int orient_launch(const OrientArgs &a, cudaStream_t s, int *launches);
 
@@ -162,6 +168,14 @@ int batch_rebase_launch(const int32_t *rp_local, const int32_t *col_local,
                         const int64_t *vtx_off, const int64_t *arc_off, int32_t G, int64_t n,
                         int64_t m, int32_t *rp, int32_t *col, int32_t *graph_of, int sms,
                         cudaStream_t s, int *launches);
+// The same for the graphs [g0, g1) of the batch only (uploaded rows
+// [row0, row1) and arcs [arc0, arc1)); also writes rp[vend] = rp_end, the
+// offset the part's last row ends at (the next part's first row).
+int batch_rebase_part_launch(const int32_t *rp_local, const int32_t *col_local,
+                             const int64_t *vtx_off, const int64_t *arc_off, int32_t G,
+                             int64_t row0, int64_t row1, int64_t arc0, int64_t arc1, int64_t vend,
+                             int32_t rp_end, int32_t *rp, int32_t *col, int32_t *graph_of, int sms,
+                             cudaStream_t s, int *launches);
 int bk_launch(int cls, int word_bits, const BKArgs &a, int grid, int block, int smem,
               cudaStream_t s, int *launches);
 

@@ -42,7 +42,7 @@ __global__ void __launch_bounds__(ORIENT_BLOCK) orient_kernel(OrientArgs a) {
   const uint32_t lt = (1u << lane) - 1u;
   const int64_t gwarp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t vv = gwarp; vv < a.n; vv += nwarps) {
+  for (int64_t vv = a.v0 + gwarp; vv < a.n; vv += nwarps) {
     const int32_t v = (int32_t)vv;
     const int32_t b = a.rp[v], e = a.rp[v + 1];
     const uint32_t pv = a.prio[v];
@@ -134,9 +134,9 @@ int orient_launch(const OrientArgs &a, cudaStream_t s, int *launches) {
   int dev = 0, sms = 0;
   MCE_CUDA(cudaGetDevice(&dev));
   MCE_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  MCE_CUDA(cudaMemsetAsync(a.shape, 0, sizeof(ShapeInfo), s));
-  if (a.n == 0) return MCE_OK;
-  const int64_t warps_needed = a.n;
+  if (!a.keep_shape) MCE_CUDA(cudaMemsetAsync(a.shape, 0, sizeof(ShapeInfo), s));
+  if (a.n <= a.v0) return MCE_OK;
+  const int64_t warps_needed = a.n - a.v0;
   int64_t blocks = (warps_needed + (ORIENT_BLOCK / 32) - 1) / (ORIENT_BLOCK / 32);
   const int64_t cap = (int64_t)sms * 8 * 4;  // enough resident warps to cover latency
   if (blocks > cap) blocks = cap;

@@ -46,6 +46,7 @@ struct PeelCtl {
   uint32_t solo_sections;
   unsigned long long t_scan, t_round, t_wait;  // ns seen by block 0 (diagnostics)
   uint32_t seg_next;   // batches: next graph to peel
+  uint32_t seg_part[4];  // ... the same per part of a batch still arriving (peeled concurrently)
 };
 
 namespace {
@@ -405,11 +406,12 @@ __global__ void __launch_bounds__(SEG_BLOCK)
     peel_segments_kernel(const int32_t *__restrict__ rp, const int32_t *__restrict__ col,
                          int32_t *deg, int32_t *core, uint32_t *prio, int32_t *fa, int32_t *fb,
                          const int64_t *__restrict__ vtx_off, const int64_t *__restrict__ arc_off,
-                         const int32_t *__restrict__ order, int32_t G, PeelCtl *ctl) {
+                         const int32_t *__restrict__ order, int32_t G, PeelCtl *ctl,
+                         uint32_t *next) {
   __shared__ SegShared sh;
   const int lane = (int)lane_id(), w = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for (;;) {
-    if (threadIdx.x == 0) sh.g = atomicAdd(&ctl->seg_next, 1u);  // next graph, largest first
+    if (threadIdx.x == 0) sh.g = atomicAdd(next, 1u);  // next graph, largest first
     __syncthreads();
     const uint32_t gi = sh.g;
     if (gi >= (uint32_t)G) break;
@@ -504,19 +506,23 @@ __global__ void __launch_bounds__(SEG_BLOCK)
 }  // namespace
 
 int peel_segments_launch(const PeelArgs &a, const int64_t *vtx_off, const int64_t *arc_off,
-                         const int32_t *order, int32_t G, cudaStream_t s, int *launches) {
+                         const int32_t *order, int32_t G, cudaStream_t s, int *launches,
+                         int part) {
   int dev = 0, sms = 0, per_sm = 0;
   MCE_CUDA(cudaGetDevice(&dev));
   MCE_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   MCE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, peel_segments_kernel, SEG_BLOCK, 0));
   if (per_sm < 1) return MCE_ECUDA;
   PeelCtl *ctl = (PeelCtl *)a.ctl;
-  MCE_CUDA(cudaMemsetAsync(ctl, 0, sizeof(PeelCtl), s));
+  if (part < 0) MCE_CUDA(cudaMemsetAsync(ctl, 0, sizeof(PeelCtl), s));
+  if (part >= 4) return MCE_EINVAL;
+  uint32_t *next = part < 0 ? &ctl->seg_next : &ctl->seg_part[part];
   int blocks = sms * per_sm;
   if (blocks > G) blocks = G;
   if (blocks < 1) return MCE_OK;
   peel_segments_kernel<<<blocks, SEG_BLOCK, 0, s>>>(a.rp, a.col, a.deg, a.core, a.prio, a.front0,
-                                                    a.front1, vtx_off, arc_off, order, G, ctl);
+                                                    a.front1, vtx_off, arc_off, order, G, ctl,
+                                                    next);
   MCE_CUDA(cudaGetLastError());
   if (launches) *launches += 1;
   return MCE_OK;

@@ -135,6 +135,7 @@ _sigs = {
     "mce_batch_upload": (C.c_int, [_P, _P, _P, _P, C.c_int32, C.c_int32, _P, _P]),
     "mce_batch_reload": (C.c_int, [_P, _P, _P, _P, _P, C.c_int32, _P]),
     "mce_batch_count": (C.c_int, [_P, _P, _P, _P, _P, _P]),
+    "mce_batch_count_host": (C.c_int, [_P, _P, _P, _P, _P, C.c_int32, _P, _P, _P, _P, _P]),
     "mce_batch_free": (C.c_int, [_P]),
     "mce_model_create": (C.c_int, [C.c_int32, C.c_uint64, _P]),
     "mce_model_free": (C.c_int, [_P]),
@@ -577,6 +578,23 @@ class Batch:
         st = _Stats()
         _check(_lib.mce_batch_count(self._h, C.byref(o), _ptr(per), C.byref(total), _ptr(hist),
                                     C.byref(st)), "batch_count")
+        return BatchResult(int(total.value), per, hist, _stats_dict(st))
+
+    def count_host(self, row_ptr_addr: int, col_addr: int, vo_addr: int, ao_addr: int,
+                   num_graphs: int, *, stream=None, cuda_graph=1, **opts) -> BatchResult:
+        """Upload from raw host addresses and count in one call
+        (mce_batch_count_host): the copy of each part of the batch overlaps the
+        peeling and orientation of the parts already on the device."""
+        o = make_opts(stream=stream, cuda_graph=cuda_graph, **opts)
+        per = np.zeros(num_graphs, np.uint64)
+        total = C.c_uint64()
+        hist = np.zeros(HIST_MAX, np.uint64)
+        st = _Stats()
+        _check(_lib.mce_batch_count_host(self._h, C.c_void_p(row_ptr_addr), C.c_void_p(col_addr),
+                                         C.c_void_p(vo_addr), C.c_void_p(ao_addr), num_graphs,
+                                         C.byref(o), _ptr(per), C.byref(total), _ptr(hist),
+                                         C.byref(st)), "batch_count_host")
+        self.num_graphs = num_graphs
         return BatchResult(int(total.value), per, hist, _stats_dict(st))
 
     def close(self) -> None:

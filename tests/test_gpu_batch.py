@@ -59,3 +59,54 @@ def test_batch_with_empty_and_tiny_graphs():
         r = db.count()
     assert list(r.per_graph) == [0, 1, oracle.count(graphs[2])[0]]
 
+
+
+def _count_host(db, b, **kw):
+    rp, col, vo, ao = mce.Batch._arrays(b)
+    return db.count_host(rp.ctypes.data, col.ctypes.data, vo.ctypes.data, ao.ctypes.data,
+                         b.num_graphs, **kw)
+
+
+@pytest.mark.parametrize("seed", [3, 4])
+def test_batch_count_host_in_parts(seed):
+    # > 2^20 arcs: copied in four parts, each rebased, peeled and oriented on arrival
+    b = mce.gen_chung_lu_batch(160, 64, 8192, 2.3, 8, 32, 5, 5, 40, seed)
+    assert b.m >= 1 << 20
+    with mce.Batch(b) as db:
+        ref = db.count()
+        small = mce.gen_chung_lu_batch(6, 64, 512, 2.3, 8, 16, 2, 5, 12, 9)  # one part
+        for _ in range(2):  # replay of the captured search after a parted upload
+            h = _count_host(db, b)
+            assert np.array_equal(h.per_graph, ref.per_graph) and h.total == ref.total
+            assert np.array_equal(h.hist, ref.hist)
+            assert h.stats["tree_nodes"] == ref.stats["tree_nodes"]
+            assert h.stats["degeneracy"] == ref.stats["degeneracy"]
+        hs = _count_host(db, small)
+        assert np.array_equal(hs.per_graph, per_graph_oracle(small))
+        for kw in ({"cuda_graph": 0}, {"sched": mce.SCHED_DEGREE}, {"worker_list": mce.WL_OFF}):
+            h = _count_host(db, b, **kw)
+            assert np.array_equal(h.per_graph, ref.per_graph), kw
+        again = db.count()  # the resident batch after the parted upload
+    assert np.array_equal(again.per_graph, ref.per_graph)
+    want = per_graph_oracle(mce.gen_chung_lu_batch(16, 64, 8192, 2.3, 8, 32, 5, 5, 40, seed))
+    assert np.array_equal(ref.per_graph[:16], want)
+
+
+def test_batch_count_host_uneven_parts():
+    # one graph holds most arcs and empty graphs sit at the part edges
+    big = mce.gen_er(60000, 0.0006, 5)
+    graphs = [mce.from_edges(np.array([], np.int64), np.array([], np.int64), 3), big,
+              mce.from_edges(np.array([], np.int64), np.array([], np.int64), 0),
+              mce.gen_er(200, 0.05, 6), mce.from_edges(np.array([0]), np.array([1]), 2)]
+    rp = np.concatenate([g.row_ptr[:g.n + 1] for g in graphs]).astype(np.int32)
+    col = np.concatenate([g.col for g in graphs]).astype(np.int32)
+    vo = np.cumsum([0] + [g.n + 1 for g in graphs]).astype(np.int64)
+    ao = np.cumsum([0] + [g.m for g in graphs]).astype(np.int64)
+    hb = mce.HostGraph(rp, col, int(sum(g.n for g in graphs)), int(col.size), len(graphs), vo, ao)
+    assert hb.m >= 1 << 20
+    with mce.Batch(hb) as db:
+        ref = db.count()
+        h = _count_host(db, hb)
+    assert np.array_equal(h.per_graph, ref.per_graph) and h.total == ref.total
+    assert list(h.per_graph[[0, 2, 4]]) == [0, 0, 1]
+    assert h.per_graph[3] == oracle.count(graphs[3])[0]
