@@ -47,21 +47,10 @@ __global__ void __launch_bounds__(ORIENT_BLOCK) orient_kernel(OrientArgs a) {
     const int32_t b = a.rp[v], e = a.rp[v + 1];
     const uint32_t pv = a.prio[v];
     int32_t cntE = 0;
-    for (int32_t j0 = b; j0 < e; j0 += 32) {
-      const int32_t j = j0 + (int32_t)lane;
-      bool earlier = false;
-      if (j < e) {
-        const int32_t u = a.col[j];
-        const uint32_t pu = a.prio[u];
-        earlier = !(pv == pu ? v < u : pv < pu);
-      }
-      cntE += __popc(__ballot_sync(MCE_FULL, earlier));
-    }
-    const int32_t sp = b + cntE;
-    int32_t eo = b, lo = sp;
-    for (int32_t j0 = b; j0 < e; j0 += 32) {
-      const int32_t j = j0 + (int32_t)lane;
-      bool later = false, valid = j < e;
+    if (e - b <= 32) {  // the whole row in one window: one gather, one pass
+      const int32_t j = b + (int32_t)lane;
+      const bool valid = j < e;
+      bool later = false;
       int32_t u = 0;
       if (valid) {
         u = a.col[j];
@@ -70,15 +59,42 @@ __global__ void __launch_bounds__(ORIENT_BLOCK) orient_kernel(OrientArgs a) {
       }
       const uint32_t mL = __ballot_sync(MCE_FULL, valid && later);
       const uint32_t mE = __ballot_sync(MCE_FULL, valid && !later);
-      if (valid) {
-        if (later)
-          a.cs[lo + __popc(mL & lt)] = u;
-        else
-          a.cs[eo + __popc(mE & lt)] = u;
+      cntE = __popc(mE);
+      if (valid) a.cs[later ? b + cntE + __popc(mL & lt) : b + __popc(mE & lt)] = u;
+    } else {
+      for (int32_t j0 = b; j0 < e; j0 += 32) {
+        const int32_t j = j0 + (int32_t)lane;
+        bool earlier = false;
+        if (j < e) {
+          const int32_t u = a.col[j];
+          const uint32_t pu = a.prio[u];
+          earlier = !(pv == pu ? v < u : pv < pu);
+        }
+        cntE += __popc(__ballot_sync(MCE_FULL, earlier));
       }
-      eo += __popc(mE);
-      lo += __popc(mL);
+      int32_t eo = b, lo = b + cntE;
+      for (int32_t j0 = b; j0 < e; j0 += 32) {
+        const int32_t j = j0 + (int32_t)lane;
+        bool later = false, valid = j < e;
+        int32_t u = 0;
+        if (valid) {
+          u = a.col[j];
+          const uint32_t pu = a.prio[u];
+          later = pv == pu ? v < u : pv < pu;
+        }
+        const uint32_t mL = __ballot_sync(MCE_FULL, valid && later);
+        const uint32_t mE = __ballot_sync(MCE_FULL, valid && !later);
+        if (valid) {
+          if (later)
+            a.cs[lo + __popc(mL & lt)] = u;
+          else
+            a.cs[eo + __popc(mE & lt)] = u;
+        }
+        eo += __popc(mE);
+        lo += __popc(mL);
+      }
     }
+    const int32_t sp = b + cntE;
     if (lane == 0) {
       a.split[v] = sp;
       const uint32_t dplus = (uint32_t)(e - sp), dminus = (uint32_t)cntE;
