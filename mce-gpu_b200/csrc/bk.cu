@@ -128,7 +128,9 @@ __global__ void __launch_bounds__(REG_BLOCK, (NR == 1 && sizeof(Word) == 4) ? 6 
 template <int EV = 0, int MINB = 1, bool LIST = false>
 __global__ void __launch_bounds__(MEM_BLOCK, MINB) bk_mem_kernel(BKArgs a, int cls) {
   __shared__ MemSmem sm_all[MEM_BLOCK / 32];
+  __shared__ u64 srows_all[MEM_BLOCK / 32][2 * MEM_SROWS_D];
   MemSmem &sm = sm_all[threadIdx.x >> 5];
+  u64 *srows = srows_all[threadIdx.x >> 5];
   const int lane = (int)lane_id();
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const Slab sl = slab_of(a, gw);
@@ -146,7 +148,7 @@ __global__ void __launch_bounds__(MEM_BLOCK, MINB) bk_mem_kernel(BKArgs a, int c
     if (i0 >= end - beg) break;
     const int32_t r = a.roots[beg + i0];
     MCE_BD(BD_ENCODE);
-    mem_encode(a, sm, sl, r, rt);
+    mem_encode(a, sm, sl, r, rt, srows);
     MCE_BD(BD_OTHER);
     if (rt.d == 0) continue;
     const int Wr = rt.Wr;
@@ -192,7 +194,7 @@ __global__ void __launch_bounds__(MEM_BLOCK, MINB) bk_mem_kernel(BKArgs a, int c
           }
           __syncwarp();
           MCE_BD(BD_ENCODE);
-          if (r != rt.r) mem_encode(a, sm, sl, r, rt);
+          if (r != rt.r) mem_encode(a, sm, sl, r, rt, srows);
           MCE_BD(BD_QUEUE);
           if (rt.d == 0) return;
           const int Wr = rt.Wr;
@@ -394,7 +396,14 @@ int bk_warps_for_class(int cls, int sms, int wide_blocks, int *warps, int *block
   } else {
     *block = MEM_BLOCK;
     *smem = 0;
-    per_sm = wide_blocks == 8 ? 8 : 4;
+    // the variant's resident blocks per SM (its registers decide), at most 4 or 8
+    if (wide_blocks == 8)
+      MCE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bk_mem_kernel<0, 8>, MEM_BLOCK, 0));
+    else
+      MCE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bk_mem_kernel<>, MEM_BLOCK, 0));
+    const int cap = wide_blocks == 8 ? 8 : 4;
+    if (per_sm > cap) per_sm = cap;
+    if (per_sm < 1) per_sm = 1;
     *warps = sms * per_sm * (MEM_BLOCK / 32);
   }
   return MCE_OK;

@@ -876,9 +876,15 @@ __device__ __forceinline__ int wide_find(const Slab &sl, int pc, int32_t w) {
 struct MemRoot {
   int32_t r = -1;
   int d = 0, Wr = 0, nX = 0;
+  const u64 *rows = nullptr;  // the induced rows: shared memory when d+ <= MEM_SROWS_D, else the slab
 };
 
-__device__ void mem_encode(const BKArgs &a, MemSmem &sm, const Slab &sl, int32_t r, MemRoot &rt) {
+// Roots of the wide engine with at most this many later neighbours keep their
+// induced rows (<= 2 words each) in shared memory, read at every pivot.
+constexpr int MEM_SROWS_D = 128;
+
+__device__ void mem_encode(const BKArgs &a, MemSmem &sm, const Slab &sl, int32_t r, MemRoot &rt,
+                           u64 *srows = nullptr) {
   const int lane = (int)lane_id();
   const uint32_t lt = (1u << lane) - 1u;
   const int32_t sb = a.split[r], d = a.rp[r + 1] - sb, ub = a.rp[r], u = sb - ub;
@@ -893,7 +899,8 @@ __device__ void mem_encode(const BKArgs &a, MemSmem &sm, const Slab &sl, int32_t
   const int Wr = (d + 63) >> 6;
   rt.Wr = Wr;
   int32_t *pl = sl.pl;
-  u64 *rows = sl.rows;
+  u64 *rows = (srows && d <= MEM_SROWS_D) ? srows : sl.rows;  // srows: 2 * MEM_SROWS_D words
+  rt.rows = rows;
   const int pc = p_cap(d);
   for (int i = lane; i < d; i += 32) pl[i] = a.cs[sb + i];
   for (int i = lane; i < d * Wr; i += 32) rows[i] = 0;
@@ -1038,7 +1045,7 @@ __device__ void mem_tree(const BKArgs &a, const Slab &sl, const MemRoot &rt, u64
   const int lane = (int)lane_id();
   const uint32_t lt = (1u << lane) - 1u;
   const int d = rt.d, Wr = rt.Wr, nX = rt.nX;
-  const u64 *rows = sl.rows;
+  const u64 *rows = rt.rows;
   const bool share = a.q.hdr != nullptr;
   u64 *F0 = sl.stk;
   // pivot of the start node
@@ -1124,9 +1131,11 @@ __device__ void mem_tree(const BKArgs &a, const Slab &sl, const MemRoot &rt, u64
     u64 *C = F + 4 * Wr;
     int pc = 0;
     bool xnz = false;
+    u64 pcw = 0, xcw = 0;
     if (lane < Wr) {
       const u64 rw = rows[(size_t)v * Wr + lane];
-      const u64 pcw = Fp[lane] & rw, xcw = Fx[lane] & rw;
+      pcw = Fp[lane] & rw;
+      xcw = Fx[lane] & rw;
       C[lane] = pcw;
       C[Wr + lane] = xcw;
       C[3 * Wr + lane] = Fs[lane] | (lane == vw ? vbit : 0ull);
@@ -1156,17 +1165,34 @@ __device__ void mem_tree(const BKArgs &a, const Slab &sl, const MemRoot &rt, u64
     MCE_BD(BD_PIVOT);
     int k = 0;
     bool el = false, nc = false;  // nc: a vertex of P' misses another one
-    for (int uu = lane; uu < d; uu += 32) {
-      const int uw = uu >> 6;
-      const u64 ub2 = 1ull << (uu & 63);
-      const bool inP = (C[uw] & ub2) != 0, inX = (C[Wr + uw] & ub2) != 0;
-      if (!(inP || inX)) continue;
-      int s = 0;
-      const u64 *ru = rows + (size_t)uu * Wr;
-      for (int w = 0; w < Wr; ++w) s += __popcll(C[w] & ru[w]);
-      k = max(k, ((s + 1) << 11) | (2047 - uu));
-      el = el || (inX && s == pc);
-      nc = nc || (inP && s != pc - 1);
+    if (Wr <= 2) {  // P' and X' words from the lanes that made them, no frame loads
+      const u64 p0 = __shfl_sync(MCE_FULL, pcw, 0), p1 = __shfl_sync(MCE_FULL, pcw, 1);
+      const u64 x0 = __shfl_sync(MCE_FULL, xcw, 0), x1 = __shfl_sync(MCE_FULL, xcw, 1);
+      for (int uu = lane; uu < d; uu += 32) {
+        const int sh = uu & 63;
+        const bool inP = (((uu < 64 ? p0 : p1) >> sh) & 1ull) != 0;
+        const bool inX = (((uu < 64 ? x0 : x1) >> sh) & 1ull) != 0;
+        if (!(inP || inX)) continue;
+        const u64 *ru = rows + (size_t)uu * Wr;
+        int s = __popcll(p0 & ru[0]);
+        if (Wr == 2) s += __popcll(p1 & ru[1]);
+        k = max(k, ((s + 1) << 11) | (2047 - uu));
+        el = el || (inX && s == pc);
+        nc = nc || (inP && s != pc - 1);
+      }
+    } else {
+      for (int uu = lane; uu < d; uu += 32) {
+        const int uw = uu >> 6;
+        const u64 ub2 = 1ull << (uu & 63);
+        const bool inP = (C[uw] & ub2) != 0, inX = (C[Wr + uw] & ub2) != 0;
+        if (!(inP || inX)) continue;
+        int s = 0;
+        const u64 *ru = rows + (size_t)uu * Wr;
+        for (int w = 0; w < Wr; ++w) s += __popcll(C[w] & ru[w]);
+        k = max(k, ((s + 1) << 11) | (2047 - uu));
+        el = el || (inX && s == pc);
+        nc = nc || (inP && s != pc - 1);
+      }
     }
     const uint32_t vote = __reduce_or_sync(MCE_FULL, (el ? 1u : 0u) | (nc ? 2u : 0u));
     if (vote & 1u) continue;
