@@ -64,17 +64,35 @@ constexpr uint32_t SOLO_ROUNDS = 65536;
 // the slot and the chunk base, so bases increase with the slot.
 constexpr int32_t HEAVY_DEG = 256;
 
-// warp-aggregated append of `pred` items to list[*cnt]
-__device__ __forceinline__ void warp_append(bool pred, int32_t val, int32_t *list,
-                                            uint32_t *cnt) {
-  const uint32_t mask = __ballot_sync(MCE_FULL, pred);
-  if (!mask) return;
+// A warp's staging buffer for the next frontier: appends gather here and
+// reach the list STAGE at a time, one atomic on its counter per flush
+// instead of one per 32-edge window (the counter is shared by the grid).
+constexpr uint32_t STAGE = 256;
+struct Stage {
+  int32_t *buf;  // STAGE entries of shared memory, one buffer per warp
+  uint32_t n;    // warp-uniform fill
+};
+
+__device__ __forceinline__ void stage_flush(Stage &st, int32_t *list, uint32_t *cnt) {
+  if (!st.n) return;
   const uint32_t lane = lane_id();
   uint32_t base = 0;
-  const int leader = __ffs(mask) - 1;
-  if ((int)lane == leader) base = atomicAdd(cnt, (uint32_t)__popc(mask));
-  base = __shfl_sync(MCE_FULL, base, leader);
-  if (pred) list[base + __popc(mask & ((1u << lane) - 1u))] = val;
+  if (lane == 0) base = atomicAdd(cnt, st.n);
+  base = __shfl_sync(MCE_FULL, base, 0);
+  for (uint32_t i = lane; i < st.n; i += 32) list[base + i] = st.buf[i];
+  __syncwarp();
+  st.n = 0;
+}
+
+__device__ __forceinline__ void stage_append(Stage &st, bool pred, int32_t val, int32_t *list,
+                                             uint32_t *cnt) {
+  const uint32_t mask = __ballot_sync(MCE_FULL, pred);
+  if (!mask) return;
+  const uint32_t k = __popc(mask);
+  if (st.n + k > STAGE) stage_flush(st, list, cnt);
+  if (pred) st.buf[st.n + __popc(mask & ((1u << lane_id()) - 1u))] = val;
+  __syncwarp();
+  st.n += k;
 }
 
 // Block-aggregated appends to two lists (one atomic per list per block);
@@ -152,8 +170,9 @@ __device__ __forceinline__ void peel_round(uint32_t q, int32_t level, uint32_t p
                                            const int32_t *__restrict__ rp,
                                            const int32_t *__restrict__ col, int32_t *deg,
                                            int32_t *core, uint32_t *prio, int32_t *const *fr,
-                                           int32_t *const *hb, PeelCtl *ctl) {
+                                           int32_t *const *hb, PeelCtl *ctl, int32_t *stage) {
   const uint32_t lane = lane_id();
+  Stage st{stage, 0};
   const int fn = (q + 1) % 3;
   if (t0 == 0) {
     ctl->fcnt[(q + 2) % 3] = 0;
@@ -170,7 +189,7 @@ __device__ __forceinline__ void peel_round(uint32_t q, int32_t level, uint32_t p
     int32_t du = 0;
     if (p) du = rp[u + 1] - rp[u];
     const bool heavy = p && du > HEAVY_DEG;
-    warp_append(p && !heavy, u, Fn, &ctl->fcnt[fn]);
+    stage_append(st, p && !heavy, u, Fn, &ctl->fcnt[fn]);
     heavy_append(heavy, u, du, Fn, HBn, cap, &ctl->hpack[fn]);
   };
   // light vertices: a warp each
@@ -201,6 +220,7 @@ __device__ __forceinline__ void peel_round(uint32_t q, int32_t level, uint32_t p
     const bool p = peel_edge(j, e, level, col, deg, core, u);
     push(p, u);
   }
+  stage_flush(st, Fn, &ctl->fcnt[fn]);
 }
 
 __global__ void __launch_bounds__(PEEL_BLOCK)
@@ -209,6 +229,8 @@ __global__ void __launch_bounds__(PEEL_BLOCK)
                 int32_t *alistA, int32_t *alistB, int32_t *front0, int32_t *front1,
                 int32_t *front2, int32_t *hb0, int32_t *hb1, int32_t *hb2, PeelCtl *ctl,
                 uint64_t limit_ns, uint32_t solo_max) {
+  __shared__ int32_t stage_all[PEEL_BLOCK / 32][STAGE];
+  int32_t *const stage = stage_all[threadIdx.x >> 5];
   const uint32_t nblocks = gridDim.x;
   const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t nthr = (int64_t)gridDim.x * blockDim.x;
@@ -324,7 +346,7 @@ __global__ void __launch_bounds__(PEEL_BLOCK)
           uint32_t it = 0;
           for (;;) {
             peel_round(q, level, priority, threadIdx.x, blockDim.x, (int64_t)n + 1, rp, col,
-                       deg, core, prio, fr, hb, ctl);
+                       deg, core, prio, fr, hb, ctl, stage);
             __syncthreads();
             ++q;
             cnt = frontier_size(ctl, q % 3);
@@ -359,7 +381,7 @@ __global__ void __launch_bounds__(PEEL_BLOCK)
         continue;
       }
       peel_round(q, level, priority, tid, nthr, (int64_t)n + 1, rp, col, deg, core, prio, fr, hb,
-                 ctl);
+                 ctl, stage);
       tick(t_tr);
       if (!grid_sync(&ctl->bar, nblocks, &ctl->err, limit_ns)) return;
       tick(t_w);
