@@ -169,6 +169,11 @@ struct RegSmem {
   int32_t hkey[64 * NR];    // hash of P: vertex id (-1: empty) ...
   uint8_t hidx[64 * NR];    // ... and its index in P
   Word xl0[32];             // the first 32 leaf-filter rows (the rest: slab xl)
+  // Long leaf-filter lists (hub roots) are compacted on the way down: lb is
+  // where the current list starts in the slab (-1: xl0 + xl), and each DFS
+  // frame keeps its list's start and length to return to.
+  int32_t lb;
+  int32_t flb[32 * NR + 1], fln[32 * NR + 1];
 };
 
 // Flattened walk over the concatenated lists of up to 32 items (lane t
@@ -490,6 +495,27 @@ __device__ __forceinline__ int xl_filter(const Word *xr, int nX, Word vb, Word *
   return nL;
 }
 
+// The rows of a leaf-filter list (i < 32 at l0[i], the rest at l1[i]) that
+// contain every vertex of S, appended to dst; returns their number.  Not
+// inlined: only hub roots' long lists take this path, and the search loop
+// keeps its registers.
+template <typename Word>
+__device__ __noinline__ int xl_compact(const Word *l0, const Word *l1, int nL, Word S, Word *dst) {
+  const int lane = (int)lane_id();
+  const uint32_t lt = (1u << lane) - 1u;
+  int k = 0;
+  for (int i0 = 0; i0 < nL; i0 += 32) {
+    const int i = i0 + lane;
+    const Word row = i < nL ? (i < 32 ? l0[i] : l1[i]) : (Word)0;
+    const bool keep = i < nL && (row & S) == S;
+    const uint32_t mk = __ballot_sync(MCE_FULL, keep);
+    if (keep) dst[k + __popc(mk & lt)] = row;
+    k += __popc(mk);
+  }
+  __syncwarp();
+  return k;
+}
+
 // Leaf-filter row i: the first 32 in shared memory, the rest in the slab.
 template <typename Word>
 __device__ __forceinline__ Word xrow(const Word *first32, const Word *rest, int i) {
@@ -599,6 +625,9 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
   // Leaf filter: for the root it is rebuilt at every depth-0 branch (rows
   // adjacent to that branch vertex); for a task it is built once (rows
   // containing the whole chosen set).
+  // List compaction runs in the 64-bit engine, where hub roots' long lists
+  // set the class's length; the 32-bit engine keeps its registers.
+  constexpr bool kCompact = NR == 2;
   const bool per_branch = (S == 0);
   int nL = 0;
   if (!per_branch && nX > 0) {
@@ -613,8 +642,9 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
       }
       nL += __popc(mk);
     }
-    __syncwarp();
   }
+  if (kCompact && lane == 0) sm.lb = -1;
+  __syncwarp();
   // pivot of the start node (select_pivot_from_P / _and_Xp, mce/mce_utils.cuh:338-402)
   int start_k = 0;
   Word start_row = 0;
@@ -670,6 +700,12 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
       X = sm.stk[depth][1];
       B = sm.stk[depth][2];
       S = sm.stk[depth][3];
+      if constexpr (kCompact) {
+        nL = sm.fln[depth];
+        __syncwarp();
+        if (lane == 0) sm.lb = sm.flb[depth];
+        __syncwarp();
+      }
       continue;
     }
     const int v = O::ctz(B);
@@ -696,8 +732,13 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
       // test_maximality (:507-524): P' and X' empty and no earlier
       // neighbour of the root adjacent to the whole clique.
       if (Xc == 0) {
-        bool covered = __any_sync(MCE_FULL, lane < nL && (sm.xl0[lane] & Sc) == Sc);
-        if (!covered && nL > 32) covered = xl_covers<Word>(sl.xl, nL, Sc);
+        bool covered = false;
+        if (nL > 0) {
+          const int lb = kCompact ? sm.lb : -1;
+          const Word *L0 = lb < 0 ? sm.xl0 : sl.xl + lb, *L1 = lb < 0 ? sl.xl : L0;
+          covered = __any_sync(MCE_FULL, lane < nL && (L0[lane] & Sc) == Sc);
+          if (!covered && nL > 32) covered = xl_covers<Word>(L1, nL, Sc);
+        }
         if (!covered) {
           ++cnt;
           if constexpr (LIST) reg_emit<Word, NR>(a, sm, rt.r, Sc);
@@ -741,8 +782,13 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
       // unless an earlier neighbour of the root covers it - the condition
       // under which the outside pivot (XP) ends the walk here instead.
       const Word Sl = Sc | Pc;
-      bool covered = __any_sync(MCE_FULL, lane < nL && (sm.xl0[lane] & Sl) == Sl);
-      if (!covered && nL > 32) covered = xl_covers<Word>(sl.xl, nL, Sl);
+      bool covered = false;
+      if (nL > 0) {
+        const int lb = kCompact ? sm.lb : -1;
+        const Word *L0 = lb < 0 ? sm.xl0 : sl.xl + lb, *L1 = lb < 0 ? sl.xl : L0;
+        covered = __any_sync(MCE_FULL, lane < nL && (L0[lane] & Sl) == Sl);
+        if (!covered && nL > 32) covered = xl_covers<Word>(L1, nL, Sl);
+      }
       if (XP && covered) continue;
       nodes += (u64)pc;
       if (Budget && a.node_budget && nodes > a.node_budget) {
@@ -766,7 +812,9 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
     if constexpr (XP) {  // earlier neighbours adjacent to the whole chosen set
       if (nL > 0) {
         bool elo;
-        ko = outside_pivot(sm.xl0, sl.xl, nL, Sc, Pc, pc, &elo);
+        const int lb = kCompact ? sm.lb : -1;
+        const Word *L0 = lb < 0 ? sm.xl0 : sl.xl + lb, *L1 = lb < 0 ? sl.xl : L0;
+        ko = outside_pivot(L0, L1, nL, Sc, Pc, pc, &elo);
         if (elo) continue;
       }
     }
@@ -796,6 +844,10 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
       sm.stk[depth][1] = X;
       sm.stk[depth][2] = B;
       sm.stk[depth][3] = S;
+      if constexpr (kCompact) {
+        sm.flb[depth] = sm.lb;
+        sm.fln[depth] = nL;
+      }
     }
     __syncwarp();
     ++depth;
@@ -803,10 +855,25 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
     X = Xc;
     S = Sc;
     // apply_pivot_to_next_level (:218-239)
-    if (XP && (ko >> 11) > (k >> 7))
-      B = Pc & ~xrow(sm.xl0, sl.xl, 2047 - (ko & 2047));
-    else
+    if (XP && (ko >> 11) > (k >> 7)) {
+      const int lb = kCompact ? sm.lb : -1;
+      const Word *L0 = lb < 0 ? sm.xl0 : sl.xl + lb, *L1 = lb < 0 ? sl.xl : L0;
+      B = Pc & ~xrow(L0, L1, 2047 - (ko & 2047));
+    } else {
       B = Pc & ~row_of<Word, NR>(r0, r1, 127 - (k & 127));
+    }
+    // a long leaf-filter list keeps only the rows containing the new chosen
+    // set (the reference's Xx compaction, mce/mce_utils.cuh:265-292); a
+    // depth-0 branch's list already holds exactly those for depth 1
+    if (kCompact && nL > 32 && depth >= (per_branch ? 2 : 1)) {
+      const int lb = sm.lb, top = lb < 0 ? nL : lb + nL;
+      if (top + nL <= sl.xc) {
+        const Word *L0 = lb < 0 ? sm.xl0 : sl.xl + lb, *L1 = lb < 0 ? sl.xl : L0;
+        nL = xl_compact<Word>(L0, L1, nL, S, sl.xl + top);
+        if (lane == 0) sm.lb = top;
+        __syncwarp();
+      }
+    }
   }
   MCE_BD(BD_OTHER);
 }
