@@ -110,3 +110,30 @@ def test_batch_count_host_uneven_parts():
     assert np.array_equal(h.per_graph, ref.per_graph) and h.total == ref.total
     assert list(h.per_graph[[0, 2, 4]]) == [0, 0, 1]
     assert h.per_graph[3] == oracle.count(graphs[3])[0]
+
+
+def test_batch_peel_numbering_matches_single_graphs():
+    # The per-graph peel numbers each graph's rounds as a run on that graph
+    # alone: the orientation, hence every tree, equals the single-graph
+    # runs'.  Graphs up to 16,384 vertices are peeled in shared memory, the
+    # 20,000-vertex one in global memory.
+    graphs = [mce.gen_er(20000, 0.0008, 3, 5, 6, 20)]
+    b = mce.gen_chung_lu_batch(12, 64, 16384, 2.3, 8, 32, 5, 5, 40, 17)
+    graphs += [b.graph(i) for i in range(b.num_graphs)]
+    rp = np.concatenate([g.row_ptr[:g.n + 1] for g in graphs]).astype(np.int32)
+    col = np.concatenate([g.col for g in graphs]).astype(np.int32)
+    vo = np.cumsum([0] + [g.n + 1 for g in graphs]).astype(np.int64)
+    ao = np.cumsum([0] + [g.m for g in graphs]).astype(np.int64)
+    hb = mce.HostGraph(rp, col, int(sum(g.n for g in graphs)), int(col.size), len(graphs), vo, ao)
+    single_nodes, single_counts, degen = 0, [], 0
+    for g in graphs:
+        with mce.Graph.from_host(g) as dg:
+            r = dg.count(worker_list=mce.WL_OFF)
+        single_nodes += r.stats["tree_nodes"]
+        single_counts.append(r.total)
+        degen = max(degen, r.stats["degeneracy"])
+    with mce.Batch(hb) as db:
+        rb = db.count(worker_list=mce.WL_OFF)
+    assert list(rb.per_graph) == single_counts
+    assert rb.stats["tree_nodes"] == single_nodes
+    assert rb.stats["degeneracy"] == degen
