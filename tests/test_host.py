@@ -115,6 +115,66 @@ def test_convert_to_bel(tmp_path):
     assert oracle.count(g)[0] == 2  # triangle 012 + edge 13
 
 
+def _scan_llu(line, p):
+    """One strtoull-style %llu conversion at line[p:] (bytes): leading blanks,
+    optional sign, decimal digits, ULLONG_MAX on overflow, '-' negating
+    modulo 2^64.  Returns (value, next position) or None."""
+    while p < len(line) and line[p] in b" \t\v\f\r\n":
+        p += 1
+    neg = False
+    if p < len(line) and line[p] in b"+-":
+        neg = line[p] == ord("-")
+        p += 1
+    q = p
+    while q < len(line) and 48 <= line[q] <= 57:
+        q += 1
+    if q == p:
+        return None
+    x = int(line[p:q])
+    x = 2**64 - 1 if x >= 2**64 else ((-x) % 2**64 if neg else x)
+    return x, q
+
+
+def _convert_model(data):
+    """graph::convert_to_bel's result (include/fileop.h:13-79) for a text
+    file: (n, undirected edges, sorted unique (src, dst) arcs), reading at
+    most the first 65,535 bytes of each line; a NUL byte ends a line's text."""
+    arcs, mx, any_edge = set(), 0, False
+    for raw in data.split(b"\n"):
+        line = raw[:65535].split(b"\0")[0]
+        if not line or not (48 <= line[0] <= 57):
+            continue
+        a = _scan_llu(line, 0)
+        b = _scan_llu(line, a[1]) if a else None
+        if not (a and b) or a[0] == b[0]:
+            continue
+        s, d = a[0], b[0]
+        arcs.add((s & 0xFFFFFFFF, d & 0xFFFFFFFF))
+        arcs.add((d & 0xFFFFFFFF, s & 0xFFFFFFFF))
+        mx, any_edge = max(mx, s, d), True
+    n = ((mx + 1) % 2**64) if any_edge else 1
+    return n if n < 2**63 else n - 2**64, len(arcs) // 2, sorted(arcs)
+
+
+def test_convert_to_bel_line_semantics(tmp_path):
+    data = (b"# comment\n% other\n1 2\n2 3\r\n3\t4\n  5 6\n7 7\n8 +9\n10 -1\n"
+            b"11 99999999999999999999999\n12 4294967308\n13 x\n14 -x\n15\n\n16 17 tail\n"
+            b"0 1\n1 2\n2 1\n18\x0019\n20 21\n"
+            + b"22" + b" " * 70000 + b"23\n"
+            + b"24 25" + b"x" * 70000 + b"\n"
+            + b"#" + b"y" * 70000 + b"\n26 27\n"
+            + b"28 29")
+    txt = tmp_path / "g.txt"
+    txt.write_bytes(data)
+    bel = tmp_path / "g.bel"
+    n, e = mce.convert_to_bel(str(txt), str(bel))
+    want_n, want_e, want_arcs = _convert_model(data)
+    assert (n, e) == (want_n, want_e)
+    rec = np.fromfile(str(bel), np.uint64).reshape(-1, 3)
+    assert [(int(s), int(d)) for d, s, _ in rec] == want_arcs
+    assert all(int(z) == 0 for _, _, z in rec)
+
+
 def test_validate_rejects_asymmetric():
     rp = np.array([0, 1, 1], np.int32)
     col = np.array([1], np.int32)
