@@ -274,8 +274,45 @@ struct HubSmem {
   int32_t hkey[128];  // hash of the hub's later list: vertex id (-1: empty) ...
   uint8_t hidx[128];  // ... and its index in the list
   u64 xs[32];         // the rows of the current 32 earlier neighbours
-  int32_t off[32], beg[32], own[32];  // flat_walk scratch
+  int32_t off[32], beg[32], own[64];  // flattened-walk scratch (two windows)
 };
+
+// flat_walk (engine.cuh) two windows at a time: the two elements of a lane
+// are loaded together, so a warp keeps two reads of the lists in flight.
+template <typename F>
+__device__ __forceinline__ void flat_walk2(const int32_t *__restrict__ cs, int32_t b, int len,
+                                           int32_t *off_sm, int32_t *beg_sm, int32_t *own_sm,
+                                           F f) {
+  const int lane = (int)lane_id();
+  const int incl = warp_incl_scan(len);
+  const int T = __shfl_sync(MCE_FULL, incl, 31);
+  const int off = incl - len;
+  off_sm[lane] = off;
+  beg_sm[lane] = b;
+  int carry = 0;
+  for (int e0 = 0; e0 < T; e0 += 64) {
+    const bool stA = len > 0 && off >= e0 && off < e0 + 32;
+    const bool stB = len > 0 && off >= e0 + 32 && off < e0 + 64;
+    if (stA) own_sm[off - e0] = lane;
+    if (stB) own_sm[off - e0] = lane;  // 32 .. 63: window B
+    const uint32_t mA = __reduce_or_sync(MCE_FULL, stA ? 1u << (off - e0) : 0u);
+    const uint32_t mB = __reduce_or_sync(MCE_FULL, stB ? 1u << (off - e0 - 32) : 0u);
+    __syncwarp();
+    const uint32_t keep = 0xFFFFFFFFu >> (31 - lane);
+    const uint32_t bA = mA & keep, bB = mB & keep;
+    const int tA = bA ? own_sm[31 - __clz(bA)] : carry;
+    const int cA = __shfl_sync(MCE_FULL, tA, 31);
+    const int tB = bB ? own_sm[32 + 31 - __clz(bB)] : cA;
+    carry = __shfl_sync(MCE_FULL, tB, 31);
+    const int eA = e0 + lane, eB = e0 + 32 + lane;
+    int32_t wA = -1, wB = -1;
+    if (eA < T) wA = cs[beg_sm[tA] + (eA - off_sm[tA])];
+    if (eB < T) wB = cs[beg_sm[tB] + (eB - off_sm[tB])];
+    if (eA < T) f(tA, wA);
+    if (eB < T) f(tB, wB);
+    __syncwarp();
+  }
+}
 
 __device__ __forceinline__ uint32_t hub_slot(int32_t w) { return ((uint32_t)w * 0x9E3779B1u) >> 25; }
 
@@ -326,7 +363,7 @@ __global__ void __launch_bounds__(HUB_BLOCK) hub_rows_kernel(
     }
     sm.xs[lane] = 0;
     __syncwarp();
-    flat_walk(cs, xb, xlen, sm.off, sm.beg, sm.own, [&](int t, int32_t w) {
+    flat_walk2(cs, xb, xlen, sm.off, sm.beg, sm.own, [&](int t, int32_t w) {
       uint32_t h = hub_slot(w);
       for (;;) {
         const int32_t k = sm.hkey[h];
