@@ -105,6 +105,7 @@ struct ServeArgs {
 
 struct Arena {
   int32_t *hkey, *hval, *hfirst, *V, *rp, *col, *split, *cs, *deg, *core, *fa, *fb, *off;
+  int32_t *rs;  // resident-row start of each row being walked (row_offsets)
   uint32_t *prio, *err;
   unsigned long long *hist;  // clique sizes above the engines' register bins
 };
@@ -131,6 +132,7 @@ __host__ __device__ inline size_t arena_layout(int ego_cap, int arc_cap, int hca
   x.fa = (int32_t *)take(4 * (size_t)ego_cap);
   x.fb = (int32_t *)take(4 * (size_t)ego_cap);
   x.off = (int32_t *)take(4 * ((size_t)ego_cap + 1));
+  x.rs = (int32_t *)take(4 * ((size_t)ego_cap + 1));
   x.prio = (uint32_t *)take(4 * (size_t)ego_cap);
   x.err = (uint32_t *)take(4);
   x.hist = (unsigned long long *)take(8 * (size_t)MCE_HIST_MAX);
@@ -237,16 +239,19 @@ __device__ __forceinline__ int block_max_scan(int x, int *ws) {
 }
 
 // off[0 .. nrows] = exclusive prefix of the resident-row lengths of the
-// vertices list[0 .. nrows); returns the total.
+// vertices list[0 .. nrows), rs[i] = where row i starts in the resident
+// graph (a window's elements then need one load less); returns the total.
 __device__ int row_offsets(const ServeArgs &S, const int32_t *list, int nrows, int32_t *off,
-                           SvShared &sh) {
+                           int32_t *rs, SvShared &sh) {
   int base = 0;
   for (int i0 = 0; i0 < nrows; i0 += blockDim.x) {
     const int i = i0 + (int)threadIdx.x;
     int len = 0;
     if (i < nrows) {
       const int32_t g = list[i];
-      len = S.grp[g + 1] - S.grp[g];
+      const int32_t r0 = S.grp[g];
+      len = S.grp[g + 1] - r0;
+      rs[i] = r0;
     }
     int ex;
     const int tot = block_scan(len, &ex, sh.ws);
@@ -291,7 +296,7 @@ __device__ int window_owner(const int32_t *off, int nrows, int e0, int carry, in
 __device__ void ego_discover(const ServeArgs &S, const Arena &A, const int32_t *list, int nrows,
                              int32_t *own_sm, SvShared &sh) {
   const int cap = S.ego_cap, hc = S.hcap;
-  const int T = row_offsets(S, list, nrows, A.off, sh);
+  const int T = row_offsets(S, list, nrows, A.off, A.rs, sh);
   int carry = -1, ia = 0, ib = 0;
   for (int e0 = 0; e0 < T; e0 += blockDim.x, ia = ib) {
     const int k = sh.k;  // read by all before thread 0 updates it below
@@ -302,8 +307,7 @@ __device__ void ego_discover(const ServeArgs &S, const Arena &A, const int32_t *
     uint32_t slot = 0;
     bool cand = false;
     if (e < T) {
-      const int32_t g = list[o];
-      w = S.gcol[S.grp[g] + (e - A.off[o])];
+      w = S.gcol[A.rs[o] + (e - A.off[o])];
       hput(A, hc, w, &slot);  // inserts or finds the vertex
       cand = A.hval[slot] == SV_PENDING;
       if (cand) atomicMin(&A.hfirst[slot], e);
@@ -369,16 +373,13 @@ __device__ int ego_extract(const ServeArgs &S, const Arena &A, int64_t seed, int
   // induced rows in one flattened pass: the i-th kept element overall is
   // col[i] (rows in order, each filtered row stays sorted), and a row starts
   // at the count of kept elements before its first one
-  const int T = row_offsets(S, A.V, n, A.off, sh);
+  const int T = row_offsets(S, A.V, n, A.off, A.rs, sh);
   int carry = -1, kept = 0, ia = 0, ib = 0;
   for (int e0 = 0; e0 < T; e0 += blockDim.x, ia = ib) {
     const int o = window_owner(A.off, n, e0, carry, ia, ib, own_sm, sh);
     const int e = e0 + (int)threadIdx.x;
     int32_t loc = -1;
-    if (e < T) {
-      const int32_t g = A.V[o];
-      loc = hget(A, hc, S.gcol[S.grp[g] + (e - A.off[o])]);
-    }
+    if (e < T) loc = hget(A, hc, S.gcol[A.rs[o] + (e - A.off[o])]);
     int pos;
     const int tot = block_scan(loc >= 0 ? 1 : 0, &pos, sh.ws);
     if (loc >= 0 && kept + pos < S.arc_cap) A.col[kept + pos] = loc;
