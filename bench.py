@@ -46,6 +46,32 @@ METRIC = "maximal cliques/s (exact count), batched+learned vs plain on 1 B200; p
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "parallel_mce_on_gpus")
 
 
+# ---- ranks (one process per GPU, replicas of the same workload) ------------
+def max_over_ranks(values, device):
+    """Each value's maximum over the ranks: a step takes as long as its
+    slowest rank.  Without a process group, the values themselves."""
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    if torch.distributed.is_available() and torch.distributed.is_initialized():
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return [float(x) for x in t.cpu()]
+
+
+def sum_over_ranks(values, device):
+    """Each value summed over the ranks (throughputs of independent replicas)."""
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    if torch.distributed.is_available() and torch.distributed.is_initialized():
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.SUM)
+    return [float(x) for x in t.cpu()]
+
+
+def job_value(units_per_rank, ms, world):
+    """Whole-job throughput of `world` replicas that each finish
+    `units_per_rank` units within `ms` (the slowest rank's time)."""
+    return world * units_per_rank / (ms / 1e3)
+
+
 def parse_args():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -331,9 +357,7 @@ def run_mine(args, rank, world, local_rank):
 
     # max over ranks
     if world > 1:
-        t = torch.tensor([step_ms, e2e_ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        step_ms, e2e_ms = float(t[0]), float(t[1])
+        step_ms, e2e_ms = max_over_ranks([step_ms, e2e_ms], "cuda")
     if rank != 0:
         dg.close()
         return None
@@ -357,7 +381,7 @@ def run_mine(args, rank, world, local_rank):
         pass
     line = {
         "metric": METRIC,
-        "value": world * total / (step_ms / 1e3),
+        "value": job_value(total, step_ms, world),
         "unit": "maximal cliques/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": step_ms,
@@ -376,7 +400,7 @@ def run_mine(args, rank, world, local_rank):
                        tasks_shared=stats[-1]["donations"],
                        settings={k: kw.get(k) for k in mce.TUNED_FIELDS},
                        tuning=tuning),
-        "e2e": {"value": world * total / (e2e_ms / 1e3), "unit": "maximal cliques/s",
+        "e2e": {"value": job_value(total, e2e_ms, world), "unit": "maximal cliques/s",
                 "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h + 8 * 4096 + 64 + 8 + 4 + 128),
                 "ms_per_step": e2e_ms, "path": e2e_path},
@@ -526,9 +550,9 @@ def run_serve(args, rank, world, local_rank):
     finally:
         s.close()
         g.close()
-    vals = torch.tensor([cliques / wall, wall], dtype=torch.float64, device="cuda")
+    vals = [cliques / wall, wall]
     if world > 1:
-        torch.distributed.all_reduce(vals[:1], op=torch.distributed.ReduceOp.SUM)
+        vals[0] = sum_over_ranks([vals[0]], "cuda")[0]
     if rank != 0:
         return None
     dev_ms = res["device_ns"][ok] / 1e6
