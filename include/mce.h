@@ -104,6 +104,10 @@ typedef struct mce_opts {
                                phase (read both with mce_warp_log)           */
   int32_t wide_blocks;      /* 0 = default (4): blocks per SM of the wide
                                engine (d+ > 64); 8 = its 64-register variant */
+  int32_t wait_limit_ms;    /* 0 = default (30 s): a search warp waiting for
+                               subtrees gives up after this long without
+                               progress anywhere and the call returns
+                               MCE_ETIMEOUT (the device stays usable)       */
   void *stream;             /* cudaStream_t to queue work on; NULL = own      */
   void *model;              /* mce_model_t for MCE_SCHED_LEARNED (NULL: the
                                degree heuristic is used instead)              */

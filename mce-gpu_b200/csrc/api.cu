@@ -90,7 +90,7 @@ struct mce_graph {
   cudaEvent_t part_fork = nullptr, part_done[4] = {nullptr};
   // search launches captured as a CUDA graph, replayed while the key matches
   cudaGraphExec_t search_exec = nullptr;
-  unsigned char search_key[256] = {0};
+  unsigned char search_key[320] = {0};
 };
 
 namespace {
@@ -741,7 +741,7 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   a.hub_nx = g->hub_nx;
   a.donate_min = o.donate_threshold > 0 ? o.donate_threshold : DEFAULT_DONATE_MIN;
   a.donate_after = o.donate_after > 0 ? (uint32_t)o.donate_after : DEFAULT_DONATE_AFTER;
-  a.wait_limit_ns = IDLE_LIMIT_NS;
+  a.wait_limit_ns = o.wait_limit_ms > 0 ? (uint64_t)o.wait_limit_ms * 1000000ull : IDLE_LIMIT_NS;
   a.policy = policy;
   a.wide8 = o.wide_blocks == 8 ? 1 : 0;
   a.level2 = o.level == MCE_LEVEL_L2 ? 1 : 0;
@@ -762,6 +762,7 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
     int grid[NCLS], block[NCLS];
     int dcap, xcap, rxcap, wbits, share, dmin, log, wide8, level2, xpiv;
     uint32_t dafter;
+    uint64_t wlimit;
     const void *slab, *graph_count, *graph_of, *root_nodes, *policy, *q[NCLS], *bufs[4], *wlog;
     const void *hub[4];
     int64_t n, G;
@@ -779,6 +780,7 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   key.share = share;
   key.dmin = a.donate_min;
   key.dafter = a.donate_after;
+  key.wlimit = a.wait_limit_ns;
   key.log = o.log_roots != 0;
   key.wide8 = a.wide8;
   key.level2 = a.level2;

@@ -47,7 +47,7 @@ class _Opts(C.Structure):
                 ("peel_solo_max", C.c_int32), ("donate_after", C.c_int32),
                 ("cuda_graph", C.c_int32), ("heavy_log2", C.c_int32),
                 ("share_log2", C.c_int32), ("warp_log", C.c_int32), ("wide_blocks", C.c_int32),
-                ("stream", C.c_void_p), ("model", C.c_void_p)]
+                ("wait_limit_ms", C.c_int32), ("stream", C.c_void_p), ("model", C.c_void_p)]
 
 
 class _Stats(C.Structure):
@@ -363,7 +363,7 @@ def _stats_dict(st: _Stats) -> dict:
 def make_opts(*, sched=SCHED_PLAIN, bitmap_width=0, log_roots=False, level=LEVEL_L1,
               induced=INDUCED_P, worker_list=WL_ON, donate_threshold=0, x_pivot=0,
               peel_solo_max=0, donate_after=0, cuda_graph=0, heavy_log2=0, share_log2=0,
-              warp_log=False, wide_blocks=0, model=None, stream=None) -> _Opts:
+              warp_log=False, wide_blocks=0, wait_limit_ms=0, model=None, stream=None) -> _Opts:
     o = _Opts()
     _lib.mce_opts_default(C.byref(o))
     o.sched, o.bitmap_width, o.log_roots = sched, bitmap_width, int(bool(log_roots))
@@ -372,6 +372,7 @@ def make_opts(*, sched=SCHED_PLAIN, bitmap_width=0, log_roots=False, level=LEVEL
     o.peel_solo_max, o.donate_after, o.cuda_graph = peel_solo_max, donate_after, cuda_graph
     o.heavy_log2, o.share_log2, o.warp_log = heavy_log2, share_log2, int(warp_log)
     o.wide_blocks = wide_blocks
+    o.wait_limit_ms = wait_limit_ms
     o.stream = stream
     o.model = model._h if model is not None else None
     return o
