@@ -166,8 +166,8 @@ struct RegSmem {
   int32_t off[32];          // flattened-walk prefix offsets of the items' lists
   int32_t beg[32];          // ... and the lists' starts
   int32_t own[32];          // ... and the item whose list starts at a window position
-  int32_t hkey[64 * NR];    // hash of P: vertex id (-1: empty) ...
-  uint8_t hidx[64 * NR];    // ... and its index in P
+  int32_t hkey[128];        // hash of P (128 slots for up to 32 * NR ids): vertex id (-1: empty) ...
+  uint8_t hidx[128];        // ... and its index in P
   Word xl0[32];             // the first 32 leaf-filter rows (the rest: slab xl)
   // Long leaf-filter lists (hub roots) are compacted on the way down: lb is
   // where the current list starts in the slab (-1: xl0 + xl), and each DFS
@@ -206,16 +206,18 @@ __device__ __forceinline__ void flat_walk(const int32_t *__restrict__ cs, int32_
   }
 }
 
-// Hash of the root's later neighbours (ids are distinct): 2x slots.
+// Hash of the root's later neighbours (ids are distinct): 128 slots, so that
+// the probes of the many later-list elements outside P end within ~1.4 slots
+// for the 32-bit engine (4 slots per id) and ~2.5 for the 64-bit one (2).
 template <typename Word, int NR>
 __device__ __forceinline__ uint32_t p_slot(int32_t w) {
-  return ((uint32_t)w * 0x9E3779B1u) >> (NR == 2 ? 25 : 26);
+  return ((uint32_t)w * 0x9E3779B1u) >> 25;
 }
 
 template <typename Word, int NR>
 __device__ __forceinline__ void p_hash_build(RegSmem<Word, NR> &sm, int d) {
   const int lane = (int)lane_id();
-  for (int i = lane; i < 64 * NR; i += 32) sm.hkey[i] = -1;
+  for (int i = lane; i < 128; i += 32) sm.hkey[i] = -1;
   __syncwarp();
 #pragma unroll
   for (int k = 0; k < NR; ++k) {
@@ -223,7 +225,7 @@ __device__ __forceinline__ void p_hash_build(RegSmem<Word, NR> &sm, int d) {
     if (i < d) {
       const int32_t w = sm.pl[i];
       uint32_t h = p_slot<Word, NR>(w);
-      while (atomicCAS(&sm.hkey[h], -1, w) != -1) h = (h + 1) & (64 * NR - 1);
+      while (atomicCAS(&sm.hkey[h], -1, w) != -1) h = (h + 1) & 127u;
       sm.hidx[h] = (uint8_t)i;
     }
   }
@@ -238,7 +240,7 @@ __device__ __forceinline__ int p_find(const RegSmem<Word, NR> &sm, int32_t w) {
     const int32_t k = sm.hkey[h];
     if (k == w) return sm.hidx[h];
     if (k == -1) return -1;
-    h = (h + 1) & (64 * NR - 1);
+    h = (h + 1) & 127u;
   }
 }
 
