@@ -271,8 +271,8 @@ __global__ void __launch_bounds__(HUB_BLOCK) hub_offsets_kernel(
 }
 
 struct HubSmem {
-  int32_t hkey[128];  // hash of the hub's later list: vertex id (-1: empty) ...
-  uint8_t hidx[128];  // ... and its index in the list
+  int32_t hkey[256];  // hash of the hub's later list (<= 64 ids): vertex id (-1: empty) ...
+  uint8_t hidx[256];  // ... and its index in the list
   u64 xs[32];         // the rows of the current 32 earlier neighbours
   int32_t off[32], beg[32], own[64];  // flattened-walk scratch (two windows)
 };
@@ -314,7 +314,7 @@ __device__ __forceinline__ void flat_walk2(const int32_t *__restrict__ cs, int32
   }
 }
 
-__device__ __forceinline__ uint32_t hub_slot(int32_t w) { return ((uint32_t)w * 0x9E3779B1u) >> 25; }
+__device__ __forceinline__ uint32_t hub_slot(int32_t w) { return ((uint32_t)w * 0x9E3779B1u) >> 24; }
 
 // Each warp takes a contiguous range of 32-row chunks; the hash of a hub's
 // later list (d+ <= 64) is rebuilt when the range moves to the next hub.
@@ -342,12 +342,12 @@ __global__ void __launch_bounds__(HUB_BLOCK) hub_rows_kernel(
       j = lo;
       cur = hub_list[j];
       const int32_t sb = split[cur], d = rp[cur + 1] - sb;
-      for (int i = lane; i < 128; i += 32) sm.hkey[i] = -1;
+      for (int i = lane; i < 256; i += 32) sm.hkey[i] = -1;
       __syncwarp();
       for (int i = lane; i < d; i += 32) {  // the later list's ids are distinct
         const int32_t w = cs[sb + i];
         uint32_t h = hub_slot(w);
-        while (atomicCAS(&sm.hkey[h], -1, w) != -1) h = (h + 1) & 127u;
+        while (atomicCAS(&sm.hkey[h], -1, w) != -1) h = (h + 1) & 255u;
         sm.hidx[h] = (uint8_t)i;
       }
       __syncwarp();
@@ -372,7 +372,7 @@ __global__ void __launch_bounds__(HUB_BLOCK) hub_rows_kernel(
           break;
         }
         if (k == -1) break;
-        h = (h + 1) & 127u;
+        h = (h + 1) & 255u;
       }
     });
     __syncwarp();
