@@ -267,3 +267,18 @@ def test_tune_table_lookup(tmp_path):
     assert mce.tune_lookup(str(t), "n14-a4-k6")["wide_blocks"] == 8
     t.write_text("# mce autotune table v3\nn14-a4-k6 2 1024 10 32 -1 8 1 800.0 1100.0\n")
     assert mce.tune_lookup(str(t), "n14-a4-k6")["x_pivot"] == 1
+
+
+def test_device_file_paths_fail_loudly_without_a_device(tmp_path):
+    # no silent host fallback: the device converter and loader report MCE_ENODEV
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is visible")
+    txt = tmp_path / "g.txt"
+    txt.write_text("0 1\n1 2\n")
+    with pytest.raises(mce.MceError) as e:
+        mce.convert_to_bel(str(txt), str(tmp_path / "g.bel"), device=0)
+    assert e.value.code == mce.ENODEV
+    with pytest.raises(mce.MceError) as e:
+        mce.Graph.load_text(str(txt))
+    assert e.value.code == mce.ENODEV
