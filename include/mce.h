@@ -76,7 +76,13 @@ typedef struct mce_opts {
   int32_t sched;            /* MCE_SCHED_*                                    */
   int32_t bitmap_width;     /* 0 = auto; 32 or 64: word width of the rows of
                                roots with at most 32 later neighbours          */
-  int32_t warps_per_root;   /* 0 = auto; 1 = one warp per root               */
+  int32_t warps_per_root;   /* 0 = auto (1); k = 1..32: each root is searched
+                               by k warps, warp j taking the root's
+                               first-level branches j, j+k, j+2k, ... (the
+                               same tree, split by its first level; the
+                               counterpart of the reference's PSIZE lanes per
+                               candidate, src/main.cu:158-165).  Buckets
+                               without their own value use this one         */
   int32_t donate_threshold; /* 0 = default (10, the reference's SZTH,
                                mce/parameter.cuh:5): smallest candidate set a
                                subtree must have to be donated                 */
@@ -108,6 +114,20 @@ typedef struct mce_opts {
                                subtrees gives up after this long without
                                progress anywhere and the call returns
                                MCE_ETIMEOUT (the device stays usable)       */
+  int32_t count_ops;        /* 1 = run the counting variants of the engines:
+                               mce_stats_t.word_ops gets the algorithmic
+                               32-bit word operations of the IP walk (per
+                               root too with log_roots, mce_root_ops); not
+                               with x_pivot, warp_log or mce_list (MCE_EINVAL).
+                               Same counts and trees; slower (a measurement
+                               run, not a timed one)                        */
+  /* Per bucket of roots - the engine classes, by bitmap width: [0] roots
+   * with d+ <= 32 (one 32- or 64-bit row per lane), [1] 33..64 (two 64-bit
+   * rows per lane), [2] wider (rows in a slab) - the settings above for that
+   * bucket alone; 0 = the value above.  The autotuner fills them.         */
+  int32_t bucket_warps_per_root[3];
+  int32_t bucket_donate_threshold[3];
+  int32_t bucket_donate_after[3];
   void *stream;             /* cudaStream_t to queue work on; NULL = own      */
   void *model;              /* mce_model_t for MCE_SCHED_LEARNED (NULL: the
                                degree heuristic is used instead)              */
@@ -136,6 +156,13 @@ typedef struct mce_stats {
   double peel_scan_ms;      /* peel time split as seen by one block: level    */
   double peel_round_ms;     /* scans, round work, and waits at grid barriers  */
   double peel_wait_ms;
+  uint64_t word_ops;        /* opts.count_ops: algorithmic 32-bit word ops of
+                               the search, W = ceil(d+/32) words per row:
+                               2W per candidate of every pivot selection
+                               (AND + POPC, mce/mce_utils.cuh:338-402) + 4W per
+                               tree node for the child sets (:321-336)       */
+  double class_ms[4];       /* search launch time per engine class: 32-bit
+                               rows (d+ <= 32), 64-bit rows (33..64), wide   */
 } mce_stats_t;
 
 /* ---- host graphs -------------------------------------------------------- */
@@ -279,6 +306,13 @@ int mce_root_log(mce_graph_t g, uint64_t *nodes_out);
  * opts.log_roots = 1 (n entries, 0 for non-roots).                          */
 int mce_root_counts(mce_graph_t g, uint64_t *count_out);
 
+/* Per-root algorithmic word operations (mce_stats_t.word_ops, split by
+ * root) of the last mce_count that ran with opts.log_roots = 1 and
+ * opts.count_ops = 1 (n entries); MCE_ESTATE otherwise.  No counterpart in
+ * the reference; it measures the work of the reference's walk
+ * (mce/mce_utils.cuh:321-402) root by root.                                */
+int mce_root_ops(mce_graph_t g, uint64_t *ops_out);
+
 /* Per-warp load of the last mce_count that ran with opts.warp_log >= 1: for
  * every search warp (all engine classes, widest class first) the SM it ran
  * on, the search-tree nodes it walked (its roots and the subtrees it took)
@@ -394,18 +428,22 @@ int mce_model_grad(mce_model_t m, const float *X, const float *Y, int64_t count,
  * implicit device synchronisation is not acceptable.
  *
  * Inputs (device pointers, caller-owned): d_row_ptr (n+1), d_split (n) and
- * d_col_split (m) - the oriented CSR that mce_split_csr returns - and
- * d_roots (num_roots vertex ids).  Output: d_hist (MCE_HIST_MAX uint64,
- * device) receives the number of maximal cliques of each size found from
- * those roots; the call zeroes it first.  Every root must have 1 to 32
- * later and at most 1024 earlier neighbours; otherwise nothing is searched
- * and MCE_ELIMIT is returned.  Work is queued on `stream` (NULL = legacy
- * default stream) and the call waits for it.  The call uses the
- * MCE_NOALLOC_SCRATCH_BYTES array: the first call on a device looks up that
- * array's address (make it before any stream capture), and calls that
- * overlap on the GPU race on the array, so serialise them.                   */
+ * d_col_split (m) - the oriented CSR that mce_split_csr returns - with its
+ * vertex count n, and d_roots (num_roots vertex ids).  Output: d_hist
+ * (MCE_HIST_MAX uint64, device) receives the number of maximal cliques of
+ * each size found from those roots (zeroed by the call once the roots have
+ * passed its checks; left untouched when it returns an error).  A root id
+ * outside [0, n) is caught before anything is read at it: nothing is
+ * searched and MCE_EINVAL is returned.  Every root must have 1 to 32 later
+ * and at most 1024 earlier neighbours; otherwise nothing is searched and
+ * MCE_ELIMIT is returned.  Work is queued on `stream` (NULL = legacy default
+ * stream) and the call synchronises that stream twice before it returns, so
+ * it cannot be captured into a CUDA graph.  The call uses the
+ * MCE_NOALLOC_SCRATCH_BYTES array (its address on the current device is
+ * looked up on every call); calls that overlap on the GPU race on the
+ * array, so serialise them.                                                  */
 int mce_count_oriented_noalloc(const int32_t *d_row_ptr, const int32_t *d_split,
-                               const int32_t *d_col_split, const int32_t *d_roots,
+                               const int32_t *d_col_split, int64_t n, const int32_t *d_roots,
                                int64_t num_roots, uint64_t *d_hist, void *stream);
 
 /* ---- autotuner ------------------------------------------------------------ */

@@ -69,6 +69,7 @@ struct mce_graph {
   uint32_t *fetch = nullptr, *err = nullptr;
   unsigned long long *hist = nullptr, *nodes = nullptr;
   unsigned long long *root_nodes = nullptr, *root_count = nullptr;
+  unsigned long long *root_ops = nullptr;  // per-root word operations (opts.count_ops)
   unsigned long long *wlog = nullptr;     // per-warp {SM, nodes, donations} (opts.warp_log)
   int64_t wlog_cap = 0, wlog_count = 0;
   float *feat = nullptr, *pred = nullptr;  // per-vertex features (n x 8) and predicted cost
@@ -80,10 +81,12 @@ struct mce_graph {
   void *qbuf[NCLS] = {nullptr};   // task queue per engine class
   size_t qbytes[NCLS] = {0};
   bool logged = false;
+  bool logged_ops = false;
   // host copies of the last call
   ShapeInfo shape_h{};
   int32_t degeneracy = 0;
   cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t cls_ev[3][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};
   // a batch arriving in parts: one stream per part, forked from and joined
   // to the caller's stream
   cudaStream_t part_s[4] = {nullptr};
@@ -111,7 +114,7 @@ void free_graph_bufs(mce_graph *g) {
   dfree(g->keys_in); dfree(g->keys_out); dfree(g->vals_in); dfree(g->roots);
   dfree(g->hub_of); dfree(g->hub_list); dfree(g->hub_off); dfree(g->hub_rows); dfree(g->hub_nx);
   g->hub_off_cap = g->hub_rows_cap = 0;
-  dfree(g->root_nodes); dfree(g->root_count);
+  dfree(g->root_nodes); dfree(g->root_count); dfree(g->root_ops);
   dfree(g->feat); dfree(g->pred); dfree(g->policy); dfree(g->wlog); dfree(g->cand);
   dfree(g->cand_n);
   g->cap_n = g->cap_m = -1;
@@ -144,6 +147,8 @@ int alloc_fixed_bufs(mce_graph *g) {
       (rc = dalloc(&g->hist, MCE_HIST_MAX)) || (rc = dalloc(&g->nodes, 4)))
     return rc;
   for (auto &e : g->ev) MCE_CUDA(cudaEventCreate(&e));
+  for (auto &pr : g->cls_ev)
+    for (auto &e : pr) MCE_CUDA(cudaEventCreate(&e));
   return MCE_OK;
 }
 
@@ -497,6 +502,9 @@ int mce_graph_free(mce_graph_t g) {
   if (g->search_exec) cudaGraphExecDestroy(g->search_exec);
   for (auto &e : g->ev)
     if (e) cudaEventDestroy(e);
+  for (auto &pr : g->cls_ev)
+    for (auto &e : pr)
+      if (e) cudaEventDestroy(e);
   for (int p = 0; p < 4; ++p) {
     if (g->part_s[p]) cudaStreamDestroy(g->part_s[p]);
     if (g->part_done[p]) cudaEventDestroy(g->part_done[p]);
@@ -614,6 +622,14 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
                mce_stats_t *stats, const BatchCtx *bc, const ListCtx *lc = nullptr) {
   if (o.bitmap_width != 0 && o.bitmap_width != 32 && o.bitmap_width != 64) return MCE_EINVAL;
   if (o.wide_blocks != 0 && o.wide_blocks != 4 && o.wide_blocks != 8) return MCE_EINVAL;
+  // the word-op count follows the IP walk; it is not an evaluation or listing run
+  if (o.count_ops && (o.x_pivot || o.induced == MCE_INDUCED_PX || o.warp_log || lc))
+    return MCE_EINVAL;
+  if (o.warps_per_root < 0 || o.warps_per_root > 32) return MCE_EINVAL;
+  for (int c = 0; c < 3; ++c)
+    if (o.bucket_warps_per_root[c] < 0 || o.bucket_warps_per_root[c] > 32 ||
+        o.bucket_donate_threshold[c] < 0 || o.bucket_donate_after[c] < 0)
+      return MCE_EINVAL;
   MCE_CUDA(cudaSetDevice(g->device));
   cudaStream_t s = pick_stream(g, o.stream);
   int launches = 0, rc;
@@ -686,14 +702,25 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   int rxcap = REG_XCAP;  // a power of two covering the register classes' earlier degrees
   while (rxcap < (int)sh.max_dminus_reg && rxcap < REG_XCAP_MAX) rxcap <<= 1;
   size_t slab_need = 0;
+  // per bucket (engine class): warps per root, donation threshold and gate
+  int parts[NCLS] = {1, 1, 1, 1, 1}, dmin[NCLS] = {0}, dafter[NCLS] = {0};
+  for (int c = CLS_R32; c <= CLS_MEM; ++c) {
+    const int w = o.bucket_warps_per_root[c] ? o.bucket_warps_per_root[c] : o.warps_per_root;
+    parts[c] = w > 1 ? w : 1;
+    const int t = o.bucket_donate_threshold[c] ? o.bucket_donate_threshold[c] : o.donate_threshold;
+    dmin[c] = t > 0 ? t : DEFAULT_DONATE_MIN;
+    const int af = o.bucket_donate_after[c] ? o.bucket_donate_after[c] : o.donate_after;
+    dafter[c] = af > 0 ? af : (int)DEFAULT_DONATE_AFTER;
+  }
   for (int c = CLS_R32; c <= CLS_MEM; ++c) {
     if (!sh.cls_cnt[c]) continue;
     int warps = 0;
     if ((rc = bk_warps_for_class(c, g->sms, o.wide_blocks, &warps, &block[c], &smem[c]))) return rc;
-    // never more warps than roots (rounded up to whole blocks); with task
-    // sharing keep at least a full wave so idle warps can take subtrees
+    // never more warps than units of work (a root's parts; rounded up to
+    // whole blocks); with task sharing keep at least a full wave so idle
+    // warps can take subtrees
     const int wpb = block[c] / 32;
-    int64_t want = (int64_t)sh.cls_cnt[c];
+    int64_t want = (int64_t)sh.cls_cnt[c] * parts[c];
     if (share) want = want > warps ? want : warps;
     if (want < warps) warps = (int)((want + wpb - 1) / wpb) * wpb;
     grid[c] = warps / wpb;
@@ -705,6 +732,8 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
     if ((rc = dalloc(&g->root_nodes, (size_t)g->cap_n + 1))) return rc;
     if ((rc = dalloc(&g->root_count, (size_t)g->cap_n + 1))) return rc;
   }
+  const bool log_ops = o.log_roots && o.count_ops;
+  if (log_ops && !g->root_ops && (rc = dalloc(&g->root_ops, (size_t)g->cap_n + 1))) return rc;
   int64_t wlog_base[NCLS] = {0}, wlog_total = 0;
   for (int c : {CLS_MEM, CLS_R64, CLS_R32}) {  // the launch order below
     wlog_base[c] = wlog_total;
@@ -739,13 +768,16 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   a.hub_off = g->hub_off;
   a.hub_rows = g->hub_rows;
   a.hub_nx = g->hub_nx;
-  a.donate_min = o.donate_threshold > 0 ? o.donate_threshold : DEFAULT_DONATE_MIN;
-  a.donate_after = o.donate_after > 0 ? (uint32_t)o.donate_after : DEFAULT_DONATE_AFTER;
+  a.donate_min = dmin[CLS_R32];  // set per class at each launch below
+  a.donate_after = (uint32_t)dafter[CLS_R32];
   a.wait_limit_ns = o.wait_limit_ms > 0 ? (uint64_t)o.wait_limit_ms * 1000000ull : IDLE_LIMIT_NS;
   a.policy = policy;
   a.wide8 = o.wide_blocks == 8 ? 1 : 0;
   a.level2 = o.level == MCE_LEVEL_L2 ? 1 : 0;
   a.x_pivot = (o.x_pivot || o.induced == MCE_INDUCED_PX) ? 1 : 0;
+  a.count_ops = o.count_ops ? 1 : 0;
+  a.ops = g->nodes + 1;
+  a.root_ops = log_ops ? g->root_ops : nullptr;
   if (lc) {
     a.list_buf = lc->buf;
     a.list_words = lc->words;
@@ -760,8 +792,8 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   // opts.cuda_graph it is captured once and replayed.
   struct SearchKey {
     int grid[NCLS], block[NCLS];
-    int dcap, xcap, rxcap, wbits, share, dmin, log, wide8, level2, xpiv;
-    uint32_t dafter;
+    int dcap, xcap, rxcap, wbits, share, log, wide8, level2, xpiv, ops;
+    int parts[NCLS], dmin[NCLS], dafter[NCLS];
     uint64_t wlimit;
     const void *slab, *graph_count, *graph_of, *root_nodes, *policy, *q[NCLS], *bufs[4], *wlog;
     const void *hub[4];
@@ -778,13 +810,17 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   key.rxcap = rxcap;
   key.wbits = wbits;
   key.share = share;
-  key.dmin = a.donate_min;
-  key.dafter = a.donate_after;
+  for (int c = 0; c < NCLS; ++c) {
+    key.parts[c] = parts[c];
+    key.dmin[c] = dmin[c];
+    key.dafter[c] = dafter[c];
+  }
   key.wlimit = a.wait_limit_ns;
   key.log = o.log_roots != 0;
   key.wide8 = a.wide8;
   key.level2 = a.level2;
   key.xpiv = a.x_pivot;
+  key.ops = a.count_ops + (log_ops ? 2 : 0);
   key.slab = g->slab;
   key.graph_count = a.graph_count;
   key.root_nodes = a.root_nodes;
@@ -802,12 +838,21 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   key.n = g->n;
   key.G = bc ? bc->G : 0;
   static_assert(sizeof(SearchKey) <= sizeof(g->search_key), "search key");
+  // per-class launch times: plain event records, or external event nodes
+  // while the launches are being captured
+  bool capturing = false;
+  auto mark = [&](cudaEvent_t e) {
+    return capturing ? cudaEventRecordWithFlags(e, s, cudaEventRecordExternal)
+                     : cudaEventRecord(e, s);
+  };
   auto record = [&]() -> int {
     int r2;
     if (o.log_roots) {
       MCE_CUDA(cudaMemsetAsync(g->root_nodes, 0, sizeof(unsigned long long) * (size_t)(g->n + 1), s));
       MCE_CUDA(cudaMemsetAsync(g->root_count, 0, sizeof(unsigned long long) * (size_t)(g->n + 1), s));
     }
+    if (log_ops)
+      MCE_CUDA(cudaMemsetAsync(g->root_ops, 0, sizeof(unsigned long long) * (size_t)(g->n + 1), s));
     if (bc) MCE_CUDA(cudaMemsetAsync(bc->graph_count, 0, sizeof(unsigned long long) * bc->G, s));
     MCE_CUDA(cudaMemsetAsync(g->fetch, 0, sizeof(uint32_t) * 8, s));
     MCE_CUDA(cudaMemsetAsync(g->err, 0, sizeof(uint32_t) * 4, s));
@@ -822,11 +867,16 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
     for (int c : order) {
       if (!grid[c]) continue;
       a.slab_words = bk_slab_words(c, dcap, xcap, rxcap);
+      a.parts = parts[c];
+      a.donate_min = dmin[c];
+      a.donate_after = (uint32_t)dafter[c];
       a.q = share ? qv[c] : QueueView();
       a.warp_log = o.warp_log ? g->wlog + WLOG_WORDS * wlog_base[c] : nullptr;
       a.warp_cycles = o.warp_log == 2 ? 1 : 0;
       if (share && (r2 = queue_launch_init(a.q, s, &launches))) return r2;
+      MCE_CUDA(mark(g->cls_ev[c][0]));
       if ((r2 = bk_launch(c, wbits, a, grid[c], block[c], smem[c], s, &launches))) return r2;
+      MCE_CUDA(mark(g->cls_ev[c][1]));
     }
     return MCE_OK;
   };
@@ -839,7 +889,9 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
       cudaGraph_t graph = nullptr;
       MCE_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
       const int lc = launches;
+      capturing = true;
       rc = record();
+      capturing = false;
       cudaError_t e = cudaStreamEndCapture(s, &graph);
       launches = lc;
       if (rc) {
@@ -862,10 +914,10 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   }
   MCE_CUDA(cudaEventRecord(g->ev[3], s));
   unsigned long long h_hist[MCE_HIST_MAX];
-  unsigned long long h_nodes = 0;
+  unsigned long long h_nodes[2] = {0, 0};
   uint32_t h_err = 0;
   MCE_CUDA(cudaMemcpyAsync(h_hist, g->hist, sizeof(h_hist), cudaMemcpyDeviceToHost, s));
-  MCE_CUDA(cudaMemcpyAsync(&h_nodes, g->nodes, sizeof(h_nodes), cudaMemcpyDeviceToHost, s));
+  MCE_CUDA(cudaMemcpyAsync(h_nodes, g->nodes, sizeof(h_nodes), cudaMemcpyDeviceToHost, s));
   MCE_CUDA(cudaMemcpyAsync(&h_err, g->err, sizeof(h_err), cudaMemcpyDeviceToHost, s));
   QueueHdr qh[NCLS];
   bool qused[NCLS] = {false};
@@ -884,6 +936,7 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   if (g->n > 0 && (rc = peel_read(g->peel_ctl, &dg, &perr, &rounds, &solo, s, pms))) return rc;
   g->degeneracy = dg;
   g->logged = o.log_roots != 0;
+  g->logged_ops = log_ops;
   uint64_t pushed = 0;
   for (int c = 0; c < NCLS; ++c)
     if (qused[c]) pushed += qh[c].pushed;
@@ -901,11 +954,15 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   st.count_ms = ms;
   cudaEventElapsedTime(&ms, g->ev[0], g->ev[4]);
   st.total_ms = ms;
+  for (int c = CLS_R32; c <= CLS_MEM; ++c)
+    if (grid[c] && cudaEventElapsedTime(&ms, g->cls_ev[c][0], g->cls_ev[c][1]) == cudaSuccess)
+      st.class_ms[c] = ms;
   st.degeneracy = dg;
   st.max_later_degree = (int32_t)sh.max_dplus;
   st.max_degree = sh.max_deg;
   st.roots = (int64_t)sh.cls_cnt[CLS_R32] + sh.cls_cnt[CLS_R64] + sh.cls_cnt[CLS_MEM];
-  st.tree_nodes = h_nodes;
+  st.tree_nodes = h_nodes[0];
+  st.word_ops = o.count_ops ? h_nodes[1] : 0;
   st.kernel_launches = launches;
   st.error_flags = h_err | (perr ? MCE_ERR_WAIT_TIMEOUT : 0);
   for (int c = 0; c < NCLS && c < 8; ++c) st.class_roots[c] = sh.cls_cnt[c];
@@ -1008,6 +1065,15 @@ int mce_warp_log(mce_graph_t g, uint32_t *sm_out, uint64_t *nodes_out, uint64_t 
     if (cycles_out)
       for (int p = 0; p < 7; ++p) cycles_out[7 * i + p] = r[3 + p];
   }
+  return MCE_OK;
+}
+
+int mce_root_ops(mce_graph_t g, uint64_t *ops_out) {
+  if (!g || !ops_out) return MCE_EINVAL;
+  if (!g->logged_ops || !g->root_ops) return MCE_ESTATE;
+  MCE_CUDA(cudaSetDevice(g->device));
+  MCE_CUDA(cudaMemcpy(ops_out, g->root_ops, sizeof(uint64_t) * (size_t)g->n,
+                      cudaMemcpyDeviceToHost));
   return MCE_OK;
 }
 

@@ -45,7 +45,9 @@ namespace {
 // 64-bit engine 4.
 // EV (opts.warp_log): 0 none, 1 per-warp load and donations, 2 plus the
 // per-phase cycle breakdown.
-template <typename Word, int NR, int EV = 0, bool LIST = false, bool XP = false>
+// OPS (opts.count_ops): the variant that sums the algorithmic word
+// operations of every walk (reg_tree / mem_tree), run outside timed calls.
+template <typename Word, int NR, int EV = 0, bool LIST = false, bool XP = false, bool OPS = false>
 __global__ void __launch_bounds__(REG_BLOCK, (NR == 1 && sizeof(Word) == 4) ? 6 : (NR == 2 ? 4 : 1))
     bk_reg_kernel(BKArgs a, int cls) {
   __shared__ RegSmem<Word, NR> sm_all[REG_BLOCK / 32];
@@ -55,28 +57,37 @@ __global__ void __launch_bounds__(REG_BLOCK, (NR == 1 && sizeof(Word) == 4) ? 6 
   const RegSlab<Word> sl = reg_slab<Word>(a, gw);
   const uint32_t beg = a.shape->cls_off[cls], end = a.shape->cls_off[cls + 1];
   const bool share = a.q.hdr != nullptr;
-  u64 h0 = 0, h1 = 0, nodes = 0;
+  u64 h0 = 0, h1 = 0, nodes = 0, ops = 0;
   RegRoot<Word> rt;
   Bd bdv, *bd = &bdv;
   if constexpr (EV == 2) bdv.start();
   if (share && lane == 0) atomicAdd(&a.q.hdr->work, 1u);
+  // units of work: (root, part) pairs, the parts of a root fetched one
+  // after the other so that different warps take them
+  const uint32_t parts = a.parts > 1 ? (uint32_t)a.parts : 1u;
+  const uint32_t units = (end - beg) * parts;
   for (;;) {
     uint32_t i0 = 0;
     if (lane == 0) i0 = atomicAdd(&a.fetch[cls], (uint32_t)REG_CHUNK);
     i0 = __shfl_sync(MCE_FULL, i0, 0);
-    if (i0 >= end - beg) break;
+    if (i0 >= units) break;
     for (int k = 0; k < REG_CHUNK; ++k) {
-      const uint32_t idx = beg + i0 + k;
-      if (idx >= end) break;
-      const int32_t r = a.roots[idx];
+      const uint32_t u = i0 + k;
+      if (u >= units) break;
+      const int32_t r = a.roots[beg + u / parts];
       MCE_BD(BD_ENCODE);
-      reg_encode<Word, NR>(a, sm, sl, r, rt);
+      if (parts == 1 || r != rt.r) reg_encode<Word, NR>(a, sm, sl, r, rt);
       MCE_BD(BD_OTHER);
-      u64 nd = 0, cnt = 0;
-      reg_tree<Word, NR, false, EV, LIST, XP>(a, sm, sl, rt, WOps<Word>::low(rt.d), (Word)0,
-                                               (Word)0, h0, h1, nd, cnt, bd);
+      u64 nd = 0, cnt = 0, op = 0;
+      reg_tree<Word, NR, false, EV, LIST, XP, OPS>(a, sm, sl, rt, WOps<Word>::low(rt.d), (Word)0,
+                                                    (Word)0, h0, h1, nd, cnt, bd, &op,
+                                                    (int)(u % parts), (int)parts);
       nodes += nd;
       root_done(a, r, nd, cnt);
+      if constexpr (OPS) {
+        ops += op;
+        root_ops_done(a, r, op);
+      }
     }
   }
   if (share) {
@@ -102,10 +113,15 @@ __global__ void __launch_bounds__(REG_BLOCK, (NR == 1 && sizeof(Word) == 4) ? 6 
           const Word S = (Word)__shfl_sync(MCE_FULL, t3, 3);
           MCE_BD(BD_ENCODE);
           if (r != rt.r) reg_encode<Word, NR>(a, sm, sl, r, rt);
-          u64 nd = 0, cnt = 0;
-          reg_tree<Word, NR, false, EV, LIST, XP>(a, sm, sl, rt, P, X, S, h0, h1, nd, cnt, bd);
+          u64 nd = 0, cnt = 0, op = 0;
+          reg_tree<Word, NR, false, EV, LIST, XP, OPS>(a, sm, sl, rt, P, X, S, h0, h1, nd, cnt, bd,
+                                                        &op);
           nodes += nd;
           root_done(a, r, nd, cnt);
+          if constexpr (OPS) {
+            ops += op;
+            root_ops_done(a, r, op);
+          }
           MCE_BD(BD_QUEUE);
         });
   }
@@ -113,6 +129,7 @@ __global__ void __launch_bounds__(REG_BLOCK, (NR == 1 && sizeof(Word) == 4) ? 6 
   if (h0) atomicAdd(&a.hist[lane + 2], h0);
   if (h1) atomicAdd(&a.hist[lane + 34], h1);
   if (lane == 0 && nodes) atomicAdd(a.nodes, nodes);  // warp-uniform count
+  if (OPS && lane == 0 && ops) atomicAdd(a.ops, ops);
   if (EV && lane == 0) {  // opts.warp_log
     u64 *w = warp_record(a);
     w[0] = sm_id();
@@ -125,7 +142,7 @@ __global__ void __launch_bounds__(REG_BLOCK, (NR == 1 && sizeof(Word) == 4) ? 6 
 // The wide engine at 4 blocks per SM (96 registers) or, with
 // opts.wide_blocks = 8, at 8 (64 registers): more warps pay on graphs whose
 // wide roots have large shared subtrees (R-MAT), fewer on many small ones.
-template <int EV = 0, int MINB = 1, bool LIST = false>
+template <int EV = 0, int MINB = 1, bool LIST = false, bool OPS = false>
 __global__ void __launch_bounds__(MEM_BLOCK, MINB) bk_mem_kernel(BKArgs a, int cls) {
   __shared__ MemSmem sm_all[MEM_BLOCK / 32];
   __shared__ u64 srows_all[MEM_BLOCK / 32][2 * MEM_SROWS_D];
@@ -136,19 +153,21 @@ __global__ void __launch_bounds__(MEM_BLOCK, MINB) bk_mem_kernel(BKArgs a, int c
   const Slab sl = slab_of(a, gw);
   const uint32_t beg = a.shape->cls_off[cls], end = a.shape->cls_off[cls + 1];
   const bool share = a.q.hdr != nullptr;
-  u64 h0 = 0, h1 = 0, nodes = 0;
+  u64 h0 = 0, h1 = 0, nodes = 0, ops = 0;
   MemRoot rt;
   Bd bdv, *bd = &bdv;
   if constexpr (EV == 2) bdv.start();
   if (share && lane == 0) atomicAdd(&a.q.hdr->work, 1u);
+  const uint32_t parts = a.parts > 1 ? (uint32_t)a.parts : 1u;  // warps per root
+  const uint32_t units = (end - beg) * parts;
   for (;;) {
     uint32_t i0 = 0;
     if (lane == 0) i0 = atomicAdd(&a.fetch[cls], 1u);
     i0 = __shfl_sync(MCE_FULL, i0, 0);
-    if (i0 >= end - beg) break;
-    const int32_t r = a.roots[beg + i0];
+    if (i0 >= units) break;
+    const int32_t r = a.roots[beg + i0 / parts];
     MCE_BD(BD_ENCODE);
-    mem_encode(a, sm, sl, r, rt, srows);
+    if (parts == 1 || r != rt.r) mem_encode(a, sm, sl, r, rt, srows);
     MCE_BD(BD_OTHER);
     if (rt.d == 0) continue;
     const int Wr = rt.Wr;
@@ -159,10 +178,15 @@ __global__ void __launch_bounds__(MEM_BLOCK, MINB) bk_mem_kernel(BKArgs a, int c
       sl.stk[3 * Wr + lane] = 0;
     }
     __syncwarp();
-    u64 nd = 0, cnt = 0;
-    mem_tree<false, EV, LIST>(a, sl, rt, h0, h1, nd, cnt, bd);
+    u64 nd = 0, cnt = 0, op = 0;
+    mem_tree<false, EV, LIST, OPS>(a, sl, rt, h0, h1, nd, cnt, bd, &op, (int)(i0 % parts),
+                                   (int)parts);
     nodes += nd;
     root_done(a, r, nd, cnt);
+    if constexpr (OPS) {
+      ops += op;
+      root_ops_done(a, r, op);
+    }
   }
   if (share) {
     if (lane == 0) {
@@ -204,10 +228,14 @@ __global__ void __launch_bounds__(MEM_BLOCK, MINB) bk_mem_kernel(BKArgs a, int c
             sl.stk[3 * Wr + lane] = ts;
           }
           __syncwarp();
-          u64 nd = 0, cnt = 0;
-          mem_tree<false, EV, LIST>(a, sl, rt, h0, h1, nd, cnt, bd);
+          u64 nd = 0, cnt = 0, op = 0;
+          mem_tree<false, EV, LIST, OPS>(a, sl, rt, h0, h1, nd, cnt, bd, &op);
           nodes += nd;
           root_done(a, r, nd, cnt);
+          if constexpr (OPS) {
+            ops += op;
+            root_ops_done(a, r, op);
+          }
           MCE_BD(BD_QUEUE);
         });
   }
@@ -215,6 +243,7 @@ __global__ void __launch_bounds__(MEM_BLOCK, MINB) bk_mem_kernel(BKArgs a, int c
   if (h0) atomicAdd(&a.hist[lane + 2], h0);
   if (h1) atomicAdd(&a.hist[lane + 34], h1);
   if (lane == 0 && nodes) atomicAdd(a.nodes, nodes);  // warp-uniform count
+  if (OPS && lane == 0 && ops) atomicAdd(a.ops, ops);
   if (EV && lane == 0) {  // opts.warp_log
     u64 *w = warp_record(a);
     w[0] = sm_id();
@@ -469,6 +498,21 @@ int bk_launch(int cls, int word_bits, const BKArgs &a, int grid, int block, int 
     if (launches) *launches += 1;
     return MCE_OK;
   }
+  if (a.count_ops) {  // the counting variants (no evaluation log, IP pivots only)
+    if (cls == CLS_R32 && word_bits == 64)
+      bk_reg_kernel<u64, 1, 0, false, false, true><<<grid, block, smem, s>>>(a, cls);
+    else if (cls == CLS_R32)
+      bk_reg_kernel<uint32_t, 1, 0, false, false, true><<<grid, block, smem, s>>>(a, cls);
+    else if (cls == CLS_R64)
+      bk_reg_kernel<u64, 2, 0, false, false, true><<<grid, block, smem, s>>>(a, cls);
+    else if (cls == CLS_MEM)
+      bk_mem_kernel<0, 1, false, true><<<grid, block, smem, s>>>(a, cls);
+    else
+      return MCE_EINVAL;
+    MCE_CUDA(cudaGetLastError());
+    if (launches) *launches += 1;
+    return MCE_OK;
+  }
   if (a.x_pivot && ev == 0 && cls != CLS_MEM) {  // -i px: pivots also from earlier neighbours
     if (cls == CLS_R32 && word_bits == 64)
       bk_reg_kernel<u64, 1, 0, false, true><<<grid, block, smem, s>>>(a, cls);
@@ -544,11 +588,13 @@ int queue_launch_init(const QueueView &q, cudaStream_t s, int *launches) {
 // per-warp scratch in the file-scope array below, which every GPU that loads
 // this library holds until the process exits.
 //
-// Set-up: the first call on a device (with that device current) resolves the
-// array's device address with cudaGetSymbolAddress and caches it; make that
-// first call before any stream capture.  Every call shares the array and
-// clears the part that must start at zero, so calls whose work overlaps on
-// the GPU race with each other: serialise them (one stream, or events).
+// Every call resolves the array's device address on the current device with
+// cudaGetSymbolAddress, checks the root ids against the vertex count before
+// any read at them, and synchronises its stream twice (the root check, the
+// status), so it cannot be captured into a CUDA graph.  Every call shares
+// the array and clears the part that must start at zero, so calls whose work
+// overlaps on the GPU race with each other: serialise them (one stream, or
+// events).
 // ===========================================================================
 namespace {
 
@@ -566,26 +612,21 @@ struct NoallocCtl {
 };
 static_assert(sizeof(NoallocCtl) <= NOALLOC_CTL_BYTES, "control block");
 
-constexpr int NOALLOC_MAX_DEVICES = 64;
-unsigned long long *g_noalloc_addr[NOALLOC_MAX_DEVICES];  // host cache of device addresses
-bool g_noalloc_ready[NOALLOC_MAX_DEVICES];
-
-int noalloc_scratch(int dev, unsigned long long **out) {
-  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return MCE_ELIMIT;
-  if (!g_noalloc_ready[dev]) {
-    // the host-side name g_noalloc_scratch is not a device address: resolve it
-    void *p = nullptr;
-    MCE_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-    g_noalloc_addr[dev] = (unsigned long long *)p;
-    g_noalloc_ready[dev] = true;
-  }
-  *out = g_noalloc_addr[dev];
+// The host-side name g_noalloc_scratch is not a device address; the address
+// of the current device's copy is looked up on every call (cheap next to the
+// call's two stream synchronisations), so there is no host-side cache to
+// guard between threads or to go stale after a device reset.
+int noalloc_scratch(unsigned long long **out) {
+  void *p = nullptr;
+  MCE_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+  *out = (unsigned long long *)p;
   return MCE_OK;
 }
 
-// Every root must fit the 32-wide engine: 1..32 later and <= REG_XCAP
-// earlier neighbours.  A root outside those limits sets err[0].
-__global__ void noalloc_check_kernel(const int32_t *rp, const int32_t *split,
+// Every root id must lie in [0, n) - tested before anything is read at that
+// id (bit 2 of err[0]) - and fit the 32-wide engine: 1..32 later and
+// <= REG_XCAP earlier neighbours (bit 1).
+__global__ void noalloc_check_kernel(const int32_t *rp, const int32_t *split, int64_t n,
                                      const int32_t *roots, uint32_t num_roots, NoallocCtl *ctl) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (threadIdx.x == 0 && blockIdx.x == 0) {
@@ -594,36 +635,46 @@ __global__ void noalloc_check_kernel(const int32_t *rp, const int32_t *split,
   }
   if (i >= num_roots) return;
   const int32_t r = roots[i];
+  if (r < 0 || (int64_t)r >= n) {
+    atomicOr(&ctl->err[0], 2u);
+    return;
+  }
   const int32_t dplus = rp[r + 1] - split[r], dminus = split[r] - rp[r];
-  if (dplus < 1 || dplus > 32 || dminus > REG_XCAP) atomicOr(&ctl->err[0], MCE_ERR_DEGREE);
+  if (dplus < 1 || dplus > 32 || dminus > REG_XCAP) atomicOr(&ctl->err[0], 1u);
 }
 
 }  // namespace
 
 extern "C" int mce_count_oriented_noalloc(const int32_t *d_row_ptr, const int32_t *d_split,
-                                          const int32_t *d_col_split, const int32_t *d_roots,
-                                          int64_t num_roots, uint64_t *d_hist, void *stream) {
-  if (num_roots < 0 || !d_hist ||
+                                          const int32_t *d_col_split, int64_t n,
+                                          const int32_t *d_roots, int64_t num_roots,
+                                          uint64_t *d_hist, void *stream) {
+  if (num_roots < 0 || n < 0 || !d_hist ||
       (num_roots > 0 && (!d_row_ptr || !d_split || !d_col_split || !d_roots)))
     return MCE_EINVAL;
-  if (num_roots >= ((int64_t)1 << 31)) return MCE_ELIMIT;
+  if (num_roots >= ((int64_t)1 << 31) || n >= ((int64_t)1 << 31)) return MCE_ELIMIT;
   int dev = 0, sms = 0, per_sm = 0;
   MCE_CUDA(cudaGetDevice(&dev));
   unsigned long long *base = nullptr;
-  int rc = noalloc_scratch(dev, &base);
+  int rc = noalloc_scratch(&base);
   if (rc) return rc;
   cudaStream_t s = (cudaStream_t)stream;
   NoallocCtl *ctl = (NoallocCtl *)base;
   MCE_CUDA(cudaMemsetAsync(ctl, 0, NOALLOC_CTL_BYTES, s));
-  MCE_CUDA(cudaMemsetAsync(d_hist, 0, sizeof(uint64_t) * MCE_HIST_MAX, s));
   const uint32_t nr = (uint32_t)num_roots;
-  noalloc_check_kernel<<<(nr + 255) / 256 + 1, 256, 0, s>>>(d_row_ptr, d_split, d_roots, nr, ctl);
+  noalloc_check_kernel<<<(nr + 255) / 256 + 1, 256, 0, s>>>(d_row_ptr, d_split, n, d_roots, nr,
+                                                             ctl);
   MCE_CUDA(cudaGetLastError());
   uint32_t err = 0;
   MCE_CUDA(cudaMemcpyAsync(&err, &ctl->err[0], sizeof(err), cudaMemcpyDeviceToHost, s));
   MCE_CUDA(cudaStreamSynchronize(s));
+  if (err & 2u) return MCE_EINVAL;
   if (err) return MCE_ELIMIT;
-  if (nr == 0) return MCE_OK;
+  MCE_CUDA(cudaMemsetAsync(d_hist, 0, sizeof(uint64_t) * MCE_HIST_MAX, s));
+  if (nr == 0) {
+    MCE_CUDA(cudaStreamSynchronize(s));
+    return MCE_OK;
+  }
   // as many whole blocks of warps as the occupancy, the roots and the array allow
   MCE_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   MCE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bk_reg_kernel<uint32_t, 1>,

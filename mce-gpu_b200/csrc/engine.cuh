@@ -104,6 +104,12 @@ __device__ __forceinline__ void root_done(const BKArgs &a, int32_t r, u64 nodes,
   if (a.graph_count && cnt) atomicAdd(&a.graph_count[a.graph_of[r]], cnt);
 }
 
+// opts.count_ops: the algorithmic 32-bit word operations of a root's (or a
+// task's) walk, per root when roots are logged.
+__device__ __forceinline__ void root_ops_done(const BKArgs &a, int32_t r, u64 ops) {
+  if (lane_id() == 0 && a.root_ops && ops) atomicAdd(&a.root_ops[r], ops);
+}
+
 // Idle phase shared by the engines: take tasks until no work is left.
 // `run(words)` processes one task whose words were stored by `put`.
 template <typename Put, typename Run>
@@ -440,7 +446,10 @@ __device__ void reg_encode(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab
       nX += __popc(mk);
       __syncwarp();
     }
-    if (hrows) {  // rows [0, nX) of the hub's region are no longer read as built
+    // rows [0, nX) of the hub's region are no longer read as built; with
+    // several warps per root two of them may encode the hub at once, so
+    // then the rows stay as built and every warp deduplicates them itself
+    if (hrows && a.parts <= 1) {
       for (int i = lane; i < nX; i += 32) hrows[i] = (u64)sl.xr[i];
       __threadfence();
       __syncwarp();
@@ -580,12 +589,24 @@ __device__ __forceinline__ void reg_emit(const BKArgs &a, const RegSmem<Word, NR
 // Budget, the walk stops once it has visited a.node_budget nodes; with EV
 // (opts.warp_log) >= 1 the warp's donations are counted in its a.warp_log
 // record, with EV == 2 its cycles are charged to *bd by phase.
+//
+// OPS (opts.count_ops) counts the algorithmic work of the reference's walk
+// in 32-bit word operations into *ops, with W = ceil(d+ / 32) words per row
+// whatever the engine's word width: 2W per candidate of a pivot selection
+// (AND + POPC over P' | X', select_pivot_from_P_and_Xp,
+// mce/mce_utils.cuh:366-402) plus 4W per node for the child sets
+// (populate_xl_and_cl, :321-336); a root's first pivot costs 2W per later
+// neighbour (select_pivot_from_P, :338-364).  A donated node is counted by
+// the warp that created it.  The clique shortcuts are off, so every node of
+// the tree is walked (same nodes, counts and histogram).
 template <typename Word, int NR, bool Budget = false, int EV = 0, bool LIST = false,
-          bool XP = false>
+          bool XP = false, bool OPS = false>
 __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<Word> &sl,
                          const RegRoot<Word> &rt, Word P, Word X, Word S, u64 &h0, u64 &h1,
-                         u64 &nodes, u64 &cnt, Bd *bd = nullptr) {
+                         u64 &nodes, u64 &cnt, Bd *bd = nullptr, u64 *ops = nullptr,
+                         int part = 0, int parts = 1) {
   using O = WOps<Word>;
+  const u64 w32 = (u64)((rt.d + 31) >> 5);
   MCE_BD(BD_PIVOT);
   const int lane = (int)lane_id();
   const uint32_t lt = (1u << lane) - 1u;
@@ -596,12 +617,16 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
   // path of d nodes (every pivot leaves exactly itself to branch on) ending
   // in the clique P, which is maximal unless an earlier neighbour of the
   // root is adjacent to all of it.  Same nodes and count, no walk.
-  if constexpr (!XP) {
+  if constexpr (!XP && !OPS) {
     const int d = rt.d;
     if (S == 0 && X == 0 && P == O::low(d) && d > 0) {
       bool full = lane >= d || ((r0 | O::bit(lane)) & P) == P;
       if constexpr (NR == 2) full = full && (lane + 32 >= d || ((r1 | O::bit(lane + 32)) & P) == P);
       if (__all_sync(MCE_FULL, full)) {
+        if (part != 0) {  // one path: part 0 walks it
+          MCE_BD(BD_OTHER);
+          return;
+        }
         bool covered = false;
         for (int i0 = 0; !covered && i0 < nX; i0 += 32) {
           const int i = i0 + lane;
@@ -654,6 +679,8 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
   {
     const Word cand = P | X;
     const int pc = O::popc(P);
+    if constexpr (OPS)
+      if (S == 0 && part == 0) *ops += 2 * w32 * (u64)O::popc(cand);  // the root's first pivot
     int k = 0;
     bool el = false;
     if ((cand >> lane) & 1) {
@@ -691,7 +718,7 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
   MCE_BD(BD_SETS);
   // apply_pivot_to_first_level (:204-216) / apply_pivot_to_next_level (:218-239)
   Word B = P & ~(start_out ? start_row : row_of<Word, NR>(r0, r1, 127 - (start_k & 127)));
-  int depth = 0, recheck = 0;
+  int depth = 0, recheck = 0, b0 = 0;  // b0: first-level branches passed
   bool want = false;
   for (;;) {
     MCE_BD(BD_BRANCH);
@@ -720,7 +747,11 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
     const Word Pc = P & rv, Xc = X & rv, Sc = S | vb;
     P &= ~vb;
     X |= vb;
+    // several warps per root: this one walks every parts-th first-level
+    // branch (the others still move from P to X, as the full walk would)
+    if (parts > 1 && depth == 0 && (b0++ % parts) != part) continue;
     ++nodes;
+    if constexpr (OPS) *ops += 2 * w32 * (u64)O::popc(Pc | Xc) + 4 * w32;
     if (Budget && a.node_budget && nodes > a.node_budget) {  // a serving request over its budget
       if (lane == 0) atomicOr(a.err, MCE_ERR_BUDGET);
       break;
@@ -777,7 +808,7 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
     }
     vote = __reduce_or_sync(MCE_FULL, vote);
     if (vote & 1u) continue;
-    if (vote == 0) {
+    if (!OPS && vote == 0) {
       // P' is a clique and no X' vertex covers it: below this node the walk
       // is one path of |P'| nodes (each pivot leaves one vertex to branch
       // on; X' never covers the shrinking P') ending in S' | P', maximal
@@ -1107,13 +1138,16 @@ __device__ __forceinline__ void mem_leaf(const BKArgs &a, const Slab &sl, int32_
   }
 }
 
-template <bool Budget = false, int EV = 0, bool LIST = false>
+// OPS: the algorithmic word operations, as in reg_tree.
+template <bool Budget = false, int EV = 0, bool LIST = false, bool OPS = false>
 __device__ void mem_tree(const BKArgs &a, const Slab &sl, const MemRoot &rt, u64 &h0, u64 &h1,
-                         u64 &nodes, u64 &cnt, Bd *bd = nullptr) {
+                         u64 &nodes, u64 &cnt, Bd *bd = nullptr, u64 *ops = nullptr,
+                         int part = 0, int parts = 1) {
   MCE_BD(BD_PIVOT);
   const int lane = (int)lane_id();
   const uint32_t lt = (1u << lane) - 1u;
   const int d = rt.d, Wr = rt.Wr, nX = rt.nX;
+  const u64 w32 = (u64)((d + 31) >> 5);
   const u64 *rows = rt.rows;
   const bool share = a.q.hdr != nullptr;
   u64 *F0 = sl.stk;
@@ -1127,6 +1161,12 @@ __device__ void mem_tree(const BKArgs &a, const Slab &sl, const MemRoot &rt, u64
     }
     pc = (int)__reduce_add_sync(MCE_FULL, (unsigned)pc);
     s_base = (int)__reduce_add_sync(MCE_FULL, (unsigned)sc);
+    if constexpr (OPS) {
+      if (s_base == 0 && part == 0) {  // the root's first pivot: 2W per candidate
+        const int cu = lane < Wr ? __popcll(F0[lane] | F0[Wr + lane]) : 0;
+        *ops += 2 * w32 * (u64)__reduce_add_sync(MCE_FULL, (unsigned)cu);
+      }
+    }
     int k = 0;
     bool el = false;
     for (int uu = lane; uu < d; uu += 32) {
@@ -1166,7 +1206,7 @@ __device__ void mem_tree(const BKArgs &a, const Slab &sl, const MemRoot &rt, u64
     }
     __syncwarp();
   }
-  int depth = 0, recheck = 0;
+  int depth = 0, recheck = 0, b0 = 0;  // b0: first-level branches passed
   bool want = false;
   for (;;) {
     MCE_BD(BD_BRANCH);
@@ -1192,6 +1232,8 @@ __device__ void mem_tree(const BKArgs &a, const Slab &sl, const MemRoot &rt, u64
       Fx[vw] |= vbit;
     }
     __syncwarp();
+    // several warps per root: every parts-th first-level branch is this one's
+    if (parts > 1 && depth == 0 && (b0++ % parts) != part) continue;
     ++nodes;
     if (Budget && a.node_budget && nodes > a.node_budget) {  // a serving request over its budget
       if (lane == 0) atomicOr(a.err, MCE_ERR_BUDGET);
@@ -1213,6 +1255,10 @@ __device__ void mem_tree(const BKArgs &a, const Slab &sl, const MemRoot &rt, u64
     }
     pc = (int)__reduce_add_sync(MCE_FULL, (unsigned)pc);
     xnz = __any_sync(MCE_FULL, xnz);
+    if constexpr (OPS) {
+      const int cu = lane < Wr ? __popcll(pcw | xcw) : 0;
+      *ops += 2 * w32 * (u64)__reduce_add_sync(MCE_FULL, (unsigned)cu) + 4 * w32;
+    }
     if (per_branch && depth == 0 && nX > 0) {
       nL = 0;
       for (int i0 = 0; i0 < nX; i0 += 32) {
@@ -1265,7 +1311,7 @@ __device__ void mem_tree(const BKArgs &a, const Slab &sl, const MemRoot &rt, u64
     }
     const uint32_t vote = __reduce_or_sync(MCE_FULL, (el ? 1u : 0u) | (nc ? 2u : 0u));
     if (vote & 1u) continue;
-    if (vote == 0) {
+    if (!OPS && vote == 0) {
       // P' is a clique and no X' vertex covers it: one path of |P'| nodes
       // below ends in S' | P' (the register engine's shortcut); the union
       // goes into the child's unused branch words.

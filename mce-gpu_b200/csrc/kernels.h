@@ -136,6 +136,11 @@ struct BKArgs {
   int32_t *list_buf;             // nullable: clique records {size, root, members...}
   unsigned long long *list_words;  // words taken in list_buf (also past list_cap)
   unsigned long long list_cap;   // words list_buf holds
+  int32_t parts;                 // warps per root of the launched class (<= 1: one); each
+                                 // takes every parts-th first-level branch of the root
+  int32_t count_ops;             // 1: the counting variants sum the algorithmic word ops ...
+  unsigned long long *ops;       // ... into *ops ...
+  unsigned long long *root_ops;  // ... and per root (nullable [n])
 };
 
 // Launch the engine of one class.  warps_out: number of warps launched (slab sizing).

@@ -12,8 +12,14 @@
 // without it one heavy root can run for minutes), times each value with
 // the device timers of mce_count / mce_batch_count, keeps a value only when
 // it is at least 2% faster, and checks that every trial returns the same
-// count.  The winner is stored in a text table, one line per class; later
-// runs of the same class read it back without trials.
+// count.  Then, bucket by bucket - the engine classes of the roots, by
+// bitmap width: d+ <= 32, 33..64, wider - it walks that bucket's warps per
+// root, donation threshold and donation gate, judged by the bucket's own
+// launch time (the classes run one after the other, so a bucket's settings
+// do not move the others' times).  The winners are stored in a text table:
+// one line per shape class and one per bucket of it ("<class>:b32",
+// ":b64", ":wide"); later runs of the same class read them back without
+// trials.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -63,14 +69,34 @@ void apply(const Knobs &k, mce_opts_t *o) {
 
 int ilog2(double x) { return x < 1.0 ? 0 : (int)std::floor(std::log2(x)); }
 
+// per bucket (engine class): 0 = the global value
+struct Bucket {
+  int32_t warps = 0, threshold = 0, after = 0;
+  double best_ms = 0, default_ms = 0;
+  bool present = false;
+};
+
 struct Entry {
   Knobs k;
   double best_ms, default_ms;
+  Bucket b[3];
 };
 
+const char *kBucketName[3] = {"b32", "b64", "wide"};
+
+void apply_buckets(const Bucket *b, mce_opts_t *o) {
+  for (int c = 0; c < 3; ++c) {
+    o->bucket_warps_per_root[c] = b[c].present ? b[c].warps : 0;
+    o->bucket_donate_threshold[c] = b[c].present ? b[c].threshold : 0;
+    o->bucket_donate_after[c] = b[c].present ? b[c].after : 0;
+  }
+}
+
 const char *kHeader =
-    "# mce autotune table v3: class worker_list donate_after donate_threshold bitmap_width "
-    "peel_solo_max wide_blocks x_pivot best_ms default_ms";
+    "# mce autotune table v4: class worker_list donate_after donate_threshold bitmap_width "
+    "peel_solo_max wide_blocks x_pivot best_ms default_ms\n"
+    "# and per bucket of roots: class:bucket warps_per_root donate_threshold donate_after "
+    "bucket_best_ms bucket_default_ms";
 
 // v3 lines have 10 fields; v2 lines (9, no x_pivot) read as x_pivot 0 and
 // v1 lines (8, no wide_blocks either) as wide_blocks 4
@@ -86,6 +112,22 @@ bool read_table(const char *path, std::map<std::string, Entry> *t) {
     double x;
     ss >> key;
     while (ss >> x) v.push_back(x);
+    const size_t colon = key.find(':');
+    if (colon != std::string::npos) {  // a bucket line
+      if (v.size() != 5) continue;
+      const std::string cls = key.substr(0, colon), bk = key.substr(colon + 1);
+      for (int c = 0; c < 3; ++c)
+        if (bk == kBucketName[c]) {
+          Bucket &b = (*t)[cls].b[c];
+          b.warps = (int32_t)v[0];
+          b.threshold = (int32_t)v[1];
+          b.after = (int32_t)v[2];
+          b.best_ms = v[3];
+          b.default_ms = v[4];
+          b.present = true;
+        }
+      continue;
+    }
     if (v.size() < 7 || v.size() > 9) continue;
     const size_t knobs = v.size() - 2;  // 5, 6 or 7
     Entry e;
@@ -98,7 +140,10 @@ bool read_table(const char *path, std::map<std::string, Entry> *t) {
     e.k.x_pivot = knobs >= 7 ? (int32_t)v[6] : 0;
     e.best_ms = v[knobs];
     e.default_ms = v[knobs + 1];
-    (*t)[key] = e;
+    Entry &dst = (*t)[key];  // keeps bucket lines read before it
+    dst.k = e.k;
+    dst.best_ms = e.best_ms;
+    dst.default_ms = e.default_ms;
   }
   return true;
 }
@@ -113,6 +158,11 @@ int write_table(const char *path, const std::map<std::string, Entry> &t) {
     std::fprintf(f, "%s %d %d %d %d %d %d %d %.4f %.4f\n", kv.first.c_str(), e.k.worker_list,
                  e.k.donate_after, e.k.donate_threshold, e.k.bitmap_width, e.k.peel_solo_max,
                  e.k.wide_blocks, e.k.x_pivot, e.best_ms, e.default_ms);
+    for (int c = 0; c < 3; ++c)
+      if (e.b[c].present)
+        std::fprintf(f, "%s:%s %d %d %d %.4f %.4f\n", kv.first.c_str(), kBucketName[c],
+                     e.b[c].warps, e.b[c].threshold, e.b[c].after, e.b[c].best_ms,
+                     e.b[c].default_ms);
   }
   if (std::fclose(f) != 0 || std::rename(tmp.c_str(), path) != 0) return MCE_EIO;
   return MCE_OK;
@@ -136,7 +186,7 @@ int shape_key(struct ::mce_graph *g, int32_t num_graphs, char *key, size_t len) 
   return MCE_OK;
 }
 
-// Run(opts, &ms, &total) -> status
+// Run(opts, &ms, &total, class_ms[3]) -> status
 template <typename Run>
 int tune(const char *key, const mce_opts_t &base, const char *table_path, int32_t reps,
          int32_t force, Run run, mce_tune_result_t *out) {
@@ -145,9 +195,10 @@ int tune(const char *key, const mce_opts_t &base, const char *table_path, int32_
   std::map<std::string, Entry> table;
   if (table_path) read_table(table_path, &table);
   out->best = base;
-  if (!force && table.count(key)) {
+  if (!force && table.count(key) && table[key].best_ms > 0) {
     const Entry &e = table[key];
     apply(e.k, &out->best);
+    apply_buckets(e.b, &out->best);
     out->best_ms = e.best_ms;
     out->default_ms = e.default_ms;
     out->from_table = 1;
@@ -156,23 +207,30 @@ int tune(const char *key, const mce_opts_t &base, const char *table_path, int32_
   if (reps < 1) reps = 1;
   uint64_t want = 0;
   bool have = false;
-  auto timed = [&](const Knobs &k, double *ms) -> int {
-    mce_opts_t o = base;
-    apply(k, &o);
+  // best of `reps` calls: total and per-class device times
+  auto timed_opts = [&](const mce_opts_t &o, double *ms, double *cls) -> int {
     double best = 1e300;
+    for (int c = 0; c < 3; ++c) cls[c] = 1e300;
     for (int r = 0; r < reps; ++r) {
-      double t = 0;
+      double t = 0, cm[3] = {0, 0, 0};
       uint64_t total = 0;
-      const int rc = run(o, &t, &total);
+      const int rc = run(o, &t, &total, cm);
       if (rc) return rc;
       if (have && total != want) return MCE_ESTATE;  // a setting changed the count
       want = total;
       have = true;
       best = std::min(best, t);
+      for (int c = 0; c < 3; ++c) cls[c] = std::min(cls[c], cm[c]);
       ++out->trials_run;
     }
     *ms = best;
     return MCE_OK;
+  };
+  auto timed = [&](const Knobs &k, double *ms) -> int {
+    mce_opts_t o = base;
+    apply(k, &o);
+    double cls[3];
+    return timed_opts(o, ms, cls);
   };
   Knobs cur = resolved(base);
   double cur_ms = 0;
@@ -211,10 +269,63 @@ int tune(const char *key, const mce_opts_t &base, const char *table_path, int32_
     cur = best;
     cur_ms = best_ms;
   }
+  // per bucket: warps per root, donation threshold and gate, each judged by
+  // the bucket's own launch time
+  Entry ent{cur, cur_ms, out->default_ms, {}};
+  mce_opts_t o = base;
+  apply(cur, &o);
+  double tot_ms = 0, cls_ms[3];
+  if ((rc = timed_opts(o, &tot_ms, cls_ms))) return rc;
+  const bool wl = cur.worker_list != MCE_WL_OFF;
+  for (int c = 0; c < 3; ++c) {
+    if (!(cls_ms[c] > 0 && cls_ms[c] < 1e299)) continue;  // no roots in this bucket
+    Bucket b;
+    b.warps = 1;
+    b.threshold = cur.donate_threshold;
+    b.after = cur.donate_after;
+    b.default_ms = b.best_ms = cls_ms[c];
+    b.present = true;
+    struct BAxis {
+      int32_t Bucket::*field;
+      std::vector<int32_t> values;
+      bool donation;
+    };
+    const BAxis baxes[] = {{&Bucket::warps, {1, 2, 4}, false},
+                           {&Bucket::threshold, {6, 10, 16}, true},
+                           {&Bucket::after, {64, 256, 1024}, true}};
+    for (const BAxis &ax : baxes) {
+      if (ax.donation && !wl) continue;
+      Bucket best = b;
+      for (int32_t v : ax.values) {
+        if (v == b.*(ax.field)) continue;
+        Bucket t = b;
+        t.*(ax.field) = v;
+        mce_opts_t ot = o;
+        Bucket all[3];
+        for (int k = 0; k < 3; ++k) all[k] = ent.b[k];
+        all[c] = t;
+        apply_buckets(all, &ot);
+        double ms = 0, cm[3];
+        if ((rc = timed_opts(ot, &ms, cm))) return rc;
+        if (cm[c] < best.best_ms * 0.98) {
+          best = t;
+          best.best_ms = cm[c];
+        }
+      }
+      b = best;
+    }
+    ent.b[c] = b;
+  }
   apply(cur, &out->best);
+  apply_buckets(ent.b, &out->best);
+  {  // the whole call with every bucket's winner
+    double cm[3];
+    if ((rc = timed_opts(out->best, &cur_ms, cm))) return rc;
+  }
+  ent.best_ms = cur_ms;
   out->best_ms = cur_ms;
   if (table_path) {
-    table[key] = Entry{cur, cur_ms, out->default_ms};
+    table[key] = ent;
     if ((rc = write_table(table_path, table))) return rc;
   }
   return MCE_OK;
@@ -239,8 +350,9 @@ extern "C" int mce_tune_lookup(const char *table_path, const char *key, mce_opts
   std::map<std::string, Entry> t;
   if (!read_table(table_path, &t)) return MCE_EIO;
   auto it = t.find(key);
-  if (it == t.end()) return MCE_ESTATE;
+  if (it == t.end() || !(it->second.best_ms > 0)) return MCE_ESTATE;
   apply(it->second.k, inout);
+  apply_buckets(it->second.b, inout);
   return MCE_OK;
 }
 
@@ -256,10 +368,11 @@ extern "C" int mce_autotune(mce_graph_t g, const mce_opts_t *base, const char *t
   int rc = mce_shape_key(g, key, sizeof(key));
   if (rc) return rc;
   return tune(key, b, table_path, reps, force,
-              [&](const mce_opts_t &o, double *ms, uint64_t *total) {
+              [&](const mce_opts_t &o, double *ms, uint64_t *total, double *cls) {
                 mce_stats_t st;
                 const int r = mce_count(g, &o, total, nullptr, &st);
                 *ms = st.total_ms;
+                for (int c = 0; c < 3; ++c) cls[c] = st.class_ms[c];
                 return r;
               },
               out);
@@ -282,10 +395,11 @@ extern "C" int mce_batch_autotune(mce_batch_t bt, const mce_opts_t *base, const 
   mce::batch_union(bt, &G);
   std::vector<uint64_t> per((size_t)std::max(G, 1));
   return tune(key, b, table_path, reps, force,
-              [&](const mce_opts_t &o, double *ms, uint64_t *total) {
+              [&](const mce_opts_t &o, double *ms, uint64_t *total, double *cls) {
                 mce_stats_t st;
                 const int r = mce_batch_count(bt, &o, per.data(), total, nullptr, &st);
                 *ms = st.total_ms;
+                for (int c = 0; c < 3; ++c) cls[c] = st.class_ms[c];
                 return r;
               },
               out);

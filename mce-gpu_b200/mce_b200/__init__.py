@@ -47,7 +47,11 @@ class _Opts(C.Structure):
                 ("peel_solo_max", C.c_int32), ("donate_after", C.c_int32),
                 ("cuda_graph", C.c_int32), ("heavy_log2", C.c_int32),
                 ("share_log2", C.c_int32), ("warp_log", C.c_int32), ("wide_blocks", C.c_int32),
-                ("wait_limit_ms", C.c_int32), ("stream", C.c_void_p), ("model", C.c_void_p)]
+                ("wait_limit_ms", C.c_int32), ("count_ops", C.c_int32),
+                ("bucket_warps_per_root", C.c_int32 * 3),
+                ("bucket_donate_threshold", C.c_int32 * 3),
+                ("bucket_donate_after", C.c_int32 * 3),
+                ("stream", C.c_void_p), ("model", C.c_void_p)]
 
 
 class _Stats(C.Structure):
@@ -58,7 +62,8 @@ class _Stats(C.Structure):
                 ("kernel_launches", C.c_int32), ("error_flags", C.c_uint32),
                 ("class_roots", C.c_int64 * 8), ("peel_rounds", C.c_int64),
                 ("peel_solo_sections", C.c_int64), ("peel_scan_ms", C.c_double),
-                ("peel_round_ms", C.c_double), ("peel_wait_ms", C.c_double)]
+                ("peel_round_ms", C.c_double), ("peel_wait_ms", C.c_double),
+                ("word_ops", C.c_uint64), ("class_ms", C.c_double * 4)]
 
 
 class _HGraph(C.Structure):
@@ -73,17 +78,23 @@ class _TuneResult(C.Structure):
 
 
 TUNED_FIELDS = ("worker_list", "donate_after", "donate_threshold", "bitmap_width", "peel_solo_max",
-                "wide_blocks", "x_pivot")
+                "wide_blocks", "x_pivot", "warps_per_root", "bucket_warps_per_root",
+                "bucket_donate_threshold", "bucket_donate_after")
+
+
+def _field(o, f):
+    v = getattr(o, f)
+    return tuple(int(x) for x in v) if isinstance(v, C.Array) else v
 
 
 def _tune_dict(r: _TuneResult) -> dict:
-    return {"key": r.key.decode(), "best": {f: getattr(r.best, f) for f in TUNED_FIELDS},
+    return {"key": r.key.decode(), "best": {f: _field(r.best, f) for f in TUNED_FIELDS},
             "best_ms": r.best_ms, "default_ms": r.default_ms, "trials_run": r.trials_run,
             "from_table": bool(r.from_table)}
 
 
 def _opts_kwargs(o: "_Opts") -> dict:
-    return {f: getattr(o, f) for f in TUNED_FIELDS}
+    return {f: _field(o, f) for f in TUNED_FIELDS}
 
 
 class _ServeOpts(C.Structure):
@@ -129,9 +140,10 @@ _sigs = {
     "mce_count": (C.c_int, [_P, _P, _P, _P, _P]),
     "mce_root_log": (C.c_int, [_P, _P]),
     "mce_root_counts": (C.c_int, [_P, _P]),
+    "mce_root_ops": (C.c_int, [_P, _P]),
     "mce_list": (C.c_int, [_P, _P, _P, C.c_int64, _P, C.c_int64, _P, _P]),
     "mce_warp_log": (C.c_int, [_P, _P, _P, _P, _P, C.c_int64, _P]),
-    "mce_count_oriented_noalloc": (C.c_int, [_P, _P, _P, _P, C.c_int64, _P, _P]),
+    "mce_count_oriented_noalloc": (C.c_int, [_P, _P, _P, C.c_int64, _P, C.c_int64, _P, _P]),
     "mce_batch_upload": (C.c_int, [_P, _P, _P, _P, C.c_int32, C.c_int32, _P, _P]),
     "mce_batch_reload": (C.c_int, [_P, _P, _P, _P, _P, C.c_int32, _P]),
     "mce_batch_count": (C.c_int, [_P, _P, _P, _P, _P, _P]),
@@ -355,15 +367,19 @@ class CountResult:
 
 
 def _stats_dict(st: _Stats) -> dict:
-    d = {k: getattr(st, k) for k, _ in _Stats._fields_ if k != "class_roots"}
+    d = {k: getattr(st, k) for k, _ in _Stats._fields_ if k not in ("class_roots", "class_ms")}
     d["class_roots"] = list(st.class_roots)
+    d["class_ms"] = list(st.class_ms)[:3]
     return d
 
 
 def make_opts(*, sched=SCHED_PLAIN, bitmap_width=0, log_roots=False, level=LEVEL_L1,
               induced=INDUCED_P, worker_list=WL_ON, donate_threshold=0, x_pivot=0,
               peel_solo_max=0, donate_after=0, cuda_graph=0, heavy_log2=0, share_log2=0,
-              warp_log=False, wide_blocks=0, wait_limit_ms=0, model=None, stream=None) -> _Opts:
+              warp_log=False, wide_blocks=0, wait_limit_ms=0, count_ops=False,
+              warps_per_root=0, bucket_warps_per_root=(0, 0, 0),
+              bucket_donate_threshold=(0, 0, 0), bucket_donate_after=(0, 0, 0), model=None,
+              stream=None) -> _Opts:
     o = _Opts()
     _lib.mce_opts_default(C.byref(o))
     o.sched, o.bitmap_width, o.log_roots = sched, bitmap_width, int(bool(log_roots))
@@ -373,6 +389,12 @@ def make_opts(*, sched=SCHED_PLAIN, bitmap_width=0, log_roots=False, level=LEVEL
     o.heavy_log2, o.share_log2, o.warp_log = heavy_log2, share_log2, int(warp_log)
     o.wide_blocks = wide_blocks
     o.wait_limit_ms = wait_limit_ms
+    o.count_ops = int(bool(count_ops))
+    o.warps_per_root = warps_per_root
+    for i in range(3):
+        o.bucket_warps_per_root[i] = int(bucket_warps_per_root[i])
+        o.bucket_donate_threshold[i] = int(bucket_donate_threshold[i])
+        o.bucket_donate_after[i] = int(bucket_donate_after[i])
     o.stream = stream
     o.model = model._h if model is not None else None
     return o
@@ -521,6 +543,13 @@ class Graph:
     def root_counts(self) -> np.ndarray:
         out = np.zeros(max(self.n, 1), np.uint64)
         _check(_lib.mce_root_counts(self._h, _ptr(out)), "root_counts")
+        return out[:self.n]
+
+    def root_ops(self) -> np.ndarray:
+        """Per-root algorithmic word operations of the last
+        count(log_roots=True, count_ops=True)."""
+        out = np.zeros(max(self.n, 1), np.uint64)
+        _check(_lib.mce_root_ops(self._h, _ptr(out)), "root_ops")
         return out[:self.n]
 
 

@@ -299,3 +299,119 @@ def test_x_pivot_changes_trees_not_counts(maker):
     assert px.total == t and np.array_equal(px.hist, h)
     assert np.array_equal(counts, rc)  # a root's cliques do not depend on its pivots
     assert px.stats["tree_nodes"] <= ip.stats["tree_nodes"]
+
+
+@pytest.mark.parametrize("maker,kw", [
+    (lambda: mce.gen_er(2000, 0.01, 1, 8, 6, 40), {}),                    # all three engines
+    (lambda: mce.gen_er(2000, 0.01, 1, 8, 6, 40), {"bitmap_width": 64}),
+    (lambda: mce.gen_er(2000, 0.01, 1, 8, 6, 40), {"worker_list": mce.WL_OFF}),
+    (lambda: mce.gen_rmat(12, 16, 0.57, 0.19, 0.19, 7), {"donate_after": 16}),  # wide roots, tasks
+    (lambda: mce.gen_ba(20000, 8, 5, 20, 20, 60), {}),
+])
+def test_word_ops_per_root_equal_the_oracle(maker, kw):
+    """opts.count_ops: the search's algorithmic 32-bit word operations (2 W
+    per row scored by a pivot selection + 4 W per tree node, W = ceil(d+/32))
+    equal the oracle's walk root by root, with subtrees shared or not, and
+    the counting variants give the same counts and trees."""
+    g = maker()
+    tot, rc_o, rn_o, ro_o = oracle.roots_ops(g)
+    with mce.Graph.from_host(g) as dg:
+        r = dg.count(log_roots=True, count_ops=True, **kw)
+        rc, rn, ro = dg.root_counts(), dg.root_log(), dg.root_ops()
+        plain = dg.count(**kw)
+    assert r.total == tot == plain.total
+    assert np.array_equal(rc, rc_o) and np.array_equal(rn, rn_o)
+    assert np.array_equal(ro, ro_o)
+    assert r.stats["word_ops"] == int(ro_o.sum()) > 0
+    assert plain.stats["word_ops"] == 0
+    assert r.stats["tree_nodes"] == plain.stats["tree_nodes"]
+
+
+def test_word_ops_on_a_batch():
+    b = mce.gen_chung_lu_batch(32, 64, 2048, 2.3, 8, 32, 3, 5, 30, 5)
+    u = mce.union(b)
+    _, _, _, ro_o = oracle.roots_ops(u)
+    with mce.Batch(b) as db:
+        r = db.count(count_ops=True)
+    assert r.stats["word_ops"] == int(ro_o.sum())
+
+
+def test_word_ops_rejects_other_modes():
+    g = mce.gen_er(500, 0.02, 1)
+    with mce.Graph.from_host(g) as dg:
+        for kw in ({"x_pivot": 1}, {"warp_log": 1}):
+            with pytest.raises(mce.MceError) as e:
+                dg.count(count_ops=True, **kw)
+            assert e.value.code == mce.EINVAL
+
+
+def _hub_graph(n):
+    """Vertex 0 adjacent to every vertex and in a K8 on 0..7 that is peeled
+    last: a root with n - 8 earlier neighbours (a hub) and 7 later ones."""
+    base = mce.gen_er(n, 6.0 / n, 11)
+    s, d = [], []
+    for v in range(base.n):
+        for w in base.col[base.row_ptr[v]:base.row_ptr[v + 1]]:
+            if v < w:
+                s.append(v); d.append(int(w))
+    s += [0] * (n - 1)
+    d += list(range(1, n))
+    for v in range(1, 8):
+        for w in range(v + 1, 8):
+            s.append(v); d.append(w)
+    return mce.from_edges(np.array(s), np.array(d), n)
+
+
+@pytest.mark.parametrize("maker", [
+    lambda: mce.gen_er(2000, 0.01, 1, 8, 6, 40),                  # all three engines
+    lambda: mce.gen_rmat(12, 16, 0.57, 0.19, 0.19, 7),            # wide roots and tasks
+    lambda: _hub_graph(5000),                                      # a hub root split in parts
+], ids=["er", "rmat12", "hub"])
+@pytest.mark.parametrize("kw", [
+    {"warps_per_root": 2}, {"warps_per_root": 4},
+    {"bucket_warps_per_root": (3, 2, 4), "bucket_donate_threshold": (6, 16, 8),
+     "bucket_donate_after": (64, 1024, 16)},
+    {"warps_per_root": 3, "worker_list": mce.WL_OFF},
+    {"warps_per_root": 2, "bitmap_width": 64, "cuda_graph": 1},
+], ids=["w2", "w4", "buckets", "w3-nowl", "w2-64bit-graph"])
+def test_warps_per_root_give_the_same_trees(maker, kw):
+    """Several warps per root split a root's tree by its first-level
+    branches: per-root counts and tree sizes stay the oracle's, and the
+    histogram the whole graph's."""
+    g = maker()
+    tot, h, rc_o, rn_o = oracle.roots(g)
+    with mce.Graph.from_host(g) as dg:
+        for _ in range(2):  # also a second call (a replayed capture with cuda_graph)
+            r = dg.count(log_roots=True, **kw)
+            assert r.stats["error_flags"] == 0
+            assert r.total == tot and np.array_equal(r.hist, h)
+            assert np.array_equal(dg.root_counts(), rc_o)
+            assert np.array_equal(dg.root_log(), rn_o)
+
+
+def test_warps_per_root_word_ops():
+    g = mce.gen_er(2000, 0.01, 1, 8, 6, 40)
+    _, _, _, ro_o = oracle.roots_ops(g)
+    with mce.Graph.from_host(g) as dg:
+        r = dg.count(count_ops=True, log_roots=True, warps_per_root=3)
+        assert np.array_equal(dg.root_ops(), ro_o)
+    assert r.stats["word_ops"] == int(ro_o.sum())
+
+
+def test_per_bucket_settings_on_a_batch():
+    b = mce.gen_chung_lu_batch(48, 64, 4096, 2.3, 8, 32, 5, 5, 40, 21)
+    per_o = [oracle.count(b.graph(i))[0] for i in range(b.num_graphs)]
+    with mce.Batch(b) as db:
+        for kw in ({}, {"bucket_warps_per_root": (1, 4, 2), "bucket_donate_threshold": (8, 6, 0)}):
+            r = db.count(**kw)
+            assert [int(x) for x in r.per_graph] == per_o
+
+
+def test_warps_per_root_bounds():
+    g = mce.gen_er(300, 0.05, 1)
+    with mce.Graph.from_host(g) as dg:
+        for kw in ({"warps_per_root": 33}, {"warps_per_root": -1},
+                   {"bucket_warps_per_root": (0, 40, 0)}):
+            with pytest.raises(mce.MceError) as e:
+                dg.count(**kw)
+            assert e.value.code == mce.EINVAL

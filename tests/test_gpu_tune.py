@@ -31,3 +31,7 @@ def test_autotune_batch(tmp_path):
         res = db.count(**r["best"])
     assert np.array_equal(res.per_graph, want)
     assert mce.tune_lookup(table, r["key"]) == r["best"]
+    # a line per bucket of roots that the batch has (its narrow roots at least)
+    lines = open(table).read().splitlines()
+    assert any(l.startswith(r["key"] + ":b32 ") for l in lines)
+    assert r["best"]["bucket_warps_per_root"][0] in (1, 2, 4)

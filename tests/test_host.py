@@ -260,13 +260,27 @@ def test_tune_table_lookup(tmp_path):
                  "b12-n23-a4-k7 2 64 16 32 64 100.0 110.0\n")
     assert mce.tune_lookup(str(t), "n10-a3-k4") == dict(
         worker_list=1, donate_after=1024, donate_threshold=6, bitmap_width=64, peel_solo_max=-1,
-        wide_blocks=4, x_pivot=0)  # a v1 line: no wide_blocks or x_pivot column
+        wide_blocks=4, x_pivot=0, warps_per_root=0, bucket_warps_per_root=(0, 0, 0),
+        bucket_donate_threshold=(0, 0, 0), bucket_donate_after=(0, 0, 0))
+    # (a v1 line: no wide_blocks or x_pivot column, no buckets)
     assert mce.tune_lookup(str(t), "b12-n23-a4-k7")["peel_solo_max"] == 64
     assert mce.tune_lookup(str(t), "n11-a3-k4") is None
     t.write_text("# mce autotune table v2\nn14-a4-k6 2 1024 10 32 -1 8 900.0 1100.0\n")
     assert mce.tune_lookup(str(t), "n14-a4-k6")["wide_blocks"] == 8
     t.write_text("# mce autotune table v3\nn14-a4-k6 2 1024 10 32 -1 8 1 800.0 1100.0\n")
     assert mce.tune_lookup(str(t), "n14-a4-k6")["x_pivot"] == 1
+    # v4: a line per bucket of roots (engine class), before or after the class line
+    t.write_text("# mce autotune table v4\n"
+                 "b12-n23-a4-k5:b64 2 6 1024 3.1 4.0\n"
+                 "b12-n23-a4-k5 2 256 10 32 -1 4 0 45.0 47.4\n"
+                 "b12-n23-a4-k5:b32 1 10 256 30.0 30.0\n"
+                 "n9-a3-k4:wide 4 16 64 1.0 2.0\n")  # buckets without a class line: none
+    r = mce.tune_lookup(str(t), "b12-n23-a4-k5")
+    assert r["bucket_warps_per_root"] == (1, 2, 0)
+    assert r["bucket_donate_threshold"] == (10, 6, 0)
+    assert r["bucket_donate_after"] == (256, 1024, 0)
+    assert r["donate_after"] == 256
+    assert mce.tune_lookup(str(t), "n9-a3-k4") is None
 
 
 def test_device_file_paths_fail_loudly_without_a_device(tmp_path):

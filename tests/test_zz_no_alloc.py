@@ -33,11 +33,11 @@ def oriented_on_device(g):
 
 def call(dev, hist, n_roots=None):
     import torch
-    n = len(dev["roots"]) if n_roots is None else n_roots
+    k = len(dev["roots"]) if n_roots is None else n_roots
     return mce._lib.mce_count_oriented_noalloc(
         C.c_void_p(dev["rp"].data_ptr()), C.c_void_p(dev["split"].data_ptr()),
-        C.c_void_p(dev["cs"].data_ptr()), C.c_void_p(dev["roots"].data_ptr()), n,
-        C.c_void_p(hist.data_ptr()), C.c_void_p(torch.cuda.current_stream().cuda_stream))
+        C.c_void_p(dev["cs"].data_ptr()), len(dev["split"]), C.c_void_p(dev["roots"].data_ptr()),
+        k, C.c_void_p(hist.data_ptr()), C.c_void_p(torch.cuda.current_stream().cuda_stream))
 
 
 def test_noalloc_matches_mce_count_twice():
@@ -61,3 +61,19 @@ def test_noalloc_rejects_roots_beyond_its_limit():
     hist = torch.zeros(mce.HIST_MAX, dtype=torch.int64, device="cuda")
     assert call(dev, hist) == mce.ELIMIT
     assert int(hist.sum().item()) == 0
+
+
+@pytest.mark.parametrize("bad", ["n", "-1"])
+def test_noalloc_rejects_root_ids_outside_the_graph(bad):
+    import torch
+    g = mce.gen_er(2000, 0.004, 3, 4, 5, 8)
+    ref, dev = oriented_on_device(g)
+    roots = dev["roots"].clone()
+    roots[len(roots) // 2] = g.n if bad == "n" else -1
+    hist = torch.full((mce.HIST_MAX,), 7, dtype=torch.int64, device="cuda")
+    assert call(dict(dev, roots=roots), hist) == mce.EINVAL
+    # caught before the search: the histogram is left as it was
+    assert bool((hist == 7).all().item())
+    # the scratch stays usable: a good call right after gives the full answer
+    assert call(dev, hist) == mce.OK
+    assert np.array_equal(hist.cpu().numpy().astype(np.uint64), ref.hist)
