@@ -213,16 +213,24 @@ static int ws_alloc(bk_ws *w, int64_t maxd, int64_t maxu) {
 }
 
 /* Count the maximal cliques whose first vertex in the order is r. */
+/* *ops_out: the walk's algorithmic 32-bit word operations, W32 =
+   ceil(d / 32) words per row: 2 W32 per row scored by a pivot selection
+   (AND + POPC; the root's over all d rows, select_pivot_from_P,
+   mce/mce_utils.cuh:338-364, a node's over P' | X',
+   select_pivot_from_P_and_Xp, :366-402) and 4 W32 per node for the child
+   sets (populate_xl_and_cl, :321-336). */
 static void root_search(bk_ws *w, int32_t r, const int32_t *row_ptr, const int32_t *split,
                         const int32_t *cs, uint64_t *hist, int hist_len, uint64_t *cnt_out,
-                        uint64_t *nodes_out) {
+                        uint64_t *nodes_out, uint64_t *ops_out) {
   const int64_t sb = split[r], d = row_ptr[r + 1] - sb; /* later neighbours: P */
   const int64_t ub = row_ptr[r], u = sb - ub;          /* earlier neighbours: Xx */
-  uint64_t cnt = 0, nodes = 0;
+  uint64_t cnt = 0, nodes = 0, ops = 0;
   *cnt_out = 0;
   *nodes_out = 0;
+  *ops_out = 0;
   if (d == 0) return; /* a root without later neighbours yields nothing */
   const int64_t W = (d + 63) / 64;
+  const uint64_t W32 = (uint64_t)((d + 31) / 32);
   uint64_t *enc = w->enc;
   memset(enc, 0, sizeof(uint64_t) * (size_t)(d * W));
   /* warp_sorted_count_and_encode_full (mce/mce_utils.cuh:90-117): for every
@@ -245,6 +253,7 @@ static void root_search(bk_ws *w, int32_t r, const int32_t *row_ptr, const int32
   /* select_pivot_from_P (mce/mce_utils.cuh:338-364): the row with the most
      bits; finalize_pivot (:191-202).  Ties: the first row. */
   int64_t piv = 0, best = -1;
+  ops += 2 * W32 * (uint64_t)d;
   for (int64_t j = 0; j < d; ++j) {
     int64_t c = 0;
     for (int64_t k = 0; k < W; ++k) c += popc64(enc[j * W + k]);
@@ -316,6 +325,11 @@ static void root_search(bk_ws *w, int32_t r, const int32_t *row_ptr, const int32
       tcl[k] = (cl[l * W + k] & ~done) & enc[v * W + k];
       curSZ += popc64(tcl[k]);
     }
+    {
+      int64_t cand = 0;
+      for (int64_t k = 0; k < W; ++k) cand += popc64(tcl[k] | txl[k]);
+      ops += 2 * W32 * (uint64_t)cand + 4 * W32;
+    }
     /* select_pivot_from_P_and_Xp (mce/mce_utils.cuh:366-402): pivot over
        P' u X'; an X' vertex adjacent to all of P' eliminates the path. */
     int more = 0, elim = 0;
@@ -357,16 +371,18 @@ static void root_search(bk_ws *w, int32_t r, const int32_t *row_ptr, const int32
   }
   *cnt_out = cnt;
   *nodes_out = nodes;
+  *ops_out = ops;
 }
 
 /*
  * Search the roots begin, begin + stride, ... < end (all roots: 0, n, 1).
  * total: maximal cliques found; hist (nullable, hist_len entries) by size;
- * root_count / root_nodes (nullable, n entries) per root.
+ * root_count / root_nodes / root_ops (nullable, n entries) per root.
  */
-int oracle_mce(int64_t n, const int32_t *row_ptr, const int32_t *split, const int32_t *cs,
-               int64_t begin, int64_t end, int64_t stride, int nthreads, uint64_t *total,
-               uint64_t *hist, int hist_len, uint64_t *root_count, uint64_t *root_nodes) {
+int oracle_mce_ops(int64_t n, const int32_t *row_ptr, const int32_t *split, const int32_t *cs,
+                   int64_t begin, int64_t end, int64_t stride, int nthreads, uint64_t *total,
+                   uint64_t *hist, int hist_len, uint64_t *root_count, uint64_t *root_nodes,
+                   uint64_t *root_ops) {
   if (n < 0 || stride < 1 || !total || (n > 0 && (!row_ptr || !split || !cs)))
     return ORACLE_EINVAL;
   if (end > n) end = n;
@@ -394,11 +410,12 @@ int oracle_mce(int64_t n, const int32_t *row_ptr, const int32_t *split, const in
 #pragma omp for schedule(dynamic, 64)
     for (int64_t r = begin; r < end; r += stride) {
       if (!ok) continue;
-      uint64_t c, nd;
-      root_search(&w, (int32_t)r, row_ptr, split, cs, lh, hist_len, &c, &nd);
+      uint64_t c, nd, op;
+      root_search(&w, (int32_t)r, row_ptr, split, cs, lh, hist_len, &c, &nd, &op);
       tot += c;
       if (root_count) root_count[r] = c;
       if (root_nodes) root_nodes[r] = nd;
+      if (root_ops) root_ops[r] = op;
     }
     if (ok) {
       if (hist) {
@@ -412,6 +429,13 @@ int oracle_mce(int64_t n, const int32_t *row_ptr, const int32_t *split, const in
   if (err) return ORACLE_ENOMEM;
   *total = tot;
   return ORACLE_OK;
+}
+
+int oracle_mce(int64_t n, const int32_t *row_ptr, const int32_t *split, const int32_t *cs,
+               int64_t begin, int64_t end, int64_t stride, int nthreads, uint64_t *total,
+               uint64_t *hist, int hist_len, uint64_t *root_count, uint64_t *root_nodes) {
+  return oracle_mce_ops(n, row_ptr, split, cs, begin, end, stride, nthreads, total, hist,
+                        hist_len, root_count, root_nodes, NULL);
 }
 
 /* Peel + orient + search in one call (all roots). */

@@ -1,4 +1,5 @@
 """The CPU oracle against closed forms, brute force and the textbook search."""
+import os
 import numpy as np
 import pytest
 
@@ -85,3 +86,30 @@ def test_per_root_sum_equals_total():
     tot, h, rc, rn = oracle.roots(g)
     assert rc.sum() == tot == oracle.count(g)[0]
     assert np.all(rn[rc > 0] > 0)
+
+
+def test_workload_generators_match_the_library():
+    """The checker's second build of the seeded generators (used where
+    libmce.so must not be loaded, e.g. bench.py's reference arm) returns the
+    library's graphs byte for byte, and its .bel file is the library's."""
+    import tempfile
+    b = mce.gen_chung_lu_batch(64, 64, 2048, 2.3, 8.0, 32.0, 5, 5, 40, 11)
+    u = mce.union(b)
+    ou, start = oracle.gen_batch_union(64, 64, 2048, 2.3, 8.0, 32.0, 5, 5, 40, 11)
+    assert np.array_equal(ou.row_ptr, u.row_ptr[:u.n + 1]) and np.array_equal(ou.col, u.col)
+    assert np.array_equal(start, b.vtx_offsets - np.arange(65))
+    for og, lg in ((oracle.gen_ba(20000, 8, 23, 20, 20, 60), mce.gen_ba(20000, 8, 23, 20, 20, 60)),
+                   (oracle.gen_rmat(10, 16, 0.57, 0.19, 0.19, 7),
+                    mce.gen_rmat(10, 16, 0.57, 0.19, 0.19, 7)),
+                   (oracle.gen_er(3000, 0.004, 1, 5, 6, 12), mce.gen_er(3000, 0.004, 1, 5, 6, 12))):
+        assert np.array_equal(og.row_ptr, lg.row_ptr[:lg.n + 1]) and np.array_equal(og.col, lg.col)
+    with tempfile.TemporaryDirectory() as d:
+        oracle.bel_write(os.path.join(d, "a.bel"), ou)
+        mce.bel_write(os.path.join(d, "b.bel"), u)
+        with open(os.path.join(d, "a.bel"), "rb") as fa, open(os.path.join(d, "b.bel"), "rb") as fb:
+            assert fa.read() == fb.read()
+    # per-graph sums of per-root counts equal each graph's own count
+    _, _, rc, _ = oracle.roots(ou)
+    per = oracle.per_graph(rc, start)
+    for i in (0, 7, 63):
+        assert int(per[i]) == oracle.count(b.graph(i))[0]
