@@ -82,7 +82,8 @@ typedef struct mce_opts {
                                same tree, split by its first level; the
                                counterpart of the reference's PSIZE lanes per
                                candidate, src/main.cu:158-165).  Buckets
-                               without their own value use this one         */
+                               without their own value use this one; runs
+                               with warp_log and mce_list use one warp       */
   int32_t donate_threshold; /* 0 = default (10, the reference's SZTH,
                                mce/parameter.cuh:5): smallest candidate set a
                                subtree must have to be donated                 */
@@ -128,6 +129,12 @@ typedef struct mce_opts {
   int32_t bucket_warps_per_root[3];
   int32_t bucket_donate_threshold[3];
   int32_t bucket_donate_after[3];
+  int32_t stage_lists;      /* 1 = the 32-bit engine (d+ <= 32, one warp per
+                               root, IP) copies each group of later lists it
+                               encodes into shared memory with 1-D bulk
+                               copies (16-byte windows, one mbarrier per
+                               warp) and reads them there; groups that do not
+                               fit 2 KB are read from global memory         */
   void *stream;             /* cudaStream_t to queue work on; NULL = own      */
   void *model;              /* mce_model_t for MCE_SCHED_LEARNED (NULL: the
                                degree heuristic is used instead)              */
@@ -358,9 +365,13 @@ int mce_batch_count(mce_batch_t b, const mce_opts_t *opts, uint64_t *per_graph_t
 /* mce_batch_reload followed by mce_batch_count in one call, for a batch in
  * host memory: batches of 2^20 arcs or more are copied in up to four parts
  * of whole graphs on a stream of the handle's own, and each part is rebased,
- * peeled and oriented as soon as it is on the device, while the next parts
- * are still being copied; one search over the whole batch follows.  Same
- * results as the two calls.  Pinned host memory lets the copies overlap. */
+ * peeled, oriented and - for counts in plain or degree order without
+ * per-root or per-warp logs - searched as soon as it is on the device, while
+ * the next parts are still being copied (parts of 1/16, 2/16, 4/16 and 9/16
+ * of the arcs); in the other modes one search over the whole batch follows.
+ * Same results as the two calls.  Pinned host memory lets the copies
+ * overlap.  In the part-by-part mode stats->peel_ms is the time until the
+ * first part is ready, orient_ms 0 and count_ms the rest.                 */
 int mce_batch_count_host(mce_batch_t b, const int32_t *row_ptr, const int32_t *col,
                          const int64_t *vtx_offsets, const int64_t *arc_offsets,
                          int32_t num_graphs, const mce_opts_t *opts, uint64_t *per_graph_total,

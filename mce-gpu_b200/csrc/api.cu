@@ -91,6 +91,17 @@ struct mce_graph {
   // to the caller's stream
   cudaStream_t part_s[4] = {nullptr};
   cudaEvent_t part_fork = nullptr, part_done[4] = {nullptr};
+  // a batch searched part by part as it arrives (mce_batch_count_host):
+  // per part its roots' summary (device and pinned host), root fetch
+  // counters, sort scratch and hub rows
+  ShapeInfo *part_shape = nullptr, *part_shape_h = nullptr;
+  uint32_t *part_fetch = nullptr;
+  void *part_tmp[4] = {nullptr};
+  size_t part_tmp_bytes[4] = {0};
+  int64_t *phub_off[4] = {nullptr};
+  int32_t *phub_nx[4] = {nullptr};
+  unsigned long long *phub_rows[4] = {nullptr};
+  int64_t phub_off_cap[4] = {0}, phub_rows_cap[4] = {0};
   // search launches captured as a CUDA graph, replayed while the key matches
   cudaGraphExec_t search_exec = nullptr;
   unsigned char search_key[320] = {0};
@@ -124,7 +135,9 @@ int alloc_graph_bufs(mce_graph *g, int64_t n, int64_t m) {
   free_graph_bufs(g);
   const size_t N = (size_t)n + 1, M = (size_t)m;
   int rc;
-  if ((rc = dalloc(&g->rp, N)) || (rc = dalloc(&g->col, M)) || (rc = dalloc(&g->cs, M)) ||
+  // cs: 4 spare entries, so that a list's 16-byte window never ends past
+  // the allocation (the bulk-copy staging of the search rounds it up)
+  if ((rc = dalloc(&g->rp, N)) || (rc = dalloc(&g->col, M)) || (rc = dalloc(&g->cs, M + 4)) ||
       (rc = dalloc(&g->split, N)) || (rc = dalloc(&g->prio, N)) || (rc = dalloc(&g->core, N)) ||
       (rc = dalloc(&g->deg, N)) || (rc = dalloc(&g->alA, N)) || (rc = dalloc(&g->alB, N)) ||
       (rc = dalloc(&g->f0, N)) || (rc = dalloc(&g->f1, N)) || (rc = dalloc(&g->f2, N)) ||
@@ -505,6 +518,15 @@ int mce_graph_free(mce_graph_t g) {
   for (auto &pr : g->cls_ev)
     for (auto &e : pr)
       if (e) cudaEventDestroy(e);
+  dfree(g->part_shape);
+  dfree(g->part_fetch);
+  if (g->part_shape_h) cudaFreeHost(g->part_shape_h);
+  for (int p = 0; p < 4; ++p) {
+    dfree(g->part_tmp[p]);
+    dfree(g->phub_off[p]);
+    dfree(g->phub_nx[p]);
+    dfree(g->phub_rows[p]);
+  }
   for (int p = 0; p < 4; ++p) {
     if (g->part_s[p]) cudaStreamDestroy(g->part_s[p]);
     if (g->part_done[p]) cudaEventDestroy(g->part_done[p]);
@@ -592,13 +614,14 @@ int ensure_feat(mce_graph *g) {
 // Features of the candidate roots (at least MLP_MIN_LATER later neighbours)
 // of the peeled, oriented graph into g->feat, their list into g->cand; with
 // zero_rest the other rows are zeroed too (mce_root_features returns them).
-int compute_features(mce_graph *g, cudaStream_t s, int *launches, bool zero_rest) {
+int compute_features(mce_graph *g, cudaStream_t s, int *launches, bool zero_rest,
+                     int min_later = MLP_MIN_LATER) {
   int rc = ensure_feat(g);
   if (rc) return rc;
   if (zero_rest && g->n)
     MCE_CUDA(cudaMemsetAsync(g->feat, 0, sizeof(float) * MLP_IN * (size_t)g->n, s));
   return features_launch(g->n, g->rp, g->split, g->cs, g->core, g->feat, g->cand, g->cand_n,
-                         g->sms, s, launches);
+                         g->sms, s, launches, min_later);
 }
 
 // Predicted cost of every vertex into g->pred: the model on the candidate
@@ -661,10 +684,10 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
       return rc;
   } else if (sched == MCE_SCHED_LEARNED && g->n > 0) {
     if (model->device != g->device) return MCE_EINVAL;
-    if ((rc = compute_features(g, s, &launches, false)) ||
+    if ((rc = compute_features(g, s, &launches, false, SCHED_MIN_LATER)) ||
         (rc = predict_candidates(g, model->wh, s, &launches)) ||
         (rc = rekey_launch(g->n, g->keys_in, g->pred, g->rp, g->split, g->policy, heavy, share_cost,
-                           g->sms, s, &launches)) ||
+                           g->sms, s, &launches, SCHED_MIN_LATER)) ||
         (rc = run_sort(g, 32, s, &launches)))
       return rc;
     policy = g->policy;
@@ -706,7 +729,7 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   int parts[NCLS] = {1, 1, 1, 1, 1}, dmin[NCLS] = {0}, dafter[NCLS] = {0};
   for (int c = CLS_R32; c <= CLS_MEM; ++c) {
     const int w = o.bucket_warps_per_root[c] ? o.bucket_warps_per_root[c] : o.warps_per_root;
-    parts[c] = w > 1 ? w : 1;
+    parts[c] = w > 1 && !o.warp_log && !lc ? w : 1;  // evaluation and listing: one warp
     const int t = o.bucket_donate_threshold[c] ? o.bucket_donate_threshold[c] : o.donate_threshold;
     dmin[c] = t > 0 ? t : DEFAULT_DONATE_MIN;
     const int af = o.bucket_donate_after[c] ? o.bucket_donate_after[c] : o.donate_after;
@@ -776,6 +799,7 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   a.level2 = o.level == MCE_LEVEL_L2 ? 1 : 0;
   a.x_pivot = (o.x_pivot || o.induced == MCE_INDUCED_PX) ? 1 : 0;
   a.count_ops = o.count_ops ? 1 : 0;
+  a.stage = o.stage_lists ? 1 : 0;
   a.ops = g->nodes + 1;
   a.root_ops = log_ops ? g->root_ops : nullptr;
   if (lc) {
@@ -792,7 +816,7 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   // opts.cuda_graph it is captured once and replayed.
   struct SearchKey {
     int grid[NCLS], block[NCLS];
-    int dcap, xcap, rxcap, wbits, share, log, wide8, level2, xpiv, ops;
+    int dcap, xcap, rxcap, wbits, share, log, wide8, level2, xpiv, ops, stage;
     int parts[NCLS], dmin[NCLS], dafter[NCLS];
     uint64_t wlimit;
     const void *slab, *graph_count, *graph_of, *root_nodes, *policy, *q[NCLS], *bufs[4], *wlog;
@@ -821,6 +845,7 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   key.level2 = a.level2;
   key.xpiv = a.x_pivot;
   key.ops = a.count_ops + (log_ops ? 2 : 0);
+  key.stage = a.stage;
   key.slab = g->slab;
   key.graph_count = a.graph_count;
   key.root_nodes = a.root_nodes;
@@ -972,6 +997,266 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   st.peel_round_ms = pms[1];
   st.peel_wait_ms = pms[2];
   st.donations = pushed;
+  if (stats) *stats = st;
+  if (perr) return MCE_ETIMEOUT;
+  if (h_err & MCE_ERR_WAIT_TIMEOUT) return MCE_ETIMEOUT;
+  if (h_err) return MCE_ELIMIT;
+  return MCE_OK;
+}
+
+}  // namespace
+
+namespace {
+
+// mce_batch_count_host, pipelined: each part of a batch arriving from the
+// host is rebased, peeled, oriented and its roots sorted on a stream of its
+// own as soon as its copy lands; the host reads the part's summary and
+// queues its search (hub rows, then the engine classes) on the call's stream,
+// so part p is searched while parts p+1.. are still being copied and peeled.
+// A part's graphs share no vertex with other parts, so its search reads only
+// its own rows.  Buffers that a later part outgrows are replaced and the old
+// ones freed after the call (earlier parts' searches may still use them).
+// Counting only: plain or degree order; the other modes take count_impl.
+int count_pipelined(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *hist,
+                    mce_stats_t *stats, const BatchCtx *bc) {
+  const BatchParts &P = *bc->parts;
+  MCE_CUDA(cudaSetDevice(g->device));
+  cudaStream_t s = pick_stream(g, o.stream);
+  int launches = 0, rc = MCE_OK;
+  mce_stats_t st;
+  std::memset(&st, 0, sizeof(st));
+  if (!g->part_shape && (rc = dalloc(&g->part_shape, MAX_PARTS))) return rc;
+  if (!g->part_fetch && (rc = dalloc(&g->part_fetch, 8 * MAX_PARTS))) return rc;
+  if (!g->part_shape_h &&
+      cudaHostAlloc((void **)&g->part_shape_h, sizeof(ShapeInfo) * MAX_PARTS,
+                    cudaHostAllocDefault) != cudaSuccess)
+    return MCE_ENOMEM;
+  for (int p = 0; p < P.k; ++p) {
+    if (!g->part_s[p]) MCE_CUDA(cudaStreamCreateWithFlags(&g->part_s[p], cudaStreamNonBlocking));
+    if (!g->part_done[p])
+      MCE_CUDA(cudaEventCreateWithFlags(&g->part_done[p], cudaEventDisableTiming));
+  }
+  if (!g->part_fork) MCE_CUDA(cudaEventCreateWithFlags(&g->part_fork, cudaEventDisableTiming));
+  std::vector<void *> retired;  // freed after the call's last search
+  auto finish = [&](int code) {
+    for (int p = 0; p < P.k; ++p) cudaStreamSynchronize(g->part_s[p]);
+    cudaStreamSynchronize(s);
+    for (void *q : retired) cudaFree(q);
+    return code;
+  };
+  const bool share = o.worker_list != MCE_WL_OFF;
+  const bool degree = o.sched == MCE_SCHED_DEGREE;
+  const float heavy = (float)(o.heavy_log2 > 0 ? o.heavy_log2 : DEFAULT_HEAVY_LOG2);
+  MCE_CUDA(cudaEventRecord(g->ev[0], s));
+  MCE_CUDA(cudaMemsetAsync(g->peel_ctl, 0, peel_ctl_bytes(), s));
+  MCE_CUDA(cudaMemsetAsync(g->part_fetch, 0, sizeof(uint32_t) * 8 * MAX_PARTS, s));
+  MCE_CUDA(cudaMemsetAsync(bc->graph_count, 0, sizeof(unsigned long long) * bc->G, s));
+  MCE_CUDA(cudaMemsetAsync(g->err, 0, sizeof(uint32_t) * 4, s));
+  MCE_CUDA(cudaMemsetAsync(g->hist, 0, sizeof(unsigned long long) * MCE_HIST_MAX, s));
+  MCE_CUDA(cudaMemsetAsync(g->nodes, 0, sizeof(unsigned long long) * 4, s));
+  MCE_CUDA(cudaEventRecord(g->part_fork, s));
+  const PeelArgs pa = peel_args(g, o.peel_solo_max);
+  int64_t vb[MAX_PARTS + 1];
+  for (int p = 0; p <= P.k; ++p) vb[p] = P.vo_h[P.g[p]] - P.g[p];
+  // the parts' preparation, each on its own stream
+  for (int p = 0; p < P.k; ++p) {
+    cudaStream_t sp = g->part_s[p];
+    const int64_t g0 = P.g[p], g1 = P.g[p + 1], vbeg = vb[p], vend = vb[p + 1];
+    MCE_CUDA(cudaStreamWaitEvent(sp, g->part_fork, 0));
+    MCE_CUDA(cudaStreamWaitEvent(sp, P.ready[p], 0));
+    if ((rc = batch_rebase_part_launch(P.rp_local, P.col_local, bc->vtx_off, bc->arc_off,
+                                       (int32_t)bc->G, P.vo_h[g0], P.vo_h[g1], P.ao_h[g0],
+                                       P.ao_h[g1], vend, (int32_t)P.ao_h[g1], g->rp, g->col,
+                                       const_cast<int32_t *>(bc->graph_of), g->sms, sp,
+                                       &launches)))
+      return finish(rc);
+    if (vend > vbeg &&
+        (rc = peel_segments_launch(pa, bc->vtx_off, bc->arc_off, bc->order + g0,
+                                   (int32_t)(g1 - g0), sp, &launches, p)))
+      return finish(rc);
+    OrientArgs oa = orient_args(g);
+    oa.v0 = vbeg;
+    oa.n = vend;
+    oa.shape = g->part_shape + p;
+    oa.hub_list = g->hub_list + vbeg;  // hub indices are the part's own
+    if ((rc = orient_launch(oa, sp, &launches))) return finish(rc);
+    const int64_t np = vend - vbeg;
+    if (degree && np > 0 &&
+        (rc = rekey_launch(np, g->keys_in + vbeg, nullptr, g->rp + vbeg, g->split + vbeg, nullptr,
+                           heavy, heavy, g->sms, sp, &launches)))
+      return finish(rc);
+    if ((rc = roots_sort(np, g->keys_in + vbeg, g->keys_out + vbeg, g->vals_in + vbeg,
+                         g->roots + vbeg, degree ? 32 : 3, &g->part_tmp[p], &g->part_tmp_bytes[p],
+                         g->part_shape + p, sp, &launches)))
+      return finish(rc);
+    MCE_CUDA(cudaMemcpyAsync(g->part_shape_h + p, g->part_shape + p, sizeof(ShapeInfo),
+                             cudaMemcpyDeviceToHost, sp));
+    MCE_CUDA(cudaEventRecord(g->part_done[p], sp));
+  }
+  // each part's search, in order, on the call's stream
+  uint32_t err_limit = 0;
+  for (int p = 0; p < P.k; ++p) {
+    MCE_CUDA(cudaEventSynchronize(g->part_done[p]));
+    const ShapeInfo sh = g->part_shape_h[p];
+    MCE_CUDA(cudaStreamWaitEvent(s, g->part_done[p], 0));
+    if (p == 0) MCE_CUDA(cudaEventRecord(g->ev[1], s));
+    if (sh.cls_cnt[CLS_BIG]) {
+      err_limit = 1;
+      break;
+    }
+    const int64_t vbeg = vb[p];
+    if (sh.hub_cnt > 0) {
+      const int64_t need_off = (int64_t)sh.hub_cnt + 1, need_rows = (int64_t)sh.hub_rows;
+      if (need_off > g->phub_off_cap[p]) {
+        if (g->phub_off[p]) retired.push_back(g->phub_off[p]);
+        if (g->phub_nx[p]) retired.push_back(g->phub_nx[p]);
+        g->phub_off[p] = nullptr;
+        g->phub_nx[p] = nullptr;
+        g->phub_off_cap[p] = 0;
+        if ((rc = dalloc(&g->phub_off[p], (size_t)need_off)) ||
+            (rc = dalloc(&g->phub_nx[p], (size_t)need_off)))
+          return finish(rc);
+        g->phub_off_cap[p] = need_off;
+      }
+      if (need_rows > g->phub_rows_cap[p]) {
+        if (g->phub_rows[p]) retired.push_back(g->phub_rows[p]);
+        g->phub_rows[p] = nullptr;
+        g->phub_rows_cap[p] = 0;
+        if ((rc = dalloc(&g->phub_rows[p], (size_t)need_rows))) return finish(rc);
+        g->phub_rows_cap[p] = need_rows;
+      }
+      if ((rc = hub_rows_launch(g->rp, g->split, g->cs, g->hub_list + vbeg, sh.hub_cnt, need_rows,
+                                g->phub_off[p], g->phub_nx[p], g->phub_rows[p], g->sms, s,
+                                &launches)))
+        return finish(rc);
+    }
+    int grid[NCLS] = {0}, block[NCLS] = {0}, smem[NCLS] = {0};
+    const int dcap = (int)(sh.max_dplus > 0 ? sh.max_dplus : 1);
+    const int xcap = (int)(sh.max_dminus_mem > 0 ? sh.max_dminus_mem : 1);
+    int rxcap = REG_XCAP;
+    while (rxcap < (int)sh.max_dminus_reg && rxcap < REG_XCAP_MAX) rxcap <<= 1;
+    int parts[NCLS] = {1, 1, 1, 1, 1}, dmin[NCLS] = {0}, dafter[NCLS] = {0};
+    size_t slab_need = 0;
+    for (int c = CLS_R32; c <= CLS_MEM; ++c) {
+      const int w = o.bucket_warps_per_root[c] ? o.bucket_warps_per_root[c] : o.warps_per_root;
+      parts[c] = w > 1 ? w : 1;
+      const int t = o.bucket_donate_threshold[c] ? o.bucket_donate_threshold[c]
+                                                 : o.donate_threshold;
+      dmin[c] = t > 0 ? t : DEFAULT_DONATE_MIN;
+      const int af = o.bucket_donate_after[c] ? o.bucket_donate_after[c] : o.donate_after;
+      dafter[c] = af > 0 ? af : (int)DEFAULT_DONATE_AFTER;
+      if (!sh.cls_cnt[c]) continue;
+      int warps = 0;
+      if ((rc = bk_warps_for_class(c, g->sms, o.wide_blocks, &warps, &block[c], &smem[c])))
+        return finish(rc);
+      const int wpb = block[c] / 32;
+      int64_t want = (int64_t)sh.cls_cnt[c] * parts[c];
+      if (share) want = want > warps ? want : warps;
+      if (want < warps) warps = (int)((want + wpb - 1) / wpb) * wpb;
+      grid[c] = warps / wpb;
+      const size_t need = (size_t)warps * bk_slab_words(c, dcap, xcap, rxcap) * 8;
+      if (need > slab_need) slab_need = need;
+    }
+    if (slab_need > g->slab_bytes) {  // the earlier parts' searches keep the old slab
+      if (g->slab) retired.push_back(g->slab);
+      g->slab = nullptr;
+      g->slab_bytes = 0;
+      MCE_CUDA(cudaMalloc((void **)&g->slab, slab_need));
+      g->slab_bytes = slab_need;
+    }
+    QueueView qv[NCLS];
+    for (int c = CLS_R32; c <= CLS_MEM; ++c) {
+      if (!share || !grid[c]) continue;
+      const uint32_t words = bk_task_words(c, dcap);
+      const size_t need = 256 + (size_t)QUEUE_CAP * 4 + (size_t)QUEUE_CAP * words * 8;
+      if (need > g->qbytes[c] && g->qbuf[c]) {  // ensure_queue would free it in use
+        retired.push_back(g->qbuf[c]);
+        g->qbuf[c] = nullptr;
+        g->qbytes[c] = 0;
+      }
+      if ((rc = ensure_queue(g, c, words, &qv[c]))) return finish(rc);
+    }
+    BKArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.rp = g->rp;
+    a.split = g->split;
+    a.cs = g->cs;
+    a.roots = g->roots + vbeg;
+    a.shape = g->part_shape + p;
+    a.fetch = g->part_fetch + 8 * p;
+    a.hist = g->hist;
+    a.nodes = g->nodes;
+    a.graph_of = bc->graph_of;
+    a.graph_count = bc->graph_count;
+    a.err = g->err;
+    a.slab = g->slab;
+    a.dcap = dcap;
+    a.xcap = xcap;
+    a.rxcap = rxcap;
+    a.hub_of = sh.hub_cnt > 0 ? g->hub_of : nullptr;
+    a.hub_off = g->phub_off[p];
+    a.hub_rows = g->phub_rows[p];
+    a.hub_nx = g->phub_nx[p];
+    a.wait_limit_ns = o.wait_limit_ms > 0 ? (uint64_t)o.wait_limit_ms * 1000000ull : IDLE_LIMIT_NS;
+    a.wide8 = o.wide_blocks == 8 ? 1 : 0;
+    a.level2 = o.level == MCE_LEVEL_L2 ? 1 : 0;
+    a.x_pivot = (o.x_pivot || o.induced == MCE_INDUCED_PX) ? 1 : 0;
+    a.stage = o.stage_lists ? 1 : 0;
+    const int wbits = o.bitmap_width == 64 ? 64 : 32;
+    for (int c : {CLS_MEM, CLS_R64, CLS_R32}) {
+      if (!grid[c]) continue;
+      a.slab_words = bk_slab_words(c, dcap, xcap, rxcap);
+      a.parts = parts[c];
+      a.donate_min = dmin[c];
+      a.donate_after = (uint32_t)dafter[c];
+      a.q = share ? qv[c] : QueueView();
+      if (share && (rc = queue_launch_init(a.q, s, &launches))) return finish(rc);
+      if ((rc = bk_launch(c, wbits, a, grid[c], block[c], smem[c], s, &launches)))
+        return finish(rc);
+    }
+    st.roots += (int64_t)sh.cls_cnt[CLS_R32] + sh.cls_cnt[CLS_R64] + sh.cls_cnt[CLS_MEM];
+    for (int c = 0; c < NCLS && c < 8; ++c) st.class_roots[c] += sh.cls_cnt[c];
+    if ((int32_t)sh.max_dplus > st.max_later_degree) st.max_later_degree = (int32_t)sh.max_dplus;
+    if ((int64_t)sh.max_deg > st.max_degree) st.max_degree = sh.max_deg;
+  }
+  MCE_CUDA(cudaEventRecord(g->ev[3], s));
+  unsigned long long h_hist[MCE_HIST_MAX];
+  unsigned long long h_nodes[2] = {0, 0};
+  uint32_t h_err = 0;
+  MCE_CUDA(cudaMemcpyAsync(h_hist, g->hist, sizeof(h_hist), cudaMemcpyDeviceToHost, s));
+  MCE_CUDA(cudaMemcpyAsync(h_nodes, g->nodes, sizeof(h_nodes), cudaMemcpyDeviceToHost, s));
+  MCE_CUDA(cudaMemcpyAsync(&h_err, g->err, sizeof(h_err), cudaMemcpyDeviceToHost, s));
+  MCE_CUDA(cudaMemcpyAsync(bc->per_graph_out, bc->graph_count,
+                           sizeof(unsigned long long) * bc->G, cudaMemcpyDeviceToHost, s));
+  MCE_CUDA(cudaEventRecord(g->ev[4], s));
+  finish(MCE_OK);
+  int32_t dg = 0;
+  uint32_t perr = 0, rounds = 0, solo = 0;
+  if (g->n > 0 && (rc = peel_read(g->peel_ctl, &dg, &perr, &rounds, &solo, s, nullptr))) return rc;
+  g->degeneracy = dg;
+  g->logged = false;
+  g->search_key[0] ^= 0xFF;  // buffers may have moved: mce_batch_count captures anew
+  if (err_limit) return MCE_ELIMIT;
+  uint64_t tot = 0;
+  for (int i = 0; i < MCE_HIST_MAX; ++i) tot += h_hist[i];
+  *total = tot;
+  if (hist)
+    for (int i = 0; i < MCE_HIST_MAX; ++i) hist[i] = h_hist[i];
+  float ms = 0;
+  // overlapped phases: until the first part is oriented, then every search
+  cudaEventElapsedTime(&ms, g->ev[0], g->ev[1]);
+  st.peel_ms = ms;
+  st.orient_ms = 0;
+  cudaEventElapsedTime(&ms, g->ev[1], g->ev[3]);
+  st.count_ms = ms;
+  cudaEventElapsedTime(&ms, g->ev[0], g->ev[4]);
+  st.total_ms = ms;
+  st.degeneracy = dg;
+  st.tree_nodes = h_nodes[0];
+  st.kernel_launches = launches;
+  st.error_flags = h_err | (perr ? MCE_ERR_WAIT_TIMEOUT : 0);
+  st.peel_rounds = rounds;
+  st.peel_solo_sections = solo;
   if (stats) *stats = st;
   if (perr) return MCE_ETIMEOUT;
   if (h_err & MCE_ERR_WAIT_TIMEOUT) return MCE_ETIMEOUT;
@@ -1274,7 +1559,14 @@ int mce_batch_count_host(mce_batch_t b, const int32_t *row_ptr, const int32_t *c
   }
   const int32_t G = num_graphs;
   const int64_t *vo = vtx_offsets, *ao = arc_offsets;
-  // parts of about equal arc count, whole graphs each; small batches in one
+  // Parts of whole graphs; small batches in one.  When the parts are
+  // searched as they arrive, they grow geometrically (1/16, 2/16, 4/16, 9/16
+  // of the arcs): the first search starts after a short copy, and since the
+  // copy moves arcs about twice as fast as they are searched, each later
+  // part lands before the search reaches it.  Otherwise they are equal.
+  const bool pipelined = !o.log_roots && !o.warp_log && !o.count_ops &&
+                         (o.sched == MCE_SCHED_PLAIN || o.sched == MCE_SCHED_DEGREE);
+  static const int64_t kGeo[MAX_PARTS] = {1, 3, 7, 16};  // cumulative sixteenths
   int k = m >= BATCH_PART_MIN_ARCS ? MAX_PARTS : 1;
   if (k > G) k = G;
   BatchParts P;
@@ -1282,7 +1574,7 @@ int mce_batch_count_host(mce_batch_t b, const int32_t *row_ptr, const int32_t *c
   P.g[0] = 0;
   for (int p = 1; p < k; ++p) {
     int64_t gp = P.g[P.k];
-    const int64_t want = m * p / k;
+    const int64_t want = pipelined && k == MAX_PARTS ? m * kGeo[p - 1] / 16 : m * p / k;
     while (gp < G && ao[gp] < want) ++gp;
     if (gp > P.g[P.k] && gp < G) P.g[++P.k] = gp;
   }
@@ -1331,7 +1623,8 @@ int mce_batch_count_host(mce_batch_t b, const int32_t *row_ptr, const int32_t *c
   P.ao_h = ao;
   BatchCtx bc{b->graph_of, b->graph_count, per_graph_total, b->G, b->vtx_off, b->arc_off, b->order};
   bc.parts = &P;
-  rc = count_impl(b->g, o, total, hist, stats, &bc);
+  rc = pipelined ? count_pipelined(b->g, o, total, hist, stats, &bc)
+                 : count_impl(b->g, o, total, hist, stats, &bc);
   if (rc) cudaStreamSynchronize(b->copy);  // no copy outlives a failed call
   return rc;
 }

@@ -47,12 +47,17 @@ namespace {
 // per-phase cycle breakdown.
 // OPS (opts.count_ops): the variant that sums the algorithmic word
 // operations of every walk (reg_tree / mem_tree), run outside timed calls.
-template <typename Word, int NR, int EV = 0, bool LIST = false, bool XP = false, bool OPS = false>
+// SPLIT: the variant for several warps per root (opts.warps_per_root > 1);
+// the others keep no state for it.  STAGE (opts.stage_lists): the encode's
+// lists are staged in shared memory by 1-D bulk copies (flat_walk_staged).
+template <typename Word, int NR, int EV = 0, bool LIST = false, bool XP = false, bool OPS = false,
+          bool SPLIT = false, bool STAGE = false>
 __global__ void __launch_bounds__(REG_BLOCK, (NR == 1 && sizeof(Word) == 4) ? 6 : (NR == 2 ? 4 : 1))
     bk_reg_kernel(BKArgs a, int cls) {
   __shared__ RegSmem<Word, NR> sm_all[REG_BLOCK / 32];
   RegSmem<Word, NR> &sm = sm_all[threadIdx.x >> 5];
   const int lane = (int)lane_id();
+  if constexpr (STAGE) stage_init();
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const RegSlab<Word> sl = reg_slab<Word>(a, gw);
   const uint32_t beg = a.shape->cls_off[cls], end = a.shape->cls_off[cls + 1];
@@ -64,7 +69,7 @@ __global__ void __launch_bounds__(REG_BLOCK, (NR == 1 && sizeof(Word) == 4) ? 6 
   if (share && lane == 0) atomicAdd(&a.q.hdr->work, 1u);
   // units of work: (root, part) pairs, the parts of a root fetched one
   // after the other so that different warps take them
-  const uint32_t parts = a.parts > 1 ? (uint32_t)a.parts : 1u;
+  const uint32_t parts = SPLIT && a.parts > 1 ? (uint32_t)a.parts : 1u;
   const uint32_t units = (end - beg) * parts;
   for (;;) {
     uint32_t i0 = 0;
@@ -76,10 +81,10 @@ __global__ void __launch_bounds__(REG_BLOCK, (NR == 1 && sizeof(Word) == 4) ? 6 
       if (u >= units) break;
       const int32_t r = a.roots[beg + u / parts];
       MCE_BD(BD_ENCODE);
-      if (parts == 1 || r != rt.r) reg_encode<Word, NR>(a, sm, sl, r, rt);
+      if (parts == 1 || r != rt.r) reg_encode<Word, NR, STAGE>(a, sm, sl, r, rt);
       MCE_BD(BD_OTHER);
       u64 nd = 0, cnt = 0, op = 0;
-      reg_tree<Word, NR, false, EV, LIST, XP, OPS>(a, sm, sl, rt, WOps<Word>::low(rt.d), (Word)0,
+      reg_tree<Word, NR, false, EV, LIST, XP, OPS, SPLIT>(a, sm, sl, rt, WOps<Word>::low(rt.d), (Word)0,
                                                     (Word)0, h0, h1, nd, cnt, bd, &op,
                                                     (int)(u % parts), (int)parts);
       nodes += nd;
@@ -112,7 +117,7 @@ __global__ void __launch_bounds__(REG_BLOCK, (NR == 1 && sizeof(Word) == 4) ? 6 
           const Word X = (Word)__shfl_sync(MCE_FULL, t2, 2);
           const Word S = (Word)__shfl_sync(MCE_FULL, t3, 3);
           MCE_BD(BD_ENCODE);
-          if (r != rt.r) reg_encode<Word, NR>(a, sm, sl, r, rt);
+          if (r != rt.r) reg_encode<Word, NR, STAGE>(a, sm, sl, r, rt);
           u64 nd = 0, cnt = 0, op = 0;
           reg_tree<Word, NR, false, EV, LIST, XP, OPS>(a, sm, sl, rt, P, X, S, h0, h1, nd, cnt, bd,
                                                         &op);
@@ -142,7 +147,7 @@ __global__ void __launch_bounds__(REG_BLOCK, (NR == 1 && sizeof(Word) == 4) ? 6 
 // The wide engine at 4 blocks per SM (96 registers) or, with
 // opts.wide_blocks = 8, at 8 (64 registers): more warps pay on graphs whose
 // wide roots have large shared subtrees (R-MAT), fewer on many small ones.
-template <int EV = 0, int MINB = 1, bool LIST = false, bool OPS = false>
+template <int EV = 0, int MINB = 1, bool LIST = false, bool OPS = false, bool SPLIT = false>
 __global__ void __launch_bounds__(MEM_BLOCK, MINB) bk_mem_kernel(BKArgs a, int cls) {
   __shared__ MemSmem sm_all[MEM_BLOCK / 32];
   __shared__ u64 srows_all[MEM_BLOCK / 32][2 * MEM_SROWS_D];
@@ -158,7 +163,7 @@ __global__ void __launch_bounds__(MEM_BLOCK, MINB) bk_mem_kernel(BKArgs a, int c
   Bd bdv, *bd = &bdv;
   if constexpr (EV == 2) bdv.start();
   if (share && lane == 0) atomicAdd(&a.q.hdr->work, 1u);
-  const uint32_t parts = a.parts > 1 ? (uint32_t)a.parts : 1u;  // warps per root
+  const uint32_t parts = SPLIT && a.parts > 1 ? (uint32_t)a.parts : 1u;  // warps per root
   const uint32_t units = (end - beg) * parts;
   for (;;) {
     uint32_t i0 = 0;
@@ -179,8 +184,8 @@ __global__ void __launch_bounds__(MEM_BLOCK, MINB) bk_mem_kernel(BKArgs a, int c
     }
     __syncwarp();
     u64 nd = 0, cnt = 0, op = 0;
-    mem_tree<false, EV, LIST, OPS>(a, sl, rt, h0, h1, nd, cnt, bd, &op, (int)(i0 % parts),
-                                   (int)parts);
+    mem_tree<false, EV, LIST, OPS, SPLIT>(a, sl, rt, h0, h1, nd, cnt, bd, &op, (int)(i0 % parts),
+                                          (int)parts);
     nodes += nd;
     root_done(a, r, nd, cnt);
     if constexpr (OPS) {
@@ -500,15 +505,47 @@ int bk_launch(int cls, int word_bits, const BKArgs &a, int grid, int block, int 
   }
   if (a.count_ops) {  // the counting variants (no evaluation log, IP pivots only)
     if (cls == CLS_R32 && word_bits == 64)
-      bk_reg_kernel<u64, 1, 0, false, false, true><<<grid, block, smem, s>>>(a, cls);
+      bk_reg_kernel<u64, 1, 0, false, false, true, true><<<grid, block, smem, s>>>(a, cls);
     else if (cls == CLS_R32)
-      bk_reg_kernel<uint32_t, 1, 0, false, false, true><<<grid, block, smem, s>>>(a, cls);
+      bk_reg_kernel<uint32_t, 1, 0, false, false, true, true><<<grid, block, smem, s>>>(a, cls);
     else if (cls == CLS_R64)
-      bk_reg_kernel<u64, 2, 0, false, false, true><<<grid, block, smem, s>>>(a, cls);
+      bk_reg_kernel<u64, 2, 0, false, false, true, true><<<grid, block, smem, s>>>(a, cls);
     else if (cls == CLS_MEM)
-      bk_mem_kernel<0, 1, false, true><<<grid, block, smem, s>>>(a, cls);
+      bk_mem_kernel<0, 1, false, true, true><<<grid, block, smem, s>>>(a, cls);
     else
       return MCE_EINVAL;
+    MCE_CUDA(cudaGetLastError());
+    if (launches) *launches += 1;
+    return MCE_OK;
+  }
+  if (a.stage && cls == CLS_R32 && word_bits == 32 && ev == 0 && a.parts <= 1 && !a.x_pivot) {
+    // the 32-bit engine with its lists staged by bulk copies
+    bk_reg_kernel<uint32_t, 1, 0, false, false, false, false, true><<<grid, block, smem, s>>>(a, cls);
+    MCE_CUDA(cudaGetLastError());
+    if (launches) *launches += 1;
+    return MCE_OK;
+  }
+  if (a.parts > 1 && ev == 0) {  // several warps per root (plain counting or -i px)
+    if (a.x_pivot && cls != CLS_MEM) {
+      if (cls == CLS_R32 && word_bits == 64)
+        bk_reg_kernel<u64, 1, 0, false, true, false, true><<<grid, block, smem, s>>>(a, cls);
+      else if (cls == CLS_R32)
+        bk_reg_kernel<uint32_t, 1, 0, false, true, false, true><<<grid, block, smem, s>>>(a, cls);
+      else
+        bk_reg_kernel<u64, 2, 0, false, true, false, true><<<grid, block, smem, s>>>(a, cls);
+    } else if (cls == CLS_R32 && word_bits == 64) {
+      bk_reg_kernel<u64, 1, 0, false, false, false, true><<<grid, block, smem, s>>>(a, cls);
+    } else if (cls == CLS_R32) {
+      bk_reg_kernel<uint32_t, 1, 0, false, false, false, true><<<grid, block, smem, s>>>(a, cls);
+    } else if (cls == CLS_R64) {
+      bk_reg_kernel<u64, 2, 0, false, false, false, true><<<grid, block, smem, s>>>(a, cls);
+    } else if (cls == CLS_MEM && a.wide8) {
+      bk_mem_kernel<0, 8, false, false, true><<<grid, block, smem, s>>>(a, cls);
+    } else if (cls == CLS_MEM) {
+      bk_mem_kernel<0, 1, false, false, true><<<grid, block, smem, s>>>(a, cls);
+    } else {
+      return MCE_EINVAL;
+    }
     MCE_CUDA(cudaGetLastError());
     if (launches) *launches += 1;
     return MCE_OK;

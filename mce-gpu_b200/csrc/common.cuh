@@ -103,6 +103,70 @@ __device__ __forceinline__ bool grid_sync(GridBarrier *b, uint32_t nblocks, uint
   return ok != 0;
 }
 
+// ---- 1-D bulk copies global -> shared through an mbarrier (the TMA unit's
+// untiled form; no multicast, this GPU's memory only).  Source, destination
+// and size must be multiples of 16 bytes.
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, uint32_t arrivals) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(arrivals)
+               : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// Orders this thread's earlier generic accesses of shared memory before its
+// later async-proxy (bulk copy) accesses.
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long *bar, uint32_t bytes) {
+  unsigned long long state;
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 %0, [%1], %2;"
+               : "=l"(state)
+               : "r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+  (void)state;
+}
+
+__device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, uint32_t bytes,
+                                              unsigned long long *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// One probe of the phase with parity `parity`: true once it has completed.
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(done)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
+// Bounded wait for the phase: false (and MCE_ERR_WAIT_TIMEOUT in *err) if
+// it has not completed within limit_ns.
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, uint32_t parity, uint32_t *err,
+                                          uint64_t limit_ns) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = globaltimer_ns();
+  while (!mbar_try_wait(bar, parity)) {
+    if (globaltimer_ns() - t0 > limit_ns) {
+      atomicOr(err, MCE_ERR_WAIT_TIMEOUT);
+      return false;
+    }
+  }
+  return true;
+}
+
 // Binary search in a sorted int array: index of key in [lo, hi) or -1.
 __device__ __forceinline__ int32_t bsearch_idx(const int32_t *a, int32_t lo, int32_t hi,
                                                int32_t key) {

@@ -212,6 +212,80 @@ __device__ __forceinline__ void flat_walk(const int32_t *__restrict__ cs, int32_
   }
 }
 
+// Staging of the lists a flattened walk reads (opts.stage_lists, the 32-bit
+// engine): each lane copies its list's 16-byte window - start rounded down,
+// end rounded up - from global to shared memory with one 1-D bulk copy, the
+// warp waits on its mbarrier, and the walk reads shared memory.  Per warp
+// of the block: STAGE_WORDS ints of buffer, the mbarrier, and a state word
+// (bit 0: parity of the barrier's next phase; bit 1: staging off after a
+// wait ran out - the warp then loads from global memory).  Only the kernels
+// that stage reference these arrays, so only they allocate them.  Lists
+// whose windows do not fit together take flat_walk.
+constexpr int STAGE_WORDS = 512;
+constexpr uint64_t STAGE_WAIT_NS = 2000000000ull;  // a copy of a few KB takes microseconds
+__shared__ __align__(16) int32_t stage_buf[REG_BLOCK / 32][STAGE_WORDS];
+__shared__ unsigned long long stage_bar[REG_BLOCK / 32];
+__shared__ uint32_t stage_state[REG_BLOCK / 32];
+
+__device__ __forceinline__ void stage_init() {
+  const int w = (int)(threadIdx.x >> 5);
+  if (lane_id() == 0) {
+    mbar_init(&stage_bar[w], 1);
+    stage_state[w] = 0;
+  }
+  __syncwarp();
+}
+
+template <typename F>
+__device__ __forceinline__ bool flat_walk_staged(const int32_t *__restrict__ cs, int32_t b, int len,
+                                                 int32_t *off_sm, int32_t *beg_sm, int32_t *own_sm,
+                                                 uint32_t *err, F f) {
+  const int lane = (int)lane_id(), w = (int)(threadIdx.x >> 5);
+  const uint32_t st0 = stage_state[w];
+  if (st0 & 2u) return false;
+  const int32_t *src = cs + b;
+  const int pad = (int)(((uintptr_t)src >> 2) & 3u);  // ints before the list in its window
+  const int words = len > 0 ? ((pad + len + 3) & ~3) : 0;
+  const int wincl = warp_incl_scan(words);
+  const int total = __shfl_sync(MCE_FULL, wincl, 31);
+  if (total == 0 || total > STAGE_WORDS) return false;
+  const int wbeg = wincl - words;
+  __syncwarp();  // the buffer's last contents are read
+  fence_proxy_async_smem();
+  if (lane == 0) mbar_arrive_expect_tx(&stage_bar[w], (uint32_t)total * 4u);
+  __syncwarp();
+  if (words > 0) bulk_copy_g2s(&stage_buf[w][wbeg], src - pad, (uint32_t)words * 4u, &stage_bar[w]);
+  const uint32_t ph = st0 & 1u;
+  const bool ok = __all_sync(MCE_FULL, mbar_wait(&stage_bar[w], ph, err, STAGE_WAIT_NS));
+  __syncwarp();
+  if (lane == 0) stage_state[w] = (st0 ^ 1u) | (ok ? 0u : 2u);
+  if (!ok) {  // let the copies in flight land before the buffer is given up
+    mbar_wait(&stage_bar[w], ph, err, STAGE_WAIT_NS);
+    __syncwarp();
+    return false;
+  }
+  const int32_t *buf = stage_buf[w];
+  const int incl = warp_incl_scan(len);
+  const int T = __shfl_sync(MCE_FULL, incl, 31);
+  const int off = incl - len;
+  off_sm[lane] = off;
+  beg_sm[lane] = wbeg + pad;  // the list's first element in the buffer
+  int carry = 0;
+  for (int e0 = 0; e0 < T; e0 += 32) {
+    const bool st = len > 0 && off >= e0 && off < e0 + 32;
+    if (st) own_sm[off - e0] = lane;
+    const uint32_t mask = __reduce_or_sync(MCE_FULL, st ? 1u << (off - e0) : 0u);
+    __syncwarp();
+    const uint32_t below = mask & (0xFFFFFFFFu >> (31 - lane));
+    const int t = below ? own_sm[31 - __clz(below)] : carry;
+    carry = __shfl_sync(MCE_FULL, t, 31);
+    const int e = e0 + lane;
+    if (e < T) f(t, buf[beg_sm[t] + (e - off_sm[t])]);
+    __syncwarp();
+  }
+  return true;
+}
+
 // Hash of the root's later neighbours (ids are distinct): 128 slots, so that
 // the probes of the many later-list elements outside P end within ~1.4 slots
 // for the 32-bit engine (4 slots per id) and ~2.5 for the 64-bit one (2).
@@ -287,12 +361,18 @@ struct RegRoot {
   Word r0 = 0, r1 = 0;
 };
 
-template <typename Word, int NR>
+// STAGE: the lists are staged in shared memory by bulk copies (*stg).
+template <typename Word, int NR, bool STAGE = false>
 __device__ void reg_encode(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<Word> &sl,
                            int32_t r, RegRoot<Word> &rt) {
   using O = WOps<Word>;
   const int lane = (int)lane_id();
   const uint32_t lt = (1u << lane) - 1u;
+  auto walk = [&](int32_t b, int len, auto f) {
+    if constexpr (STAGE)
+      if (flat_walk_staged(a.cs, b, len, sm.off, sm.beg, sm.own, a.err, f)) return;
+    flat_walk(a.cs, b, len, sm.off, sm.beg, sm.own, f);
+  };
   const int32_t sb = a.split[r], d = a.rp[r + 1] - sb, ub = a.rp[r], u = sb - ub;
   if (u > sl.xc) {  // more earlier neighbours than the slab's rows (classification bounds it)
     if (lane == 0) atomicOr(a.err, MCE_ERR_XROWS);
@@ -324,7 +404,7 @@ __device__ void reg_encode(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab
     }
     sm.xs[lane] = 0;
     __syncwarp();
-    flat_walk(a.cs, b, len, sm.off, sm.beg, sm.own, [&](int t, int32_t w) {
+    walk(b, len, [&](int t, int32_t w) {
       const int i = p_find(sm, w);
       if (i >= 0) {
         if (t < d) {
@@ -363,7 +443,7 @@ __device__ void reg_encode(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab
       vb = a.split[v];
       vlen = a.rp[v + 1] - vb;
     }
-    flat_walk(a.cs, vb, vlen, sm.off, sm.beg, sm.own, [&](int t, int32_t w) {
+    walk(vb, vlen, [&](int t, int32_t w) {
       const int i = p_find(sm, w);
       if (i >= 0) {
         const int j = c * 32 + t;
@@ -418,7 +498,7 @@ __device__ void reg_encode(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab
         }
         sm.xs[lane] = 0;
         __syncwarp();
-        flat_walk(a.cs, xb, xlen, sm.off, sm.beg, sm.own, [&](int t, int32_t w) {
+        walk(xb, xlen, [&](int t, int32_t w) {
           const int i = p_find(sm, w);
           if (i >= 0) atomicOr(&sm.xs[t], O::bit(i));
         });
@@ -599,8 +679,9 @@ __device__ __forceinline__ void reg_emit(const BKArgs &a, const RegSmem<Word, NR
 // neighbour (select_pivot_from_P, :338-364).  A donated node is counted by
 // the warp that created it.  The clique shortcuts are off, so every node of
 // the tree is walked (same nodes, counts and histogram).
+// SPLIT: the variant for several warps per root (part / parts below).
 template <typename Word, int NR, bool Budget = false, int EV = 0, bool LIST = false,
-          bool XP = false, bool OPS = false>
+          bool XP = false, bool OPS = false, bool SPLIT = false>
 __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<Word> &sl,
                          const RegRoot<Word> &rt, Word P, Word X, Word S, u64 &h0, u64 &h1,
                          u64 &nodes, u64 &cnt, Bd *bd = nullptr, u64 *ops = nullptr,
@@ -749,7 +830,8 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
     X |= vb;
     // several warps per root: this one walks every parts-th first-level
     // branch (the others still move from P to X, as the full walk would)
-    if (parts > 1 && depth == 0 && (b0++ % parts) != part) continue;
+    if constexpr (SPLIT)
+      if (parts > 1 && depth == 0 && (b0++ % parts) != part) continue;
     ++nodes;
     if constexpr (OPS) *ops += 2 * w32 * (u64)O::popc(Pc | Xc) + 4 * w32;
     if (Budget && a.node_budget && nodes > a.node_budget) {  // a serving request over its budget
@@ -1138,8 +1220,10 @@ __device__ __forceinline__ void mem_leaf(const BKArgs &a, const Slab &sl, int32_
   }
 }
 
-// OPS: the algorithmic word operations, as in reg_tree.
-template <bool Budget = false, int EV = 0, bool LIST = false, bool OPS = false>
+// OPS: the algorithmic word operations, SPLIT: several warps per root, as
+// in reg_tree.
+template <bool Budget = false, int EV = 0, bool LIST = false, bool OPS = false,
+          bool SPLIT = false>
 __device__ void mem_tree(const BKArgs &a, const Slab &sl, const MemRoot &rt, u64 &h0, u64 &h1,
                          u64 &nodes, u64 &cnt, Bd *bd = nullptr, u64 *ops = nullptr,
                          int part = 0, int parts = 1) {
@@ -1233,7 +1317,8 @@ __device__ void mem_tree(const BKArgs &a, const Slab &sl, const MemRoot &rt, u64
     }
     __syncwarp();
     // several warps per root: every parts-th first-level branch is this one's
-    if (parts > 1 && depth == 0 && (b0++ % parts) != part) continue;
+    if constexpr (SPLIT)
+      if (parts > 1 && depth == 0 && (b0++ % parts) != part) continue;
     ++nodes;
     if (Budget && a.node_budget && nodes > a.node_budget) {  // a serving request over its budget
       if (lane == 0) atomicOr(a.err, MCE_ERR_BUDGET);

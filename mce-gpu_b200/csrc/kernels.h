@@ -138,6 +138,8 @@ struct BKArgs {
   unsigned long long list_cap;   // words list_buf holds
   int32_t parts;                 // warps per root of the launched class (<= 1: one); each
                                  // takes every parts-th first-level branch of the root
+  int32_t stage;                 // 1: the 32-bit engine stages its lists by bulk copies
+                                 // (cs must have 16 readable bytes past its end)
   int32_t count_ops;             // 1: the counting variants sum the algorithmic word ops ...
   unsigned long long *ops;       // ... into *ops ...
   unsigned long long *root_ops;  // ... and per root (nullable [n])
@@ -152,21 +154,29 @@ int queue_launch_init(const QueueView &q, cudaStream_t s, int *launches);
 // ---- cost model -----------------------------------------------------------------
 constexpr int MLP_IN = 8, MLP_HIDDEN = 64;
 constexpr int MLP_MIN_LATER = 16;  // roots the model sees: at least this many later neighbours
+// The learned schedule runs the model only on the roots whose trees decide
+// the tails of the search (the 64-bit-row and wide roots); the others keep
+// the degree heuristic.  With every root from MLP_MIN_LATER on, the feature
+// pass cost 5.3 ms per call on the 4,096-graph batch.
+constexpr int SCHED_MIN_LATER = 33;
 constexpr int MLP_PARAMS = MLP_HIDDEN * MLP_IN + MLP_HIDDEN + MLP_HIDDEN * MLP_HIDDEN + MLP_HIDDEN +
                            MLP_HIDDEN + 1;
+// Features of the roots with at least min_later later neighbours (0:
+// MLP_MIN_LATER), listed in cand / *cand_count.
 int features_launch(int64_t n, const int32_t *rp, const int32_t *split, const int32_t *cs,
                     const int32_t *core, float *out, int32_t *cand, uint32_t *cand_count, int sms,
-                    cudaStream_t s, int *launches);
+                    cudaStream_t s, int *launches, int min_later = 0);
 int mlp_forward_launch(const void *wh, const float *X, const int32_t *idx, const uint32_t *idx_count,
                        int64_t count, float *out, int sms, cudaStream_t s, int *launches);
 int mlp_grad_launch(const void *wh, const float *X, const float *Y, const int32_t *idx,
                     int64_t begin, int64_t end, float *grad, float *loss, cudaStream_t s);
 int mlp_adam_launch(float *master, void *wh, float *grad, float *m1, float *m2, float lr,
                     int step, cudaStream_t s);
+// Sort keys by cost: with `cost`, roots with at least cost_min later
+// neighbours take it and the others the degree heuristic.
 int rekey_launch(int64_t n, uint32_t *keys, const float *cost, const int32_t *rp,
                  const int32_t *split, uint8_t *policy, float heavy_cost, float share_cost,
-                 int sms, cudaStream_t s,
-                 int *launches);
+                 int sms, cudaStream_t s, int *launches, int cost_min = 0);
 
 // ---- batches ------------------------------------------------------------------
 int batch_rebase_launch(const int32_t *rp_local, const int32_t *col_local,

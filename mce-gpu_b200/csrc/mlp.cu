@@ -51,11 +51,11 @@ constexpr int FEAT_MIN = MLP_MIN_LATER;
 // their order does not matter).
 __global__ void cand_list_kernel(int64_t n, const int32_t *__restrict__ rp,
                                  const int32_t *__restrict__ split, int32_t *list,
-                                 uint32_t *count) {
+                                 uint32_t *count, int min_later) {
   const int lane = (int)lane_id();
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v - lane < n; v += stride) {
-    const bool c = v < n && rp[v + 1] - split[v] >= FEAT_MIN;
+    const bool c = v < n && rp[v + 1] - split[v] >= min_later;
     const uint32_t mk = __ballot_sync(MCE_FULL, c);
     if (!mk) continue;
     uint32_t base = 0;
@@ -309,24 +309,28 @@ __global__ void adam_kernel(float *__restrict__ master, __half *__restrict__ wh,
 // larger first; every other root keeps the key 0x0FFFFFFF, so the stable
 // sort leaves them in vertex order (neighbouring roots share adjacency
 // lists, and in a batch each graph stays together in L2).
+// With a model, roots with at least cost_min later neighbours take its
+// prediction and the others the degree heuristic.
 __global__ void rekey_kernel(int64_t n, uint32_t *keys, const float *__restrict__ cost,
                              const int32_t *__restrict__ rp, const int32_t *__restrict__ split,
-                             uint8_t *policy, float heavy_cost, float share_cost) {
+                             uint8_t *policy, float heavy_cost, float share_cost, int cost_min) {
   for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n;
        v += (int64_t)gridDim.x * blockDim.x) {
     const uint32_t cls = keys[v] & 0xF;
+    const int32_t dpi = rp[v + 1] - split[v];
+    const bool learned = cost && dpi >= cost_min;
     float c;
-    if (cost) {
+    if (learned) {
       c = cost[v];
     } else {  // degree heuristic: trees grow with the later degree
-      const float dp = (float)(rp[v + 1] - split[v]);
+      const float dp = (float)dpi;
       c = dp >= 16.f ? log2f(1.f + dp * dp * log2f(2.f + (float)(split[v] - rp[v]))) : 0.f;
     }
     c = c < 0.f ? 0.f : (c > 63.f ? 63.f : c);
     const bool heavy = c >= heavy_cost;
     const uint32_t q = heavy ? (uint32_t)(c * (float)(1 << 22)) : 0u;  // < 2^28
     keys[v] = (cls << 28) | (0x0FFFFFFFu - q);
-    if (policy) policy[v] = cost && c >= share_cost ? 1 : 0;
+    if (policy) policy[v] = learned && c >= share_cost ? 1 : 0;
   }
 }
 
@@ -334,10 +338,11 @@ __global__ void rekey_kernel(int64_t n, uint32_t *keys, const float *__restrict_
 
 int features_launch(int64_t n, const int32_t *rp, const int32_t *split, const int32_t *cs,
                     const int32_t *core, float *out, int32_t *cand, uint32_t *cand_count, int sms,
-                    cudaStream_t s, int *launches) {
+                    cudaStream_t s, int *launches, int min_later) {
   if (n == 0) return MCE_OK;
   MCE_CUDA(cudaMemsetAsync(cand_count, 0, sizeof(uint32_t), s));
-  cand_list_kernel<<<sms * 8, 256, 0, s>>>(n, rp, split, cand, cand_count);
+  cand_list_kernel<<<sms * 8, 256, 0, s>>>(n, rp, split, cand, cand_count,
+                                           min_later > 0 ? min_later : FEAT_MIN);
   MCE_CUDA(cudaGetLastError());
   features_kernel<<<sms * 8, 256, 0, s>>>(cand, cand_count, rp, split, cs, core, out);
   MCE_CUDA(cudaGetLastError());
@@ -387,10 +392,10 @@ int mlp_adam_launch(float *master, void *wh, float *grad, float *m1, float *m2, 
 
 int rekey_launch(int64_t n, uint32_t *keys, const float *cost, const int32_t *rp,
                  const int32_t *split, uint8_t *policy, float heavy_cost, float share_cost,
-                 int sms, cudaStream_t s,
-                 int *launches) {
+                 int sms, cudaStream_t s, int *launches, int cost_min) {
   if (n == 0) return MCE_OK;
-  rekey_kernel<<<sms * 8, 256, 0, s>>>(n, keys, cost, rp, split, policy, heavy_cost, share_cost);
+  rekey_kernel<<<sms * 8, 256, 0, s>>>(n, keys, cost, rp, split, policy, heavy_cost, share_cost,
+                                       cost_min);
   MCE_CUDA(cudaGetLastError());
   if (launches) *launches += 1;
   return MCE_OK;

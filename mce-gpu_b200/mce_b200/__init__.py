@@ -50,7 +50,7 @@ class _Opts(C.Structure):
                 ("wait_limit_ms", C.c_int32), ("count_ops", C.c_int32),
                 ("bucket_warps_per_root", C.c_int32 * 3),
                 ("bucket_donate_threshold", C.c_int32 * 3),
-                ("bucket_donate_after", C.c_int32 * 3),
+                ("bucket_donate_after", C.c_int32 * 3), ("stage_lists", C.c_int32),
                 ("stream", C.c_void_p), ("model", C.c_void_p)]
 
 
@@ -378,8 +378,8 @@ def make_opts(*, sched=SCHED_PLAIN, bitmap_width=0, log_roots=False, level=LEVEL
               peel_solo_max=0, donate_after=0, cuda_graph=0, heavy_log2=0, share_log2=0,
               warp_log=False, wide_blocks=0, wait_limit_ms=0, count_ops=False,
               warps_per_root=0, bucket_warps_per_root=(0, 0, 0),
-              bucket_donate_threshold=(0, 0, 0), bucket_donate_after=(0, 0, 0), model=None,
-              stream=None) -> _Opts:
+              bucket_donate_threshold=(0, 0, 0), bucket_donate_after=(0, 0, 0), stage_lists=0,
+              model=None, stream=None) -> _Opts:
     o = _Opts()
     _lib.mce_opts_default(C.byref(o))
     o.sched, o.bitmap_width, o.log_roots = sched, bitmap_width, int(bool(log_roots))
@@ -391,6 +391,7 @@ def make_opts(*, sched=SCHED_PLAIN, bitmap_width=0, log_roots=False, level=LEVEL
     o.wait_limit_ms = wait_limit_ms
     o.count_ops = int(bool(count_ops))
     o.warps_per_root = warps_per_root
+    o.stage_lists = int(stage_lists)
     for i in range(3):
         o.bucket_warps_per_root[i] = int(bucket_warps_per_root[i])
         o.bucket_donate_threshold[i] = int(bucket_donate_threshold[i])

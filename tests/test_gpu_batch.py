@@ -137,3 +137,55 @@ def test_batch_peel_numbering_matches_single_graphs():
     assert list(rb.per_graph) == single_counts
     assert rb.stats["tree_nodes"] == single_nodes
     assert rb.stats["degeneracy"] == degen
+
+
+def _concat(graphs):
+    rp = np.concatenate([g.row_ptr[:g.n + 1] for g in graphs]).astype(np.int32)
+    col = np.concatenate([g.col for g in graphs]).astype(np.int32)
+    vo = np.cumsum([0] + [g.n + 1 for g in graphs]).astype(np.int64)
+    ao = np.cumsum([0] + [g.m for g in graphs]).astype(np.int64)
+    return mce.HostGraph(rp, col, int(sum(g.n for g in graphs)), int(col.size), len(graphs), vo, ao)
+
+
+def _hub(n, seed):
+    """Vertex 0 adjacent to all, in a K8 peeled last: a hub root (n - 8
+    earlier neighbours, 7 later ones)."""
+    base = mce.gen_er(n, 6.0 / n, seed)
+    s, d = [], []
+    for v in range(base.n):
+        for w in base.col[base.row_ptr[v]:base.row_ptr[v + 1]]:
+            if v < w:
+                s.append(v); d.append(int(w))
+    s += [0] * (n - 1)
+    d += list(range(1, n))
+    for v in range(1, 8):
+        for w in range(v + 1, 8):
+            s.append(v); d.append(w)
+    return mce.from_edges(np.array(s), np.array(d), n)
+
+
+@pytest.mark.parametrize("kw", [
+    {}, {"sched": mce.SCHED_DEGREE}, {"warps_per_root": 2},
+    {"bucket_warps_per_root": (1, 2, 4), "bucket_donate_threshold": (10, 16, 6)},
+    {"x_pivot": 1}, {"log_roots": True},  # the last one: one search after all parts
+], ids=["plain", "degree", "w2", "buckets", "ipx", "logged"])
+def test_batch_count_host_part_by_part_search(kw):
+    """Parts searched as they land (hub roots in early and late parts, a
+    wide-engine R-MAT graph): per-graph counts equal the resident batch's and
+    the oracle's, twice in a row, and the resident count after it too."""
+    cl = mce.gen_chung_lu_batch(120, 64, 8192, 2.3, 8, 32, 5, 5, 40, 7)
+    graphs = [_hub(3000, 1)] + [cl.graph(i) for i in range(cl.num_graphs)] + \
+        [_hub(6000, 2), mce.gen_rmat(11, 16, 0.57, 0.19, 0.19, 3)]
+    hb = _concat(graphs)
+    assert hb.m >= 1 << 20
+    want = np.array([oracle.count(g)[0] for g in graphs], np.uint64)
+    with mce.Batch(hb) as db:
+        ref = db.count(**{k: v for k, v in kw.items() if k != "log_roots"})
+        assert np.array_equal(ref.per_graph, want)
+        for _ in range(2):
+            h = _count_host(db, hb, **kw)
+            assert h.stats["error_flags"] == 0
+            assert np.array_equal(h.per_graph, want) and h.total == int(want.sum())
+            assert np.array_equal(h.hist, ref.hist)
+        again = db.count()
+    assert np.array_equal(again.per_graph, want)
