@@ -84,6 +84,9 @@ def parse_args():
     p.add_argument("--rate", type=float, default=2000.0, help="serve: Poisson arrivals per second")
     p.add_argument("--requests", type=int, default=4000, help="serve: requests per timed step")
     p.add_argument("--max-nodes", type=int, default=0, help="serve: search-node budget per request")
+    p.add_argument("--small-cap", type=int, default=None,
+                   help="serve: footprint bound of the 256-thread slots (0: one slot class; "
+                        "default: automatic)")
     p.add_argument("--scale", type=int, default=15)
     p.add_argument("--graphs", type=int, default=4096)
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -588,7 +591,7 @@ def extra_serve(args, local_rank):
     import oracle
     hg = mce.gen_ba(4_000_000, 8, 31, 200, 20, 60)
     g = mce.Graph.from_host(hg, device=local_rank)
-    s = mce.Serve(g, ego_cap=args.ego_cap)
+    s = mce.Serve(g, ego_cap=args.ego_cap, small_cap=args.small_cap)
     try:
         s.run(*serve_trace(hg.n, 256, 2000.0, 1000))  # first touch of the slots
         res_all, lat_all, wall = [], [], 0.0
@@ -622,7 +625,8 @@ def extra_serve(args, local_rank):
             "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99), "max_ms": float(lat.max()),
             "requests_per_s": len(res) / wall,
             "cliques_per_s": float(res["count"][ok].sum()) / wall,
-            "slots": st["slots"], "peak_in_flight": st.get("peak_running"),
+            "slots": st["slots"], "small_slots": st["small_slots"],
+            "small_cap": st["small_cap"], "peak_in_flight": st["peak_in_flight"],
             "oracle_sample": {"checked": checked, "mismatches": mism}}
 
 
@@ -671,7 +675,7 @@ def run_serve(args, rank, world, local_rank):
     hg, desc = serve_graph(args)
     log(f"serve: resident graph n={hg.n} arcs={hg.m}")
     g = mce.Graph.from_host(hg, device=local_rank)
-    s = mce.Serve(g, ego_cap=args.ego_cap, max_nodes=args.max_nodes)
+    s = mce.Serve(g, ego_cap=args.ego_cap, max_nodes=args.max_nodes, small_cap=args.small_cap)
     try:
         for w in range(args.warmup):  # short traces: first-touch of arenas and code
             seeds, arr = serve_trace(hg.n, 256, args.rate, 1000 + w)
@@ -753,7 +757,9 @@ def run_serve(args, rank, world, local_rank):
                          "requests_per_s": len(res_b) / burst_s,
                          "cliques_per_s": float(res_b["count"][res_b["status"] == mce.OK].sum())
                          / burst_s, "p99_ms": pct(lat_b / 1e3, 99)},
-            "slots": st["slots"], "arena_bytes": st["arena_bytes"], "slab_bytes": st["slab_bytes"],
+            "slots": st["slots"], "small_slots": st["small_slots"], "small_cap": st["small_cap"],
+            "peak_in_flight": st["peak_in_flight"],
+            "arena_bytes": st["arena_bytes"], "slab_bytes": st["slab_bytes"],
             "oracle_sample": {"checked": checked, "mismatches": mism},
             "parallelism": f"replicas x{world}",
         },

@@ -53,9 +53,12 @@ extern "C" {
 /* ---- options ------------------------------------------------------------ */
 /* -p (include/config.h:52-61): level of the subtrees that are parallelised.
  * L1: a root's subtrees go to idle warps once its walk is under way
- * (donate_after nodes); L2: its first-level subtrees (one per edge from the
- * root, the reference's edge-rooted L2 instances) are offered to idle warps
- * at once.                                                                  */
+ * (donate_after nodes).  L2: the reference's edge-rooted scheme
+ * (mce/mce_kernel_wl.cuh:307-485): every oriented edge (r, v) is a unit
+ * whose candidates are the triangle list N+(r) & N+(v), whose pivot comes
+ * from them alone, and whose outside set is the neighbours of r before v in
+ * the degeneracy order adjacent to v; units are offered to idle warps at
+ * once.  Same counts; the trees are the reference's L2 trees.              */
 #define MCE_LEVEL_L1 1
 #define MCE_LEVEL_L2 2
 /* -i (include/config.h:72-81): which sets the induced subgraph is built on */
@@ -92,8 +95,8 @@ typedef struct mce_opts {
                                neighbours adjacent to the chosen set, and prune
                                a subtree when one of them covers P (the -i px
                                rule; also set by induced = MCE_INDUCED_PX).
-                               Register engines only; the count is unchanged,
-                               the search trees are not                      */
+                               All engines; the count is unchanged, the
+                               search trees are not                          */
   int32_t peel_solo_max;    /* 0 = default (off); < 0 = off; > 0: frontiers of at most
                                this many vertices are peeled by one block           */
   int32_t donate_after;     /* 0 = default (256): a warp shares subtrees of a
@@ -502,14 +505,23 @@ int mce_batch_autotune(mce_batch_t b, const mce_opts_t *base, const char *table_
  * A request whose ego graph has at least 1,024 vertices opens its root
  * search to slots that have nothing to do, so a large request does not
  * run on one block alone while the GPU idles.
+ * Admission by footprint: with small_cap > 0 the slots come in two
+ * classes.  The first big_slots blocks are whole-block slots (1,024
+ * threads) for any request; every other block holds four 256-thread slots
+ * for requests whose bound deg(seed) + sum of its neighbours' degrees + 1
+ * is at most small_cap (computed for every vertex at open), so many small
+ * requests run side by side instead of one per block.  Such a request goes
+ * to the small slots only while every whole-block slot holds a request
+ * (submitted and not yet polled): below that load a whole block answers it
+ * sooner.  Request ids carry the class in bit 0.
  * While requests keep coming the kernel stays resident on every SM; a
  * cudaDeviceSynchronize by the caller returns only after the slots have
  * been idle for idle_ms (or after mce_serve_close).                       */
 typedef struct mce_serve *mce_serve_t;
 
 typedef struct mce_serve_opts {
-  int32_t ego_cap;  /* ego-graph vertex cap, 2..4096 (default 1024)          */
-  int32_t slots;    /* concurrent requests; <= 0: as many blocks as fit      */
+  int32_t ego_cap;  /* ego-graph vertex cap, 2..16384 (default 1024)         */
+  int32_t slots;    /* resident blocks; <= 0: as many as fit                 */
   uint32_t ring;    /* requests submitted and not yet polled (default 4096)  */
   int32_t idle_ms;  /* a slot idle this long leaves; the next submit or poll
                        relaunches the kernel (default 1000)                  */
@@ -517,7 +529,12 @@ typedef struct mce_serve_opts {
                        ego_cap * (ego_cap - 1)).  More: status MCE_ELIMIT    */
   int64_t max_nodes; /* search-tree nodes per request; 0: no limit.  More:
                         status MCE_ELIMIT (the request's search stops)       */
-  int64_t reserved[3];
+  int32_t small_cap; /* footprint bound of the 256-thread slots' requests:
+                        0 one class only; < 0 automatic (1,024 when ego_cap
+                        is above 2,048, else 0); else 2..ego_cap            */
+  int32_t big_slots; /* whole-block slots when small_cap is on; <= 0: half
+                        the blocks (at least one block stays split)         */
+  int64_t reserved[2];
 } mce_serve_opts_t;
 
 typedef struct mce_serve_result {
@@ -541,12 +558,15 @@ typedef struct mce_serve_result {
                                        or a slab's earlier rows (0x4)       */
 
 typedef struct mce_serve_stats {
-  int32_t slots, running;
+  int32_t slots, running;   /* slots of both classes                          */
   uint32_t ring, pad;
   uint64_t submitted, served, tree_nodes;
   int64_t kernel_launches;
   uint64_t arena_bytes, slab_bytes;
   uint64_t helps;     /* times an idle slot joined another slot's search    */
+  int32_t small_slots; /* of `slots`: the 256-thread ones                   */
+  int32_t small_cap;   /* their footprint bound (0: one class)              */
+  uint64_t peak_in_flight; /* most requests held by slots at once           */
 } mce_serve_stats_t;
 
 void mce_serve_opts_default(mce_serve_opts_t *o);

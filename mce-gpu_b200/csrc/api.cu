@@ -179,6 +179,16 @@ struct BatchParts {
   const int64_t *vo_h, *ao_h;           // host: the layout
 };
 
+// the most vertices of a graph of part p
+inline int64_t part_max_n(const BatchParts &P, int p) {
+  int64_t mx = 0;
+  for (int64_t g = P.g[p]; g < P.g[p + 1]; ++g) {
+    const int64_t n = P.vo_h[g + 1] - P.vo_h[g] - 1;
+    if (n > mx) mx = n;
+  }
+  return mx;
+}
+
 struct BatchCtx {
   const int32_t *graph_of;             // device, n
   unsigned long long *graph_count;     // device, G
@@ -187,6 +197,7 @@ struct BatchCtx {
   const int64_t *vtx_off, *arc_off;    // device, G + 1: the uploaded layout
   const int32_t *order;                // device, G: graphs largest first (within each part)
   const BatchParts *parts = nullptr;   // nullable: rebase, peel and orient part by part
+  int64_t max_n = 0;                   // the most vertices of a graph (0: unknown)
 };
 
 int check_args(const int32_t *row_ptr, const int32_t *col, int64_t n, int64_t m) {
@@ -221,7 +232,7 @@ int run_peel(mce_graph *g, cudaStream_t s, int *launches, int solo_opt = 0,
   const PeelArgs pa = peel_args(g, solo_opt);
   if (bc)  // a batch: every graph peeled by one block, no grid-wide rounds
     return peel_segments_launch(pa, bc->vtx_off, bc->arc_off, bc->order, (int32_t)bc->G, s,
-                                launches);
+                                launches, -1, bc->max_n);
   return peel_launch(pa, s, launches);
 }
 
@@ -309,7 +320,7 @@ int run_parts(mce_graph *g, cudaStream_t s, int *launches, const BatchCtx *bc, i
     if (rc) return rc;
     if (vend > vbeg &&
         (rc = peel_segments_launch(pa, bc->vtx_off, bc->arc_off, bc->order + g0,
-                                   (int32_t)(g1 - g0), sp, launches, p)))
+                                   (int32_t)(g1 - g0), sp, launches, p, part_max_n(P, p))))
       return rc;
     OrientArgs oa = orient_args(g);
     oa.v0 = vbeg;
@@ -646,7 +657,8 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   if (o.bitmap_width != 0 && o.bitmap_width != 32 && o.bitmap_width != 64) return MCE_EINVAL;
   if (o.wide_blocks != 0 && o.wide_blocks != 4 && o.wide_blocks != 8) return MCE_EINVAL;
   // the word-op count follows the IP walk; it is not an evaluation or listing run
-  if (o.count_ops && (o.x_pivot || o.induced == MCE_INDUCED_PX || o.warp_log || lc))
+  if (o.count_ops &&
+      (o.x_pivot || o.induced == MCE_INDUCED_PX || o.warp_log || lc || o.level == MCE_LEVEL_L2))
     return MCE_EINVAL;
   if (o.warps_per_root < 0 || o.warps_per_root > 32) return MCE_EINVAL;
   for (int c = 0; c < 3; ++c)
@@ -729,7 +741,8 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   int parts[NCLS] = {1, 1, 1, 1, 1}, dmin[NCLS] = {0}, dafter[NCLS] = {0};
   for (int c = CLS_R32; c <= CLS_MEM; ++c) {
     const int w = o.bucket_warps_per_root[c] ? o.bucket_warps_per_root[c] : o.warps_per_root;
-    parts[c] = w > 1 && !o.warp_log && !lc ? w : 1;  // evaluation and listing: one warp
+    // evaluation, listing and L2 (whose units split a root already): one warp
+    parts[c] = w > 1 && !o.warp_log && !lc && o.level != MCE_LEVEL_L2 ? w : 1;
     const int t = o.bucket_donate_threshold[c] ? o.bucket_donate_threshold[c] : o.donate_threshold;
     dmin[c] = t > 0 ? t : DEFAULT_DONATE_MIN;
     const int af = o.bucket_donate_after[c] ? o.bucket_donate_after[c] : o.donate_after;
@@ -797,6 +810,7 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   a.policy = policy;
   a.wide8 = o.wide_blocks == 8 ? 1 : 0;
   a.level2 = o.level == MCE_LEVEL_L2 ? 1 : 0;
+  a.prio = g->prio;
   a.x_pivot = (o.x_pivot || o.induced == MCE_INDUCED_PX) ? 1 : 0;
   a.count_ops = o.count_ops ? 1 : 0;
   a.stage = o.stage_lists ? 1 : 0;
@@ -1072,7 +1086,7 @@ int count_pipelined(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t
       return finish(rc);
     if (vend > vbeg &&
         (rc = peel_segments_launch(pa, bc->vtx_off, bc->arc_off, bc->order + g0,
-                                   (int32_t)(g1 - g0), sp, &launches, p)))
+                                   (int32_t)(g1 - g0), sp, &launches, p, part_max_n(P, p))))
       return finish(rc);
     OrientArgs oa = orient_args(g);
     oa.v0 = vbeg;
@@ -1139,7 +1153,7 @@ int count_pipelined(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t
     size_t slab_need = 0;
     for (int c = CLS_R32; c <= CLS_MEM; ++c) {
       const int w = o.bucket_warps_per_root[c] ? o.bucket_warps_per_root[c] : o.warps_per_root;
-      parts[c] = w > 1 ? w : 1;
+      parts[c] = w > 1 && o.level != MCE_LEVEL_L2 ? w : 1;
       const int t = o.bucket_donate_threshold[c] ? o.bucket_donate_threshold[c]
                                                  : o.donate_threshold;
       dmin[c] = t > 0 ? t : DEFAULT_DONATE_MIN;
@@ -1200,6 +1214,7 @@ int count_pipelined(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t
     a.wait_limit_ns = o.wait_limit_ms > 0 ? (uint64_t)o.wait_limit_ms * 1000000ull : IDLE_LIMIT_NS;
     a.wide8 = o.wide_blocks == 8 ? 1 : 0;
     a.level2 = o.level == MCE_LEVEL_L2 ? 1 : 0;
+    a.prio = g->prio;
     a.x_pivot = (o.x_pivot || o.induced == MCE_INDUCED_PX) ? 1 : 0;
     a.stage = o.stage_lists ? 1 : 0;
     const int wbits = o.bitmap_width == 64 ? 64 : 32;
@@ -1386,6 +1401,7 @@ struct mce_batch {
   int32_t *order = nullptr;    // graph ids by arc count, largest first (per-graph peel)
   int32_t *order_h = nullptr;  // its pinned host staging copy
   int64_t cap_rows = -1, cap_m = -1, cap_g = -1;
+  int64_t max_n = 0;           // the most vertices of a graph of the batch
   // mce_batch_count_host: copies on their own stream, one event per part
   cudaStream_t copy = nullptr;
   cudaEvent_t start = nullptr, ready[MAX_PARTS] = {nullptr};
@@ -1466,6 +1482,8 @@ int batch_load(mce_batch *b, const int32_t *row_ptr, const int32_t *col, const i
   // the previous call's copy out of order_h finished before that call returned
   int32_t *order = b->order_h;
   for (int32_t i = 0; i < G; ++i) order[i] = i;
+  b->max_n = 0;
+  for (int32_t i = 0; i < G; ++i) b->max_n = std::max<int64_t>(b->max_n, vo[i + 1] - vo[i] - 1);
   std::stable_sort(order, order + G, [&](int32_t x, int32_t y) {
     return ao[x + 1] - ao[x] > ao[y + 1] - ao[y];
   });
@@ -1539,6 +1557,7 @@ int mce_batch_count(mce_batch_t b, const mce_opts_t *opts, uint64_t *per_graph_t
     o.cuda_graph = 1;
   }
   BatchCtx bc{b->graph_of, b->graph_count, per_graph_total, b->G, b->vtx_off, b->arc_off, b->order};
+  bc.max_n = b->max_n;
   return count_impl(b->g, o, total, hist, stats, &bc);
 }
 
@@ -1592,6 +1611,8 @@ int mce_batch_count_host(mce_batch_t b, const int32_t *row_ptr, const int32_t *c
   // graphs largest first within each part (the per-graph peel's order)
   int32_t *order = b->order_h;
   for (int32_t i = 0; i < G; ++i) order[i] = i;
+  b->max_n = 0;
+  for (int32_t i = 0; i < G; ++i) b->max_n = std::max<int64_t>(b->max_n, vo[i + 1] - vo[i] - 1);
   for (int p = 0; p < P.k; ++p)
     std::stable_sort(order + P.g[p], order + P.g[p + 1], [&](int32_t x, int32_t y) {
       return ao[x + 1] - ao[x] > ao[y + 1] - ao[y];
@@ -1623,6 +1644,7 @@ int mce_batch_count_host(mce_batch_t b, const int32_t *row_ptr, const int32_t *c
   P.ao_h = ao;
   BatchCtx bc{b->graph_of, b->graph_count, per_graph_total, b->G, b->vtx_off, b->arc_off, b->order};
   bc.parts = &P;
+  bc.max_n = b->max_n;
   rc = pipelined ? count_pipelined(b->g, o, total, hist, stats, &bc)
                  : count_impl(b->g, o, total, hist, stats, &bc);
   if (rc) cudaStreamSynchronize(b->copy);  // no copy outlives a failed call

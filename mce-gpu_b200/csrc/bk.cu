@@ -50,8 +50,9 @@ namespace {
 // SPLIT: the variant for several warps per root (opts.warps_per_root > 1);
 // the others keep no state for it.  STAGE (opts.stage_lists): the encode's
 // lists are staged in shared memory by 1-D bulk copies (flat_walk_staged).
+// L2 (-p l2): the edge-rooted variant.
 template <typename Word, int NR, int EV = 0, bool LIST = false, bool XP = false, bool OPS = false,
-          bool SPLIT = false, bool STAGE = false>
+          bool SPLIT = false, bool STAGE = false, bool L2 = false>
 __global__ void __launch_bounds__(REG_BLOCK, (NR == 1 && sizeof(Word) == 4) ? 6 : (NR == 2 ? 4 : 1))
     bk_reg_kernel(BKArgs a, int cls) {
   __shared__ RegSmem<Word, NR> sm_all[REG_BLOCK / 32];
@@ -84,9 +85,26 @@ __global__ void __launch_bounds__(REG_BLOCK, (NR == 1 && sizeof(Word) == 4) ? 6 
       if (parts == 1 || r != rt.r) reg_encode<Word, NR, STAGE>(a, sm, sl, r, rt);
       MCE_BD(BD_OTHER);
       u64 nd = 0, cnt = 0, op = 0;
-      reg_tree<Word, NR, false, EV, LIST, XP, OPS, SPLIT>(a, sm, sl, rt, WOps<Word>::low(rt.d), (Word)0,
-                                                    (Word)0, h0, h1, nd, cnt, bd, &op,
-                                                    (int)(u % parts), (int)parts);
+      if constexpr (L2) {  // -p l2: the root's edges are the units
+        reg_l2_units<Word, NR, LIST>(a, sm, sl, rt, h0, cnt, [&](Word Pv, Word Sv, Word XOv) {
+          if (share && q_wants(a.q)) {  // offered to idle warps at once
+            const u64 w0 = (u64)(uint32_t)rt.r, w1 = (u64)Pv, w3 = (u64)Sv, w4 = (u64)XOv;
+            if (q_push(a.q, [&](uint32_t k2) {
+                  return k2 == 0 ? w0 : k2 == 1 ? w1 : k2 == 2 ? 0ull : k2 == 3 ? w3 : w4;
+                })) {
+              if (EV && lane == 0) warp_record(a)[2] += 1;
+              return;
+            }
+          }
+          reg_tree<Word, NR, false, EV, LIST, XP, OPS, SPLIT, true>(a, sm, sl, rt, Pv, (Word)0, Sv,
+                                                                    h0, h1, nd, cnt, bd, &op, 0, 1,
+                                                                    XOv);
+        });
+      } else {
+        reg_tree<Word, NR, false, EV, LIST, XP, OPS, SPLIT>(a, sm, sl, rt, WOps<Word>::low(rt.d),
+                                                            (Word)0, (Word)0, h0, h1, nd, cnt, bd,
+                                                            &op, (int)(u % parts), (int)parts);
+      }
       nodes += nd;
       root_done(a, r, nd, cnt);
       if constexpr (OPS) {
@@ -100,7 +118,7 @@ __global__ void __launch_bounds__(REG_BLOCK, (NR == 1 && sizeof(Word) == 4) ? 6 
       atomicSub(&a.q.hdr->work, 1u);
       atomicAdd(&a.q.hdr->epoch, 1u);
     }
-    u64 t0 = 0, t1 = 0, t2 = 0, t3 = 0;
+    u64 t0 = 0, t1 = 0, t2 = 0, t3 = 0, t4 = 0;
     MCE_BD(BD_QUEUE);
     idle_phase(
         a,
@@ -109,6 +127,7 @@ __global__ void __launch_bounds__(REG_BLOCK, (NR == 1 && sizeof(Word) == 4) ? 6 
           if (k == 1) t1 = w;
           if (k == 2) t2 = w;
           if (k == 3) t3 = w;
+          if (k == 4) t4 = w;
         },
         [&]() {
           // word k of the task arrived on lane k
@@ -116,11 +135,12 @@ __global__ void __launch_bounds__(REG_BLOCK, (NR == 1 && sizeof(Word) == 4) ? 6 
           const Word P = (Word)__shfl_sync(MCE_FULL, t1, 1);
           const Word X = (Word)__shfl_sync(MCE_FULL, t2, 2);
           const Word S = (Word)__shfl_sync(MCE_FULL, t3, 3);
+          const Word XO = L2 ? (Word)__shfl_sync(MCE_FULL, t4, 4) : (Word)0;  // L2 unit's outside rows
           MCE_BD(BD_ENCODE);
           if (r != rt.r) reg_encode<Word, NR, STAGE>(a, sm, sl, r, rt);
           u64 nd = 0, cnt = 0, op = 0;
-          reg_tree<Word, NR, false, EV, LIST, XP, OPS>(a, sm, sl, rt, P, X, S, h0, h1, nd, cnt, bd,
-                                                        &op);
+          reg_tree<Word, NR, false, EV, LIST, XP, OPS, false, L2>(a, sm, sl, rt, P, X, S, h0, h1, nd,
+                                                                  cnt, bd, &op, 0, 1, XO);
           nodes += nd;
           root_done(a, r, nd, cnt);
           if constexpr (OPS) {
@@ -147,7 +167,8 @@ __global__ void __launch_bounds__(REG_BLOCK, (NR == 1 && sizeof(Word) == 4) ? 6 
 // The wide engine at 4 blocks per SM (96 registers) or, with
 // opts.wide_blocks = 8, at 8 (64 registers): more warps pay on graphs whose
 // wide roots have large shared subtrees (R-MAT), fewer on many small ones.
-template <int EV = 0, int MINB = 1, bool LIST = false, bool OPS = false, bool SPLIT = false>
+template <int EV = 0, int MINB = 1, bool LIST = false, bool OPS = false, bool SPLIT = false,
+          bool XP = false, bool L2 = false>
 __global__ void __launch_bounds__(MEM_BLOCK, MINB) bk_mem_kernel(BKArgs a, int cls) {
   __shared__ MemSmem sm_all[MEM_BLOCK / 32];
   __shared__ u64 srows_all[MEM_BLOCK / 32][2 * MEM_SROWS_D];
@@ -176,16 +197,36 @@ __global__ void __launch_bounds__(MEM_BLOCK, MINB) bk_mem_kernel(BKArgs a, int c
     MCE_BD(BD_OTHER);
     if (rt.d == 0) continue;
     const int Wr = rt.Wr;
-    if (lane < Wr) {  // root frame: P = all of N+(r), X = 0, S = 0
-      const u64 all = (lane == Wr - 1 && (rt.d & 63)) ? ((1ull << (rt.d & 63)) - 1ull) : ~0ull;
-      sl.stk[lane] = all;
-      sl.stk[Wr + lane] = 0;
-      sl.stk[3 * Wr + lane] = 0;
-    }
-    __syncwarp();
     u64 nd = 0, cnt = 0, op = 0;
-    mem_tree<false, EV, LIST, OPS, SPLIT>(a, sl, rt, h0, h1, nd, cnt, bd, &op, (int)(i0 % parts),
-                                          (int)parts);
+    if constexpr (L2) {  // -p l2: the root's edges are the units
+      const int WM = (a.dcap + 63) >> 6;
+      mem_l2_units<LIST>(a, sl, rt, h0, h1, cnt, [&](bool xo_any) {
+        if (share && q_wants(a.q)) {  // offered to idle warps at once
+          const u64 *F0 = sl.stk;
+          if (q_push(a.q, [&](uint32_t k2) -> u64 {
+                if (k2 == 0) return (u64)(uint32_t)r;
+                const uint32_t part = (k2 - 1) / WM, w = (k2 - 1) % WM;
+                if ((int)w >= Wr) return 0ull;
+                return part == 0 ? F0[w] : part == 1 ? 0ull : part == 2 ? F0[3 * Wr + w] : sl.xo[w];
+              })) {
+            if (EV && lane == 0) warp_record(a)[2] += 1;
+            return;
+          }
+        }
+        mem_tree<false, EV, LIST, OPS, SPLIT, XP, true>(a, sl, rt, h0, h1, nd, cnt, bd, &op, 0, 1,
+                                                        xo_any);
+      });
+    } else {
+      if (lane < Wr) {  // root frame: P = all of N+(r), X = 0, S = 0
+        const u64 all = (lane == Wr - 1 && (rt.d & 63)) ? ((1ull << (rt.d & 63)) - 1ull) : ~0ull;
+        sl.stk[lane] = all;
+        sl.stk[Wr + lane] = 0;
+        sl.stk[3 * Wr + lane] = 0;
+      }
+      __syncwarp();
+      mem_tree<false, EV, LIST, OPS, SPLIT, XP>(a, sl, rt, h0, h1, nd, cnt, bd, &op, (int)(i0 % parts),
+                                            (int)parts);
+    }
     nodes += nd;
     root_done(a, r, nd, cnt);
     if constexpr (OPS) {
@@ -215,11 +256,12 @@ __global__ void __launch_bounds__(MEM_BLOCK, MINB) bk_mem_kernel(BKArgs a, int c
           const int32_t r = __shfl_sync(MCE_FULL, task_root, 0);
           __syncwarp();
           // the staging area is rewritten by mem_encode: keep the task first
-          u64 tp = 0, tx = 0, ts = 0;
+          u64 tp = 0, tx = 0, ts = 0, to = 0;
           if (lane < WM) {
             tp = sl.xs[lane];
             tx = sl.xs[WM + lane];
             ts = sl.xs[2 * WM + lane];
+            to = sl.xs[3 * WM + lane];  // an L2 unit's outside rows (0 otherwise)
           }
           __syncwarp();
           MCE_BD(BD_ENCODE);
@@ -231,10 +273,13 @@ __global__ void __launch_bounds__(MEM_BLOCK, MINB) bk_mem_kernel(BKArgs a, int c
             sl.stk[lane] = tp;
             sl.stk[Wr + lane] = tx;
             sl.stk[3 * Wr + lane] = ts;
+            sl.xo[lane] = to;
           }
+          const bool xo_any = __any_sync(MCE_FULL, lane < Wr && to != 0);
           __syncwarp();
           u64 nd = 0, cnt = 0, op = 0;
-          mem_tree<false, EV, LIST, OPS>(a, sl, rt, h0, h1, nd, cnt, bd, &op);
+          mem_tree<false, EV, LIST, OPS, false, XP, L2>(a, sl, rt, h0, h1, nd, cnt, bd, &op, 0, 1,
+                                                        xo_any);
           nodes += nd;
           root_done(a, r, nd, cnt);
           if constexpr (OPS) {
@@ -441,16 +486,17 @@ size_t bk_slab_words(int cls, int dcap, int xcap, int rxcap) {
   if (cls == CLS_R32 || cls == CLS_R64) return 4 * (size_t)rxcap;  // hash, rows, leaf list
   const size_t WM = (size_t)(dcap + 63) / 64;
   size_t w = (size_t)dcap * WM + (size_t)(dcap + 1) * 4 * WM + 32 * WM + (size_t)xcap * WM;
+  w += WM;                                          // xo (an L2 unit's outside rows)
   w += (size_t)hash_cap(xcap);                      // hash set (one-word rows)
-  w += ((size_t)dcap + (size_t)xcap + 1) / 2 + 1;  // pl and xl (int32)
+  w += (3 * (size_t)dcap + (size_t)xcap + 1) / 2 + 1;  // pl, xl (xcap + dcap) and pk (int32)
   w += (size_t)p_cap(dcap);                         // hash of P: keys and indices (int32)
   w = w > 3 * WM + 1 ? w : 3 * WM + 1;
   return (w + 31) & ~(size_t)31;                    // 256-byte aligned slabs
 }
 
 uint32_t bk_task_words(int cls, int dcap) {
-  if (cls == CLS_R32 || cls == CLS_R64) return 4;
-  return 1 + 3 * (uint32_t)((dcap + 63) / 64);
+  if (cls == CLS_R32 || cls == CLS_R64) return 5;  // root, P, X, chosen set, L2 outside rows
+  return 1 + 4 * (uint32_t)((dcap + 63) / 64);     // the same, W words each
 }
 
 int bk_warps_for_class(int cls, int sms, int wide_blocks, int *warps, int *block, int *smem) {
@@ -480,129 +526,73 @@ int bk_warps_for_class(int cls, int sms, int wide_blocks, int *warps, int *block
   return MCE_OK;
 }
 
+namespace {
+
+// One engine-class launch of the variant <EV, LIST, XP, OPS, SPLIT, STAGE, L2>.
+template <int EV, bool LIST, bool XP, bool OPS, bool SPLIT, bool STAGE, bool L2>
+int launch_cls(int cls, int word_bits, const BKArgs &a, int grid, int block, int smem,
+               cudaStream_t s) {
+  if (cls == CLS_R32 && word_bits == 64)
+    bk_reg_kernel<u64, 1, EV, LIST, XP, OPS, SPLIT, false, L2><<<grid, block, smem, s>>>(a, cls);
+  else if (cls == CLS_R32)
+    bk_reg_kernel<uint32_t, 1, EV, LIST, XP, OPS, SPLIT, STAGE, L2><<<grid, block, smem, s>>>(a, cls);
+  else if (cls == CLS_R64)
+    bk_reg_kernel<u64, 2, EV, LIST, XP, OPS, SPLIT, false, L2><<<grid, block, smem, s>>>(a, cls);
+  else if (cls == CLS_MEM && a.wide8 && EV == 0)
+    bk_mem_kernel<EV, 8, LIST, OPS, SPLIT, XP, L2><<<grid, block, smem, s>>>(a, cls);
+  else if (cls == CLS_MEM)
+    bk_mem_kernel<EV, 1, LIST, OPS, SPLIT, XP, L2><<<grid, block, smem, s>>>(a, cls);
+  else
+    return MCE_EINVAL;
+  MCE_CUDA(cudaGetLastError());
+  return MCE_OK;
+}
+
+}  // namespace
+
+// The variant a call needs: listing, the evaluation logs (per-warp load, and
+// cycles), the word-op count, several warps per root, -i px, staged lists,
+// L2 units.  Modes that do not combine: the evaluation and listing variants
+// run with one warp per root and IP pivots; the word-op count with IP and L1.
 int bk_launch(int cls, int word_bits, const BKArgs &a, int grid, int block, int smem,
               cudaStream_t s, int *launches) {
   if (grid <= 0) return MCE_OK;
-  // the evaluation variants record per-warp load (1) and cycles (2); the
-  // listing variants write every clique
   const int ev = a.warp_log == nullptr ? 0 : (a.warp_cycles ? 2 : 1);
-  if (a.list_buf) {
-    if (cls == CLS_R32 && word_bits == 64)
-      bk_reg_kernel<u64, 1, 0, true><<<grid, block, smem, s>>>(a, cls);
-    else if (cls == CLS_R32)
-      bk_reg_kernel<uint32_t, 1, 0, true><<<grid, block, smem, s>>>(a, cls);
-    else if (cls == CLS_R64)
-      bk_reg_kernel<u64, 2, 0, true><<<grid, block, smem, s>>>(a, cls);
-    else if (cls == CLS_MEM && a.wide8)
-      bk_mem_kernel<0, 8, true><<<grid, block, smem, s>>>(a, cls);
-    else if (cls == CLS_MEM)
-      bk_mem_kernel<0, 1, true><<<grid, block, smem, s>>>(a, cls);
+  const bool xp = a.x_pivot != 0, split = a.parts > 1;
+  int rc;
+  if (a.level2) {
+    if (a.list_buf)
+      rc = launch_cls<0, true, false, false, false, false, true>(cls, word_bits, a, grid, block, smem, s);
+    else if (ev == 2)
+      rc = launch_cls<2, false, false, false, false, false, true>(cls, word_bits, a, grid, block, smem, s);
+    else if (ev == 1)
+      rc = launch_cls<1, false, false, false, false, false, true>(cls, word_bits, a, grid, block, smem, s);
+    else if (xp)
+      rc = launch_cls<0, false, true, false, false, false, true>(cls, word_bits, a, grid, block, smem, s);
     else
-      return MCE_EINVAL;
-    MCE_CUDA(cudaGetLastError());
-    if (launches) *launches += 1;
-    return MCE_OK;
-  }
-  if (a.count_ops) {  // the counting variants (no evaluation log, IP pivots only)
-    if (cls == CLS_R32 && word_bits == 64)
-      bk_reg_kernel<u64, 1, 0, false, false, true, true><<<grid, block, smem, s>>>(a, cls);
-    else if (cls == CLS_R32)
-      bk_reg_kernel<uint32_t, 1, 0, false, false, true, true><<<grid, block, smem, s>>>(a, cls);
-    else if (cls == CLS_R64)
-      bk_reg_kernel<u64, 2, 0, false, false, true, true><<<grid, block, smem, s>>>(a, cls);
-    else if (cls == CLS_MEM)
-      bk_mem_kernel<0, 1, false, true, true><<<grid, block, smem, s>>>(a, cls);
+      rc = launch_cls<0, false, false, false, false, false, true>(cls, word_bits, a, grid, block, smem, s);
+  } else if (a.list_buf) {
+    rc = launch_cls<0, true, false, false, false, false, false>(cls, word_bits, a, grid, block, smem, s);
+  } else if (a.count_ops) {
+    rc = launch_cls<0, false, false, true, true, false, false>(cls, word_bits, a, grid, block, smem, s);
+  } else if (ev == 2) {
+    rc = launch_cls<2, false, false, false, false, false, false>(cls, word_bits, a, grid, block, smem, s);
+  } else if (ev == 1) {
+    rc = launch_cls<1, false, false, false, false, false, false>(cls, word_bits, a, grid, block, smem, s);
+  } else if (split) {
+    if (xp)
+      rc = launch_cls<0, false, true, false, true, false, false>(cls, word_bits, a, grid, block, smem, s);
     else
-      return MCE_EINVAL;
-    MCE_CUDA(cudaGetLastError());
-    if (launches) *launches += 1;
-    return MCE_OK;
+      rc = launch_cls<0, false, false, false, true, false, false>(cls, word_bits, a, grid, block, smem, s);
+  } else if (xp) {
+    rc = launch_cls<0, false, true, false, false, false, false>(cls, word_bits, a, grid, block, smem, s);
+  } else if (a.stage) {
+    rc = launch_cls<0, false, false, false, false, true, false>(cls, word_bits, a, grid, block, smem, s);
+  } else {
+    rc = launch_cls<0, false, false, false, false, false, false>(cls, word_bits, a, grid, block, smem, s);
   }
-  if (a.stage && cls == CLS_R32 && word_bits == 32 && ev == 0 && a.parts <= 1 && !a.x_pivot) {
-    // the 32-bit engine with its lists staged by bulk copies
-    bk_reg_kernel<uint32_t, 1, 0, false, false, false, false, true><<<grid, block, smem, s>>>(a, cls);
-    MCE_CUDA(cudaGetLastError());
-    if (launches) *launches += 1;
-    return MCE_OK;
-  }
-  if (a.parts > 1 && ev == 0) {  // several warps per root (plain counting or -i px)
-    if (a.x_pivot && cls != CLS_MEM) {
-      if (cls == CLS_R32 && word_bits == 64)
-        bk_reg_kernel<u64, 1, 0, false, true, false, true><<<grid, block, smem, s>>>(a, cls);
-      else if (cls == CLS_R32)
-        bk_reg_kernel<uint32_t, 1, 0, false, true, false, true><<<grid, block, smem, s>>>(a, cls);
-      else
-        bk_reg_kernel<u64, 2, 0, false, true, false, true><<<grid, block, smem, s>>>(a, cls);
-    } else if (cls == CLS_R32 && word_bits == 64) {
-      bk_reg_kernel<u64, 1, 0, false, false, false, true><<<grid, block, smem, s>>>(a, cls);
-    } else if (cls == CLS_R32) {
-      bk_reg_kernel<uint32_t, 1, 0, false, false, false, true><<<grid, block, smem, s>>>(a, cls);
-    } else if (cls == CLS_R64) {
-      bk_reg_kernel<u64, 2, 0, false, false, false, true><<<grid, block, smem, s>>>(a, cls);
-    } else if (cls == CLS_MEM && a.wide8) {
-      bk_mem_kernel<0, 8, false, false, true><<<grid, block, smem, s>>>(a, cls);
-    } else if (cls == CLS_MEM) {
-      bk_mem_kernel<0, 1, false, false, true><<<grid, block, smem, s>>>(a, cls);
-    } else {
-      return MCE_EINVAL;
-    }
-    MCE_CUDA(cudaGetLastError());
-    if (launches) *launches += 1;
-    return MCE_OK;
-  }
-  if (a.x_pivot && ev == 0 && cls != CLS_MEM) {  // -i px: pivots also from earlier neighbours
-    if (cls == CLS_R32 && word_bits == 64)
-      bk_reg_kernel<u64, 1, 0, false, true><<<grid, block, smem, s>>>(a, cls);
-    else if (cls == CLS_R32)
-      bk_reg_kernel<uint32_t, 1, 0, false, true><<<grid, block, smem, s>>>(a, cls);
-    else
-      bk_reg_kernel<u64, 2, 0, false, true><<<grid, block, smem, s>>>(a, cls);
-    MCE_CUDA(cudaGetLastError());
-    if (launches) *launches += 1;
-    return MCE_OK;
-  }
-  switch (cls) {
-    case CLS_R32:
-      if (word_bits == 64) {
-        if (ev == 2)
-          bk_reg_kernel<u64, 1, 2><<<grid, block, smem, s>>>(a, cls);
-        else if (ev == 1)
-          bk_reg_kernel<u64, 1, 1><<<grid, block, smem, s>>>(a, cls);
-        else
-          bk_reg_kernel<u64, 1><<<grid, block, smem, s>>>(a, cls);
-      } else {
-        if (ev == 2)
-          bk_reg_kernel<uint32_t, 1, 2><<<grid, block, smem, s>>>(a, cls);
-        else if (ev == 1)
-          bk_reg_kernel<uint32_t, 1, 1><<<grid, block, smem, s>>>(a, cls);
-        else
-          bk_reg_kernel<uint32_t, 1><<<grid, block, smem, s>>>(a, cls);
-      }
-      break;
-    case CLS_R64:
-      if (ev == 2)
-        bk_reg_kernel<u64, 2, 2><<<grid, block, smem, s>>>(a, cls);
-      else if (ev == 1)
-        bk_reg_kernel<u64, 2, 1><<<grid, block, smem, s>>>(a, cls);
-      else
-        bk_reg_kernel<u64, 2><<<grid, block, smem, s>>>(a, cls);
-      break;
-    case CLS_MEM:
-      if (ev == 2)
-        bk_mem_kernel<2><<<grid, block, smem, s>>>(a, cls);
-      else if (ev == 1)
-        bk_mem_kernel<1><<<grid, block, smem, s>>>(a, cls);
-      else if (a.wide8)
-        bk_mem_kernel<0, 8><<<grid, block, smem, s>>>(a, cls);
-      else
-        bk_mem_kernel<><<<grid, block, smem, s>>>(a, cls);
-      break;
-    default:
-      return MCE_EINVAL;
-  }
-  MCE_CUDA(cudaGetLastError());
-  if (launches) *launches += 1;
-  return MCE_OK;
+  if (rc == MCE_OK && launches) *launches += 1;
+  return rc;
 }
 
 int queue_launch_init(const QueueView &q, cudaStream_t s, int *launches) {

@@ -123,12 +123,9 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
 }
 
 __device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long *bar, uint32_t bytes) {
-  unsigned long long state;
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 %0, [%1], %2;"
-               : "=l"(state)
-               : "r"(smem_u32(bar)), "r"(bytes)
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
                : "memory");
-  (void)state;
 }
 
 __device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, uint32_t bytes,

@@ -632,7 +632,8 @@ __device__ __forceinline__ int outside_pivot(const Word *first32, const Word *re
       if ((row & chosen) == chosen) {
         const int sc = WOps<Word>::popc(Pn & row);
         el |= sc == pcn;
-        k = max(k, ((sc + 1) << 11) | (2047 - i));
+        // the key holds 11 bits of index: rows past 2,047 prune but are not pivots
+        if (i < 2048) k = max(k, ((sc + 1) << 11) | (2047 - i));
       }
     }
   }
@@ -680,12 +681,14 @@ __device__ __forceinline__ void reg_emit(const BKArgs &a, const RegSmem<Word, NR
 // the warp that created it.  The clique shortcuts are off, so every node of
 // the tree is walked (same nodes, counts and histogram).
 // SPLIT: the variant for several warps per root (part / parts below).
+// L2: the variant that carries an L2 unit's outside rows (XO); the others
+// ignore XO.
 template <typename Word, int NR, bool Budget = false, int EV = 0, bool LIST = false,
-          bool XP = false, bool OPS = false, bool SPLIT = false>
+          bool XP = false, bool OPS = false, bool SPLIT = false, bool L2 = false>
 __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<Word> &sl,
                          const RegRoot<Word> &rt, Word P, Word X, Word S, u64 &h0, u64 &h1,
                          u64 &nodes, u64 &cnt, Bd *bd = nullptr, u64 *ops = nullptr,
-                         int part = 0, int parts = 1) {
+                         int part = 0, int parts = 1, Word XO = 0) {
   using O = WOps<Word>;
   const u64 w32 = (u64)((rt.d + 31) >> 5);
   MCE_BD(BD_PIVOT);
@@ -744,6 +747,23 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
       const Word row = i < nX ? sl.xr[i] : (Word)0;
       const bool has = i < nX && (row & S) == S;
       const uint32_t mk = __ballot_sync(MCE_FULL, has);
+      if (has) {
+        const int at = nL + __popc(mk & lt);
+        (at < 32 ? sm.xl0 : sl.xl)[at] = row;
+      }
+      nL += __popc(mk);
+    }
+  }
+  if (L2 && XO) {  // an L2 unit's outside rows: the root's later neighbours earlier than its edge
+#pragma unroll
+    for (int k = 0; k < NR; ++k) {
+      const Word row = k == 0 ? r0 : r1;
+      const bool has = ((XO >> (lane + 32 * k)) & 1) && (row & S) == S;
+      const uint32_t mk = __ballot_sync(MCE_FULL, has);
+      if (nL + __popc(mk) > 32 + sl.xc) {  // the list's capacity (never reached: nL <= d-)
+        if (lane == 0) atomicOr(a.err, MCE_ERR_XROWS);
+        return;
+      }
       if (has) {
         const int at = nL + __popc(mk & lt);
         (at < 32 ? sm.xl0 : sl.xl)[at] = row;
@@ -943,8 +963,11 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
         recheck = 32;
       }
       if (want) {
-        const u64 w0 = (u64)(uint32_t)rt.r, w1 = (u64)Pc, w2 = (u64)Xc, w3 = (u64)Sc;
-        if (q_push(a.q, [&](uint32_t k2) { return k2 == 0 ? w0 : k2 == 1 ? w1 : k2 == 2 ? w2 : w3; })) {
+        const u64 w0 = (u64)(uint32_t)rt.r, w1 = (u64)Pc, w2 = (u64)Xc, w3 = (u64)Sc,
+                  w4 = L2 ? (u64)XO : 0ull;
+        if (q_push(a.q, [&](uint32_t k2) {
+              return k2 == 0 ? w0 : k2 == 1 ? w1 : k2 == 2 ? w2 : k2 == 3 ? w3 : w4;
+            })) {
           if (EV && lane == 0) warp_record(a)[2] += 1;  // opts.warp_log
           continue;
         }
@@ -993,8 +1016,57 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
   MCE_BD(BD_OTHER);
 }
 
+// L2 (-p l2): the root's units are its oriented edges (r, v), the scheme of
+// mce/mce_kernel_wl.cuh:307-485 (setup_stack_original_L2_IP,
+// mce/mce_utils.cuh:664-712): the unit's candidates are the triangle list
+// P = N+(r) & N+(v) (block_count_and_set_tri, :151-171), its pivot is taken
+// from P alone, and the root's neighbours earlier than v and adjacent to it
+// are outside rows tested at the leaves only - the earlier neighbours of r
+// (the rows of sl.xr containing v) and the later ones before v in the
+// degeneracy order (prio, then id: include/main_support.cuh:14), passed as
+// XO.  An empty triangle list counts the edge when nothing covers it.
+// Units are not tree nodes (the reference counts branches inside a unit).
+// `unit(P, S, XO)` searches or hands off one unit.
+template <typename Word, int NR, bool LIST, typename Unit>
+__device__ __forceinline__ void reg_l2_units(const BKArgs &a, const RegSmem<Word, NR> &sm,
+                                             const RegSlab<Word> &sl, const RegRoot<Word> &rt,
+                                             u64 &h0, u64 &cnt, Unit unit) {
+  using O = WOps<Word>;
+  const int lane = (int)lane_id(), d = rt.d, nX = rt.nX;
+  uint32_t pk0 = 0xFFFFFFFFu, pk1 = 0xFFFFFFFFu;  // degeneracy-order key of each index
+  if (lane < d) pk0 = a.prio[sm.pl[lane]];
+  if (NR == 2 && lane + 32 < d) pk1 = a.prio[sm.pl[lane + 32]];
+  for (int v = 0; v < d; ++v) {
+    const uint32_t pv = __shfl_sync(MCE_FULL, v < 32 ? pk0 : pk1, v & 31);
+    // indices later than v: larger key, or the same key and a larger id
+    // (ids ascend with the index)
+    Word lat = (Word)__ballot_sync(MCE_FULL, lane < d && (pk0 > pv || (pk0 == pv && lane > v)));
+    if constexpr (NR == 2)
+      lat |= (Word)__ballot_sync(MCE_FULL,
+                                 lane + 32 < d && (pk1 > pv || (pk1 == pv && lane + 32 > v)))
+             << 32;
+    const Word rv = row_of<Word, NR>(rt.r0, rt.r1, v);
+    const Word Pv = rv & lat, XOv = rv & ~lat, vb = O::bit(v);
+    if (Pv == 0) {  // the edge {r, v}
+      bool covered = XOv != 0;
+      for (int i0 = 0; !covered && i0 < nX; i0 += 32) {
+        const int i = i0 + lane;
+        covered = __any_sync(MCE_FULL, i < nX && (sl.xr[i] & vb));
+      }
+      if (!covered) {
+        ++cnt;
+        if constexpr (LIST) reg_emit<Word, NR>(a, sm, rt.r, vb);
+        if (lane == 0) ++h0;  // size 2: bin 0
+      }
+      continue;
+    }
+    unit(Pv, vb, XOv);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Wide engine: any d+ <= 2048, rows of W = ceil(d+/64) words in a slab.
+// (mem_l2_units, after mem_tree, is the wide engine's reg_l2_units.)
 // ---------------------------------------------------------------------------
 struct MemSmem {
   int32_t off[32];
@@ -1005,7 +1077,9 @@ struct MemSmem {
 struct Slab {
   int32_t *pl;
   u64 *rows, *stk, *xs, *xr, *hash;
-  int32_t *xl;
+  u64 *xo;       // an L2 unit's outside rows among the later neighbours (one bitmap)
+  int32_t *xl;   // leaf-filter list: rows of xr (>= 0) or, -1 - i, induced row i (L2)
+  uint32_t *pk;  // the later neighbours' degeneracy keys (L2)
   int32_t *pkey, *pidx;  // hash of P: vertex id (-1: empty) and its index in P
   int hcap;  // hash set entries: a power of two >= 2 * xcap
 };
@@ -1031,11 +1105,13 @@ __device__ __forceinline__ Slab slab_of(const BKArgs &a, int64_t gw) {
   s.stk = s.rows + (size_t)D * WM;
   s.xs = s.stk + (size_t)(D + 1) * 4 * WM;
   s.xr = s.xs + (size_t)32 * WM;
-  s.hash = s.xr + (size_t)XC * WM;
+  s.xo = s.xr + (size_t)XC * WM;
+  s.hash = s.xo + (size_t)WM;
   s.hcap = hash_cap(XC);
   s.pl = (int32_t *)(s.hash + (size_t)s.hcap);
   s.xl = s.pl + D;
-  s.pkey = s.xl + XC;
+  s.pk = (uint32_t *)(s.xl + XC + D);
+  s.pkey = (int32_t *)(s.pk + D);
   s.pidx = s.pkey + p_cap(D);
   return s;
 }
@@ -1167,13 +1243,15 @@ __device__ void mem_encode(const BKArgs &a, MemSmem &sm, const Slab &sl, int32_t
 // Walk the subtree under frame 0 of the slab stack (P, X, S already there).
 // Whether one of the nL filtered earlier-neighbour rows contains the chosen
 // set Cs (Wr words in the slab): the leaf's clique is then not maximal.
-__device__ __forceinline__ bool mem_covered(const Slab &sl, int nL, int Wr, const u64 *Cs) {
+__device__ __forceinline__ bool mem_covered(const Slab &sl, int nL, int Wr, const u64 *Cs,
+                                            const u64 *rows) {
   const int lane = (int)lane_id();
   for (int i0 = 0; i0 < nL; i0 += 32) {
     const int i = i0 + lane;
     bool hit = false;
     if (i < nL) {
-      const u64 *xrow = sl.xr + (size_t)sl.xl[i] * Wr;
+      const int32_t k = sl.xl[i];
+      const u64 *xrow = k >= 0 ? sl.xr + (size_t)k * Wr : rows + (size_t)(-1 - k) * Wr;
       hit = true;
       for (int w = 0; w < Wr && hit; ++w) hit = (xrow[w] & Cs[w]) == Cs[w];
     }
@@ -1222,11 +1300,58 @@ __device__ __forceinline__ void mem_leaf(const BKArgs &a, const Slab &sl, int32_
 
 // OPS: the algorithmic word operations, SPLIT: several warps per root, as
 // in reg_tree.
+// XO (an L2 unit): sl.xo holds the unit's outside rows among the later
+// neighbours (tested at the leaves like earlier-neighbour rows).
+// Outside pivot of the wide engine (-i px): over the earlier-neighbour rows
+// that contain the chosen set S - and, in an L2 unit, the unit's outside
+// rows (sl.xo) - the best score |P & row| with the lowest row id (earlier-
+// neighbour rows first).  Returns score + 1 (0: no such row) with the row in
+// *row_out; *elim: one of them covers P.
+__device__ __forceinline__ int mem_outside_pivot(const Slab &sl, const u64 *rows, int nX, int d,
+                                                 int Wr, bool xo, const u64 *S, const u64 *P,
+                                                 int pc, bool *elim, const u64 **row_out) {
+  const int lane = (int)lane_id();
+  int best = 0;
+  uint32_t bid = 0xFFFFFFFFu;
+  bool el = false;
+  const int total = nX + (xo ? d : 0);
+  for (int i = lane; i < total; i += 32) {
+    const u64 *row;
+    if (i < nX) {
+      row = sl.xr + (size_t)i * Wr;
+    } else {
+      const int j = i - nX;
+      if (!((sl.xo[j >> 6] >> (j & 63)) & 1ull)) continue;
+      row = rows + (size_t)j * Wr;
+    }
+    bool has = true;
+    int sc = 0;
+    for (int w = 0; w < Wr; ++w) {
+      has = has && (row[w] & S[w]) == S[w];
+      sc += __popcll(row[w] & P[w]);
+    }
+    if (!has) continue;
+    el = el || sc == pc;
+    if (sc + 1 > best) {  // ids ascend within a lane: ties keep the lowest
+      best = sc + 1;
+      bid = (uint32_t)i;
+    }
+  }
+  *elim = __any_sync(MCE_FULL, el);
+  const int mb = (int)__reduce_max_sync(MCE_FULL, (unsigned)best);
+  const uint32_t id = __reduce_min_sync(MCE_FULL, best == mb ? bid : 0xFFFFFFFFu);
+  if (mb > 0)
+    *row_out = (int)id < nX ? sl.xr + (size_t)id * Wr : rows + (size_t)((int)id - nX) * Wr;
+  return mb;
+}
+
+// XP (-i px): pivots also from the outside rows adjacent to the whole
+// chosen set, and a node one of them covers is pruned (reg_tree's rule).
 template <bool Budget = false, int EV = 0, bool LIST = false, bool OPS = false,
-          bool SPLIT = false>
+          bool SPLIT = false, bool XP = false, bool L2 = false>
 __device__ void mem_tree(const BKArgs &a, const Slab &sl, const MemRoot &rt, u64 &h0, u64 &h1,
                          u64 &nodes, u64 &cnt, Bd *bd = nullptr, u64 *ops = nullptr,
-                         int part = 0, int parts = 1) {
+                         int part = 0, int parts = 1, bool XO = false) {
   MCE_BD(BD_PIVOT);
   const int lane = (int)lane_id();
   const uint32_t lt = (1u << lane) - 1u;
@@ -1264,13 +1389,18 @@ __device__ void mem_tree(const BKArgs &a, const Slab &sl, const MemRoot &rt, u64
       k = max(k, ((s + 1) << 11) | (2047 - uu));
       el = el || (inX && s == pc);
     }
-    if (__any_sync(MCE_FULL, el) || pc == 0) {
+    const u64 *orow = nullptr;
+    int mb = 0;
+    bool elo = false;
+    if constexpr (XP) mb = mem_outside_pivot(sl, rows, nX, d, Wr, L2 && XO, F0 + 3 * Wr, F0, pc, &elo, &orow);
+    if (__any_sync(MCE_FULL, el) || elo || pc == 0) {
       MCE_BD(BD_OTHER);
       return;
     }
     k = (int)__reduce_max_sync(MCE_FULL, (unsigned)k);
     const int piv = 2047 - (k & 2047);
-    if (lane < Wr) F0[2 * Wr + lane] = F0[lane] & ~rows[(size_t)piv * Wr + lane];
+    const u64 *prow = (XP && mb > (k >> 11)) ? orow : rows + (size_t)piv * Wr;
+    if (lane < Wr) F0[2 * Wr + lane] = F0[lane] & ~prow[lane];
     __syncwarp();
   }
   const bool per_branch = (s_base == 0);
@@ -1286,6 +1416,18 @@ __device__ void mem_tree(const BKArgs &a, const Slab &sl, const MemRoot &rt, u64
       }
       const uint32_t m2 = __ballot_sync(MCE_FULL, has);
       if (has) sl.xl[nL + __popc(m2 & lt)] = i;
+      nL += __popc(m2);
+    }
+    __syncwarp();
+  }
+  if (L2 && XO) {  // an L2 unit's outside rows among the later neighbours containing S
+    const u64 *S0 = F0 + 3 * Wr;
+    for (int i0 = 0; i0 < d; i0 += 32) {
+      const int i = i0 + lane;
+      bool has = i < d && ((sl.xo[i >> 6] >> (i & 63)) & 1ull);
+      for (int w = 0; w < Wr && has; ++w) has = (rows[(size_t)i * Wr + w] & S0[w]) == S0[w];
+      const uint32_t m2 = __ballot_sync(MCE_FULL, has);
+      if (has) sl.xl[nL + __popc(m2 & lt)] = -1 - i;
       nL += __popc(m2);
     }
     __syncwarp();
@@ -1358,7 +1500,7 @@ __device__ void mem_tree(const BKArgs &a, const Slab &sl, const MemRoot &rt, u64
     if (pc == 0) {
       MCE_BD(BD_MAXIMAL);
       const u64 *Cs = C + 3 * Wr;
-      if (!xnz && !mem_covered(sl, nL, Wr, Cs))
+      if (!xnz && !mem_covered(sl, nL, Wr, Cs, rows))
         mem_leaf<LIST>(a, sl, rt.r, Wr, Cs, s_base + depth, h0, h1, cnt);
       continue;
     }
@@ -1399,18 +1541,27 @@ __device__ void mem_tree(const BKArgs &a, const Slab &sl, const MemRoot &rt, u64
     if (!OPS && vote == 0) {
       // P' is a clique and no X' vertex covers it: one path of |P'| nodes
       // below ends in S' | P' (the register engine's shortcut); the union
-      // goes into the child's unused branch words.
+      // goes into the child's unused branch words.  With -i px an outside
+      // row covering the union would have ended the path here.
       u64 *Cl = C + 2 * Wr;
       if (lane < Wr) Cl[lane] = C[3 * Wr + lane] | C[lane];
       __syncwarp();
+      const bool cov = mem_covered(sl, nL, Wr, Cl, rows);
+      if (XP && cov) continue;
       nodes += (u64)pc;
       if (Budget && a.node_budget && nodes > a.node_budget) {
         if (lane == 0) atomicOr(a.err, MCE_ERR_BUDGET);
         break;
       }
-      if (!mem_covered(sl, nL, Wr, Cl))
-        mem_leaf<LIST>(a, sl, rt.r, Wr, Cl, s_base + depth + pc, h0, h1, cnt);
+      if (!cov) mem_leaf<LIST>(a, sl, rt.r, Wr, Cl, s_base + depth + pc, h0, h1, cnt);
       continue;
+    }
+    const u64 *orow = nullptr;
+    int mbo = 0;
+    if constexpr (XP) {  // outside rows adjacent to the whole chosen set
+      bool elo = false;
+      mbo = mem_outside_pivot(sl, rows, nX, d, Wr, L2 && XO, C + 3 * Wr, C, pc, &elo, &orow);
+      if (elo) continue;
     }
     if (share && pc >= a.donate_min &&
         (nodes >= a.donate_after || (a.policy && a.policy[rt.r]) || (a.level2 && depth == 0)) &&
@@ -1422,7 +1573,7 @@ __device__ void mem_tree(const BKArgs &a, const Slab &sl, const MemRoot &rt, u64
             if (k2 == 0) return (u64)(uint32_t)rt.r;
             const uint32_t part = (k2 - 1) / WM, w = (k2 - 1) % WM;
             if ((int)w >= Wr) return 0ull;
-            return part == 0 ? Cp[w] : part == 1 ? Cx[w] : Cs[w];
+            return part == 0 ? Cp[w] : part == 1 ? Cx[w] : part == 2 ? Cs[w] : (L2 && XO ? sl.xo[w] : 0ull);
           })) {
         if (EV && lane == 0) warp_record(a)[2] += 1;  // opts.warp_log
         continue;
@@ -1433,11 +1584,57 @@ __device__ void mem_tree(const BKArgs &a, const Slab &sl, const MemRoot &rt, u64
     k = (int)__reduce_max_sync(MCE_FULL, (unsigned)k);
     const int up = 2047 - (k & 2047);
     MCE_BD(BD_BRANCH);
-    if (lane < Wr) C[2 * Wr + lane] = C[lane] & ~rows[(size_t)up * Wr + lane];
+    const u64 *prow = (XP && mbo > (k >> 11)) ? orow : rows + (size_t)up * Wr;
+    if (lane < Wr) C[2 * Wr + lane] = C[lane] & ~prow[lane];
     __syncwarp();
     ++depth;
   }
   MCE_BD(BD_OTHER);
+}
+
+// L2 units of a wide root (see reg_l2_units): frame 0 gets the unit's P
+// (the triangle list), X = 0 and S = {v}; sl.xo its outside rows among the
+// later neighbours.  `unit(xo_any)` searches or hands off the unit.
+template <bool LIST, typename Unit>
+__device__ __forceinline__ void mem_l2_units(const BKArgs &a, const Slab &sl, const MemRoot &rt,
+                                             u64 &h0, u64 &h1, u64 &cnt, Unit unit) {
+  const int lane = (int)lane_id(), d = rt.d, Wr = rt.Wr, nX = rt.nX;
+  const u64 *rows = rt.rows;
+  for (int i = lane; i < d; i += 32) sl.pk[i] = a.prio[sl.pl[i]];
+  __syncwarp();
+  for (int v = 0; v < d; ++v) {
+    const uint32_t pv = sl.pk[v];
+    u64 lat = 0;  // lane w < Wr: word w of the indices later than v
+    for (int c = 0; c * 32 < d; ++c) {
+      const int i = c * 32 + lane;
+      const bool later = i < d && (sl.pk[i] > pv || (sl.pk[i] == pv && i > v));
+      const uint32_t m = __ballot_sync(MCE_FULL, later);
+      if (lane == (c >> 1)) lat |= (u64)m << (32 * (c & 1));
+    }
+    u64 pw = 0, xw = 0;
+    if (lane < Wr) {
+      const u64 rw = rows[(size_t)v * Wr + lane];
+      pw = rw & lat;
+      xw = rw & ~lat;
+      sl.stk[lane] = pw;
+      sl.stk[Wr + lane] = 0;
+      sl.stk[3 * Wr + lane] = (lane == (v >> 6)) ? 1ull << (v & 63) : 0ull;
+      sl.xo[lane] = xw;
+    }
+    const bool tri = __any_sync(MCE_FULL, pw != 0), xo_any = __any_sync(MCE_FULL, xw != 0);
+    __syncwarp();
+    if (!tri) {  // the edge {r, v}: maximal unless an outside row contains v
+      bool covered = xo_any;
+      for (int i0 = 0; !covered && i0 < nX; i0 += 32) {
+        const int i = i0 + lane;
+        covered = __any_sync(MCE_FULL,
+                             i < nX && ((sl.xr[(size_t)i * Wr + (v >> 6)] >> (v & 63)) & 1ull));
+      }
+      if (!covered) mem_leaf<LIST>(a, sl, rt.r, Wr, sl.stk + 3 * Wr, 0, h0, h1, cnt);  // size 2
+      continue;
+    }
+    unit(xo_any);
+  }
 }
 
 }  // namespace

@@ -28,9 +28,11 @@ int peel_launch(const PeelArgs &a, cudaStream_t s, int *launches);
 // part >= 0 (0..3): one part of a batch still arriving, peeled concurrently
 // with the others; the control block was zeroed before the first part and
 // each part takes graphs from its own counter.  part < 0: the whole batch.
+// max_n: the most vertices of a graph of the launch (0: unknown); graphs up
+// to 16,384 vertices are peeled with their state in shared memory.
 int peel_segments_launch(const PeelArgs &a, const int64_t *vtx_off, const int64_t *arc_off,
                          const int32_t *order, int32_t G, cudaStream_t s, int *launches,
-                         int part = -1);
+                         int part = -1, int64_t max_n = 0);
 int peel_read(const void *ctl_dev, int32_t *degeneracy, uint32_t *err, uint32_t *rounds,
               uint32_t *solo_sections, cudaStream_t s, double *phase_ms = nullptr);
 
@@ -131,7 +133,8 @@ struct BKArgs {
                                  // cycles per phase[7]}
   int32_t warp_cycles;           // 1: also the per-phase cycle breakdown
   int32_t wide8;                 // 1: the wide engine's 8-blocks-per-SM variant
-  int32_t level2;                // 1 (-p l2): first-level subtrees go to idle warps at once
+  int32_t level2;                // 1 (-p l2): edge-rooted units, offered to idle warps at once
+  const uint32_t *prio;          // peel priorities (the degeneracy order of the L2 units)
   int32_t x_pivot;               // 1 (-i px): register engines also pivot on earlier neighbours
   int32_t *list_buf;             // nullable: clique records {size, root, members...}
   unsigned long long *list_words;  // words taken in list_buf (also past list_cap)

@@ -24,6 +24,8 @@
 
 #include <cooperative_groups.h>
 
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -428,13 +430,128 @@ struct SegShared {
   uint32_t g;
 };
 
+// Graphs of at most SEG_SMEM_N vertices keep their remaining degrees (16-bit
+// halves of 32-bit words, decremented by one atomic on the word: a degree
+// never falls below zero, so no borrow reaches the other half) and their
+// core numbers (16-bit, -1 while unpeeled) in shared memory: the rounds'
+// decrements and tests stay on the SM.  Their frontiers hold local ids.
+constexpr int SEG_SMEM_N = 16384;
+
+__device__ __forceinline__ int sdeg_get(const uint32_t *w, int i) {
+  return (int)((w[i >> 1] >> ((i & 1) * 16)) & 0xFFFFu);
+}
+__device__ __forceinline__ int sdeg_dec(uint32_t *w, int i) {  // returns the old degree
+  const uint32_t sh = (uint32_t)(i & 1) * 16u;
+  return (int)((atomicSub(&w[i >> 1], 1u << sh) >> sh) & 0xFFFFu);
+}
+
+// One graph (local vertices 0..n-1 = union vertices vb..vb+n-1) with its
+// state in shared memory; the rounds and their numbering are those of the
+// global-memory path below.
+__device__ void peel_graph_smem(const int32_t *__restrict__ rp, const int32_t *__restrict__ col,
+                                int32_t *core, uint32_t *prio, int32_t *F0, int32_t *G0,
+                                int64_t vb, int n, uint32_t mg, uint32_t *sdeg, int16_t *score,
+                                SegShared &sh, PeelCtl *ctl) {
+  const int lane = (int)lane_id(), w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int k = threadIdx.x; 2 * k < n; k += blockDim.x) {
+    const int64_t v = vb + 2 * k;
+    const uint32_t d0 = (uint32_t)(rp[v + 1] - rp[v]);
+    const uint32_t d1 = 2 * k + 1 < n ? (uint32_t)(rp[v + 2] - rp[v + 1]) : 0u;
+    sdeg[k] = d0 | (d1 << 16);
+  }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    score[i] = -1;
+    prio[vb + i] = mg;
+  }
+  if (threadIdx.x == 0) {
+    sh.todo = n;
+    sh.level = 0;
+  }
+  __syncthreads();
+  uint32_t priority = 0;
+  int last_level = -1;
+  while (sh.todo > 0) {
+    const int level = sh.level;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      sh.fcnt = 0;
+      sh.minv = INT_MAX;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      if (score[i] == -1) {
+        const int d = sdeg_get(sdeg, i);
+        if (d <= level) {  // == level: a remaining vertex never has less
+          score[i] = (int16_t)level;
+          F0[atomicAdd(&sh.fcnt, 1)] = i;
+        } else {
+          atomicMin(&sh.minv, d);
+        }
+      }
+    }
+    __syncthreads();
+    if (sh.fcnt == 0) {  // no vertex at this level: go to the lowest remaining degree
+      __syncthreads();
+      if (threadIdx.x == 0) sh.level = sh.minv;
+      __syncthreads();
+      continue;
+    }
+    int32_t *F = F0, *Gq = G0;
+    for (;;) {
+      const int cnt = sh.fcnt;
+      __syncthreads();
+      if (cnt == 0) break;
+      last_level = level;
+      if (threadIdx.x == 0) {
+        sh.todo -= cnt;
+        sh.ncnt = 0;
+      }
+      __syncthreads();
+      if (sh.todo == 0) break;  // the final round keeps priority m_g
+      for (int i = threadIdx.x; i < cnt; i += blockDim.x) prio[vb + F[i]] = priority;
+      for (int i = w; i < cnt; i += nw) {
+        const int64_t v = vb + F[i];
+        for (int32_t j = rp[v] + lane; j < rp[v + 1]; j += 32) {
+          const int u = (int)(col[j] - vb);
+          if ((unsigned)u >= (unsigned)n) continue;  // not this graph's vertex (invalid input)
+          if (*(volatile int16_t *)&score[u] == -1) {
+            const int old = sdeg_dec(sdeg, u);
+            if (old == level + 1) {
+              score[u] = (int16_t)level;
+              Gq[atomicAdd(&sh.ncnt, 1)] = u;
+            }
+          }
+        }
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) sh.fcnt = sh.ncnt;
+      int32_t *t = F;
+      F = Gq;
+      Gq = t;
+      ++priority;
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) sh.level = level + 1;
+    __syncthreads();
+  }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) core[vb + i] = score[i];
+  if (threadIdx.x == 0) {
+    atomicMax(&ctl->rounds, priority);
+    atomicMax(&ctl->degeneracy, last_level < 0 ? 0 : last_level);
+  }
+  __syncthreads();
+}
+
 __global__ void __launch_bounds__(SEG_BLOCK)
     peel_segments_kernel(const int32_t *__restrict__ rp, const int32_t *__restrict__ col,
                          int32_t *deg, int32_t *core, uint32_t *prio, int32_t *fa, int32_t *fb,
                          const int64_t *__restrict__ vtx_off, const int64_t *__restrict__ arc_off,
                          const int32_t *__restrict__ order, int32_t G, PeelCtl *ctl,
-                         uint32_t *next) {
+                         uint32_t *next, int smem_n) {
   __shared__ SegShared sh;
+  extern __shared__ uint32_t seg_dyn[];  // smem_n / 2 degree words, then smem_n cores
+  uint32_t *sdeg = seg_dyn;
+  int16_t *score = (int16_t *)(seg_dyn + smem_n / 2);
   const int lane = (int)lane_id(), w = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for (;;) {
     if (threadIdx.x == 0) sh.g = atomicAdd(next, 1u);  // next graph, largest first
@@ -444,6 +561,10 @@ __global__ void __launch_bounds__(SEG_BLOCK)
     const int32_t gr = order[gi];
     const int64_t vb = vtx_off[gr] - gr, n = vtx_off[gr + 1] - vtx_off[gr] - 1;
     const uint32_t mg = (uint32_t)(arc_off[gr + 1] - arc_off[gr]);
+    if (n <= smem_n) {
+      peel_graph_smem(rp, col, core, prio, fa + vb, fb + vb, vb, (int)n, mg, sdeg, score, sh, ctl);
+      continue;
+    }
     for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
       const int64_t v = vb + i;
       deg[v] = rp[v + 1] - rp[v];
@@ -533,11 +654,21 @@ __global__ void __launch_bounds__(SEG_BLOCK)
 
 int peel_segments_launch(const PeelArgs &a, const int64_t *vtx_off, const int64_t *arc_off,
                          const int32_t *order, int32_t G, cudaStream_t s, int *launches,
-                         int part) {
+                         int part, int64_t max_n) {
   int dev = 0, sms = 0, per_sm = 0;
   MCE_CUDA(cudaGetDevice(&dev));
   MCE_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  MCE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, peel_segments_kernel, SEG_BLOCK, 0));
+  // shared state for the launch's largest graph, if it fits (an even count)
+  const int smem_n = max_n <= 0 ? 0 : (int)((std::min<int64_t>(max_n, SEG_SMEM_N) + 1) & ~1);
+  const size_t smem = (size_t)smem_n * 4;  // 2 bytes of degree + 2 of core per vertex
+  static bool attr = false;
+  if (!attr) {
+    MCE_CUDA(cudaFuncSetAttribute(peel_segments_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  SEG_SMEM_N * 4));
+    attr = true;
+  }
+  MCE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, peel_segments_kernel, SEG_BLOCK,
+                                                         smem));
   if (per_sm < 1) return MCE_ECUDA;
   PeelCtl *ctl = (PeelCtl *)a.ctl;
   if (part < 0) MCE_CUDA(cudaMemsetAsync(ctl, 0, sizeof(PeelCtl), s));
@@ -546,9 +677,9 @@ int peel_segments_launch(const PeelArgs &a, const int64_t *vtx_off, const int64_
   int blocks = sms * per_sm;
   if (blocks > G) blocks = G;
   if (blocks < 1) return MCE_OK;
-  peel_segments_kernel<<<blocks, SEG_BLOCK, 0, s>>>(a.rp, a.col, a.deg, a.core, a.prio, a.front0,
-                                                    a.front1, vtx_off, arc_off, order, G, ctl,
-                                                    next);
+  peel_segments_kernel<<<blocks, SEG_BLOCK, smem, s>>>(a.rp, a.col, a.deg, a.core, a.prio,
+                                                       a.front0, a.front1, vtx_off, arc_off, order,
+                                                       G, ctl, next, smem_n);
   MCE_CUDA(cudaGetLastError());
   if (launches) *launches += 1;
   return MCE_OK;

@@ -7,14 +7,20 @@
 // most `ego_cap` vertices, relabelled in ascending id order
 // (mce_ego_subgraph builds the same graph on the host).
 //
-// One persistent kernel serves a session.  Each block is a slot: it claims
-// the next published request, extracts the ego subgraph into its own
-// arena, peels and orients it with block barriers (the same synchronous
-// rounds and orientation rule as peel.cu / orient.cu), searches its roots
-// with its 8 warps (the engines of engine.cuh) and writes the count back to
-// mapped host memory.  Requests that arrive while others run are taken by
+// Persistent kernels serve a session.  Each block is a slot: it claims the
+// next published request, extracts the ego subgraph into its own arena,
+// peels and orients it with block barriers (the same synchronous rounds and
+// orientation rule as peel.cu / orient.cu), searches its roots with its
+// warps (the engines of engine.cuh) and writes the count back to mapped
+// host memory.  Requests that arrive while others run are taken by
 // whichever slot frees first, so unrelated requests overlap on the device:
 // continuous batching at request granularity with no launch per request.
+// Two slot classes, one kernel each: class 0, 1,024-thread blocks, takes
+// any request; class 1, 256-thread blocks (four in the room of one class-0
+// block), takes the requests whose footprint bound (deg(seed) + the sum of
+// its neighbours' degrees + 1) fits its smaller cap, which the host routes
+// there while every class-0 slot holds a request.  Each class has its own
+// ring; class-0 slots also take class-1 requests when their ring is empty.
 //
 // Ring protocol (mapped pinned host memory): the host writes entry
 // id % ring, then releases `tail` = id + 1.  On the device one waiting
@@ -45,8 +51,15 @@ namespace {
 // req/s (143 k; the search inside a slot spills at 64 registers).
 constexpr int SV_BLOCK = 1024;
 constexpr int SV_WARPS = SV_BLOCK / 32;
+// Small requests (their footprint bound fits the class-1 cap) run in
+// 256-thread blocks: four at once in the room of one whole-block slot.
+constexpr int SV_SMALL = 256;
 constexpr int SV_DCAP = 256;            // widest root (later neighbours) a slot searches
-constexpr uint64_t SV_POLL_NS = 500;    // host tail read at most this often
+// The host tail of ring 0 is read at most every SV_POLL_NS, ring 1's every
+// 4 x SV_POLL_NS (at 500 ns both, the bus reads of the second ring cost
+// 0.04 ms of median latency at 2,000 requests/s; ring 1 fills under load,
+// when 2 us is small beside a request's service time).
+constexpr uint64_t SV_POLL_NS = 500;
 constexpr int SV_MAX_EGO = 16384;
 
 struct SvEntry {             // one request, in mapped host memory
@@ -67,8 +80,10 @@ struct SvHostHdr {           // mapped host memory, host-written
 };
 
 struct SvCtl {               // device memory
-  uint32_t next, dtail, dstop, pad;
+  uint32_t next, dtail, dstop;
+  uint32_t board_n;          // entries on the help board (class 0's counts them)
   unsigned long long poll_ns, served, nodes, helped;
+  unsigned long long inflight, peak;  // requests on the device (class 0's counts both classes)
 };
 
 // The root work of a slot's current request, shared with helping slots.
@@ -85,21 +100,30 @@ constexpr int SV_HELP_MIN = 1024;             // roots from which a request take
 constexpr uint32_t SV_HELP = 0x40000000u;     // claim(): help slot (value & 0xFFFFFF)
 constexpr uint64_t SV_HELP_WAIT_NS = 60ull * 1000 * 1000 * 1000;
 
-struct ServeArgs {
-  const int32_t *grp, *gcol;  // resident graph
-  int64_t gn;
-  const SvHostHdr *hdr;       // device views of the mapped ring
+// A class of slots with its own request ring and arenas: class 0, whole
+// blocks, takes requests of any footprint up to ego_cap vertices; class 1,
+// 256-thread quarters of blocks, the requests whose footprint bound fits its
+// smaller cap (the host routes each request by it).
+struct SvClass {
+  const SvHostHdr *hdr;       // device views of the class's mapped ring
   SvEntry *ent;
   uint32_t ring;
   SvCtl *ctl;
   char *arena;                // per-slot ego-graph arenas
   size_t arena_bytes;
   int32_t ego_cap, arc_cap, hcap;
-  unsigned long long *slab;   // per-warp engine scratch: register part, then wide part
-  size_t slab_words, reg_words;
+  int32_t slots;
+  unsigned long long *slab;   // per-warp engine scratch of the class's kernel, by block and warp
+};
+
+struct ServeArgs {
+  const int32_t *grp, *gcol;  // resident graph
+  int64_t gn;
+  SvClass cls[2];
+  size_t slab_words, reg_words;  // per warp: register engines' part, then the wide engine's
   uint64_t idle_ns;
   unsigned long long node_budget;  // per request; 0: none
-  SvHelp *help;                    // per slot
+  SvHelp *help;                    // per class-0 slot
   uint32_t *board;                 // slot + 1 of requests open for help (0: empty)
 };
 
@@ -176,28 +200,42 @@ __device__ __forceinline__ bool hput(const Arena &A, int hcap, int32_t key, uint
   return false;  // cannot happen: the table has twice the keys it can receive
 }
 
-// exclusive scan of one value per thread over the block; returns the total
+// A slot's threads: one block of G threads (SV_BLOCK for class 0, SV_SMALL
+// for class 1), so a slot's barriers are the block's.
+template <int G>
+struct Grp {
+  __device__ static int tid() { return (int)threadIdx.x; }
+  __device__ static void sync() { __syncthreads(); }
+  // the number of the slot's threads with p set (and a barrier)
+  __device__ static int count(bool p) { return __syncthreads_count(p); }
+};
+
+// exclusive scan of one value per thread over the slot; returns the total
+template <int G>
 __device__ __forceinline__ int block_scan(int x, int *excl, int *ws) {
-  const int lane = (int)lane_id(), w = threadIdx.x >> 5;
+  using Gp = Grp<G>;
+  const int lane = (int)lane_id(), w = Gp::tid() >> 5;
   const int incl = warp_incl_scan(x);
   if (lane == 31) ws[w] = incl;
-  __syncthreads();
+  Gp::sync();
   int base = 0, total = 0;
 #pragma unroll
-  for (int i = 0; i < SV_WARPS; ++i) {
+  for (int i = 0; i < (G / 32); ++i) {
     base += i < w ? ws[i] : 0;
     total += ws[i];
   }
   *excl = base + incl - x;
-  __syncthreads();
+  Gp::sync();
   return total;
 }
 
 // bitonic sort of buf[0 .. n_pow2) in shared memory
+template <int G>
 __device__ void block_sort(int32_t *buf, int n_pow2) {
+  using Gp = Grp<G>;
   for (int k = 2; k <= n_pow2; k <<= 1)
     for (int j = k >> 1; j > 0; j >>= 1) {
-      for (int i = threadIdx.x; i < n_pow2; i += blockDim.x) {
+      for (int i = Gp::tid(); i < n_pow2; i += G) {
         const int p = i ^ j;
         if (p > i) {
           const bool up = (i & k) == 0;
@@ -208,12 +246,13 @@ __device__ void block_sort(int32_t *buf, int n_pow2) {
           }
         }
       }
-      __syncthreads();
+      Gp::sync();
     }
 }
 
-struct SvShared {
+struct SvShared {  // one per slot
   uint32_t req;
+  int32_t rcls;  // the ring of the claimed request
   int32_t posted, broken;
   int32_t k, fcnt, ncnt, todo, level, minv, acnt, carry;
   unsigned long long total, nodes;
@@ -223,29 +262,33 @@ struct SvShared {
 constexpr int32_t SV_PENDING = -3;  // hval of a vertex first seen in the current window
 
 // inclusive max over the block (one value per thread)
+template <int G>
 __device__ __forceinline__ int block_max_scan(int x, int *ws) {
-  const int lane = (int)lane_id(), w = threadIdx.x >> 5;
+  using Gp = Grp<G>;
+  const int lane = (int)lane_id(), w = Gp::tid() >> 5;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
     const int y = __shfl_up_sync(MCE_FULL, x, o);
     if (lane >= o) x = max(x, y);
   }
   if (lane == 31) ws[w] = x;
-  __syncthreads();
+  Gp::sync();
   int before = -1;
   for (int i = 0; i < w; ++i) before = max(before, ws[i]);
-  __syncthreads();
+  Gp::sync();
   return max(x, before);
 }
 
 // off[0 .. nrows] = exclusive prefix of the resident-row lengths of the
 // vertices list[0 .. nrows), rs[i] = where row i starts in the resident
 // graph (a window's elements then need one load less); returns the total.
+template <int G>
 __device__ int row_offsets(const ServeArgs &S, const int32_t *list, int nrows, int32_t *off,
                            int32_t *rs, SvShared &sh) {
+  using Gp = Grp<G>;
   int base = 0;
-  for (int i0 = 0; i0 < nrows; i0 += blockDim.x) {
-    const int i = i0 + (int)threadIdx.x;
+  for (int i0 = 0; i0 < nrows; i0 += G) {
+    const int i = i0 + Gp::tid();
     int len = 0;
     if (i < nrows) {
       const int32_t g = list[i];
@@ -254,55 +297,59 @@ __device__ int row_offsets(const ServeArgs &S, const int32_t *list, int nrows, i
       rs[i] = r0;
     }
     int ex;
-    const int tot = block_scan(len, &ex, sh.ws);
+    const int tot = block_scan<G>(len, &ex, sh.ws);
     if (i < nrows) off[i] = base + ex;
     base += tot;
   }
-  if (threadIdx.x == 0) off[nrows] = base;
-  __syncthreads();
+  if (Gp::tid() == 0) off[nrows] = base;
+  Gp::sync();
   return base;
 }
 
 // The rows list[0 .. nrows) of the resident graph are walked as one
-// flattened sequence, blockDim elements per window.  This returns the row
-// that owns position e0 + threadIdx.x: the last row starting at or before
+// flattened sequence, G elements per window.  This returns the row
+// that owns position e0 + (the thread's index in its slot): the last row starting at or before
 // it (`carry`, the owner of the previous window's last position, covers a
 // window in which no row starts before a thread's position).  [ia, ib) are
 // the rows starting in the window; ia comes in as the previous window's ib
 // (0 at the start): starts are ascending, so they are found by one pass of
 // coalesced loads, not a search.
+template <int G>
 __device__ int window_owner(const int32_t *off, int nrows, int e0, int carry, int &ia, int &ib,
                             int32_t *own_sm, SvShared &sh) {
-  own_sm[threadIdx.x] = -1;
-  __syncthreads();
-  const int B = (int)blockDim.x;
+  using Gp = Grp<G>;
+  own_sm[Gp::tid()] = -1;
+  Gp::sync();
+  const int B = G;
   int count = 0;
   for (;;) {
-    const int i = ia + count + (int)threadIdx.x;
+    const int i = ia + count + Gp::tid();
     const bool in = i < nrows && off[i] < e0 + B;
     // rows of length 0 start where the next row starts: the larger index wins
     if (in) atomicMax(&own_sm[off[i] - e0], i);
-    const int c = __syncthreads_count(in);
+    const int c = Gp::count(in);
     count += c;
     if (c < B) break;
   }
   ib = ia + count;
-  return max(block_max_scan(own_sm[threadIdx.x], sh.ws), carry);
+  return max(block_max_scan<G>(own_sm[Gp::tid()], sh.ws), carry);
 }
 
 // Append the vertices first met in the rows of list[0 .. nrows) (row order,
 // then position: discovery order) to the ego list, up to the cap.  A vertex
 // seen at several positions of one window is appended at the first.
-__device__ void ego_discover(const ServeArgs &S, const Arena &A, const int32_t *list, int nrows,
+template <int G>
+__device__ void ego_discover(const ServeArgs &S, const SvClass &C, const Arena &A, const int32_t *list, int nrows,
                              int32_t *own_sm, SvShared &sh) {
-  const int cap = S.ego_cap, hc = S.hcap;
-  const int T = row_offsets(S, list, nrows, A.off, A.rs, sh);
+  using Gp = Grp<G>;
+  const int cap = C.ego_cap, hc = C.hcap;
+  const int T = row_offsets<G>(S, list, nrows, A.off, A.rs, sh);
   int carry = -1, ia = 0, ib = 0;
-  for (int e0 = 0; e0 < T; e0 += blockDim.x, ia = ib) {
+  for (int e0 = 0; e0 < T; e0 += G, ia = ib) {
     const int k = sh.k;  // read by all before thread 0 updates it below
     if (k >= cap) break;
-    const int o = window_owner(A.off, nrows, e0, carry, ia, ib, own_sm, sh);
-    const int e = e0 + (int)threadIdx.x;
+    const int o = window_owner<G>(A.off, nrows, e0, carry, ia, ib, own_sm, sh);
+    const int e = e0 + Gp::tid();
     int32_t w = -1;
     uint32_t slot = 0;
     bool cand = false;
@@ -312,10 +359,10 @@ __device__ void ego_discover(const ServeArgs &S, const Arena &A, const int32_t *
       cand = A.hval[slot] == SV_PENDING;
       if (cand) atomicMin(&A.hfirst[slot], e);
     }
-    __syncthreads();
+    Gp::sync();
     const bool fresh = cand && A.hfirst[slot] == e;
     int pos;
-    const int tot = block_scan(fresh ? 1 : 0, &pos, sh.ws);
+    const int tot = block_scan<G>(fresh ? 1 : 0, &pos, sh.ws);
     if (fresh) {
       if (k + pos < cap) {
         A.hval[slot] = k + pos;
@@ -324,105 +371,110 @@ __device__ void ego_discover(const ServeArgs &S, const Arena &A, const int32_t *
         A.hval[slot] = -1;  // beyond the cap: not in the ego graph
       }
     }
-    if (threadIdx.x == blockDim.x - 1) {
+    if (Gp::tid() == G - 1) {
       sh.k = min(cap, k + tot);
       sh.carry = o;
     }
-    __syncthreads();
+    Gp::sync();
     carry = sh.carry;
   }
 }
 
 // Build the ego graph of `seed` in the arena: sorted local CSR in rp/col.
 // Returns its vertex count, or -1 if it has more arcs than the arena holds.
-__device__ int ego_extract(const ServeArgs &S, const Arena &A, int64_t seed, int32_t *sortbuf,
+template <int G>
+__device__ int ego_extract(const ServeArgs &S, const SvClass &C, const Arena &A, int64_t seed,
+                           int32_t *sortbuf,
                            int32_t *own_sm, SvShared &sh) {
-  const int hc = S.hcap;
-  for (int i = threadIdx.x; i < hc; i += blockDim.x) {
+  using Gp = Grp<G>;
+  const int hc = C.hcap;
+  for (int i = Gp::tid(); i < hc; i += G) {
     A.hkey[i] = -1;
     A.hval[i] = SV_PENDING;
     A.hfirst[i] = INT_MAX;
   }
-  __syncthreads();
-  if (threadIdx.x == 0) {
+  Gp::sync();
+  if (Gp::tid() == 0) {
     uint32_t slot = 0;
     hput(A, hc, (int32_t)seed, &slot);
     A.hval[slot] = 0;
     A.V[0] = (int32_t)seed;
     sh.k = 1;
   }
-  __syncthreads();
-  ego_discover(S, A, A.V, 1, own_sm, sh);  // 1-hop: the seed's row
+  Gp::sync();
+  ego_discover<G>(S, C, A, A.V, 1, own_sm, sh);  // 1-hop: the seed's row
   const int k1 = sh.k;
-  if (k1 < S.ego_cap && k1 > 1) ego_discover(S, A, A.V + 1, k1 - 1, own_sm, sh);  // 2-hop
+  if (k1 < C.ego_cap && k1 > 1) ego_discover<G>(S, C, A, A.V + 1, k1 - 1, own_sm, sh);  // 2-hop
   const int n = sh.k;
   // local ids in ascending resident-graph id
   int np2 = 1;
   while (np2 < n) np2 <<= 1;
-  for (int i = threadIdx.x; i < np2; i += blockDim.x) sortbuf[i] = i < n ? A.V[i] : INT_MAX;
-  __syncthreads();
-  block_sort(sortbuf, np2);
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+  for (int i = Gp::tid(); i < np2; i += G) sortbuf[i] = i < n ? A.V[i] : INT_MAX;
+  Gp::sync();
+  block_sort<G>(sortbuf, np2);
+  for (int i = Gp::tid(); i < n; i += G) {
     const int32_t w = sortbuf[i];
     A.V[i] = w;
     uint32_t h = hslot(w, hc);
     for (int p = 0; p < hc && A.hkey[h] != w; ++p) h = (h + 1) & (uint32_t)(hc - 1);
     A.hval[h] = i;
   }
-  __syncthreads();
+  Gp::sync();
   // induced rows in one flattened pass: the i-th kept element overall is
   // col[i] (rows in order, each filtered row stays sorted), and a row starts
   // at the count of kept elements before its first one
-  const int T = row_offsets(S, A.V, n, A.off, A.rs, sh);
+  const int T = row_offsets<G>(S, A.V, n, A.off, A.rs, sh);
   int carry = -1, kept = 0, ia = 0, ib = 0;
-  for (int e0 = 0; e0 < T; e0 += blockDim.x, ia = ib) {
-    const int o = window_owner(A.off, n, e0, carry, ia, ib, own_sm, sh);
-    const int e = e0 + (int)threadIdx.x;
+  for (int e0 = 0; e0 < T; e0 += G, ia = ib) {
+    const int o = window_owner<G>(A.off, n, e0, carry, ia, ib, own_sm, sh);
+    const int e = e0 + Gp::tid();
     int32_t loc = -1;
     if (e < T) loc = hget(A, hc, S.gcol[A.rs[o] + (e - A.off[o])]);
     int pos;
-    const int tot = block_scan(loc >= 0 ? 1 : 0, &pos, sh.ws);
-    if (loc >= 0 && kept + pos < S.arc_cap) A.col[kept + pos] = loc;
-    own_sm[threadIdx.x] = pos;  // kept elements of this window before each position
-    __syncthreads();
-    for (int i = ia + (int)threadIdx.x; i < ib; i += blockDim.x)  // rows starting here
+    const int tot = block_scan<G>(loc >= 0 ? 1 : 0, &pos, sh.ws);
+    if (loc >= 0 && kept + pos < C.arc_cap) A.col[kept + pos] = loc;
+    own_sm[Gp::tid()] = pos;  // kept elements of this window before each position
+    Gp::sync();
+    for (int i = ia + Gp::tid(); i < ib; i += G)  // rows starting here
       A.rp[i] = kept + own_sm[A.off[i] - e0];
-    if (threadIdx.x == blockDim.x - 1) sh.carry = o;
-    __syncthreads();
+    if (Gp::tid() == G - 1) sh.carry = o;
+    Gp::sync();
     carry = sh.carry;
     kept += tot;
   }
-  for (int i = threadIdx.x; i <= n; i += blockDim.x)  // rows starting at the end (empty)
+  for (int i = Gp::tid(); i <= n; i += G)  // rows starting at the end (empty)
     if (A.off[i] == T) A.rp[i] = kept;
-  __syncthreads();
-  return kept > S.arc_cap ? -1 : n;
+  Gp::sync();
+  return kept > C.arc_cap ? -1 : n;
 }
 
 // Degeneracy priorities of the ego graph: synchronous peeling rounds over
 // all levels, the final round keeping priority m (peel.cu's order).
+template <int G>
 __device__ void ego_peel(const Arena &A, int n, SvShared &sh) {
+  using Gp = Grp<G>;
   const int m = A.rp[n];
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+  for (int i = Gp::tid(); i < n; i += G) {
     A.deg[i] = A.rp[i + 1] - A.rp[i];
     A.core[i] = -1;
     A.prio[i] = (uint32_t)m;
   }
-  if (threadIdx.x == 0) {
+  if (Gp::tid() == 0) {
     sh.todo = n;
     sh.level = 0;
   }
-  __syncthreads();
+  Gp::sync();
   uint32_t priority = 0;
-  const int lane = (int)lane_id(), w = threadIdx.x >> 5;
+  const int lane = (int)lane_id(), w = Gp::tid() >> 5;
   while (sh.todo > 0) {
     const int level = sh.level;
-    __syncthreads();
-    if (threadIdx.x == 0) {
+    Gp::sync();
+    if (Gp::tid() == 0) {
       sh.fcnt = 0;
       sh.minv = INT_MAX;
     }
-    __syncthreads();
-    for (int i = threadIdx.x; i < n; i += blockDim.x)
+    Gp::sync();
+    for (int i = Gp::tid(); i < n; i += G)
       if (A.core[i] == -1) {
         if (A.deg[i] <= level) {  // == level: a remaining vertex never has less
           A.core[i] = level;
@@ -431,26 +483,26 @@ __device__ void ego_peel(const Arena &A, int n, SvShared &sh) {
           atomicMin(&sh.minv, A.deg[i]);
         }
       }
-    __syncthreads();
+    Gp::sync();
     if (sh.fcnt == 0) {  // no vertex at this level: go to the lowest remaining degree
-      __syncthreads();
-      if (threadIdx.x == 0) sh.level = sh.minv;
-      __syncthreads();
+      Gp::sync();
+      if (Gp::tid() == 0) sh.level = sh.minv;
+      Gp::sync();
       continue;
     }
-    int32_t *F = A.fa, *G = A.fb;
+    int32_t *F = A.fa, *Nx = A.fb;
     for (;;) {
       const int cnt = sh.fcnt;
-      __syncthreads();
+      Gp::sync();
       if (cnt == 0) break;
-      if (threadIdx.x == 0) {
+      if (Gp::tid() == 0) {
         sh.todo -= cnt;
         sh.ncnt = 0;
       }
-      __syncthreads();
+      Gp::sync();
       if (sh.todo == 0) break;  // the final round keeps priority m
-      for (int i = threadIdx.x; i < cnt; i += blockDim.x) A.prio[F[i]] = priority;
-      for (int i = w; i < cnt; i += SV_WARPS) {
+      for (int i = Gp::tid(); i < cnt; i += G) A.prio[F[i]] = priority;
+      for (int i = w; i < cnt; i += (G / 32)) {
         const int v = F[i];
         for (int j = A.rp[v] + lane; j < A.rp[v + 1]; j += 32) {
           const int u = A.col[j];
@@ -458,30 +510,32 @@ __device__ void ego_peel(const Arena &A, int n, SvShared &sh) {
             const int old = atomicSub(&A.deg[u], 1);
             if (old == level + 1) {
               A.core[u] = level;
-              G[atomicAdd(&sh.ncnt, 1)] = u;
+              Nx[atomicAdd(&sh.ncnt, 1)] = u;
             }
           }
         }
       }
-      __syncthreads();
-      if (threadIdx.x == 0) sh.fcnt = sh.ncnt;
+      Gp::sync();
+      if (Gp::tid() == 0) sh.fcnt = sh.ncnt;
       int32_t *t = F;
-      F = G;
-      G = t;
+      F = Nx;
+      Nx = t;
       ++priority;
-      __syncthreads();
+      Gp::sync();
     }
-    if (threadIdx.x == 0) sh.level = level + 1;
-    __syncthreads();
+    if (Gp::tid() == 0) sh.level = level + 1;
+    Gp::sync();
   }
 }
 
 // Rows become [earlier | later]; u is later than v iff
 // prio[v] == prio[u] ? v < u : prio[v] < prio[u] (include/main_support.cuh:14).
+template <int G>
 __device__ void ego_orient(const Arena &A, int n) {
-  const int lane = (int)lane_id(), w = threadIdx.x >> 5;
+  using Gp = Grp<G>;
+  const int lane = (int)lane_id(), w = Gp::tid() >> 5;
   const uint32_t lt = (1u << lane) - 1u;
-  for (int v = w; v < n; v += SV_WARPS) {
+  for (int v = w; v < n; v += (G / 32)) {
     const int b = A.rp[v], e = A.rp[v + 1];
     const uint32_t pv = A.prio[v];
     int ne = 0;
@@ -514,7 +568,7 @@ __device__ void ego_orient(const Arena &A, int n) {
     }
     if (lane == 0) A.split[v] = b + ne;
   }
-  __syncthreads();
+  Gp::sync();
 }
 
 union WarpSmem {
@@ -525,38 +579,67 @@ union WarpSmem {
 
 constexpr uint32_t SV_EXIT = 0xFFFFFFFFu;
 
-// Thread 0 of a slot: wait for a published request and claim it; SV_EXIT
-// when the session stops or the slot has been idle for idle_ns.
-__device__ uint32_t claim(const ServeArgs &S) {
-  SvCtl *c = S.ctl;
+// Mirror the class's host tail and stop flag into device memory (one
+// thread at a time, at most every SV_POLL_NS); stop first: the host
+// publishes its last request before stopping, so a tail read after a stop
+// read sees that request.
+__device__ __forceinline__ void poll_ring(const SvClass &C, uint64_t now, uint64_t every) {
+  SvCtl *c = C.ctl;
+  const unsigned long long last = ld_volatile(&c->poll_ns);
+  if (now - last >= every && atomicCAS(&c->poll_ns, last, now) == last) {
+    const uint32_t st = ld_acquire_sys(&C.hdr->stop);
+    const uint32_t t = ld_acquire_sys(&C.hdr->tail);
+    atomicMax(&c->dtail, t);
+    __threadfence();
+    if (st) atomicExch(&c->dstop, 1u);
+  }
+}
+
+// Claim the next published request of class C: its id, or SV_EXIT if none
+// is waiting (*stop: the class is stopping).
+__device__ __forceinline__ uint32_t try_claim(const SvClass &C, bool *stop) {
+  SvCtl *c = C.ctl;
+  *stop = ld_volatile(&c->dstop) != 0;  // before dtail, as poll_ring writes them
+  __threadfence();
+  for (;;) {
+    const uint32_t k = ld_volatile(&c->next);
+    if (k >= ld_volatile(&c->dtail)) return SV_EXIT;
+    if (atomicCAS(&c->next, k, k + 1) == k) {
+      __threadfence_system();  // the entry's seed is read after this
+      return k;
+    }
+  }
+}
+
+// Thread 0 of a slot of class `mine`: wait for a published request and
+// claim it (*cls: the ring it came from); SV_HELP | j to help class-0 slot
+// j's search; SV_EXIT when the session stops or the slot has been idle for
+// idle_ns.  A class-0 slot also takes class-1 requests (its arena holds
+// them) when its own ring is empty.
+__device__ uint32_t claim(const ServeArgs &S, int mine, int *cls) {
   const uint64_t t_idle = globaltimer_ns();
   uint32_t ns = 64;
   for (;;) {
     const uint64_t now = globaltimer_ns();
-    const unsigned long long last = ld_volatile(&c->poll_ns);
-    if (now - last >= SV_POLL_NS && atomicCAS(&c->poll_ns, last, now) == last) {
-      // stop first: the host publishes its last request before stopping,
-      // so a tail read after a stop read sees that request
-      const uint32_t st = ld_acquire_sys(&S.hdr->stop);
-      const uint32_t t = ld_acquire_sys(&S.hdr->tail);
-      atomicMax(&c->dtail, t);
-      __threadfence();
-      if (st) atomicExch(&c->dstop, 1u);
-    }
-    const uint32_t stop = ld_volatile(&c->dstop);  // before dtail, as written above
-    __threadfence();
-    const uint32_t k = ld_volatile(&c->next);
-    if (k < ld_volatile(&c->dtail)) {
-      if (atomicCAS(&c->next, k, k + 1) == k) {
-        __threadfence_system();  // the entry's seed is read after this
+    bool stop0 = true, stop1 = true;
+    for (int c = mine; c < 2; ++c) {
+      if (S.cls[c].slots == 0 && c != mine) continue;
+      poll_ring(S.cls[c], now, c == 0 ? SV_POLL_NS : 4 * SV_POLL_NS);
+      bool st = false;
+      const uint32_t k = try_claim(S.cls[c], &st);
+      if (k != SV_EXIT) {
+        *cls = c;
         return k;
       }
-      continue;
+      (c == 0 ? stop0 : stop1) = st;
     }
-    if (stop) return SV_EXIT;
+    if (mine == 0 ? (stop0 && (stop1 || S.cls[1].slots == 0)) : stop1) return SV_EXIT;
     if (now - t_idle > S.idle_ns) return SV_EXIT;
-    // no new request: join the search of a large one another slot runs
-    for (int e = 0; e < SV_BOARD; ++e) {
+    // no new request: join the search of a large one a class-0 slot runs
+    // (the board is scanned only when something is posted: hundreds of idle
+    // slots reading its 64 words saturated the L2 slices that hold them)
+    const int posted = ld_volatile(&S.cls[0].ctl->board_n) != 0 ? SV_BOARD : 0;
+    for (int e = 0; e < posted; ++e) {
       const uint32_t j1 = ld_volatile(&S.board[e]);
       if (j1 == 0) continue;
       SvHelp *h = &S.help[j1 - 1];
@@ -627,29 +710,29 @@ __device__ void search_roots(const ServeArgs &S, const BKArgs &a, const BKArgs &
   if (lane == 0 && mine) atomicAdd(&h->total, mine);
 }
 
-__global__ void __launch_bounds__(SV_BLOCK) serve_kernel(ServeArgs S) {
-  // dynamic: the warps' engine state, then the sort buffer (next power of
-  // two >= ego_cap ints)
-  extern __shared__ __align__(16) unsigned char sv_dyn[];
-  WarpSmem *wsm = (WarpSmem *)sv_dyn;
-  int32_t *sortbuf = (int32_t *)(sv_dyn + sizeof(WarpSmem) * SV_WARPS);
-  __shared__ SvShared sh;
-  __shared__ int32_t own_sm[SV_BLOCK];
-  const int lane = (int)lane_id(), w = threadIdx.x >> 5;
+// One slot: one block, of SV_BLOCK threads (class 0) or SV_SMALL (class 1),
+// with its own shared state sh and windows own_sm (one int per thread), its
+// sort buffer (the next power of two >= its class's cap, ints), its arena,
+// and its warps' engine state and slabs.
+template <bool BIG>
+__device__ __forceinline__ void serve_slot(const ServeArgs &S, int slot, SvShared &sh,
+                                           int32_t *own_sm, int32_t *sortbuf, WarpSmem *wsm) {
+  constexpr bool big = BIG;
+  constexpr int G = BIG ? SV_BLOCK : SV_SMALL;
+  const int mine = big ? 0 : 1;
+  const int tid = (int)threadIdx.x;
+  const int w = (int)(threadIdx.x >> 5);
+  const SvClass &M = S.cls[mine];
   Arena A;
-  arena_layout(S.ego_cap, S.arc_cap, S.hcap, S.arena + (size_t)blockIdx.x * S.arena_bytes, &A);
+  arena_layout(M.ego_cap, M.arc_cap, M.hcap, M.arena + (size_t)slot * M.arena_bytes, &A);
   unsigned long long *wslab =
-      S.slab + ((size_t)blockIdx.x * SV_WARPS + (size_t)w) * S.slab_words;
-  // engine arguments over the slot's arena (no task sharing, no per-root logs)
+      M.slab + ((size_t)blockIdx.x * (G / 32) + (size_t)w) * S.slab_words;
+  // engine arguments (no task sharing, no per-root logs); the slabs are laid
+  // out for class 0's cap; the arena fields are set per search
   BKArgs a;
   memset(&a, 0, sizeof(a));
-  a.rp = A.rp;
-  a.split = A.split;
-  a.cs = A.cs;
-  a.hist = A.hist;
-  a.err = A.err;
   a.dcap = SV_DCAP;
-  a.xcap = S.ego_cap;
+  a.xcap = S.cls[0].ego_cap;
   a.node_budget = S.node_budget;
   a.slab = wslab + S.reg_words;
   a.slab_words = 0;
@@ -658,83 +741,105 @@ __global__ void __launch_bounds__(SV_BLOCK) serve_kernel(ServeArgs S) {
   ar.slab = wslab;
   const RegSlab<uint32_t> rs32 = reg_slab<uint32_t>(ar, 0);
   const RegSlab<u64> rs64 = reg_slab<u64>(ar, 0);
-  SvHelp *own = &S.help[blockIdx.x];
+  SvHelp *own = &S.help[mine == 0 ? slot : S.cls[0].slots + slot];
+  SvCtl *inflight = S.cls[0].ctl;  // requests on the device, over both classes
   for (;;) {
-    if (threadIdx.x == 0) sh.req = claim(S);
+    if (tid == 0) {
+      int c = mine;
+      sh.req = claim(S, mine, &c);
+      sh.rcls = c;
+    }
     __syncthreads();
     const uint32_t req = sh.req;
+    const int rc_cls = sh.rcls;
     if (req == SV_EXIT) break;
-    if (req & SV_HELP) {  // search roots of another slot's request in its arena
-      const uint32_t j = req & 0xFFFFFFu;
-      Arena B;
-      arena_layout(S.ego_cap, S.arc_cap, S.hcap, S.arena + (size_t)j * S.arena_bytes, &B);
-      BKArgs hb = a, hr = ar;
-      hb.rp = hr.rp = B.rp;
-      hb.split = hr.split = B.split;
-      hb.cs = hr.cs = B.cs;
-      hb.hist = hr.hist = B.hist;
-      hb.err = hr.err = B.err;
-      search_roots(S, hb, hr, msl, rs32, rs64, wsm[w], &S.help[j]);
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        __threadfence();  // this block's counts land before it leaves
-        atomicSub(&S.help[j].state, 1u);
-        atomicAdd(&S.ctl->helped, 1ull);
-      }
-      continue;
-    }
-    if (threadIdx.x == 0) {
-      *A.err = 0;
-      sh.posted = -1;
-      sh.broken = 0;
-    }
-    __syncthreads();
-    const uint64_t t0 = globaltimer_ns();
-    uint64_t t1 = t0, t2 = t0;
-    SvEntry *E = S.ent + (req % S.ring);
-    const int64_t seed = *(volatile int64_t *)&E->seed;
+    const bool helping = (req & SV_HELP) != 0;
+    // the request whose roots this slot searches: a class-0 slot's (helping)
+    // or its own
+    Arena X = A;
+    SvHelp *h = own;
+    const SvClass &R = S.cls[rc_cls];
+    SvEntry *E = nullptr;
     int32_t status = MCE_OK;
     uint32_t limits = 0;
     int n = 0;
-    if (seed < 0 || seed >= S.gn) {
-      status = MCE_EINVAL;
+    uint64_t t0 = 0, t1 = 0, t2 = 0;
+    if (helping) {
+      const uint32_t j = req & 0xFFFFFFu;
+      const SvClass &B0 = S.cls[0];
+      arena_layout(B0.ego_cap, B0.arc_cap, B0.hcap, B0.arena + (size_t)j * B0.arena_bytes, &X);
+      h = &S.help[j];
     } else {
-      n = ego_extract(S, A, seed, sortbuf, own_sm, sh);
-      t1 = t2 = globaltimer_ns();
-      if (n < 0) {
-        status = MCE_ELIMIT;
-        limits = MCE_ERR_ARCS;
-        n = 0;
+      if (tid == 0) {
+        *A.err = 0;
+        sh.posted = -1;
+        sh.broken = 0;
+        sh.total = 0;
+        sh.nodes = 0;
+        const unsigned long long on = atomicAdd(&inflight->inflight, 1ull) + 1;
+        atomicMax(&inflight->peak, on);
       }
-    }
-    if (threadIdx.x == 0) {
-      sh.total = 0;
-      sh.nodes = 0;
-    }
-    if (status == MCE_OK) {
-      ego_peel(A, n, sh);
-      ego_orient(A, n);
-      t2 = globaltimer_ns();
-      if (threadIdx.x == 0) {  // open the roots; large requests also to helping slots
-        own->rootnext = 0;
-        own->n = n;
-        own->total = 0;
-        own->nodes = 0;
-        __threadfence();  // the arena and the fields above before the opening
-        if (n >= SV_HELP_MIN) {
-          atomicExch(&own->state, SV_OPEN);
-          for (int e = 0; e < SV_BOARD; ++e)
-            if (atomicCAS(&S.board[e], 0u, blockIdx.x + 1) == 0u) {
-              sh.posted = e;
-              break;
-            }
+      __syncthreads();
+      t0 = t1 = t2 = globaltimer_ns();
+      E = R.ent + (req % R.ring);
+      const int64_t seed = *(volatile int64_t *)&E->seed;
+      if (seed < 0 || seed >= S.gn) {
+        status = MCE_EINVAL;
+      } else {
+        n = ego_extract<G>(S, M, A, seed, sortbuf, own_sm, sh);
+        t1 = t2 = globaltimer_ns();
+        if (n < 0) {
+          status = MCE_ELIMIT;
+          limits = MCE_ERR_ARCS;
+          n = 0;
         }
       }
-      __syncthreads();
-      search_roots(S, a, ar, msl, rs32, rs64, wsm[w], own);
-      __syncthreads();
-      if (threadIdx.x == 0) {  // close, then wait (bounded) for the helpers to leave
-        if (sh.posted >= 0) atomicExch(&S.board[sh.posted], 0u);
+      if (status == MCE_OK) {
+        ego_peel<G>(A, n, sh);
+        ego_orient<G>(A, n);
+        t2 = globaltimer_ns();
+        if (tid == 0) {  // open the roots; large requests also to helping slots
+          own->rootnext = 0;
+          own->n = n;
+          own->total = 0;
+          own->nodes = 0;
+          __threadfence();  // the arena and the fields above before the opening
+          if (mine == 0 && n >= SV_HELP_MIN) {
+            atomicExch(&own->state, SV_OPEN);
+            for (int e = 0; e < SV_BOARD; ++e)
+              if (atomicCAS(&S.board[e], 0u, (uint32_t)slot + 1) == 0u) {
+                atomicAdd(&S.cls[0].ctl->board_n, 1u);
+                sh.posted = e;
+                break;
+              }
+          }
+        }
+        __syncthreads();
+      }
+    }
+    if (status == MCE_OK) {
+      a.rp = ar.rp = X.rp;
+      a.split = ar.split = X.split;
+      a.cs = ar.cs = X.cs;
+      a.hist = ar.hist = X.hist;
+      a.err = ar.err = X.err;
+      search_roots(S, a, ar, msl, rs32, rs64, wsm[w], h);
+    }
+    __syncthreads();
+    if (helping) {
+      if (tid == 0) {
+        __threadfence();  // this slot's counts land before it leaves
+        atomicSub(&h->state, 1u);
+        atomicAdd(&M.ctl->helped, 1ull);
+      }
+      continue;
+    }
+    if (status == MCE_OK) {
+      if (tid == 0) {  // close, then wait (bounded) for the helpers to leave
+        if (sh.posted >= 0) {
+          atomicExch(&S.board[sh.posted], 0u);
+          atomicSub(&S.cls[0].ctl->board_n, 1u);
+        }
         atomicAnd(&own->state, ~SV_OPEN);
         const uint64_t tw = globaltimer_ns();
         while ((ld_volatile(&own->state) & 0xFFFFFFu) != 0) {
@@ -754,7 +859,7 @@ __global__ void __launch_bounds__(SV_BLOCK) serve_kernel(ServeArgs S) {
       if (sh.broken) status = MCE_ETIMEOUT;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (tid == 0) {
       E->count = status == MCE_OK ? sh.total : 0ull;
       const uint64_t t3 = globaltimer_ns();
       E->device_ns = t3 - t0;
@@ -768,12 +873,53 @@ __global__ void __launch_bounds__(SV_BLOCK) serve_kernel(ServeArgs S) {
       E->ego_arcs = n > 0 ? A.rp[n] : 0;
       __threadfence_system();
       *(volatile uint32_t *)&E->done = req + 1;
-      atomicAdd(&S.ctl->served, 1ull);
-      atomicAdd(&S.ctl->nodes, sh.nodes);
+      atomicAdd(&R.ctl->served, 1ull);
+      atomicAdd(&R.ctl->nodes, sh.nodes);
+      atomicAdd(&inflight->inflight, ~0ull);  // minus one
     }
     __syncthreads();
     // a helper that never left may still read the arena: the slot retires
     if (sh.broken) break;
+  }
+}
+
+// One kernel per slot class, launched side by side on two streams: a block
+// of serve_kernel<true> (SV_BLOCK threads) is one class-0 slot, a block of
+// serve_kernel<false> (SV_SMALL threads, four to an SM's room of one
+// class-0 block) one class-1 slot.  Dynamic shared memory: the warps'
+// engine state, then the sort buffer.
+template <bool BIG>
+__global__ void __launch_bounds__(BIG ? SV_BLOCK : SV_SMALL, BIG ? 1 : SV_BLOCK / SV_SMALL)
+    serve_kernel(ServeArgs S) {
+  constexpr int G = BIG ? SV_BLOCK : SV_SMALL;
+  extern __shared__ __align__(16) unsigned char sv_dyn[];
+  WarpSmem *wsm = (WarpSmem *)sv_dyn;
+  int32_t *sortbuf = (int32_t *)(sv_dyn + sizeof(WarpSmem) * (G / 32));
+  __shared__ SvShared sh;
+  __shared__ int32_t own[G];
+  serve_slot<BIG>(S, (int)blockIdx.x, sh, own, sortbuf, wsm);
+}
+
+// Per vertex: deg(v) + the sum of its neighbours' degrees, capped at
+// INT32_MAX - a bound on the 2-hop ego graph's size minus one (one warp per
+// vertex).
+__global__ void footprint_kernel(const int32_t *__restrict__ rp, const int32_t *__restrict__ col,
+                                 int64_t n, int32_t *__restrict__ bound) {
+  const int lane = (int)lane_id();
+  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t v = gw; v < n; v += nw) {
+    const int32_t b = rp[v], e = rp[v + 1];
+    long long acc = 0;
+    for (int32_t j = b + lane; j < e; j += 32) {
+      const int32_t u = col[j];
+      acc += rp[u + 1] - rp[u];
+    }
+    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(MCE_FULL, acc, o);
+    if (lane == 0) {
+      acc += e - b;
+      bound[v] = (int32_t)(acc > 0x7FFFFFFFll ? 0x7FFFFFFFll : acc);
+    }
   }
 }
 
@@ -789,68 +935,107 @@ int graph_device_view(const struct ::mce_graph *g, const int32_t **rp, const int
 // ---------------------------------------------------------------------------
 using namespace mce;
 
-struct mce_serve {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  ServeArgs args{};
-  size_t smem = 0;
-  uint32_t slots = 0, ring = 0;
+// One class's request ring in mapped pinned memory, its arenas and control.
+struct SvRing {
   char *host = nullptr;        // mapped: SvHostHdr then the ring entries
   SvHostHdr *hdr = nullptr;    // host views
   SvEntry *ent = nullptr;
   uint32_t tail = 0;           // requests published
   uint32_t low = 0;            // lowest id whose entry is not yet free
+  uint32_t open = 0;           // submitted, answer not yet taken
   std::vector<uint8_t> taken;  // per entry: answer handed to the caller
   char *arena = nullptr;
-  unsigned long long *slab = nullptr;
   SvCtl *ctl = nullptr;
+};
+
+struct mce_serve {
+  int device = 0;
+  cudaStream_t stream[2] = {nullptr, nullptr};  // one kernel per class
+  ServeArgs args{};
+  size_t smem[2] = {0, 0};
+  uint32_t grid[2] = {0, 0};    // blocks of each class's kernel
+  uint32_t blocks = 0, ring = 0;
+  SvRing cls[2];                // 0: whole-block slots, 1: quarter-block slots
+  std::vector<int32_t> bound;   // per vertex: its footprint bound (2-hop degree sum)
+  int32_t small_cap = 0;        // class-1 cap (0: one class)
+  unsigned long long *slab = nullptr;
   SvHelp *help = nullptr;
   uint32_t *board = nullptr;
   int64_t launches = 0;
   bool closed = false;
+  std::chrono::steady_clock::time_point checked[2];  // last look at each kernel's stream
 };
 
 namespace {
 
-int sv_launch(mce_serve *s) {
-  serve_kernel<<<s->slots, SV_BLOCK, s->smem, s->stream>>>(s->args);
+// a request id names its ring in bit 0 and its place in the ring above it
+inline int id_cls(uint64_t id) { return (int)(id & 1u); }
+inline uint32_t id_local(uint64_t id) { return (uint32_t)(id >> 1); }
+
+int sv_launch(mce_serve *s, int c) {
+  if (c == 0)
+    serve_kernel<true><<<s->grid[0], SV_BLOCK, s->smem[0], s->stream[0]>>>(s->args);
+  else
+    serve_kernel<false><<<s->grid[1], SV_SMALL, s->smem[1], s->stream[1]>>>(s->args);
   MCE_CUDA(cudaGetLastError());
   ++s->launches;
   return MCE_OK;
 }
 
-// relaunch when requests are waiting and every slot has left
+// relaunch a class's kernel when requests of its ring wait and every slot
+// of that kernel has left.  Each stream is looked at most every 100 us (a
+// kernel leaves only after idle_ms): with a driver call per poll of every
+// open request, the median host-observed latency at 2,000 requests/s was
+// 0.06 ms higher with two slot classes.
 int sv_ensure_running(mce_serve *s) {
-  const cudaError_t q = cudaStreamQuery(s->stream);
-  if (q == cudaErrorNotReady) return MCE_OK;
-  if (q != cudaSuccess) return MCE_ECUDA;
-  SvCtl c;
-  MCE_CUDA(cudaMemcpy(&c, s->ctl, sizeof(c), cudaMemcpyDeviceToHost));
-  if (c.next >= s->tail) return MCE_OK;  // nothing unclaimed
-  return sv_launch(s);
+  const auto now = std::chrono::steady_clock::now();
+  for (int c = 0; c < 2; ++c) {
+    if (!s->cls[c].ctl || now - s->checked[c] < std::chrono::microseconds(100)) continue;
+    s->checked[c] = now;
+    const cudaError_t q = cudaStreamQuery(s->stream[c]);
+    if (q == cudaErrorNotReady) continue;
+    if (q != cudaSuccess) return MCE_ECUDA;
+    SvCtl ct;
+    MCE_CUDA(cudaMemcpy(&ct, s->cls[c].ctl, sizeof(ct), cudaMemcpyDeviceToHost));
+    if (ct.next < s->cls[c].tail) {  // something unclaimed
+      const int rc = sv_launch(s, c);
+      if (rc != MCE_OK) return rc;
+    }
+  }
+  return MCE_OK;
 }
 
-bool sv_done(const mce_serve *s, uint32_t id) {
-  const SvEntry &e = s->ent[id % s->ring];
+bool sv_done(const mce_serve *s, int c, uint32_t id) {
+  const SvEntry &e = s->cls[c].ent[id % s->ring];
   return __atomic_load_n(&e.done, __ATOMIC_ACQUIRE) == id + 1;
 }
 
-void sv_retire(mce_serve *s) {
-  while (s->low < s->tail && s->taken[s->low % s->ring]) {
-    s->taken[s->low % s->ring] = 0;
-    ++s->low;
+void sv_retire(mce_serve *s, int c) {
+  SvRing &R = s->cls[c];
+  while (R.low < R.tail && R.taken[R.low % s->ring]) {
+    R.taken[R.low % s->ring] = 0;
+    ++R.low;
   }
 }
 
 void sv_free(mce_serve *s) {
-  if (s->stream) cudaStreamDestroy(s->stream);
-  if (s->host) cudaFreeHost(s->host);
-  if (s->arena) cudaFree(s->arena);
+  for (cudaStream_t st : s->stream)
+    if (st) cudaStreamDestroy(st);
+  for (SvRing &R : s->cls) {
+    if (R.host) cudaFreeHost(R.host);
+    if (R.arena) cudaFree(R.arena);
+    if (R.ctl) cudaFree(R.ctl);
+  }
   if (s->slab) cudaFree(s->slab);
-  if (s->ctl) cudaFree(s->ctl);
   if (s->help) cudaFree(s->help);
   if (s->board) cudaFree(s->board);
   delete s;
+}
+
+int hash_cap_for(int ego_cap, int threads) {  // the table also takes the up to
+  int hcap = 32;                              // threads - 1 vertices of the window
+  while (hcap < 2 * (ego_cap + threads)) hcap <<= 1;  // that crosses the cap
+  return hcap;
 }
 
 }  // namespace
@@ -863,6 +1048,8 @@ extern "C" void mce_serve_opts_default(mce_serve_opts_t *o) {
   o->slots = 0;
   o->ring = 4096;
   o->idle_ms = 1000;
+  o->small_cap = -1;  // automatic
+  o->big_slots = 0;
 }
 
 extern "C" int mce_serve_open(mce_graph_t g, const mce_serve_opts_t *opts, mce_serve_t *out) {
@@ -871,8 +1058,13 @@ extern "C" int mce_serve_open(mce_graph_t g, const mce_serve_opts_t *opts, mce_s
   mce_serve_opts_default(&o);
   if (opts) o = *opts;
   if (o.ego_cap < 2 || o.ego_cap > SV_MAX_EGO || o.ring < 1 || o.ring > (1u << 24) ||
-      o.idle_ms < 1 || o.max_arcs < 0 || o.max_nodes < 0)
+      o.idle_ms < 1 || o.max_arcs < 0 || o.max_nodes < 0 || o.small_cap > o.ego_cap ||
+      o.big_slots < 0)
     return MCE_EINVAL;
+  // class 1 (quarter-block slots) for requests whose footprint bound fits
+  // small_cap vertices; automatic: 1,024 when the cap is above 2,048
+  const int32_t small_cap = o.small_cap < 0 ? (o.ego_cap > 2048 ? 1024 : 0)
+                                            : (o.small_cap >= 2 ? o.small_cap : 0);
   const int32_t *rp = nullptr, *col = nullptr;
   int64_t n = 0;
   int device = 0;
@@ -884,74 +1076,118 @@ extern "C" int mce_serve_open(mce_graph_t g, const mce_serve_opts_t *opts, mce_s
   mce_serve *s = new mce_serve();
   s->device = device;
   s->ring = o.ring;
-  int np2 = 1;
+  s->small_cap = small_cap;
+  int np2 = 1, np2s = 1;
   while (np2 < o.ego_cap) np2 <<= 1;
-  s->smem = sizeof(WarpSmem) * SV_WARPS + sizeof(int32_t) * (size_t)np2;
+  while (np2s < small_cap) np2s <<= 1;
+  s->smem[0] = sizeof(WarpSmem) * SV_WARPS + sizeof(int32_t) * (size_t)np2;
+  s->smem[1] = sizeof(WarpSmem) * (SV_SMALL / 32) + sizeof(int32_t) * (size_t)np2s;
   auto fail = [&](int code) {
     sv_free(s);
     return code;
   };
-  if (cudaFuncSetAttribute(serve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)s->smem) != cudaSuccess)
+  // blocks resident at once on the device: class 0 takes `big` SMs' room,
+  // class 1 the rest, per_small blocks in the room of one class-0 block
+  int per_sm = 0, per_small = 0;
+  if (cudaFuncSetAttribute(serve_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)s->smem[0]) != cudaSuccess ||
+      cudaFuncSetAttribute(serve_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)s->smem[1]) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, serve_kernel<true>, SV_BLOCK,
+                                                    s->smem[0]) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_small, serve_kernel<false>, SV_SMALL,
+                                                    s->smem[1]) != cudaSuccess ||
+      per_sm < 1 || per_small < 1)
     return fail(MCE_ECUDA);
-  int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, serve_kernel, SV_BLOCK, s->smem) !=
-          cudaSuccess ||
-      per_sm < 1)
-    return fail(MCE_ECUDA);
-  const uint32_t fit = (uint32_t)(sms * per_sm);  // every slot resident at once
-  s->slots = o.slots > 0 ? std::min((uint32_t)o.slots, fit) : fit;
-  if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess)
-    return fail(MCE_ECUDA);
-  const size_t host_bytes = sizeof(SvHostHdr) + sizeof(SvEntry) * (size_t)o.ring;
-  if (cudaHostAlloc((void **)&s->host, host_bytes, cudaHostAllocMapped) != cudaSuccess)
-    return fail(MCE_ENOMEM);
-  std::memset(s->host, 0, host_bytes);
-  s->hdr = (SvHostHdr *)s->host;
-  s->ent = (SvEntry *)(s->host + sizeof(SvHostHdr));
-  s->taken.assign(o.ring, 0);
-  char *dh = nullptr;
-  if (cudaHostGetDevicePointer((void **)&dh, s->host, 0) != cudaSuccess) return fail(MCE_ECUDA);
+  const uint32_t fit = (uint32_t)(sms * per_sm);
+  s->blocks = o.slots > 0 ? std::min((uint32_t)o.slots, fit) : fit;
+  uint32_t big = s->blocks;
+  if (small_cap && s->blocks >= 2)
+    big = o.big_slots > 0 ? std::min<uint32_t>((uint32_t)o.big_slots, s->blocks - 1)
+                          : (s->blocks + 1) / 2;
+  const uint32_t small_slots =
+      (s->blocks - big) * (uint32_t)std::min(per_small / per_sm, SV_BLOCK / SV_SMALL);
+  if (!small_slots) s->small_cap = 0;  // one class: every request to class 0
+  s->grid[0] = big;
+  s->grid[1] = small_slots;
+  for (int c = 0; c < 2; ++c)
+    if (cudaStreamCreateWithFlags(&s->stream[c], cudaStreamNonBlocking) != cudaSuccess)
+      return fail(MCE_ECUDA);
   ServeArgs &A = s->args;
   A.grp = rp;
   A.gcol = col;
   A.gn = n;
-  A.hdr = (const SvHostHdr *)dh;
-  A.ent = (SvEntry *)(dh + sizeof(SvHostHdr));
-  A.ring = o.ring;
-  A.ego_cap = o.ego_cap;
-  // the table also takes the up to SV_BLOCK - 1 vertices of the chunk
-  // that crosses the cap
-  int hcap = 32;
-  while (hcap < 2 * (o.ego_cap + SV_BLOCK)) hcap <<= 1;
-  A.hcap = hcap;
   const int64_t full = (int64_t)o.ego_cap * (o.ego_cap - 1);
   const int64_t want = o.max_arcs > 0 ? o.max_arcs : (int64_t)o.ego_cap * 128;
-  A.arc_cap = (int32_t)std::max<int64_t>(1, std::min<int64_t>(std::min(full, want), INT32_MAX / 2));
-  A.arena_bytes = arena_layout(A.ego_cap, A.arc_cap, A.hcap, nullptr, nullptr);
+  const int32_t arc0 =
+      (int32_t)std::max<int64_t>(1, std::min<int64_t>(std::min(full, want), INT32_MAX / 2));
+  for (int c = 0; c < 2; ++c) {
+    SvRing &R = s->cls[c];
+    SvClass &C = A.cls[c];
+    std::memset(&C, 0, sizeof(C));
+    if (c == 1 && small_slots == 0) continue;
+    const size_t host_bytes = sizeof(SvHostHdr) + sizeof(SvEntry) * (size_t)o.ring;
+    if (cudaHostAlloc((void **)&R.host, host_bytes, cudaHostAllocMapped) != cudaSuccess)
+      return fail(MCE_ENOMEM);
+    std::memset(R.host, 0, host_bytes);
+    R.hdr = (SvHostHdr *)R.host;
+    R.ent = (SvEntry *)(R.host + sizeof(SvHostHdr));
+    R.taken.assign(o.ring, 0);
+    char *dh = nullptr;
+    if (cudaHostGetDevicePointer((void **)&dh, R.host, 0) != cudaSuccess) return fail(MCE_ECUDA);
+    C.hdr = (const SvHostHdr *)dh;
+    C.ent = (SvEntry *)(dh + sizeof(SvHostHdr));
+    C.ring = o.ring;
+    C.slots = (int32_t)(c == 0 ? big : small_slots);
+    C.ego_cap = c == 0 ? o.ego_cap : small_cap;
+    C.hcap = hash_cap_for(C.ego_cap, c == 0 ? SV_BLOCK : SV_SMALL);
+    // class 1 holds every arc its vertices can have (up to class 0's limit)
+    C.arc_cap = c == 0 ? arc0
+                       : (int32_t)std::max<int64_t>(
+                             1, std::min<int64_t>((int64_t)small_cap * (small_cap - 1), arc0));
+    C.arena_bytes = arena_layout(C.ego_cap, C.arc_cap, C.hcap, nullptr, nullptr);
+    if (cudaMalloc((void **)&R.arena, C.arena_bytes * (size_t)C.slots) != cudaSuccess ||
+        cudaMalloc((void **)&R.ctl, sizeof(SvCtl)) != cudaSuccess ||
+        cudaMemset(R.ctl, 0, sizeof(SvCtl)) != cudaSuccess)
+      return fail(MCE_ENOMEM);
+    C.arena = R.arena;
+    C.ctl = R.ctl;
+  }
   A.reg_words = bk_slab_words(CLS_R64, 0, 0);
-  A.slab_words = A.reg_words + bk_slab_words(CLS_MEM, SV_DCAP, A.ego_cap);
+  A.slab_words = A.reg_words + bk_slab_words(CLS_MEM, SV_DCAP, o.ego_cap);
   A.idle_ns = (uint64_t)o.idle_ms * 1000000ull;
   A.node_budget = (unsigned long long)o.max_nodes;
-  if (cudaMalloc((void **)&s->arena, A.arena_bytes * s->slots) != cudaSuccess ||
-      cudaMalloc((void **)&s->slab, A.slab_words * 8 * (size_t)s->slots * SV_WARPS) !=
-          cudaSuccess ||
-      cudaMalloc((void **)&s->ctl, sizeof(SvCtl)) != cudaSuccess ||
-      cudaMalloc((void **)&s->help, sizeof(SvHelp) * s->slots) != cudaSuccess ||
+  const size_t helps = (size_t)big + small_slots;
+  const size_t warps = (size_t)big * SV_WARPS + (size_t)small_slots * (SV_SMALL / 32);
+  if (cudaMalloc((void **)&s->slab, A.slab_words * 8 * warps) != cudaSuccess ||
+      cudaMalloc((void **)&s->help, sizeof(SvHelp) * helps) != cudaSuccess ||
       cudaMalloc((void **)&s->board, sizeof(uint32_t) * SV_BOARD) != cudaSuccess)
     return fail(MCE_ENOMEM);
-  if (cudaMemset(s->ctl, 0, sizeof(SvCtl)) != cudaSuccess ||
-      cudaMemset(s->help, 0, sizeof(SvHelp) * s->slots) != cudaSuccess ||
+  if (cudaMemset(s->help, 0, sizeof(SvHelp) * helps) != cudaSuccess ||
       cudaMemset(s->board, 0, sizeof(uint32_t) * SV_BOARD) != cudaSuccess)
     return fail(MCE_ECUDA);
   A.help = s->help;
   A.board = s->board;
-  A.arena = s->arena;
-  A.slab = s->slab;
-  A.ctl = s->ctl;
+  A.cls[0].slab = s->slab;
+  A.cls[1].slab = s->slab + A.slab_words * SV_WARPS * (size_t)big;
+  if (small_slots) {  // the footprint bound of every seed, for routing on the host
+    int32_t *db = nullptr;
+    if (cudaMalloc((void **)&db, sizeof(int32_t) * (size_t)std::max<int64_t>(n, 1)) !=
+        cudaSuccess)
+      return fail(MCE_ENOMEM);
+    s->bound.assign((size_t)n, 0);
+    footprint_kernel<<<sms * 8, 256, 0, s->stream[0]>>>(rp, col, n, db);
+    const bool ok = cudaGetLastError() == cudaSuccess &&
+                    cudaMemcpyAsync(s->bound.data(), db, sizeof(int32_t) * (size_t)n,
+                                    cudaMemcpyDeviceToHost, s->stream[0]) == cudaSuccess &&
+                    cudaStreamSynchronize(s->stream[0]) == cudaSuccess;
+    cudaFree(db);
+    if (!ok) return fail(MCE_ECUDA);
+  }
   // the graph's upload (queued on its own stream) completes first
   if (cudaDeviceSynchronize() != cudaSuccess) return fail(MCE_ECUDA);
-  if (sv_launch(s) != MCE_OK) return fail(MCE_ECUDA);
+  for (int c = 0; c < 2; ++c)
+    if (s->grid[c] && sv_launch(s, c) != MCE_OK) return fail(MCE_ECUDA);
   *out = s;
   return MCE_OK;
 }
@@ -959,28 +1195,39 @@ extern "C" int mce_serve_open(mce_graph_t g, const mce_serve_opts_t *opts, mce_s
 extern "C" int mce_serve_submit(mce_serve_t s, int64_t seed, uint64_t *id_out) {
   if (!s || !id_out) return MCE_EINVAL;
   if (s->closed) return MCE_ESTATE;
-  sv_retire(s);
-  if (s->tail - s->low >= s->ring) return MCE_ELIMIT;  // ring full: take answers first
-  if (s->tail >= 0x3FFFFFF0u) return MCE_ELIMIT;       // ids exhausted (below SV_HELP)
-  const uint32_t id = s->tail;
-  SvEntry &e = s->ent[id % s->ring];
+  // admission by footprint: a seed whose 2-hop bound fits the class-1 cap
+  // goes to the 256-thread slots once every whole-block slot has a request
+  // (below that load a whole block answers it sooner); any other seed to the
+  // whole-block slots
+  const bool fits = s->small_cap && seed >= 0 && seed < (int64_t)s->bound.size() &&
+                    (int64_t)s->bound[(size_t)seed] + 1 <= s->small_cap;
+  const int c = fits && s->cls[0].open >= s->grid[0] ? 1 : 0;
+  SvRing &R = s->cls[c];
+  sv_retire(s, c);
+  if (R.tail - R.low >= s->ring) return MCE_ELIMIT;  // ring full: take answers first
+  if (R.tail >= 0x3FFFFFF0u) return MCE_ELIMIT;      // ids exhausted (below SV_HELP)
+  const uint32_t id = R.tail;
+  SvEntry &e = R.ent[id % s->ring];
   e.seed = seed;
   __atomic_store_n(&e.done, 0u, __ATOMIC_RELAXED);
-  s->tail = id + 1;
-  __atomic_store_n(&s->hdr->tail, s->tail, __ATOMIC_RELEASE);
-  *id_out = id;
+  R.tail = id + 1;
+  ++R.open;
+  __atomic_store_n(&R.hdr->tail, R.tail, __ATOMIC_RELEASE);
+  *id_out = ((uint64_t)id << 1) | (uint64_t)c;
   return sv_ensure_running(s);
 }
 
 extern "C" int mce_serve_poll(mce_serve_t s, uint64_t id, mce_serve_result_t *res) {
   if (!s || !res) return MCE_EINVAL;
-  if (id >= s->tail || id < s->low || s->taken[id % s->ring]) return MCE_EINVAL;
-  const uint32_t i = (uint32_t)id;
-  if (!sv_done(s, i)) {
+  const int c = id_cls(id);
+  const uint32_t i = id_local(id);
+  SvRing &R = s->cls[c];
+  if (!R.host || i >= R.tail || i < R.low || R.taken[i % s->ring]) return MCE_EINVAL;
+  if (!sv_done(s, c, i)) {
     const int rc = s->closed ? MCE_OK : sv_ensure_running(s);
     return rc != MCE_OK ? rc : MCE_EAGAIN;
   }
-  const SvEntry &e = s->ent[i % s->ring];
+  const SvEntry &e = R.ent[i % s->ring];
   res->count = e.count;
   res->seed = e.seed;
   res->status = e.status;
@@ -991,8 +1238,9 @@ extern "C" int mce_serve_poll(mce_serve_t s, uint64_t id, mce_serve_result_t *re
   res->extract_ns = e.extract_ns;
   res->order_ns = e.order_ns;
   res->search_ns = e.search_ns;
-  s->taken[i % s->ring] = 1;
-  sv_retire(s);
+  R.taken[i % s->ring] = 1;
+  --R.open;
+  sv_retire(s, c);
   return MCE_OK;
 }
 
@@ -1020,7 +1268,7 @@ extern "C" int mce_serve_run(mce_serve_t s, const int64_t *seeds, const double *
   auto now_us = [&]() { return std::chrono::duration<double, std::micro>(clk::now() - t0).count(); };
   std::vector<uint64_t> ids((size_t)count);
   std::vector<int64_t> open;  // submitted, answer not yet taken
-  open.reserve(s->ring);
+  open.reserve(2 * s->ring);
   int64_t next = 0, finished = 0;
   while (finished < count) {
     const double t = now_us();
@@ -1053,19 +1301,28 @@ extern "C" int mce_serve_run(mce_serve_t s, const int64_t *seeds, const double *
 
 extern "C" int mce_serve_stats(mce_serve_t s, mce_serve_stats_t *st) {
   if (!s || !st) return MCE_EINVAL;
-  SvCtl c;
-  MCE_CUDA(cudaMemcpy(&c, s->ctl, sizeof(c), cudaMemcpyDeviceToHost));
   std::memset(st, 0, sizeof(*st));
-  st->slots = (int32_t)s->slots;
+  for (int c = 0; c < 2; ++c) {
+    const SvRing &R = s->cls[c];
+    if (!R.ctl) continue;
+    SvCtl ct;
+    MCE_CUDA(cudaMemcpy(&ct, R.ctl, sizeof(ct), cudaMemcpyDeviceToHost));
+    st->submitted += R.tail;
+    st->served += ct.served;
+    st->tree_nodes += ct.nodes;
+    st->helps += ct.helped;
+    st->arena_bytes += (uint64_t)s->args.cls[c].arena_bytes * (uint64_t)s->args.cls[c].slots;
+    if (c == 0) st->peak_in_flight = ct.peak;
+  }
+  st->slots = s->args.cls[0].slots + s->args.cls[1].slots;
+  st->small_slots = s->args.cls[1].slots;
+  st->small_cap = s->small_cap;
   st->ring = s->ring;
-  st->submitted = s->tail;
-  st->served = c.served;
-  st->tree_nodes = c.nodes;
   st->kernel_launches = s->launches;
-  st->arena_bytes = (uint64_t)s->args.arena_bytes * s->slots;
-  st->slab_bytes = (uint64_t)s->args.slab_words * 8 * s->slots * SV_WARPS;
-  st->helps = c.helped;
-  st->running = cudaStreamQuery(s->stream) == cudaErrorNotReady ? 1 : 0;
+  st->slab_bytes = (uint64_t)s->args.slab_words * 8 *
+                   ((uint64_t)s->grid[0] * SV_WARPS + (uint64_t)s->grid[1] * (SV_SMALL / 32));
+  for (cudaStream_t q : s->stream)
+    if (q && cudaStreamQuery(q) == cudaErrorNotReady) st->running = 1;
   return MCE_OK;
 }
 
@@ -1073,21 +1330,30 @@ extern "C" int mce_serve_close(mce_serve_t s) {
   if (!s) return MCE_EINVAL;
   if (!s->closed) {
     s->closed = true;
-    __atomic_store_n(&s->hdr->stop, 1u, __ATOMIC_RELEASE);
+    for (SvRing &R : s->cls)
+      if (R.hdr) __atomic_store_n(&R.hdr->stop, 1u, __ATOMIC_RELEASE);
   }
   // Every slot finishes its request and leaves once nothing is published.
   // A request published just as the last slot left idle is served by one
-  // more launch (which sees the stop flag and leaves when done).
+  // more launch (which sees the stop flags and leaves when done).
   int rc = MCE_OK;
   for (int pass = 0; pass < 3 && rc == MCE_OK; ++pass) {
-    if (cudaStreamSynchronize(s->stream) != cudaSuccess) {
-      rc = MCE_ECUDA;
-      break;
+    for (cudaStream_t q : s->stream)
+      if (q && cudaStreamSynchronize(q) != cudaSuccess) rc = MCE_ECUDA;
+    if (rc != MCE_OK) break;
+    bool pending = false;
+    for (int c = 0; c < 2 && rc == MCE_OK; ++c) {
+      const SvRing &R = s->cls[c];
+      if (!R.ctl) continue;
+      SvCtl ct;
+      if (cudaMemcpy(&ct, R.ctl, sizeof(ct), cudaMemcpyDeviceToHost) != cudaSuccess) {
+        rc = MCE_ECUDA;
+      } else if (ct.next < R.tail) {
+        pending = true;
+        rc = sv_launch(s, c);
+      }
     }
-    SvCtl c;
-    if (cudaMemcpy(&c, s->ctl, sizeof(c), cudaMemcpyDeviceToHost) != cudaSuccess) rc = MCE_ECUDA;
-    if (rc != MCE_OK || c.next >= s->tail) break;
-    rc = sv_launch(s);
+    if (!pending) break;
   }
   sv_free(s);
   return rc;

@@ -100,7 +100,8 @@ def _opts_kwargs(o: "_Opts") -> dict:
 class _ServeOpts(C.Structure):
     _fields_ = [("ego_cap", C.c_int32), ("slots", C.c_int32), ("ring", C.c_uint32),
                 ("idle_ms", C.c_int32), ("max_arcs", C.c_int64), ("max_nodes", C.c_int64),
-                ("reserved", C.c_int64 * 3)]
+                ("small_cap", C.c_int32), ("big_slots", C.c_int32),
+                ("reserved", C.c_int64 * 2)]
 
 
 class _ServeResult(C.Structure):
@@ -114,7 +115,9 @@ class _ServeStats(C.Structure):
     _fields_ = [("slots", C.c_int32), ("running", C.c_int32), ("ring", C.c_uint32),
                 ("pad", C.c_uint32), ("submitted", C.c_uint64), ("served", C.c_uint64),
                 ("tree_nodes", C.c_uint64), ("kernel_launches", C.c_int64),
-                ("arena_bytes", C.c_uint64), ("slab_bytes", C.c_uint64), ("helps", C.c_uint64)]
+                ("arena_bytes", C.c_uint64), ("slab_bytes", C.c_uint64), ("helps", C.c_uint64),
+                ("small_slots", C.c_int32), ("small_cap", C.c_int32),
+                ("peak_in_flight", C.c_uint64)]
 
 
 _P = C.c_void_p
@@ -737,14 +740,20 @@ class Serve:
 
     Each request is a seed vertex; its answer is the maximal-clique count of
     the seed's 2-hop ego subgraph (ego_subgraph(host_graph, seed, ego_cap)).
+    small_cap (None: automatic) routes the requests whose footprint bound
+    fits it to 256-thread slots, four per block; big_slots whole-block slots
+    take the others (0: half the blocks).  Request ids carry their class in
+    bit 0.
     """
 
     def __init__(self, g: Graph, *, ego_cap=1024, slots=0, ring=4096, idle_ms=1000, max_arcs=0,
-                 max_nodes=0):
+                 max_nodes=0, small_cap=None, big_slots=0):
         o = _ServeOpts()
         _lib.mce_serve_opts_default(C.byref(o))
         o.ego_cap, o.slots, o.ring, o.idle_ms = ego_cap, slots, ring, idle_ms
         o.max_arcs, o.max_nodes = max_arcs, max_nodes
+        o.small_cap = -1 if small_cap is None else small_cap
+        o.big_slots = big_slots
         self._h = C.c_void_p()
         self.graph = g  # the session reads the graph's device arrays
         _check(_lib.mce_serve_open(g._h, C.byref(o), C.byref(self._h)), "serve_open")

@@ -181,11 +181,12 @@ typedef struct {
   int32_t *xx;     /* maxu         : earlier neighbours of the root (Xx)   */
   int32_t *xaux;   /* maxu                                                  */
   int64_t *xsz;    /* (maxd+3)     : |Xx| at each level                    */
+  uint64_t *xo;    /* (maxd+2) x W : L2 outside rows of the root's later nbrs */
 } bk_ws;
 
 static void ws_free(bk_ws *w) {
   free(w->enc); free(w->pl); free(w->cl); free(w->xl); free(w->ptr);
-  free(w->cnode); free(w->xx); free(w->xaux); free(w->xsz);
+  free(w->cnode); free(w->xx); free(w->xaux); free(w->xsz); free(w->xo);
 }
 
 static int ws_alloc(bk_ws *w, int64_t maxd, int64_t maxu) {
@@ -204,24 +205,150 @@ static int ws_alloc(bk_ws *w, int64_t maxd, int64_t maxu) {
   w->xx = (int32_t *)calloc((size_t)(maxu ? maxu : 1), 4);
   w->xaux = (int32_t *)calloc((size_t)(maxu ? maxu : 1), 4);
   w->xsz = (int64_t *)calloc(L + 1, 8);
+  w->xo = (uint64_t *)calloc(L * w->W, 8);
   if (!w->enc || !w->pl || !w->cl || !w->xl || !w->ptr || !w->cnode || !w->xx || !w->xaux ||
-      !w->xsz) {
+      !w->xsz || !w->xo) {
     ws_free(w);
     return ORACLE_ENOMEM;
   }
   return ORACLE_OK;
 }
 
-/* Count the maximal cliques whose first vertex in the order is r. */
-/* *ops_out: the walk's algorithmic 32-bit word operations, W32 =
+/* The walk below level 0 of one search tree (L1: the root's; L2: a unit's),
+   the reference's state machine of mce/mce_kernel_nowl.cuh:9-109 over the
+   bitmaps of the workspace.  Level 0 (pl, cl, xl, ptr, xx/xsz, and for L2
+   the outside rows xo) is set up by the caller.  base = the clique's size
+   before level 0's branch (1: the root; 2: root and L2 edge). */
+static void bk_walk(bk_ws *w, int64_t d, int64_t W, uint64_t W32, const int32_t *row_ptr,
+                    const int32_t *split, const int32_t *cs, int64_t sb, int64_t ub, int l2,
+                    int64_t base, uint64_t *hist, int hist_len, uint64_t *cnt, uint64_t *nodes,
+                    uint64_t *ops) {
+  uint64_t *enc = w->enc, *pl = w->pl, *cl = w->cl, *xl = w->xl, *xo = w->xo;
+  uint64_t *tcl = (uint64_t *)alloca(sizeof(uint64_t) * (size_t)W);
+  uint64_t *txl = (uint64_t *)alloca(sizeof(uint64_t) * (size_t)W);
+  uint64_t *txo = (uint64_t *)alloca(sizeof(uint64_t) * (size_t)W);
+  int64_t l = 0; /* level index (the reference's l - 2) */
+  while (l >= 0) {
+    /* get_next_candidate (mce/mce_utils.cuh:526-563): next set bit of the
+       level's branch set at or after ptr[l]; none left -> backtrack. */
+    int64_t v = -1;
+    for (int64_t b = w->ptr[l]; b < d;) {
+      const uint64_t word = pl[l * W + b / 64] & (~0ull << (b % 64));
+      if (word) {
+        v = (b / 64) * 64 + __builtin_ctzll(word);
+        break;
+      }
+      b = (b / 64 + 1) * 64;
+    }
+    if (v < 0 || v >= d) {
+      --l;
+      continue;
+    }
+    ++*nodes;
+    w->ptr[l] = v + 1; /* clean_level_L1_IP (:786-805) */
+    const int32_t cn = cs[sb + v];
+    /* Xx_compaction_for_IP (mce/mce_utils.cuh:265-292): the root's earlier
+       neighbours adjacent to the chosen vertex (binary search in its
+       earlier list) move to the front; their count is the next level's |Xx|. */
+    {
+      const int64_t lim = w->xsz[l];
+      int64_t f = 0, b2 = lim;
+      const int64_t cb = row_ptr[cn], ce = split[cn];
+      for (int64_t k = 0; k < lim; ++k) {
+        const int32_t cur = w->xx[k];
+        if (bsearch_i32(cs, cb, ce, cs[ub + cur]))
+          w->xaux[f++] = cur;
+        else
+          w->xaux[--b2] = cur;
+      }
+      memcpy(w->xx, w->xaux, sizeof(int32_t) * (size_t)lim);
+      w->xsz[l + 1] = f;
+    }
+    /* populate_xl_and_cl (mce/mce_utils.cuh:321-336): branch bits before v
+       move from P to X; child P' = P & N(v), X' = X & N(v); L2's outside
+       rows of the root's later neighbours keep those adjacent to v. */
+    int64_t curSZ = 0;
+    int xo_any = 0;
+    for (int64_t k = 0; k < W; ++k) {
+      uint64_t before;
+      if (k < v / 64)
+        before = ~0ull;
+      else if (k > v / 64)
+        before = 0;
+      else
+        before = (1ull << (v % 64)) - 1;
+      const uint64_t done = pl[l * W + k] & before;
+      txl[k] = (xl[l * W + k] | done) & enc[v * W + k];
+      tcl[k] = (cl[l * W + k] & ~done) & enc[v * W + k];
+      txo[k] = l2 ? (xo[l * W + k] & enc[v * W + k]) : 0;
+      xo_any |= txo[k] != 0;
+      curSZ += popc64(tcl[k]);
+    }
+    /* select_pivot_from_P_and_Xp (mce/mce_utils.cuh:366-402): pivot over
+       P' u X'; an X' vertex adjacent to all of P' eliminates the path. */
+    int more = 0, elim = 0;
+    int64_t pv = -1, pbest = -1, cand = 0;
+    for (int64_t j = 0; j < d; ++j) {
+      const uint64_t bit = 1ull << (j % 64);
+      const int inP = (tcl[j / 64] & bit) != 0, inX = (txl[j / 64] & bit) != 0;
+      if (!inP && !inX) continue;
+      ++cand;
+      int64_t c = 0;
+      for (int64_t k = 0; k < W; ++k) c += popc64(tcl[k] & enc[j * W + k]);
+      if (c == curSZ) elim = 1; /* only possible for j in X' */
+      more = 1;
+      if (c > pbest) {
+        pbest = c;
+        pv = j;
+      }
+    }
+    *ops += 2 * W32 * (uint64_t)cand + 4 * W32;
+    if (!more || elim) {
+      /* test_maximality (mce/mce_utils.cuh:507-524) */
+      if (w->xsz[l + 1] == 0 && !xo_any) {
+        int xe = 1;
+        for (int64_t k = 0; k < W; ++k) xe &= (txl[k] == 0);
+        if (xe && curSZ == 0) {
+          ++*cnt;
+          const int64_t size = base + l + 1; /* one vertex per level */
+          if (hist && size < hist_len) hist[size]++;
+        }
+      }
+      continue;
+    }
+    /* apply_pivot_to_next_level (mce/mce_utils.cuh:218-239) + go_to_next_level */
+    for (int64_t k = 0; k < W; ++k) {
+      pl[(l + 1) * W + k] = ~enc[pv * W + k] & tcl[k];
+      cl[(l + 1) * W + k] = tcl[k];
+      xl[(l + 1) * W + k] = txl[k];
+      if (l2) xo[(l + 1) * W + k] = txo[k];
+    }
+    w->ptr[l + 1] = 0;
+    ++l;
+  }
+}
+
+/* Count the maximal cliques whose first vertex in the order is r.
+   *ops_out: the walk's algorithmic 32-bit word operations, W32 =
    ceil(d / 32) words per row: 2 W32 per row scored by a pivot selection
    (AND + POPC; the root's over all d rows, select_pivot_from_P,
    mce/mce_utils.cuh:338-364, a node's over P' | X',
    select_pivot_from_P_and_Xp, :366-402) and 4 W32 per node for the child
-   sets (populate_xl_and_cl, :321-336). */
+   sets (populate_xl_and_cl, :321-336).
+
+   l2prio != NULL: the L2 scheme (mce/mce_kernel_wl.cuh:307-485 with
+   setup_stack_original_L2_IP, mce/mce_utils.cuh:664-712): every oriented
+   edge (r, v), v a later neighbour, is a unit whose candidates are the
+   triangle list P = N+(r) & N+(v) (block_count_and_set_tri, :151-171) and
+   whose outside list holds the neighbours of r earlier than v and adjacent
+   to it (the reference's Xx over r's whole row); an empty P counts the edge
+   when that list is empty; otherwise the unit's pivot is taken from P alone
+   and the walk below is the L1 one.  Units are not tree nodes (the
+   reference's traversed_nodes counts branches inside a unit,
+   mce/mce_kernel_wl_lb.cuh:445). */
 static void root_search(bk_ws *w, int32_t r, const int32_t *row_ptr, const int32_t *split,
                         const int32_t *cs, uint64_t *hist, int hist_len, uint64_t *cnt_out,
-                        uint64_t *nodes_out, uint64_t *ops_out) {
+                        uint64_t *nodes_out, uint64_t *ops_out, const uint32_t *l2prio) {
   const int64_t sb = split[r], d = row_ptr[r + 1] - sb; /* later neighbours: P */
   const int64_t ub = row_ptr[r], u = sb - ub;          /* earlier neighbours: Xx */
   uint64_t cnt = 0, nodes = 0, ops = 0;
@@ -244,130 +371,83 @@ static void root_search(bk_ws *w, int32_t r, const int32_t *row_ptr, const int32
         enc[i * W + j / 64] |= 1ull << (j % 64);
       }
   }
-  /* setup_stack_original_L1_IP (mce/mce_utils.cuh:565-611): Xx = all
-     earlier neighbours, level 0 holds P = all of N+(r), X = 0. */
-  for (int64_t k = 0; k < u; ++k) w->xx[k] = (int32_t)k;
-  w->xsz[0] = u;
-  uint64_t *pl = w->pl, *cl = w->cl, *xl = w->xl;
+  uint64_t *pl = w->pl, *cl = w->cl, *xl = w->xl, *xo = w->xo;
   const uint64_t lastmask = (d % 64) ? ((1ull << (d % 64)) - 1) : ~0ull;
-  /* select_pivot_from_P (mce/mce_utils.cuh:338-364): the row with the most
-     bits; finalize_pivot (:191-202).  Ties: the first row. */
-  int64_t piv = 0, best = -1;
-  ops += 2 * W32 * (uint64_t)d;
-  for (int64_t j = 0; j < d; ++j) {
-    int64_t c = 0;
-    for (int64_t k = 0; k < W; ++k) c += popc64(enc[j * W + k]);
-    if (c > best) {
-      best = c;
-      piv = j;
-    }
-  }
-  /* apply_pivot_to_first_level (mce/mce_utils.cuh:204-216) */
-  for (int64_t k = 0; k < W; ++k) {
-    const uint64_t m = (k == W - 1) ? lastmask : ~0ull;
-    pl[k] = ~enc[piv * W + k] & m;
-    cl[k] = m;
-    xl[k] = 0;
-  }
-  w->ptr[0] = 0;
-  int64_t l = 0; /* level index (the reference's l - 2) */
-  uint64_t *tcl = (uint64_t *)alloca(sizeof(uint64_t) * (size_t)W);
-  uint64_t *txl = (uint64_t *)alloca(sizeof(uint64_t) * (size_t)W);
-  while (l >= 0) {
-    /* get_next_candidate (mce/mce_utils.cuh:526-563): next set bit of the
-       level's branch set at or after ptr[l]; none left -> backtrack. */
-    int64_t v = -1;
-    for (int64_t b = w->ptr[l]; b < d;) {
-      const uint64_t word = pl[l * W + b / 64] & (~0ull << (b % 64));
-      if (word) {
-        v = (b / 64) * 64 + __builtin_ctzll(word);
-        break;
-      }
-      b = (b / 64 + 1) * 64;
-    }
-    if (v < 0 || v >= d) {
-      --l;
-      continue;
-    }
-    ++nodes;
-    w->ptr[l] = v + 1; /* clean_level_L1_IP (:786-805) */
-    const int32_t cn = cs[sb + v];
-    /* Xx_compaction_for_IP (mce/mce_utils.cuh:265-292): the root's earlier
-       neighbours adjacent to the chosen vertex (binary search in its
-       earlier list) move to the front; their count is the next level's |Xx|. */
-    {
-      const int64_t lim = w->xsz[l];
-      int64_t f = 0, b2 = lim;
-      const int64_t cb = row_ptr[cn], ce = split[cn];
-      for (int64_t k = 0; k < lim; ++k) {
-        const int32_t cur = w->xx[k];
-        if (bsearch_i32(cs, cb, ce, cs[ub + cur]))
-          w->xaux[f++] = cur;
-        else
-          w->xaux[--b2] = cur;
-      }
-      memcpy(w->xx, w->xaux, sizeof(int32_t) * (size_t)lim);
-      w->xsz[l + 1] = f;
-    }
-    /* populate_xl_and_cl (mce/mce_utils.cuh:321-336): branch bits before v
-       move from P to X; child P' = P & N(v), X' = X & N(v). */
-    int64_t curSZ = 0;
-    for (int64_t k = 0; k < W; ++k) {
-      uint64_t before;
-      if (k < v / 64)
-        before = ~0ull;
-      else if (k > v / 64)
-        before = 0;
-      else
-        before = (1ull << (v % 64)) - 1;
-      const uint64_t done = pl[l * W + k] & before;
-      txl[k] = (xl[l * W + k] | done) & enc[v * W + k];
-      tcl[k] = (cl[l * W + k] & ~done) & enc[v * W + k];
-      curSZ += popc64(tcl[k]);
-    }
-    {
-      int64_t cand = 0;
-      for (int64_t k = 0; k < W; ++k) cand += popc64(tcl[k] | txl[k]);
-      ops += 2 * W32 * (uint64_t)cand + 4 * W32;
-    }
-    /* select_pivot_from_P_and_Xp (mce/mce_utils.cuh:366-402): pivot over
-       P' u X'; an X' vertex adjacent to all of P' eliminates the path. */
-    int more = 0, elim = 0;
-    int64_t pv = -1, pbest = -1;
+  if (!l2prio) {
+    /* setup_stack_original_L1_IP (mce/mce_utils.cuh:565-611): Xx = all
+       earlier neighbours, level 0 holds P = all of N+(r), X = 0;
+       select_pivot_from_P (:338-364): the row with the most bits,
+       finalize_pivot (:191-202), ties: the first row;
+       apply_pivot_to_first_level (:204-216). */
+    for (int64_t k = 0; k < u; ++k) w->xx[k] = (int32_t)k;
+    w->xsz[0] = u;
+    int64_t piv = 0, best = -1;
+    ops += 2 * W32 * (uint64_t)d;
     for (int64_t j = 0; j < d; ++j) {
-      const uint64_t bit = 1ull << (j % 64);
-      const int inP = (tcl[j / 64] & bit) != 0, inX = (txl[j / 64] & bit) != 0;
-      if (!inP && !inX) continue;
       int64_t c = 0;
-      for (int64_t k = 0; k < W; ++k) c += popc64(tcl[k] & enc[j * W + k]);
-      if (c == curSZ) elim = 1; /* only possible for j in X' */
-      more = 1;
-      if (c > pbest) {
-        pbest = c;
-        pv = j;
+      for (int64_t k = 0; k < W; ++k) c += popc64(enc[j * W + k]);
+      if (c > best) {
+        best = c;
+        piv = j;
       }
     }
-    if (!more || elim) {
-      /* test_maximality (mce/mce_utils.cuh:507-524) */
-      if (w->xsz[l + 1] == 0) {
-        int xe = 1;
-        for (int64_t k = 0; k < W; ++k) xe &= (txl[k] == 0);
-        if (xe && curSZ == 0) {
-          ++cnt;
-          const int64_t size = l + 2; /* root + one vertex per level */
-          if (hist && size < hist_len) hist[size]++;
+    for (int64_t k = 0; k < W; ++k) {
+      const uint64_t m = (k == W - 1) ? lastmask : ~0ull;
+      pl[k] = ~enc[piv * W + k] & m;
+      cl[k] = m;
+      xl[k] = 0;
+    }
+    w->ptr[0] = 0;
+    bk_walk(w, d, W, W32, row_ptr, split, cs, sb, ub, 0, 1, hist, hist_len, &cnt, &nodes, &ops);
+  } else {
+    for (int64_t vj = 0; vj < d; ++vj) { /* unit (r, v) */
+      const int32_t v = cs[sb + vj];
+      const uint32_t pv = l2prio[v];
+      /* the triangle list (later than v) and r's later neighbours earlier
+         than v and adjacent to it (outside rows) */
+      int tri_any = 0, xo_any = 0;
+      for (int64_t k = 0; k < W; ++k) pl[k] = cl[k] = xl[k] = xo[k] = 0;
+      for (int64_t j = 0; j < d; ++j) {
+        if (!(enc[vj * W + j / 64] >> (j % 64) & 1ull)) continue;
+        const int32_t x = cs[sb + j];
+        const uint32_t px = l2prio[x];
+        const int later = px == pv ? v < x : pv < px; /* include/main_support.cuh:14 */
+        if (later) {
+          cl[j / 64] |= 1ull << (j % 64);
+          tri_any = 1;
+        } else {
+          xo[j / 64] |= 1ull << (j % 64);
+          xo_any = 1;
         }
       }
-      continue;
+      /* the root's earlier neighbours adjacent to v (earlier than v too) */
+      int64_t f = 0;
+      const int64_t cb = row_ptr[v], ce = split[v];
+      for (int64_t k = 0; k < u; ++k)
+        if (bsearch_i32(cs, cb, ce, cs[ub + k])) w->xx[f++] = (int32_t)k;
+      w->xsz[0] = f;
+      if (!tri_any) { /* the edge alone: maximal unless its outside list is not empty */
+        if (f == 0 && !xo_any) {
+          ++cnt;
+          if (hist && 2 < hist_len) hist[2]++;
+        }
+        continue;
+      }
+      /* select_pivot_from_P over the triangle list alone */
+      int64_t piv = -1, best = -1;
+      for (int64_t j = 0; j < d; ++j) {
+        if (!(cl[j / 64] >> (j % 64) & 1ull)) continue;
+        int64_t c = 0;
+        for (int64_t k = 0; k < W; ++k) c += popc64(cl[k] & enc[j * W + k]);
+        if (c > best) {
+          best = c;
+          piv = j;
+        }
+      }
+      for (int64_t k = 0; k < W; ++k) pl[k] = cl[k] & ~enc[piv * W + k];
+      w->ptr[0] = 0;
+      bk_walk(w, d, W, W32, row_ptr, split, cs, sb, ub, 1, 2, hist, hist_len, &cnt, &nodes, &ops);
     }
-    /* apply_pivot_to_next_level (mce/mce_utils.cuh:218-239) + go_to_next_level */
-    for (int64_t k = 0; k < W; ++k) {
-      pl[(l + 1) * W + k] = ~enc[pv * W + k] & tcl[k];
-      cl[(l + 1) * W + k] = tcl[k];
-      xl[(l + 1) * W + k] = txl[k];
-    }
-    w->ptr[l + 1] = 0;
-    ++l;
   }
   *cnt_out = cnt;
   *nodes_out = nodes;
@@ -379,10 +459,10 @@ static void root_search(bk_ws *w, int32_t r, const int32_t *row_ptr, const int32
  * total: maximal cliques found; hist (nullable, hist_len entries) by size;
  * root_count / root_nodes / root_ops (nullable, n entries) per root.
  */
-int oracle_mce_ops(int64_t n, const int32_t *row_ptr, const int32_t *split, const int32_t *cs,
-                   int64_t begin, int64_t end, int64_t stride, int nthreads, uint64_t *total,
-                   uint64_t *hist, int hist_len, uint64_t *root_count, uint64_t *root_nodes,
-                   uint64_t *root_ops) {
+static int mce_roots(int64_t n, const int32_t *row_ptr, const int32_t *split, const int32_t *cs,
+                     int64_t begin, int64_t end, int64_t stride, int nthreads, uint64_t *total,
+                     uint64_t *hist, int hist_len, uint64_t *root_count, uint64_t *root_nodes,
+                     uint64_t *root_ops, const uint32_t *l2prio) {
   if (n < 0 || stride < 1 || !total || (n > 0 && (!row_ptr || !split || !cs)))
     return ORACLE_EINVAL;
   if (end > n) end = n;
@@ -411,7 +491,7 @@ int oracle_mce_ops(int64_t n, const int32_t *row_ptr, const int32_t *split, cons
     for (int64_t r = begin; r < end; r += stride) {
       if (!ok) continue;
       uint64_t c, nd, op;
-      root_search(&w, (int32_t)r, row_ptr, split, cs, lh, hist_len, &c, &nd, &op);
+      root_search(&w, (int32_t)r, row_ptr, split, cs, lh, hist_len, &c, &nd, &op, l2prio);
       tot += c;
       if (root_count) root_count[r] = c;
       if (root_nodes) root_nodes[r] = nd;
@@ -431,11 +511,28 @@ int oracle_mce_ops(int64_t n, const int32_t *row_ptr, const int32_t *split, cons
   return ORACLE_OK;
 }
 
+int oracle_mce_ops(int64_t n, const int32_t *row_ptr, const int32_t *split, const int32_t *cs,
+                   int64_t begin, int64_t end, int64_t stride, int nthreads, uint64_t *total,
+                   uint64_t *hist, int hist_len, uint64_t *root_count, uint64_t *root_nodes,
+                   uint64_t *root_ops) {
+  return mce_roots(n, row_ptr, split, cs, begin, end, stride, nthreads, total, hist, hist_len,
+                   root_count, root_nodes, root_ops, NULL);
+}
+
 int oracle_mce(int64_t n, const int32_t *row_ptr, const int32_t *split, const int32_t *cs,
                int64_t begin, int64_t end, int64_t stride, int nthreads, uint64_t *total,
                uint64_t *hist, int hist_len, uint64_t *root_count, uint64_t *root_nodes) {
-  return oracle_mce_ops(n, row_ptr, split, cs, begin, end, stride, nthreads, total, hist,
-                        hist_len, root_count, root_nodes, NULL);
+  return mce_roots(n, row_ptr, split, cs, begin, end, stride, nthreads, total, hist, hist_len,
+                   root_count, root_nodes, NULL, NULL);
+}
+
+/* The L2 (edge-rooted) scheme over every root; prio = the peel's priorities. */
+int oracle_mce_l2(int64_t n, const int32_t *row_ptr, const int32_t *split, const int32_t *cs,
+                  const uint32_t *prio, int nthreads, uint64_t *total, uint64_t *hist,
+                  int hist_len, uint64_t *root_count, uint64_t *root_nodes) {
+  if (!prio && n > 0) return ORACLE_EINVAL;
+  return mce_roots(n, row_ptr, split, cs, 0, n, 1, nthreads, total, hist, hist_len, root_count,
+                   root_nodes, NULL, prio);
 }
 
 /* Peel + orient + search in one call (all roots). */

@@ -13,6 +13,11 @@ Each graph is given by the generator call that makes it, so the tests can
 rebuild it without storing the graph.  The reference runs with
 `-p l1 -i p -w nowl`: the worker-list kernels spin until every block of a
 full-GPU grid is resident, which a shared GPU does not guarantee.
+
+It also runs `-m mce-lb-eval -p l1` and `-p l2` (no worker list) and sums
+the per-block "Number of traversed nodes" lines: the search-tree sizes of
+the L1 and the edge-rooted L2 schemes, which pin the oracle's trees, not
+only its counts (the count does not depend on the scheme).
 """
 import json
 import os
@@ -64,6 +69,18 @@ def run_reference(bel):
     return int(found[0].replace(",", "")), int(core[0])
 
 
+def run_lb(bel, level):
+    """Total traversed nodes of the reference's -m mce-lb-eval run."""
+    r = subprocess.run([REF, "-m", "mce-lb-eval", "-g", bel, "-d", "0", "-p", level, "-i", "p",
+                        "-w", "nowl"], capture_output=True, text=True, timeout=600)
+    out = re.sub(r"\x1b\[[0-9;]*m", "", r.stdout)
+    if r.returncode != 0 or "Number of traversed nodes" not in out:
+        raise RuntimeError(f"reference lb-eval failed on {bel}: rc={r.returncode}")
+    body = out.split("Number of traversed nodes", 1)[1]
+    return sum(int(m.group(1)) for m in re.finditer(r"^\s*\d+,\s*\d+,\s*(\d+)\s*$", body,
+                                                   re.M))
+
+
 def main():
     out = {}
     tmp = tempfile.mkdtemp(prefix="golden_")
@@ -72,13 +89,17 @@ def main():
         bel = os.path.join(tmp, name + ".bel")
         mce.bel_write(bel, g)
         count, core = run_reference(bel)
+        nodes_l1, nodes_l2 = run_lb(bel, "l1"), run_lb(bel, "l2")
         os.remove(bel)
         out[name] = {"generator": GRAPHS[name][0], "args": GRAPHS[name][1], "n": int(g.n),
-                     "arcs": int(g.m), "reference_count": count, "reference_max_core": core}
-        print(name, count, core, flush=True)
+                     "arcs": int(g.m), "reference_count": count, "reference_max_core": core,
+                     "reference_tree_nodes_l1": nodes_l1, "reference_tree_nodes_l2": nodes_l2}
+        print(name, count, core, nodes_l1, nodes_l2, flush=True)
     dst = sys.argv[1] if len(sys.argv) > 1 else os.path.join(HERE, "reference_counts.json")
     with open(dst, "w") as f:
-        json.dump({"source": "reference binary (oracle/_ref) -m mce -p l1 -i p -w nowl on a B200",
+        json.dump({"source": "reference binary (oracle/_ref) on a B200: -m mce -p l1 -i p -w nowl "
+                             "(count, max core); -m mce-lb-eval -p l1|l2 -i p -w nowl (traversed "
+                             "nodes summed over blocks)",
                    "graphs": out}, f, indent=1)
 
 

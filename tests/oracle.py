@@ -98,6 +98,25 @@ def roots_ops(g, threads=0, prepared=None):
     return tot.value, rc[:g.n], rn[:g.n], ro[:g.n]
 
 
+_o.oracle_mce_l2.argtypes = [C.c_int64, _P, _P, _P, _P, C.c_int, _P, _P, C.c_int, _P, _P]
+
+
+def roots_l2(g, threads=0):
+    """Per-root (count, nodes) of the L2 (edge-rooted) scheme and the total:
+    no pivot at the root, first-level branches in the degeneracy order."""
+    prio, _, _ = peel(g)
+    split, cs = orient(g, prio)
+    rp, _ = _csr(g)
+    pr = np.ascontiguousarray(prio, dtype=np.uint32)
+    rc = np.zeros(max(g.n, 1), np.uint64)
+    rn = np.zeros(max(g.n, 1), np.uint64)
+    tot = C.c_uint64()
+    hist = np.zeros(HIST, np.uint64)
+    assert _o.oracle_mce_l2(g.n, _p(rp), _p(split), _p(cs), _p(pr), threads, C.byref(tot),
+                            _p(hist), HIST, _p(rc), _p(rn)) == 0
+    return tot.value, hist, rc[:g.n], rn[:g.n]
+
+
 def brute(g):
     rp, col = _csr(g)
     tot = C.c_uint64()

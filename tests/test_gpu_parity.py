@@ -271,16 +271,46 @@ def test_wide_engine_occupancy_variants(wide_blocks):
     assert np.array_equal(nodes, oracle.roots(g)[3])
 
 
-def test_level2_offers_first_level_subtrees():
-    g = mce.gen_rmat(12, 16, 0.57, 0.19, 0.19, 7)
-    t, h, _ = oracle.count(g)
-    _, _, rc, rn = oracle.roots(g)
+@pytest.mark.parametrize("maker", [
+    lambda: mce.gen_er(2000, 0.01, 1, 8, 6, 40),            # all three engines
+    lambda: mce.gen_rmat(12, 16, 0.57, 0.19, 0.19, 7),      # wide roots
+    lambda: mce.gen_ba(20000, 8, 5, 20, 20, 60),            # 64-bit rows, long lists
+    lambda: _hub_graph(5000),                               # hub rows
+    lambda: mce.union(mce.gen_chung_lu_batch(32, 64, 4096, 2.3, 8, 32, 5, 5, 40, 13)),
+], ids=["er", "rmat12", "ba", "hub", "batch"])
+@pytest.mark.parametrize("kw", [{}, {"worker_list": mce.WL_OFF}, {"bitmap_width": 64},
+                                {"cuda_graph": 1}], ids=["wl", "nowl", "64bit", "graph"])
+def test_level2_edge_rooted_units(maker, kw):
+    """-p l2: every oriented edge (r, v) is a unit (the triangle list as its
+    candidates, its pivot from them alone, the root's neighbours before v
+    outside): counts, histogram and per-root counts are those of L1, and the
+    per-root tree sizes those of the oracle's L2 walk (units are not nodes)."""
+    g = maker()
+    t, h, rc, rn = oracle.roots_l2(g)
     with mce.Graph.from_host(g) as dg:
-        r = dg.count(level=mce.LEVEL_L2, log_roots=True)
-        counts, nodes = dg.root_counts(), dg.root_log()
-    assert r.total == t and np.array_equal(r.hist, h)
-    assert np.array_equal(counts, rc) and np.array_equal(nodes, rn)  # same trees, shared sooner
-    assert r.stats["donations"] > 0
+        for _ in range(2):
+            r = dg.count(level=mce.LEVEL_L2, log_roots=True, **kw)
+            assert r.stats["error_flags"] == 0
+            assert r.total == t and np.array_equal(r.hist, h)
+            assert np.array_equal(dg.root_counts(), rc)
+            assert np.array_equal(dg.root_log(), rn)
+    assert t == oracle.count(g)[0]
+
+
+def test_level2_lists_the_same_cliques():
+    g = mce.gen_er(600, 0.03, 2, 6, 5, 14)
+    with mce.Graph.from_host(g) as dg:
+        l1 = sorted(tuple(sorted(c)) for c in dg.list_cliques())
+        l2 = sorted(tuple(sorted(c)) for c in dg.list_cliques(level=mce.LEVEL_L2))
+    assert l1 == l2
+
+
+def test_level2_on_a_batch():
+    b = mce.gen_chung_lu_batch(48, 64, 4096, 2.3, 8, 32, 5, 5, 40, 17)
+    per_o = [oracle.count(b.graph(i))[0] for i in range(b.num_graphs)]
+    with mce.Batch(b) as db:
+        r = db.count(level=mce.LEVEL_L2)
+    assert [int(x) for x in r.per_graph] == per_o
 
 
 @pytest.mark.parametrize("maker", [
@@ -299,6 +329,30 @@ def test_x_pivot_changes_trees_not_counts(maker):
     assert px.total == t and np.array_equal(px.hist, h)
     assert np.array_equal(counts, rc)  # a root's cliques do not depend on its pivots
     assert px.stats["tree_nodes"] <= ip.stats["tree_nodes"]
+
+
+@pytest.mark.parametrize("kw", [{}, {"worker_list": mce.WL_OFF}, {"wide_blocks": 8},
+                                {"warps_per_root": 2}, {"level": mce.LEVEL_L2}],
+                         ids=["wl", "nowl", "wide8", "w2", "l2"])
+def test_x_pivot_in_the_wide_engine(kw):
+    """-i px in the wide engine (roots with more than 64 later neighbours):
+    the same counts and per-root counts, no more tree nodes in its class."""
+    g = mce.gen_rmat(13, 16, 0.57, 0.19, 0.19, 7)
+    t, h, _ = oracle.count(g)
+    _, _, rc, _ = oracle.roots(g)
+    with mce.Graph.from_host(g) as dg:
+        ip = dg.count(log_roots=True, **kw)
+        n_ip = dg.root_log()
+        px = dg.count(x_pivot=1, log_roots=True, **kw)
+        counts, n_px = dg.root_counts(), dg.root_log()
+        split, _ = dg.split_csr()
+    assert px.stats["class_roots"][2] > 0 and px.stats["error_flags"] == 0
+    assert px.total == t and np.array_equal(px.hist, h)
+    assert np.array_equal(counts, rc)
+    wide = (g.row_ptr[1:g.n + 1] - split) > 64
+    assert n_px[wide].sum() <= n_ip[wide].sum()  # the outside pivots prune wide trees
+    if not kw:
+        assert n_px[wide].sum() < n_ip[wide].sum()
 
 
 @pytest.mark.parametrize("maker,kw", [

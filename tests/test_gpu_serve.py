@@ -33,7 +33,9 @@ def test_serve_counts_match_oracle(ba, cap):
     with mce.Serve(g, ego_cap=cap) as s:
         res, lat = s.run(seeds, timeout_ms=120000)
         st = s.stats()
-    assert st["served"] == len(seeds) and st["kernel_launches"] == 1
+    # one launch per slot class (two when the cap turns the 256-thread class on)
+    assert st["served"] == len(seeds) and st["kernel_launches"] == (2 if st["small_slots"] else 1)
+    assert (st["small_slots"] > 0) == (cap > 2048)
     for r, seed in zip(res, seeds):
         want, n, m = ego_count(hg, seed, cap)
         assert r["status"] == mce.OK and r["seed"] == seed
@@ -140,3 +142,33 @@ def test_serve_idle_slots_help_large_requests(ba):
         assert r["status"] == mce.OK and n >= 1024
         assert (int(r["count"]), int(r["ego_n"])) == (want, n)
     assert st["helps"] > 0
+
+
+def test_serve_footprint_classes(ba):
+    """Requests whose footprint bound fits small_cap go to the 256-thread
+    slots (id bit 0 set) once every whole-block slot holds a request, the
+    others to the whole-block slots; every answer matches the oracle either
+    way."""
+    hg, g = ba
+    deg = np.diff(hg.row_ptr[:hg.n + 1]).astype(np.int64)
+    bound = deg + np.array([deg[hg.col[hg.row_ptr[v]:hg.row_ptr[v + 1]]].sum()
+                            for v in range(hg.n)])
+    small = np.flatnonzero(bound + 1 <= 256)[:40]
+    large = np.argsort(deg)[-6:]
+    seeds = np.concatenate([small, large, small[:10]]).astype(np.int64)
+    with mce.Serve(g, ego_cap=2048, small_cap=256, big_slots=4) as s:
+        ids = [s.submit(int(x)) for x in seeds]
+        got = [s.wait(i) for i in ids]
+        res, _ = s.run(seeds, timeout_ms=120000)
+        st = s.stats()
+    assert st["small_cap"] == 256 and st["small_slots"] > 0
+    assert st["slots"] == 4 + st["small_slots"]
+    assert 1 <= st["peak_in_flight"] <= len(seeds)
+    cls = [rid & 1 for rid in ids]
+    fits = [bool(bound[x] + 1 <= 256) for x in seeds]
+    assert cls[:4] == [0] * 4  # the four whole-block slots take the first ones
+    assert cls[4:] == [1 if f else 0 for f in fits[4:]]
+    for r, rr, x in zip(got, res, seeds):
+        want, n, m = ego_count(hg, x, 2048)
+        assert r["status"] == mce.OK and (int(r["count"]), int(r["ego_n"])) == (want, n), x
+        assert int(rr["count"]) == want
