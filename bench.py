@@ -237,29 +237,40 @@ def algorithmic_bytes(g, split, cs):
             "search_with_earlier_rows": int(np.sum(8 + 4 * deg[roots] + sum_all[roots]))}
 
 
-def kernel_source_hash():
-    """Hash of the CUDA sources: a profile figure is current only while the
-    kernels it was captured on are unchanged."""
+def kernel_source_hash(files=None):
+    """Hash of CUDA sources (all of csrc/, or the named files in it): a
+    profile figure is current only while the kernels it was captured on are
+    unchanged."""
     import glob
     import hashlib
     h = hashlib.sha256()
-    for f in sorted(glob.glob(os.path.join(ROOT, "mce-gpu_b200", "csrc", "*"))):
+    paths = (sorted(glob.glob(os.path.join(ROOT, "mce-gpu_b200", "csrc", "*"))) if files is None
+             else [os.path.join(ROOT, "mce-gpu_b200", "csrc", f) for f in sorted(files)])
+    for f in paths:
         with open(f, "rb") as fh:
             h.update(os.path.basename(f).encode() + fh.read())
     return h.hexdigest()[:16]
 
 
 def profile_figures(workload):
-    """ncu figures committed under profiles/ for this workload, if they were
-    captured on the current kernel sources (else {} and the reason)."""
+    """ncu figures committed in profiles/traffic.json for this workload,
+    each kept only while the sources its kernels compile from are the ones
+    it was captured on.  Returns ({figure: value}, note on what was dropped)."""
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
             tj = json.load(f)
     except Exception:
         return {}, "no profiles/traffic.json"
-    if tj.get("kernel_source_hash") != kernel_source_hash():
-        return {}, "profiles/traffic.json was captured on other kernel sources"
-    return {k.split(":", 1)[1]: v for k, v in tj.items() if k.startswith(workload + ":")}, None
+    out, stale = {}, []
+    for k, v in tj.items():
+        if not k.startswith(workload + ":") or not isinstance(v, dict):
+            continue
+        name = k.split(":", 1)[1]
+        if v.get("hash") == kernel_source_hash(v.get("sources")):
+            out[name] = v["value"]
+        else:
+            stale.append(name)
+    return out, (f"captured on other kernel sources: {', '.join(stale)}" if stale else None)
 
 
 def measured_peaks():
@@ -404,7 +415,17 @@ def run_mine(args, rank, world, local_rank):
     assert re2e.total == total
     barrier()
     e2e_ms = sum(e2e_times) / len(e2e_times)
-    e2e_path = ("mce_batch_count_host (each part's copy overlapping the work on the parts "
+    # this box's pinned host -> device bandwidth: one plain copy of the arcs
+    # (the e2e step cannot end before its copies do)
+    col_d = torch.empty_like(col_h, device="cuda")
+
+    def copy_arcs():
+        with torch.cuda.stream(stream):
+            col_d.copy_(col_h, non_blocking=True)
+    h2d_times, _ = timed(stream, flush, copy_arcs, 3)
+    h2d_gbs = col_h.numel() * col_h.element_size() / (min(h2d_times) / 1e3) / 1e9
+    del col_d
+    e2e_path =("mce_batch_count_host (each part's copy overlapping the work on the parts "
                 "before it)" if hb is not None else "mce_graph_reload + mce_count")
 
     # max over ranks
@@ -422,8 +443,17 @@ def run_mine(args, rank, world, local_rank):
     phases = {"search": count_ms, "peel": peel_ms, "orient": orient_ms}
     # ---- the search's algorithmic word operations, from the counting
     # variants of the engines (one call outside the timed steps)
-    ops = dg.count(stream=sptr, **dict(kw, count_ops=True))
-    assert ops.total == total and ops.stats["tree_nodes"] == stats[-1]["tree_nodes"]
+    # (the counter models the IP walk: with IPX tuned on, the IP search of the
+    # same graph is timed for it separately)
+    ip_kw = dict(kw, x_pivot=0)
+    ops = dg.count(stream=sptr, **dict(ip_kw, count_ops=True))
+    if kw.get("x_pivot"):
+        _, rip = timed(stream, flush, lambda: dg.count(stream=sptr, **ip_kw), 2)
+        search_ms_c, walk_c = rip.stats["count_ms"], "IP, timed apart from the IPX steps"
+    else:
+        rip, search_ms_c, walk_c = None, count_ms, "IP, the timed steps"
+    ip_nodes = rip.stats["tree_nodes"] if rip else stats[-1]["tree_nodes"]
+    assert ops.total == total and ops.stats["tree_nodes"] == ip_nodes
     word_ops = int(ops.stats["word_ops"])
     sms = torch.cuda.get_device_properties(local_rank).multi_processor_count
     clk_hz = (clocks.get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)) * 1e6
@@ -453,7 +483,9 @@ def run_mine(args, rank, world, local_rank):
         "e2e": {"value": job_value(total, e2e_ms, world), "unit": "maximal cliques/s",
                 "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h + 8 * 4096 + 64 + 8 + 4 + 128),
-                "ms_per_step": e2e_ms, "path": e2e_path},
+                "ms_per_step": e2e_ms, "path": e2e_path,
+                "h2d_copy_gbs": round(h2d_gbs, 2),
+                "copy_bound_ms": round(h2d / h2d_gbs / 1e6, 3)},
         "gpu_launches": int(sum(s_["kernel_launches"] for s_ in stats)),
         # the search (all engine launches of a step) against HBM by its
         # stage-B algorithmic bytes
@@ -475,10 +507,11 @@ def run_mine(args, rank, world, local_rank):
         # search time, against the INT32 lanes (128 per SM per clock) and
         # against AND+POPC pairs at the POPC rate (16 per SM per clock)
         "roofline_stageC": {"bound": "int32", "kernel": "search", "word_ops": word_ops,
-                            "achieved": word_ops / (count_ms / 1e3) / 1e9,
+                            "walk": walk_c, "search_ms": round(search_ms_c, 3),
+                            "achieved": word_ops / (search_ms_c / 1e3) / 1e9,
                             "peak": 128 * sms * clk_hz / 1e9, "unit": "G word-ops/s",
-                            "frac": word_ops / (count_ms / 1e3) / (128 * sms * clk_hz),
-                            "frac_popc_pairs": word_ops / (count_ms / 1e3) / (32 * sms * clk_hz),
+                            "frac": word_ops / (search_ms_c / 1e3) / (128 * sms * clk_hz),
+                            "frac_popc_pairs": word_ops / (search_ms_c / 1e3) / (32 * sms * clk_hz),
                             "peak_source": "128 INT32 lanes x SMs x sampled SM clock; "
                                            "popc pairs: 16 POPC + 16 AND per SM per clock"},
         "clocks": clocks,

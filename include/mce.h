@@ -451,8 +451,8 @@ int mce_model_grad(mce_model_t m, const float *X, const float *Y, int64_t count,
  * searched and MCE_EINVAL is returned.  Every root must have 1 to 32 later
  * and at most 1024 earlier neighbours; otherwise nothing is searched and
  * MCE_ELIMIT is returned.  Work is queued on `stream` (NULL = legacy default
- * stream) and the call synchronises that stream twice before it returns, so
- * it cannot be captured into a CUDA graph.  The call uses the
+ * stream) and the call synchronises that stream twice before it returns.
+ * The call uses the
  * MCE_NOALLOC_SCRATCH_BYTES array (its address on the current device is
  * looked up on every call); calls that overlap on the GPU race on the
  * array, so serialise them.                                                  */

@@ -67,6 +67,8 @@ struct mce_graph {
   size_t sort_tmp_bytes = 0;
   // search
   uint32_t *fetch = nullptr, *err = nullptr;
+  uint32_t *orient_next = nullptr;  // orientation counters, two per launch: [0] whole graph,
+                                    // [2 + 2p] part p
   unsigned long long *hist = nullptr, *nodes = nullptr;
   unsigned long long *root_nodes = nullptr, *root_count = nullptr;
   unsigned long long *root_ops = nullptr;  // per-root word operations (opts.count_ops)
@@ -117,6 +119,8 @@ constexpr int64_t BATCH_PART_MIN_ARCS = 1 << 20;  // mce_batch_count_host: small
 constexpr uint32_t DEFAULT_SOLO_MAX = 0;     // measured slower than grid-wide rounds
 constexpr uint32_t DEFAULT_DONATE_AFTER = 256;  // the reference's SZTH (mce/parameter.cuh:5)
 
+constexpr int MAX_PARTS = 4;  // a host batch is copied and prepared in at most this many parts
+
 void free_graph_bufs(mce_graph *g) {
   dfree(g->rp); dfree(g->col); dfree(g->cs); dfree(g->split);
   dfree(g->prio); dfree(g->core); dfree(g->deg); dfree(g->alA); dfree(g->alB);
@@ -156,6 +160,7 @@ int alloc_graph_bufs(mce_graph *g, int64_t n, int64_t m) {
 int alloc_fixed_bufs(mce_graph *g) {
   int rc;
   if ((rc = dalloc((char **)&g->peel_ctl, peel_ctl_bytes())) || (rc = dalloc(&g->shape, 1)) ||
+      (rc = dalloc(&g->orient_next, 2 * (1 + MAX_PARTS))) ||
       (rc = dalloc(&g->fetch, 8)) || (rc = dalloc(&g->err, 4)) ||
       (rc = dalloc(&g->hist, MCE_HIST_MAX)) || (rc = dalloc(&g->nodes, 4)))
     return rc;
@@ -170,7 +175,6 @@ cudaStream_t pick_stream(mce_graph *g, void *s) { return s ? (cudaStream_t)s : g
 // Per-graph counting of a batch handle.
 // A batch still arriving from the host in parts (mce_batch_count_host):
 // graphs [g[p], g[p+1]) are on the device once ready[p] has fired.
-constexpr int MAX_PARTS = 4;
 struct BatchParts {
   int k;
   int64_t g[MAX_PARTS + 1];
@@ -280,6 +284,8 @@ OrientArgs orient_args(mce_graph *g) {
   oa.sched = MCE_SCHED_PLAIN;
   oa.hub_of = g->hub_of;
   oa.hub_list = g->hub_list;
+  oa.next = g->orient_next;
+  oa.long_list = reinterpret_cast<int32_t *>(g->keys_out);  // free until the roots' sort
   return oa;
 }
 
@@ -326,6 +332,8 @@ int run_parts(mce_graph *g, cudaStream_t s, int *launches, const BatchCtx *bc, i
     oa.v0 = vbeg;
     oa.n = vend;
     oa.keep_shape = true;
+    oa.next = g->orient_next + 2 + 2 * p;  // the parts' orientations run at the same time
+    oa.long_list = reinterpret_cast<int32_t *>(g->keys_out) + vbeg;
     if ((rc = orient_launch(oa, sp, launches))) return rc;
     MCE_CUDA(cudaEventRecord(g->part_done[p], sp));
   }
@@ -516,6 +524,7 @@ int mce_graph_free(mce_graph_t g) {
   free_graph_bufs(g);
   dfree(g->peel_ctl);
   dfree(g->shape);
+  dfree(g->orient_next);
   dfree(g->fetch);
   dfree(g->err);
   dfree(g->hist);
@@ -710,7 +719,7 @@ int count_impl(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t *his
   if (sh.cls_cnt[CLS_BIG]) return MCE_ELIMIT;
   // earlier-neighbour rows of the hub roots, built by many warps at once
   if (sh.hub_cnt > 0) {
-    const int64_t need_off = (int64_t)sh.hub_cnt + 1, need_rows = (int64_t)sh.hub_rows;
+    const int64_t need_off = (int64_t)sh.hub_cnt + 2, need_rows = (int64_t)sh.hub_rows;
     if (need_off > g->hub_off_cap) {
       dfree(g->hub_off);
       dfree(g->hub_nx);
@@ -1093,6 +1102,8 @@ int count_pipelined(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t
     oa.n = vend;
     oa.shape = g->part_shape + p;
     oa.hub_list = g->hub_list + vbeg;  // hub indices are the part's own
+    oa.next = g->orient_next + 2 + 2 * p;
+    oa.long_list = reinterpret_cast<int32_t *>(g->keys_out) + vbeg;
     if ((rc = orient_launch(oa, sp, &launches))) return finish(rc);
     const int64_t np = vend - vbeg;
     if (degree && np > 0 &&
@@ -1120,7 +1131,7 @@ int count_pipelined(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t
     }
     const int64_t vbeg = vb[p];
     if (sh.hub_cnt > 0) {
-      const int64_t need_off = (int64_t)sh.hub_cnt + 1, need_rows = (int64_t)sh.hub_rows;
+      const int64_t need_off = (int64_t)sh.hub_cnt + 2, need_rows = (int64_t)sh.hub_rows;
       if (need_off > g->phub_off_cap[p]) {
         if (g->phub_off[p]) retired.push_back(g->phub_off[p]);
         if (g->phub_nx[p]) retired.push_back(g->phub_nx[p]);

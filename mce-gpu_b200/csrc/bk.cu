@@ -310,43 +310,59 @@ __global__ void __launch_bounds__(MEM_BLOCK, MINB) bk_mem_kernel(BKArgs a, int c
 // loads that leaves the rest of its class idle at the end).
 // ---------------------------------------------------------------------------
 constexpr int HUB_BLOCK = 256;
+constexpr int HUB_FETCH = 4;  // 32-row chunks a warp of hub_rows_kernel takes at a time
 
 // off[j] = sum over k < j of hub k's earlier degree rounded up to 32; one
-// block walks the list in tiles of HUB_BLOCK.
-__global__ void __launch_bounds__(HUB_BLOCK) hub_offsets_kernel(
+// block of HUB_OFF_BLOCK threads walks the list in tiles of HUB_OFF_PER
+// hubs per thread (their offsets gathered together), scanning each tile.
+constexpr int HUB_OFF_BLOCK = 1024, HUB_OFF_PER = 8;
+__global__ void __launch_bounds__(HUB_OFF_BLOCK) hub_offsets_kernel(
     const int32_t *__restrict__ rp, const int32_t *__restrict__ split,
     const int32_t *__restrict__ hub_list, uint32_t cnt, int64_t *__restrict__ off,
     int32_t *__restrict__ nx) {
-  __shared__ long long wsum[HUB_BLOCK / 32];
+  __shared__ long long wsum[HUB_OFF_BLOCK / 32];
   __shared__ long long carry;
   const int lane = (int)lane_id(), wid = (int)(threadIdx.x >> 5);
   if (threadIdx.x == 0) carry = 0;
   __syncthreads();
-  for (uint32_t base = 0; base < cnt; base += HUB_BLOCK) {
-    const uint32_t j = base + threadIdx.x;
-    long long v = 0;
-    if (j < cnt) {
-      const int32_t r = hub_list[j];
-      v = (long long)(((uint32_t)(split[r] - rp[r]) + 31u) & ~31u);
+  for (uint32_t base = 0; base < cnt; base += HUB_OFF_BLOCK * HUB_OFF_PER) {
+    const uint32_t j0 = base + threadIdx.x * HUB_OFF_PER;
+    long long v[HUB_OFF_PER];
+    long long mine = 0;
+#pragma unroll
+    for (int k = 0; k < HUB_OFF_PER; ++k) {
+      v[k] = 0;
+      if (j0 + k < cnt) {
+        const int32_t r = hub_list[j0 + k];
+        v[k] = (long long)(((uint32_t)(split[r] - rp[r]) + 31u) & ~31u);
+      }
+      mine += v[k];
     }
-    long long x = v;  // inclusive scan in the warp
+    long long x = mine;  // inclusive scan of the threads' sums in the warp
     for (int o = 1; o < 32; o <<= 1) {
       const long long y = __shfl_up_sync(MCE_FULL, x, o);
       if (lane >= o) x += y;
     }
     if (lane == 31) wsum[wid] = x;
     __syncthreads();
-    long long before = carry;
+    long long before = carry + x - mine;
     for (int w = 0; w < wid; ++w) before += wsum[w];
-    if (j < cnt) {
-      off[j] = (int64_t)(before + x - v);
-      nx[j] = -1;
+#pragma unroll
+    for (int k = 0; k < HUB_OFF_PER; ++k) {
+      if (j0 + k < cnt) {
+        off[j0 + k] = (int64_t)before;
+        nx[j0 + k] = -1;
+      }
+      before += v[k];
     }
     __syncthreads();
-    if (threadIdx.x == HUB_BLOCK - 1) carry = before + x;
+    if (threadIdx.x == HUB_OFF_BLOCK - 1) carry = before;
     __syncthreads();
   }
-  if (threadIdx.x == 0) off[cnt] = (int64_t)carry;
+  if (threadIdx.x == 0) {
+    off[cnt] = (int64_t)carry;
+    off[cnt + 1] = 0;  // hub_rows_kernel's chunk counter
+  }
 }
 
 struct HubSmem {
@@ -395,23 +411,30 @@ __device__ __forceinline__ void flat_walk2(const int32_t *__restrict__ cs, int32
 
 __device__ __forceinline__ uint32_t hub_slot(int32_t w) { return ((uint32_t)w * 0x9E3779B1u) >> 24; }
 
-// Each warp takes a contiguous range of 32-row chunks; the hash of a hub's
-// later list (d+ <= 64) is rebuilt when the range moves to the next hub.
+// Warps fetch HUB_FETCH 32-row chunks at a time from a counter (off[cnt + 1],
+// zeroed by hub_offsets_kernel), so a warp whose chunks walk long lists takes
+// fewer; the hash of a hub's later list (d+ <= 64) is rebuilt when a warp's
+// chunks move on to the next hub (a warp's chunks only move forward).
 __global__ void __launch_bounds__(HUB_BLOCK) hub_rows_kernel(
     const int32_t *__restrict__ rp, const int32_t *__restrict__ split,
     const int32_t *__restrict__ cs, const int32_t *__restrict__ hub_list, uint32_t cnt,
-    const int64_t *__restrict__ off, int64_t chunks, unsigned long long *__restrict__ rows) {
+    const int64_t *__restrict__ off, int64_t chunks, unsigned long long *__restrict__ rows,
+    unsigned long long *next) {
   __shared__ HubSmem sm_all[HUB_BLOCK / 32];
   HubSmem &sm = sm_all[threadIdx.x >> 5];
   const int lane = (int)lane_id();
-  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  const int64_t per = (chunks + nw - 1) / nw;
-  const int64_t c0 = gw * per, c1 = min(chunks, c0 + per);
   int32_t cur = -1;  // hub whose hash is built
   uint32_t j = 0;
-  for (int64_t c = c0; c < c1; ++c) {
-    const int64_t row0 = 32 * c;
+  int64_t c = 0, c1 = 0;
+  for (;;) {
+    if (c == c1) {
+      unsigned long long f = 0;
+      if (lane == 0) f = atomicAdd(next, (unsigned long long)HUB_FETCH);
+      c = (int64_t)__shfl_sync(MCE_FULL, f, 0);
+      if (c >= chunks) break;
+      c1 = min(chunks, c + HUB_FETCH);
+    }
+    const int64_t row0 = 32 * c++;
     if (cur < 0 || row0 >= off[j + 1]) {  // first chunk, or the next hub: last j with off[j] <= row0
       uint32_t lo = 0, hi = cnt - 1;
       while (lo < hi) {
@@ -468,15 +491,16 @@ int hub_rows_launch(const int32_t *rp, const int32_t *split, const int32_t *cs,
                     int32_t *nx, unsigned long long *rows, int sms, cudaStream_t s,
                     int *launches) {
   if (cnt == 0) return MCE_OK;
-  hub_offsets_kernel<<<1, HUB_BLOCK, 0, s>>>(rp, split, hub_list, cnt, off, nx);
+  hub_offsets_kernel<<<1, HUB_OFF_BLOCK, 0, s>>>(rp, split, hub_list, cnt, off, nx);
   MCE_CUDA(cudaGetLastError());
   const int64_t chunks = total_rows / 32;
   int64_t blocks = ((chunks + 7) / 8 + 0);  // up to one chunk per warp
   const int64_t cap = (int64_t)sms * 8;
   if (blocks > cap) blocks = cap;
   if (blocks < 1) blocks = 1;
-  hub_rows_kernel<<<(unsigned)blocks, HUB_BLOCK, 0, s>>>(rp, split, cs, hub_list, cnt, off, chunks,
-                                                        rows);
+  hub_rows_kernel<<<(unsigned)blocks, HUB_BLOCK, 0, s>>>(
+      rp, split, cs, hub_list, cnt, off, chunks, rows,
+      reinterpret_cast<unsigned long long *>(off + cnt + 1));
   MCE_CUDA(cudaGetLastError());
   if (launches) *launches += 2;
   return MCE_OK;
@@ -618,7 +642,7 @@ int queue_launch_init(const QueueView &q, cudaStream_t s, int *launches) {
 // Every call resolves the array's device address on the current device with
 // cudaGetSymbolAddress, checks the root ids against the vertex count before
 // any read at them, and synchronises its stream twice (the root check, the
-// status), so it cannot be captured into a CUDA graph.  Every call shares
+// status) before it returns.  Every call shares
 // the array and clears the part that must start at zero, so calls whose work
 // overlaps on the GPU race with each other: serialise them (one stream, or
 // events).

@@ -85,6 +85,11 @@ struct OrientArgs {
   int32_t *hub_list;    // n: the hub roots, in no particular order
   int64_t v0 = 0;       // vertices [v0, n) are oriented (a batch part: its range)
   bool keep_shape = false;  // add to the summary of earlier parts instead of zeroing it
+  uint32_t *next = nullptr; // two counters (zeroed by the launcher): the launch's row groups
+                            // and its long rows; launches that run at the same time need
+                            // their own
+  int32_t *long_list = nullptr;  // room for the vertices of [v0, n) whose rows are long
+                                 // (any scratch of n - v0 ints, free until the roots' sort)
 };
 int orient_launch(const OrientArgs &a, cudaStream_t s, int *launches);
 

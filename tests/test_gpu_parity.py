@@ -52,11 +52,25 @@ def test_small_plain_config():
     assert r.total == 97157  # the reference binary prints the same count (tests/golden)
 
 
+def hubs_graph(n, hubs, seed):
+    """ER(n, 4/n) plus the given vertices adjacent to every other vertex:
+    rows of n - 1 arcs among many short ones."""
+    base = mce.gen_er(n, 4.0 / n, seed)
+    edges = {(v, int(w)) for v in range(base.n)
+             for w in base.col[base.row_ptr[v]:base.row_ptr[v + 1]] if v < w}
+    for h in hubs:
+        edges |= {(min(h, v), max(h, v)) for v in range(n) if v != h}
+    return build(n, sorted(edges))
+
+
 @pytest.mark.parametrize("maker", [
     lambda: mce.gen_er(3000, 0.01, 3, 10, 6, 20),
     lambda: mce.gen_rmat(11, 16, 0.57, 0.19, 0.19, 7),
     lambda: mce.gen_ba(20000, 8, 5, 20, 20, 60),
     lambda: build(5, [(0, 1), (1, 2), (2, 3), (3, 4)]),
+    # rows longer than 2,048 arcs: split by a whole block, after the rest
+    lambda: mce.gen_rmat(14, 16, 0.57, 0.19, 0.19, 7),
+    lambda: hubs_graph(12000, [0, 5, 77], 3),
 ])
 def test_degeneracy_bit_exact(maker):
     g = maker()
