@@ -93,6 +93,10 @@ struct mce_graph {
   // to the caller's stream
   cudaStream_t part_s[4] = {nullptr};
   cudaEvent_t part_fork = nullptr, part_done[4] = {nullptr};
+  // a batch's per-graph peel: the small graphs' launch runs on a side stream
+  // ([0] whole batch, [1 + p] part p)
+  cudaStream_t seg_side[5] = {nullptr};
+  cudaEvent_t seg_fork[5] = {nullptr}, seg_join[5] = {nullptr};
   // a batch searched part by part as it arrives (mce_batch_count_host):
   // per part its roots' summary (device and pinned host), root fetch
   // counters, sort scratch and hub rows
@@ -184,6 +188,35 @@ struct BatchParts {
 };
 
 // the most vertices of a graph of part p
+// Graphs of part p (or of the whole batch) with more than PEEL_SMALL_N vertices.
+inline int64_t count_big(const int64_t *vo, int64_t g0, int64_t g1) {
+  int64_t k = 0;
+  for (int64_t g = g0; g < g1; ++g) k += vo[g + 1] - vo[g] - 1 > PEEL_SMALL_N;
+  return k;
+}
+
+// The per-graph peel's order of graphs [g0, g1): those with more than
+// PEEL_SMALL_N vertices first (their own launch), each set largest first.
+void order_graphs(int32_t *order, int64_t g0, int64_t g1, const int64_t *vo, const int64_t *ao) {
+  std::stable_sort(order + g0, order + g1, [&](int32_t x, int32_t y) {
+    const bool bx = vo[x + 1] - vo[x] - 1 > PEEL_SMALL_N, by = vo[y + 1] - vo[y] - 1 > PEEL_SMALL_N;
+    if (bx != by) return bx;
+    return ao[x + 1] - ao[x] > ao[y + 1] - ao[y];
+  });
+}
+
+// The side stream and events of a per-graph peel launch (i: 0 whole batch,
+// 1 + p part p), made on first use.
+int seg_side(mce_graph *g, int i, PeelSide *ps) {
+  if (!g->seg_side[i]) MCE_CUDA(cudaStreamCreateWithFlags(&g->seg_side[i], cudaStreamNonBlocking));
+  if (!g->seg_fork[i]) MCE_CUDA(cudaEventCreateWithFlags(&g->seg_fork[i], cudaEventDisableTiming));
+  if (!g->seg_join[i]) MCE_CUDA(cudaEventCreateWithFlags(&g->seg_join[i], cudaEventDisableTiming));
+  ps->side = g->seg_side[i];
+  ps->fork = g->seg_fork[i];
+  ps->join = g->seg_join[i];
+  return MCE_OK;
+}
+
 inline int64_t part_max_n(const BatchParts &P, int p) {
   int64_t mx = 0;
   for (int64_t g = P.g[p]; g < P.g[p + 1]; ++g) {
@@ -202,6 +235,7 @@ struct BatchCtx {
   const int32_t *order;                // device, G: graphs largest first (within each part)
   const BatchParts *parts = nullptr;   // nullable: rebase, peel and orient part by part
   int64_t max_n = 0;                   // the most vertices of a graph (0: unknown)
+  int64_t g_big = 0;                   // graphs of `order` with more than PEEL_SMALL_N vertices
 };
 
 int check_args(const int32_t *row_ptr, const int32_t *col, int64_t n, int64_t m) {
@@ -234,9 +268,13 @@ int run_peel(mce_graph *g, cudaStream_t s, int *launches, int solo_opt = 0,
              const BatchCtx *bc = nullptr) {
   if (g->n == 0) return MCE_OK;
   const PeelArgs pa = peel_args(g, solo_opt);
-  if (bc)  // a batch: every graph peeled by one block, no grid-wide rounds
-    return peel_segments_launch(pa, bc->vtx_off, bc->arc_off, bc->order, (int32_t)bc->G, s,
-                                launches, -1, bc->max_n);
+  if (bc) {  // a batch: every graph peeled by one block, no grid-wide rounds
+    PeelSide ps;
+    int rc = seg_side(g, 0, &ps);
+    if (rc) return rc;
+    return peel_segments_launch(pa, bc->vtx_off, bc->arc_off, bc->order, (int32_t)bc->G,
+                                (int32_t)bc->g_big, s, ps, launches, -1, bc->max_n);
+  }
   return peel_launch(pa, s, launches);
 }
 
@@ -324,9 +362,12 @@ int run_parts(mce_graph *g, cudaStream_t s, int *launches, const BatchCtx *bc, i
                                       P.ao_h[g1], vend, (int32_t)P.ao_h[g1], g->rp, g->col,
                                       const_cast<int32_t *>(bc->graph_of), g->sms, sp, launches);
     if (rc) return rc;
+    PeelSide ps;
+    if ((rc = seg_side(g, 1 + p, &ps))) return rc;
     if (vend > vbeg &&
         (rc = peel_segments_launch(pa, bc->vtx_off, bc->arc_off, bc->order + g0,
-                                   (int32_t)(g1 - g0), sp, launches, p, part_max_n(P, p))))
+                                   (int32_t)(g1 - g0), (int32_t)count_big(P.vo_h, g0, g1), sp,
+                                   ps, launches, p, part_max_n(P, p))))
       return rc;
     OrientArgs oa = orient_args(g);
     oa.v0 = vbeg;
@@ -552,6 +593,11 @@ int mce_graph_free(mce_graph_t g) {
     if (g->part_done[p]) cudaEventDestroy(g->part_done[p]);
   }
   if (g->part_fork) cudaEventDestroy(g->part_fork);
+  for (int i = 0; i < 5; ++i) {
+    if (g->seg_side[i]) cudaStreamDestroy(g->seg_side[i]);
+    if (g->seg_fork[i]) cudaEventDestroy(g->seg_fork[i]);
+    if (g->seg_join[i]) cudaEventDestroy(g->seg_join[i]);
+  }
   if (g->own) cudaStreamDestroy(g->own);
   delete g;
   return MCE_OK;
@@ -1093,9 +1139,12 @@ int count_pipelined(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t
                                        const_cast<int32_t *>(bc->graph_of), g->sms, sp,
                                        &launches)))
       return finish(rc);
+    PeelSide ps;
+    if ((rc = seg_side(g, 1 + p, &ps))) return finish(rc);
     if (vend > vbeg &&
         (rc = peel_segments_launch(pa, bc->vtx_off, bc->arc_off, bc->order + g0,
-                                   (int32_t)(g1 - g0), sp, &launches, p, part_max_n(P, p))))
+                                   (int32_t)(g1 - g0), (int32_t)count_big(P.vo_h, g0, g1), sp,
+                                   ps, &launches, p, part_max_n(P, p))))
       return finish(rc);
     OrientArgs oa = orient_args(g);
     oa.v0 = vbeg;
@@ -1413,6 +1462,7 @@ struct mce_batch {
   int32_t *order_h = nullptr;  // its pinned host staging copy
   int64_t cap_rows = -1, cap_m = -1, cap_g = -1;
   int64_t max_n = 0;           // the most vertices of a graph of the batch
+  int64_t g_big = 0;           // its graphs with more than PEEL_SMALL_N vertices
   // mce_batch_count_host: copies on their own stream, one event per part
   cudaStream_t copy = nullptr;
   cudaEvent_t start = nullptr, ready[MAX_PARTS] = {nullptr};
@@ -1495,9 +1545,8 @@ int batch_load(mce_batch *b, const int32_t *row_ptr, const int32_t *col, const i
   for (int32_t i = 0; i < G; ++i) order[i] = i;
   b->max_n = 0;
   for (int32_t i = 0; i < G; ++i) b->max_n = std::max<int64_t>(b->max_n, vo[i + 1] - vo[i] - 1);
-  std::stable_sort(order, order + G, [&](int32_t x, int32_t y) {
-    return ao[x + 1] - ao[x] > ao[y + 1] - ao[y];
-  });
+  order_graphs(order, 0, G, vo, ao);
+  b->g_big = count_big(vo, 0, G);
   MCE_CUDA(cudaMemcpyAsync(b->order, order, sizeof(int32_t) * (size_t)G, cudaMemcpyHostToDevice,
                            s));
   return batch_rebase_launch(b->rp_local, b->col_local, b->vtx_off, b->arc_off, G, n, m, g->rp,
@@ -1569,6 +1618,7 @@ int mce_batch_count(mce_batch_t b, const mce_opts_t *opts, uint64_t *per_graph_t
   }
   BatchCtx bc{b->graph_of, b->graph_count, per_graph_total, b->G, b->vtx_off, b->arc_off, b->order};
   bc.max_n = b->max_n;
+  bc.g_big = b->g_big;
   return count_impl(b->g, o, total, hist, stats, &bc);
 }
 
@@ -1624,10 +1674,8 @@ int mce_batch_count_host(mce_batch_t b, const int32_t *row_ptr, const int32_t *c
   for (int32_t i = 0; i < G; ++i) order[i] = i;
   b->max_n = 0;
   for (int32_t i = 0; i < G; ++i) b->max_n = std::max<int64_t>(b->max_n, vo[i + 1] - vo[i] - 1);
-  for (int p = 0; p < P.k; ++p)
-    std::stable_sort(order + P.g[p], order + P.g[p + 1], [&](int32_t x, int32_t y) {
-      return ao[x + 1] - ao[x] > ao[y + 1] - ao[y];
-    });
+  for (int p = 0; p < P.k; ++p) order_graphs(order, P.g[p], P.g[p + 1], vo, ao);
+  b->g_big = G;  // the order is per part now: a later resident count peels all in one launch
   // the copies wait for earlier work on the caller's stream, then run on
   // their own stream while the caller's stream processes the parts already
   // on the device
@@ -1656,6 +1704,7 @@ int mce_batch_count_host(mce_batch_t b, const int32_t *row_ptr, const int32_t *c
   BatchCtx bc{b->graph_of, b->graph_count, per_graph_total, b->G, b->vtx_off, b->arc_off, b->order};
   bc.parts = &P;
   bc.max_n = b->max_n;
+  bc.g_big = b->g_big;
   rc = pipelined ? count_pipelined(b->g, o, total, hist, stats, &bc)
                  : count_impl(b->g, o, total, hist, stats, &bc);
   if (rc) cudaStreamSynchronize(b->copy);  // no copy outlives a failed call

@@ -30,9 +30,18 @@ int peel_launch(const PeelArgs &a, cudaStream_t s, int *launches);
 // each part takes graphs from its own counter.  part < 0: the whole batch.
 // max_n: the most vertices of a graph of the launch (0: unknown); graphs up
 // to 16,384 vertices are peeled with their state in shared memory.
+// The first g_big graphs of `order` are peeled by 512-thread blocks; the
+// rest, which must have at most PEEL_SMALL_N vertices each, by 128-thread
+// blocks on `side` (forked from s by `fork`, joined back by `join`; all
+// three null: on s after the others), so that more small graphs run at once.
+constexpr int64_t PEEL_SMALL_N = 2048;
+struct PeelSide {
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+};
 int peel_segments_launch(const PeelArgs &a, const int64_t *vtx_off, const int64_t *arc_off,
-                         const int32_t *order, int32_t G, cudaStream_t s, int *launches,
-                         int part = -1, int64_t max_n = 0);
+                         const int32_t *order, int32_t G, int32_t g_big, cudaStream_t s,
+                         const PeelSide &ps, int *launches, int part = -1, int64_t max_n = 0);
 int peel_read(const void *ctl_dev, int32_t *degeneracy, uint32_t *err, uint32_t *rounds,
               uint32_t *solo_sections, cudaStream_t s, double *phase_ms = nullptr);
 

@@ -49,6 +49,8 @@ struct PeelCtl {
   unsigned long long t_scan, t_round, t_wait;  // ns seen by block 0 (diagnostics)
   uint32_t seg_next;   // batches: next graph to peel
   uint32_t seg_part[4];  // ... the same per part of a batch still arriving (peeled concurrently)
+  uint32_t seg_small_next;     // the same for the small graphs' launch
+  uint32_t seg_small_part[4];
 };
 
 namespace {
@@ -652,36 +654,63 @@ __global__ void __launch_bounds__(SEG_BLOCK)
 
 }  // namespace
 
+// 128 threads per small graph (at most PEEL_SMALL_N vertices): sixteen such
+// blocks fit on an SM where three 512-thread blocks with room for 16,384
+// vertices do.
+constexpr int SEG_SMALL_BLOCK = 128;
+
 int peel_segments_launch(const PeelArgs &a, const int64_t *vtx_off, const int64_t *arc_off,
-                         const int32_t *order, int32_t G, cudaStream_t s, int *launches,
-                         int part, int64_t max_n) {
-  int dev = 0, sms = 0, per_sm = 0;
+                         const int32_t *order, int32_t G, int32_t g_big, cudaStream_t s,
+                         const PeelSide &ps, int *launches, int part, int64_t max_n) {
+  int dev = 0, sms = 0;
   MCE_CUDA(cudaGetDevice(&dev));
   MCE_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  // shared state for the launch's largest graph, if it fits (an even count)
-  const int smem_n = max_n <= 0 ? 0 : (int)((std::min<int64_t>(max_n, SEG_SMEM_N) + 1) & ~1);
-  const size_t smem = (size_t)smem_n * 4;  // 2 bytes of degree + 2 of core per vertex
   static bool attr = false;
   if (!attr) {
     MCE_CUDA(cudaFuncSetAttribute(peel_segments_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   SEG_SMEM_N * 4));
     attr = true;
   }
-  MCE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, peel_segments_kernel, SEG_BLOCK,
-                                                         smem));
-  if (per_sm < 1) return MCE_ECUDA;
+  if (part >= 4) return MCE_EINVAL;
+  if (g_big < 0 || g_big > G) return MCE_EINVAL;
   PeelCtl *ctl = (PeelCtl *)a.ctl;
   if (part < 0) MCE_CUDA(cudaMemsetAsync(ctl, 0, sizeof(PeelCtl), s));
-  if (part >= 4) return MCE_EINVAL;
-  uint32_t *next = part < 0 ? &ctl->seg_next : &ctl->seg_part[part];
-  int blocks = sms * per_sm;
-  if (blocks > G) blocks = G;
-  if (blocks < 1) return MCE_OK;
-  peel_segments_kernel<<<blocks, SEG_BLOCK, smem, s>>>(a.rp, a.col, a.deg, a.core, a.prio,
-                                                       a.front0, a.front1, vtx_off, arc_off, order,
-                                                       G, ctl, next, smem_n);
-  MCE_CUDA(cudaGetLastError());
-  if (launches) *launches += 1;
+  // one launch: `cnt` graphs of order[first..], blocks of `threads`, shared
+  // state for graphs of up to `nmax` vertices
+  auto launch = [&](int32_t first, int32_t cnt, int threads, int64_t nmax, uint32_t *next,
+                    cudaStream_t st) -> int {
+    if (cnt <= 0) return MCE_OK;
+    const int smem_n = nmax <= 0 ? 0 : (int)((std::min<int64_t>(nmax, SEG_SMEM_N) + 1) & ~1);
+    const size_t smem = (size_t)smem_n * 4;  // 2 bytes of degree + 2 of core per vertex
+    int per_sm = 0;
+    MCE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, peel_segments_kernel, threads,
+                                                           smem));
+    if (per_sm < 1) return MCE_ECUDA;
+    int blocks = sms * per_sm;
+    if (blocks > cnt) blocks = cnt;
+    peel_segments_kernel<<<blocks, threads, smem, st>>>(a.rp, a.col, a.deg, a.core, a.prio,
+                                                        a.front0, a.front1, vtx_off, arc_off,
+                                                        order + first, cnt, ctl, next, smem_n);
+    MCE_CUDA(cudaGetLastError());
+    if (launches) *launches += 1;
+    return MCE_OK;
+  };
+  uint32_t *next_big = part < 0 ? &ctl->seg_next : &ctl->seg_part[part];
+  uint32_t *next_small = part < 0 ? &ctl->seg_small_next : &ctl->seg_small_part[part];
+  const bool fork = ps.side && ps.fork && ps.join && G > g_big;
+  if (fork) {
+    MCE_CUDA(cudaEventRecord(ps.fork, s));
+    MCE_CUDA(cudaStreamWaitEvent(ps.side, ps.fork, 0));
+  }
+  int rc = launch(0, g_big, SEG_BLOCK, max_n, next_big, s);
+  if (rc) return rc;
+  rc = launch(g_big, G - g_big, SEG_SMALL_BLOCK, std::min<int64_t>(max_n, PEEL_SMALL_N),
+              next_small, fork ? ps.side : s);
+  if (rc) return rc;
+  if (fork) {
+    MCE_CUDA(cudaEventRecord(ps.join, ps.side));
+    MCE_CUDA(cudaStreamWaitEvent(s, ps.join, 0));
+  }
   return MCE_OK;
 }
 
