@@ -410,6 +410,8 @@ def run_mine(args, rank, world, local_rank):
             dg.reload_ptr(rp_h.data_ptr(), col_h.data_ptr(), g.n, g.m, stream=sptr)
             return dg.count(stream=sptr, **kw)
         d2h = 0
+    for _ in range(args.warmup):  # the end-to-end path's own warm-up (its first allocations)
+        run_e2e()
     barrier()
     e2e_times, re2e = timed(stream, flush, run_e2e, args.steps)
     assert re2e.total == total
@@ -484,6 +486,7 @@ def run_mine(args, rank, world, local_rank):
                 "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h + 8 * 4096 + 64 + 8 + 4 + 128),
                 "ms_per_step": e2e_ms, "path": e2e_path,
+                "ms_steps": [round(t, 3) for t in e2e_times],
                 "h2d_copy_gbs": round(h2d_gbs, 2),
                 "copy_bound_ms": round(h2d / h2d_gbs / 1e6, 3)},
         "gpu_launches": int(sum(s_["kernel_launches"] for s_ in stats)),

@@ -98,16 +98,12 @@ struct mce_graph {
   cudaStream_t seg_side[5] = {nullptr};
   cudaEvent_t seg_fork[5] = {nullptr}, seg_join[5] = {nullptr};
   // a batch searched part by part as it arrives (mce_batch_count_host):
-  // per part its roots' summary (device and pinned host), root fetch
-  // counters, sort scratch and hub rows
+  // per part its roots' summary and its search's (device and pinned host),
+  // root fetch counters and sort scratch; the same for the deferred search
   ShapeInfo *part_shape = nullptr, *part_shape_h = nullptr;
   uint32_t *part_fetch = nullptr;
   void *part_tmp[4] = {nullptr};
   size_t part_tmp_bytes[4] = {0};
-  int64_t *phub_off[4] = {nullptr};
-  int32_t *phub_nx[4] = {nullptr};
-  unsigned long long *phub_rows[4] = {nullptr};
-  int64_t phub_off_cap[4] = {0}, phub_rows_cap[4] = {0};
   // search launches captured as a CUDA graph, replayed while the key matches
   cudaGraphExec_t search_exec = nullptr;
   unsigned char search_key[320] = {0};
@@ -584,9 +580,6 @@ int mce_graph_free(mce_graph_t g) {
   if (g->part_shape_h) cudaFreeHost(g->part_shape_h);
   for (int p = 0; p < 4; ++p) {
     dfree(g->part_tmp[p]);
-    dfree(g->phub_off[p]);
-    dfree(g->phub_nx[p]);
-    dfree(g->phub_rows[p]);
   }
   for (int p = 0; p < 4; ++p) {
     if (g->part_s[p]) cudaStreamDestroy(g->part_s[p]);
@@ -1094,10 +1087,12 @@ int count_pipelined(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t
   int launches = 0, rc = MCE_OK;
   mce_stats_t st;
   std::memset(&st, 0, sizeof(st));
-  if (!g->part_shape && (rc = dalloc(&g->part_shape, MAX_PARTS))) return rc;
-  if (!g->part_fetch && (rc = dalloc(&g->part_fetch, 8 * MAX_PARTS))) return rc;
+  // part shapes: [0, MAX_PARTS) the parts', [MAX_PARTS, 2 MAX_PARTS) their searches',
+  // [2 MAX_PARTS] the deferred roots'
+  if (!g->part_shape && (rc = dalloc(&g->part_shape, 2 * MAX_PARTS + 1))) return rc;
+  if (!g->part_fetch && (rc = dalloc(&g->part_fetch, 8 * (MAX_PARTS + 1)))) return rc;
   if (!g->part_shape_h &&
-      cudaHostAlloc((void **)&g->part_shape_h, sizeof(ShapeInfo) * MAX_PARTS,
+      cudaHostAlloc((void **)&g->part_shape_h, sizeof(ShapeInfo) * (2 * MAX_PARTS + 1),
                     cudaHostAllocDefault) != cudaSuccess)
     return MCE_ENOMEM;
   for (int p = 0; p < P.k; ++p) {
@@ -1118,7 +1113,7 @@ int count_pipelined(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t
   const float heavy = (float)(o.heavy_log2 > 0 ? o.heavy_log2 : DEFAULT_HEAVY_LOG2);
   MCE_CUDA(cudaEventRecord(g->ev[0], s));
   MCE_CUDA(cudaMemsetAsync(g->peel_ctl, 0, peel_ctl_bytes(), s));
-  MCE_CUDA(cudaMemsetAsync(g->part_fetch, 0, sizeof(uint32_t) * 8 * MAX_PARTS, s));
+  MCE_CUDA(cudaMemsetAsync(g->part_fetch, 0, sizeof(uint32_t) * 8 * (MAX_PARTS + 1), s));
   MCE_CUDA(cudaMemsetAsync(bc->graph_count, 0, sizeof(unsigned long long) * bc->G, s));
   MCE_CUDA(cudaMemsetAsync(g->err, 0, sizeof(uint32_t) * 4, s));
   MCE_CUDA(cudaMemsetAsync(g->hist, 0, sizeof(unsigned long long) * MCE_HIST_MAX, s));
@@ -1155,20 +1150,109 @@ int count_pipelined(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t
     oa.long_list = reinterpret_cast<int32_t *>(g->keys_out) + vbeg;
     if ((rc = orient_launch(oa, sp, &launches))) return finish(rc);
     const int64_t np = vend - vbeg;
-    if (degree && np > 0 &&
-        (rc = rekey_launch(np, g->keys_in + vbeg, nullptr, g->rp + vbeg, g->split + vbeg, nullptr,
-                           heavy, heavy, g->sms, sp, &launches)))
+    // keys: class, hubs first, then (degree order) the cost; vertex order
+    // within a key (plain order: no cost)
+    if (np > 0 && (rc = rekey_launch(np, g->keys_in + vbeg, nullptr, g->rp + vbeg,
+                                     g->split + vbeg, nullptr, degree ? heavy : 1e30f,
+                                     degree ? heavy : 1e30f, g->sms, sp, &launches, 0,
+                                     g->hub_of + vbeg)))
       return finish(rc);
     if ((rc = roots_sort(np, g->keys_in + vbeg, g->keys_out + vbeg, g->vals_in + vbeg,
-                         g->roots + vbeg, degree ? 32 : 3, &g->part_tmp[p], &g->part_tmp_bytes[p],
+                         g->roots + vbeg, 32, &g->part_tmp[p], &g->part_tmp_bytes[p],
                          g->part_shape + p, sp, &launches)))
       return finish(rc);
     MCE_CUDA(cudaMemcpyAsync(g->part_shape_h + p, g->part_shape + p, sizeof(ShapeInfo),
                              cudaMemcpyDeviceToHost, sp));
     MCE_CUDA(cudaEventRecord(g->part_done[p], sp));
   }
-  // each part's search, in order, on the call's stream
+  // The searches, in order on the call's stream.  As each part lands, its
+  // 32-bit roots without hub rows are searched (most of the work).  Every
+  // other root - the hubs of all classes, the 64-bit and wide classes, whose
+  // largest trees set a launch's tail - waits for one search at the end,
+  // with one hub table built over all parts: one tail instead of one per part.
   uint32_t err_limit = 0;
+  const bool share_q = share;
+  const int wbits = o.bitmap_width == 64 ? 64 : 32;
+  ShapeInfo *sh_search = g->part_shape + MAX_PARTS;   // [MAX_PARTS]: per-part searches
+  ShapeInfo *sh_final = g->part_shape + 2 * MAX_PARTS;
+  ShapeInfo *hs_search = g->part_shape_h + MAX_PARTS;
+  ShapeInfo *hs_final = g->part_shape_h + 2 * MAX_PARTS;
+  struct Seg {
+    int64_t at, cnt;
+  };
+  std::vector<Seg> defer[3];  // by class: R32 hubs, R64, MEM (offsets into g->roots)
+  std::vector<Seg> hubsegs;   // the parts' hub lists (offsets into g->hub_list)
+  uint64_t hub_rows_total = 0;
+  uint32_t mx_dplus = 0, mx_dm_mem = 0, mx_dm_reg = 0, mx_deg = 0;
+  // grid, slab and queue of one class launch; returns MCE_OK or an error
+  auto plan = [&](int c, int64_t roots, int dcap, int xcap, int rxcap, int *grid, int *block,
+                  int *smem, int *parts_c, int *dmin_c, int *dafter_c, QueueView *qv) -> int {
+    int r;
+    const int w = o.bucket_warps_per_root[c] ? o.bucket_warps_per_root[c] : o.warps_per_root;
+    *parts_c = w > 1 && o.level != MCE_LEVEL_L2 ? w : 1;
+    const int t = o.bucket_donate_threshold[c] ? o.bucket_donate_threshold[c] : o.donate_threshold;
+    *dmin_c = t > 0 ? t : DEFAULT_DONATE_MIN;
+    const int af = o.bucket_donate_after[c] ? o.bucket_donate_after[c] : o.donate_after;
+    *dafter_c = af > 0 ? af : (int)DEFAULT_DONATE_AFTER;
+    int warps = 0;
+    if ((r = bk_warps_for_class(c, g->sms, o.wide_blocks, &warps, block, smem))) return r;
+    const int wpb = *block / 32;
+    int64_t want = roots * *parts_c;
+    if (share_q) want = want > warps ? want : warps;
+    if (want < warps) warps = (int)((want + wpb - 1) / wpb) * wpb;
+    *grid = warps / wpb;
+    const size_t need = (size_t)warps * bk_slab_words(c, dcap, xcap, rxcap) * 8;
+    if (need > g->slab_bytes) {  // earlier searches of the call keep the old slab
+      if (g->slab) retired.push_back(g->slab);
+      g->slab = nullptr;
+      g->slab_bytes = 0;
+      MCE_CUDA(cudaMalloc((void **)&g->slab, need));
+      g->slab_bytes = need;
+    }
+    if (share_q) {
+      const uint32_t words = bk_task_words(c, dcap);
+      const size_t qneed = 256 + (size_t)QUEUE_CAP * 4 + (size_t)QUEUE_CAP * words * 8;
+      if (qneed > g->qbytes[c] && g->qbuf[c]) {  // ensure_queue would free it in use
+        retired.push_back(g->qbuf[c]);
+        g->qbuf[c] = nullptr;
+        g->qbytes[c] = 0;
+      }
+      if ((r = ensure_queue(g, c, words, qv))) return r;
+    }
+    return MCE_OK;
+  };
+  auto base_args = [&](BKArgs &a, int dcap, int xcap, int rxcap) {
+    std::memset(&a, 0, sizeof(a));
+    a.rp = g->rp;
+    a.split = g->split;
+    a.cs = g->cs;
+    a.hist = g->hist;
+    a.nodes = g->nodes;
+    a.graph_of = bc->graph_of;
+    a.graph_count = bc->graph_count;
+    a.err = g->err;
+    a.dcap = dcap;
+    a.xcap = xcap;
+    a.rxcap = rxcap;
+    a.wait_limit_ns = o.wait_limit_ms > 0 ? (uint64_t)o.wait_limit_ms * 1000000ull : IDLE_LIMIT_NS;
+    a.wide8 = o.wide_blocks == 8 ? 1 : 0;
+    a.level2 = o.level == MCE_LEVEL_L2 ? 1 : 0;
+    a.prio = g->prio;
+    a.x_pivot = (o.x_pivot || o.induced == MCE_INDUCED_PX) ? 1 : 0;
+    a.stage = o.stage_lists ? 1 : 0;
+  };
+  auto run_class = [&](int c, BKArgs &a, int grid, int block, int smem, int parts_c, int dmin_c,
+                       int dafter_c, const QueueView &qv, int dcap, int xcap, int rxcap) -> int {
+    int r;
+    a.slab = g->slab;  // after plan(): the slab may have grown
+    a.slab_words = bk_slab_words(c, dcap, xcap, rxcap);
+    a.parts = parts_c;
+    a.donate_min = dmin_c;
+    a.donate_after = (uint32_t)dafter_c;
+    a.q = share_q ? qv : QueueView();
+    if (share_q && (r = queue_launch_init(a.q, s, &launches))) return r;
+    return bk_launch(c, wbits, a, grid, block, smem, s, &launches);
+  };
   for (int p = 0; p < P.k; ++p) {
     MCE_CUDA(cudaEventSynchronize(g->part_done[p]));
     const ShapeInfo sh = g->part_shape_h[p];
@@ -1179,120 +1263,127 @@ int count_pipelined(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t
       break;
     }
     const int64_t vbeg = vb[p];
-    if (sh.hub_cnt > 0) {
-      const int64_t need_off = (int64_t)sh.hub_cnt + 2, need_rows = (int64_t)sh.hub_rows;
-      if (need_off > g->phub_off_cap[p]) {
-        if (g->phub_off[p]) retired.push_back(g->phub_off[p]);
-        if (g->phub_nx[p]) retired.push_back(g->phub_nx[p]);
-        g->phub_off[p] = nullptr;
-        g->phub_nx[p] = nullptr;
-        g->phub_off_cap[p] = 0;
-        if ((rc = dalloc(&g->phub_off[p], (size_t)need_off)) ||
-            (rc = dalloc(&g->phub_nx[p], (size_t)need_off)))
-          return finish(rc);
-        g->phub_off_cap[p] = need_off;
-      }
-      if (need_rows > g->phub_rows_cap[p]) {
-        if (g->phub_rows[p]) retired.push_back(g->phub_rows[p]);
-        g->phub_rows[p] = nullptr;
-        g->phub_rows_cap[p] = 0;
-        if ((rc = dalloc(&g->phub_rows[p], (size_t)need_rows))) return finish(rc);
-        g->phub_rows_cap[p] = need_rows;
-      }
-      if ((rc = hub_rows_launch(g->rp, g->split, g->cs, g->hub_list + vbeg, sh.hub_cnt, need_rows,
-                                g->phub_off[p], g->phub_nx[p], g->phub_rows[p], g->sms, s,
-                                &launches)))
-        return finish(rc);
-    }
-    int grid[NCLS] = {0}, block[NCLS] = {0}, smem[NCLS] = {0};
-    const int dcap = (int)(sh.max_dplus > 0 ? sh.max_dplus : 1);
-    const int xcap = (int)(sh.max_dminus_mem > 0 ? sh.max_dminus_mem : 1);
-    int rxcap = REG_XCAP;
-    while (rxcap < (int)sh.max_dminus_reg && rxcap < REG_XCAP_MAX) rxcap <<= 1;
-    int parts[NCLS] = {1, 1, 1, 1, 1}, dmin[NCLS] = {0}, dafter[NCLS] = {0};
-    size_t slab_need = 0;
-    for (int c = CLS_R32; c <= CLS_MEM; ++c) {
-      const int w = o.bucket_warps_per_root[c] ? o.bucket_warps_per_root[c] : o.warps_per_root;
-      parts[c] = w > 1 && o.level != MCE_LEVEL_L2 ? w : 1;
-      const int t = o.bucket_donate_threshold[c] ? o.bucket_donate_threshold[c]
-                                                 : o.donate_threshold;
-      dmin[c] = t > 0 ? t : DEFAULT_DONATE_MIN;
-      const int af = o.bucket_donate_after[c] ? o.bucket_donate_after[c] : o.donate_after;
-      dafter[c] = af > 0 ? af : (int)DEFAULT_DONATE_AFTER;
-      if (!sh.cls_cnt[c]) continue;
-      int warps = 0;
-      if ((rc = bk_warps_for_class(c, g->sms, o.wide_blocks, &warps, &block[c], &smem[c])))
-        return finish(rc);
-      const int wpb = block[c] / 32;
-      int64_t want = (int64_t)sh.cls_cnt[c] * parts[c];
-      if (share) want = want > warps ? want : warps;
-      if (want < warps) warps = (int)((want + wpb - 1) / wpb) * wpb;
-      grid[c] = warps / wpb;
-      const size_t need = (size_t)warps * bk_slab_words(c, dcap, xcap, rxcap) * 8;
-      if (need > slab_need) slab_need = need;
-    }
-    if (slab_need > g->slab_bytes) {  // the earlier parts' searches keep the old slab
-      if (g->slab) retired.push_back(g->slab);
-      g->slab = nullptr;
-      g->slab_bytes = 0;
-      MCE_CUDA(cudaMalloc((void **)&g->slab, slab_need));
-      g->slab_bytes = slab_need;
-    }
-    QueueView qv[NCLS];
-    for (int c = CLS_R32; c <= CLS_MEM; ++c) {
-      if (!share || !grid[c]) continue;
-      const uint32_t words = bk_task_words(c, dcap);
-      const size_t need = 256 + (size_t)QUEUE_CAP * 4 + (size_t)QUEUE_CAP * words * 8;
-      if (need > g->qbytes[c] && g->qbuf[c]) {  // ensure_queue would free it in use
-        retired.push_back(g->qbuf[c]);
-        g->qbuf[c] = nullptr;
-        g->qbytes[c] = 0;
-      }
-      if ((rc = ensure_queue(g, c, words, &qv[c]))) return finish(rc);
-    }
-    BKArgs a;
-    std::memset(&a, 0, sizeof(a));
-    a.rp = g->rp;
-    a.split = g->split;
-    a.cs = g->cs;
-    a.roots = g->roots + vbeg;
-    a.shape = g->part_shape + p;
-    a.fetch = g->part_fetch + 8 * p;
-    a.hist = g->hist;
-    a.nodes = g->nodes;
-    a.graph_of = bc->graph_of;
-    a.graph_count = bc->graph_count;
-    a.err = g->err;
-    a.slab = g->slab;
-    a.dcap = dcap;
-    a.xcap = xcap;
-    a.rxcap = rxcap;
-    a.hub_of = sh.hub_cnt > 0 ? g->hub_of : nullptr;
-    a.hub_off = g->phub_off[p];
-    a.hub_rows = g->phub_rows[p];
-    a.hub_nx = g->phub_nx[p];
-    a.wait_limit_ns = o.wait_limit_ms > 0 ? (uint64_t)o.wait_limit_ms * 1000000ull : IDLE_LIMIT_NS;
-    a.wide8 = o.wide_blocks == 8 ? 1 : 0;
-    a.level2 = o.level == MCE_LEVEL_L2 ? 1 : 0;
-    a.prio = g->prio;
-    a.x_pivot = (o.x_pivot || o.induced == MCE_INDUCED_PX) ? 1 : 0;
-    a.stage = o.stage_lists ? 1 : 0;
-    const int wbits = o.bitmap_width == 64 ? 64 : 32;
-    for (int c : {CLS_MEM, CLS_R64, CLS_R32}) {
-      if (!grid[c]) continue;
-      a.slab_words = bk_slab_words(c, dcap, xcap, rxcap);
-      a.parts = parts[c];
-      a.donate_min = dmin[c];
-      a.donate_after = (uint32_t)dafter[c];
-      a.q = share ? qv[c] : QueueView();
-      if (share && (rc = queue_launch_init(a.q, s, &launches))) return finish(rc);
-      if ((rc = bk_launch(c, wbits, a, grid[c], block[c], smem[c], s, &launches)))
-        return finish(rc);
-    }
+    // roots of the part, class-sorted, hubs first within a class
+    const int64_t n32 = (int64_t)sh.cls_cnt[CLS_R32] - sh.hub_r32;
+    defer[0].push_back({vbeg + sh.cls_off[CLS_R32], (int64_t)sh.hub_r32});
+    defer[1].push_back({vbeg + sh.cls_off[CLS_R64], (int64_t)sh.cls_cnt[CLS_R64]});
+    defer[2].push_back({vbeg + sh.cls_off[CLS_MEM], (int64_t)sh.cls_cnt[CLS_MEM]});
+    hubsegs.push_back({vbeg, (int64_t)sh.hub_cnt});
+    hub_rows_total += sh.hub_rows;
+    mx_dplus = std::max(mx_dplus, sh.max_dplus);
+    mx_dm_mem = std::max(mx_dm_mem, sh.max_dminus_mem);
+    mx_dm_reg = std::max(mx_dm_reg, sh.max_dminus_reg);
+    mx_deg = std::max(mx_deg, sh.max_deg);
     st.roots += (int64_t)sh.cls_cnt[CLS_R32] + sh.cls_cnt[CLS_R64] + sh.cls_cnt[CLS_MEM];
     for (int c = 0; c < NCLS && c < 8; ++c) st.class_roots[c] += sh.cls_cnt[c];
     if ((int32_t)sh.max_dplus > st.max_later_degree) st.max_later_degree = (int32_t)sh.max_dplus;
     if ((int64_t)sh.max_deg > st.max_degree) st.max_degree = sh.max_deg;
+    if (n32 <= 0) continue;
+    // the part's 32-bit roots after its hubs: earlier degree <= HUB_XMIN, no hub rows
+    ShapeInfo ss{};
+    for (int c = 1; c < 9; ++c) ss.cls_off[c] = (uint32_t)n32;
+    ss.cls_cnt[CLS_R32] = (uint32_t)n32;
+    hs_search[p] = ss;
+    MCE_CUDA(cudaMemcpyAsync(sh_search + p, hs_search + p, sizeof(ShapeInfo),
+                             cudaMemcpyHostToDevice, s));
+    const int dcap = 32, xcap = 1, rxcap = REG_XCAP;
+    int grid = 0, block = 0, smem = 0, pc = 1, dm = 0, da = 0;
+    QueueView qv;
+    if ((rc = plan(CLS_R32, n32, dcap, xcap, rxcap, &grid, &block, &smem, &pc, &dm, &da, &qv)))
+      return finish(rc);
+    BKArgs a;
+    base_args(a, dcap, xcap, rxcap);
+    a.roots = g->roots + vbeg + sh.cls_off[CLS_R32] + sh.hub_r32;
+    a.shape = sh_search + p;
+    a.fetch = g->part_fetch + 8 * p;
+    if ((rc = run_class(CLS_R32, a, grid, block, smem, pc, dm, da, qv, dcap, xcap, rxcap)))
+      return finish(rc);
+  }
+  // the deferred roots of every part: one list (R32 hubs, R64, MEM) in the
+  // sort's key buffer and one hub list in its value buffer, both free now
+  int64_t ncls[3] = {0, 0, 0};
+  int32_t *dlist = reinterpret_cast<int32_t *>(g->keys_out);
+  int32_t *hlist = g->vals_in;
+  if (!err_limit) {
+    int64_t at = 0;
+    for (int c = 0; c < 3; ++c)
+      for (const Seg &sg : defer[c]) {
+        if (sg.cnt > 0)
+          MCE_CUDA(cudaMemcpyAsync(dlist + at, g->roots + sg.at, sizeof(int32_t) * (size_t)sg.cnt,
+                                   cudaMemcpyDeviceToDevice, s));
+        at += sg.cnt;
+        ncls[c] += sg.cnt;
+      }
+    int64_t nh = 0;
+    for (const Seg &sg : hubsegs) {
+      if (sg.cnt > 0)
+        MCE_CUDA(cudaMemcpyAsync(hlist + nh, g->hub_list + sg.at, sizeof(int32_t) * (size_t)sg.cnt,
+                                 cudaMemcpyDeviceToDevice, s));
+      nh += sg.cnt;
+    }
+    if (nh > 0) {
+      if ((rc = hub_index_launch(hlist, (uint32_t)nh, g->hub_of, s, &launches))) return finish(rc);
+      const int64_t need_off = nh + 2, need_rows = (int64_t)hub_rows_total;
+      if (need_off > g->hub_off_cap) {
+        if (g->hub_off) retired.push_back(g->hub_off);
+        if (g->hub_nx) retired.push_back(g->hub_nx);
+        g->hub_off = nullptr;
+        g->hub_nx = nullptr;
+        g->hub_off_cap = 0;
+        if ((rc = dalloc(&g->hub_off, (size_t)need_off)) ||
+            (rc = dalloc(&g->hub_nx, (size_t)need_off)))
+          return finish(rc);
+        g->hub_off_cap = need_off;
+      }
+      if (need_rows > g->hub_rows_cap) {
+        if (g->hub_rows) retired.push_back(g->hub_rows);
+        g->hub_rows = nullptr;
+        g->hub_rows_cap = 0;
+        if ((rc = dalloc(&g->hub_rows, (size_t)need_rows))) return finish(rc);
+        g->hub_rows_cap = need_rows;
+      }
+      if ((rc = hub_rows_launch(g->rp, g->split, g->cs, hlist, (uint32_t)nh, need_rows,
+                                g->hub_off, g->hub_nx, g->hub_rows, g->sms, s, &launches)))
+        return finish(rc);
+    }
+    const int64_t nd = ncls[0] + ncls[1] + ncls[2];
+    if (nd > 0) {
+      ShapeInfo fs{};
+      fs.cls_cnt[CLS_R32] = (uint32_t)ncls[0];
+      fs.cls_cnt[CLS_R64] = (uint32_t)ncls[1];
+      fs.cls_cnt[CLS_MEM] = (uint32_t)ncls[2];
+      fs.cls_off[CLS_R32] = 0;
+      fs.cls_off[CLS_R64] = (uint32_t)ncls[0];
+      fs.cls_off[CLS_MEM] = (uint32_t)(ncls[0] + ncls[1]);
+      for (int c = CLS_MEM + 1; c < 9; ++c) fs.cls_off[c] = (uint32_t)nd;
+      hs_final[0] = fs;
+      MCE_CUDA(cudaMemcpyAsync(sh_final, hs_final, sizeof(ShapeInfo), cudaMemcpyHostToDevice, s));
+      const int dcap = (int)(mx_dplus > 0 ? mx_dplus : 1);
+      const int xcap = (int)(mx_dm_mem > 0 ? mx_dm_mem : 1);
+      int rxcap = REG_XCAP;
+      while (rxcap < (int)mx_dm_reg && rxcap < REG_XCAP_MAX) rxcap <<= 1;
+      const int cls_of[3] = {CLS_R32, CLS_R64, CLS_MEM};
+      int grid[3] = {0}, block[3] = {0}, smem[3] = {0}, pc[3] = {1, 1, 1}, dm[3] = {0},
+          da[3] = {0};
+      QueueView qv[3];
+      for (int i = 0; i < 3; ++i)
+        if (ncls[i] > 0 && (rc = plan(cls_of[i], ncls[i], dcap, xcap, rxcap, &grid[i], &block[i],
+                                      &smem[i], &pc[i], &dm[i], &da[i], &qv[i])))
+          return finish(rc);
+      BKArgs a;
+      base_args(a, dcap, xcap, rxcap);
+      a.roots = dlist;
+      a.shape = sh_final;
+      a.fetch = g->part_fetch + 8 * MAX_PARTS;
+      a.hub_of = nh > 0 ? g->hub_of : nullptr;
+      a.hub_off = g->hub_off;
+      a.hub_rows = g->hub_rows;
+      a.hub_nx = g->hub_nx;
+      for (int i : {2, 1, 0})  // wide, 64-bit, then the 32-bit hubs
+        if (ncls[i] > 0 && (rc = run_class(cls_of[i], a, grid[i], block[i], smem[i], pc[i], dm[i],
+                                           da[i], qv[i], dcap, xcap, rxcap)))
+          return finish(rc);
+    }
   }
   MCE_CUDA(cudaEventRecord(g->ev[3], s));
   unsigned long long h_hist[MCE_HIST_MAX];

@@ -486,6 +486,23 @@ __global__ void __launch_bounds__(HUB_BLOCK) hub_rows_kernel(
 }  // namespace
 
 
+namespace {
+__global__ void hub_index_kernel(const int32_t *__restrict__ list, uint32_t cnt, int32_t *hub_of) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x)
+    hub_of[list[i]] = (int32_t)i;
+}
+}  // namespace
+
+int hub_index_launch(const int32_t *list, uint32_t cnt, int32_t *hub_of, cudaStream_t s,
+                     int *launches) {
+  if (cnt == 0) return MCE_OK;
+  hub_index_kernel<<<(cnt + 255) / 256 < 1184 ? (cnt + 255) / 256 : 1184, 256, 0, s>>>(list, cnt,
+                                                                                   hub_of);
+  MCE_CUDA(cudaGetLastError());
+  if (launches) *launches += 1;
+  return MCE_OK;
+}
+
 int hub_rows_launch(const int32_t *rp, const int32_t *split, const int32_t *cs,
                     const int32_t *hub_list, uint32_t cnt, int64_t total_rows, int64_t *off,
                     int32_t *nx, unsigned long long *rows, int sms, cudaStream_t s,

@@ -76,7 +76,7 @@ struct ShapeInfo {
   uint32_t max_deg;
   uint32_t max_dminus_reg; // over roots of CLS_R32 and CLS_R64
   uint32_t hub_cnt;        // register-class roots with d- > HUB_XMIN
-  uint32_t pad;
+  uint32_t hub_r32;        // ... of them in CLS_R32
   unsigned long long hub_rows;  // their earlier degrees, each rounded up to 32
 };
 
@@ -106,6 +106,10 @@ int orient_launch(const OrientArgs &a, cudaStream_t s, int *launches);
 // off[j] = first row of hub j (rows padded to 32 per hub), rows[k] = the
 // bitmap over the hub's later list of one earlier neighbour's later list.
 // nx[j] = -1: hub j's distinct rows are not known yet (the search sets it).
+// hub_of[list[i]] = i for the cnt hubs of `list` (one hub numbering for
+// hub lists gathered from several parts of a batch).
+int hub_index_launch(const int32_t *list, uint32_t cnt, int32_t *hub_of, cudaStream_t s,
+                     int *launches);
 int hub_rows_launch(const int32_t *rp, const int32_t *split, const int32_t *cs,
                     const int32_t *hub_list, uint32_t cnt, int64_t total_rows, int64_t *off,
                     int32_t *nx, unsigned long long *rows, int sms, cudaStream_t s,
@@ -191,9 +195,12 @@ int mlp_adam_launch(float *master, void *wh, float *grad, float *m1, float *m2, 
                     int step, cudaStream_t s);
 // Sort keys by cost: with `cost`, roots with at least cost_min later
 // neighbours take it and the others the degree heuristic.
+// hub_of (nullable, the same n vertices): hub roots sort before the other
+// roots of their class (key bit 27; the cost keeps 27 bits).
 int rekey_launch(int64_t n, uint32_t *keys, const float *cost, const int32_t *rp,
                  const int32_t *split, uint8_t *policy, float heavy_cost, float share_cost,
-                 int sms, cudaStream_t s, int *launches, int cost_min = 0);
+                 int sms, cudaStream_t s, int *launches, int cost_min = 0,
+                 const int32_t *hub_of = nullptr);
 
 // ---- batches ------------------------------------------------------------------
 int batch_rebase_launch(const int32_t *rp_local, const int32_t *col_local,

@@ -313,7 +313,8 @@ __global__ void adam_kernel(float *__restrict__ master, __half *__restrict__ wh,
 // prediction and the others the degree heuristic.
 __global__ void rekey_kernel(int64_t n, uint32_t *keys, const float *__restrict__ cost,
                              const int32_t *__restrict__ rp, const int32_t *__restrict__ split,
-                             uint8_t *policy, float heavy_cost, float share_cost, int cost_min) {
+                             uint8_t *policy, float heavy_cost, float share_cost, int cost_min,
+                             const int32_t *__restrict__ hub_of) {
   for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n;
        v += (int64_t)gridDim.x * blockDim.x) {
     const uint32_t cls = keys[v] & 0xF;
@@ -329,7 +330,10 @@ __global__ void rekey_kernel(int64_t n, uint32_t *keys, const float *__restrict_
     c = c < 0.f ? 0.f : (c > 63.f ? 63.f : c);
     const bool heavy = c >= heavy_cost;
     const uint32_t q = heavy ? (uint32_t)(c * (float)(1 << 22)) : 0u;  // < 2^28
-    keys[v] = (cls << 28) | (0x0FFFFFFFu - q);
+    if (hub_of)  // hubs first within the class, then the cost in 27 bits
+      keys[v] = (cls << 28) | ((hub_of[v] < 0 ? 1u : 0u) << 27) | (0x07FFFFFFu - (q >> 1));
+    else
+      keys[v] = (cls << 28) | (0x0FFFFFFFu - q);
     if (policy) policy[v] = learned && c >= share_cost ? 1 : 0;
   }
 }
@@ -392,10 +396,10 @@ int mlp_adam_launch(float *master, void *wh, float *grad, float *m1, float *m2, 
 
 int rekey_launch(int64_t n, uint32_t *keys, const float *cost, const int32_t *rp,
                  const int32_t *split, uint8_t *policy, float heavy_cost, float share_cost,
-                 int sms, cudaStream_t s, int *launches, int cost_min) {
+                 int sms, cudaStream_t s, int *launches, int cost_min, const int32_t *hub_of) {
   if (n == 0) return MCE_OK;
   rekey_kernel<<<sms * 8, 256, 0, s>>>(n, keys, cost, rp, split, policy, heavy_cost, share_cost,
-                                       cost_min);
+                                       cost_min, hub_of);
   MCE_CUDA(cudaGetLastError());
   if (launches) *launches += 1;
   return MCE_OK;

@@ -104,6 +104,7 @@ __device__ __forceinline__ uint32_t finish_vertex(const OrientArgs &a, int32_t v
       hi = (int32_t)atomicAdd(&a.shape->hub_cnt, 1u);
       a.hub_list[hi] = v;
       atomicAdd(&a.shape->hub_rows, (unsigned long long)((dminus + 31u) & ~31u));
+      if (cls == CLS_R32) atomicAdd(&a.shape->hub_r32, 1u);
     }
     a.hub_of[v] = hi;
   }
