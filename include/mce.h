@@ -366,13 +366,13 @@ int mce_batch_count(mce_batch_t b, const mce_opts_t *opts, uint64_t *per_graph_t
                     uint64_t *total, uint64_t *hist, mce_stats_t *stats);
 
 /* mce_batch_reload followed by mce_batch_count in one call, for a batch in
- * host memory: batches of 2^20 arcs or more are copied in up to four parts
+ * host memory: batches of 2^20 arcs or more are copied in up to six parts
  * of whole graphs on a stream of the handle's own, and each part is rebased,
  * peeled, oriented and - for counts in plain or degree order without
  * per-root or per-warp logs - its roots with at most 32 later and 256
  * earlier neighbours are searched as soon as it is on the device, while the
- * next parts are still being copied (parts of 1/16, 2/16, 4/16 and 9/16 of
- * the arcs); the other roots of every part (hub roots, wider bitmaps) follow
+ * next parts are still being copied (parts of 3, 5, 8, 12, 16 and 20 64ths
+ * of the arcs); the other roots of every part (hub roots, wider bitmaps) follow
  * in one search.  In the other modes one search over the whole batch follows.
  * Same results as the two calls.  Pinned host memory lets the copies
  * overlap.  In the part-by-part mode stats->peel_ms is the time until the

@@ -91,19 +91,19 @@ struct mce_graph {
   cudaEvent_t cls_ev[3][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};
   // a batch arriving in parts: one stream per part, forked from and joined
   // to the caller's stream
-  cudaStream_t part_s[4] = {nullptr};
-  cudaEvent_t part_fork = nullptr, part_done[4] = {nullptr};
+  cudaStream_t part_s[MAX_BATCH_PARTS] = {nullptr};
+  cudaEvent_t part_fork = nullptr, part_done[MAX_BATCH_PARTS] = {nullptr};
   // a batch's per-graph peel: the small graphs' launch runs on a side stream
   // ([0] whole batch, [1 + p] part p)
-  cudaStream_t seg_side[5] = {nullptr};
-  cudaEvent_t seg_fork[5] = {nullptr}, seg_join[5] = {nullptr};
+  cudaStream_t seg_side[1 + MAX_BATCH_PARTS] = {nullptr};
+  cudaEvent_t seg_fork[1 + MAX_BATCH_PARTS] = {nullptr}, seg_join[1 + MAX_BATCH_PARTS] = {nullptr};
   // a batch searched part by part as it arrives (mce_batch_count_host):
   // per part its roots' summary and its search's (device and pinned host),
   // root fetch counters and sort scratch; the same for the deferred search
   ShapeInfo *part_shape = nullptr, *part_shape_h = nullptr;
   uint32_t *part_fetch = nullptr;
-  void *part_tmp[4] = {nullptr};
-  size_t part_tmp_bytes[4] = {0};
+  void *part_tmp[MAX_BATCH_PARTS] = {nullptr};
+  size_t part_tmp_bytes[MAX_BATCH_PARTS] = {0};
   // search launches captured as a CUDA graph, replayed while the key matches
   cudaGraphExec_t search_exec = nullptr;
   unsigned char search_key[320] = {0};
@@ -119,7 +119,7 @@ constexpr int64_t BATCH_PART_MIN_ARCS = 1 << 20;  // mce_batch_count_host: small
 constexpr uint32_t DEFAULT_SOLO_MAX = 0;     // measured slower than grid-wide rounds
 constexpr uint32_t DEFAULT_DONATE_AFTER = 256;  // the reference's SZTH (mce/parameter.cuh:5)
 
-constexpr int MAX_PARTS = 4;  // a host batch is copied and prepared in at most this many parts
+constexpr int MAX_PARTS = MAX_BATCH_PARTS;
 
 void free_graph_bufs(mce_graph *g) {
   dfree(g->rp); dfree(g->col); dfree(g->cs); dfree(g->split);
@@ -335,7 +335,6 @@ int run_orient(mce_graph *g, cudaStream_t s, int *launches, bool skip_sort = fal
 // graphs' round chains) overlap; the roots' summary accumulates over them.
 int run_parts(mce_graph *g, cudaStream_t s, int *launches, const BatchCtx *bc, int solo_opt) {
   const BatchParts &P = *bc->parts;
-  static_assert(MAX_PARTS <= 4, "part streams");
   const PeelArgs pa = peel_args(g, solo_opt);
   for (int p = 0; p < P.k; ++p) {
     if (!g->part_s[p]) MCE_CUDA(cudaStreamCreateWithFlags(&g->part_s[p], cudaStreamNonBlocking));
@@ -578,15 +577,15 @@ int mce_graph_free(mce_graph_t g) {
   dfree(g->part_shape);
   dfree(g->part_fetch);
   if (g->part_shape_h) cudaFreeHost(g->part_shape_h);
-  for (int p = 0; p < 4; ++p) {
+  for (int p = 0; p < MAX_PARTS; ++p) {
     dfree(g->part_tmp[p]);
   }
-  for (int p = 0; p < 4; ++p) {
+  for (int p = 0; p < MAX_PARTS; ++p) {
     if (g->part_s[p]) cudaStreamDestroy(g->part_s[p]);
     if (g->part_done[p]) cudaEventDestroy(g->part_done[p]);
   }
   if (g->part_fork) cudaEventDestroy(g->part_fork);
-  for (int i = 0; i < 5; ++i) {
+  for (int i = 0; i < 1 + MAX_PARTS; ++i) {
     if (g->seg_side[i]) cudaStreamDestroy(g->seg_side[i]);
     if (g->seg_fork[i]) cudaEventDestroy(g->seg_fork[i]);
     if (g->seg_join[i]) cudaEventDestroy(g->seg_join[i]);
@@ -1731,13 +1730,15 @@ int mce_batch_count_host(mce_batch_t b, const int32_t *row_ptr, const int32_t *c
   const int32_t G = num_graphs;
   const int64_t *vo = vtx_offsets, *ao = arc_offsets;
   // Parts of whole graphs; small batches in one.  When the parts are
-  // searched as they arrive, they grow geometrically (1/16, 2/16, 4/16, 9/16
-  // of the arcs): the first search starts after a short copy, and since the
-  // copy moves arcs about twice as fast as they are searched, each later
-  // part lands before the search reaches it.  Otherwise they are equal.
+  // searched as they arrive, they grow (3, 5, 8, 12, 16 and 20 64ths of the
+  // arcs): the first search starts after a short copy, and since the copy
+  // moves arcs about 1.5x as fast as the narrow roots are searched, each
+  // part lands (and is prepared) before the search stream reaches it; parts
+  // growing 2x per step left the stream waiting for the last ones.
+  // Otherwise they are equal.
   const bool pipelined = !o.log_roots && !o.warp_log && !o.count_ops &&
                          (o.sched == MCE_SCHED_PLAIN || o.sched == MCE_SCHED_DEGREE);
-  static const int64_t kGeo[MAX_PARTS] = {1, 3, 7, 16};  // cumulative sixteenths
+  static const int64_t kGeo[MAX_PARTS] = {3, 8, 16, 28, 44, 64};  // cumulative 64ths
   int k = m >= BATCH_PART_MIN_ARCS ? MAX_PARTS : 1;
   if (k > G) k = G;
   BatchParts P;
@@ -1745,7 +1746,7 @@ int mce_batch_count_host(mce_batch_t b, const int32_t *row_ptr, const int32_t *c
   P.g[0] = 0;
   for (int p = 1; p < k; ++p) {
     int64_t gp = P.g[P.k];
-    const int64_t want = pipelined && k == MAX_PARTS ? m * kGeo[p - 1] / 16 : m * p / k;
+    const int64_t want = pipelined && k == MAX_PARTS ? m * kGeo[p - 1] / 64 : m * p / k;
     while (gp < G && ao[gp] < want) ++gp;
     if (gp > P.g[P.k] && gp < G) P.g[++P.k] = gp;
   }

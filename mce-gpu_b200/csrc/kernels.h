@@ -35,6 +35,8 @@ int peel_launch(const PeelArgs &a, cudaStream_t s, int *launches);
 // blocks on `side` (forked from s by `fork`, joined back by `join`; all
 // three null: on s after the others), so that more small graphs run at once.
 constexpr int64_t PEEL_SMALL_N = 2048;
+// A host batch is copied, prepared and searched in at most this many parts.
+constexpr int MAX_BATCH_PARTS = 6;
 struct PeelSide {
   cudaStream_t side = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;

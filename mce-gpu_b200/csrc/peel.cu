@@ -48,9 +48,9 @@ struct PeelCtl {
   uint32_t solo_sections;
   unsigned long long t_scan, t_round, t_wait;  // ns seen by block 0 (diagnostics)
   uint32_t seg_next;   // batches: next graph to peel
-  uint32_t seg_part[4];  // ... the same per part of a batch still arriving (peeled concurrently)
+  uint32_t seg_part[MAX_BATCH_PARTS];  // ... the same per part of a batch still arriving
   uint32_t seg_small_next;     // the same for the small graphs' launch
-  uint32_t seg_small_part[4];
+  uint32_t seg_small_part[MAX_BATCH_PARTS];
 };
 
 namespace {
@@ -671,7 +671,7 @@ int peel_segments_launch(const PeelArgs &a, const int64_t *vtx_off, const int64_
                                   SEG_SMEM_N * 4));
     attr = true;
   }
-  if (part >= 4) return MCE_EINVAL;
+  if (part >= MAX_BATCH_PARTS) return MCE_EINVAL;
   if (g_big < 0 || g_big > G) return MCE_EINVAL;
   PeelCtl *ctl = (PeelCtl *)a.ctl;
   if (part < 0) MCE_CUDA(cudaMemsetAsync(ctl, 0, sizeof(PeelCtl), s));

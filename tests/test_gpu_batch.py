@@ -69,7 +69,7 @@ def _count_host(db, b, **kw):
 
 @pytest.mark.parametrize("seed", [3, 4])
 def test_batch_count_host_in_parts(seed):
-    # > 2^20 arcs: copied in four parts, each rebased, peeled and oriented on arrival
+    # > 2^20 arcs: copied in parts, each rebased, peeled and oriented on arrival
     b = mce.gen_chung_lu_batch(160, 64, 8192, 2.3, 8, 32, 5, 5, 40, seed)
     assert b.m >= 1 << 20
     with mce.Batch(b) as db:
