@@ -93,10 +93,11 @@ struct mce_graph {
   // to the caller's stream
   cudaStream_t part_s[MAX_BATCH_PARTS] = {nullptr};
   cudaEvent_t part_fork = nullptr, part_done[MAX_BATCH_PARTS] = {nullptr};
-  // a batch's per-graph peel: the small graphs' launch runs on a side stream
-  // ([0] whole batch, [1 + p] part p)
-  cudaStream_t seg_side[1 + MAX_BATCH_PARTS] = {nullptr};
-  cudaEvent_t seg_fork[1 + MAX_BATCH_PARTS] = {nullptr}, seg_join[1 + MAX_BATCH_PARTS] = {nullptr};
+  // a batch's per-graph peel: the middle and small graphs' launches run on
+  // side streams ([k][0] whole batch, [k][1 + p] part p)
+  cudaStream_t seg_side[2][1 + MAX_BATCH_PARTS] = {{nullptr}};
+  cudaEvent_t seg_fork[1 + MAX_BATCH_PARTS] = {nullptr};
+  cudaEvent_t seg_join[2][1 + MAX_BATCH_PARTS] = {{nullptr}};
   // a batch searched part by part as it arrives (mce_batch_count_host):
   // per part its roots' summary and its search's (device and pinned host),
   // root fetch counters and sort scratch; the same for the deferred search
@@ -184,32 +185,43 @@ struct BatchParts {
 };
 
 // the most vertices of a graph of part p
-// Graphs of part p (or of the whole batch) with more than PEEL_SMALL_N vertices.
-inline int64_t count_big(const int64_t *vo, int64_t g0, int64_t g1) {
-  int64_t k = 0;
-  for (int64_t g = g0; g < g1; ++g) k += vo[g + 1] - vo[g] - 1 > PEEL_SMALL_N;
-  return k;
+// The per-graph peel's size class of a graph of n vertices: 0 more than
+// PEEL_MID_N, 1 more than PEEL_SMALL_N, 2 the rest.
+inline int peel_class(int64_t n) { return n > PEEL_MID_N ? 0 : n > PEEL_SMALL_N ? 1 : 2; }
+
+// Graphs [g0, g1) of the large and middle peel classes.
+inline void count_classes(const int64_t *vo, int64_t g0, int64_t g1, int32_t *big, int32_t *mid) {
+  *big = *mid = 0;
+  for (int64_t g = g0; g < g1; ++g) {
+    const int c = peel_class(vo[g + 1] - vo[g] - 1);
+    *big += c == 0;
+    *mid += c == 1;
+  }
 }
 
-// The per-graph peel's order of graphs [g0, g1): those with more than
-// PEEL_SMALL_N vertices first (their own launch), each set largest first.
+// The per-graph peel's order of graphs [g0, g1): by size class (each class
+// its own launch), each class largest first.
 void order_graphs(int32_t *order, int64_t g0, int64_t g1, const int64_t *vo, const int64_t *ao) {
   std::stable_sort(order + g0, order + g1, [&](int32_t x, int32_t y) {
-    const bool bx = vo[x + 1] - vo[x] - 1 > PEEL_SMALL_N, by = vo[y + 1] - vo[y] - 1 > PEEL_SMALL_N;
-    if (bx != by) return bx;
+    const int cx = peel_class(vo[x + 1] - vo[x] - 1), cy = peel_class(vo[y + 1] - vo[y] - 1);
+    if (cx != cy) return cx < cy;
     return ao[x + 1] - ao[x] > ao[y + 1] - ao[y];
   });
 }
 
-// The side stream and events of a per-graph peel launch (i: 0 whole batch,
+// The side streams and events of a per-graph peel launch (i: 0 whole batch,
 // 1 + p part p), made on first use.
 int seg_side(mce_graph *g, int i, PeelSide *ps) {
-  if (!g->seg_side[i]) MCE_CUDA(cudaStreamCreateWithFlags(&g->seg_side[i], cudaStreamNonBlocking));
+  for (int k = 0; k < 2; ++k) {
+    if (!g->seg_side[k][i])
+      MCE_CUDA(cudaStreamCreateWithFlags(&g->seg_side[k][i], cudaStreamNonBlocking));
+    if (!g->seg_join[k][i])
+      MCE_CUDA(cudaEventCreateWithFlags(&g->seg_join[k][i], cudaEventDisableTiming));
+    ps->side[k] = g->seg_side[k][i];
+    ps->join[k] = g->seg_join[k][i];
+  }
   if (!g->seg_fork[i]) MCE_CUDA(cudaEventCreateWithFlags(&g->seg_fork[i], cudaEventDisableTiming));
-  if (!g->seg_join[i]) MCE_CUDA(cudaEventCreateWithFlags(&g->seg_join[i], cudaEventDisableTiming));
-  ps->side = g->seg_side[i];
   ps->fork = g->seg_fork[i];
-  ps->join = g->seg_join[i];
   return MCE_OK;
 }
 
@@ -231,7 +243,7 @@ struct BatchCtx {
   const int32_t *order;                // device, G: graphs largest first (within each part)
   const BatchParts *parts = nullptr;   // nullable: rebase, peel and orient part by part
   int64_t max_n = 0;                   // the most vertices of a graph (0: unknown)
-  int64_t g_big = 0;                   // graphs of `order` with more than PEEL_SMALL_N vertices
+  int32_t g_big = 0, g_mid = 0;        // graphs of `order` in the large and middle peel classes
 };
 
 int check_args(const int32_t *row_ptr, const int32_t *col, int64_t n, int64_t m) {
@@ -269,7 +281,7 @@ int run_peel(mce_graph *g, cudaStream_t s, int *launches, int solo_opt = 0,
     int rc = seg_side(g, 0, &ps);
     if (rc) return rc;
     return peel_segments_launch(pa, bc->vtx_off, bc->arc_off, bc->order, (int32_t)bc->G,
-                                (int32_t)bc->g_big, s, ps, launches, -1, bc->max_n);
+                                bc->g_big, bc->g_mid, s, ps, launches, -1, bc->max_n);
   }
   return peel_launch(pa, s, launches);
 }
@@ -357,12 +369,16 @@ int run_parts(mce_graph *g, cudaStream_t s, int *launches, const BatchCtx *bc, i
                                       P.ao_h[g1], vend, (int32_t)P.ao_h[g1], g->rp, g->col,
                                       const_cast<int32_t *>(bc->graph_of), g->sms, sp, launches);
     if (rc) return rc;
+    // a part's peel in two launches, its large and middle graphs together:
+    // a third launch per part measured slower end to end (53.1 against 51.3 ms)
     PeelSide ps;
+    int32_t nbig = 0, nmid = 0;
     if ((rc = seg_side(g, 1 + p, &ps))) return rc;
     if (vend > vbeg &&
-        (rc = peel_segments_launch(pa, bc->vtx_off, bc->arc_off, bc->order + g0,
-                                   (int32_t)(g1 - g0), (int32_t)count_big(P.vo_h, g0, g1), sp,
-                                   ps, launches, p, part_max_n(P, p))))
+        (count_classes(P.vo_h, g0, g1, &nbig, &nmid),
+         rc = peel_segments_launch(pa, bc->vtx_off, bc->arc_off, bc->order + g0,
+                                   (int32_t)(g1 - g0), nbig + nmid, 0, sp, ps, launches, p,
+                                   part_max_n(P, p))))
       return rc;
     OrientArgs oa = orient_args(g);
     oa.v0 = vbeg;
@@ -586,9 +602,11 @@ int mce_graph_free(mce_graph_t g) {
   }
   if (g->part_fork) cudaEventDestroy(g->part_fork);
   for (int i = 0; i < 1 + MAX_PARTS; ++i) {
-    if (g->seg_side[i]) cudaStreamDestroy(g->seg_side[i]);
+    for (int k = 0; k < 2; ++k) {
+      if (g->seg_side[k][i]) cudaStreamDestroy(g->seg_side[k][i]);
+      if (g->seg_join[k][i]) cudaEventDestroy(g->seg_join[k][i]);
+    }
     if (g->seg_fork[i]) cudaEventDestroy(g->seg_fork[i]);
-    if (g->seg_join[i]) cudaEventDestroy(g->seg_join[i]);
   }
   if (g->own) cudaStreamDestroy(g->own);
   delete g;
@@ -1133,12 +1151,16 @@ int count_pipelined(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t
                                        const_cast<int32_t *>(bc->graph_of), g->sms, sp,
                                        &launches)))
       return finish(rc);
+    // a part's peel in two launches, its large and middle graphs together:
+    // a third launch per part measured slower end to end (53.1 against 51.3 ms)
     PeelSide ps;
+    int32_t nbig = 0, nmid = 0;
     if ((rc = seg_side(g, 1 + p, &ps))) return finish(rc);
     if (vend > vbeg &&
-        (rc = peel_segments_launch(pa, bc->vtx_off, bc->arc_off, bc->order + g0,
-                                   (int32_t)(g1 - g0), (int32_t)count_big(P.vo_h, g0, g1), sp,
-                                   ps, &launches, p, part_max_n(P, p))))
+        (count_classes(P.vo_h, g0, g1, &nbig, &nmid),
+         rc = peel_segments_launch(pa, bc->vtx_off, bc->arc_off, bc->order + g0,
+                                   (int32_t)(g1 - g0), nbig + nmid, 0, sp, ps, &launches, p,
+                                   part_max_n(P, p))))
       return finish(rc);
     OrientArgs oa = orient_args(g);
     oa.v0 = vbeg;
@@ -1552,7 +1574,7 @@ struct mce_batch {
   int32_t *order_h = nullptr;  // its pinned host staging copy
   int64_t cap_rows = -1, cap_m = -1, cap_g = -1;
   int64_t max_n = 0;           // the most vertices of a graph of the batch
-  int64_t g_big = 0;           // its graphs with more than PEEL_SMALL_N vertices
+  int32_t g_big = 0, g_mid = 0;  // its graphs in the large and middle peel classes
   // mce_batch_count_host: copies on their own stream, one event per part
   cudaStream_t copy = nullptr;
   cudaEvent_t start = nullptr, ready[MAX_PARTS] = {nullptr};
@@ -1636,7 +1658,7 @@ int batch_load(mce_batch *b, const int32_t *row_ptr, const int32_t *col, const i
   b->max_n = 0;
   for (int32_t i = 0; i < G; ++i) b->max_n = std::max<int64_t>(b->max_n, vo[i + 1] - vo[i] - 1);
   order_graphs(order, 0, G, vo, ao);
-  b->g_big = count_big(vo, 0, G);
+  count_classes(vo, 0, G, &b->g_big, &b->g_mid);
   MCE_CUDA(cudaMemcpyAsync(b->order, order, sizeof(int32_t) * (size_t)G, cudaMemcpyHostToDevice,
                            s));
   return batch_rebase_launch(b->rp_local, b->col_local, b->vtx_off, b->arc_off, G, n, m, g->rp,
@@ -1709,6 +1731,7 @@ int mce_batch_count(mce_batch_t b, const mce_opts_t *opts, uint64_t *per_graph_t
   BatchCtx bc{b->graph_of, b->graph_count, per_graph_total, b->G, b->vtx_off, b->arc_off, b->order};
   bc.max_n = b->max_n;
   bc.g_big = b->g_big;
+  bc.g_mid = b->g_mid;
   return count_impl(b->g, o, total, hist, stats, &bc);
 }
 
@@ -1768,6 +1791,7 @@ int mce_batch_count_host(mce_batch_t b, const int32_t *row_ptr, const int32_t *c
   for (int32_t i = 0; i < G; ++i) b->max_n = std::max<int64_t>(b->max_n, vo[i + 1] - vo[i] - 1);
   for (int p = 0; p < P.k; ++p) order_graphs(order, P.g[p], P.g[p + 1], vo, ao);
   b->g_big = G;  // the order is per part now: a later resident count peels all in one launch
+  b->g_mid = 0;
   // the copies wait for earlier work on the caller's stream, then run on
   // their own stream while the caller's stream processes the parts already
   // on the device
@@ -1797,6 +1821,7 @@ int mce_batch_count_host(mce_batch_t b, const int32_t *row_ptr, const int32_t *c
   bc.parts = &P;
   bc.max_n = b->max_n;
   bc.g_big = b->g_big;
+  bc.g_mid = b->g_mid;
   rc = pipelined ? count_pipelined(b->g, o, total, hist, stats, &bc)
                  : count_impl(b->g, o, total, hist, stats, &bc);
   if (rc) cudaStreamSynchronize(b->copy);  // no copy outlives a failed call

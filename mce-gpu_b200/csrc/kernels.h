@@ -30,20 +30,25 @@ int peel_launch(const PeelArgs &a, cudaStream_t s, int *launches);
 // each part takes graphs from its own counter.  part < 0: the whole batch.
 // max_n: the most vertices of a graph of the launch (0: unknown); graphs up
 // to 16,384 vertices are peeled with their state in shared memory.
-// The first g_big graphs of `order` are peeled by 512-thread blocks; the
-// rest, which must have at most PEEL_SMALL_N vertices each, by 128-thread
-// blocks on `side` (forked from s by `fork`, joined back by `join`; all
-// three null: on s after the others), so that more small graphs run at once.
+// `order` holds the large graphs (more than PEEL_MID_N vertices) first, g_big
+// of them, peeled by 512-thread blocks; then g_mid middle ones (at most
+// PEEL_MID_N) by 256-thread blocks and the small rest (at most PEEL_SMALL_N)
+// by 128-thread blocks, those two launches on the side streams (forked from
+// s by `fork`, joined back by `join`; all null: on s after the others), so
+// that the smaller graphs' blocks, which need less shared memory, run many
+// at a time beside the large ones.
 constexpr int64_t PEEL_SMALL_N = 2048;
+constexpr int64_t PEEL_MID_N = 8192;
 // A host batch is copied, prepared and searched in at most this many parts.
 constexpr int MAX_BATCH_PARTS = 6;
 struct PeelSide {
-  cudaStream_t side = nullptr;
-  cudaEvent_t fork = nullptr, join = nullptr;
+  cudaStream_t side[2] = {nullptr, nullptr};
+  cudaEvent_t fork = nullptr, join[2] = {nullptr, nullptr};
 };
 int peel_segments_launch(const PeelArgs &a, const int64_t *vtx_off, const int64_t *arc_off,
-                         const int32_t *order, int32_t G, int32_t g_big, cudaStream_t s,
-                         const PeelSide &ps, int *launches, int part = -1, int64_t max_n = 0);
+                         const int32_t *order, int32_t G, int32_t g_big, int32_t g_mid,
+                         cudaStream_t s, const PeelSide &ps, int *launches, int part = -1,
+                         int64_t max_n = 0);
 int peel_read(const void *ctl_dev, int32_t *degeneracy, uint32_t *err, uint32_t *rounds,
               uint32_t *solo_sections, cudaStream_t s, double *phase_ms = nullptr);
 

@@ -372,12 +372,10 @@ int mlp_grad_launch(const void *wh, const float *X, const float *Y, const int32_
                     int64_t begin, int64_t end, float *grad, float *loss, cudaStream_t s) {
   const int64_t cnt = end - begin;
   if (cnt <= 0) return MCE_OK;
-  static bool attr = false;
-  if (!attr) {
-    MCE_CUDA(cudaFuncSetAttribute(mlp_train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)mlp_train_smem()));
-    attr = true;
-  }
+  // set on every call: the attribute belongs to the current device, and a
+  // cached flag would be shared by every device and host thread
+  MCE_CUDA(cudaFuncSetAttribute(mlp_train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)mlp_train_smem()));
   mlp_train_kernel<<<(unsigned)((cnt + TB - 1) / TB), TB, mlp_train_smem(), s>>>(
       (const __half *)wh, X, Y, idx, begin, end, 1.0f / (float)cnt, grad, loss);
   MCE_CUDA(cudaGetLastError());

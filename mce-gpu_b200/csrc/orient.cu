@@ -324,9 +324,8 @@ int orient_launch(const OrientArgs &a, cudaStream_t s, int *launches) {
   int64_t blocks = (groups + ORIENT_WARPS - 1) / ORIENT_WARPS;
   // one wave of resident blocks striding over the groups: a block's warps
   // meet at its final barrier once, not once per wave
-  static int per_sm = 0;
-  if (!per_sm)
-    MCE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, orient_kernel, ORIENT_BLOCK, 0));
+  int per_sm = 0;
+  MCE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, orient_kernel, ORIENT_BLOCK, 0));
   const int64_t cap = (int64_t)sms * (per_sm > 0 ? per_sm : 1);
   if (blocks > cap) blocks = cap;
   orient_kernel<<<(unsigned)blocks, ORIENT_BLOCK, 0, s>>>(a);

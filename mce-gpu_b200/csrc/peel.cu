@@ -49,7 +49,9 @@ struct PeelCtl {
   unsigned long long t_scan, t_round, t_wait;  // ns seen by block 0 (diagnostics)
   uint32_t seg_next;   // batches: next graph to peel
   uint32_t seg_part[MAX_BATCH_PARTS];  // ... the same per part of a batch still arriving
-  uint32_t seg_small_next;     // the same for the small graphs' launch
+  uint32_t seg_mid_next;       // the same for the middle and small graphs' launches
+  uint32_t seg_mid_part[MAX_BATCH_PARTS];
+  uint32_t seg_small_next;
   uint32_t seg_small_part[MAX_BATCH_PARTS];
 };
 
@@ -654,25 +656,24 @@ __global__ void __launch_bounds__(SEG_BLOCK)
 
 }  // namespace
 
-// 128 threads per small graph (at most PEEL_SMALL_N vertices): sixteen such
-// blocks fit on an SM where three 512-thread blocks with room for 16,384
-// vertices do.
-constexpr int SEG_SMALL_BLOCK = 128;
+// 128 threads per small graph (at most PEEL_SMALL_N vertices) and 256 per
+// middle one (at most PEEL_MID_N): blocks that need 8 or 32 KB of shared
+// memory, so many more of them fit on an SM than of the 512-thread blocks
+// with room for 16,384 vertices.
+constexpr int SEG_SMALL_BLOCK = 128, SEG_MID_BLOCK = 256;
 
 int peel_segments_launch(const PeelArgs &a, const int64_t *vtx_off, const int64_t *arc_off,
-                         const int32_t *order, int32_t G, int32_t g_big, cudaStream_t s,
-                         const PeelSide &ps, int *launches, int part, int64_t max_n) {
+                         const int32_t *order, int32_t G, int32_t g_big, int32_t g_mid,
+                         cudaStream_t s, const PeelSide &ps, int *launches, int part,
+                         int64_t max_n) {
   int dev = 0, sms = 0;
   MCE_CUDA(cudaGetDevice(&dev));
   MCE_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  static bool attr = false;
-  if (!attr) {
-    MCE_CUDA(cudaFuncSetAttribute(peel_segments_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  SEG_SMEM_N * 4));
-    attr = true;
-  }
+  // set on every call: the attribute belongs to the current device
+  MCE_CUDA(cudaFuncSetAttribute(peel_segments_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                SEG_SMEM_N * 4));
   if (part >= MAX_BATCH_PARTS) return MCE_EINVAL;
-  if (g_big < 0 || g_big > G) return MCE_EINVAL;
+  if (g_big < 0 || g_mid < 0 || g_big + g_mid > G) return MCE_EINVAL;
   PeelCtl *ctl = (PeelCtl *)a.ctl;
   if (part < 0) MCE_CUDA(cudaMemsetAsync(ctl, 0, sizeof(PeelCtl), s));
   // one launch: `cnt` graphs of order[first..], blocks of `threads`, shared
@@ -695,21 +696,28 @@ int peel_segments_launch(const PeelArgs &a, const int64_t *vtx_off, const int64_
     if (launches) *launches += 1;
     return MCE_OK;
   };
-  uint32_t *next_big = part < 0 ? &ctl->seg_next : &ctl->seg_part[part];
-  uint32_t *next_small = part < 0 ? &ctl->seg_small_next : &ctl->seg_small_part[part];
-  const bool fork = ps.side && ps.fork && ps.join && G > g_big;
+  const bool p0 = part < 0;
+  const int32_t g_small = G - g_big - g_mid;
+  const bool fork = ps.side[0] && ps.side[1] && ps.fork && ps.join[0] && ps.join[1] &&
+                    (g_mid > 0 || g_small > 0);
   if (fork) {
     MCE_CUDA(cudaEventRecord(ps.fork, s));
-    MCE_CUDA(cudaStreamWaitEvent(ps.side, ps.fork, 0));
+    MCE_CUDA(cudaStreamWaitEvent(ps.side[0], ps.fork, 0));
+    MCE_CUDA(cudaStreamWaitEvent(ps.side[1], ps.fork, 0));
   }
-  int rc = launch(0, g_big, SEG_BLOCK, max_n, next_big, s);
+  int rc = launch(0, g_big, SEG_BLOCK, max_n, p0 ? &ctl->seg_next : &ctl->seg_part[part], s);
   if (rc) return rc;
-  rc = launch(g_big, G - g_big, SEG_SMALL_BLOCK, std::min<int64_t>(max_n, PEEL_SMALL_N),
-              next_small, fork ? ps.side : s);
+  rc = launch(g_big, g_mid, SEG_MID_BLOCK, std::min<int64_t>(max_n, PEEL_MID_N),
+              p0 ? &ctl->seg_mid_next : &ctl->seg_mid_part[part], fork ? ps.side[0] : s);
+  if (rc) return rc;
+  rc = launch(g_big + g_mid, g_small, SEG_SMALL_BLOCK, std::min<int64_t>(max_n, PEEL_SMALL_N),
+              p0 ? &ctl->seg_small_next : &ctl->seg_small_part[part], fork ? ps.side[1] : s);
   if (rc) return rc;
   if (fork) {
-    MCE_CUDA(cudaEventRecord(ps.join, ps.side));
-    MCE_CUDA(cudaStreamWaitEvent(s, ps.join, 0));
+    MCE_CUDA(cudaEventRecord(ps.join[0], ps.side[0]));
+    MCE_CUDA(cudaEventRecord(ps.join[1], ps.side[1]));
+    MCE_CUDA(cudaStreamWaitEvent(s, ps.join[0], 0));
+    MCE_CUDA(cudaStreamWaitEvent(s, ps.join[1], 0));
   }
   return MCE_OK;
 }
