@@ -69,6 +69,8 @@ constexpr uint32_t SOLO_ROUNDS = 65536;
 // of the grid waits at the next barrier.  One 64-bit atomic hands out both
 // the slot and the chunk base, so bases increase with the slot.
 constexpr int32_t HEAVY_DEG = 256;
+// Light frontier vertices a warp takes at a time in a large frontier.
+constexpr int PEEL_GROUP = 8;
 
 // A warp's staging buffer for the next frontier: appends gather here and
 // reach the list STAGE at a time, one atomic on its counter per flush
@@ -198,14 +200,62 @@ __device__ __forceinline__ void peel_round(uint32_t q, int32_t level, uint32_t p
     stage_append(st, p && !heavy, u, Fn, &ctl->fcnt[fn]);
     heavy_append(heavy, u, du, Fn, HBn, cap, &ctl->hpack[fn]);
   };
-  // light vertices: a warp each
-  for (int64_t i = t0 >> 5; i < lc; i += nt >> 5) {
-    const int32_t v = Fc[i];
-    const int32_t b = rp[v], e = rp[v + 1];
-    for (int32_t j0 = b; j0 < e; j0 += 32) {
-      int32_t u;
-      const bool p = peel_edge(j0 + (int32_t)lane, e, level, col, deg, core, u);
-      push(p, u);
+  // light vertices: a warp each; in a frontier with at least PEEL_GROUP of
+  // them per warp, a warp takes PEEL_GROUP at a time and keeps the loads
+  // and degree updates of their first windows in flight together (one chain
+  // of dependent accesses per group instead of one per vertex)
+  const int64_t nwarp = nt >> 5;
+  if (lc >= (int64_t)PEEL_GROUP * nwarp) {
+    constexpr int R = PEEL_GROUP;
+    const int64_t groups = (lc + R - 1) / R;
+    for (int64_t gi = t0 >> 5; gi < groups; gi += nwarp) {
+      const int64_t i0 = gi * R;
+      const int rows = lc - i0 < R ? (int)(lc - i0) : R;
+      int32_t v = 0, b = 0, e = 0;
+      if ((int)lane < rows) {
+        v = Fc[i0 + lane];
+        b = rp[v];
+        e = rp[v + 1];
+      }
+      int32_t U[R];
+      bool live[R];
+#pragma unroll
+      for (int k = 0; k < R; ++k) {  // every row's first window
+        const int32_t j = __shfl_sync(MCE_FULL, b, k) + (int32_t)lane;
+        const bool in = k < rows && j < __shfl_sync(MCE_FULL, e, k);
+        U[k] = in ? col[j] : 0;
+        live[k] = in;
+      }
+#pragma unroll
+      for (int k = 0; k < R; ++k)
+        live[k] = live[k] && ld_volatile((const uint32_t *)&core[U[k]]) == 0xFFFFFFFFu;
+      int32_t old[R];
+#pragma unroll
+      for (int k = 0; k < R; ++k) old[k] = live[k] ? atomicSub(&deg[U[k]], 1) : 0;
+#pragma unroll
+      for (int k = 0; k < R; ++k) {
+        const bool p = live[k] && old[k] == level + 1;
+        if (p) core[U[k]] = level;
+        push(p, U[k]);
+      }
+      for (int k = 0; k < rows; ++k) {  // the rest of rows longer than a window
+        const int32_t bk = __shfl_sync(MCE_FULL, b, k), ek = __shfl_sync(MCE_FULL, e, k);
+        for (int32_t j0 = bk + 32; j0 < ek; j0 += 32) {
+          int32_t u;
+          const bool p = peel_edge(j0 + (int32_t)lane, ek, level, col, deg, core, u);
+          push(p, u);
+        }
+      }
+    }
+  } else {
+    for (int64_t i = t0 >> 5; i < lc; i += nwarp) {
+      const int32_t v = Fc[i];
+      const int32_t b = rp[v], e = rp[v + 1];
+      for (int32_t j0 = b; j0 < e; j0 += 32) {
+        int32_t u;
+        const bool p = peel_edge(j0 + (int32_t)lane, e, level, col, deg, core, u);
+        push(p, u);
+      }
     }
   }
   // heavy vertices: chunk c belongs to the last slot whose base is <= c
