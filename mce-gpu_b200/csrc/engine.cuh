@@ -832,11 +832,12 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
   // All such branches are settled together from the pivot scores (one node
   // each, the same count and histogram as walking them) and leave the branch
   // set; their moves from P to X are applied when a later sibling is
-  // branched (Lp, kept in the frame).  Not in the listing, op-counting or
-  // budgeted variants, nor for the first level of a root split over warps.
+  // branched (Lp, kept in the frame).  Not in the listing or op-counting
+  // variants, nor for the first level of a root split over warps; with a
+  // node budget the walk stops as soon as settled leaves pass it.
   // The 64-bit engine keeps its walk: the extra live values made it spill
   // more than the settled leaves saved (8.45 -> 8.77 ms on the batch).
-  constexpr bool kBulk = !OPS && !LIST && !Budget && NR == 1;
+  constexpr bool kBulk = !OPS && !LIST && NR == 1;
   Word Lp = 0;   // the current frame's settled leaves not yet moved from P to X
   Word xuni = 0; // the union of the root's earlier-neighbour rows (depth-0 leaves)
   if constexpr (kBulk) {
@@ -895,6 +896,11 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
     if (!(SPLIT && parts > 1)) {  // a split root's first level keeps its order
       Lp = take_leaves(B, P, X, S);
       B &= ~Lp;
+    }
+    if (Budget && a.node_budget && nodes > a.node_budget) {  // a serving request over its budget
+      if (lane == 0) atomicOr(a.err, MCE_ERR_BUDGET);
+      MCE_BD(BD_OTHER);
+      return;
     }
   }
   for (;;) {
@@ -1104,6 +1110,10 @@ __device__ void reg_tree(const BKArgs &a, RegSmem<Word, NR> &sm, const RegSlab<W
     if constexpr (kBulk) {  // the new node's leaf branches
       Lp = take_leaves(B, P, X, S);
       B &= ~Lp;
+      if (Budget && a.node_budget && nodes > a.node_budget) {
+        if (lane == 0) atomicOr(a.err, MCE_ERR_BUDGET);
+        break;
+      }
     }
   }
   MCE_BD(BD_OTHER);
