@@ -61,6 +61,7 @@ constexpr int SV_DCAP = 256;            // widest root (later neighbours) a slot
 // when 2 us is small beside a request's service time).
 constexpr uint64_t SV_POLL_NS = 500;
 constexpr int SV_MAX_EGO = 16384;
+constexpr int SV_RUN = 4;  // consecutive positions a thread takes per window of the induced-row pass
 
 struct SvEntry {             // one request, in mapped host memory
   int64_t seed;              // host -> device
@@ -337,46 +338,80 @@ __device__ int window_owner(const int32_t *off, int nrows, int e0, int carry, in
 
 // Append the vertices first met in the rows of list[0 .. nrows) (row order,
 // then position: discovery order) to the ego list, up to the cap.  A vertex
-// seen at several positions of one window is appended at the first.
+// seen at several positions of one window is appended at the first.  As in
+// the induced-row pass, a window holds SV_RUN consecutive positions per
+// thread, each thread finding the row of its first one by a binary search.
 template <int G>
 __device__ void ego_discover(const ServeArgs &S, const SvClass &C, const Arena &A, const int32_t *list, int nrows,
                              int32_t *own_sm, SvShared &sh) {
   using Gp = Grp<G>;
+  constexpr int K = SV_RUN;
   const int cap = C.ego_cap, hc = C.hcap;
   const int T = row_offsets<G>(S, list, nrows, A.off, A.rs, sh);
-  int carry = -1, ia = 0, ib = 0;
-  for (int e0 = 0; e0 < T; e0 += G, ia = ib) {
-    const int k = sh.k;  // read by all before thread 0 updates it below
-    if (k >= cap) break;
-    const int o = window_owner<G>(A.off, nrows, e0, carry, ia, ib, own_sm, sh);
-    const int e = e0 + Gp::tid();
-    int32_t w = -1;
-    uint32_t slot = 0;
-    bool cand = false;
-    if (e < T) {
-      w = S.gcol[A.rs[o] + (e - A.off[o])];
-      hput(A, hc, w, &slot);  // inserts or finds the vertex
-      cand = A.hval[slot] == SV_PENDING;
-      if (cand) atomicMin(&A.hfirst[slot], e);
-    }
-    Gp::sync();
-    const bool fresh = cand && A.hfirst[slot] == e;
-    int pos;
-    const int tot = block_scan<G>(fresh ? 1 : 0, &pos, sh.ws);
-    if (fresh) {
-      if (k + pos < cap) {
-        A.hval[slot] = k + pos;
-        A.V[k + pos] = w;
-      } else {
-        A.hval[slot] = -1;  // beyond the cap: not in the ego graph
+  for (int w0 = 0; w0 < T; w0 += G * K) {
+    const int k0 = sh.k;  // read by all before thread 0 updates it below
+    if (k0 >= cap) break;
+    const int p0 = w0 + Gp::tid() * K;
+    int32_t wv[K];
+    uint32_t slot[K];
+    bool cand[K];
+    if (p0 < T) {
+      int lo = 0, hi = nrows + 1;  // the first row starting after p0
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (A.off[mid] <= p0)
+          lo = mid + 1;
+        else
+          hi = mid;
+      }
+      int r = lo - 1;  // the last row starting at or before p0
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        const int e = p0 + k;
+        wv[k] = -1;
+        slot[k] = 0;
+        cand[k] = false;
+        if (e < T) {
+          while (A.off[r + 1] <= e) ++r;  // stops at nrows at the latest: off[nrows] = T > e
+          wv[k] = S.gcol[A.rs[r] + (e - A.off[r])];
+          hput(A, hc, wv[k], &slot[k]);  // inserts or finds the vertex
+          cand[k] = A.hval[slot[k]] == SV_PENDING;
+          if (cand[k]) atomicMin(&A.hfirst[slot[k]], e);
+        }
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        wv[k] = -1;
+        slot[k] = 0;
+        cand[k] = false;
       }
     }
-    if (Gp::tid() == G - 1) {
-      sh.k = min(cap, k + tot);
-      sh.carry = o;
-    }
     Gp::sync();
-    carry = sh.carry;
+    bool fresh[K];
+    int cnt = 0;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      fresh[k] = cand[k] && A.hfirst[slot[k]] == p0 + k;
+      cnt += fresh[k];
+    }
+    int pos;
+    const int tot = block_scan<G>(cnt, &pos, sh.ws);
+    int at = k0 + pos;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      if (fresh[k]) {
+        if (at < cap) {
+          A.hval[slot[k]] = at;
+          A.V[at] = wv[k];
+        } else {
+          A.hval[slot[k]] = -1;  // beyond the cap: not in the ego graph
+        }
+        ++at;
+      }
+    }
+    if (Gp::tid() == 0) sh.k = min(cap, k0 + tot);
+    Gp::sync();
   }
 }
 
@@ -422,25 +457,62 @@ __device__ int ego_extract(const ServeArgs &S, const SvClass &C, const Arena &A,
   Gp::sync();
   // induced rows in one flattened pass: the i-th kept element overall is
   // col[i] (rows in order, each filtered row stays sorted), and a row starts
-  // at the count of kept elements before its first one
+  // at the count of kept elements before its first one.  A window holds
+  // SV_RUN * G positions, SV_RUN consecutive ones per thread: a thread finds
+  // the row of its first position by a binary search over the row offsets,
+  // looks its elements up with their loads in flight together, and after one
+  // scan of the threads' kept counts writes them and the starts of the rows
+  // that begin in its positions (four times fewer windows and barriers than
+  // one position per thread).
   const int T = row_offsets<G>(S, A.V, n, A.off, A.rs, sh);
-  int carry = -1, kept = 0, ia = 0, ib = 0;
-  for (int e0 = 0; e0 < T; e0 += G, ia = ib) {
-    const int o = window_owner<G>(A.off, n, e0, carry, ia, ib, own_sm, sh);
-    const int e = e0 + Gp::tid();
-    int32_t loc = -1;
-    if (e < T) loc = hget(A, hc, S.gcol[A.rs[o] + (e - A.off[o])]);
+  int kept = 0;
+  constexpr int K = SV_RUN;
+  for (int w0 = 0; w0 < T; w0 += G * K) {
+    const int p0 = w0 + Gp::tid() * K;
+    int r0 = -1;  // the last row starting at or before p0 - 1 (off[0] = 0, off[n] = T)
+    int32_t loc[K];
+    int cnt = 0;
+    if (p0 < T) {
+      int lo = 0, hi = n + 1;
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (A.off[mid] <= p0 - 1)
+          lo = mid + 1;
+        else
+          hi = mid;
+      }
+      r0 = lo - 1;
+    }
+    int r = r0;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int e = p0 + k;
+      loc[k] = -1;
+      if (e < T) {
+        while (A.off[r + 1] <= e) ++r;  // stops at n at the latest: off[n] = T > e
+        loc[k] = hget(A, hc, S.gcol[A.rs[r] + (e - A.off[r])]);
+        cnt += loc[k] >= 0;
+      }
+    }
     int pos;
-    const int tot = block_scan<G>(loc >= 0 ? 1 : 0, &pos, sh.ws);
-    if (loc >= 0 && kept + pos < C.arc_cap) A.col[kept + pos] = loc;
-    own_sm[Gp::tid()] = pos;  // kept elements of this window before each position
-    Gp::sync();
-    for (int i = ia + Gp::tid(); i < ib; i += G)  // rows starting here
-      A.rp[i] = kept + own_sm[A.off[i] - e0];
-    if (Gp::tid() == G - 1) sh.carry = o;
-    Gp::sync();
-    carry = sh.carry;
+    const int tot = block_scan<G>(cnt, &pos, sh.ws);
+    if (p0 < T) {
+      int q = kept + pos;
+      r = r0;
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        const int e = p0 + k;
+        if (e < T) {
+          while (A.off[r + 1] <= e) A.rp[++r] = q;  // rows (empty ones too) starting at e
+          if (loc[k] >= 0) {
+            if (q < C.arc_cap) A.col[q] = loc[k];
+            ++q;
+          }
+        }
+      }
+    }
     kept += tot;
+    Gp::sync();  // the scan's shared words are reused by the next window
   }
   for (int i = Gp::tid(); i <= n; i += G)  // rows starting at the end (empty)
     if (A.off[i] == T) A.rp[i] = kept;
