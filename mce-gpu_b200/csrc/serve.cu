@@ -61,7 +61,7 @@ constexpr int SV_DCAP = 256;            // widest root (later neighbours) a slot
 // when 2 us is small beside a request's service time).
 constexpr uint64_t SV_POLL_NS = 500;
 constexpr int SV_MAX_EGO = 16384;
-constexpr int SV_RUN = 4;  // consecutive positions a thread takes per window of the induced-row pass
+constexpr int SV_RUN = 4;  // consecutive positions a thread takes per window of the extraction passes
 
 struct SvEntry {             // one request, in mapped host memory
   int64_t seed;              // host -> device
@@ -1104,9 +1104,11 @@ void sv_free(mce_serve *s) {
   delete s;
 }
 
-int hash_cap_for(int ego_cap, int threads) {  // the table also takes the up to
-  int hcap = 32;                              // threads - 1 vertices of the window
-  while (hcap < 2 * (ego_cap + threads)) hcap <<= 1;  // that crosses the cap
+// The table also takes the vertices of the discovery window that crosses
+// the cap: up to threads * SV_RUN of them (a window's positions).
+int hash_cap_for(int ego_cap, int threads) {
+  int hcap = 32;
+  while (hcap < 2 * (ego_cap + threads * SV_RUN)) hcap <<= 1;
   return hcap;
 }
 
