@@ -27,6 +27,8 @@ from pinned host memory and the count read back inside the timed region
 binary built from source into oracle/_ref) on the same workload.
 """
 import argparse
+import atexit
+import contextlib
 import json
 import os
 import re
@@ -159,13 +161,15 @@ def plain_per_graph(hb, graphs, stream, kw):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms; only the
+    samples taken inside `window()` (the timed steps) are kept."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, gpu):
         self.gpu, self.rows, self.proc = gpu, [], None
+        self.active, self.started = False, threading.Event()
 
     def __enter__(self):
         try:
@@ -174,21 +178,33 @@ class ClockSampler:
                  "--format=csv,noheader,nounits", "-lms", "200"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             threading.Thread(target=self._read, daemon=True).start()
+            self.started.wait(5.0)  # nvidia-smi takes a moment to start sampling
         except Exception:
             self.proc = None
         return self
 
     def _read(self):
         for line in self.proc.stdout:
-            self.rows.append([x.strip() for x in line.split(",")])
+            self.started.set()
+            if self.active:
+                self.rows.append([x.strip() for x in line.split(",")])
+
+    @contextlib.contextmanager
+    def window(self):
+        self.active = True
+        try:
+            yield self
+        finally:
+            self.active = False
 
     def __exit__(self, *a):
-        if self.proc:
-            self.proc.terminate()
+        proc, self.proc = self.proc, None
+        if proc:
+            proc.terminate()
             try:
-                self.proc.wait(timeout=5)
+                proc.wait(timeout=5)
             except Exception:
-                self.proc.kill()
+                proc.kill()
 
     def summary(self):
         if not self.rows:
@@ -378,7 +394,9 @@ def run_mine(args, rank, world, local_rank):
 
     # ---- device-resident steps
     times, stats = [], []
-    with ClockSampler(local_rank) as clk:
+    clk = ClockSampler(local_rank).__enter__()  # through the end-to-end steps
+    atexit.register(clk.__exit__)
+    with clk.window():
         barrier()
         for _ in range(args.steps):
             flush.zero_()  # evict L2 between steps (outside the timed region)
@@ -413,7 +431,9 @@ def run_mine(args, rank, world, local_rank):
     for _ in range(args.warmup):  # the end-to-end path's own warm-up (its first allocations)
         run_e2e()
     barrier()
-    e2e_times, re2e = timed(stream, flush, run_e2e, args.steps)
+    with clk.window():
+        e2e_times, re2e = timed(stream, flush, run_e2e, args.steps)
+    clk.__exit__()
     assert re2e.total == total
     barrier()
     e2e_ms = sum(e2e_times) / len(e2e_times)
@@ -716,7 +736,7 @@ def run_serve(args, rank, world, local_rank):
         for w in range(args.warmup):  # short traces: first-touch of arenas and code
             seeds, arr = serve_trace(hg.n, 256, args.rate, 1000 + w)
             s.run(seeds, arr)
-        with ClockSampler(local_rank) as clk:
+        with ClockSampler(local_rank) as clk, clk.window():
             if world > 1:
                 torch.distributed.barrier()
             res_all, lat_all, makespans = [], [], []

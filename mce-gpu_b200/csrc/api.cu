@@ -8,6 +8,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <thread>
 #include <vector>
 
 #include "../host/host.h"
@@ -93,6 +94,7 @@ struct mce_graph {
   // to the caller's stream
   cudaStream_t part_s[MAX_BATCH_PARTS] = {nullptr};
   cudaEvent_t part_fork = nullptr, part_done[MAX_BATCH_PARTS] = {nullptr};
+  cudaEvent_t part_sdone = nullptr;  // the latest part search of a call has ended
   // a batch's per-graph peel: the middle and small graphs' launches run on
   // side streams ([k][0] whole batch, [k][1 + p] part p)
   cudaStream_t seg_side[2][1 + MAX_BATCH_PARTS] = {{nullptr}};
@@ -207,6 +209,11 @@ void order_graphs(int32_t *order, int64_t g0, int64_t g1, const int64_t *vo, con
     if (cx != cy) return cx < cy;
     return ao[x + 1] - ao[x] > ao[y + 1] - ao[y];
   });
+}
+
+// One search's root summary, written on the device.
+__global__ void shape_set_kernel(ShapeInfo *dst, ShapeInfo v) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *dst = v;
 }
 
 // The side streams and events of a per-graph peel launch (i: 0 whole batch,
@@ -601,6 +608,7 @@ int mce_graph_free(mce_graph_t g) {
     if (g->part_done[p]) cudaEventDestroy(g->part_done[p]);
   }
   if (g->part_fork) cudaEventDestroy(g->part_fork);
+  if (g->part_sdone) cudaEventDestroy(g->part_sdone);
   for (int i = 0; i < 1 + MAX_PARTS; ++i) {
     for (int k = 0; k < 2; ++k) {
       if (g->seg_side[k][i]) cudaStreamDestroy(g->seg_side[k][i]);
@@ -1139,8 +1147,8 @@ int count_pipelined(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t
   const PeelArgs pa = peel_args(g, o.peel_solo_max);
   int64_t vb[MAX_PARTS + 1];
   for (int p = 0; p <= P.k; ++p) vb[p] = P.vo_h[P.g[p]] - P.g[p];
-  // the parts' preparation, each on its own stream
-  for (int p = 0; p < P.k; ++p) {
+  // a part's preparation, on its own stream
+  auto prep = [&](int p) -> int {
     cudaStream_t sp = g->part_s[p];
     const int64_t g0 = P.g[p], g1 = P.g[p + 1], vbeg = vb[p], vend = vb[p + 1];
     MCE_CUDA(cudaStreamWaitEvent(sp, g->part_fork, 0));
@@ -1150,18 +1158,24 @@ int count_pipelined(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t
                                        P.ao_h[g1], vend, (int32_t)P.ao_h[g1], g->rp, g->col,
                                        const_cast<int32_t *>(bc->graph_of), g->sms, sp,
                                        &launches)))
-      return finish(rc);
+      return rc;
     // a part's peel in two launches, its large and middle graphs together:
     // a third launch per part measured slower end to end (53.1 against 51.3 ms)
     PeelSide ps;
     int32_t nbig = 0, nmid = 0;
-    if ((rc = seg_side(g, 1 + p, &ps))) return finish(rc);
+    if ((rc = seg_side(g, 1 + p, &ps))) return rc;
     if (vend > vbeg &&
         (count_classes(P.vo_h, g0, g1, &nbig, &nmid),
          rc = peel_segments_launch(pa, bc->vtx_off, bc->arc_off, bc->order + g0,
                                    (int32_t)(g1 - g0), nbig + nmid, 0, sp, ps, &launches, p,
                                    part_max_n(P, p))))
-      return finish(rc);
+      return rc;
+    return MCE_OK;
+  };
+  // ... then its orientation and root sort
+  auto prep_b = [&](int p) -> int {
+    cudaStream_t sp = g->part_s[p];
+    const int64_t vbeg = vb[p], vend = vb[p + 1];
     OrientArgs oa = orient_args(g);
     oa.v0 = vbeg;
     oa.n = vend;
@@ -1169,7 +1183,7 @@ int count_pipelined(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t
     oa.hub_list = g->hub_list + vbeg;  // hub indices are the part's own
     oa.next = g->orient_next + 2 + 2 * p;
     oa.long_list = reinterpret_cast<int32_t *>(g->keys_out) + vbeg;
-    if ((rc = orient_launch(oa, sp, &launches))) return finish(rc);
+    if ((rc = orient_launch(oa, sp, &launches))) return rc;
     const int64_t np = vend - vbeg;
     // keys: class, hubs first, then (degree order) the cost; vertex order
     // within a key (plain order: no cost)
@@ -1177,15 +1191,16 @@ int count_pipelined(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t
                                      g->split + vbeg, nullptr, degree ? heavy : 1e30f,
                                      degree ? heavy : 1e30f, g->sms, sp, &launches, 0,
                                      g->hub_of + vbeg)))
-      return finish(rc);
+      return rc;
     if ((rc = roots_sort(np, g->keys_in + vbeg, g->keys_out + vbeg, g->vals_in + vbeg,
                          g->roots + vbeg, 32, &g->part_tmp[p], &g->part_tmp_bytes[p],
                          g->part_shape + p, sp, &launches)))
-      return finish(rc);
+      return rc;
     MCE_CUDA(cudaMemcpyAsync(g->part_shape_h + p, g->part_shape + p, sizeof(ShapeInfo),
                              cudaMemcpyDeviceToHost, sp));
     MCE_CUDA(cudaEventRecord(g->part_done[p], sp));
-  }
+    return MCE_OK;
+  };
   // The searches, in order on the call's stream.  As each part lands, its
   // 32-bit roots without hub rows are searched (most of the work).  Every
   // other root - the hubs of all classes, the 64-bit and wide classes, whose
@@ -1274,14 +1289,15 @@ int count_pipelined(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t
     if (share_q && (r = queue_launch_init(a.q, s, &launches))) return r;
     return bk_launch(c, wbits, a, grid, block, smem, s, &launches);
   };
-  for (int p = 0; p < P.k; ++p) {
+  // a part's search, once its preparation is done
+  auto search = [&](int p) -> int {
     MCE_CUDA(cudaEventSynchronize(g->part_done[p]));
     const ShapeInfo sh = g->part_shape_h[p];
     MCE_CUDA(cudaStreamWaitEvent(s, g->part_done[p], 0));
     if (p == 0) MCE_CUDA(cudaEventRecord(g->ev[1], s));
     if (sh.cls_cnt[CLS_BIG]) {
       err_limit = 1;
-      break;
+      return MCE_OK;
     }
     const int64_t vbeg = vb[p];
     // roots of the part, class-sorted, hubs first within a class
@@ -1299,27 +1315,60 @@ int count_pipelined(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t
     for (int c = 0; c < NCLS && c < 8; ++c) st.class_roots[c] += sh.cls_cnt[c];
     if ((int32_t)sh.max_dplus > st.max_later_degree) st.max_later_degree = (int32_t)sh.max_dplus;
     if ((int64_t)sh.max_deg > st.max_degree) st.max_degree = sh.max_deg;
-    if (n32 <= 0) continue;
+    if (n32 <= 0) return MCE_OK;
     // the part's 32-bit roots after its hubs: earlier degree <= HUB_XMIN, no hub rows
     ShapeInfo ss{};
     for (int c = 1; c < 9; ++c) ss.cls_off[c] = (uint32_t)n32;
     ss.cls_cnt[CLS_R32] = (uint32_t)n32;
     hs_search[p] = ss;
-    MCE_CUDA(cudaMemcpyAsync(sh_search + p, hs_search + p, sizeof(ShapeInfo),
-                             cudaMemcpyHostToDevice, s));
+    // written by a kernel rather than copied from the host on the call's
+    // stream, whose copy would share the copy engine with the part copies
+    // still in flight (0.3 ms end to end)
+    shape_set_kernel<<<1, 32, 0, s>>>(sh_search + p, ss);
+    MCE_CUDA(cudaGetLastError());
     const int dcap = 32, xcap = 1, rxcap = REG_XCAP;
     int grid = 0, block = 0, smem = 0, pc = 1, dm = 0, da = 0;
     QueueView qv;
     if ((rc = plan(CLS_R32, n32, dcap, xcap, rxcap, &grid, &block, &smem, &pc, &dm, &da, &qv)))
-      return finish(rc);
+      return rc;
     BKArgs a;
     base_args(a, dcap, xcap, rxcap);
     a.roots = g->roots + vbeg + sh.cls_off[CLS_R32] + sh.hub_r32;
     a.shape = sh_search + p;
     a.fetch = g->part_fetch + 8 * p;
     if ((rc = run_class(CLS_R32, a, grid, block, smem, pc, dm, da, qv, dcap, xcap, rxcap)))
-      return finish(rc);
+      return rc;
+    return MCE_OK;
+  };
+  // Each part's rebase and peel are enqueued once its copy has landed, its
+  // orientation and sort once the search before it has ended, and its
+  // search once those are done: no stream then waits on an event at the
+  // head of a hardware queue that other streams share.
+  if (!g->part_sdone) MCE_CUDA(cudaEventCreateWithFlags(&g->part_sdone, cudaEventDisableTiming));
+  int na = 0, nb = 0, ns = 0;
+  auto ready = [&](cudaEvent_t e, int *bad) {
+    const cudaError_t q = cudaEventQuery(e);
+    if (q != cudaSuccess && q != cudaErrorNotReady) *bad = 1;
+    return q == cudaSuccess;
+  };
+  int bad = 0;
+  while (ns < P.k && !err_limit && !bad) {
+    if (na < P.k && ready(P.ready[na], &bad)) {
+      if ((rc = prep(na++))) return finish(rc);
+      continue;
+    }
+    if (nb < na && (nb == 0 || (ns == nb && ready(g->part_sdone, &bad)))) {
+      if ((rc = prep_b(nb++))) return finish(rc);
+      continue;
+    }
+    if (ns < nb && ready(g->part_done[ns], &bad)) {
+      if ((rc = search(ns++))) return finish(rc);
+      MCE_CUDA(cudaEventRecord(g->part_sdone, s));
+      continue;
+    }
+    std::this_thread::yield();
   }
+  if (bad) return finish(MCE_ECUDA);
   // the deferred roots of every part: one list (R32 hubs, R64, MEM) in the
   // sort's key buffer and one hub list in its value buffer, both free now
   int64_t ncls[3] = {0, 0, 0};
