@@ -370,10 +370,13 @@ int mce_batch_count(mce_batch_t b, const mce_opts_t *opts, uint64_t *per_graph_t
  * of whole graphs on a stream of the handle's own, and each part is rebased,
  * peeled, oriented and - for counts in plain or degree order without
  * per-root or per-warp logs - its roots with at most 32 later and 256
- * earlier neighbours are searched as soon as it is on the device, while the
- * next parts are still being copied (parts of 3, 5, 8, 12, 16 and 20 64ths
- * of the arcs); the other roots of every part (hub roots, wider bitmaps) follow
- * in one search.  In the other modes one search over the whole batch follows.
+ * earlier neighbours are searched while the next parts are still being
+ * copied (parts of 3, 5, 8, 12, 16 and 20 64ths of the arcs): the host
+ * enqueues a part's rebase and peel once its copy has landed, its
+ * orientation once the search of the part before it has ended, and its
+ * search once it is oriented; the other roots of every part (hub roots,
+ * wider bitmaps) follow in one search.  In the other modes one search over
+ * the whole batch follows.
  * Same results as the two calls.  Pinned host memory lets the copies
  * overlap.  In the part-by-part mode stats->peel_ms is the time until the
  * first part is ready, orient_ms 0 and count_ms the rest.                 */
