@@ -1326,6 +1326,7 @@ int count_pipelined(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t
     // still in flight (0.3 ms end to end)
     shape_set_kernel<<<1, 32, 0, s>>>(sh_search + p, ss);
     MCE_CUDA(cudaGetLastError());
+    launches += 1;
     const int dcap = 32, xcap = 1, rxcap = REG_XCAP;
     int grid = 0, block = 0, smem = 0, pc = 1, dm = 0, da = 0;
     QueueView qv;
