@@ -371,7 +371,7 @@ int mce_batch_count(mce_batch_t b, const mce_opts_t *opts, uint64_t *per_graph_t
  * peeled, oriented and - for counts in plain or degree order without
  * per-root or per-warp logs - its roots with at most 32 later and 256
  * earlier neighbours are searched while the next parts are still being
- * copied (parts of 3, 5, 8, 12, 16 and 20 64ths of the arcs): the host
+ * copied (parts of 2, 4, 7, 11, 16 and 24 64ths of the arcs): the host
  * enqueues a part's rebase and peel once its copy has landed, its
  * orientation once the search of the part before it has ended, and its
  * search once it is oriented; the other roots of every part (hub roots,

@@ -1803,15 +1803,15 @@ int mce_batch_count_host(mce_batch_t b, const int32_t *row_ptr, const int32_t *c
   const int32_t G = num_graphs;
   const int64_t *vo = vtx_offsets, *ao = arc_offsets;
   // Parts of whole graphs; small batches in one.  When the parts are
-  // searched as they arrive, they grow (3, 5, 8, 12, 16 and 20 64ths of the
+  // searched as they arrive, they grow (2, 4, 7, 11, 16 and 24 64ths of the
   // arcs): the first search starts after a short copy, and since the copy
-  // moves arcs about 1.5x as fast as the narrow roots are searched, each
-  // part lands (and is prepared) before the search stream reaches it; parts
-  // growing 2x per step left the stream waiting for the last ones.
-  // Otherwise they are equal.
+  // moves arcs faster than the narrow roots are searched, each part lands
+  // before the search stream reaches it; parts growing 2x per step left the
+  // stream waiting for the last ones, and 3, 5, 8, 12, 16, 20 measured
+  // 0.3 ms slower end to end.  Otherwise they are equal.
   const bool pipelined = !o.log_roots && !o.warp_log && !o.count_ops &&
                          (o.sched == MCE_SCHED_PLAIN || o.sched == MCE_SCHED_DEGREE);
-  static const int64_t kGeo[MAX_PARTS] = {3, 8, 16, 28, 44, 64};  // cumulative 64ths
+  static const int64_t kGeo[MAX_PARTS] = {2, 6, 13, 24, 40, 64};  // cumulative 64ths
   int k = m >= BATCH_PART_MIN_ARCS ? MAX_PARTS : 1;
   if (k > G) k = G;
   BatchParts P;
