@@ -161,8 +161,9 @@ def plain_per_graph(hb, graphs, stream, kw):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms; only the
-    samples taken inside `window()` (the timed steps) are kept."""
+    """nvidia-smi clocks and throttle reasons sampled every 50 ms.  Only the
+    samples taken inside `window()` (the timed steps) are kept; a window
+    shorter than the sampling interval keeps the first sample after it."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -170,12 +171,13 @@ class ClockSampler:
     def __init__(self, gpu):
         self.gpu, self.rows, self.proc = gpu, [], None
         self.active, self.started = False, threading.Event()
+        self.want_next = False  # a window closed without a sample of its own
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             threading.Thread(target=self._read, daemon=True).start()
             self.started.wait(5.0)  # nvidia-smi takes a moment to start sampling
@@ -186,16 +188,26 @@ class ClockSampler:
     def _read(self):
         for line in self.proc.stdout:
             self.started.set()
-            if self.active:
+            if self.active or self.want_next:
                 self.rows.append([x.strip() for x in line.split(",")])
+                self.in_window += 1
+                self.want_next = False
 
     @contextlib.contextmanager
     def window(self):
+        self.in_window = 0
         self.active = True
         try:
             yield self
         finally:
             self.active = False
+            if self.in_window == 0:
+                self.want_next = True
+                for _ in range(100):  # up to 1 s for the sample that ends the window
+                    if not self.want_next or not self.proc:
+                        break
+                    time.sleep(0.01)
+                self.want_next = False
 
     def __exit__(self, *a):
         proc, self.proc = self.proc, None
