@@ -172,7 +172,9 @@ def _hub(n, seed):
 def test_batch_count_host_part_by_part_search(kw):
     """Parts searched as they land (hub roots in early and late parts, a
     wide-engine R-MAT graph): per-graph counts equal the resident batch's and
-    the oracle's, twice in a row, and the resident count after it too."""
+    the oracle's, twice in a row, and the resident count after it too.  The
+    batch has 64-bit-row roots (planted cliques of up to 40 vertices), so the
+    32-bit hubs share the final 64-bit launch."""
     cl = mce.gen_chung_lu_batch(120, 64, 8192, 2.3, 8, 32, 5, 5, 40, 7)
     graphs = [_hub(3000, 1)] + [cl.graph(i) for i in range(cl.num_graphs)] + \
         [_hub(6000, 2), mce.gen_rmat(11, 16, 0.57, 0.19, 0.19, 3)]
@@ -182,6 +184,7 @@ def test_batch_count_host_part_by_part_search(kw):
     with mce.Batch(hb) as db:
         ref = db.count(**{k: v for k, v in kw.items() if k != "log_roots"})
         assert np.array_equal(ref.per_graph, want)
+        assert ref.stats["class_roots"][1] > 0  # 33 <= d+ <= 64
         for _ in range(2):
             h = _count_host(db, hb, **kw)
             assert h.stats["error_flags"] == 0
