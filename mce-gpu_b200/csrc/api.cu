@@ -1211,7 +1211,6 @@ int count_pipelined(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t
   const int wbits = o.bitmap_width == 64 ? 64 : 32;
   ShapeInfo *sh_search = g->part_shape + MAX_PARTS;   // [MAX_PARTS]: per-part searches
   ShapeInfo *sh_final = g->part_shape + 2 * MAX_PARTS;
-  ShapeInfo *hs_search = g->part_shape_h + MAX_PARTS;
   ShapeInfo *hs_final = g->part_shape_h + 2 * MAX_PARTS;
   struct Seg {
     int64_t at, cnt;
@@ -1320,7 +1319,6 @@ int count_pipelined(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t
     ShapeInfo ss{};
     for (int c = 1; c < 9; ++c) ss.cls_off[c] = (uint32_t)n32;
     ss.cls_cnt[CLS_R32] = (uint32_t)n32;
-    hs_search[p] = ss;
     // written by a kernel rather than copied from the host on the call's
     // stream, whose copy would share the copy engine with the part copies
     // still in flight (0.3 ms end to end)
