@@ -379,7 +379,10 @@ int mce_batch_count(mce_batch_t b, const mce_opts_t *opts, uint64_t *per_graph_t
  * the whole batch follows.
  * Same results as the two calls.  Pinned host memory lets the copies
  * overlap.  In the part-by-part mode stats->peel_ms is the time until the
- * first part is ready, orient_ms 0 and count_ms the rest.                 */
+ * first part is ready, orient_ms 0 and count_ms the rest.  With the
+ * environment variable MCE_TRACE_PARTS=1 the part-by-part mode prints the
+ * call's timeline (copies, peels, orientations, searches; ms from the
+ * call's start) to stderr, for diagnostics.                               */
 int mce_batch_count_host(mce_batch_t b, const int32_t *row_ptr, const int32_t *col,
                          const int64_t *vtx_offsets, const int64_t *arc_offsets,
                          int32_t num_graphs, const mce_opts_t *opts, uint64_t *per_graph_total,

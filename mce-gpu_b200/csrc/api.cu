@@ -95,6 +95,12 @@ struct mce_graph {
   cudaStream_t part_s[MAX_BATCH_PARTS] = {nullptr};
   cudaEvent_t part_fork = nullptr, part_done[MAX_BATCH_PARTS] = {nullptr};
   cudaEvent_t part_sdone = nullptr;  // the latest part search of a call has ended
+  // opt-in timeline of a part-by-part batch call (environment MCE_TRACE_PARTS=1):
+  // events on the streams it uses, printed to stderr in ms from the call's start
+  static constexpr int TRACE_MAX = 64;
+  cudaEvent_t trace_ev[TRACE_MAX] = {nullptr};
+  char trace_name[TRACE_MAX][12];
+  int trace_n = -1;  // < 0: off for this call
   // a batch's per-graph peel: the middle and small graphs' launches run on
   // side streams ([k][0] whole batch, [k][1 + p] part p)
   cudaStream_t seg_side[2][1 + MAX_BATCH_PARTS] = {{nullptr}};
@@ -214,6 +220,38 @@ void order_graphs(int32_t *order, int64_t g0, int64_t g1, const int64_t *vo, con
 // One search's root summary, written on the device.
 __global__ void shape_set_kernel(ShapeInfo *dst, ShapeInfo v) {
   if (threadIdx.x == 0 && blockIdx.x == 0) *dst = v;
+}
+
+// The opt-in timeline (diagnostics only): trace_mark records an event on a
+// stream under a short name, trace_dump prints the call's events once the
+// last has completed.
+void trace_mark(mce_graph *g, cudaStream_t st, const char *what, int i = -1) {
+  if (g->trace_n < 0 || g->trace_n >= mce_graph::TRACE_MAX) return;
+  const int k = g->trace_n++;
+  if (!g->trace_ev[k] && cudaEventCreate(&g->trace_ev[k]) != cudaSuccess) {
+    g->trace_ev[k] = nullptr;
+    g->trace_n = -1;
+    return;
+  }
+  if (i >= 0)
+    snprintf(g->trace_name[k], sizeof(g->trace_name[k]), "%s%d", what, i);
+  else
+    snprintf(g->trace_name[k], sizeof(g->trace_name[k]), "%s", what);
+  cudaEventRecord(g->trace_ev[k], st);
+}
+
+void trace_dump(mce_graph *g) {
+  if (g->trace_n <= 0) return;
+  const int n = g->trace_n;
+  g->trace_n = -1;
+  for (int k = 0; k < n; ++k) cudaEventSynchronize(g->trace_ev[k]);
+  fprintf(stderr, "mce parts timeline (ms):");
+  for (int k = 0; k < n; ++k) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, g->trace_ev[0], g->trace_ev[k]);
+    fprintf(stderr, " %s=%.2f", g->trace_name[k], ms);
+  }
+  fprintf(stderr, "\n");
 }
 
 // The side streams and events of a per-graph peel launch (i: 0 whole batch,
@@ -609,6 +647,8 @@ int mce_graph_free(mce_graph_t g) {
   }
   if (g->part_fork) cudaEventDestroy(g->part_fork);
   if (g->part_sdone) cudaEventDestroy(g->part_sdone);
+  for (cudaEvent_t e : g->trace_ev)
+    if (e) cudaEventDestroy(e);
   for (int i = 0; i < 1 + MAX_PARTS; ++i) {
     for (int k = 0; k < 2; ++k) {
       if (g->seg_side[k][i]) cudaStreamDestroy(g->seg_side[k][i]);
@@ -1170,6 +1210,7 @@ int count_pipelined(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t
                                    (int32_t)(g1 - g0), nbig + nmid, 0, sp, ps, &launches, p,
                                    part_max_n(P, p))))
       return rc;
+    trace_mark(g, sp, "peel", p);
     return MCE_OK;
   };
   // ... then its orientation and root sort
@@ -1199,6 +1240,7 @@ int count_pipelined(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t
     MCE_CUDA(cudaMemcpyAsync(g->part_shape_h + p, g->part_shape + p, sizeof(ShapeInfo),
                              cudaMemcpyDeviceToHost, sp));
     MCE_CUDA(cudaEventRecord(g->part_done[p], sp));
+    trace_mark(g, sp, "prep", p);
     return MCE_OK;
   };
   // The searches, in order on the call's stream.  As each part lands, its
@@ -1335,8 +1377,10 @@ int count_pipelined(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t
     a.roots = g->roots + vbeg + sh.cls_off[CLS_R32] + sh.hub_r32;
     a.shape = sh_search + p;
     a.fetch = g->part_fetch + 8 * p;
+    trace_mark(g, s, "sb", p);
     if ((rc = run_class(CLS_R32, a, grid, block, smem, pc, dm, da, qv, dcap, xcap, rxcap)))
       return rc;
+    trace_mark(g, s, "se", p);
     return MCE_OK;
   };
   // Each part's rebase and peel are enqueued once its copy has landed, its
@@ -1383,6 +1427,7 @@ int count_pipelined(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t
         at += sg.cnt;
         ncls[c] += sg.cnt;
       }
+    trace_mark(g, s, "defer");
     int64_t nh = 0;
     for (const Seg &sg : hubsegs) {
       if (sg.cnt > 0)
@@ -1415,6 +1460,7 @@ int count_pipelined(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t
                                 g->hub_off, g->hub_nx, g->hub_rows, g->sms, s, &launches)))
         return finish(rc);
     }
+    trace_mark(g, s, "hubrows");
     const int64_t nd = ncls[0] + ncls[1] + ncls[2];
     if (nd > 0) {
       // the 32-bit hubs run in the 64-bit launch, ahead of its roots: one
@@ -1463,6 +1509,7 @@ int count_pipelined(mce_graph *g, const mce_opts_t &o, uint64_t *total, uint64_t
           return finish(rc);
     }
   }
+  trace_mark(g, s, "final");
   MCE_CUDA(cudaEventRecord(g->ev[3], s));
   unsigned long long h_hist[MCE_HIST_MAX];
   unsigned long long h_nodes[2] = {0, 0};
@@ -1852,6 +1899,11 @@ int mce_batch_count_host(mce_batch_t b, const int32_t *row_ptr, const int32_t *c
   // the copies wait for earlier work on the caller's stream, then run on
   // their own stream while the caller's stream processes the parts already
   // on the device
+  {
+    const char *tr = getenv("MCE_TRACE_PARTS");
+    b->g->trace_n = tr && *tr && *tr != '0' ? 0 : -1;
+  }
+  trace_mark(b->g, s, "start");
   MCE_CUDA(cudaEventRecord(b->start, s));
   MCE_CUDA(cudaStreamWaitEvent(b->copy, b->start, 0));
   MCE_CUDA(cudaMemcpyAsync(b->vtx_off, vo, sizeof(int64_t) * (size_t)(G + 1),
@@ -1868,6 +1920,7 @@ int mce_batch_count_host(mce_batch_t b, const int32_t *row_ptr, const int32_t *c
       MCE_CUDA(cudaMemcpyAsync(b->col_local + a0, col + a0, sizeof(int32_t) * (size_t)(a1 - a0),
                                cudaMemcpyHostToDevice, b->copy));
     MCE_CUDA(cudaEventRecord(b->ready[p], b->copy));
+    trace_mark(b->g, b->copy, "copy", p);
     P.ready[p] = b->ready[p];
   }
   P.rp_local = b->rp_local;
@@ -1881,6 +1934,7 @@ int mce_batch_count_host(mce_batch_t b, const int32_t *row_ptr, const int32_t *c
   bc.g_mid = b->g_mid;
   rc = pipelined ? count_pipelined(b->g, o, total, hist, stats, &bc)
                  : count_impl(b->g, o, total, hist, stats, &bc);
+  trace_dump(b->g);
   if (rc) cudaStreamSynchronize(b->copy);  // no copy outlives a failed call
   return rc;
 }
