@@ -14,7 +14,7 @@
 // it is at least 2% faster, and checks that every trial returns the same
 // count.  Then, bucket by bucket - the engine classes of the roots, by
 // bitmap width: d+ <= 32, 33..64, wider - it walks that bucket's warps per
-// root, donation threshold and donation gate, judged by the bucket's own
+// root, donation threshold and donation gate, scored by the bucket's own
 // launch time (the classes run one after the other, so a bucket's settings
 // do not move the others' times).  The winners are stored in a text table:
 // one line per shape class and one per bucket of it ("<class>:b32",
@@ -269,7 +269,7 @@ int tune(const char *key, const mce_opts_t &base, const char *table_path, int32_
     cur = best;
     cur_ms = best_ms;
   }
-  // per bucket: warps per root, donation threshold and gate, each judged by
+  // per bucket: warps per root, donation threshold and gate, each scored by
   // the bucket's own launch time
   Entry ent{cur, cur_ms, out->default_ms, {}};
   mce_opts_t o = base;
